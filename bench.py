@@ -1,0 +1,307 @@
+"""SCC throughput benchmark (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl kspn|reference]
+                    [--workload rmat24|rmat26|rgg24|gnm16] [--pipeline fast|reference]
+
+A step is one complete decomposition of the workload graph (strongly
+connected components, canonical min-id labels).  Default workload: directed
+R-MAT scale 24, edge factor 16, a,b,c,d = .57,.19,.19,.05, seeded id
+permutation, self-loops and duplicates removed, u32 ids, u64 offsets --
+generated on the device by the library's own seeded generator.
+
+value   = edges of the graph / device time per step (CUDA events on the
+          library's stream; graph and transpose resident in HBM, > L2).
+e2e     = the same metric through the host C-ABI call kspn_scc with pinned
+          HOST buffers: forward CSR copied in, transpose built on the device,
+          labels copied out, every step.
+roofline: the dominant kernel class's algorithmic bytes / its event-timed
+          duration, against MEASURED_PEAKS.json's HBM copy bandwidth.
+cpu_baseline: the reference's own kaspan::scc (oracle/_ref, compiled from its
+          sources; 1 core, MPI absent) on a bounded sample of the workload.
+
+Multi-GPU (torchrun): every rank decomposes its own seeded instance (seed +
+rank); value = edges over all ranks / max-over-ranks time ("weak" scaling,
+no data-path collective).  --impl reference runs on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SCC edges/sec on 1 B200 (learned vs plain pivots, exact) + % HBM roofline"
+UNIT = "edges/s"
+
+WORKLOADS = {
+    # name: (kind, params, description)
+    "rmat24": ("rmat", dict(scale=24, ef=16, seed=2), "R-MAT scale 24, edge factor 16, a,b,c,d=.57,.19,.19,.05, permuted ids"),
+    "rmat26": ("rmat", dict(scale=26, ef=16, seed=4), "R-MAT scale 26, edge factor 16, a,b,c,d=.57,.19,.19,.05, permuted ids"),
+    "gnm16": ("gnm", dict(n=1 << 16, draws=1 << 19, seed=1), "directed G(n,m) n=2^16, 2^19 draws"),
+    "rmat22": ("rmat", dict(scale=22, ef=16, seed=2), "R-MAT scale 22, edge factor 16, a,b,c,d=.57,.19,.19,.05, permuted ids"),
+}
+# bounded CPU sample of each workload for the reference arm / cpu_baseline
+CPU_SAMPLE = {"rmat24": "rmat22", "rmat26": "rmat22", "gnm16": "gnm16", "rmat22": "rmat22"}
+
+
+def measured_peak_gbs():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = [r.split(", ") for r in (self.out or "").strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_graph(ctx, name, rank_seed=0):
+    import kaspan_b200.graphs as KG
+
+    kind, p, _ = WORKLOADS[name]
+    if kind == "rmat":
+        return KG.rmat(ctx, p["scale"], p["ef"], p["seed"] + rank_seed)
+    return KG.gnm(ctx, p["n"], p["draws"], p["seed"] + rank_seed)
+
+
+def cpu_reference_sample(name, steps=1, warmup=0, threads_note=True):
+    """Reference kaspan::scc (oracle/_ref) on the CPU sample of `name`:
+    returns (edges/s list per timed step, sample description, m)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    if O.ref_lib() is None:
+        return None
+    sname = CPU_SAMPLE[name]
+    kind, p, desc = WORKLOADS[sname]
+    G = O.rmat(p["scale"], p["ef"], p["seed"]) if kind == "rmat" else O.gnm(p["n"], p["draws"], p["seed"])
+    for _ in range(warmup):
+        O.ref_scc(G)
+    rates = []
+    for _ in range(steps):
+        _, secs = O.ref_scc(G)
+        rates.append(G.m / secs)
+    return rates, f"{desc}: n={G.n}, m={G.m}; one kaspan::scc call per step (reference code, 1 rank, 1 core)", G.m
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    res = cpu_reference_sample(args.workload, steps=args.steps, warmup=args.warmup)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libkspn_ref.so was not built (reference sources absent at build time)"}))
+        return 0
+    rates, sample, m = res
+    v = statistics.mean(rates)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * m / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded generators standing in for KaGen R-MAT / G(n,m))",
+        "config": {"workload": WORKLOADS[args.workload][2], "sample": sample, "mpi": "absent on this host: single rank"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_kspn(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import kaspan_b200 as K
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    stream = torch.cuda.current_stream()
+    ctx = K.Context(local, stream=stream)
+    G = make_graph(ctx, args.workload, rank_seed=rank)
+    torch.cuda.synchronize()
+    out = torch.empty(G.n, dtype=torch.int32, device="cuda")
+    opt = K.default_options(pipeline=K.PIPELINE_FAST if args.pipeline == "fast" else K.PIPELINE_REFERENCE, validate=0, profile=1)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident steps
+    st = K.Stats()
+    for _ in range(args.warmup):
+        ctx.scc_device(G.n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, opt, st)
+    agg = {k: [0.0, 0, 0] for k in K.KERNEL_CLASSES}
+    step_stats = []
+    barrier()
+    l0 = ctx.launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            ctx.scc_device(G.n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, opt, st)
+            d = st.as_dict()
+            step_stats.append(d)
+            for k, v in d["kernels"].items():
+                agg[k][0] += v["ms"]
+                agg[k][1] += v["bytes"]
+                agg[k][2] += v["calls"]
+        ev1.record(stream)
+        barrier()
+    launches = ctx.launches - l0
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        mt = torch.tensor([float(G.m)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(mt)
+        m_total = float(mt.item())
+    else:
+        m_total = float(G.m)
+    value = m_total / (ms * 1e-3)
+
+    # correctness spot check of the last step (canonical ids are min members)
+    ids = out.cpu().numpy().view(np.uint32)
+    assert (ids <= np.arange(G.n, dtype=np.uint32)).all(), "ids must name a member no larger than the vertex"
+
+    # ---- end to end through the host C ABI (pinned buffers, bw built on device)
+    fwh_h = G.fwh.cpu().pin_memory()
+    fwc_h = G.fwc.cpu().pin_memory()
+    out_h = torch.empty(G.n, dtype=torch.int32).pin_memory()
+    e2e_opt = K.default_options(pipeline=opt.pipeline, validate=0)
+    for _ in range(max(1, min(args.warmup, 2))):
+        ctx.scc_host_ptr(G.n, G.m, fwh_h, fwc_h, None, None, out_h, e2e_opt)
+    barrier()
+    e2e_steps = max(1, min(args.steps, 5))
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(e2e_steps):
+        ctx.scc_host_ptr(G.n, G.m, fwh_h, fwc_h, None, None, out_h, e2e_opt)
+    ev1.record(stream)
+    barrier()
+    e2e_ms = max(ev0.elapsed_time(ev1), (time.perf_counter() - t0) * 1e3) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    assert np.array_equal(out_h.numpy().view(np.uint32), ids), "host path and device path disagree"
+    h2d = 8 * (G.n + 1) + 4 * G.m
+    d2h = 4 * G.n
+
+    # ---- roofline of the dominant kernel class
+    peak, peak_kind = measured_peak_gbs()
+    dom = max(agg, key=lambda k: agg[k][0])
+    kms, kbytes, kcalls = agg[dom]
+    achieved = (kbytes / (kms * 1e-3)) / 1e9 if kms > 0 else 0.0
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get(f"{args.workload}:{dom}")
+        except Exception:
+            traffic = None
+    last = step_stats[-1]
+    b_min = 2 * (8 * (G.n + 1) + 4 * G.m) + 4 * G.n
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded device generator standing in for KaGen; graph > L2 so no flush between steps)",
+            "config": {"workload": WORKLOADS[args.workload][2], "n": G.n, "m": G.m, "pipeline": args.pipeline,
+                       "parallelism": f"{world} independent instance(s), one per GPU", "l2": "inputs larger than L2 (126 MB)"},
+            "e2e": {"value": m_total / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
+                         "bytes_per_step": kbytes / args.steps, "ms_per_step": kms / args.steps, "calls_per_step": kcalls / args.steps,
+                         "pipeline_min_bytes": b_min, "pipeline_frac": (b_min / (ms * 1e-3)) / 1e9 / peak},
+            "clocks": clk.summary(),
+            "phases": {"decided": last["decided"], "ms": {k: round(v, 4) for k, v in last["ms"].items()}, "levels_fw": last["levels_fw"],
+                       "levels_bw": last["levels_bw"], "bottom_up": last["levels_bottom_up"], "label_calls": last["label_calls"],
+                       "edges_scanned": last["edges_scanned"], "kernels": {k: {"ms": round(a[0] / args.steps, 4), "GB/s": round(a[1] / (a[0] * 1e-3) / 1e9, 1) if a[0] else 0}
+                                                                            for k, a in agg.items()}},
+        }
+        if not args.no_cpu_baseline:
+            res = cpu_reference_sample(args.workload, steps=1, warmup=0)
+            if res is not None:
+                rates, sample, _ = res
+                line["cpu_baseline"] = {"value": rates[0], "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample}
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="kspn", choices=["kspn", "reference"])
+    ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS))
+    ap.add_argument("--pipeline", default="fast", choices=["fast", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "kspn":
+        args.warmup = 3
+    return run_reference(args) if args.impl == "reference" else run_kspn(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

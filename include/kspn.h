@@ -1,0 +1,234 @@
+/*
+ * kspn -- strongly connected components of a directed graph on one NVIDIA
+ * B200, as a drop-in for the `scc` entry point of rawbby/KaSpan.
+ *
+ * C ABI: plain pointers and sizes, no exceptions cross it, every entry point
+ * returns a status (KSPN_OK or a KSPN_ERR_* code, see kspn_strerror).
+ *
+ * Graph layout everywhere: n vertices with u32 ids; forward CSR
+ * fw_head[n+1] (u64 offsets) / fw_csr[m] (u32 neighbour ids) and its
+ * transpose bw_head / bw_csr.  This is the reference's
+ * bidi_graph_part_view at one rank built with KASPAN_INDEX64
+ * (kaspan/graph/bidi_graph_part.hpp:12-28, kaspan/graph/base.hpp:18-28).
+ * Duplicate edges and self-loops are allowed, as in the reference.
+ *
+ * Output contract: scc_id[v] is the MINIMUM vertex id of v's strongly
+ * connected component.  The reference promises "some member of the
+ * component" (tool/bench_kaspan/src/main.cpp:74-80); the minimum member is
+ * one, and it is what kaspan::normalise_scc_id (kaspan/test/normalise_scc.hpp:10-25)
+ * produces, so outputs compare bit for bit after that relabel.
+ *
+ * Vertex-state bitsets in the phase-level entry points use the reference's
+ * bits layout: ceil(n/64) u64 words, bit v%64 of word v/64 set = vertex v
+ * undecided (kaspan/memory/bits_ops.hpp).
+ */
+#ifndef KSPN_H
+#define KSPN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define KSPN_OK 0
+#define KSPN_ERR_INVALID_ARGUMENT 1 /* null pointer, bad size, unknown option */
+#define KSPN_ERR_INVALID_GRAPH 2    /* offsets not monotone / out of range, id >= n */
+#define KSPN_ERR_OOM 3              /* device or pinned allocation failed */
+#define KSPN_ERR_TIMEOUT 4          /* an iteration cap or wait limit was hit */
+#define KSPN_ERR_CUDA 5             /* a CUDA runtime call failed */
+#define KSPN_ERR_NO_DEVICE 6        /* no usable CUDA device */
+#define KSPN_ERR_INTERNAL 7         /* a device-side consistency check failed */
+
+#define KSPN_UNDECIDED 0xFFFFFFFFu /* reference: scc_id_undecided, kaspan/graph/base.hpp:135 */
+
+/* ---------------------------------------------------------------- options */
+#define KSPN_PIPELINE_FAST 0      /* trim fixpoint, pivot FW-BW, label rounds, residual finish */
+#define KSPN_PIPELINE_REFERENCE 1 /* the phase order of kaspan::scc (kaspan/scc/scc.hpp:21-87) */
+
+typedef struct kspn_options
+{
+  uint32_t struct_size;     /* sizeof(kspn_options); filled by kspn_options_default */
+  int32_t  pipeline;        /* KSPN_PIPELINE_* */
+  int32_t  trim2;           /* 1: run the exact size-2 trim in the fast pipeline */
+  int32_t  validate;        /* 1: check the CSR (monotone offsets, ids < n) before running */
+  uint32_t bu_enter_div;    /* reachability: go bottom-up when frontier > undecided / this */
+  uint32_t bu_leave_div;    /* ... and back top-down when frontier < undecided / this */
+  uint32_t max_levels;      /* cap on reachability levels per search (0 = n + 2) */
+  uint32_t max_label_iters; /* cap on label-propagation sweeps per search (0 = n + 2) */
+  uint32_t max_rounds;      /* cap on pipeline rounds (0 = n + 2) */
+  int32_t  profile;         /* 1: time kernel classes with CUDA events (kspn_stats.kernel_*) */
+  uint32_t reserved[6];
+} kspn_options;
+
+/* Per-call statistics (all fields written by a successful call). */
+#define KSPN_PHASES 8
+#define KSPN_PHASE_TRIM_FIRST 0
+#define KSPN_PHASE_TRIM 1
+#define KSPN_PHASE_FWBW 2
+#define KSPN_PHASE_TRIM_NORMAL 3
+#define KSPN_PHASE_LABEL 4
+#define KSPN_PHASE_TRIM2 5
+#define KSPN_PHASE_RESIDUAL 6
+#define KSPN_PHASE_CANON 7
+/* Kernel classes timed when kspn_options.profile is set.  Bytes follow the
+ * algorithmic model: 16 B per adjacency row opened (two u64 offsets), 4 B
+ * per neighbour id read, 4 B per state probe of that neighbour, 4 B per
+ * queue entry read or written and per id written; bitmap sweeps n/8 B. */
+#define KSPN_KERNEL_CLASSES 4
+#define KSPN_KERNEL_EXPAND 0    /* top-down frontier expansion (reachability, labels) */
+#define KSPN_KERNEL_BOTTOM_UP 1 /* bottom-up reachability sweep */
+#define KSPN_KERNEL_TRIM 2      /* trim push levels + live-degree counting */
+#define KSPN_KERNEL_STREAM 3    /* trim_1_first pass */
+typedef struct kspn_stats
+{
+  uint32_t n;
+  uint64_t m;
+  uint64_t decided[KSPN_PHASES];       /* vertices decided per phase */
+  double   ms[KSPN_PHASES];            /* device time per phase (CUDA events) */
+  double   ms_total;                   /* device time of the whole call, inputs resident */
+  uint64_t edges_scanned;              /* adjacency entries read by reachability + label kernels */
+  uint32_t pivot;                      /* first FW-BW pivot (n if none) */
+  uint32_t levels_fw, levels_bw;       /* reachability levels of the first FW-BW */
+  uint32_t levels_bottom_up;           /* of those, bottom-up sweeps */
+  uint32_t label_calls;                /* label searches run */
+  uint32_t rounds;                     /* pipeline rounds after the first FW-BW */
+  uint64_t kernel_launches;            /* kspn kernels launched by the call */
+  double   kernel_ms[KSPN_KERNEL_CLASSES];       /* event-timed device ms per class */
+  uint64_t kernel_bytes[KSPN_KERNEL_CLASSES];    /* algorithmic bytes per class */
+  uint64_t kernel_calls[KSPN_KERNEL_CLASSES];    /* timed launches per class */
+} kspn_stats;
+
+typedef struct kspn_context kspn_context;
+
+/* ---------------------------------------------------------------- lifetime */
+int         kspn_options_default(kspn_options* opt);
+const char* kspn_strerror(int status);
+const char* kspn_last_error(const kspn_context* ctx); /* detail of the last failure on ctx */
+int         kspn_context_create(int device, kspn_context** out);
+/* Uses a caller stream (cudaStream_t passed as void*); NULL = a new stream. */
+int         kspn_context_create_on_stream(int device, void* stream, kspn_context** out);
+int         kspn_context_destroy(kspn_context* ctx);
+int         kspn_context_synchronize(kspn_context* ctx);
+/* Number of kspn kernel launches made on ctx since it was created. */
+uint64_t    kspn_context_launches(const kspn_context* ctx);
+
+/* ---------------------------------------------------------------- whole path */
+/*
+ * Replaces kaspan::scc(bidi_graph_part_view<single_part_view>, vertex_t*)
+ * (kaspan/scc/scc.hpp:21-25).  HOST pointers: the graph is copied to the
+ * device, the result copied back into scc_id[n].  bw_head/bw_csr may both be
+ * NULL: the transpose is then built on the device (the reference's
+ * backward_complement_graph, kaspan/scc/backward_complement.hpp:22-68).
+ * ctx may be NULL (a context on device 0 is created for the call).
+ */
+int kspn_scc(kspn_context* ctx, uint32_t n, uint64_t m,
+             const uint64_t* fw_head, const uint32_t* fw_csr,
+             const uint64_t* bw_head, const uint32_t* bw_csr,
+             uint32_t* scc_id, const kspn_options* opt, kspn_stats* stats);
+
+/* Same with DEVICE pointers, on ctx's stream, inputs left untouched.
+ * bw_head/bw_csr may be NULL (transpose built in ctx's workspace). */
+int kspn_scc_device(kspn_context* ctx, uint32_t n, uint64_t m,
+                    const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
+                    const uint64_t* d_bw_head, const uint32_t* d_bw_csr,
+                    uint32_t* d_scc_id, const kspn_options* opt, kspn_stats* stats);
+
+/* ---------------------------------------------------------------- phases */
+/*
+ * Phase-level entry points on DEVICE pointers.  Each mirrors one reference
+ * function at one rank; `undecided` is the reference bitset (see top),
+ * scc_id receives the same member ids the reference writes.
+ */
+
+/* trim_1_first (kaspan/scc/trim_1_local.hpp:12-46): decide in- or
+ * out-degree-0 vertices (id = itself); *pivot = argmax in*out over the
+ * rest, lowest id on ties, n if none.  undecided is written in full. */
+int kspn_trim_1_first(kspn_context* ctx, uint32_t n, uint64_t m,
+                      const uint64_t* d_fw_head, const uint64_t* d_bw_head,
+                      uint64_t* d_undecided, uint32_t* d_scc_id, uint32_t* pivot);
+
+/* cache_forward_backward_search / forward_backward_search
+ * (kaspan/scc/cache_pivot_search.hpp:16-104, pivot_search.hpp:15-85). */
+int kspn_forward_backward_search(kspn_context* ctx, uint32_t n, uint64_t m,
+                                 const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
+                                 const uint64_t* d_bw_head, const uint32_t* d_bw_csr,
+                                 uint64_t* d_undecided, uint32_t* d_scc_id, uint32_t pivot,
+                                 uint32_t* decided);
+
+/* trim_1_normal (kaspan/scc/trim_1_local.hpp:48-73). */
+int kspn_trim_1_normal(kspn_context* ctx, uint32_t n, uint64_t m,
+                       const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
+                       const uint64_t* d_bw_head, const uint32_t* d_bw_csr,
+                       uint64_t* d_undecided, uint32_t* d_scc_id, uint32_t* decided);
+
+/* One cache_label_search_pull with map = rotr(., rotation)
+ * (kaspan/scc/cache_multi_pivot_search_pull.hpp:40-244; the rotated
+ * wrapper :246-266 draws rotation from a process-global counter, here the
+ * caller passes it).  d_label (nullable, n entries) receives the labels. */
+int kspn_label_search(kspn_context* ctx, uint32_t n, uint64_t m,
+                      const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
+                      const uint64_t* d_bw_head, const uint32_t* d_bw_csr,
+                      uint64_t* d_undecided, uint32_t* d_scc_id, int rotation,
+                      uint32_t* d_label, uint32_t* decided);
+
+/* trim_1_exhaustive_first (kaspan/scc/trim_1_exhaustive.hpp:71-131):
+ * in-degree sweep to its fixpoint, then out-degree sweep; d_outdegree /
+ * d_indegree receive the live degree arrays it leaves. */
+int kspn_trim_1_exhaustive_first(kspn_context* ctx, uint32_t n, uint64_t m,
+                                 const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
+                                 const uint64_t* d_bw_head, const uint32_t* d_bw_csr,
+                                 uint64_t* d_undecided, uint32_t* d_scc_id,
+                                 uint32_t* d_outdegree, uint32_t* d_indegree, uint32_t* decided);
+
+/* Trim-1 to its fixpoint in both directions on the undecided sub-graph
+ * (what alternating trim_1_exhaustive fw/bw converges to,
+ * kaspan/scc/trim_1_exhaustive.hpp:48-69). */
+int kspn_trim_1_fixpoint(kspn_context* ctx, uint32_t n, uint64_t m,
+                         const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
+                         const uint64_t* d_bw_head, const uint32_t* d_bw_csr,
+                         uint64_t* d_undecided, uint32_t* d_scc_id, uint32_t* decided);
+
+/* Exact size-2 trim (no reference counterpart; an addition): decides
+ * undecided pairs {u,v} where u's only undecided out-neighbour is v and v's
+ * is u, or the same with in-neighbours. */
+int kspn_trim_2(kspn_context* ctx, uint32_t n, uint64_t m,
+                const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
+                const uint64_t* d_bw_head, const uint32_t* d_bw_csr,
+                uint64_t* d_undecided, uint32_t* d_scc_id, uint32_t* decided);
+
+/* normalise_scc_id (kaspan/test/normalise_scc.hpp:10-25) on the device:
+ * every id becomes the minimum vertex carrying it.  Ids must be < n. */
+int kspn_normalise(kspn_context* ctx, uint32_t n, uint32_t* d_scc_id);
+
+/* backward_complement_graph (kaspan/scc/backward_complement.hpp:22-68) on
+ * the device: d_bw_head[n+1] / d_bw_csr[m] receive the transpose with rows
+ * in ascending order. */
+int kspn_transpose(kspn_context* ctx, uint32_t n, uint64_t m,
+                   const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
+                   uint64_t* d_bw_head, uint32_t* d_bw_csr);
+
+/* ---------------------------------------------------------------- inputs */
+/*
+ * Seeded synthetic edge lists on the device (no reference counterpart:
+ * they stand in for the KaGen generators the reference benchmarks with).
+ * Draw i of a stream is SplitMix64's finaliser applied to key + (i+1)*gamma.
+ */
+int kspn_gen_gnm(kspn_context* ctx, uint32_t n, uint64_t draws, uint64_t seed,
+                 uint32_t* d_src, uint32_t* d_dst);
+int kspn_gen_rmat(kspn_context* ctx, int scale, uint64_t draws, uint64_t seed,
+                  uint64_t t_a, uint64_t t_ab, uint64_t t_abc, int permute,
+                  uint32_t* d_src, uint32_t* d_dst);
+/* Edge list -> CSR with self-loops and duplicates removed, rows ascending.
+ * d_src/d_dst are overwritten (used as scratch).  *m_out = edges kept. */
+int kspn_build_csr(kspn_context* ctx, uint32_t n, uint64_t m_raw,
+                   uint32_t* d_src, uint32_t* d_dst,
+                   uint64_t* d_head, uint32_t* d_csr, uint64_t* m_out);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* KSPN_H */

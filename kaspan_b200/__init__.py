@@ -1,0 +1,308 @@
+"""kaspan_b200 -- strongly connected components on one NVIDIA B200.
+
+Python view of the C ABI in include/kspn.h (libkspn.so, built from
+kaspan_b200/csrc by ``python -m kaspan_b200.build``).  There is no CPU
+fallback: every call runs the CUDA library, and importing the bindings fails
+loudly when the library is missing.
+
+Whole path (the reference's ``kaspan::scc(bidi_graph_part_view, vertex_t*)``,
+kaspan/scc/scc.hpp:21-25):
+
+    ids = kaspan_b200.scc(n, fw_head, fw_csr, bw_head, bw_csr)  # numpy, host
+    ctx.scc_device(n, m, fwh, fwc, bwh, bwc, out)                # torch cuda
+
+Output: ids[v] = minimum vertex id of v's strongly connected component.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libkspn.so")
+
+PIPELINE_FAST = 0
+PIPELINE_REFERENCE = 1
+UNDECIDED = 0xFFFFFFFF
+
+STATUS = {
+    0: "KSPN_OK",
+    1: "KSPN_ERR_INVALID_ARGUMENT",
+    2: "KSPN_ERR_INVALID_GRAPH",
+    3: "KSPN_ERR_OOM",
+    4: "KSPN_ERR_TIMEOUT",
+    5: "KSPN_ERR_CUDA",
+    6: "KSPN_ERR_NO_DEVICE",
+    7: "KSPN_ERR_INTERNAL",
+}
+
+PHASES = ["trim_first", "trim", "fwbw", "trim_normal", "label", "trim2", "residual", "canon"]
+KERNEL_CLASSES = ["expand", "bottom_up", "trim", "stream"]
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("pipeline", C.c_int32),
+        ("trim2", C.c_int32),
+        ("validate", C.c_int32),
+        ("bu_enter_div", C.c_uint32),
+        ("bu_leave_div", C.c_uint32),
+        ("max_levels", C.c_uint32),
+        ("max_label_iters", C.c_uint32),
+        ("max_rounds", C.c_uint32),
+        ("profile", C.c_int32),
+        ("reserved", C.c_uint32 * 6),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("n", C.c_uint32),
+        ("m", C.c_uint64),
+        ("decided", C.c_uint64 * 8),
+        ("ms", C.c_double * 8),
+        ("ms_total", C.c_double),
+        ("edges_scanned", C.c_uint64),
+        ("pivot", C.c_uint32),
+        ("levels_fw", C.c_uint32),
+        ("levels_bw", C.c_uint32),
+        ("levels_bottom_up", C.c_uint32),
+        ("label_calls", C.c_uint32),
+        ("rounds", C.c_uint32),
+        ("kernel_launches", C.c_uint64),
+        ("kernel_ms", C.c_double * 4),
+        ("kernel_bytes", C.c_uint64 * 4),
+        ("kernel_calls", C.c_uint64 * 4),
+    ]
+
+    def as_dict(self) -> dict:
+        return {
+            "n": self.n,
+            "m": self.m,
+            "decided": {p: int(self.decided[i]) for i, p in enumerate(PHASES)},
+            "ms": {p: float(self.ms[i]) for i, p in enumerate(PHASES)},
+            "ms_total": self.ms_total,
+            "edges_scanned": int(self.edges_scanned),
+            "pivot": self.pivot,
+            "levels_fw": self.levels_fw,
+            "levels_bw": self.levels_bw,
+            "levels_bottom_up": self.levels_bottom_up,
+            "label_calls": self.label_calls,
+            "rounds": self.rounds,
+            "kernel_launches": int(self.kernel_launches),
+            "kernels": {k: {"ms": float(self.kernel_ms[i]), "bytes": int(self.kernel_bytes[i]), "calls": int(self.kernel_calls[i])}
+                        for i, k in enumerate(KERNEL_CLASSES)},
+        }
+
+
+class KspnError(RuntimeError):
+    def __init__(self, status: int, detail: str = ""):
+        self.status = status
+        super().__init__(f"{STATUS.get(status, status)}: {detail}")
+
+
+# every symbol include/kspn.h declares, with its ctypes signature
+_P = C.c_void_p
+_u32, _u64, _i32 = C.c_uint32, C.c_uint64, C.c_int
+SIGNATURES = {
+    "kspn_options_default": (_i32, [_P]),
+    "kspn_strerror": (C.c_char_p, [_i32]),
+    "kspn_last_error": (C.c_char_p, [_P]),
+    "kspn_context_create": (_i32, [_i32, _P]),
+    "kspn_context_create_on_stream": (_i32, [_i32, _P, _P]),
+    "kspn_context_destroy": (_i32, [_P]),
+    "kspn_context_synchronize": (_i32, [_P]),
+    "kspn_context_launches": (_u64, [_P]),
+    "kspn_scc": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P]),
+    "kspn_scc_device": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P]),
+    "kspn_trim_1_first": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P]),
+    "kspn_forward_backward_search": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _u32, _P]),
+    "kspn_trim_1_normal": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P]),
+    "kspn_label_search": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _i32, _P, _P]),
+    "kspn_trim_1_exhaustive_first": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "kspn_trim_1_fixpoint": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P]),
+    "kspn_trim_2": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P]),
+    "kspn_normalise": (_i32, [_P, _u32, _P]),
+    "kspn_transpose": (_i32, [_P, _u32, _u64, _P, _P, _P, _P]),
+    "kspn_gen_gnm": (_i32, [_P, _u32, _u64, _u64, _P, _P]),
+    "kspn_gen_rmat": (_i32, [_P, _i32, _u64, _u64, _u64, _u64, _u64, _i32, _P, _P]),
+    "kspn_build_csr": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The CUDA library; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libkspn.so not found at {LIB_PATH}; build it with `python -m kaspan_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    lib().kspn_options_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def _ptr(x) -> int | None:
+    """Device/host address of a torch tensor or numpy array (None passes through)."""
+    if x is None:
+        return None
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if isinstance(x, int):
+        return x
+    raise TypeError(f"cannot take the address of {type(x)}")
+
+
+class Context:
+    """One kspn_context: a device, a stream, a reusable workspace."""
+
+    def __init__(self, device: int = 0, stream=None):
+        L = lib()
+        h = C.c_void_p()
+        if stream is None:
+            rc = L.kspn_context_create(device, C.byref(h))
+        else:
+            s = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+            rc = L.kspn_context_create_on_stream(device, C.c_void_p(s), C.byref(h))
+        if rc != 0:
+            raise KspnError(rc, "context creation")
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if self.h:
+            lib().kspn_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            detail = lib().kspn_last_error(self.h)
+            raise KspnError(rc, f"{what}: {detail.decode() if detail else ''}")
+
+    @property
+    def launches(self) -> int:
+        return int(lib().kspn_context_launches(self.h))
+
+    def synchronize(self):
+        self._check(lib().kspn_context_synchronize(self.h), "synchronize")
+
+    # ---- whole path
+    def scc(self, n, fw_head, fw_csr, bw_head=None, bw_csr=None, out=None, options=None, stats=None):
+        """Host (numpy) arrays in, canonical ids out (numpy uint32[n])."""
+        fw_head = np.ascontiguousarray(fw_head, dtype=np.uint64)
+        m = int(fw_head[n]) if n else 0
+        fw_csr = np.ascontiguousarray(fw_csr, dtype=np.uint32)
+        if bw_head is not None:
+            bw_head = np.ascontiguousarray(bw_head, dtype=np.uint64)
+            bw_csr = np.ascontiguousarray(bw_csr, dtype=np.uint32)
+        if out is None:
+            out = np.empty(max(n, 1), np.uint32)
+        opt = options if options is not None else default_options()
+        rc = lib().kspn_scc(self.h, n, m, _ptr(fw_head), _ptr(fw_csr), _ptr(bw_head), _ptr(bw_csr), _ptr(out),
+                            C.byref(opt), C.byref(stats) if stats is not None else None)
+        self._check(rc, "kspn_scc")
+        return out[:n]
+
+    def scc_host_ptr(self, n, m, fwh, fwc, bwh, bwc, out, options=None, stats=None):
+        """Host pointers (pinned torch tensors or numpy), result into `out`."""
+        opt = options if options is not None else default_options()
+        rc = lib().kspn_scc(self.h, n, m, _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc), _ptr(out),
+                            C.byref(opt), C.byref(stats) if stats is not None else None)
+        self._check(rc, "kspn_scc")
+
+    def scc_device(self, n, m, fwh, fwc, bwh, bwc, out, options=None, stats=None):
+        """Device pointers (torch cuda tensors); result into `out`."""
+        opt = options if options is not None else default_options()
+        rc = lib().kspn_scc_device(self.h, n, m, _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc), _ptr(out),
+                                   C.byref(opt), C.byref(stats) if stats is not None else None)
+        self._check(rc, "kspn_scc_device")
+
+    # ---- phases (device pointers)
+    def trim_1_first(self, n, m, fwh, bwh, und, scc_id) -> int:
+        pivot = C.c_uint32()
+        self._check(lib().kspn_trim_1_first(self.h, n, m, _ptr(fwh), _ptr(bwh), _ptr(und), _ptr(scc_id), C.byref(pivot)), "trim_1_first")
+        return pivot.value
+
+    def forward_backward_search(self, n, m, fwh, fwc, bwh, bwc, und, scc_id, pivot) -> int:
+        d = C.c_uint32()
+        self._check(lib().kspn_forward_backward_search(self.h, n, m, _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc), _ptr(und), _ptr(scc_id), pivot, C.byref(d)), "forward_backward_search")
+        return d.value
+
+    def trim_1_normal(self, n, m, fwh, fwc, bwh, bwc, und, scc_id) -> int:
+        d = C.c_uint32()
+        self._check(lib().kspn_trim_1_normal(self.h, n, m, _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc), _ptr(und), _ptr(scc_id), C.byref(d)), "trim_1_normal")
+        return d.value
+
+    def label_search(self, n, m, fwh, fwc, bwh, bwc, und, scc_id, rotation, label=None) -> int:
+        d = C.c_uint32()
+        self._check(lib().kspn_label_search(self.h, n, m, _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc), _ptr(und), _ptr(scc_id), rotation, _ptr(label), C.byref(d)), "label_search")
+        return d.value
+
+    def trim_1_exhaustive_first(self, n, m, fwh, fwc, bwh, bwc, und, scc_id, outdeg, indeg) -> int:
+        d = C.c_uint32()
+        self._check(lib().kspn_trim_1_exhaustive_first(self.h, n, m, _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc), _ptr(und), _ptr(scc_id), _ptr(outdeg), _ptr(indeg), C.byref(d)), "trim_1_exhaustive_first")
+        return d.value
+
+    def trim_1_fixpoint(self, n, m, fwh, fwc, bwh, bwc, und, scc_id) -> int:
+        d = C.c_uint32()
+        self._check(lib().kspn_trim_1_fixpoint(self.h, n, m, _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc), _ptr(und), _ptr(scc_id), C.byref(d)), "trim_1_fixpoint")
+        return d.value
+
+    def trim_2(self, n, m, fwh, fwc, bwh, bwc, und, scc_id) -> int:
+        d = C.c_uint32()
+        self._check(lib().kspn_trim_2(self.h, n, m, _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc), _ptr(und), _ptr(scc_id), C.byref(d)), "trim_2")
+        return d.value
+
+    def normalise(self, n, scc_id):
+        self._check(lib().kspn_normalise(self.h, n, _ptr(scc_id)), "normalise")
+
+    def transpose(self, n, m, fwh, fwc, bwh, bwc):
+        self._check(lib().kspn_transpose(self.h, n, m, _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc)), "transpose")
+
+    # ---- inputs
+    def gen_gnm(self, n, draws, seed, src, dst):
+        self._check(lib().kspn_gen_gnm(self.h, n, draws, seed, _ptr(src), _ptr(dst)), "gen_gnm")
+
+    def gen_rmat(self, scale, draws, seed, ta, tab, tabc, permute, src, dst):
+        self._check(lib().kspn_gen_rmat(self.h, scale, draws, seed, ta, tab, tabc, int(permute), _ptr(src), _ptr(dst)), "gen_rmat")
+
+    def build_csr(self, n, m_raw, src, dst, head, csr) -> int:
+        m = C.c_uint64()
+        self._check(lib().kspn_build_csr(self.h, n, m_raw, _ptr(src), _ptr(dst), _ptr(head), _ptr(csr), C.byref(m)), "build_csr")
+        return m.value
+
+
+def scc(n, fw_head, fw_csr, bw_head=None, bw_csr=None, options=None, device: int = 0):
+    """One-shot host call: canonical SCC ids (numpy uint32[n])."""
+    with Context(device) as ctx:
+        return ctx.scc(n, fw_head, fw_csr, bw_head, bw_csr, options=options).copy()

@@ -1,0 +1,667 @@
+// C ABI of libkspn: contexts, workspace, the whole-path entry points and the
+// phase-level entry points (include/kspn.h).  No exception crosses the ABI:
+// every entry point catches, records the detail on the context and returns
+// a KSPN_ERR_* status.
+//
+// Pipelines (both end in the canonical min-id relabel):
+//  REFERENCE  the phase order of kaspan::scc (kaspan/scc/scc.hpp:21-87):
+//             trim_1_first -> FW-BW(pivot) -> trim_1_normal -> label
+//             searches with rotation 1, 2, 3, ... until every vertex is
+//             decided.
+//  FAST       trim_1_first -> trim-1 fixpoint -> FW-BW from the live
+//             degree-product pivot -> rounds of {trim-1 fixpoint, trim-2,
+//             label search} until every vertex is decided.  Same partition
+//             (every phase only decides whole SCCs).
+#include "kspn_internal.cuh"
+
+#include "prim.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+
+namespace kspn {
+
+namespace {
+
+constexpr size_t ALIGN = 256;
+
+size_t
+align_up(size_t x)
+{
+  return (x + ALIGN - 1) & ~(ALIGN - 1);
+}
+
+struct carver
+{
+  char*  base;
+  size_t off = 0;
+  template<typename T>
+  T* take(size_t count)
+  {
+    off    = align_up(off);
+    T* p   = base ? reinterpret_cast<T*>(base + off) : nullptr;
+    off += count * sizeof(T);
+    return p;
+  }
+};
+
+// Lays out (or, with base == nullptr, measures) the workspace.
+size_t
+layout(workspace& ws, char* base, uint32_t n, uint64_t m)
+{
+  carver         c{ base };
+  size_t const   words = (static_cast<size_t>(n) + 63) / 64 * 2 + 2; // u32 words, u64-rounded
+  size_t const   nn    = static_cast<size_t>(n) + 2;
+  ws.ctr               = c.take<uint32_t>(64);
+  ws.ctr64             = reinterpret_cast<uint64_t*>(ws.ctr ? ws.ctr + 32 : nullptr); // same block: one D2H copy
+  ws.q0                = c.take<uint32_t>(nn);
+  ws.q1                = c.take<uint32_t>(nn);
+  ws.vis_a             = c.take<uint32_t>(words);
+  ws.vis_b             = c.take<uint32_t>(words);
+  ws.mark              = c.take<uint32_t>(words);
+  ws.und               = c.take<uint32_t>(words);
+  ws.label             = c.take<uint32_t>(nn);
+  ws.indeg             = c.take<uint32_t>(nn);
+  ws.outdeg            = c.take<uint32_t>(nn);
+  ws.prefix            = c.take<uint64_t>(nn);
+  ws.blocks            = c.take<uint64_t>(std::max<size_t>(scan_partial_entries(nn), 4096));
+  ws.pivot             = c.take<uint64_t>(8192);
+  ws.tile_start        = c.take<uint32_t>(m / 2048 + 4);
+  return align_up(c.off);
+}
+
+} // namespace
+
+void
+ensure_workspace(kspn_context* ctx, uint32_t n, uint64_t m)
+{
+  auto& ws = ctx->ws;
+  if (ws.base && n <= ws.n_cap && m <= ws.m_cap) return;
+  uint32_t const ncap = std::max(n, ws.n_cap);
+  uint64_t const mcap = std::max(m, ws.m_cap);
+  if (ws.base) {
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+    cudaFree(ws.base);
+    ws.base = nullptr;
+  }
+  size_t const bytes = layout(ws, nullptr, ncap, mcap);
+  void*        p     = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    ws.n_cap = ws.m_cap = 0;
+    throw error{ KSPN_ERR_OOM, "workspace of " + std::to_string(bytes) + " bytes" };
+  }
+  ws.base  = p;
+  ws.bytes = bytes;
+  ws.n_cap = ncap;
+  ws.m_cap = mcap;
+  layout(ws, static_cast<char*>(p), ncap, mcap);
+  KSPN_CUDA(cudaMemsetAsync(ws.ctr, 0, 64 * sizeof(uint32_t), ctx->stream));
+}
+
+void
+read_counters(kspn_context* ctx)
+{
+  KSPN_CUDA(cudaMemcpyAsync(ctx->h_ctr, ctx->ws.ctr, 64 * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+  KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+void
+zero_counters(kspn_context* ctx)
+{
+  KSPN_CUDA(cudaMemsetAsync(ctx->ws.ctr, 0, CTR_COUNT * sizeof(uint32_t), ctx->stream));
+}
+
+int
+fail(kspn_context* ctx, error const& e)
+{
+  if (ctx) ctx->last_error = e.what;
+  return e.code;
+}
+
+namespace {
+
+// Owned device copy of a host graph (and a device-built transpose).
+struct graph_store
+{
+  void*  base  = nullptr;
+  size_t bytes = 0;
+  ~graph_store()
+  {
+    if (base) cudaFree(base);
+  }
+};
+
+void
+check_options(kspn_options const& o)
+{
+  if (o.pipeline != KSPN_PIPELINE_FAST && o.pipeline != KSPN_PIPELINE_REFERENCE) throw error{ KSPN_ERR_INVALID_ARGUMENT, "unknown pipeline" };
+}
+
+kspn_options
+options_or_default(kspn_options const* opt)
+{
+  kspn_options o;
+  kspn_options_default(&o);
+  if (opt) {
+    if (opt->struct_size != sizeof(kspn_options)) throw error{ KSPN_ERR_INVALID_ARGUMENT, "kspn_options.struct_size mismatch (use kspn_options_default)" };
+    o = *opt;
+  }
+  check_options(o);
+  return o;
+}
+
+struct phase_clock
+{
+  kspn_context* ctx;
+  kspn_stats*   st;
+  int           next = 1;
+  void          start() { KSPN_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream)); }
+  // attributes the device time since the previous mark to `phase`
+  void mark(int phase)
+  {
+    if (!st) return;
+    KSPN_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
+    KSPN_CUDA(cudaEventSynchronize(ctx->ev[1]));
+    float ms = 0;
+    KSPN_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    st->ms[phase] += ms;
+    std::swap(ctx->ev[0], ctx->ev[1]);
+  }
+};
+
+// The whole path on a resident graph; writes the canonical ids into scc_id.
+void
+run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options const& opt, kspn_stats* st)
+{
+  auto& ws = ctx->ws;
+  ensure_workspace(ctx, g.n, g.m);
+  if (st) {
+    std::memset(st, 0, sizeof(*st));
+    st->n     = g.n;
+    st->m     = g.m;
+    st->pivot = g.n;
+  }
+  uint64_t const launches0 = ctx->launches;
+  KSPN_CUDA(cudaMemsetAsync(ws.ctr, 0, 64 * sizeof(uint32_t), ctx->stream));
+  std::memset(ctx->h_ctr, 0, 64 * sizeof(uint32_t));
+  ctx->prof = (opt.profile && st) ? st : nullptr;
+  struct prof_reset
+  {
+    kspn_context* c;
+    ~prof_reset() { c->prof = nullptr; }
+  } prof_guard{ ctx };
+  cudaEvent_t t_begin = ctx->ev[KSPN_PHASES], t_end = ctx->ev[KSPN_PHASES + 1];
+  KSPN_CUDA(cudaEventRecord(t_begin, ctx->stream));
+  phase_clock clk{ ctx, st };
+  clk.start();
+  if (opt.validate) validate(ctx, g);
+  if (g.n == 0) return;
+
+  uint32_t* und     = ws.und;
+  uint64_t  decided = 0;
+  auto      add     = [&](int phase, uint32_t d) {
+    decided += d;
+    if (st) st->decided[phase] += d;
+    clk.mark(phase);
+  };
+  uint32_t const round_cap = opt.max_rounds ? opt.max_rounds : g.n + 2;
+
+  if (opt.pipeline == KSPN_PIPELINE_REFERENCE) {
+    uint32_t const pivot = trim_1_first(ctx, g, und, scc_id, nullptr, nullptr, false);
+    add(KSPN_PHASE_TRIM_FIRST, ctx->h_ctr[CTR_AUX]);
+    if (decided < g.n) {
+      if (st) st->pivot = pivot;
+      add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pivot, opt, st));
+    }
+    if (decided < g.n) add(KSPN_PHASE_TRIM_NORMAL, trim_1_normal(ctx, g, und, scc_id));
+    int rotation = 0;
+    while (decided < g.n) {
+      if (st && st->label_calls >= round_cap) throw error{ KSPN_ERR_TIMEOUT, "label-search call cap exceeded" };
+      add(KSPN_PHASE_LABEL, label_search(ctx, g, und, scc_id, ++rotation, opt, st));
+    }
+  } else {
+    uint32_t seeds = 0;
+    trim_1_first(ctx, g, und, scc_id, ws.q0, &seeds, true);
+    add(KSPN_PHASE_TRIM_FIRST, ctx->h_ctr[CTR_AUX]);
+    if (decided < g.n) add(KSPN_PHASE_TRIM, trim_fixpoint(ctx, g, und, scc_id, true, seeds));
+    if (decided < g.n) {
+      uint32_t const pivot = select_pivot_live(ctx, g, und);
+      if (st) st->pivot = pivot;
+      if (pivot < g.n) add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pivot, opt, st));
+    }
+    int      rotation = 0;
+    uint32_t rounds   = 0;
+    while (decided < g.n) {
+      if (++rounds > round_cap) throw error{ KSPN_ERR_TIMEOUT, "pipeline round cap exceeded" };
+      add(KSPN_PHASE_TRIM, trim_fixpoint(ctx, g, und, scc_id, false, 0));
+      if (decided < g.n && opt.trim2) {
+        uint32_t const d2 = trim_2(ctx, g, und, scc_id);
+        add(KSPN_PHASE_TRIM2, d2);
+        if (d2 && decided < g.n) add(KSPN_PHASE_TRIM, trim_fixpoint(ctx, g, und, scc_id, false, 0));
+      }
+      if (decided < g.n) add(KSPN_PHASE_LABEL, label_search(ctx, g, und, scc_id, ++rotation, opt, st));
+    }
+    if (st) st->rounds = rounds;
+  }
+  if (decided != g.n || count_undecided(ctx, g.n, und) != 0) throw error{ KSPN_ERR_INTERNAL, "decided-vertex count does not match n" };
+  canonicalise(ctx, g.n, scc_id, ws.label);
+  add(KSPN_PHASE_CANON, 0);
+  KSPN_CUDA(cudaEventRecord(t_end, ctx->stream));
+  KSPN_CUDA(cudaEventSynchronize(t_end));
+  if (st) {
+    float ms = 0;
+    KSPN_CUDA(cudaEventElapsedTime(&ms, t_begin, t_end));
+    st->ms_total        = ms;
+    st->kernel_launches = ctx->launches - launches0;
+  }
+}
+
+// Resolves the transpose: given, or built on the device into `store`.
+dgraph
+with_transpose(kspn_context* ctx, uint32_t n, uint64_t m, uint64_t const* fh, uint32_t const* fc, uint64_t const* bh, uint32_t const* bc, graph_store& store)
+{
+  dgraph g{ n, m, fh, fc, bh, bc };
+  if ((bh == nullptr) != (bc == nullptr)) throw error{ KSPN_ERR_INVALID_ARGUMENT, "bw_head and bw_csr must both be given or both be NULL" };
+  if (!bh) {
+    size_t const bytes = align_up((static_cast<size_t>(n) + 1) * 8) + align_up(std::max<uint64_t>(m, 1) * 4);
+    if (cudaMalloc(&store.base, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      throw error{ KSPN_ERR_OOM, "device transpose" };
+    }
+    store.bytes = bytes;
+    auto* nbh   = static_cast<uint64_t*>(store.base);
+    auto* nbc   = reinterpret_cast<uint32_t*>(static_cast<char*>(store.base) + align_up((static_cast<size_t>(n) + 1) * 8));
+    transpose(ctx, n, m, fh, fc, nbh, nbc, nullptr);
+    g.bh = nbh;
+    g.bc = nbc;
+  }
+  return g;
+}
+
+int
+guard(kspn_context* ctx, auto&& body)
+{
+  try {
+    body();
+    return KSPN_OK;
+  } catch (error const& e) {
+    return fail(ctx, e);
+  } catch (std::bad_alloc const&) {
+    return fail(ctx, error{ KSPN_ERR_OOM, "host allocation" });
+  } catch (...) {
+    return fail(ctx, error{ KSPN_ERR_INTERNAL, "unexpected exception" });
+  }
+}
+
+void
+require(bool ok, char const* what)
+{
+  if (!ok) throw error{ KSPN_ERR_INVALID_ARGUMENT, what };
+}
+
+void
+bind_device(kspn_context* ctx)
+{
+  KSPN_CUDA(cudaSetDevice(ctx->device));
+}
+
+// The phase entry points take the reference's u64 bitset; clear the bits
+// past n in its last word so device words past n stay zero.
+void
+clear_bitset_tail(kspn_context* ctx, uint64_t* bits, uint32_t n)
+{
+  if (n % 64) KSPN_CUDA(cudaMemsetAsync(bits + n / 64, 0, 8, ctx->stream)); // rewritten by the kernel for bits < n
+}
+
+} // namespace
+
+} // namespace kspn
+
+using namespace kspn;
+
+extern "C" {
+
+int
+kspn_options_default(kspn_options* opt)
+{
+  if (!opt) return KSPN_ERR_INVALID_ARGUMENT;
+  std::memset(opt, 0, sizeof(*opt));
+  opt->struct_size  = sizeof(kspn_options);
+  opt->pipeline     = KSPN_PIPELINE_FAST;
+  opt->trim2        = 1;
+  opt->validate     = 1;
+  opt->bu_enter_div = 24;
+  opt->bu_leave_div = 96;
+  return KSPN_OK;
+}
+
+const char*
+kspn_strerror(int status)
+{
+  switch (status) {
+    case KSPN_OK: return "ok";
+    case KSPN_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case KSPN_ERR_INVALID_GRAPH: return "invalid graph";
+    case KSPN_ERR_OOM: return "out of memory";
+    case KSPN_ERR_TIMEOUT: return "iteration cap or wait limit reached";
+    case KSPN_ERR_CUDA: return "CUDA error";
+    case KSPN_ERR_NO_DEVICE: return "no CUDA device";
+    case KSPN_ERR_INTERNAL: return "internal consistency check failed";
+    default: return "unknown status";
+  }
+}
+
+const char*
+kspn_last_error(const kspn_context* ctx)
+{
+  return ctx ? ctx->last_error.c_str() : "";
+}
+
+int
+kspn_context_create_on_stream(int device, void* stream, kspn_context** out)
+{
+  if (!out) return KSPN_ERR_INVALID_ARGUMENT;
+  *out      = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= device || device < 0) {
+    cudaGetLastError();
+    return KSPN_ERR_NO_DEVICE;
+  }
+  auto* ctx   = new (std::nothrow) kspn_context;
+  if (!ctx) return KSPN_ERR_OOM;
+  ctx->device = device;
+  int const rc = guard(ctx, [&] {
+    bind_device(ctx);
+    if (stream) {
+      ctx->stream = static_cast<cudaStream_t>(stream);
+    } else {
+      KSPN_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+      ctx->own_stream = true;
+    }
+    void* h = nullptr;
+    KSPN_CUDA(cudaMallocHost(&h, 64 * sizeof(uint32_t)));
+    ctx->h_ctr   = static_cast<uint32_t*>(h);
+    ctx->h_ctr64 = reinterpret_cast<uint64_t*>(ctx->h_ctr + 32);
+    for (auto& e : ctx->ev) KSPN_CUDA(cudaEventCreate(&e));
+    for (auto& e : ctx->pe) KSPN_CUDA(cudaEventCreate(&e));
+  });
+  if (rc != KSPN_OK) {
+    kspn_context_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return KSPN_OK;
+}
+
+int
+kspn_context_create(int device, kspn_context** out)
+{
+  return kspn_context_create_on_stream(device, nullptr, out);
+}
+
+int
+kspn_context_destroy(kspn_context* ctx)
+{
+  if (!ctx) return KSPN_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->ws.base) cudaFree(ctx->ws.base);
+  if (ctx->h_ctr) cudaFreeHost(ctx->h_ctr);
+  for (auto& e : ctx->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : ctx->pe)
+    if (e) cudaEventDestroy(e);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return KSPN_OK;
+}
+
+int
+kspn_context_synchronize(kspn_context* ctx)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] { KSPN_CUDA(cudaStreamSynchronize(ctx->stream)); });
+}
+
+uint64_t
+kspn_context_launches(const kspn_context* ctx)
+{
+  return ctx ? ctx->launches : 0;
+}
+
+int
+kspn_scc_device(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_head, const uint32_t* d_fw_csr, const uint64_t* d_bw_head, const uint32_t* d_bw_csr, uint32_t* d_scc_id, const kspn_options* opt, kspn_stats* stats)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(d_fw_head && (m == 0 || d_fw_csr) && (n == 0 || d_scc_id), "null device pointer");
+    require(n < UNDECIDED, "n must be below 2^32 - 1");
+    kspn_options const o = options_or_default(opt);
+    bind_device(ctx);
+    graph_store  store;
+    dgraph const g = with_transpose(ctx, n, m, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr, store);
+    run_pipeline(ctx, g, d_scc_id, o, stats);
+  });
+}
+
+int
+kspn_scc(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* fw_head, const uint32_t* fw_csr, const uint64_t* bw_head, const uint32_t* bw_csr, uint32_t* scc_id, const kspn_options* opt, kspn_stats* stats)
+{
+  kspn_context* own = nullptr;
+  if (!ctx) {
+    int const rc = kspn_context_create(0, &own);
+    if (rc != KSPN_OK) return rc;
+    ctx = own;
+  }
+  int const rc = guard(ctx, [&] {
+    require(fw_head && (m == 0 || fw_csr) && (n == 0 || scc_id), "null host pointer");
+    require((bw_head == nullptr) == (bw_csr == nullptr), "bw_head and bw_csr must both be given or both be NULL");
+    require(n < UNDECIDED, "n must be below 2^32 - 1");
+    kspn_options const o = options_or_default(opt);
+    bind_device(ctx);
+    cudaStream_t const s         = ctx->stream;
+    size_t const       head_b    = align_up((static_cast<size_t>(n) + 1) * 8);
+    size_t const       csr_b     = align_up(std::max<uint64_t>(m, 1) * 4);
+    size_t const       out_b     = align_up(std::max<size_t>(n, 1) * 4);
+    bool const         has_bw    = bw_head != nullptr;
+    size_t const       bytes     = 2 * head_b + 2 * csr_b + out_b;
+    graph_store        store;
+    if (cudaMalloc(&store.base, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      throw error{ KSPN_ERR_OOM, "device copy of the graph (" + std::to_string(bytes) + " bytes)" };
+    }
+    char* p   = static_cast<char*>(store.base);
+    auto* dfh = reinterpret_cast<uint64_t*>(p);
+    auto* dbh = reinterpret_cast<uint64_t*>(p + head_b);
+    auto* dfc = reinterpret_cast<uint32_t*>(p + 2 * head_b);
+    auto* dbc = reinterpret_cast<uint32_t*>(p + 2 * head_b + csr_b);
+    auto* dout = reinterpret_cast<uint32_t*>(p + 2 * head_b + 2 * csr_b);
+    KSPN_CUDA(cudaMemcpyAsync(dfh, fw_head, (static_cast<size_t>(n) + 1) * 8, cudaMemcpyHostToDevice, s));
+    if (m) KSPN_CUDA(cudaMemcpyAsync(dfc, fw_csr, m * 4, cudaMemcpyHostToDevice, s));
+    if (has_bw) {
+      KSPN_CUDA(cudaMemcpyAsync(dbh, bw_head, (static_cast<size_t>(n) + 1) * 8, cudaMemcpyHostToDevice, s));
+      if (m) KSPN_CUDA(cudaMemcpyAsync(dbc, bw_csr, m * 4, cudaMemcpyHostToDevice, s));
+    } else {
+      transpose(ctx, n, m, dfh, dfc, dbh, dbc, nullptr);
+    }
+    dgraph const g{ n, m, dfh, dfc, dbh, dbc };
+    run_pipeline(ctx, g, dout, o, stats);
+    if (n) KSPN_CUDA(cudaMemcpyAsync(scc_id, dout, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToHost, s));
+    KSPN_CUDA(cudaStreamSynchronize(s));
+  });
+  if (own) {
+    if (rc != KSPN_OK) std::fprintf(stderr, "kspn_scc: %s\n", own->last_error.c_str());
+    kspn_context_destroy(own);
+  }
+  return rc;
+}
+
+int
+kspn_trim_1_first(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_head, const uint64_t* d_bw_head, uint64_t* d_undecided, uint32_t* d_scc_id, uint32_t* pivot)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(d_fw_head && d_bw_head && d_undecided && d_scc_id && pivot, "null pointer");
+    bind_device(ctx);
+    ensure_workspace(ctx, n, m);
+    clear_bitset_tail(ctx, d_undecided, n);
+    dgraph const g{ n, m, d_fw_head, nullptr, d_bw_head, nullptr };
+    *pivot = n ? trim_1_first(ctx, g, reinterpret_cast<uint32_t*>(d_undecided), d_scc_id, nullptr, nullptr, false) : 0;
+  });
+}
+
+int
+kspn_forward_backward_search(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_head, const uint32_t* d_fw_csr, const uint64_t* d_bw_head, const uint32_t* d_bw_csr, uint64_t* d_undecided, uint32_t* d_scc_id, uint32_t pivot, uint32_t* decided)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(d_fw_head && d_fw_csr && d_bw_head && d_bw_csr && d_undecided && d_scc_id, "null pointer");
+    require(pivot < n, "pivot must be < n");
+    bind_device(ctx);
+    ensure_workspace(ctx, n, m);
+    kspn_options o;
+    kspn_options_default(&o);
+    dgraph const   g{ n, m, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr };
+    uint32_t const d = fw_bw(ctx, g, reinterpret_cast<uint32_t*>(d_undecided), d_scc_id, pivot, o, nullptr);
+    if (decided) *decided = d;
+  });
+}
+
+int
+kspn_trim_1_normal(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_head, const uint32_t* d_fw_csr, const uint64_t* d_bw_head, const uint32_t* d_bw_csr, uint64_t* d_undecided, uint32_t* d_scc_id, uint32_t* decided)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(d_fw_head && d_fw_csr && d_bw_head && d_bw_csr && d_undecided && d_scc_id, "null pointer");
+    bind_device(ctx);
+    ensure_workspace(ctx, n, m);
+    dgraph const   g{ n, m, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr };
+    uint32_t const d = n ? trim_1_normal(ctx, g, reinterpret_cast<uint32_t*>(d_undecided), d_scc_id) : 0;
+    if (decided) *decided = d;
+  });
+}
+
+int
+kspn_label_search(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_head, const uint32_t* d_fw_csr, const uint64_t* d_bw_head, const uint32_t* d_bw_csr, uint64_t* d_undecided, uint32_t* d_scc_id, int rotation, uint32_t* d_label, uint32_t* decided)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(d_fw_head && d_fw_csr && d_bw_head && d_bw_csr && d_undecided && d_scc_id, "null pointer");
+    bind_device(ctx);
+    ensure_workspace(ctx, n, m);
+    kspn_options o;
+    kspn_options_default(&o);
+    dgraph const   g{ n, m, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr };
+    uint32_t const d = n ? label_search(ctx, g, reinterpret_cast<uint32_t*>(d_undecided), d_scc_id, rotation, o, nullptr) : 0;
+    if (d_label && n) KSPN_CUDA(cudaMemcpyAsync(d_label, ctx->ws.label, static_cast<size_t>(n) * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (decided) *decided = d;
+  });
+}
+
+int
+kspn_trim_1_exhaustive_first(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_head, const uint32_t* d_fw_csr, const uint64_t* d_bw_head, const uint32_t* d_bw_csr, uint64_t* d_undecided, uint32_t* d_scc_id, uint32_t* d_outdegree, uint32_t* d_indegree, uint32_t* decided)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(d_fw_head && d_fw_csr && d_bw_head && d_bw_csr && d_undecided && d_scc_id && d_outdegree && d_indegree, "null pointer");
+    bind_device(ctx);
+    ensure_workspace(ctx, n, m);
+    clear_bitset_tail(ctx, d_undecided, n);
+    dgraph const   g{ n, m, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr };
+    uint32_t const d = n ? trim_exhaustive_first(ctx, g, reinterpret_cast<uint32_t*>(d_undecided), d_scc_id, d_outdegree, d_indegree) : 0;
+    if (decided) *decided = d;
+  });
+}
+
+int
+kspn_trim_1_fixpoint(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_head, const uint32_t* d_fw_csr, const uint64_t* d_bw_head, const uint32_t* d_bw_csr, uint64_t* d_undecided, uint32_t* d_scc_id, uint32_t* decided)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(d_fw_head && d_fw_csr && d_bw_head && d_bw_csr && d_undecided && d_scc_id, "null pointer");
+    bind_device(ctx);
+    ensure_workspace(ctx, n, m);
+    dgraph const   g{ n, m, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr };
+    uint32_t const d = n ? trim_fixpoint(ctx, g, reinterpret_cast<uint32_t*>(d_undecided), d_scc_id, false, 0) : 0;
+    if (decided) *decided = d;
+  });
+}
+
+int
+kspn_trim_2(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_head, const uint32_t* d_fw_csr, const uint64_t* d_bw_head, const uint32_t* d_bw_csr, uint64_t* d_undecided, uint32_t* d_scc_id, uint32_t* decided)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(d_fw_head && d_fw_csr && d_bw_head && d_bw_csr && d_undecided && d_scc_id, "null pointer");
+    bind_device(ctx);
+    ensure_workspace(ctx, n, m);
+    dgraph const   g{ n, m, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr };
+    uint32_t const d = n ? trim_2(ctx, g, reinterpret_cast<uint32_t*>(d_undecided), d_scc_id) : 0;
+    if (decided) *decided = d;
+  });
+}
+
+int
+kspn_normalise(kspn_context* ctx, uint32_t n, uint32_t* d_scc_id)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(n == 0 || d_scc_id, "null pointer");
+    bind_device(ctx);
+    ensure_workspace(ctx, n, 0);
+    canonicalise(ctx, n, d_scc_id, ctx->ws.label);
+  });
+}
+
+int
+kspn_transpose(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_head, const uint32_t* d_fw_csr, uint64_t* d_bw_head, uint32_t* d_bw_csr)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(d_fw_head && d_bw_head && (m == 0 || (d_fw_csr && d_bw_csr)), "null pointer");
+    bind_device(ctx);
+    transpose(ctx, n, m, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr, nullptr);
+  });
+}
+
+int
+kspn_gen_gnm(kspn_context* ctx, uint32_t n, uint64_t draws, uint64_t seed, uint32_t* d_src, uint32_t* d_dst)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(draws == 0 || (d_src && d_dst), "null pointer");
+    bind_device(ctx);
+    gen_gnm(ctx, n, draws, seed, d_src, d_dst);
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int
+kspn_gen_rmat(kspn_context* ctx, int scale, uint64_t draws, uint64_t seed, uint64_t t_a, uint64_t t_ab, uint64_t t_abc, int permute, uint32_t* d_src, uint32_t* d_dst)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(draws == 0 || (d_src && d_dst), "null pointer");
+    require(scale >= 0 && scale <= 31, "scale must be in [0, 31]");
+    bind_device(ctx);
+    gen_rmat(ctx, scale, draws, seed, t_a, t_ab, t_abc, permute, d_src, d_dst);
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int
+kspn_build_csr(kspn_context* ctx, uint32_t n, uint64_t m_raw, uint32_t* d_src, uint32_t* d_dst, uint64_t* d_head, uint32_t* d_csr, uint64_t* m_out)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(d_head && (m_raw == 0 || (d_src && d_dst && d_csr)), "null pointer");
+    bind_device(ctx);
+    uint64_t const m = build_csr(ctx, n, m_raw, d_src, d_dst, d_head, d_csr);
+    if (m_out) *m_out = m;
+  });
+}
+
+} // extern "C"

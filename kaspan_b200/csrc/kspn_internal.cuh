@@ -1,0 +1,250 @@
+// Internal declarations shared by the kspn CUDA sources (not installed).
+//
+// Device data layout (one graph, one GPU):
+//   fw_head u64[n+1], fw_csr u32[m]   out-edges (CSR)
+//   bw_head u64[n+1], bw_csr u32[m]   in-edges  (transpose, "CSC")
+//   und     u32[ceil(n/32)]           bit v%32 of word v/32 set = v undecided;
+//                                     byte-identical to the reference's u64
+//                                     bitset words on a little-endian host
+//   scc_id  u32[n]                    member id of v's component, UNDECIDED
+//                                     (0xFFFFFFFF) while v is undecided
+#pragma once
+
+#include "../../include/kspn.h"
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <string>
+
+namespace kspn {
+
+constexpr uint32_t UNDECIDED = 0xFFFFFFFFu;
+
+// ---------------------------------------------------------------- errors
+struct error
+{
+  int         code;
+  std::string what;
+};
+
+#define KSPN_CUDA(call)                                                                                  \
+  do {                                                                                                   \
+    cudaError_t const e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) throw ::kspn::error{ KSPN_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_) }; \
+  } while (0)
+
+#define KSPN_CHECK_LAUNCH() KSPN_CUDA(cudaGetLastError())
+
+inline unsigned
+div_up(uint64_t a, uint64_t b)
+{
+  return static_cast<unsigned>((a + b - 1) / b);
+}
+
+// ---------------------------------------------------------------- device helpers
+__device__ __forceinline__ bool
+bit_get(uint32_t const* bm, uint32_t v)
+{
+  return (bm[v >> 5] >> (v & 31)) & 1u;
+}
+
+// Clears bit v; true iff this call cleared it (exactly one caller wins).
+__device__ __forceinline__ bool
+bit_take(uint32_t* bm, uint32_t v)
+{
+  uint32_t const mask = 1u << (v & 31);
+  return (atomicAnd(bm + (v >> 5), ~mask) & mask) != 0;
+}
+
+// Sets bit v; true iff this call set it.
+__device__ __forceinline__ bool
+bit_claim(uint32_t* bm, uint32_t v)
+{
+  uint32_t const mask = 1u << (v & 31);
+  return (atomicOr(bm + (v >> 5), mask) & mask) == 0;
+}
+
+__device__ __forceinline__ unsigned
+lane_id()
+{
+  return threadIdx.x & 31u;
+}
+
+// Warp-aggregated append: every lane of the (fully active) warp calls it;
+// lanes with pred append v.  One atomic per warp.
+__device__ __forceinline__ void
+warp_push(bool pred, uint32_t v, uint32_t* queue, uint32_t* count)
+{
+  unsigned const ballot = __ballot_sync(0xFFFFFFFFu, pred);
+  if (!ballot) return;
+  unsigned const lane   = lane_id();
+  unsigned const leader = __ffs(ballot) - 1;
+  uint32_t       base   = 0;
+  if (lane == leader) base = atomicAdd(count, static_cast<uint32_t>(__popc(ballot)));
+  base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  if (pred) queue[base + __popc(ballot & ((1u << lane) - 1u))] = v;
+}
+
+// Same, for lanes that may be inactive (uses the active mask).
+__device__ __forceinline__ void
+warp_push_active(uint32_t v, uint32_t* queue, uint32_t* count)
+{
+  unsigned const mask   = __activemask();
+  unsigned const lane   = lane_id();
+  unsigned const leader = __ffs(mask) - 1;
+  uint32_t       base   = 0;
+  if (lane == leader) base = atomicAdd(count, static_cast<uint32_t>(__popc(mask)));
+  base = __shfl_sync(mask, base, leader);
+  queue[base + __popc(mask & ((1u << lane) - 1u))] = v;
+}
+
+__device__ __forceinline__ uint32_t
+rotr32(uint32_t x, int r)
+{
+  return __funnelshift_r(x, x, r & 31);
+}
+__device__ __forceinline__ uint32_t
+rotl32(uint32_t x, int r)
+{
+  return __funnelshift_l(x, x, r & 31);
+}
+
+// ---------------------------------------------------------------- graph + context
+struct dgraph
+{
+  uint32_t        n  = 0;
+  uint64_t        m  = 0;
+  uint64_t const* fh = nullptr; // fw head
+  uint32_t const* fc = nullptr; // fw csr
+  uint64_t const* bh = nullptr; // bw head
+  uint32_t const* bc = nullptr; // bw csr
+};
+
+// Device counters (one cache line each would be nicer; they are few).
+enum ctr_slot : int
+{
+  CTR_Q0 = 0,   // queue 0 size
+  CTR_Q1,       // queue 1 size
+  CTR_DECIDED,  // vertices decided by the running phase
+  CTR_AUX,      // phase-specific
+  CTR_ERR,      // error word (bounds checks, caps)
+  CTR_COUNT = 16 // slots 5.. are phase-specific (8: expansion tile count)
+};
+
+// Scratch owned by a context, sized for the largest graph seen.
+struct workspace
+{
+  uint32_t n_cap = 0;
+  uint64_t m_cap = 0;
+  void*    base  = nullptr;
+  size_t   bytes = 0;
+
+  uint32_t* q0       = nullptr; // n
+  uint32_t* q1       = nullptr; // n
+  uint32_t* vis_a    = nullptr; // bitmap
+  uint32_t* vis_b    = nullptr; // bitmap
+  uint32_t* mark     = nullptr; // bitmap
+  uint32_t* label    = nullptr; // n
+  uint32_t* indeg    = nullptr; // n
+  uint32_t* outdeg   = nullptr; // n
+  uint64_t* prefix   = nullptr; // n+1 (u64 scan output)
+  uint64_t* blocks   = nullptr; // scan partials
+  uint32_t* ctr      = nullptr; // CTR_COUNT
+  uint64_t* ctr64    = nullptr; // 8 (64-bit counters)
+  uint64_t* pivot    = nullptr; // per-block pivot keys (4096 u64 products + 4096 u32 ids)
+  uint32_t* tile_start = nullptr; // m / 2048 + 2 (frontier expansion)
+  // owned graph storage (host inputs, or a CSC built on device)
+  uint64_t* g_fh = nullptr;
+  uint32_t* g_fc = nullptr;
+  uint64_t* g_bh = nullptr;
+  uint32_t* g_bc = nullptr;
+  uint32_t* g_out = nullptr;
+  uint32_t* und   = nullptr; // bitmap
+  size_t    g_bytes = 0;
+  void*     g_base  = nullptr;
+};
+
+} // namespace kspn
+
+struct kspn_context
+{
+  int                device     = 0;
+  cudaStream_t       stream     = nullptr;
+  bool               own_stream = false;
+  kspn::workspace    ws;
+  uint32_t*          h_ctr      = nullptr; // pinned mirror of ws.ctr
+  uint64_t*          h_ctr64    = nullptr;
+  int                rotation   = 0; // label-search calls made by this context
+  cudaEvent_t        ev[KSPN_PHASES + 2] = {};
+  uint64_t           launches   = 0;
+  std::string        last_error;
+  // kernel-class timing (kspn_options.profile): one event pair in flight
+  kspn_stats*        prof       = nullptr;
+  cudaEvent_t        pe[2]      = {};
+};
+
+namespace kspn {
+
+// Kernel-class timing: prof_start/prof_stop bracket launches on the stream;
+// prof_add (after the stream was synchronised) books the elapsed time and
+// the algorithmic bytes of the bracketed work.
+inline void
+prof_start(kspn_context* ctx)
+{
+  if (ctx->prof) cudaEventRecord(ctx->pe[0], ctx->stream);
+}
+inline void
+prof_stop(kspn_context* ctx)
+{
+  if (ctx->prof) cudaEventRecord(ctx->pe[1], ctx->stream);
+}
+inline void
+prof_add(kspn_context* ctx, int cls, uint64_t bytes, uint64_t calls = 1)
+{
+  if (!ctx->prof) return;
+  float ms = 0;
+  if (cudaEventElapsedTime(&ms, ctx->pe[0], ctx->pe[1]) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  ctx->prof->kernel_ms[cls] += ms;
+  ctx->prof->kernel_bytes[cls] += bytes;
+  ctx->prof->kernel_calls[cls] += calls;
+}
+
+// workspace / context helpers (context.cu)
+void ensure_workspace(kspn_context* ctx, uint32_t n, uint64_t m);
+void read_counters(kspn_context* ctx); // D2H of ws.ctr / ws.ctr64 + stream sync
+void zero_counters(kspn_context* ctx);
+int  fail(kspn_context* ctx, error const& e);
+
+// trim.cu
+uint32_t trim_1_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* queue_out, uint32_t* queue_count_host, bool init_degrees);
+uint32_t trim_1_normal(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id);
+uint32_t trim_fixpoint(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, bool degrees_from_first, uint32_t seed_count);
+uint32_t trim_exhaustive_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* outdeg, uint32_t* indeg);
+uint32_t trim_2(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id);
+uint32_t select_pivot_live(kspn_context* ctx, dgraph const& g, uint32_t const* und);
+uint32_t count_undecided(kspn_context* ctx, uint32_t n, uint32_t const* und);
+
+// reach.cu
+uint32_t fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t pivot, kspn_options const& opt, kspn_stats* st);
+
+// label.cu
+uint32_t label_search(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, int rotation, kspn_options const& opt, kspn_stats* st);
+
+// canon.cu
+void canonicalise(kspn_context* ctx, uint32_t n, uint32_t* scc_id, uint32_t* scratch);
+
+// csr.cu
+void     transpose(kspn_context* ctx, uint32_t n, uint64_t m, uint64_t const* fh, uint32_t const* fc, uint64_t* bh, uint32_t* bc, uint32_t* scratch_n);
+uint64_t build_csr(kspn_context* ctx, uint32_t n, uint64_t m_raw, uint32_t* src, uint32_t* dst, uint64_t* head, uint32_t* csr);
+void     validate(kspn_context* ctx, dgraph const& g);
+
+// gen.cu
+void gen_gnm(kspn_context* ctx, uint32_t n, uint64_t draws, uint64_t seed, uint32_t* src, uint32_t* dst);
+void gen_rmat(kspn_context* ctx, int scale, uint64_t draws, uint64_t seed, uint64_t ta, uint64_t tab, uint64_t tabc, int do_perm, uint32_t* src, uint32_t* dst);
+
+} // namespace kspn

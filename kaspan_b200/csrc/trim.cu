@@ -1,0 +1,589 @@
+// Trim phases and pivot selection.
+//
+//  trim_1_first      kaspan/scc/trim_1_local.hpp:12-46
+//  trim_1_normal     kaspan/scc/trim_1_local.hpp:48-73
+//  trim_exhaustive_first / trim_fixpoint
+//                    kaspan/scc/trim_1_exhaustive.hpp:14-131 (live in/out
+//                    degrees; a vertex whose degree drops to 0 is decided and
+//                    its neighbours' degrees drop in turn).  On the device the
+//                    reference's LIFO frontier becomes a level-synchronous
+//                    queue; every directional fixpoint is order-free, so the
+//                    decided sets are the same.
+//  trim_2            exact size-2 trim (an addition, no reference row)
+//  select_pivot_*    kaspan/scc/trim_1_local.hpp:24-45, kaspan/scc/pivot.hpp:53-74
+//
+// Work per launch is one thread per vertex (streaming passes) or one thread
+// per queued vertex with rows of 32+ entries taken by the whole warp.
+#include "kspn_internal.cuh"
+
+namespace kspn {
+
+namespace {
+
+constexpr int      T_THREADS = 256;
+constexpr uint32_t NONE      = 0xFFFFFFFFu;
+constexpr int      WARP_BIG  = 32;
+
+unsigned
+stream_grid(uint64_t items)
+{
+  uint64_t const b = (items + T_THREADS - 1) / T_THREADS;
+  return static_cast<unsigned>(b < 148ull * 16 ? (b ? b : 1) : 148ull * 16);
+}
+
+// (product, id) pairs: larger product wins, then smaller id
+struct pv
+{
+  uint64_t prod;
+  uint32_t id;
+};
+__device__ __forceinline__ pv
+pv_best(pv a, pv b)
+{
+  if (b.prod > a.prod || (b.prod == a.prod && b.id < a.id)) return b;
+  return a;
+}
+__device__ __forceinline__ pv
+pv_warp_reduce(pv x)
+{
+#pragma unroll
+  for (int d = 16; d; d >>= 1) {
+    pv y;
+    y.prod = __shfl_down_sync(0xFFFFFFFFu, x.prod, d);
+    y.id   = __shfl_down_sync(0xFFFFFFFFu, x.id, d);
+    x      = pv_best(x, y);
+  }
+  return x;
+}
+__device__ __forceinline__ void
+pv_block_store(pv x, uint64_t* out_prod, uint32_t* out_id)
+{
+  __shared__ uint64_t sp[T_THREADS / 32];
+  __shared__ uint32_t si[T_THREADS / 32];
+  x = pv_warp_reduce(x);
+  if ((threadIdx.x & 31) == 0) sp[threadIdx.x >> 5] = x.prod, si[threadIdx.x >> 5] = x.id;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    pv y = { 0, NONE };
+    if (threadIdx.x < T_THREADS / 32) y = { sp[threadIdx.x], si[threadIdx.x] };
+    y = pv_warp_reduce(y);
+    if (threadIdx.x == 0) out_prod[blockIdx.x] = y.prod, out_id[blockIdx.x] = y.id;
+  }
+}
+
+// Final reduction of per-block pairs; result id in out_id[0] (NONE if no
+// pair had a product > min_prod... the caller interprets).
+__global__ void
+k_pv_final(uint32_t nb, uint64_t* prod, uint32_t* id)
+{
+  pv x = { 0, NONE };
+  for (uint32_t i = threadIdx.x; i < nb; i += 32) x = pv_best(x, pv{ prod[i], id[i] });
+  x = pv_warp_reduce(x);
+  if (threadIdx.x == 0) prod[0] = x.prod, id[0] = x.id;
+}
+
+// ---------------------------------------------------------------- trim_1_first
+__global__ void __launch_bounds__(T_THREADS)
+k_trim_first(uint32_t n,
+             uint64_t const* __restrict__ fh,
+             uint64_t const* __restrict__ bh,
+             uint32_t* __restrict__ und,
+             uint32_t* __restrict__ scc_id,
+             uint32_t* __restrict__ indeg,
+             uint32_t* __restrict__ outdeg,
+             uint32_t* __restrict__ queue,
+             uint32_t* __restrict__ ctr,
+             uint64_t* __restrict__ blk_prod,
+             uint32_t* __restrict__ blk_id)
+{
+  pv       best = { 0, NONE };
+  uint32_t dec  = 0;
+  uint64_t const nwords_threads = (static_cast<uint64_t>(n) + 31) & ~31ull;
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < nwords_threads; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+    uint32_t const v     = static_cast<uint32_t>(t);
+    bool const     valid = t < n;
+    uint64_t       out = 0, in = 0;
+    if (valid) {
+      out = fh[v + 1] - fh[v];
+      in  = bh[v + 1] - bh[v];
+    }
+    bool const     trimmed = valid && (in == 0 || out == 0);
+    bool const     live    = valid && !trimmed;
+    unsigned const word    = __ballot_sync(0xFFFFFFFFu, live);
+    if ((threadIdx.x & 31) == 0) und[v >> 5] = word;
+    if (valid) scc_id[v] = trimmed ? v : UNDECIDED;
+    if (live) {
+      if (indeg) indeg[v] = static_cast<uint32_t>(in);
+      if (outdeg) outdeg[v] = static_cast<uint32_t>(out);
+      uint64_t const prod = in * out;
+      if (prod > best.prod) best = { prod, v }; // ascending v: first strict max wins
+    }
+    if (queue) warp_push(trimmed, v, queue, ctr + CTR_Q0);
+    dec += trimmed;
+  }
+  // decided count
+  unsigned d = dec;
+#pragma unroll
+  for (int s = 16; s; s >>= 1) d += __shfl_down_sync(0xFFFFFFFFu, d, s);
+  if ((threadIdx.x & 31) == 0 && d) atomicAdd(ctr + CTR_DECIDED, d);
+  pv_block_store(best, blk_prod, blk_id);
+}
+
+// ---------------------------------------------------------------- trim_1_normal
+__global__ void __launch_bounds__(T_THREADS)
+k_trim_normal(uint32_t n,
+              uint64_t const* __restrict__ fh,
+              uint32_t const* __restrict__ fc,
+              uint64_t const* __restrict__ bh,
+              uint32_t const* __restrict__ bc,
+              uint32_t* __restrict__ und,
+              uint32_t* __restrict__ scc_id,
+              uint32_t* __restrict__ ctr)
+{
+  uint32_t dec = 0;
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < n; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+    uint32_t const v = static_cast<uint32_t>(t);
+    if (!bit_get(und, v)) continue;
+    bool has = false;
+    for (uint64_t e = fh[v], end = fh[v + 1]; e < end && !has; ++e) has = bit_get(und, fc[e]);
+    for (uint64_t e = bh[v], end = bh[v + 1]; e < end && !has; ++e) has = bit_get(und, bc[e]);
+    if (!has && bit_take(und, v)) {
+      scc_id[v] = v;
+      ++dec;
+    }
+  }
+  if (dec) atomicAdd(ctr + CTR_DECIDED, dec);
+}
+
+// ---------------------------------------------------------------- live degrees (pull)
+// For every undecided v: indeg/outdeg = undecided neighbours (with
+// multiplicity).  Counting only; k_seed_dead decides in a second launch so
+// every count sees the same undecided set (a vertex decided while others
+// still count would be subtracted twice by the push levels).
+__global__ void __launch_bounds__(T_THREADS)
+k_live_degrees(uint32_t n,
+               uint64_t const* __restrict__ fh,
+               uint32_t const* __restrict__ fc,
+               uint64_t const* __restrict__ bh,
+               uint32_t const* __restrict__ bc,
+               uint32_t const* __restrict__ und,
+               uint32_t* __restrict__ indeg,
+               uint32_t* __restrict__ outdeg)
+{
+  unsigned const lane = threadIdx.x & 31u;
+  uint64_t const span = (static_cast<uint64_t>(n) + 31) & ~31ull;
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+    uint32_t const v    = static_cast<uint32_t>(t);
+    bool const     have = t < n && bit_get(und, v);
+    uint64_t       fb = 0, fe = 0, bb = 0, be = 0;
+    if (have) fb = fh[v], fe = fh[v + 1], bb = bh[v], be = bh[v + 1];
+    uint32_t   outc  = 0, inc = 0;
+    bool const small = have && (fe - fb) < WARP_BIG && (be - bb) < WARP_BIG;
+    if (small) {
+      for (uint64_t e = fb; e < fe; ++e) outc += bit_get(und, fc[e]);
+      for (uint64_t e = bb; e < be; ++e) inc += bit_get(und, bc[e]);
+    }
+    unsigned todo = __ballot_sync(0xFFFFFFFFu, have && !small);
+    while (todo) {
+      unsigned const l = __ffs(todo) - 1;
+      todo &= todo - 1;
+      uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, fb, l), e0 = __shfl_sync(0xFFFFFFFFu, fe, l);
+      uint64_t const b1 = __shfl_sync(0xFFFFFFFFu, bb, l), e1 = __shfl_sync(0xFFFFFFFFu, be, l);
+      uint32_t       a = 0, c = 0;
+      for (uint64_t e = b0 + lane; e < e0; e += 32) a += bit_get(und, fc[e]);
+      for (uint64_t e = b1 + lane; e < e1; e += 32) c += bit_get(und, bc[e]);
+#pragma unroll
+      for (int s = 16; s; s >>= 1) a += __shfl_xor_sync(0xFFFFFFFFu, a, s), c += __shfl_xor_sync(0xFFFFFFFFu, c, s);
+      if (lane == l) outc = a, inc = c;
+    }
+    if (have) {
+      indeg[v]  = inc;
+      outdeg[v] = outc;
+    }
+  }
+}
+
+// Decides (and queues) every undecided vertex whose live in- or out-degree is 0.
+__global__ void __launch_bounds__(T_THREADS)
+k_seed_dead(uint32_t n, uint32_t* __restrict__ und, uint32_t* __restrict__ scc_id, uint32_t const* __restrict__ indeg, uint32_t const* __restrict__ outdeg, uint32_t* __restrict__ queue, uint32_t* __restrict__ ctr)
+{
+  uint64_t const span = (static_cast<uint64_t>(n) + 31) & ~31ull;
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+    uint32_t const v    = static_cast<uint32_t>(t);
+    bool const     dead = t < n && bit_get(und, v) && (indeg[v] == 0 || outdeg[v] == 0);
+    bool const     won  = dead && bit_take(und, v);
+    if (won) scc_id[v] = v;
+    warp_push(won, v, queue, ctr + CTR_Q0);
+  }
+}
+
+// ---------------------------------------------------------------- push-based trim level
+// Each queued (just decided) u lowers the live in-degree of its undecided
+// out-neighbours (dirs & 1) and the live out-degree of its undecided
+// in-neighbours (dirs & 2); a neighbour reaching 0 is decided and queued.
+template<int DIRS>
+__global__ void __launch_bounds__(T_THREADS)
+k_trim_push(uint64_t const* __restrict__ fh,
+            uint32_t const* __restrict__ fc,
+            uint64_t const* __restrict__ bh,
+            uint32_t const* __restrict__ bc,
+            uint32_t* __restrict__ und,
+            uint32_t* __restrict__ scc_id,
+            uint32_t* __restrict__ indeg,
+            uint32_t* __restrict__ outdeg,
+            uint32_t const* __restrict__ qin,
+            uint32_t qn,
+            uint32_t* __restrict__ qout,
+            uint32_t* __restrict__ qout_n,
+            uint32_t* __restrict__ ctr,
+            unsigned long long* __restrict__ edges)
+{
+  unsigned const lane = threadIdx.x & 31u;
+  uint64_t const span = (static_cast<uint64_t>(qn) + 31) & ~31ull;
+  uint32_t       dec  = 0;
+  uint64_t       ne   = 0;
+  auto const     hit  = [&](uint32_t w, uint32_t* deg) {
+    if (bit_get(und, w) && atomicSub(deg + w, 1u) == 1u && bit_take(und, w)) {
+      scc_id[w] = w;
+      ++dec;
+      warp_push_active(w, qout, qout_n);
+    }
+  };
+#pragma unroll
+  for (int dir = 0; dir < 2; ++dir) {
+    if (!(DIRS & (1 << dir))) continue;
+    uint64_t const* head = dir == 0 ? fh : bh;
+    uint32_t const* adj  = dir == 0 ? fc : bc;
+    uint32_t*       deg  = dir == 0 ? indeg : outdeg;
+    for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+      bool const     have = t < qn;
+      uint32_t const u    = have ? qin[t] : 0;
+      uint64_t       b = 0, e = 0;
+      if (have) b = head[u], e = head[u + 1];
+      bool const big = have && (e - b) >= WARP_BIG;
+      ne += e - b;
+      if (have && !big)
+        for (uint64_t x = b; x < e; ++x) hit(adj[x], deg);
+      unsigned todo = __ballot_sync(0xFFFFFFFFu, big);
+      while (todo) {
+        unsigned const l = __ffs(todo) - 1;
+        todo &= todo - 1;
+        uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b, l), e0 = __shfl_sync(0xFFFFFFFFu, e, l);
+        for (uint64_t x = b0 + lane; x < e0; x += 32) hit(adj[x], deg);
+      }
+    }
+  }
+  if (dec) atomicAdd(ctr + CTR_DECIDED, dec);
+#pragma unroll
+  for (int sh = 16; sh; sh >>= 1) ne += __shfl_down_sync(0xFFFFFFFFu, ne, sh);
+  if (lane == 0 && ne) atomicAdd(edges, static_cast<unsigned long long>(ne));
+}
+
+// Reference-exact seeding of trim_1_exhaustive_first's sweeps
+// (kaspan/scc/trim_1_exhaustive.hpp:82-97 and :108-123): over the vertices
+// still undecided, deg = raw degree in this direction; raw 0 => decided now.
+__global__ void __launch_bounds__(T_THREADS)
+k_seed_raw(uint32_t n, uint64_t const* __restrict__ head, uint32_t* __restrict__ und, uint32_t* __restrict__ scc_id, uint32_t* __restrict__ deg, uint32_t* __restrict__ queue, uint32_t* __restrict__ ctr)
+{
+  uint64_t const span = (static_cast<uint64_t>(n) + 31) & ~31ull;
+  uint32_t       dec  = 0;
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+    uint32_t const v    = static_cast<uint32_t>(t);
+    bool const     have = t < n && bit_get(und, v);
+    bool           won  = false;
+    if (have) {
+      uint64_t const d = head[v + 1] - head[v];
+      if (d > 0) deg[v] = static_cast<uint32_t>(d);
+      else if (bit_take(und, v)) {
+        scc_id[v] = v;
+        won       = true;
+        ++dec;
+      }
+    }
+    warp_push(won, v, queue, ctr + CTR_Q0);
+  }
+  if (dec) atomicAdd(ctr + CTR_DECIDED, dec);
+}
+
+// ---------------------------------------------------------------- trim-2
+// one[v] = the single distinct undecided neighbour of v in a direction, or
+// NONE (zero or several distinct ones).
+__global__ void __launch_bounds__(T_THREADS)
+k_unique_neighbour(uint32_t n, uint64_t const* __restrict__ fh, uint32_t const* __restrict__ fc, uint64_t const* __restrict__ bh, uint32_t const* __restrict__ bc, uint32_t const* __restrict__ und, uint32_t* __restrict__ out_one, uint32_t* __restrict__ in_one)
+{
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < n; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+    uint32_t const v = static_cast<uint32_t>(t);
+    if (!bit_get(und, v)) continue;
+#pragma unroll
+    for (int dir = 0; dir < 2; ++dir) {
+      uint64_t const* head = dir ? bh : fh;
+      uint32_t const* adj  = dir ? bc : fc;
+      uint32_t        one  = NONE;
+      bool            many = false;
+      for (uint64_t e = head[v], end = head[v + 1]; e < end; ++e) {
+        uint32_t const w = adj[e];
+        if (!bit_get(und, w)) continue;
+        if (one == NONE) one = w;
+        else if (w != one) {
+          many = true;
+          break;
+        }
+      }
+      (dir ? in_one : out_one)[v] = many ? NONE : one;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(T_THREADS)
+k_trim2_decide(uint32_t n, uint32_t const* __restrict__ out_one, uint32_t const* __restrict__ in_one, uint32_t* __restrict__ und, uint32_t* __restrict__ scc_id, uint32_t* __restrict__ ctr)
+{
+  uint32_t dec = 0;
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < n; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+    uint32_t const u = static_cast<uint32_t>(t);
+    if (!bit_get(und, u)) continue;
+#pragma unroll
+    for (int dir = 0; dir < 2; ++dir) {
+      uint32_t const* one = dir ? in_one : out_one;
+      uint32_t const  v   = one[u];
+      if (v == NONE || v <= u || v >= n) continue;
+      if (one[v] != u) continue;
+      // u < v, each the other's only undecided neighbour in this direction:
+      // {u, v} is closed under that direction, so it is an SCC
+      if (bit_take(und, u)) {
+        bit_take(und, v);
+        scc_id[u] = u;
+        scc_id[v] = u;
+        dec += 2;
+      }
+    }
+  }
+  if (dec) atomicAdd(ctr + CTR_DECIDED, dec);
+}
+
+// ---------------------------------------------------------------- pivots / counts
+__global__ void __launch_bounds__(T_THREADS)
+k_pivot_live(uint32_t n, uint32_t const* __restrict__ und, uint32_t const* __restrict__ indeg, uint32_t const* __restrict__ outdeg, uint64_t* __restrict__ blk_prod, uint32_t* __restrict__ blk_id)
+{
+  pv best = { 0, NONE };
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < n; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+    uint32_t const v = static_cast<uint32_t>(t);
+    if (!bit_get(und, v)) continue;
+    pv const c = { static_cast<uint64_t>(outdeg[v]) * indeg[v] + 1, v }; // +1: any undecided vertex beats none
+    best       = pv_best(best, c);
+  }
+  pv_block_store(best, blk_prod, blk_id);
+}
+
+__global__ void __launch_bounds__(T_THREADS)
+k_popcount(uint32_t words, uint32_t n, uint32_t const* __restrict__ bm, uint32_t* __restrict__ out)
+{
+  uint32_t c = 0;
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < words; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+    uint32_t w = bm[t];
+    if ((t + 1) * 32 > n) {
+      uint32_t const valid = n - static_cast<uint32_t>(t) * 32;
+      w &= valid >= 32 ? 0xFFFFFFFFu : ((1u << valid) - 1u);
+    }
+    c += __popc(w);
+  }
+#pragma unroll
+  for (int s = 16; s; s >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, s);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+uint32_t
+pv_result(kspn_context* ctx, unsigned nb, uint64_t* min_prod_out)
+{
+  auto&     ws   = ctx->ws;
+  uint64_t* prod = ws.pivot;
+  uint32_t* id   = reinterpret_cast<uint32_t*>(ws.pivot + 4096);
+  k_pv_final<<<1, 32, 0, ctx->stream>>>(nb, prod, id);
+  KSPN_CHECK_LAUNCH();
+  ctx->launches += 1;
+  uint64_t hp = 0;
+  uint32_t hi = 0;
+  KSPN_CUDA(cudaMemcpyAsync(&hp, prod, sizeof(hp), cudaMemcpyDeviceToHost, ctx->stream));
+  KSPN_CUDA(cudaMemcpyAsync(&hi, id, sizeof(hi), cudaMemcpyDeviceToHost, ctx->stream));
+  KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (min_prod_out) *min_prod_out = hp;
+  return hi;
+}
+
+// Runs push levels from the queue in q0 (size qn) until no vertex is
+// decided; returns the number decided by the levels.
+template<int DIRS>
+uint32_t
+run_push_levels(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t qn)
+{
+  auto&    ws    = ctx->ws;
+  uint32_t total = 0;
+  uint32_t* qa = ws.q0, *qb = ws.q1;
+  uint32_t const cap = g.n + 2;
+  for (uint32_t level = 0; qn > 0; ++level) {
+    if (level > cap) throw error{ KSPN_ERR_TIMEOUT, "trim: level cap exceeded" };
+    KSPN_CUDA(cudaMemsetAsync(ws.ctr + CTR_Q1, 0, sizeof(uint32_t), ctx->stream));
+    KSPN_CUDA(cudaMemsetAsync(ws.ctr + CTR_DECIDED, 0, sizeof(uint32_t), ctx->stream));
+    uint64_t const e0 = ctx->h_ctr64[2];
+    prof_start(ctx);
+    k_trim_push<DIRS><<<stream_grid(qn), T_THREADS, 0, ctx->stream>>>(g.fh, g.fc, g.bh, g.bc, und, scc_id, ws.indeg, ws.outdeg, qa, qn, qb, ws.ctr + CTR_Q1, ws.ctr,
+                                                                       reinterpret_cast<unsigned long long*>(ws.ctr64 + 2));
+    prof_stop(ctx);
+    KSPN_CHECK_LAUNCH();
+    ctx->launches += 1;
+    read_counters(ctx);
+    // per queued vertex and direction: queue entry + offset pair; per edge:
+    // id + degree atomic; per decided vertex: id write + queue write
+    int const ndir = (DIRS & 1) + ((DIRS >> 1) & 1);
+    prof_add(ctx, KSPN_KERNEL_TRIM, 20ull * ndir * qn + 8 * (ctx->h_ctr64[2] - e0) + 8ull * ctx->h_ctr[CTR_DECIDED]);
+    qn = ctx->h_ctr[CTR_Q1];
+    total += ctx->h_ctr[CTR_DECIDED];
+    uint32_t* t = qa;
+    qa          = qb;
+    qb          = t;
+  }
+  // leave the workspace queues in their canonical order for the next user
+  return total;
+}
+
+} // namespace
+
+uint32_t
+trim_1_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* queue_out, uint32_t* queue_count_host, bool init_degrees)
+{
+  auto& ws = ctx->ws;
+  zero_counters(ctx);
+  unsigned const nb = stream_grid(g.n);
+  prof_start(ctx);
+  k_trim_first<<<nb, T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.bh, und, scc_id, init_degrees ? ws.indeg : nullptr, init_degrees ? ws.outdeg : nullptr, queue_out, ws.ctr, ws.pivot, reinterpret_cast<uint32_t*>(ws.pivot + 4096));
+  prof_stop(ctx);
+  KSPN_CHECK_LAUNCH();
+  ctx->launches += 1;
+  uint64_t       prod  = 0;
+  uint32_t const pivot = pv_result(ctx, nb, &prod);
+  read_counters(ctx);
+  {
+    // both offset arrays streamed (8 B per vertex each), id + bitmap written,
+    // live degrees written, trimmed vertices queued
+    uint64_t const dec  = ctx->h_ctr[CTR_DECIDED];
+    uint64_t const live = g.n - dec;
+    prof_add(ctx, KSPN_KERNEL_STREAM, 16ull * (g.n + 1) + 4ull * g.n + g.n / 8 + (init_degrees ? 8 * live : 0) + (queue_out ? 4 * dec : 0));
+  }
+  if (queue_count_host) *queue_count_host = ctx->h_ctr[CTR_Q0];
+  ctx->h_ctr[CTR_AUX] = ctx->h_ctr[CTR_DECIDED];
+  // no undecided vertex: the reference returns n (trim_1_local.hpp:21,44)
+  return (prod == 0 || pivot == NONE) ? g.n : pivot;
+}
+
+uint32_t
+trim_1_normal(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id)
+{
+  zero_counters(ctx);
+  k_trim_normal<<<stream_grid(g.n), T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.fc, g.bh, g.bc, und, scc_id, ctx->ws.ctr);
+  KSPN_CHECK_LAUNCH();
+  ctx->launches += 1;
+  read_counters(ctx);
+  return ctx->h_ctr[CTR_DECIDED];
+}
+
+// Full trim-1 fixpoint on the undecided sub-graph.  degrees_from_first:
+// the live degrees and the seed queue (seed_count entries in q0) come from
+// trim_1_first; otherwise they are counted here (pull) first.
+uint32_t
+trim_fixpoint(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, bool degrees_from_first, uint32_t seed_count)
+{
+  auto&    ws    = ctx->ws;
+  uint32_t total = 0, qn = seed_count;
+  if (!degrees_from_first) {
+    zero_counters(ctx);
+    k_live_degrees<<<stream_grid(g.n), T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.fc, g.bh, g.bc, und, ws.indeg, ws.outdeg);
+    k_seed_dead<<<stream_grid(g.n), T_THREADS, 0, ctx->stream>>>(g.n, und, scc_id, ws.indeg, ws.outdeg, ws.q0, ws.ctr);
+    KSPN_CHECK_LAUNCH();
+    ctx->launches += 2;
+    read_counters(ctx);
+    qn    = ctx->h_ctr[CTR_Q0];
+    total = qn;
+  }
+  total += run_push_levels<3>(ctx, g, und, scc_id, qn);
+  return total;
+}
+
+uint32_t
+trim_exhaustive_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* outdeg, uint32_t* indeg)
+{
+  auto&    ws    = ctx->ws;
+  uint32_t total = 0;
+  // every vertex starts undecided
+  KSPN_CUDA(cudaMemsetAsync(und, 0xFF, (static_cast<size_t>(g.n) + 31) / 32 * 4, ctx->stream));
+  KSPN_CUDA(cudaMemsetAsync(scc_id, 0xFF, static_cast<size_t>(g.n) * 4, ctx->stream));
+  uint32_t* save_in = ws.indeg, *save_out = ws.outdeg;
+  ws.indeg  = indeg;
+  ws.outdeg = outdeg;
+  try {
+    // in-degree sweep: raw in-degree 0 decided, decrements along out-edges
+    zero_counters(ctx);
+    k_seed_raw<<<stream_grid(g.n), T_THREADS, 0, ctx->stream>>>(g.n, g.bh, und, scc_id, indeg, ws.q0, ws.ctr);
+    KSPN_CHECK_LAUNCH();
+    read_counters(ctx);
+    total += ctx->h_ctr[CTR_DECIDED];
+    total += run_push_levels<1>(ctx, g, und, scc_id, ctx->h_ctr[CTR_Q0]);
+    // out-degree sweep over the survivors: raw out-degree, decrements along in-edges
+    zero_counters(ctx);
+    k_seed_raw<<<stream_grid(g.n), T_THREADS, 0, ctx->stream>>>(g.n, g.fh, und, scc_id, outdeg, ws.q0, ws.ctr);
+    KSPN_CHECK_LAUNCH();
+    read_counters(ctx);
+    total += ctx->h_ctr[CTR_DECIDED];
+    total += run_push_levels<2>(ctx, g, und, scc_id, ctx->h_ctr[CTR_Q0]);
+    ctx->launches += 2;
+  } catch (...) {
+    ws.indeg  = save_in;
+    ws.outdeg = save_out;
+    throw;
+  }
+  ws.indeg  = save_in;
+  ws.outdeg = save_out;
+  return total;
+}
+
+uint32_t
+trim_2(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id)
+{
+  auto& ws = ctx->ws;
+  zero_counters(ctx);
+  k_unique_neighbour<<<stream_grid(g.n), T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.fc, g.bh, g.bc, und, ws.indeg, ws.outdeg);
+  k_trim2_decide<<<stream_grid(g.n), T_THREADS, 0, ctx->stream>>>(g.n, ws.indeg, ws.outdeg, und, scc_id, ws.ctr);
+  KSPN_CHECK_LAUNCH();
+  ctx->launches += 2;
+  read_counters(ctx);
+  return ctx->h_ctr[CTR_DECIDED];
+}
+
+// argmax over undecided v of live outdeg*indeg, lowest id on ties; n if no
+// vertex is undecided.  Degrees must be current (after a trim fixpoint).
+uint32_t
+select_pivot_live(kspn_context* ctx, dgraph const& g, uint32_t const* und)
+{
+  auto&          ws = ctx->ws;
+  unsigned const nb = stream_grid(g.n);
+  k_pivot_live<<<nb, T_THREADS, 0, ctx->stream>>>(g.n, und, ws.indeg, ws.outdeg, ws.pivot, reinterpret_cast<uint32_t*>(ws.pivot + 4096));
+  KSPN_CHECK_LAUNCH();
+  ctx->launches += 1;
+  uint64_t       prod = 0;
+  uint32_t const p    = pv_result(ctx, nb, &prod);
+  return (prod == 0 || p == NONE) ? g.n : p;
+}
+
+uint32_t
+count_undecided(kspn_context* ctx, uint32_t n, uint32_t const* und)
+{
+  uint32_t const words = (n + 31) / 32;
+  zero_counters(ctx);
+  if (words) {
+    k_popcount<<<stream_grid(words), T_THREADS, 0, ctx->stream>>>(words, n, und, ctx->ws.ctr + CTR_AUX);
+    KSPN_CHECK_LAUNCH();
+    ctx->launches += 1;
+  }
+  read_counters(ctx);
+  return ctx->h_ctr[CTR_AUX];
+}
+
+} // namespace kspn

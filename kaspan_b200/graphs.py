@@ -1,0 +1,86 @@
+"""Device-resident graphs and the seeded synthetic inputs, built with libkspn.
+
+The generators stand in for the KaGen inputs the reference benchmarks with
+(experiment/horeka/bootstrap.py:35-39): directed G(n, m) and R-MAT with a
+seeded id permutation.  Every step runs on the GPU through the C ABI:
+draw the edge list (kspn_gen_*), sort + dedupe into a CSR (kspn_build_csr),
+build the transpose (kspn_transpose).  torch provides the device buffers.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import Context
+
+
+@dataclass
+class DeviceGraph:
+    n: int
+    m: int
+    fwh: "torch.Tensor"  # int64[n+1] holding u64 offsets
+    fwc: "torch.Tensor"  # int32[m]   holding u32 ids
+    bwh: "torch.Tensor"
+    bwc: "torch.Tensor"
+
+    def nbytes(self) -> int:
+        return 2 * 8 * (self.n + 1) + 2 * 4 * self.m
+
+    def to_host(self):
+        """(fwh, fwc, bwh, bwc) as numpy u64/u32 arrays."""
+        return (self.fwh.cpu().numpy().view(np.uint64), self.fwc.cpu().numpy().view(np.uint32),
+                self.bwh.cpu().numpy().view(np.uint64), self.bwc.cpu().numpy().view(np.uint32))
+
+
+def rmat_thresholds(a: float, b: float, c: float):
+    s = float(1 << 32)
+    return int(math.floor(a * s)), int(math.floor((a + b) * s)), int(math.floor((a + b + c) * s))
+
+
+def from_edges(ctx: Context, n: int, src, dst, device="cuda") -> DeviceGraph:
+    """Edge list (device int32 tensors, consumed) -> DeviceGraph."""
+    import torch
+
+    m_raw = src.numel()
+    head = torch.empty(n + 1, dtype=torch.int64, device=device)
+    csr = torch.empty(max(m_raw, 1), dtype=torch.int32, device=device)
+    m = ctx.build_csr(n, m_raw, src, dst, head, csr)
+    del src, dst
+    csr = csr[:m].clone() if m < csr.numel() else csr
+    bwh = torch.empty(n + 1, dtype=torch.int64, device=device)
+    bwc = torch.empty(max(m, 1), dtype=torch.int32, device=device)
+    ctx.transpose(n, m, head, csr, bwh, bwc)
+    return DeviceGraph(n, m, head, csr, bwh, bwc)
+
+
+def from_host_csr(n: int, fwh, fwc, bwh, bwc, device="cuda") -> DeviceGraph:
+    import torch
+
+    def t(a, dt):
+        a = np.ascontiguousarray(a)
+        return torch.from_numpy(a.view(dt).copy()).to(device)
+
+    m = int(fwh[n]) if n else 0
+    return DeviceGraph(n, m, t(fwh, np.int64), t(fwc[: max(m, 1)], np.int32), t(bwh, np.int64), t(bwc[: max(m, 1)], np.int32))
+
+
+def gnm(ctx: Context, n: int, draws: int, seed: int, device="cuda") -> DeviceGraph:
+    import torch
+
+    src = torch.empty(max(draws, 1), dtype=torch.int32, device=device)
+    dst = torch.empty(max(draws, 1), dtype=torch.int32, device=device)
+    ctx.gen_gnm(n, draws, seed, src, dst)
+    return from_edges(ctx, n, src[:draws], dst[:draws], device)
+
+
+def rmat(ctx: Context, scale: int, edge_factor: int, seed: int, a=0.57, b=0.19, c=0.19, permute=True, device="cuda") -> DeviceGraph:
+    import torch
+
+    draws = edge_factor << scale
+    ta, tab, tabc = rmat_thresholds(a, b, c)
+    src = torch.empty(max(draws, 1), dtype=torch.int32, device=device)
+    dst = torch.empty(max(draws, 1), dtype=torch.int32, device=device)
+    ctx.gen_rmat(scale, draws, seed, ta, tab, tabc, permute, src, dst)
+    return from_edges(ctx, 1 << scale, src[:draws], dst[:draws], device)
