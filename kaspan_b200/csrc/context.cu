@@ -68,6 +68,7 @@ layout(workspace& ws, char* base, uint32_t n, uint64_t m)
   ws.blocks            = c.take<uint64_t>(std::max<size_t>(scan_partial_entries(nn), 4096));
   ws.pivot             = c.take<uint64_t>(8192);
   ws.tile_start        = c.take<uint32_t>(m / 2048 + 4);
+  ws.rstate            = c.take<char>(512);
   return align_up(c.off);
 }
 
@@ -82,6 +83,7 @@ ensure_workspace(kspn_context* ctx, uint32_t n, uint64_t m)
   uint64_t const mcap = std::max(m, ws.m_cap);
   if (ws.base) {
     KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+    release_graphs(ctx); // they name the old workspace
     cudaFree(ws.base);
     ws.base = nullptr;
   }
@@ -98,6 +100,26 @@ ensure_workspace(kspn_context* ctx, uint32_t n, uint64_t m)
   ws.m_cap = mcap;
   layout(ws, static_cast<char*>(p), ncap, mcap);
   KSPN_CUDA(cudaMemsetAsync(ws.ctr, 0, 64 * sizeof(uint32_t), ctx->stream));
+}
+
+void*
+context_buffer(kspn_context* ctx, int slot, size_t bytes)
+{
+  auto& b = ctx->bufs[slot];
+  if (b.p && b.bytes >= bytes) return b.p;
+  if (b.p) {
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+    release_graphs(ctx); // a cached graph may name the old buffer
+    cudaFree(b.p);
+    b = {};
+  }
+  if (cudaMalloc(&b.p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    b = {};
+    throw error{ KSPN_ERR_OOM, "device buffer of " + std::to_string(bytes) + " bytes" };
+  }
+  b.bytes = bytes;
+  return b.p;
 }
 
 void
@@ -186,7 +208,8 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
   uint64_t const launches0 = ctx->launches;
   KSPN_CUDA(cudaMemsetAsync(ws.ctr, 0, 64 * sizeof(uint32_t), ctx->stream));
   std::memset(ctx->h_ctr, 0, 64 * sizeof(uint32_t));
-  ctx->prof = (opt.profile && st) ? st : nullptr;
+  ctx->td_edges = 0;
+  ctx->prof     = (opt.profile && st) ? st : nullptr;
   struct prof_reset
   {
     kspn_context* c;
@@ -199,8 +222,9 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
   if (opt.validate) validate(ctx, g);
   if (g.n == 0) return;
 
-  uint32_t* und     = ws.und;
-  uint64_t  decided = 0;
+  uint32_t* und       = ws.und;
+  uint64_t  decided   = 0;
+  bool      label_ran = false;
   auto      add     = [&](int phase, uint32_t d) {
     decided += d;
     if (st) st->decided[phase] += d;
@@ -213,12 +237,13 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
     add(KSPN_PHASE_TRIM_FIRST, ctx->h_ctr[CTR_AUX]);
     if (decided < g.n) {
       if (st) st->pivot = pivot;
-      add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pivot, opt, st));
+      add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pivot, opt, st, true));
     }
     if (decided < g.n) add(KSPN_PHASE_TRIM_NORMAL, trim_1_normal(ctx, g, und, scc_id));
     int rotation = 0;
     while (decided < g.n) {
       if (st && st->label_calls >= round_cap) throw error{ KSPN_ERR_TIMEOUT, "label-search call cap exceeded" };
+      label_ran = true;
       add(KSPN_PHASE_LABEL, label_search(ctx, g, und, scc_id, ++rotation, opt, st));
     }
   } else {
@@ -229,7 +254,7 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
     if (decided < g.n) {
       uint32_t const pivot = select_pivot_live(ctx, g, und);
       if (st) st->pivot = pivot;
-      if (pivot < g.n) add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pivot, opt, st));
+      if (pivot < g.n) add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pivot, opt, st, true));
     }
     int      rotation = 0;
     uint32_t rounds   = 0;
@@ -241,12 +266,19 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
         add(KSPN_PHASE_TRIM2, d2);
         if (d2 && decided < g.n) add(KSPN_PHASE_TRIM, trim_fixpoint(ctx, g, und, scc_id, false, 0));
       }
-      if (decided < g.n) add(KSPN_PHASE_LABEL, label_search(ctx, g, und, scc_id, ++rotation, opt, st));
+      if (decided < g.n) {
+        label_ran = true;
+        add(KSPN_PHASE_LABEL, label_search(ctx, g, und, scc_id, ++rotation, opt, st));
+      }
     }
     if (st) st->rounds = rounds;
   }
   if (decided != g.n || count_undecided(ctx, g.n, und) != 0) throw error{ KSPN_ERR_INTERNAL, "decided-vertex count does not match n" };
-  canonicalise(ctx, g.n, scc_id, ws.label);
+  if (st) st->edges_scanned = ctx->h_ctr64[0] + ctx->td_edges;
+  // trim (id = itself), trim-2 (id = the smaller of the pair) and FW-BW
+  // (id = smallest member) already name components canonically; label
+  // searches name them after their root, so only then is a relabel needed
+  if (label_ran) canonicalise(ctx, g.n, scc_id, ws.label, true);
   add(KSPN_PHASE_CANON, 0);
   KSPN_CUDA(cudaEventRecord(t_end, ctx->stream));
   KSPN_CUDA(cudaEventSynchronize(t_end));
@@ -266,13 +298,10 @@ with_transpose(kspn_context* ctx, uint32_t n, uint64_t m, uint64_t const* fh, ui
   if ((bh == nullptr) != (bc == nullptr)) throw error{ KSPN_ERR_INVALID_ARGUMENT, "bw_head and bw_csr must both be given or both be NULL" };
   if (!bh) {
     size_t const bytes = align_up((static_cast<size_t>(n) + 1) * 8) + align_up(std::max<uint64_t>(m, 1) * 4);
-    if (cudaMalloc(&store.base, bytes) != cudaSuccess) {
-      cudaGetLastError();
-      throw error{ KSPN_ERR_OOM, "device transpose" };
-    }
-    store.bytes = bytes;
-    auto* nbh   = static_cast<uint64_t*>(store.base);
-    auto* nbc   = reinterpret_cast<uint32_t*>(static_cast<char*>(store.base) + align_up((static_cast<size_t>(n) + 1) * 8));
+    char*        base  = static_cast<char*>(context_buffer(ctx, BUF_TRANSPOSE, bytes));
+    (void)store;
+    auto* nbh = reinterpret_cast<uint64_t*>(base);
+    auto* nbc = reinterpret_cast<uint32_t*>(base + align_up((static_cast<size_t>(n) + 1) * 8));
     transpose(ctx, n, m, fh, fc, nbh, nbc, nullptr);
     g.bh = nbh;
     g.bc = nbc;
@@ -384,6 +413,7 @@ kspn_context_create_on_stream(int device, void* stream, kspn_context** out)
     KSPN_CUDA(cudaMallocHost(&h, 64 * sizeof(uint32_t)));
     ctx->h_ctr   = static_cast<uint32_t*>(h);
     ctx->h_ctr64 = reinterpret_cast<uint64_t*>(ctx->h_ctr + 32);
+    KSPN_CUDA(cudaMallocHost(&ctx->h_state, 512));
     for (auto& e : ctx->ev) KSPN_CUDA(cudaEventCreate(&e));
     for (auto& e : ctx->pe) KSPN_CUDA(cudaEventCreate(&e));
   });
@@ -407,8 +437,12 @@ kspn_context_destroy(kspn_context* ctx)
   if (!ctx) return KSPN_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  release_graphs(ctx);
   if (ctx->ws.base) cudaFree(ctx->ws.base);
   if (ctx->h_ctr) cudaFreeHost(ctx->h_ctr);
+  if (ctx->h_state) cudaFreeHost(ctx->h_state);
+  for (auto& b : ctx->bufs)
+    if (b.p) cudaFree(b.p);
   for (auto& e : ctx->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : ctx->pe)
@@ -467,12 +501,7 @@ kspn_scc(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* fw_head, con
     size_t const       out_b     = align_up(std::max<size_t>(n, 1) * 4);
     bool const         has_bw    = bw_head != nullptr;
     size_t const       bytes     = 2 * head_b + 2 * csr_b + out_b;
-    graph_store        store;
-    if (cudaMalloc(&store.base, bytes) != cudaSuccess) {
-      cudaGetLastError();
-      throw error{ KSPN_ERR_OOM, "device copy of the graph (" + std::to_string(bytes) + " bytes)" };
-    }
-    char* p   = static_cast<char*>(store.base);
+    char*              p         = static_cast<char*>(context_buffer(ctx, BUF_HOST_GRAPH, bytes));
     auto* dfh = reinterpret_cast<uint64_t*>(p);
     auto* dbh = reinterpret_cast<uint64_t*>(p + head_b);
     auto* dfc = reinterpret_cast<uint32_t*>(p + 2 * head_b);
@@ -524,7 +553,7 @@ kspn_forward_backward_search(kspn_context* ctx, uint32_t n, uint64_t m, const ui
     kspn_options o;
     kspn_options_default(&o);
     dgraph const   g{ n, m, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr };
-    uint32_t const d = fw_bw(ctx, g, reinterpret_cast<uint32_t*>(d_undecided), d_scc_id, pivot, o, nullptr);
+    uint32_t const d = fw_bw(ctx, g, reinterpret_cast<uint32_t*>(d_undecided), d_scc_id, pivot, o, nullptr, false);
     if (decided) *decided = d;
   });
 }
@@ -612,7 +641,7 @@ kspn_normalise(kspn_context* ctx, uint32_t n, uint32_t* d_scc_id)
     require(n == 0 || d_scc_id, "null pointer");
     bind_device(ctx);
     ensure_workspace(ctx, n, 0);
-    canonicalise(ctx, n, d_scc_id, ctx->ws.label);
+    canonicalise(ctx, n, d_scc_id, ctx->ws.label, false);
   });
 }
 

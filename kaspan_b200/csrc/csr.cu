@@ -38,11 +38,18 @@ k_expand_rows(uint32_t n, uint64_t const* __restrict__ head, uint32_t* __restric
   }
 }
 
+// head[v] = first index of key v in the ascending keys[0, m) (= m past the
+// last key): every boundary between two different keys writes the heads of
+// the ids it spans, so each head is written exactly once, without atomics.
 __global__ void
-k_count_keys(uint64_t m, uint32_t const* __restrict__ keys, uint32_t* __restrict__ cnt)
+k_heads_from_sorted(uint32_t n, uint64_t m, uint32_t const* __restrict__ keys, uint64_t* __restrict__ head)
 {
-  for (uint64_t e = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < m; e += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-    atomicAdd(&cnt[keys[e]], 1u);
+  uint64_t const stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i <= m; i += stride) {
+    int64_t const lo = i == 0 ? -1 : static_cast<int64_t>(keys[i - 1]);
+    int64_t const hi = i == m ? static_cast<int64_t>(n) : static_cast<int64_t>(keys[i]);
+    for (int64_t v = lo + 1; v <= hi; ++v) head[v] = i;
+  }
 }
 
 // keep[i] = 1 for the first copy of each (src, dst) with src != dst
@@ -59,13 +66,12 @@ struct f_keep
 };
 
 __global__ void
-k_compact_edges(uint64_t m_raw, uint32_t const* __restrict__ s, uint32_t const* __restrict__ d, uint32_t const* __restrict__ pos, uint32_t* __restrict__ csr, uint32_t* __restrict__ rowcnt)
+k_compact_edges(uint64_t m_raw, uint32_t const* __restrict__ s, uint32_t const* __restrict__ d, uint32_t const* __restrict__ pos, uint32_t* __restrict__ csr, uint32_t* __restrict__ src_kept)
 {
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < m_raw; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-    bool const keep = pos[i + 1] != pos[i];
-    if (keep) {
-      csr[pos[i]] = d[i];
-      atomicAdd(&rowcnt[s[i]], 1u);
+    if (pos[i + 1] != pos[i]) {
+      csr[pos[i]]      = d[i];
+      src_kept[pos[i]] = s[i];
     }
   }
 }
@@ -92,10 +98,6 @@ struct scratch
 {
   void*  p     = nullptr;
   size_t bytes = 0;
-  ~scratch()
-  {
-    if (p) cudaFree(p);
-  }
   template<typename T>
   T* carve(size_t& off, size_t count)
   {
@@ -107,12 +109,9 @@ struct scratch
 };
 
 void
-alloc_scratch(scratch& s, size_t bytes)
+alloc_scratch(kspn_context* ctx, scratch& s, size_t bytes)
 {
-  if (cudaMalloc(&s.p, bytes) != cudaSuccess) {
-    cudaGetLastError();
-    throw error{ KSPN_ERR_OOM, "device scratch for graph construction (" + std::to_string(bytes) + " bytes)" };
-  }
+  s.p     = context_buffer(ctx, BUF_BUILD, bytes);
   s.bytes = bytes;
 }
 
@@ -129,7 +128,7 @@ transpose(kspn_context* ctx, uint32_t n, uint64_t m, uint64_t const* fh, uint32_
   size_t const hist_n = radix_hist_entries(m);
   size_t const part_n = scan_partial_entries(hist_n > n + 1 ? hist_n : n + 1);
   scratch      sc;
-  alloc_scratch(sc, 3 * (m + 64) * sizeof(uint32_t) + (hist_n + part_n + n + 64) * sizeof(uint64_t) + 4096);
+  alloc_scratch(ctx, sc, 3 * (m + 64) * sizeof(uint32_t) + (hist_n + part_n + n + 64) * sizeof(uint64_t) + 4096);
   size_t    off   = 0;
   uint32_t* keys  = sc.carve<uint32_t>(off, m + 1);
   uint32_t* kalt  = sc.carve<uint32_t>(off, m + 1);
@@ -145,14 +144,11 @@ transpose(kspn_context* ctx, uint32_t n, uint64_t m, uint64_t const* fh, uint32_
     KSPN_CHECK_LAUNCH();
     radix_sort_pairs(ctx, keys, bc, kalt, valt, m, 0, bits_for(n), hist, part);
   }
-  KSPN_CUDA(cudaMemsetAsync(cnt, 0, (n + 1) * sizeof(uint32_t), s));
-  if (m) {
-    k_count_keys<<<grid_for(m, 256), 256, 0, s>>>(m, keys, cnt);
-    KSPN_CHECK_LAUNCH();
-  }
-  exclusive_scan<uint64_t>(s, f_array_u32{ cnt }, n, bh, part64, &ctx->launches);
+  k_heads_from_sorted<<<grid_for(m + 1, 256), 256, 0, s>>>(n, m, keys, bh);
+  KSPN_CHECK_LAUNCH();
   ctx->launches += 2;
-  KSPN_CUDA(cudaStreamSynchronize(s)); // scratch is freed on return
+  (void)cnt;
+  (void)part64;
 }
 
 uint64_t
@@ -163,7 +159,7 @@ build_csr(kspn_context* ctx, uint32_t n, uint64_t m_raw, uint32_t* src, uint32_t
   size_t const hist_n = radix_hist_entries(m_raw);
   size_t const part_n = scan_partial_entries((hist_n > m_raw + 1 ? hist_n : m_raw + 1) + n + 1);
   scratch      sc;
-  alloc_scratch(sc, 3 * (m_raw + 64) * sizeof(uint32_t) + (hist_n + part_n + n + 64) * sizeof(uint64_t) + 4096);
+  alloc_scratch(ctx, sc, 3 * (m_raw + 64) * sizeof(uint32_t) + (hist_n + part_n + n + 64) * sizeof(uint64_t) + 4096);
   size_t    off    = 0;
   uint32_t* kalt   = sc.carve<uint32_t>(off, m_raw + 1);
   uint32_t* valt   = sc.carve<uint32_t>(off, m_raw + 1);
@@ -178,15 +174,20 @@ build_csr(kspn_context* ctx, uint32_t n, uint64_t m_raw, uint32_t* src, uint32_t
   radix_sort_pairs(ctx, dst, src, kalt, valt, m_raw, 0, b, hist, part);
   radix_sort_pairs(ctx, src, dst, kalt, valt, m_raw, 0, b, hist, part);
   exclusive_scan<uint32_t>(s, f_keep{ src, dst }, m_raw, pos, part, &ctx->launches);
-  KSPN_CUDA(cudaMemsetAsync(rowcnt, 0, (n + 1) * sizeof(uint32_t), s));
+  uint32_t m32 = 0;
+  KSPN_CUDA(cudaMemcpyAsync(&m32, pos + m_raw, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  KSPN_CUDA(cudaStreamSynchronize(s));
+  uint64_t const m = m32;
   if (m_raw) {
-    k_compact_edges<<<grid_for(m_raw, 256), 256, 0, s>>>(m_raw, src, dst, pos, csr, rowcnt);
+    k_compact_edges<<<grid_for(m_raw, 256), 256, 0, s>>>(m_raw, src, dst, pos, csr, kalt);
     KSPN_CHECK_LAUNCH();
     ctx->launches += 1;
   }
-  exclusive_scan<uint64_t>(s, f_array_u32{ rowcnt }, n, head, part64, &ctx->launches);
-  uint64_t m = 0;
-  KSPN_CUDA(cudaMemcpyAsync(&m, head + n, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+  k_heads_from_sorted<<<grid_for(m + 1, 256), 256, 0, s>>>(n, m, kalt, head);
+  KSPN_CHECK_LAUNCH();
+  ctx->launches += 1;
+  (void)rowcnt;
+  (void)part64;
   KSPN_CUDA(cudaStreamSynchronize(s));
   return m;
 }

@@ -30,12 +30,30 @@ constexpr int EX_ITEMS   = 8;
 constexpr int EX_TILE    = EX_THREADS * EX_ITEMS;
 constexpr int EX_BLOCKS  = 148 * 8;
 
-// counters used by an expansion (indices into a u32 device array)
-struct ex_ctrs
+// Frontier in/out queues.  With cur == nullptr (host-driven levels) the
+// input is (q0, n0) and the output (q1, n1); inside a device-driven loop
+// `cur` selects which pair is the input this level, so a captured graph can
+// alternate queues without host involvement.
+struct fio
 {
-  uint32_t const* qn;     // queue length (read)
-  uint32_t*       ntiles; // written by k_fs_partials
-  unsigned long long* edges; // running total of expanded edges (added)
+  uint32_t*       q0;
+  uint32_t*       q1;
+  uint32_t*       n0;
+  uint32_t*       n1;
+  uint32_t const* cur;
+  __device__ __forceinline__ bool            sw() const { return cur && (*cur & 1u); }
+  __device__ __forceinline__ uint32_t const* in() const { return sw() ? q1 : q0; }
+  __device__ __forceinline__ uint32_t        in_n() const { return sw() ? *n1 : *n0; }
+  __device__ __forceinline__ uint32_t*       out() const { return sw() ? q0 : q1; }
+  __device__ __forceinline__ uint32_t*       out_n() const { return sw() ? n0 : n1; }
+};
+
+// A kernel whose gate is closed returns at once (device-chosen direction).
+struct gate
+{
+  uint32_t const* word;
+  uint32_t        want;
+  __device__ __forceinline__ bool closed() const { return word && *word != want; }
 };
 
 __device__ __forceinline__ void
@@ -49,10 +67,11 @@ fs_chunk(uint32_t qn, uint32_t& beg, uint32_t& end)
 }
 
 static __global__ void __launch_bounds__(FS_THREADS)
-k_fs_reduce(uint64_t const* __restrict__ head, uint32_t const* __restrict__ q, uint32_t const* __restrict__ qn_ptr, uint64_t* __restrict__ partial)
+k_fs_reduce(uint64_t const* __restrict__ head, fio f, uint64_t* __restrict__ partial)
 {
-  uint32_t beg, end;
-  fs_chunk(*qn_ptr, beg, end);
+  uint32_t const* q = f.in();
+  uint32_t        beg, end;
+  fs_chunk(f.in_n(), beg, end);
   uint64_t s = 0;
   for (uint32_t i = beg + threadIdx.x; i < end; i += FS_THREADS) {
     uint32_t const v = q[i];
@@ -63,25 +82,29 @@ k_fs_reduce(uint64_t const* __restrict__ head, uint32_t const* __restrict__ q, u
   if (threadIdx.x == 0) partial[blockIdx.x] = total;
 }
 
+// prefix[qn] = total; *ntiles = tiles; *edges += total (nullable);
+// *last = total (nullable).
 static __global__ void __launch_bounds__(1024)
-k_fs_partials(uint64_t* __restrict__ partial, uint64_t* __restrict__ prefix, uint32_t const* __restrict__ qn_ptr, uint32_t* __restrict__ ntiles, unsigned long long* __restrict__ edges)
+k_fs_partials(uint64_t* __restrict__ partial, uint64_t* __restrict__ prefix, fio f, uint32_t* __restrict__ ntiles, unsigned long long* __restrict__ edges, unsigned long long* __restrict__ last)
 {
   uint64_t const v = threadIdx.x < FS_BLOCKS ? partial[threadIdx.x] : 0;
   uint64_t       total;
   uint64_t const pre = block_exclusive_scan<uint64_t, 1024>(v, &total);
   if (threadIdx.x < FS_BLOCKS) partial[threadIdx.x] = pre;
   if (threadIdx.x == 0) {
-    prefix[*qn_ptr] = total;
-    *ntiles         = static_cast<uint32_t>((total + EX_TILE - 1) / EX_TILE);
+    prefix[f.in_n()] = total;
+    *ntiles          = static_cast<uint32_t>((total + EX_TILE - 1) / EX_TILE);
     if (edges) *edges += total;
+    if (last) *last = total;
   }
 }
 
 static __global__ void __launch_bounds__(FS_THREADS)
-k_fs_down(uint64_t const* __restrict__ head, uint32_t const* __restrict__ q, uint32_t const* __restrict__ qn_ptr, uint64_t const* __restrict__ partial, uint64_t* __restrict__ prefix, uint32_t* __restrict__ tile_start)
+k_fs_down(uint64_t const* __restrict__ head, fio f, uint64_t const* __restrict__ partial, uint64_t* __restrict__ prefix, uint32_t* __restrict__ tile_start)
 {
-  uint32_t beg, end;
-  fs_chunk(*qn_ptr, beg, end);
+  uint32_t const* q = f.in();
+  uint32_t        beg, end;
+  fs_chunk(f.in_n(), beg, end);
   uint64_t run = partial[blockIdx.x];
   for (uint32_t base = beg; base < end; base += FS_THREADS) {
     uint32_t const i   = base + threadIdx.x;
@@ -136,23 +159,32 @@ tile_max_scan(uint32_t* s)
   __syncthreads();
 }
 
-// op(u, v, valid): u = source (queued vertex), v = neighbour.
+// op(u, v, valid) -> bool: u = source (queued vertex), v = neighbour; true
+// appends v to the output queue.  Called by every lane (valid == false on
+// padding lanes).
 template<typename Op>
 __global__ void __launch_bounds__(EX_THREADS)
 k_expand(uint64_t const* __restrict__ head,
          uint32_t const* __restrict__ adj,
-         uint32_t const* __restrict__ q,
-         uint32_t const* __restrict__ qn_ptr,
+         fio f,
          uint64_t const* __restrict__ prefix,
          uint32_t const* __restrict__ tile_start,
          uint32_t const* __restrict__ ntiles_ptr,
+         gate g,
          Op op)
 {
+  if (g.closed()) return;
   __shared__ uint32_t s_j[EX_TILE];
-  __shared__ uint32_t s_i0, s_i1;
-  uint32_t const      qn     = *qn_ptr;
+  __shared__ uint32_t s_out[EX_TILE];
+  __shared__ uint32_t s_i0, s_i1, s_n, s_base;
+  uint32_t const*     q      = f.in();
+  uint32_t* const     qout   = f.out();
+  uint32_t* const     qout_n = f.out_n();
+  uint32_t const      qn     = f.in_n();
   uint32_t const      ntiles = *ntiles_ptr;
   uint64_t const      total  = prefix[qn];
+  if (threadIdx.x == 0) s_n = 0;
+  block_queue bq{ s_out, &s_n };
   for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     uint64_t const t0 = static_cast<uint64_t>(tile) * EX_TILE;
     uint64_t const t1 = t0 + EX_TILE < total ? t0 + EX_TILE : total;
@@ -170,7 +202,7 @@ k_expand(uint64_t const* __restrict__ head,
     }
     __syncthreads();
     tile_max_scan(s_j);
-#pragma unroll 2
+#pragma unroll 4
     for (int k = 0; k < EX_ITEMS; ++k) {
       uint32_t const slot  = k * EX_THREADS + threadIdx.x;
       uint64_t const e     = t0 + slot;
@@ -181,9 +213,9 @@ k_expand(uint64_t const* __restrict__ head,
         u                = q[j];
         v                = adj[head[u] + (e - prefix[j])];
       }
-      op(u, v, valid);
+      bq.push(op(u, v, valid), v);
     }
-    __syncthreads();
+    bq.flush(qout, qout_n, &s_base);
   }
 }
 
@@ -198,20 +230,43 @@ expand_bytes(uint64_t frontier, uint64_t edges, uint64_t pushed, uint64_t extra_
 
 // Host: one top-down level over queue q (length at qn_dev), partials /
 // prefix / tile_start from the workspace.
-template<typename Op>
-void
-expand_level(kspn_context* ctx, uint64_t const* head, uint32_t const* adj, uint32_t const* q, uint32_t const* qn_dev, uint32_t* ntiles_dev, unsigned long long* edges_dev, uint32_t* tile_start, Op op)
+// Scan of the queue's degrees (prefix, tile starts, tile count).  The edge
+// total is added to *edges (nullable) and stored to *last (nullable).
+inline void
+frontier_scan(kspn_context* ctx, uint64_t const* head, fio f, uint32_t* ntiles_dev, unsigned long long* edges, unsigned long long* last, uint32_t* tile_start)
 {
   auto&              ws = ctx->ws;
   cudaStream_t const s  = ctx->stream;
-  k_fs_reduce<<<FS_BLOCKS, FS_THREADS, 0, s>>>(head, q, qn_dev, ws.blocks);
-  k_fs_partials<<<1, 1024, 0, s>>>(ws.blocks, ws.prefix, qn_dev, ntiles_dev, edges_dev);
-  k_fs_down<<<FS_BLOCKS, FS_THREADS, 0, s>>>(head, q, qn_dev, ws.blocks, ws.prefix, tile_start);
+  k_fs_reduce<<<FS_BLOCKS, FS_THREADS, 0, s>>>(head, f, ws.blocks);
+  k_fs_partials<<<1, 1024, 0, s>>>(ws.blocks, ws.prefix, f, ntiles_dev, edges, last);
+  k_fs_down<<<FS_BLOCKS, FS_THREADS, 0, s>>>(head, f, ws.blocks, ws.prefix, tile_start);
+  KSPN_CHECK_LAUNCH();
+  ctx->launches += 3;
+}
+
+// Expansion of a scanned queue; tiles_host bounds the grid (0: unknown,
+// use the full persistent grid).
+template<typename Op>
+void
+expand_scanned(kspn_context* ctx, uint64_t const* head, uint32_t const* adj, fio f, uint32_t* ntiles_dev, uint32_t* tile_start, uint64_t tiles_host, Op op)
+{
+  auto&          ws   = ctx->ws;
+  unsigned const grid = tiles_host ? static_cast<unsigned>(tiles_host < EX_BLOCKS ? tiles_host : EX_BLOCKS) : EX_BLOCKS;
   prof_start(ctx);
-  k_expand<Op><<<EX_BLOCKS, EX_THREADS, 0, s>>>(head, adj, q, qn_dev, ws.prefix, tile_start, ntiles_dev, op);
+  k_expand<Op><<<grid, EX_THREADS, 0, ctx->stream>>>(head, adj, f, ws.prefix, tile_start, ntiles_dev, gate{ nullptr, 0 }, op);
   prof_stop(ctx);
   KSPN_CHECK_LAUNCH();
-  ctx->launches += 4;
+  ctx->launches += 1;
+}
+
+// Host-driven level: input (q, *qn_in), output (qout, *qn_out).
+template<typename Op>
+void
+expand_level(kspn_context* ctx, uint64_t const* head, uint32_t const* adj, uint32_t* q, uint32_t* qn_in, uint32_t* ntiles_dev, unsigned long long* edges_dev, uint32_t* tile_start, uint32_t* qout, uint32_t* qout_n, Op op)
+{
+  fio const f{ q, qout, qn_in, qout_n, nullptr };
+  frontier_scan(ctx, head, f, ntiles_dev, edges_dev, nullptr, tile_start);
+  expand_scanned(ctx, head, adj, f, ntiles_dev, tile_start, 0, op);
 }
 
 } // namespace kspn

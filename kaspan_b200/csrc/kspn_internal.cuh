@@ -100,6 +100,46 @@ warp_push_active(uint32_t v, uint32_t* queue, uint32_t* count)
   queue[base + __popc(mask & ((1u << lane) - 1u))] = v;
 }
 
+// Block-aggregated append: pushes collected in shared memory during a tile (or sweep step)
+// are reserved in the global queue with ONE atomic per block and copied out
+// coalesced (a per-warp atomic on one counter serialises in L2 when a level
+// discovers millions of vertices).
+struct block_queue
+{
+  uint32_t* s_buf; // EX_TILE entries
+  uint32_t* s_n;
+  __device__ __forceinline__ void push(bool pred, uint32_t v)
+  {
+    unsigned const ballot = __ballot_sync(0xFFFFFFFFu, pred);
+    if (!ballot) return;
+    unsigned const lane   = threadIdx.x & 31u;
+    unsigned const leader = __ffs(ballot) - 1;
+    uint32_t       base   = 0;
+    if (lane == leader) base = atomicAdd(s_n, static_cast<uint32_t>(__popc(ballot)));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    if (pred) s_buf[base + __popc(ballot & ((1u << lane) - 1u))] = v;
+  }
+  // all threads; leaves s_n == 0 for the next tile
+  __device__ __forceinline__ void flush(uint32_t* queue, uint32_t* count, uint32_t* s_base)
+  {
+    __syncthreads();
+    uint32_t const cnt = *s_n;
+    if (cnt) {
+      if (threadIdx.x == 0) *s_base = atomicAdd(count, cnt);
+      __syncthreads();
+      uint32_t const b = *s_base;
+      for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) queue[b + i] = s_buf[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *s_n = 0;
+    __syncthreads();
+  }
+};
+
+// Dense vertex sweeps push through a block_queue of DENSE_BUF entries and
+// flush when fewer than one step's worth of slots is left.
+constexpr int DENSE_BUF = 2048;
+
 __device__ __forceinline__ uint32_t
 rotr32(uint32_t x, int r)
 {
@@ -155,6 +195,7 @@ struct workspace
   uint64_t* ctr64    = nullptr; // 8 (64-bit counters)
   uint64_t* pivot    = nullptr; // per-block pivot keys (4096 u64 products + 4096 u32 ids)
   uint32_t* tile_start = nullptr; // m / 2048 + 2 (frontier expansion)
+  void*     rstate     = nullptr; // 512 B device control block of a FW-BW
   // owned graph storage (host inputs, or a CSC built on device)
   uint64_t* g_fh = nullptr;
   uint32_t* g_fc = nullptr;
@@ -168,6 +209,50 @@ struct workspace
 
 } // namespace kspn
 
+namespace kspn {
+// Identity of a cached CUDA graph: the buffers its kernel arguments name.
+struct graph_key
+{
+  void const* a[7] = {};
+  uint32_t    n    = 0;
+  uint64_t    m    = 0;
+  graph_key() = default;
+  graph_key(void const* p0, void const* p1, void const* p2, void const* p3, void const* p4, void const* p5, void const* p6, uint32_t n_, uint64_t m_)
+    : a{ p0, p1, p2, p3, p4, p5, p6 }
+    , n(n_)
+    , m(m_)
+  {
+  }
+  bool operator==(graph_key const& o) const
+  {
+    for (int i = 0; i < 7; ++i)
+      if (a[i] != o.a[i]) return false;
+    return n == o.n && m == o.m;
+  }
+};
+// A device buffer owned by a context, grown on demand and reused by later
+// calls (host-pointer calls, graph construction scratch).
+struct dev_buffer
+{
+  void*  p     = nullptr;
+  size_t bytes = 0;
+};
+enum buffer_slot : int
+{
+  BUF_HOST_GRAPH = 0, // device copy of a host graph + output (kspn_scc)
+  BUF_BUILD      = 1, // radix-sort scratch (transpose, build_csr)
+  BUF_TRANSPOSE  = 2, // transpose built for kspn_scc_device without bw
+  BUF_COUNT      = 4
+};
+
+struct cached_graph
+{
+  graph_key       key;
+  cudaGraph_t     graph = nullptr;
+  cudaGraphExec_t exec  = nullptr;
+};
+} // namespace kspn
+
 struct kspn_context
 {
   int                device     = 0;
@@ -179,10 +264,14 @@ struct kspn_context
   int                rotation   = 0; // label-search calls made by this context
   cudaEvent_t        ev[KSPN_PHASES + 2] = {};
   uint64_t           launches   = 0;
+  uint64_t           td_edges   = 0; // top-down reachability edges (host tally; the rest count on device)
   std::string        last_error;
-  // kernel-class timing (kspn_options.profile): one event pair in flight
+  // kernel-class timing (kspn_options.profile): two event pairs in flight
   kspn_stats*        prof       = nullptr;
-  cudaEvent_t        pe[2]      = {};
+  cudaEvent_t        pe[4]      = {};
+  void*              h_state    = nullptr; // pinned 512 B mirror of ws.rstate
+  kspn::cached_graph fwbw;                 // one-launch FW-BW graph
+  kspn::dev_buffer   bufs[kspn::BUF_COUNT];
 };
 
 namespace kspn {
@@ -191,21 +280,21 @@ namespace kspn {
 // prof_add (after the stream was synchronised) books the elapsed time and
 // the algorithmic bytes of the bracketed work.
 inline void
-prof_start(kspn_context* ctx)
+prof_start(kspn_context* ctx, int pair = 0)
 {
-  if (ctx->prof) cudaEventRecord(ctx->pe[0], ctx->stream);
+  if (ctx->prof) cudaEventRecord(ctx->pe[2 * pair], ctx->stream);
 }
 inline void
-prof_stop(kspn_context* ctx)
+prof_stop(kspn_context* ctx, int pair = 0)
 {
-  if (ctx->prof) cudaEventRecord(ctx->pe[1], ctx->stream);
+  if (ctx->prof) cudaEventRecord(ctx->pe[2 * pair + 1], ctx->stream);
 }
 inline void
-prof_add(kspn_context* ctx, int cls, uint64_t bytes, uint64_t calls = 1)
+prof_add(kspn_context* ctx, int pair, int cls, uint64_t bytes, uint64_t calls = 1)
 {
   if (!ctx->prof) return;
   float ms = 0;
-  if (cudaEventElapsedTime(&ms, ctx->pe[0], ctx->pe[1]) != cudaSuccess) {
+  if (cudaEventElapsedTime(&ms, ctx->pe[2 * pair], ctx->pe[2 * pair + 1]) != cudaSuccess) {
     cudaGetLastError();
     return;
   }
@@ -215,7 +304,8 @@ prof_add(kspn_context* ctx, int cls, uint64_t bytes, uint64_t calls = 1)
 }
 
 // workspace / context helpers (context.cu)
-void ensure_workspace(kspn_context* ctx, uint32_t n, uint64_t m);
+void  ensure_workspace(kspn_context* ctx, uint32_t n, uint64_t m);
+void* context_buffer(kspn_context* ctx, int slot, size_t bytes); // grown on demand, kept
 void read_counters(kspn_context* ctx); // D2H of ws.ctr / ws.ctr64 + stream sync
 void zero_counters(kspn_context* ctx);
 int  fail(kspn_context* ctx, error const& e);
@@ -230,13 +320,18 @@ uint32_t select_pivot_live(kspn_context* ctx, dgraph const& g, uint32_t const* u
 uint32_t count_undecided(kspn_context* ctx, uint32_t n, uint32_t const* und);
 
 // reach.cu
-uint32_t fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t pivot, kspn_options const& opt, kspn_stats* st);
+size_t reach_state_bytes();
+void   release_graphs(kspn_context* ctx);
+// min_ids: name the SCC after its smallest member (else the pivot, as the reference does)
+uint32_t fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t pivot, kspn_options const& opt, kspn_stats* st, bool min_ids);
 
 // label.cu
 uint32_t label_search(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, int rotation, kspn_options const& opt, kspn_stats* st);
 
 // canon.cu
-void canonicalise(kspn_context* ctx, uint32_t n, uint32_t* scc_id, uint32_t* scratch);
+// members: every id is a member of its own class (pipeline output); else
+// arbitrary ids < n (normalise_scc_id semantics).
+void canonicalise(kspn_context* ctx, uint32_t n, uint32_t* scc_id, uint32_t* scratch, bool members);
 
 // csr.cu
 void     transpose(kspn_context* ctx, uint32_t n, uint64_t m, uint64_t const* fh, uint32_t const* fc, uint64_t* bh, uint32_t* bc, uint32_t* scratch_n);

@@ -33,13 +33,22 @@ l_grid(uint64_t items)
 __global__ void __launch_bounds__(L_THREADS)
 k_label_init(uint32_t n, uint32_t const* __restrict__ und, uint32_t* __restrict__ label, int rot, uint32_t* __restrict__ q, uint32_t* __restrict__ qn)
 {
-  uint64_t const span = (static_cast<uint64_t>(n) + 31) & ~31ull;
-  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * L_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * L_THREADS) {
+  __shared__ uint32_t s_buf[DENSE_BUF];
+  __shared__ uint32_t s_n, s_base;
+  if (threadIdx.x == 0) s_n = 0;
+  __syncthreads();
+  block_queue    bq{ s_buf, &s_n };
+  uint64_t const span = (static_cast<uint64_t>(n) + L_THREADS - 1) / L_THREADS * L_THREADS;
+  for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * L_THREADS; base < span; base += static_cast<uint64_t>(gridDim.x) * L_THREADS) {
+    uint64_t const t    = base + threadIdx.x;
     uint32_t const v    = static_cast<uint32_t>(t);
     bool const     live = t < n && bit_get(und, v);
     if (t < n) label[v] = live ? rotr32(v, rot) : UNDECIDED;
-    warp_push(live, v, q, qn);
+    bq.push(live, v);
+    __syncthreads();
+    if (s_n > DENSE_BUF - L_THREADS) bq.flush(q, qn, &s_base);
   }
+  bq.flush(q, qn, &s_base);
 }
 
 struct label_fw_op
@@ -47,19 +56,13 @@ struct label_fw_op
   uint32_t const* und;
   uint32_t*       label;
   uint32_t*       claim_next;
-  uint32_t*       qout;
-  uint32_t*       qout_n;
-  __device__ __forceinline__ void operator()(uint32_t u, uint32_t v, bool valid) const
+  __device__ __forceinline__ bool operator()(uint32_t u, uint32_t v, bool valid) const
   {
-    bool won = false;
-    if (valid && bit_get(und, v)) {
-      uint32_t const lu = __ldcg(label + u);
-      if (lu < __ldcg(label + v)) {
-        uint32_t const old = atomicMin(label + v, lu);
-        won                = lu < old && bit_claim(claim_next, v);
-      }
-    }
-    warp_push(won, v, qout, qout_n);
+    if (!valid || !bit_get(und, v)) return false;
+    uint32_t const lu = __ldcg(label + u);
+    if (lu >= __ldcg(label + v)) return false;
+    uint32_t const old = atomicMin(label + v, lu);
+    return lu < old && bit_claim(claim_next, v);
   }
 };
 
@@ -79,9 +82,15 @@ k_unclaim(uint32_t const* __restrict__ q, uint32_t const* __restrict__ qn_ptr, u
 __global__ void __launch_bounds__(L_THREADS)
 k_label_roots(uint32_t n, uint32_t* __restrict__ und, uint32_t const* __restrict__ label, uint32_t* __restrict__ scc_id, int rot, uint32_t* __restrict__ q, uint32_t* __restrict__ qn, uint32_t* __restrict__ decided)
 {
-  uint64_t const span = (static_cast<uint64_t>(n) + 31) & ~31ull;
+  __shared__ uint32_t s_buf[DENSE_BUF];
+  __shared__ uint32_t s_n, s_base;
+  if (threadIdx.x == 0) s_n = 0;
+  __syncthreads();
+  block_queue    bq{ s_buf, &s_n };
+  uint64_t const span = (static_cast<uint64_t>(n) + L_THREADS - 1) / L_THREADS * L_THREADS;
   uint32_t       dec  = 0;
-  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * L_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * L_THREADS) {
+  for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * L_THREADS; base < span; base += static_cast<uint64_t>(gridDim.x) * L_THREADS) {
+    uint64_t const t    = base + threadIdx.x;
     uint32_t const v    = static_cast<uint32_t>(t);
     bool const     root = t < n && bit_get(und, v) && label[v] == rotr32(v, rot);
     bool const     won  = root && bit_take(und, v);
@@ -89,8 +98,11 @@ k_label_roots(uint32_t n, uint32_t* __restrict__ und, uint32_t const* __restrict
       scc_id[v] = v;
       ++dec;
     }
-    warp_push(won, v, q, qn);
+    bq.push(won, v);
+    __syncthreads();
+    if (s_n > DENSE_BUF - L_THREADS) bq.flush(q, qn, &s_base);
   }
+  bq.flush(q, qn, &s_base);
   if (dec) atomicAdd(decided, dec);
 }
 
@@ -100,21 +112,14 @@ struct label_bw_op
   uint32_t const* label;
   uint32_t*       scc_id;
   int             rot;
-  uint32_t*       qout;
-  uint32_t*       qout_n;
-  uint32_t*       decided;
-  // u = decided vertex, v = one of its in-neighbours
-  __device__ __forceinline__ void operator()(uint32_t u, uint32_t v, bool valid) const
+  // u = decided vertex, v = one of its in-neighbours; every push is a decision
+  __device__ __forceinline__ bool operator()(uint32_t u, uint32_t v, bool valid) const
   {
-    bool won = false;
-    if (valid && bit_get(und, v)) {
-      uint32_t const lu = label[u];
-      won               = label[v] == lu && bit_take(und, v);
-      if (won) scc_id[v] = rotl32(lu, rot);
-    }
-    unsigned const b = __ballot_sync(0xFFFFFFFFu, won);
-    if (b && (threadIdx.x & 31) == 0) atomicAdd(decided, static_cast<uint32_t>(__popc(b)));
-    warp_push(won, v, qout, qout_n);
+    if (!valid || !bit_get(und, v)) return false;
+    uint32_t const lu = label[u];
+    if (label[v] != lu || !bit_take(und, v)) return false;
+    scc_id[v] = rotl32(lu, rot);
+    return true;
   }
 };
 
@@ -151,11 +156,10 @@ label_search(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id
       k_unclaim<<<l_grid(g.n), L_THREADS, 0, ctx->stream>>>(q[cur], qc[cur], claim[cur]);
       ctx->launches += 1;
     }
-    label_fw_op op{ und, ws.label, claim[nxt], q[nxt], qc[nxt] };
-    expand_level(ctx, g.fh, g.fc, q[cur], qc[cur], ws.ctr + CTR_NTILES, edges, ws.tile_start, op);
+    expand_level(ctx, g.fh, g.fc, q[cur], qc[cur], ws.ctr + CTR_NTILES, edges, ws.tile_start, q[nxt], qc[nxt], label_fw_op{ und, ws.label, claim[nxt] });
     read_counters(ctx);
     uint32_t const qn = ctx->h_ctr[CTR_Q0 + nxt];
-    prof_add(ctx, KSPN_KERNEL_EXPAND, expand_bytes(qn_cur, ctx->h_ctr64[0] - e0, qn, 4)); // + label[u] read per row
+    prof_add(ctx, 0, KSPN_KERNEL_EXPAND, expand_bytes(qn_cur, ctx->h_ctr64[0] - e0, qn, 4)); // + label[u] read per row
     e0     = ctx->h_ctr64[0];
     qn_cur = qn;
     if (qn == 0) break;
@@ -169,24 +173,23 @@ label_search(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id
   KSPN_CHECK_LAUNCH();
   ctx->launches += 1;
   read_counters(ctx);
-  cur = 0;
+  uint32_t decided = ctx->h_ctr[CTR_DECIDED];
+  cur              = 0;
   for (uint32_t level = 0; ctx->h_ctr[CTR_Q0 + cur] > 0; ++level) {
     if (level >= cap) throw error{ KSPN_ERR_TIMEOUT, "label search: closure cap exceeded" };
     int const nxt = cur ^ 1;
     KSPN_CUDA(cudaMemsetAsync(qc[nxt], 0, sizeof(uint32_t), ctx->stream));
     uint32_t const fq = ctx->h_ctr[CTR_Q0 + cur];
     uint64_t const eb = ctx->h_ctr64[0];
-    label_bw_op op{ und, ws.label, scc_id, rotation, q[nxt], qc[nxt], ws.ctr + CTR_DECIDED };
-    expand_level(ctx, g.bh, g.bc, q[cur], qc[cur], ws.ctr + CTR_NTILES, edges, ws.tile_start, op);
+    expand_level(ctx, g.bh, g.bc, q[cur], qc[cur], ws.ctr + CTR_NTILES, edges, ws.tile_start, q[nxt], qc[nxt], label_bw_op{ und, ws.label, scc_id, rotation });
     read_counters(ctx);
-    prof_add(ctx, KSPN_KERNEL_EXPAND, expand_bytes(fq, ctx->h_ctr64[0] - eb, ctx->h_ctr[CTR_Q0 + nxt], 4));
+    uint32_t const pushed = ctx->h_ctr[CTR_Q0 + nxt];
+    decided += pushed;
+    prof_add(ctx, 0, KSPN_KERNEL_EXPAND, expand_bytes(fq, ctx->h_ctr64[0] - eb, pushed, 4));
     cur = nxt;
   }
-  if (st) {
-    st->label_calls += 1;
-    st->edges_scanned = ctx->h_ctr64[0];
-  }
-  return ctx->h_ctr[CTR_DECIDED];
+  if (st) st->label_calls += 1;
+  return decided;
 }
 
 } // namespace kspn

@@ -46,8 +46,11 @@ k_radix_scatter(uint32_t const* __restrict__ kin,
                 uint32_t num_tiles)
 {
   __shared__ uint32_t tile_base[256];
+  __shared__ uint32_t local_off[256];
   __shared__ uint32_t run[256];
-  __shared__ uint32_t wcnt[2][RX_WARPS][256];
+  __shared__ uint16_t wcnt[2][RX_WARPS][256];
+  __shared__ uint32_t s_key[RX_TILE];
+  __shared__ uint32_t s_val[RX_TILE];
 
   unsigned const t = threadIdx.x, w = t >> 5, lane = t & 31u;
   tile_base[t]     = hist_scanned[static_cast<uint64_t>(t) * num_tiles + blockIdx.x];
@@ -58,34 +61,71 @@ k_radix_scatter(uint32_t const* __restrict__ kin,
 
   uint64_t const base    = static_cast<uint64_t>(blockIdx.x) * RX_TILE;
   unsigned const lane_lt = (1u << lane) - 1u;
+  uint32_t       key[RX_ITEMS], val[RX_ITEMS], pos[RX_ITEMS];
+  // 1. stable rank of every key among the tile's keys of the same digit
+#pragma unroll
   for (int r = 0; r < RX_ITEMS; ++r) {
     int const      buf   = r & 1;
     uint64_t const i     = base + static_cast<uint64_t>(r) * RX_THREADS + t;
     bool const     valid = i < count;
-    uint32_t const key   = valid ? kin[i] : 0u;
-    uint32_t const val   = valid ? vin[i] : 0u;
-    uint32_t const d     = valid ? ((key >> shift) & 255u) : 0x100u;
+    key[r]               = valid ? kin[i] : 0u;
+    val[r]               = valid ? vin[i] : 0u;
+    uint32_t const d     = valid ? ((key[r] >> shift) & 255u) : 0x100u;
     unsigned const peers = __match_any_sync(0xFFFFFFFFu, d);
     unsigned const rank  = __popc(peers & lane_lt);
-    if (valid && rank == 0) wcnt[buf][w][d] = __popc(peers);
+    if (valid && rank == 0) wcnt[buf][w][d] = static_cast<uint16_t>(__popc(peers));
     __syncthreads();
     {
       uint32_t acc = run[t];
 #pragma unroll
       for (int ww = 0; ww < RX_WARPS; ++ww) {
-        uint32_t const c   = wcnt[buf][ww][t];
-        wcnt[buf][ww][t]   = acc;
+        uint32_t const c     = wcnt[buf][ww][t];
+        wcnt[buf][ww][t]     = static_cast<uint16_t>(acc);
         wcnt[buf ^ 1][ww][t] = 0;
         acc += c;
       }
       run[t] = acc;
     }
     __syncthreads();
-    if (valid) {
-      uint32_t const pos = tile_base[d] + wcnt[buf][w][d] + rank;
-      kout[pos]          = key;
-      vout[pos]          = val;
+    pos[r] = valid ? wcnt[buf][w][d] + rank : 0xFFFFFFFFu;
+  }
+  // 2. digit offsets inside the tile, keys staged in digit order
+  {
+    uint32_t const c = run[t];
+    uint32_t       x = c;
+#pragma unroll
+    for (int dd = 1; dd < 32; dd <<= 1) {
+      uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, x, dd);
+      if (lane >= static_cast<unsigned>(dd)) x += y;
     }
+    __shared__ uint32_t wsum[RX_WARPS];
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    uint32_t carry = 0;
+    for (unsigned k = 0; k < w; ++k) carry += wsum[k];
+    local_off[t] = carry + x - c;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < RX_ITEMS; ++r) {
+    if (pos[r] != 0xFFFFFFFFu) {
+      uint32_t const d   = (key[r] >> shift) & 255u;
+      uint32_t const p   = local_off[d] + pos[r];
+      s_key[p]           = key[r];
+      s_val[p]           = val[r];
+    }
+  }
+  __syncthreads();
+  // 3. coalesced write-out: consecutive slots of one digit go to
+  //    consecutive global positions
+  uint64_t const left = count - base;
+  uint32_t const n    = left < RX_TILE ? static_cast<uint32_t>(left) : RX_TILE;
+  for (uint32_t p = t; p < n; p += RX_THREADS) {
+    uint32_t const k = s_key[p];
+    uint32_t const d = (k >> shift) & 255u;
+    uint32_t const o = tile_base[d] + (p - local_off[d]);
+    kout[o]          = k;
+    vout[o]          = s_val[p];
   }
 }
 

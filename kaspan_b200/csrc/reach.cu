@@ -6,22 +6,44 @@
 //   BW  = vertices of FW that reach the pivot through FW vertices
 //   BW is the pivot's SCC; each member is decided with id = pivot.
 // The reference walks a LIFO stack on one core; here each search is a
-// level-synchronous, direction-optimising reachability:
-//   top-down  : load-balanced expansion of the frontier's rows (expand.cuh),
-//               visited set = a bitmap claimed with atomicOr;
+// level-synchronous, direction-optimising reachability (Beamer, Asanovic,
+// Patterson, SC'12), of which only the reached SET matters:
+//   top-down  : load-balanced expansion of the frontier's rows (expand.cuh);
 //   bottom-up : every candidate scans its opposite-direction row and stops
-//               at the first visited neighbour (used while the frontier is a
-//               large share of the candidates).
-// Only the reached SET matters, which neither order changes.
+//               at the first visited neighbour.
+// Before each level the frontier's edge count m_f is known (frontier scan);
+// the level runs bottom-up when m_f > m_u / alpha (m_u: edges not yet
+// explored) and returns top-down when the frontier holds fewer than
+// n_candidates / beta vertices.
+//
+// Vertex state per search, one bit each (u32 words, atomics on words):
+//   FW: cand = undecided and not yet reached (a copy of und, bits taken on
+//       discovery), vis_a = reached;
+//   BW: vis_a = FW-reached and not yet BW-reached (bits taken on discovery),
+//       vis_b = BW-reached.
+// Each edge costs at most one probe and each discovery two atomics; the
+// undecided set and ids are written once at the end, a word at a time.
+//
+// Level control lives on the device (reach_state): a `decide` kernel picks
+// the direction from the scan, both expansion kernels are launched and the
+// one whose gate is closed returns at once, and an `advance` kernel flips the
+// queues and sets the loop condition.  The whole FW-BW is ONE CUDA graph
+// launch with two conditional while-nodes (one per search); with profiling
+// on, the same kernels run from a host loop with CUDA events around the
+// expansion kernels.
 #include "expand.cuh"
+
+#include <cstring>
+#include <tuple>
 
 namespace kspn {
 
 namespace {
 
-constexpr int      R_THREADS = 256;
-constexpr int      CTR_NTILES = 8;
-constexpr int      R_BIG      = 32;
+constexpr int R_THREADS = 256;
+constexpr int R_BIG     = 32;
+constexpr int BU_BUF    = 2048;
+constexpr int BU_ILP    = 4;
 
 unsigned
 r_grid(uint64_t items)
@@ -30,252 +52,513 @@ r_grid(uint64_t items)
   return static_cast<unsigned>(b < 148ull * 8 ? (b ? b : 1) : 148ull * 8);
 }
 
-__global__ void
-k_reach_seed(uint32_t* vis, uint32_t* q, uint32_t* qn, uint32_t pivot)
+// Device-side control block of one FW-BW (lives in the workspace).
+struct reach_state
 {
-  q[0]  = pivot;
-  *qn   = 1;
-  vis[pivot >> 5] |= 1u << (pivot & 31);
+  uint32_t           cur;      // frontier selector (fio)
+  uint32_t           qn[2];    // queue lengths
+  uint32_t           mode;     // 0 top-down, 1 bottom-up
+  uint32_t           level;    // levels of the running search
+  uint32_t           cap;      // level cap per search
+  uint32_t           err;      // 1: a search hit the cap
+  uint32_t           ntiles;   // frontier tiles (scan)
+  uint32_t           bu;       // bottom-up levels of the running search
+  uint32_t           pivot;
+  uint32_t           n_und;    // undecided vertices (candidates of FW)
+  uint32_t           id;       // id given to the SCC
+  uint32_t           decided;  // SCC size
+  uint32_t           min_ids;  // 1: id = smallest member, 0: id = pivot
+  uint32_t           levels_fw, bu_fw, levels_bw, bu_bw;
+  unsigned long long m_u, m_out, m_in, m_f, alpha, beta;
+  unsigned long long edges_td, edges_bu, cands_bu;
+};
+static_assert(sizeof(reach_state) <= 512, "reach_state must fit its workspace slot");
+
+__global__ void __launch_bounds__(R_THREADS)
+k_r_init(uint32_t words, uint32_t const* __restrict__ und, uint32_t* __restrict__ cand, uint32_t* __restrict__ vis_a, uint32_t* __restrict__ vis_b, reach_state* st)
+{
+  for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) {
+    cand[w]  = und[w];
+    vis_a[w] = 0;
+    vis_b[w] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->n_und = 0;
+    st->m_out = st->m_in = 0;
+    st->edges_td = st->edges_bu = st->cands_bu = 0;
+    st->err                                    = 0;
+    st->decided                                = 0;
+    st->levels_fw = st->bu_fw = st->levels_bw = st->bu_bw = 0;
+  }
 }
 
-// BW seed: the pivot leaves FW, joins BW, is decided with id = itself.
-__global__ void
-k_bw_seed(uint32_t* fwvis, uint32_t* bwvis, uint32_t* und, uint32_t* scc_id, uint32_t* q, uint32_t* qn, uint32_t pivot)
+// n_und, and the out-/in-degree sums of undecided vertices.
+__global__ void __launch_bounds__(R_THREADS)
+k_und_degrees(uint32_t n, uint32_t const* __restrict__ und, uint64_t const* __restrict__ fh, uint64_t const* __restrict__ bh, reach_state* st)
 {
-  uint32_t const mask = 1u << (pivot & 31);
-  fwvis[pivot >> 5] &= ~mask;
-  bwvis[pivot >> 5] |= mask;
-  und[pivot >> 5] &= ~mask;
-  scc_id[pivot] = pivot;
-  q[0]          = pivot;
-  *qn           = 1;
+  uint64_t       so = 0, si = 0;
+  uint32_t       c  = 0;
+  unsigned const lane = threadIdx.x & 31u;
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; t < n; t += static_cast<uint64_t>(gridDim.x) * R_THREADS) {
+    uint32_t const v = static_cast<uint32_t>(t);
+    if (!bit_get(und, v)) continue;
+    ++c;
+    so += fh[v + 1] - fh[v];
+    si += bh[v + 1] - bh[v];
+  }
+#pragma unroll
+  for (int s = 16; s; s >>= 1) {
+    c += __shfl_down_sync(0xFFFFFFFFu, c, s);
+    so += __shfl_down_sync(0xFFFFFFFFu, so, s);
+    si += __shfl_down_sync(0xFFFFFFFFu, si, s);
+  }
+  if (lane == 0) {
+    if (c) atomicAdd(&st->n_und, c);
+    if (so) atomicAdd(&st->m_out, static_cast<unsigned long long>(so));
+    if (si) atomicAdd(&st->m_in, static_cast<unsigned long long>(si));
+  }
 }
 
-struct fw_td_op
-{
-  uint32_t const* und;
-  uint32_t*       vis;
-  uint32_t*       qout;
-  uint32_t*       qout_n;
-  __device__ __forceinline__ void operator()(uint32_t, uint32_t v, bool valid) const
-  {
-    bool const won = valid && bit_get(und, v) && !bit_get(vis, v) && bit_claim(vis, v);
-    warp_push(won, v, qout, qout_n);
-  }
-};
-
-struct bw_td_op
-{
-  uint32_t* fwvis;
-  uint32_t* bwvis;
-  uint32_t* und;
-  uint32_t* scc_id;
-  uint32_t  pivot;
-  uint32_t* qout;
-  uint32_t* qout_n;
-  uint32_t* decided;
-  __device__ __forceinline__ void operator()(uint32_t, uint32_t v, bool valid) const
-  {
-    bool const won = valid && bit_get(fwvis, v) && bit_take(fwvis, v);
-    if (won) {
-      bit_take(und, v);
-      bit_claim(bwvis, v);
-      scc_id[v] = pivot;
-    }
-    unsigned const b = __ballot_sync(0xFFFFFFFFu, won);
-    if (b && (threadIdx.x & 31) == 0) atomicAdd(decided, static_cast<uint32_t>(__popc(b)));
-    warp_push(won, v, qout, qout_n);
-  }
-};
-
-// Bottom-up sweep.  Candidates: FW = undecided and not visited; BW =
-// FW-visited (not yet BW-visited).  A candidate joins when a neighbour in
-// `row` (FW: in-edges, BW: out-edges) is in `seen`.
+// Starts a search at the pivot: taken from `avail`, set in `mark`.
 template<bool BW>
+__global__ void
+k_r_seed(uint32_t* avail, uint32_t* mark, uint32_t* q0, reach_state* st)
+{
+  uint32_t const p = st->pivot;
+  uint32_t const m = 1u << (p & 31);
+  avail[p >> 5] &= ~m;
+  mark[p >> 5] |= m;
+  q0[0]     = p;
+  st->qn[0] = 1;
+  st->qn[1] = 0;
+  st->cur   = 0;
+  st->level = 0;
+  st->bu    = 0;
+  st->mode  = 0;
+  st->m_u   = BW ? st->m_in : st->m_out;
+}
+
+__global__ void
+k_r_decide(reach_state* st)
+{
+  unsigned long long const mf = st->m_f;
+  uint32_t const           qn = st->qn[st->cur & 1u];
+  if (st->mode == 0 && mf * st->alpha > st->m_u) st->mode = 1;
+  else if (st->mode == 1 && static_cast<unsigned long long>(qn) * st->beta < st->n_und && mf * st->alpha <= st->m_u) st->mode = 0;
+  st->qn[(st->cur & 1u) ^ 1u] = 0;
+  if (st->mode == 0) st->edges_td += mf;
+}
+
+template<bool BW>
+__global__ void
+k_r_advance(reach_state* st, cudaGraphConditionalHandle h, int in_graph)
+{
+  unsigned long long const mf = st->m_f;
+  st->m_u                     = st->m_u > mf ? st->m_u - mf : 0;
+  st->level += 1;
+  st->bu += st->mode;
+  st->cur ^= 1u;
+  unsigned cond = st->qn[st->cur & 1u] > 0;
+  if (cond && st->level >= st->cap) {
+    st->err = 1;
+    cond    = 0;
+  }
+  if (!cond) {
+    if (BW) st->levels_bw = st->level, st->bu_bw = st->bu;
+    else st->levels_fw = st->level, st->bu_fw = st->bu;
+  }
+  if (in_graph) cudaGraphSetConditional(h, cond);
+}
+
+// top-down, both directions: v joins when its bit in `avail` is taken
+struct take_op
+{
+  uint32_t* avail; // FW: cand; BW: vis_a
+  uint32_t* mark;  // FW: vis_a; BW: vis_b
+  __device__ __forceinline__ bool operator()(uint32_t, uint32_t v, bool valid) const
+  {
+    if (!valid || !bit_get(avail, v) || !bit_take(avail, v)) return false;
+    bit_claim(mark, v);
+    return true;
+  }
+};
+
+// Bottom-up sweep: candidates are the set bits of `avail`; a candidate
+// joins (taken from avail, set in mark, queued) when a neighbour in its
+// `head/adj` row is in `mark`.  Each thread carries BU_ILP candidates at once
+// (interleaved row walks) so their dependent loads overlap; rows of R_BIG+
+// entries are walked by the whole warp.
 __global__ void __launch_bounds__(R_THREADS)
 k_bottom_up(uint32_t n,
             uint64_t const* __restrict__ head,
             uint32_t const* __restrict__ adj,
-            uint32_t* __restrict__ und,
-            uint32_t* __restrict__ cand_bm, // FW: vis (claimed into); BW: fwvis (taken from)
-            uint32_t* __restrict__ seen,    // FW: vis;                  BW: bwvis
-            uint32_t* __restrict__ scc_id,
-            uint32_t pivot,
-            uint32_t* __restrict__ qout,
-            uint32_t* __restrict__ qout_n,
-            uint32_t* __restrict__ decided,
-            unsigned long long* __restrict__ edges)
+            uint32_t* __restrict__ avail,
+            uint32_t* __restrict__ mark,
+            fio f,
+            gate g,
+            reach_state* st)
 {
-  unsigned const lane  = threadIdx.x & 31u;
-  uint64_t const span  = (static_cast<uint64_t>(n) + 31) & ~31ull;
-  uint64_t       nedge = 0, ncand = 0;
-  uint32_t       ndec  = 0;
-  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * R_THREADS) {
-    uint32_t const v = static_cast<uint32_t>(t);
-    bool           cand;
-    if (BW) cand = t < n && bit_get(cand_bm, v);
-    else cand = t < n && bit_get(und, v) && !bit_get(cand_bm, v);
-    uint64_t b = 0, e = 0;
-    if (cand) b = head[v], e = head[v + 1], ++ncand;
-    bool       found = false;
-    bool const big   = cand && (e - b) >= R_BIG;
-    if (cand && !big) {
-      for (uint64_t x = b; x < e; ++x) {
-        ++nedge;
-        if (bit_get(seen, adj[x])) {
-          found = true;
-          break;
+  if (g.closed()) return;
+  __shared__ uint32_t s_buf[BU_BUF];
+  __shared__ uint32_t s_n, s_base;
+  if (threadIdx.x == 0) s_n = 0;
+  __syncthreads();
+  uint32_t* const qout   = f.out();
+  uint32_t* const qout_n = f.out_n();
+  block_queue     bq{ s_buf, &s_n };
+  unsigned const  lane  = threadIdx.x & 31u;
+  uint64_t const  step  = static_cast<uint64_t>(R_THREADS) * BU_ILP;
+  uint64_t const  span  = (static_cast<uint64_t>(n) + step - 1) / step * step;
+  uint64_t        nedge = 0, ncand = 0;
+  for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * step; base < span; base += static_cast<uint64_t>(gridDim.x) * step) {
+    uint32_t v[BU_ILP];
+    uint64_t b[BU_ILP], e[BU_ILP];
+    bool     live[BU_ILP], found[BU_ILP];
+#pragma unroll
+    for (int k = 0; k < BU_ILP; ++k) {
+      uint64_t const t = base + static_cast<uint64_t>(k) * R_THREADS + threadIdx.x;
+      v[k]             = static_cast<uint32_t>(t);
+      bool const cand  = t < n && bit_get(avail, v[k]);
+      b[k] = e[k] = 0;
+      if (cand) b[k] = head[v[k]], e[k] = head[v[k] + 1];
+      ncand += cand;
+      found[k] = false;
+      live[k]  = cand && (e[k] - b[k]) < R_BIG; // walked by this thread
+    }
+    // interleaved walks of the short rows
+    for (;;) {
+      bool any = false;
+#pragma unroll
+      for (int k = 0; k < BU_ILP; ++k) {
+        if (live[k] && b[k] < e[k]) {
+          uint32_t const w = adj[b[k]++];
+          ++nedge;
+          if (bit_get(mark, w)) found[k] = true, live[k] = false;
+          any = true;
+        } else {
+          live[k] = false;
         }
       }
+      if (!any) break;
     }
-    unsigned todo = __ballot_sync(0xFFFFFFFFu, big);
-    while (todo) {
-      unsigned const l = __ffs(todo) - 1;
-      todo &= todo - 1;
-      uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b, l), e0 = __shfl_sync(0xFFFFFFFFu, e, l);
-      bool           hit = false;
-      for (uint64_t x = b0; x < e0; x += 32) {
-        bool const mine = x + lane < e0 && bit_get(seen, adj[x + lane]);
-        nedge += (x + lane < e0);
-        if (__any_sync(0xFFFFFFFFu, mine)) {
-          hit = true;
-          break;
+    // long rows: the whole warp, one row at a time
+#pragma unroll
+    for (int k = 0; k < BU_ILP; ++k) {
+      bool const big  = (e[k] - b[k]) >= R_BIG && !found[k];
+      unsigned   todo = __ballot_sync(0xFFFFFFFFu, big);
+      while (todo) {
+        unsigned const l = __ffs(todo) - 1;
+        todo &= todo - 1;
+        uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b[k], l), e0 = __shfl_sync(0xFFFFFFFFu, e[k], l);
+        bool           hit = false;
+        for (uint64_t x = b0; x < e0; x += 32) {
+          bool const in   = x + lane < e0;
+          bool const mine = in && bit_get(mark, adj[x + lane]);
+          nedge += in;
+          if (__any_sync(0xFFFFFFFFu, mine)) {
+            hit = true;
+            break;
+          }
         }
-      }
-      if (lane == l) found = hit;
-    }
-    bool won = false;
-    if (found) {
-      if (BW) {
-        won = bit_take(cand_bm, v);
-        if (won) {
-          bit_take(und, v);
-          bit_claim(seen, v);
-          scc_id[v] = pivot;
-          ++ndec;
-        }
-      } else {
-        won = bit_claim(cand_bm, v);
+        if (lane == l) found[k] = hit;
       }
     }
-    warp_push(won, v, qout, qout_n);
+#pragma unroll
+    for (int k = 0; k < BU_ILP; ++k) {
+      bool const won = found[k] && bit_take(avail, v[k]);
+      if (won) bit_claim(mark, v[k]);
+      bq.push(won, v[k]);
+    }
+    __syncthreads();
+    if (s_n > BU_BUF - static_cast<uint32_t>(step)) bq.flush(qout, qout_n, &s_base);
   }
+  bq.flush(qout, qout_n, &s_base);
 #pragma unroll
   for (int s = 16; s; s >>= 1) {
     nedge += __shfl_down_sync(0xFFFFFFFFu, nedge, s);
     ncand += __shfl_down_sync(0xFFFFFFFFu, ncand, s);
-    ndec += __shfl_down_sync(0xFFFFFFFFu, ndec, s);
   }
   if (lane == 0) {
-    if (nedge) atomicAdd(edges, static_cast<unsigned long long>(nedge));
-    if (ncand) atomicAdd(edges + 1, static_cast<unsigned long long>(ncand));
-    if (ndec) atomicAdd(decided, ndec);
+    if (nedge) atomicAdd(&st->edges_bu, static_cast<unsigned long long>(nedge));
+    if (ncand) atomicAdd(&st->cands_bu, static_cast<unsigned long long>(ncand));
   }
 }
 
-struct search_result
+__global__ void
+k_r_setid(reach_state* st)
 {
-  uint32_t levels    = 0;
-  uint32_t bottom_up = 0;
+  st->id = st->min_ids ? UNDECIDED : st->pivot;
+}
+
+// Smallest member of the SCC (first set bit of vis_b) into st->id when
+// min_ids is set; one atomic per block.
+__global__ void __launch_bounds__(R_THREADS)
+k_bitmap_min(uint32_t n, uint32_t const* __restrict__ bm, reach_state* st)
+{
+  if (!st->min_ids) return;
+  __shared__ uint32_t s_min;
+  if (threadIdx.x == 0) s_min = UNDECIDED;
+  __syncthreads();
+  uint32_t const words = (n + 31) / 32;
+  uint32_t       best  = UNDECIDED;
+  for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) {
+    uint32_t const s = bm[w];
+    if (s) {
+      best = min(best, w * 32 + (__ffs(s) - 1));
+      break; // later words of this thread only hold larger ids
+    }
+  }
+  best = __reduce_min_sync(0xFFFFFFFFu, best);
+  if ((threadIdx.x & 31) == 0 && best != UNDECIDED) atomicMin(&s_min, best);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_min != UNDECIDED) atomicMin(&st->id, s_min);
+}
+
+// The SCC is vis_b: it leaves the undecided set with id st->id.  One
+// thread per bitmap word, so no atomics on und.
+__global__ void __launch_bounds__(R_THREADS)
+k_fwbw_finalize(uint32_t n, uint32_t const* __restrict__ vis_b, uint32_t* __restrict__ und, uint32_t* __restrict__ scc_id, reach_state* st)
+{
+  uint32_t const words = (n + 31) / 32;
+  uint32_t const id    = st->id;
+  uint32_t       c     = 0;
+  for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) {
+    uint32_t s = vis_b[w];
+    if (!s) continue;
+    und[w] &= ~s;
+    c += __popc(s);
+    while (s) {
+      uint32_t const b = __ffs(s) - 1;
+      s &= s - 1;
+      scc_id[w * 32 + b] = id;
+    }
+  }
+#pragma unroll
+  for (int sh = 16; sh; sh >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, sh);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(&st->decided, c);
+}
+
+// ---------------------------------------------------------------- graph building
+// Adds kernel `fn` with arguments `vals` (converted to the kernel's
+// parameter types) to graph g after `dep`.
+template<typename... KArgs, typename... Vals>
+cudaGraphNode_t
+add_kernel(cudaGraph_t g, cudaGraphNode_t dep, void (*fn)(KArgs...), unsigned grid, unsigned block, Vals... vals)
+{
+  static_assert(sizeof...(KArgs) == sizeof...(Vals), "argument count");
+  std::tuple<std::decay_t<KArgs>...> held(static_cast<std::decay_t<KArgs>>(vals)...);
+  void*                              params[sizeof...(KArgs) ? sizeof...(KArgs) : 1];
+  std::apply(
+    [&](auto&... a) {
+      int i = 0;
+      ((params[i++] = static_cast<void*>(&a)), ...);
+    },
+    held);
+  cudaKernelNodeParams p = {};
+  p.func                 = reinterpret_cast<void*>(fn);
+  p.gridDim              = dim3(grid);
+  p.blockDim             = dim3(block);
+  p.sharedMemBytes       = 0;
+  p.kernelParams         = params;
+  cudaGraphNode_t node   = nullptr;
+  KSPN_CUDA(cudaGraphAddKernelNode(&node, g, dep ? &dep : nullptr, dep ? 1 : 0, &p));
+  return node;
+}
+
+struct search_io
+{
+  uint64_t const* td_head;
+  uint32_t const* td_adj;
+  uint64_t const* bu_head;
+  uint32_t const* bu_adj;
+  uint32_t*       avail;
+  uint32_t*       mark;
 };
 
-// Runs one search from the queue seeded in q0 (length in ctr[CTR_Q0]).
+// The kernels of one level, in order: into graph g (a while-body) when g is
+// given, else launched on the stream with the expansion kernels bracketed
+// by the profiling events.
 template<bool BW>
-search_result
-run_search(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t pivot, uint32_t n_cand, kspn_options const& opt)
+void
+level_body(kspn_context* ctx, cudaGraph_t g, dgraph const& gr, search_io const& io, reach_state* st, cudaGraphConditionalHandle h)
 {
-  auto&          ws  = ctx->ws;
-  search_result  res;
-  uint32_t*      q[2]  = { ws.q0, ws.q1 };
-  uint32_t*      qc[2] = { ws.ctr + CTR_Q0, ws.ctr + CTR_Q1 };
-  auto*          edges = reinterpret_cast<unsigned long long*>(ws.ctr64);
-  uint32_t const enter = opt.bu_enter_div ? opt.bu_enter_div : 1;
-  uint32_t const leave = opt.bu_leave_div ? opt.bu_leave_div : 1;
-  uint32_t const cap   = opt.max_levels ? opt.max_levels : g.n + 2;
-  bool           bu    = false;
-  int            cur   = 0;
-  // top-down: FW expands out-rows, BW expands in-rows; bottom-up the opposite
-  uint64_t const* td_head = BW ? g.bh : g.fh;
-  uint32_t const* td_adj  = BW ? g.bc : g.fc;
-  uint64_t const* bu_head = BW ? g.fh : g.bh;
-  uint32_t const* bu_adj  = BW ? g.fc : g.bc;
-  uint32_t qn_cur = 1;
-  uint64_t e0 = ctx->h_ctr64[0], c0 = ctx->h_ctr64[1];
-  for (;;) {
-    if (res.levels >= cap) throw error{ KSPN_ERR_TIMEOUT, "reachability: level cap exceeded" };
-    int const nxt = cur ^ 1;
-    KSPN_CUDA(cudaMemsetAsync(qc[nxt], 0, sizeof(uint32_t), ctx->stream));
-    if (!bu) {
-      if (BW) {
-        bw_td_op op{ ws.vis_a, ws.vis_b, und, scc_id, pivot, q[nxt], qc[nxt], ws.ctr + CTR_DECIDED };
-        expand_level(ctx, td_head, td_adj, q[cur], qc[cur], ws.ctr + CTR_NTILES, edges, ws.tile_start, op);
-      } else {
-        fw_td_op op{ und, ws.vis_a, q[nxt], qc[nxt] };
-        expand_level(ctx, td_head, td_adj, q[cur], qc[cur], ws.ctr + CTR_NTILES, edges, ws.tile_start, op);
-      }
-    } else {
-      prof_start(ctx);
-      k_bottom_up<BW><<<r_grid(g.n), R_THREADS, 0, ctx->stream>>>(g.n, bu_head, bu_adj, und, ws.vis_a, BW ? ws.vis_b : ws.vis_a, scc_id, pivot, q[nxt], qc[nxt], ws.ctr + CTR_DECIDED, edges);
-      prof_stop(ctx);
-      KSPN_CHECK_LAUNCH();
-      ctx->launches += 1;
-      res.bottom_up += 1;
-    }
-    res.levels += 1;
-    read_counters(ctx);
-    uint32_t const qn = ctx->h_ctr[CTR_Q0 + nxt];
-    {
-      uint64_t const de = ctx->h_ctr64[0] - e0, dc = ctx->h_ctr64[1] - c0;
-      e0 = ctx->h_ctr64[0];
-      c0 = ctx->h_ctr64[1];
-      if (!bu) prof_add(ctx, KSPN_KERNEL_EXPAND, expand_bytes(qn_cur, de, qn, BW ? 4 : 0));
-      // bottom-up: candidate sweep reads the bitmaps (n/8 B each), then per
-      // candidate its offset pair, per edge id + probe, per join 4 B (+4 B BW id)
-      else prof_add(ctx, KSPN_KERNEL_BOTTOM_UP, (BW ? 1 : 2) * (static_cast<uint64_t>(g.n) / 8) + 16 * dc + 8 * de + (BW ? 8 : 4) * static_cast<uint64_t>(qn));
-    }
-    qn_cur = qn;
-    if (qn == 0) break;
-    if (!bu && static_cast<uint64_t>(qn) * enter > n_cand) bu = true;
-    else if (bu && static_cast<uint64_t>(qn) * leave < n_cand) bu = false;
-    cur = nxt;
+  auto&     ws = ctx->ws;
+  fio const f{ ws.q0, ws.q1, &st->qn[0], &st->qn[1], &st->cur };
+  if (g) {
+    cudaGraphNode_t dep = nullptr;
+    dep                 = add_kernel(g, dep, &k_fs_reduce, FS_BLOCKS, FS_THREADS, io.td_head, f, ws.blocks);
+    dep                 = add_kernel(g, dep, &k_fs_partials, 1, 1024, ws.blocks, ws.prefix, f, &st->ntiles, static_cast<unsigned long long*>(nullptr), &st->m_f);
+    dep                 = add_kernel(g, dep, &k_fs_down, FS_BLOCKS, FS_THREADS, io.td_head, f, ws.blocks, ws.prefix, ws.tile_start);
+    dep                 = add_kernel(g, dep, &k_r_decide, 1, 1, st);
+    dep = add_kernel(g, dep, &k_expand<take_op>, EX_BLOCKS, EX_THREADS, io.td_head, io.td_adj, f, ws.prefix, ws.tile_start, &st->ntiles, gate{ &st->mode, 0 }, take_op{ io.avail, io.mark });
+    dep = add_kernel(g, dep, &k_bottom_up, r_grid(gr.n), R_THREADS, gr.n, io.bu_head, io.bu_adj, io.avail, io.mark, f, gate{ &st->mode, 1 }, st);
+    add_kernel(g, dep, &k_r_advance<BW>, 1, 1, st, h, 1);
+    return;
   }
-  return res;
+  cudaStream_t const s = ctx->stream;
+  k_fs_reduce<<<FS_BLOCKS, FS_THREADS, 0, s>>>(io.td_head, f, ws.blocks);
+  k_fs_partials<<<1, 1024, 0, s>>>(ws.blocks, ws.prefix, f, &st->ntiles, nullptr, &st->m_f);
+  k_fs_down<<<FS_BLOCKS, FS_THREADS, 0, s>>>(io.td_head, f, ws.blocks, ws.prefix, ws.tile_start);
+  k_r_decide<<<1, 1, 0, s>>>(st);
+  prof_start(ctx, 0);
+  k_expand<take_op><<<EX_BLOCKS, EX_THREADS, 0, s>>>(io.td_head, io.td_adj, f, ws.prefix, ws.tile_start, &st->ntiles, gate{ &st->mode, 0 }, take_op{ io.avail, io.mark });
+  prof_stop(ctx, 0);
+  prof_start(ctx, 1);
+  k_bottom_up<<<r_grid(gr.n), R_THREADS, 0, s>>>(gr.n, io.bu_head, io.bu_adj, io.avail, io.mark, f, gate{ &st->mode, 1 }, st);
+  prof_stop(ctx, 1);
+  k_r_advance<BW><<<1, 1, 0, s>>>(st, h, 0);
+  KSPN_CHECK_LAUNCH();
+  ctx->launches += 7;
+}
+
+search_io
+fw_io(kspn_context* ctx, dgraph const& g)
+{
+  return { g.fh, g.fc, g.bh, g.bc, ctx->ws.mark, ctx->ws.vis_a };
+}
+search_io
+bw_io(kspn_context* ctx, dgraph const& g)
+{
+  return { g.bh, g.bc, g.fh, g.fc, ctx->ws.vis_a, ctx->ws.vis_b };
+}
+
+// Builds the one-launch FW-BW graph for (graph, und, scc_id).
+void
+build_fwbw_graph(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id)
+{
+  auto&          ws    = ctx->ws;
+  auto*          st    = reinterpret_cast<reach_state*>(ws.rstate);
+  uint32_t const words = (g.n + 31) / 32;
+  cudaGraph_t    graph = nullptr;
+  KSPN_CUDA(cudaGraphCreate(&graph, 0));
+  try {
+    cudaGraphNode_t dep = nullptr;
+    dep = add_kernel(graph, dep, &k_r_init, r_grid(words), R_THREADS, words, und, ws.mark, ws.vis_a, ws.vis_b, st);
+    dep = add_kernel(graph, dep, &k_und_degrees, r_grid(g.n), R_THREADS, g.n, und, g.fh, g.bh, st);
+    for (int bw = 0; bw < 2; ++bw) {
+      search_io const io = bw ? bw_io(ctx, g) : fw_io(ctx, g);
+      dep = bw ? add_kernel(graph, dep, &k_r_seed<true>, 1, 1, io.avail, io.mark, ws.q0, st) : add_kernel(graph, dep, &k_r_seed<false>, 1, 1, io.avail, io.mark, ws.q0, st);
+      cudaGraphConditionalHandle h;
+      KSPN_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault));
+      cudaGraphNodeParams cp = {};
+      cp.type                = cudaGraphNodeTypeConditional;
+      cp.conditional.handle  = h;
+      cp.conditional.type    = cudaGraphCondTypeWhile;
+      cp.conditional.size    = 1;
+      cudaGraphNode_t loop   = nullptr;
+      KSPN_CUDA(cudaGraphAddNode(&loop, graph, &dep, 1, &cp));
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      if (bw) level_body<true>(ctx, body, g, io, st, h);
+      else level_body<false>(ctx, body, g, io, st, h);
+      dep = loop;
+    }
+    dep = add_kernel(graph, dep, &k_r_setid, 1, 1, st);
+    dep = add_kernel(graph, dep, &k_bitmap_min, r_grid(words), R_THREADS, g.n, ws.vis_b, st);
+    add_kernel(graph, dep, &k_fwbw_finalize, r_grid(words), R_THREADS, g.n, ws.vis_b, und, scc_id, st);
+    cudaGraphExec_t exec = nullptr;
+    KSPN_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    ctx->fwbw.graph = graph;
+    ctx->fwbw.exec  = exec;
+  } catch (...) {
+    cudaGraphDestroy(graph);
+    throw;
+  }
 }
 
 } // namespace
 
-uint32_t
-fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t pivot, kspn_options const& opt, kspn_stats* st)
+size_t
+reach_state_bytes()
 {
-  auto&        ws    = ctx->ws;
-  size_t const words = (static_cast<size_t>(g.n) + 31) / 32;
-  if (pivot >= g.n) throw error{ KSPN_ERR_INVALID_ARGUMENT, "forward_backward_search: pivot >= n" };
-  uint32_t const n_und = count_undecided(ctx, g.n, und);
-  KSPN_CUDA(cudaMemsetAsync(ws.vis_a, 0, words * 4, ctx->stream));
-  KSPN_CUDA(cudaMemsetAsync(ws.vis_b, 0, words * 4, ctx->stream));
-  zero_counters(ctx);
-  k_reach_seed<<<1, 1, 0, ctx->stream>>>(ws.vis_a, ws.q0, ws.ctr + CTR_Q0, pivot);
-  KSPN_CHECK_LAUNCH();
-  ctx->launches += 1;
-  search_result const fw = run_search<false>(ctx, g, und, scc_id, pivot, n_und, opt);
+  return sizeof(reach_state);
+}
 
-  KSPN_CUDA(cudaMemsetAsync(ws.ctr + CTR_DECIDED, 0, sizeof(uint32_t), ctx->stream));
-  k_bw_seed<<<1, 1, 0, ctx->stream>>>(ws.vis_a, ws.vis_b, und, scc_id, ws.q0, ws.ctr + CTR_Q0, pivot);
-  KSPN_CHECK_LAUNCH();
-  ctx->launches += 1;
-  read_counters(ctx); // CTR_DECIDED was reset after the FW counters were read
-  search_result const bw = run_search<true>(ctx, g, und, scc_id, pivot, n_und, opt);
-  read_counters(ctx);
-  uint32_t const decided = ctx->h_ctr[CTR_DECIDED] + 1; // + the pivot
-  if (st) {
-    if (st->levels_fw == 0 && st->levels_bw == 0) {
-      st->levels_fw        = fw.levels;
-      st->levels_bw        = bw.levels;
-      st->levels_bottom_up = fw.bottom_up + bw.bottom_up;
+void
+release_graphs(kspn_context* ctx)
+{
+  if (ctx->fwbw.exec) cudaGraphExecDestroy(ctx->fwbw.exec);
+  if (ctx->fwbw.graph) cudaGraphDestroy(ctx->fwbw.graph);
+  ctx->fwbw = {};
+}
+
+uint32_t
+fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t pivot, kspn_options const& opt, kspn_stats* st, bool min_ids)
+{
+  auto& ws = ctx->ws;
+  if (pivot >= g.n) throw error{ KSPN_ERR_INVALID_ARGUMENT, "forward_backward_search: pivot >= n" };
+  auto* rs = reinterpret_cast<reach_state*>(ws.rstate);
+  auto* hs = reinterpret_cast<reach_state*>(ctx->h_state);
+  // parameters of this search
+  std::memset(hs, 0, sizeof(reach_state));
+  hs->pivot   = pivot;
+  hs->cap     = opt.max_levels ? opt.max_levels : g.n + 2;
+  hs->alpha   = opt.bu_enter_div ? opt.bu_enter_div : 1;
+  hs->beta    = opt.bu_leave_div ? opt.bu_leave_div : 1;
+  hs->min_ids = min_ids ? 1u : 0u;
+  KSPN_CUDA(cudaMemcpyAsync(rs, hs, sizeof(reach_state), cudaMemcpyHostToDevice, ctx->stream));
+
+  if (!ctx->prof) {
+    graph_key const key{ g.fh, g.fc, g.bh, g.bc, und, scc_id, ws.base, g.n, g.m };
+    if (!ctx->fwbw.exec || !(ctx->fwbw.key == key)) {
+      release_graphs(ctx);
+      build_fwbw_graph(ctx, g, und, scc_id);
+      ctx->fwbw.key = key;
     }
-    st->edges_scanned = ctx->h_ctr64[0];
+    KSPN_CUDA(cudaGraphLaunch(ctx->fwbw.exec, ctx->stream));
+  } else {
+    // host-driven loop over the same kernels, expansion kernels bracketed
+    // by CUDA events (kspn_options.profile)
+    uint32_t const words = (g.n + 31) / 32;
+    k_r_init<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(words, und, ws.mark, ws.vis_a, ws.vis_b, rs);
+    k_und_degrees<<<r_grid(g.n), R_THREADS, 0, ctx->stream>>>(g.n, und, g.fh, g.bh, rs);
+    ctx->launches += 2;
+    for (int bw = 0; bw < 2; ++bw) {
+      search_io const io = bw ? bw_io(ctx, g) : fw_io(ctx, g);
+      if (bw) k_r_seed<true><<<1, 1, 0, ctx->stream>>>(io.avail, io.mark, ws.q0, rs);
+      else k_r_seed<false><<<1, 1, 0, ctx->stream>>>(io.avail, io.mark, ws.q0, rs);
+      ctx->launches += 1;
+      for (;;) {
+        KSPN_CUDA(cudaMemcpyAsync(hs, rs, sizeof(reach_state), cudaMemcpyDeviceToHost, ctx->stream));
+        KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+        uint32_t const           qn0 = hs->qn[hs->cur & 1u];
+        unsigned long long const e0 = hs->edges_bu, c0 = hs->cands_bu;
+        if (qn0 == 0 || hs->err) break;
+        if (hs->level >= hs->cap) {
+          hs->err = 1;
+          break;
+        }
+        if (bw) level_body<true>(ctx, nullptr, g, io, rs, cudaGraphConditionalHandle{});
+        else level_body<false>(ctx, nullptr, g, io, rs, cudaGraphConditionalHandle{});
+        KSPN_CUDA(cudaMemcpyAsync(hs, rs, sizeof(reach_state), cudaMemcpyDeviceToHost, ctx->stream));
+        KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+        uint32_t const qn1 = hs->qn[hs->cur & 1u];
+        if (hs->mode == 0) prof_add(ctx, 0, KSPN_KERNEL_EXPAND, expand_bytes(qn0, hs->m_f, qn1, 4));
+        // bottom-up: candidate sweep reads the avail bitmap (n/8 B), then per
+        // candidate its offset pair, per edge id + probe, per join queue
+        // entry + two bit writes
+        else prof_add(ctx, 1, KSPN_KERNEL_BOTTOM_UP, static_cast<uint64_t>(g.n) / 8 + 16 * (hs->cands_bu - c0) + 8 * (hs->edges_bu - e0) + 8ull * qn1);
+      }
+      if (hs->err) break;
+    }
+    if (hs->err) throw error{ KSPN_ERR_TIMEOUT, "reachability: level cap exceeded" };
+    k_r_setid<<<1, 1, 0, ctx->stream>>>(rs);
+    k_bitmap_min<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(g.n, ws.vis_b, rs);
+    k_fwbw_finalize<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(g.n, ws.vis_b, und, scc_id, rs);
+    KSPN_CHECK_LAUNCH();
+    ctx->launches += 3;
   }
-  return decided;
+  KSPN_CUDA(cudaMemcpyAsync(hs, rs, sizeof(reach_state), cudaMemcpyDeviceToHost, ctx->stream));
+  KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (hs->err) throw error{ KSPN_ERR_TIMEOUT, "reachability: level cap exceeded" };
+  // kernels the graph ran: init, degrees, 2 seeds, 7 per level, 3 to finish
+  if (!ctx->prof) ctx->launches += 7 + 7ull * (hs->levels_fw + hs->levels_bw);
+  ctx->td_edges += hs->edges_td + hs->edges_bu;
+  if (st && st->levels_fw == 0 && st->levels_bw == 0) {
+    st->levels_fw        = hs->levels_fw;
+    st->levels_bw        = hs->levels_bw;
+    st->levels_bottom_up = hs->bu_fw + hs->bu_bw;
+  }
+  return hs->decided;
 }
 
 } // namespace kspn

@@ -96,10 +96,16 @@ k_trim_first(uint32_t n,
              uint64_t* __restrict__ blk_prod,
              uint32_t* __restrict__ blk_id)
 {
-  pv       best = { 0, NONE };
-  uint32_t dec  = 0;
-  uint64_t const nwords_threads = (static_cast<uint64_t>(n) + 31) & ~31ull;
-  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < nwords_threads; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+  __shared__ uint32_t s_buf[DENSE_BUF];
+  __shared__ uint32_t s_n, s_base;
+  if (threadIdx.x == 0) s_n = 0;
+  __syncthreads();
+  block_queue    bq{ s_buf, &s_n };
+  pv             best = { 0, NONE };
+  uint32_t       dec  = 0;
+  uint64_t const span = (static_cast<uint64_t>(n) + T_THREADS - 1) / T_THREADS * T_THREADS;
+  for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * T_THREADS; base < span; base += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+    uint64_t const t     = base + threadIdx.x;
     uint32_t const v     = static_cast<uint32_t>(t);
     bool const     valid = t < n;
     uint64_t       out = 0, in = 0;
@@ -110,7 +116,7 @@ k_trim_first(uint32_t n,
     bool const     trimmed = valid && (in == 0 || out == 0);
     bool const     live    = valid && !trimmed;
     unsigned const word    = __ballot_sync(0xFFFFFFFFu, live);
-    if ((threadIdx.x & 31) == 0) und[v >> 5] = word;
+    if ((threadIdx.x & 31) == 0 && t < n) und[v >> 5] = word; // t = the warp's first vertex
     if (valid) scc_id[v] = trimmed ? v : UNDECIDED;
     if (live) {
       if (indeg) indeg[v] = static_cast<uint32_t>(in);
@@ -118,9 +124,14 @@ k_trim_first(uint32_t n,
       uint64_t const prod = in * out;
       if (prod > best.prod) best = { prod, v }; // ascending v: first strict max wins
     }
-    if (queue) warp_push(trimmed, v, queue, ctr + CTR_Q0);
+    if (queue) {
+      bq.push(trimmed, v);
+      __syncthreads();
+      if (s_n > DENSE_BUF - T_THREADS) bq.flush(queue, ctr + CTR_Q0, &s_base);
+    }
     dec += trimmed;
   }
+  if (queue) bq.flush(queue, ctr + CTR_Q0, &s_base);
   // decided count
   unsigned d = dec;
 #pragma unroll
@@ -207,14 +218,23 @@ k_live_degrees(uint32_t n,
 __global__ void __launch_bounds__(T_THREADS)
 k_seed_dead(uint32_t n, uint32_t* __restrict__ und, uint32_t* __restrict__ scc_id, uint32_t const* __restrict__ indeg, uint32_t const* __restrict__ outdeg, uint32_t* __restrict__ queue, uint32_t* __restrict__ ctr)
 {
-  uint64_t const span = (static_cast<uint64_t>(n) + 31) & ~31ull;
-  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+  __shared__ uint32_t s_buf[DENSE_BUF];
+  __shared__ uint32_t s_n, s_base;
+  if (threadIdx.x == 0) s_n = 0;
+  __syncthreads();
+  block_queue    bq{ s_buf, &s_n };
+  uint64_t const span = (static_cast<uint64_t>(n) + T_THREADS - 1) / T_THREADS * T_THREADS;
+  for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * T_THREADS; base < span; base += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+    uint64_t const t    = base + threadIdx.x;
     uint32_t const v    = static_cast<uint32_t>(t);
     bool const     dead = t < n && bit_get(und, v) && (indeg[v] == 0 || outdeg[v] == 0);
     bool const     won  = dead && bit_take(und, v);
     if (won) scc_id[v] = v;
-    warp_push(won, v, queue, ctr + CTR_Q0);
+    bq.push(won, v);
+    __syncthreads();
+    if (s_n > DENSE_BUF - T_THREADS) bq.flush(queue, ctr + CTR_Q0, &s_base);
   }
+  bq.flush(queue, ctr + CTR_Q0, &s_base);
 }
 
 // ---------------------------------------------------------------- push-based trim level
@@ -285,9 +305,15 @@ k_trim_push(uint64_t const* __restrict__ fh,
 __global__ void __launch_bounds__(T_THREADS)
 k_seed_raw(uint32_t n, uint64_t const* __restrict__ head, uint32_t* __restrict__ und, uint32_t* __restrict__ scc_id, uint32_t* __restrict__ deg, uint32_t* __restrict__ queue, uint32_t* __restrict__ ctr)
 {
-  uint64_t const span = (static_cast<uint64_t>(n) + 31) & ~31ull;
+  __shared__ uint32_t s_buf[DENSE_BUF];
+  __shared__ uint32_t s_n, s_base;
+  if (threadIdx.x == 0) s_n = 0;
+  __syncthreads();
+  block_queue    bq{ s_buf, &s_n };
+  uint64_t const span = (static_cast<uint64_t>(n) + T_THREADS - 1) / T_THREADS * T_THREADS;
   uint32_t       dec  = 0;
-  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+  for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * T_THREADS; base < span; base += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+    uint64_t const t    = base + threadIdx.x;
     uint32_t const v    = static_cast<uint32_t>(t);
     bool const     have = t < n && bit_get(und, v);
     bool           won  = false;
@@ -300,8 +326,11 @@ k_seed_raw(uint32_t n, uint64_t const* __restrict__ head, uint32_t* __restrict__
         ++dec;
       }
     }
-    warp_push(won, v, queue, ctr + CTR_Q0);
+    bq.push(won, v);
+    __syncthreads();
+    if (s_n > DENSE_BUF - T_THREADS) bq.flush(queue, ctr + CTR_Q0, &s_base);
   }
+  bq.flush(queue, ctr + CTR_Q0, &s_base);
   if (dec) atomicAdd(ctr + CTR_DECIDED, dec);
 }
 
@@ -434,7 +463,7 @@ run_push_levels(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc
     // per queued vertex and direction: queue entry + offset pair; per edge:
     // id + degree atomic; per decided vertex: id write + queue write
     int const ndir = (DIRS & 1) + ((DIRS >> 1) & 1);
-    prof_add(ctx, KSPN_KERNEL_TRIM, 20ull * ndir * qn + 8 * (ctx->h_ctr64[2] - e0) + 8ull * ctx->h_ctr[CTR_DECIDED]);
+    prof_add(ctx, 0, KSPN_KERNEL_TRIM, 20ull * ndir * qn + 8 * (ctx->h_ctr64[2] - e0) + 8ull * ctx->h_ctr[CTR_DECIDED]);
     qn = ctx->h_ctr[CTR_Q1];
     total += ctx->h_ctr[CTR_DECIDED];
     uint32_t* t = qa;
@@ -466,7 +495,7 @@ trim_1_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id
     // live degrees written, trimmed vertices queued
     uint64_t const dec  = ctx->h_ctr[CTR_DECIDED];
     uint64_t const live = g.n - dec;
-    prof_add(ctx, KSPN_KERNEL_STREAM, 16ull * (g.n + 1) + 4ull * g.n + g.n / 8 + (init_degrees ? 8 * live : 0) + (queue_out ? 4 * dec : 0));
+    prof_add(ctx, 0, KSPN_KERNEL_STREAM, 16ull * (g.n + 1) + 4ull * g.n + g.n / 8 + (init_degrees ? 8 * live : 0) + (queue_out ? 4 * dec : 0));
   }
   if (queue_count_host) *queue_count_host = ctx->h_ctr[CTR_Q0];
   ctx->h_ctr[CTR_AUX] = ctx->h_ctr[CTR_DECIDED];
