@@ -204,9 +204,10 @@ def run_kspn(args):
     # event brackets on (levels driven from the host so every expansion
     # kernel launch is bracketed on the library's stream)
     agg = {k: [0.0, 0, 0] for k in K.KERNEL_CLASSES}
-    prof_steps = max(1, min(args.steps, 3))
+    prof_steps = args.profile_steps if args.profile_steps is not None else max(1, min(args.steps, 3))
     for _ in range(prof_steps):
         ctx.scc_device(G.n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, prof_opt, st)
+        trace = st.as_dict()["trace"]
         for k, v in st.as_dict()["kernels"].items():
             agg[k][0] += v["ms"]
             agg[k][1] += v["bytes"]
@@ -283,7 +284,7 @@ def run_kspn(args):
             "clocks": clk.summary(),
             "phases": {"decided": last["decided"], "ms": {k: round(v, 4) for k, v in last["ms"].items()}, "levels_fw": last["levels_fw"],
                        "levels_bw": last["levels_bw"], "bottom_up": last["levels_bottom_up"], "label_calls": last["label_calls"],
-                       "edges_scanned": last["edges_scanned"], "kernels": {k: {"ms": round(a[0] / prof_steps, 4), "GB/s": round(a[1] / (a[0] * 1e-3) / 1e9, 1) if a[0] else 0}
+                       "edges_scanned": last["edges_scanned"], "trace": trace, "kernels": {k: {"ms": round(a[0] / prof_steps, 4), "GB/s": round(a[1] / (a[0] * 1e-3) / 1e9, 1) if a[0] else 0}
                                                                             for k, a in agg.items()}},
         }
         if not args.no_cpu_baseline:
@@ -307,6 +308,7 @@ def main():
     ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS))
     ap.add_argument("--pipeline", default="fast", choices=["fast", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=None, help="steps run with per-kernel event timing (default min(steps, 3))")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "kspn":
         args.warmup = 3

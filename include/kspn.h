@@ -45,7 +45,7 @@ extern "C" {
 #define KSPN_UNDECIDED 0xFFFFFFFFu /* reference: scc_id_undecided, kaspan/graph/base.hpp:135 */
 
 /* ---------------------------------------------------------------- options */
-#define KSPN_PIPELINE_FAST 0      /* trim fixpoint, pivot FW-BW, label rounds, residual finish */
+#define KSPN_PIPELINE_FAST 0      /* trim_1_first, pivot FW-BW, then rounds of trim fixpoint / trim-2 / label search */
 #define KSPN_PIPELINE_REFERENCE 1 /* the phase order of kaspan::scc (kaspan/scc/scc.hpp:21-87) */
 
 typedef struct kspn_options
@@ -99,12 +99,30 @@ typedef struct kspn_stats
   double   kernel_ms[KSPN_KERNEL_CLASSES];       /* event-timed device ms per class */
   uint64_t kernel_bytes[KSPN_KERNEL_CLASSES];    /* algorithmic bytes per class */
   uint64_t kernel_calls[KSPN_KERNEL_CLASSES];    /* timed launches per class */
+  /* Per-level trace of the first FW-BW, filled when kspn_options.profile is set. */
+  uint32_t trace_levels;
+  struct kspn_level_trace
+  {
+    uint32_t backward;       /* 0 FW, 1 BW */
+    uint32_t bottom_up;      /* direction the level ran in */
+    uint32_t frontier;       /* vertices expanded (top-down) / joined before it */
+    uint32_t discovered;     /* vertices the level added */
+    uint64_t frontier_edges; /* edges of the frontier (top-down direction) */
+    uint64_t scanned;        /* adjacency entries read (bottom-up) */
+    uint64_t candidates;     /* vertices swept (bottom-up) */
+    float    ms;             /* event time of the level's expansion kernel */
+    uint32_t pad;
+  } trace[32];
 } kspn_stats;
 
 typedef struct kspn_context kspn_context;
 
 /* ---------------------------------------------------------------- lifetime */
 int         kspn_options_default(kspn_options* opt);
+/* sizeof(kspn_options) / sizeof(kspn_stats) as compiled into the library,
+ * for FFI bindings to check their struct layouts. */
+size_t      kspn_options_size(void);
+size_t      kspn_stats_size(void);
 const char* kspn_strerror(int status);
 const char* kspn_last_error(const kspn_context* ctx); /* detail of the last failure on ctx */
 int         kspn_context_create(int device, kspn_context** out);

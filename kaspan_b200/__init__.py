@@ -58,6 +58,20 @@ class Options(C.Structure):
     ]
 
 
+class LevelTrace(C.Structure):
+    _fields_ = [
+        ("backward", C.c_uint32),
+        ("bottom_up", C.c_uint32),
+        ("frontier", C.c_uint32),
+        ("discovered", C.c_uint32),
+        ("frontier_edges", C.c_uint64),
+        ("scanned", C.c_uint64),
+        ("candidates", C.c_uint64),
+        ("ms", C.c_float),
+        ("pad", C.c_uint32),
+    ]
+
+
 class Stats(C.Structure):
     _fields_ = [
         ("n", C.c_uint32),
@@ -76,6 +90,8 @@ class Stats(C.Structure):
         ("kernel_ms", C.c_double * 4),
         ("kernel_bytes", C.c_uint64 * 4),
         ("kernel_calls", C.c_uint64 * 4),
+        ("trace_levels", C.c_uint32),
+        ("trace", LevelTrace * 32),
     ]
 
     def as_dict(self) -> dict:
@@ -95,6 +111,10 @@ class Stats(C.Structure):
             "kernel_launches": int(self.kernel_launches),
             "kernels": {k: {"ms": float(self.kernel_ms[i]), "bytes": int(self.kernel_bytes[i]), "calls": int(self.kernel_calls[i])}
                         for i, k in enumerate(KERNEL_CLASSES)},
+            "trace": [{"dir": "bw" if t.backward else "fw", "mode": "bu" if t.bottom_up else "td", "frontier": t.frontier,
+                       "discovered": t.discovered, "frontier_edges": int(t.frontier_edges), "scanned": int(t.scanned),
+                       "candidates": int(t.candidates), "ms": round(float(t.ms), 4)}
+                      for t in self.trace[: min(self.trace_levels, 32)]],
         }
 
 
@@ -109,6 +129,8 @@ _P = C.c_void_p
 _u32, _u64, _i32 = C.c_uint32, C.c_uint64, C.c_int
 SIGNATURES = {
     "kspn_options_default": (_i32, [_P]),
+    "kspn_options_size": (C.c_size_t, []),
+    "kspn_stats_size": (C.c_size_t, []),
     "kspn_strerror": (C.c_char_p, [_i32]),
     "kspn_last_error": (C.c_char_p, [_P]),
     "kspn_context_create": (_i32, [_i32, _P]),

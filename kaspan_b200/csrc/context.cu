@@ -8,10 +8,9 @@
 //             trim_1_first -> FW-BW(pivot) -> trim_1_normal -> label
 //             searches with rotation 1, 2, 3, ... until every vertex is
 //             decided.
-//  FAST       trim_1_first -> trim-1 fixpoint -> FW-BW from the live
-//             degree-product pivot -> rounds of {trim-1 fixpoint, trim-2,
-//             label search} until every vertex is decided.  Same partition
-//             (every phase only decides whole SCCs).
+//  FAST       trim_1_first -> FW-BW from its pivot -> rounds of {trim-1
+//             fixpoint, trim-2, label search} until every vertex is decided.
+//             Same partition (every phase only decides whole SCCs).
 #include "kspn_internal.cuh"
 
 #include "prim.cuh"
@@ -247,14 +246,14 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
       add(KSPN_PHASE_LABEL, label_search(ctx, g, und, scc_id, ++rotation, opt, st));
     }
   } else {
-    uint32_t seeds = 0;
-    trim_1_first(ctx, g, und, scc_id, ws.q0, &seeds, true);
+    // trim_1_first's pivot (argmax in*out) lies in the giant component of
+    // the graphs this targets; FW-BW runs before any further trimming, and
+    // the trim fixpoint then only walks the (small) remainder
+    uint32_t const pivot = trim_1_first(ctx, g, und, scc_id, nullptr, nullptr, false);
     add(KSPN_PHASE_TRIM_FIRST, ctx->h_ctr[CTR_AUX]);
-    if (decided < g.n) add(KSPN_PHASE_TRIM, trim_fixpoint(ctx, g, und, scc_id, true, seeds));
     if (decided < g.n) {
-      uint32_t const pivot = select_pivot_live(ctx, g, und);
       if (st) st->pivot = pivot;
-      if (pivot < g.n) add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pivot, opt, st, true));
+      add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pivot, opt, st, true));
     }
     int      rotation = 0;
     uint32_t rounds   = 0;
@@ -364,6 +363,18 @@ kspn_options_default(kspn_options* opt)
   opt->bu_enter_div = 24;
   opt->bu_leave_div = 96;
   return KSPN_OK;
+}
+
+size_t
+kspn_options_size(void)
+{
+  return sizeof(kspn_options);
+}
+
+size_t
+kspn_stats_size(void)
+{
+  return sizeof(kspn_stats);
 }
 
 const char*

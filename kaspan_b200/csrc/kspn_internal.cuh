@@ -289,18 +289,19 @@ prof_stop(kspn_context* ctx, int pair = 0)
 {
   if (ctx->prof) cudaEventRecord(ctx->pe[2 * pair + 1], ctx->stream);
 }
-inline void
+inline float
 prof_add(kspn_context* ctx, int pair, int cls, uint64_t bytes, uint64_t calls = 1)
 {
-  if (!ctx->prof) return;
+  if (!ctx->prof) return 0.f;
   float ms = 0;
   if (cudaEventElapsedTime(&ms, ctx->pe[2 * pair], ctx->pe[2 * pair + 1]) != cudaSuccess) {
     cudaGetLastError();
-    return;
+    return 0.f;
   }
   ctx->prof->kernel_ms[cls] += ms;
   ctx->prof->kernel_bytes[cls] += bytes;
   ctx->prof->kernel_calls[cls] += calls;
+  return ms;
 }
 
 // workspace / context helpers (context.cu)

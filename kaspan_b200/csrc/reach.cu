@@ -52,6 +52,15 @@ r_grid(uint64_t items)
   return static_cast<unsigned>(b < 148ull * 8 ? (b ? b : 1) : 148ull * 8);
 }
 
+// bottom-up: one block per chunk of R_THREADS bitmap words, capped at the
+// resident-block count
+unsigned
+bu_grid(uint32_t n)
+{
+  uint64_t const chunks = ((static_cast<uint64_t>(n) + 31) / 32 + R_THREADS - 1) / R_THREADS;
+  return static_cast<unsigned>(chunks < 148ull * 4 ? (chunks ? chunks : 1) : 148ull * 4);
+}
+
 // Device-side control block of one FW-BW (lives in the workspace).
 struct reach_state
 {
@@ -144,7 +153,7 @@ k_r_decide(reach_state* st)
   unsigned long long const mf = st->m_f;
   uint32_t const           qn = st->qn[st->cur & 1u];
   if (st->mode == 0 && mf * st->alpha > st->m_u) st->mode = 1;
-  else if (st->mode == 1 && static_cast<unsigned long long>(qn) * st->beta < st->n_und && mf * st->alpha <= st->m_u) st->mode = 0;
+  else if (st->mode == 1 && static_cast<unsigned long long>(qn) * st->beta < st->n_und) st->mode = 0;
   st->qn[(st->cur & 1u) ^ 1u] = 0;
   if (st->mode == 0) st->edges_td += mf;
 }
@@ -185,9 +194,16 @@ struct take_op
 
 // Bottom-up sweep: candidates are the set bits of `avail`; a candidate
 // joins (taken from avail, set in mark, queued) when a neighbour in its
-// `head/adj` row is in `mark`.  Each thread carries BU_ILP candidates at once
-// (interleaved row walks) so their dependent loads overlap; rows of R_BIG+
-// entries are walked by the whole warp.
+// `head/adj` row is in `mark`.
+//  * Compaction: a block reads BU_WORDS bitmap words (one per thread), and a
+//    block scan of their popcounts packs the candidate ids into shared
+//    memory, so a sweep over few candidates costs about one pass over the
+//    bitmap and lanes never idle on non-candidates.
+//  * Each thread then carries BU_ILP candidates at once (interleaved row
+//    walks) so their dependent loads overlap; a row with no visited
+//    neighbour among its first R_BIG entries is finished by the whole warp.
+constexpr int BU_WORDS = R_THREADS;
+
 __global__ void __launch_bounds__(R_THREADS)
 k_bottom_up(uint32_t n,
             uint64_t const* __restrict__ head,
@@ -199,6 +215,7 @@ k_bottom_up(uint32_t n,
             reach_state* st)
 {
   if (g.closed()) return;
+  __shared__ uint32_t s_cand[BU_WORDS * 32];
   __shared__ uint32_t s_buf[BU_BUF];
   __shared__ uint32_t s_n, s_base;
   if (threadIdx.x == 0) s_n = 0;
@@ -207,81 +224,91 @@ k_bottom_up(uint32_t n,
   uint32_t* const qout_n = f.out_n();
   block_queue     bq{ s_buf, &s_n };
   unsigned const  lane  = threadIdx.x & 31u;
-  uint64_t const  step  = static_cast<uint64_t>(R_THREADS) * BU_ILP;
-  uint64_t const  span  = (static_cast<uint64_t>(n) + step - 1) / step * step;
+  uint32_t const  words = (n + 31) / 32;
   uint64_t        nedge = 0, ncand = 0;
-  for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * step; base < span; base += static_cast<uint64_t>(gridDim.x) * step) {
-    uint32_t v[BU_ILP];
-    uint64_t b[BU_ILP], e[BU_ILP];
-    bool     live[BU_ILP], found[BU_ILP];
-#pragma unroll
-    for (int k = 0; k < BU_ILP; ++k) {
-      uint64_t const t = base + static_cast<uint64_t>(k) * R_THREADS + threadIdx.x;
-      v[k]             = static_cast<uint32_t>(t);
-      bool const cand  = t < n && bit_get(avail, v[k]);
-      b[k] = e[k] = 0;
-      if (cand) b[k] = head[v[k]], e[k] = head[v[k] + 1];
-      ncand += cand;
-      found[k] = false;
-      live[k]  = cand && (e[k] - b[k]) < R_BIG; // walked by this thread
-    }
-    // interleaved walks of the short rows
-    for (;;) {
-      bool any = false;
-#pragma unroll
-      for (int k = 0; k < BU_ILP; ++k) {
-        if (live[k] && b[k] < e[k]) {
-          uint32_t const w = adj[b[k]++];
-          ++nedge;
-          if (bit_get(mark, w)) found[k] = true, live[k] = false;
-          any = true;
-        } else {
-          live[k] = false;
-        }
-      }
-      if (!any) break;
-    }
-    // long rows: the whole warp, one row at a time
-#pragma unroll
-    for (int k = 0; k < BU_ILP; ++k) {
-      bool const big  = (e[k] - b[k]) >= R_BIG && !found[k];
-      unsigned   todo = __ballot_sync(0xFFFFFFFFu, big);
-      while (todo) {
-        unsigned const l = __ffs(todo) - 1;
-        todo &= todo - 1;
-        uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b[k], l), e0 = __shfl_sync(0xFFFFFFFFu, e[k], l);
-        bool           hit = false;
-        for (uint64_t x = b0; x < e0; x += 32) {
-          bool const in   = x + lane < e0;
-          bool const mine = in && bit_get(mark, adj[x + lane]);
-          nedge += in;
-          if (__any_sync(0xFFFFFFFFu, mine)) {
-            hit = true;
-            break;
-          }
-        }
-        if (lane == l) found[k] = hit;
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < BU_ILP; ++k) {
-      bool const won = found[k] && bit_take(avail, v[k]);
-      if (won) bit_claim(mark, v[k]);
-      bq.push(won, v[k]);
+  for (uint32_t wbase = blockIdx.x * BU_WORDS; wbase < words; wbase += gridDim.x * BU_WORDS) {
+    // 1. pack this chunk's candidates
+    uint32_t const w    = wbase + threadIdx.x;
+    uint32_t       word = w < words ? avail[w] : 0u;
+    if (w == words - 1 && (n & 31)) word &= (1u << (n & 31)) - 1u;
+    uint32_t       total;
+    uint32_t       j = block_exclusive_scan<uint32_t, R_THREADS>(static_cast<uint32_t>(__popc(word)), &total);
+    while (word) {
+      uint32_t const b = __ffs(word) - 1;
+      word &= word - 1;
+      s_cand[j++] = w * 32 + b;
     }
     __syncthreads();
-    if (s_n > BU_BUF - static_cast<uint32_t>(step)) bq.flush(qout, qout_n, &s_base);
+    ncand += threadIdx.x == 0 ? total : 0;
+    // 2. walk the packed candidates, BU_ILP per thread
+    for (uint32_t r = 0; r < total; r += R_THREADS * BU_ILP) {
+      uint32_t v[BU_ILP];
+      uint64_t b[BU_ILP], e[BU_ILP];
+      bool     live[BU_ILP], found[BU_ILP];
+#pragma unroll
+      for (int k = 0; k < BU_ILP; ++k) {
+        uint32_t const i = r + k * R_THREADS + threadIdx.x;
+        live[k]          = i < total;
+        v[k]             = live[k] ? s_cand[i] : 0u;
+        b[k] = e[k] = 0;
+        if (live[k]) b[k] = head[v[k]], e[k] = head[v[k] + 1];
+        found[k] = false;
+      }
+      // interleaved walks: every candidate checks up to R_BIG neighbours
+      // itself (most meet a visited one within the first few)
+      for (int step_i = 0; step_i < R_BIG; ++step_i) {
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < BU_ILP; ++k) {
+          if (live[k] && b[k] < e[k]) {
+            uint32_t const x = adj[b[k]++];
+            ++nedge;
+            if (bit_get(mark, x)) found[k] = true, live[k] = false;
+            any = true;
+          } else {
+            live[k] = false;
+          }
+        }
+        if (!any) break;
+      }
+      // rows still open after R_BIG neighbours: the whole warp, one at a time
+#pragma unroll
+      for (int k = 0; k < BU_ILP; ++k) {
+        bool const open = live[k] && b[k] < e[k];
+        unsigned   todo = __ballot_sync(0xFFFFFFFFu, open);
+        while (todo) {
+          unsigned const l = __ffs(todo) - 1;
+          todo &= todo - 1;
+          uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b[k], l), e0 = __shfl_sync(0xFFFFFFFFu, e[k], l);
+          bool           hit = false;
+          for (uint64_t x = b0; x < e0; x += 32) {
+            bool const in   = x + lane < e0;
+            bool const mine = in && bit_get(mark, adj[x + lane]);
+            nedge += in;
+            if (__any_sync(0xFFFFFFFFu, mine)) {
+              hit = true;
+              break;
+            }
+          }
+          if (lane == l) found[k] = hit;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < BU_ILP; ++k) {
+        bool const won = found[k] && bit_take(avail, v[k]);
+        if (won) bit_claim(mark, v[k]);
+        bq.push(won, v[k]);
+      }
+      __syncthreads();
+      if (s_n > BU_BUF - R_THREADS * BU_ILP) bq.flush(qout, qout_n, &s_base);
+    }
+    __syncthreads(); // s_cand is rewritten by the next chunk
   }
   bq.flush(qout, qout_n, &s_base);
 #pragma unroll
-  for (int s = 16; s; s >>= 1) {
-    nedge += __shfl_down_sync(0xFFFFFFFFu, nedge, s);
-    ncand += __shfl_down_sync(0xFFFFFFFFu, ncand, s);
-  }
-  if (lane == 0) {
-    if (nedge) atomicAdd(&st->edges_bu, static_cast<unsigned long long>(nedge));
-    if (ncand) atomicAdd(&st->cands_bu, static_cast<unsigned long long>(ncand));
-  }
+  for (int s = 16; s; s >>= 1) nedge += __shfl_down_sync(0xFFFFFFFFu, nedge, s);
+  if (lane == 0 && nedge) atomicAdd(&st->edges_bu, static_cast<unsigned long long>(nedge));
+  if (threadIdx.x == 0 && ncand) atomicAdd(&st->cands_bu, static_cast<unsigned long long>(ncand));
 }
 
 __global__ void
@@ -391,7 +418,7 @@ level_body(kspn_context* ctx, cudaGraph_t g, dgraph const& gr, search_io const& 
     dep                 = add_kernel(g, dep, &k_fs_down, FS_BLOCKS, FS_THREADS, io.td_head, f, ws.blocks, ws.prefix, ws.tile_start);
     dep                 = add_kernel(g, dep, &k_r_decide, 1, 1, st);
     dep = add_kernel(g, dep, &k_expand<take_op>, EX_BLOCKS, EX_THREADS, io.td_head, io.td_adj, f, ws.prefix, ws.tile_start, &st->ntiles, gate{ &st->mode, 0 }, take_op{ io.avail, io.mark });
-    dep = add_kernel(g, dep, &k_bottom_up, r_grid(gr.n), R_THREADS, gr.n, io.bu_head, io.bu_adj, io.avail, io.mark, f, gate{ &st->mode, 1 }, st);
+    dep = add_kernel(g, dep, &k_bottom_up, bu_grid(gr.n), R_THREADS, gr.n, io.bu_head, io.bu_adj, io.avail, io.mark, f, gate{ &st->mode, 1 }, st);
     add_kernel(g, dep, &k_r_advance<BW>, 1, 1, st, h, 1);
     return;
   }
@@ -404,7 +431,7 @@ level_body(kspn_context* ctx, cudaGraph_t g, dgraph const& gr, search_io const& 
   k_expand<take_op><<<EX_BLOCKS, EX_THREADS, 0, s>>>(io.td_head, io.td_adj, f, ws.prefix, ws.tile_start, &st->ntiles, gate{ &st->mode, 0 }, take_op{ io.avail, io.mark });
   prof_stop(ctx, 0);
   prof_start(ctx, 1);
-  k_bottom_up<<<r_grid(gr.n), R_THREADS, 0, s>>>(gr.n, io.bu_head, io.bu_adj, io.avail, io.mark, f, gate{ &st->mode, 1 }, st);
+  k_bottom_up<<<bu_grid(gr.n), R_THREADS, 0, s>>>(gr.n, io.bu_head, io.bu_adj, io.avail, io.mark, f, gate{ &st->mode, 1 }, st);
   prof_stop(ctx, 1);
   k_r_advance<BW><<<1, 1, 0, s>>>(st, h, 0);
   KSPN_CHECK_LAUNCH();
@@ -508,7 +535,8 @@ fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint3
   } else {
     // host-driven loop over the same kernels, expansion kernels bracketed
     // by CUDA events (kspn_options.profile)
-    uint32_t const words = (g.n + 31) / 32;
+    bool const     trace_done = st && st->levels_fw != 0; // trace the first FW-BW only
+    uint32_t const words      = (g.n + 31) / 32;
     k_r_init<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(words, und, ws.mark, ws.vis_a, ws.vis_b, rs);
     k_und_degrees<<<r_grid(g.n), R_THREADS, 0, ctx->stream>>>(g.n, und, g.fh, g.bh, rs);
     ctx->launches += 2;
@@ -532,11 +560,23 @@ fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint3
         KSPN_CUDA(cudaMemcpyAsync(hs, rs, sizeof(reach_state), cudaMemcpyDeviceToHost, ctx->stream));
         KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
         uint32_t const qn1 = hs->qn[hs->cur & 1u];
-        if (hs->mode == 0) prof_add(ctx, 0, KSPN_KERNEL_EXPAND, expand_bytes(qn0, hs->m_f, qn1, 4));
+        float          ms  = 0;
+        if (hs->mode == 0) ms = prof_add(ctx, 0, KSPN_KERNEL_EXPAND, expand_bytes(qn0, hs->m_f, qn1, 4));
         // bottom-up: candidate sweep reads the avail bitmap (n/8 B), then per
         // candidate its offset pair, per edge id + probe, per join queue
         // entry + two bit writes
-        else prof_add(ctx, 1, KSPN_KERNEL_BOTTOM_UP, static_cast<uint64_t>(g.n) / 8 + 16 * (hs->cands_bu - c0) + 8 * (hs->edges_bu - e0) + 8ull * qn1);
+        else ms = prof_add(ctx, 1, KSPN_KERNEL_BOTTOM_UP, static_cast<uint64_t>(g.n) / 8 + 16 * (hs->cands_bu - c0) + 8 * (hs->edges_bu - e0) + 8ull * qn1);
+        if (st && st->trace_levels < 32 && !trace_done) {
+          auto& t          = st->trace[st->trace_levels++];
+          t.backward       = static_cast<uint32_t>(bw);
+          t.bottom_up      = hs->mode;
+          t.frontier       = qn0;
+          t.discovered     = qn1;
+          t.frontier_edges = hs->m_f;
+          t.scanned        = hs->mode ? hs->edges_bu - e0 : hs->m_f;
+          t.candidates     = hs->mode ? hs->cands_bu - c0 : 0;
+          t.ms             = ms;
+        }
       }
       if (hs->err) break;
     }

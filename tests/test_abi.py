@@ -39,6 +39,8 @@ def test_struct_layouts_match_header():
     o = K.Options()
     assert K.lib().kspn_options_default(C.byref(o)) == 0
     assert o.struct_size == C.sizeof(K.Options)
+    assert K.lib().kspn_options_size() == C.sizeof(K.Options)
+    assert K.lib().kspn_stats_size() == C.sizeof(K.Stats)
     assert o.pipeline == K.PIPELINE_FAST and o.trim2 == 1 and o.validate == 1
 
 
