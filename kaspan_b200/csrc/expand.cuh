@@ -67,8 +67,9 @@ fs_chunk(uint32_t qn, uint32_t& beg, uint32_t& end)
 }
 
 static __global__ void __launch_bounds__(FS_THREADS)
-k_fs_reduce(uint64_t const* __restrict__ head, fio f, uint64_t* __restrict__ partial)
+k_fs_reduce(uint64_t const* __restrict__ head, fio f, uint64_t* __restrict__ partial, gate g)
 {
+  if (g.closed()) return;
   uint32_t const* q = f.in();
   uint32_t        beg, end;
   fs_chunk(f.in_n(), beg, end);
@@ -85,8 +86,9 @@ k_fs_reduce(uint64_t const* __restrict__ head, fio f, uint64_t* __restrict__ par
 // prefix[qn] = total; *ntiles = tiles; *edges += total (nullable);
 // *last = total (nullable).
 static __global__ void __launch_bounds__(1024)
-k_fs_partials(uint64_t* __restrict__ partial, uint64_t* __restrict__ prefix, fio f, uint32_t* __restrict__ ntiles, unsigned long long* __restrict__ edges, unsigned long long* __restrict__ last)
+k_fs_partials(uint64_t* __restrict__ partial, uint64_t* __restrict__ prefix, fio f, uint32_t* __restrict__ ntiles, unsigned long long* __restrict__ edges, unsigned long long* __restrict__ last, gate g)
 {
+  if (g.closed()) return;
   uint64_t const v = threadIdx.x < FS_BLOCKS ? partial[threadIdx.x] : 0;
   uint64_t       total;
   uint64_t const pre = block_exclusive_scan<uint64_t, 1024>(v, &total);
@@ -100,8 +102,9 @@ k_fs_partials(uint64_t* __restrict__ partial, uint64_t* __restrict__ prefix, fio
 }
 
 static __global__ void __launch_bounds__(FS_THREADS)
-k_fs_down(uint64_t const* __restrict__ head, fio f, uint64_t const* __restrict__ partial, uint64_t* __restrict__ prefix, uint32_t* __restrict__ tile_start)
+k_fs_down(uint64_t const* __restrict__ head, fio f, uint64_t const* __restrict__ partial, uint64_t* __restrict__ prefix, uint32_t* __restrict__ tile_start, gate g)
 {
+  if (g.closed()) return;
   uint32_t const* q = f.in();
   uint32_t        beg, end;
   fs_chunk(f.in_n(), beg, end);
@@ -237,9 +240,10 @@ frontier_scan(kspn_context* ctx, uint64_t const* head, fio f, uint32_t* ntiles_d
 {
   auto&              ws = ctx->ws;
   cudaStream_t const s  = ctx->stream;
-  k_fs_reduce<<<FS_BLOCKS, FS_THREADS, 0, s>>>(head, f, ws.blocks);
-  k_fs_partials<<<1, 1024, 0, s>>>(ws.blocks, ws.prefix, f, ntiles_dev, edges, last);
-  k_fs_down<<<FS_BLOCKS, FS_THREADS, 0, s>>>(head, f, ws.blocks, ws.prefix, tile_start);
+  gate const         open{ nullptr, 0 };
+  k_fs_reduce<<<FS_BLOCKS, FS_THREADS, 0, s>>>(head, f, ws.blocks, open);
+  k_fs_partials<<<1, 1024, 0, s>>>(ws.blocks, ws.prefix, f, ntiles_dev, edges, last, open);
+  k_fs_down<<<FS_BLOCKS, FS_THREADS, 0, s>>>(head, f, ws.blocks, ws.prefix, tile_start, open);
   KSPN_CHECK_LAUNCH();
   ctx->launches += 3;
 }

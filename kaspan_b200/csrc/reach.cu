@@ -77,6 +77,7 @@ struct reach_state
   uint32_t           id;       // id given to the SCC
   uint32_t           decided;  // SCC size
   uint32_t           min_ids;  // 1: id = smallest member, 0: id = pivot
+  uint32_t           scan;     // 1: this level scans its frontier
   uint32_t           levels_fw, bu_fw, levels_bw, bu_bw;
   unsigned long long m_u, m_out, m_in, m_f, alpha, beta;
   unsigned long long edges_td, edges_bu, cands_bu;
@@ -147,14 +148,25 @@ k_r_seed(uint32_t* avail, uint32_t* mark, uint32_t* q0, reach_state* st)
   st->m_u   = BW ? st->m_in : st->m_out;
 }
 
+// Before the frontier scan: a bottom-up search whose frontier is still
+// large stays bottom-up and needs no scan (scan = 0); otherwise scan = 1 and
+// the direction is settled after the scan by k_r_decide.
+__global__ void
+k_r_prescan(reach_state* st)
+{
+  uint32_t const qn = st->qn[st->cur & 1u];
+  st->scan          = !(st->mode == 1 && static_cast<unsigned long long>(qn) * st->beta >= st->n_und);
+  st->m_f           = 0;
+  st->qn[(st->cur & 1u) ^ 1u] = 0;
+}
+
 __global__ void
 k_r_decide(reach_state* st)
 {
+  if (!st->scan) return; // stays bottom-up
   unsigned long long const mf = st->m_f;
-  uint32_t const           qn = st->qn[st->cur & 1u];
   if (st->mode == 0 && mf * st->alpha > st->m_u) st->mode = 1;
-  else if (st->mode == 1 && static_cast<unsigned long long>(qn) * st->beta < st->n_und) st->mode = 0;
-  st->qn[(st->cur & 1u) ^ 1u] = 0;
+  else if (st->mode == 1) st->mode = 0; // frontier fell below n_und / beta
   if (st->mode == 0) st->edges_td += mf;
 }
 
@@ -216,6 +228,7 @@ k_bottom_up(uint32_t n,
 {
   if (g.closed()) return;
   __shared__ uint32_t s_cand[BU_WORDS * 32];
+  __shared__ uint32_t s_found[BU_WORDS];
   __shared__ uint32_t s_buf[BU_BUF];
   __shared__ uint32_t s_n, s_base;
   if (threadIdx.x == 0) s_n = 0;
@@ -230,6 +243,7 @@ k_bottom_up(uint32_t n,
     // 1. pack this chunk's candidates
     uint32_t const w    = wbase + threadIdx.x;
     uint32_t       word = w < words ? avail[w] : 0u;
+    s_found[threadIdx.x] = 0;
     if (w == words - 1 && (n & 31)) word &= (1u << (n & 31)) - 1u;
     uint32_t       total;
     uint32_t       j = block_exclusive_scan<uint32_t, R_THREADS>(static_cast<uint32_t>(__popc(word)), &total);
@@ -293,16 +307,23 @@ k_bottom_up(uint32_t n,
           if (lane == l) found[k] = hit;
         }
       }
+      // a candidate belongs to this block's chunk only, so its bits can be
+      // collected in shared memory and written once per word below
 #pragma unroll
       for (int k = 0; k < BU_ILP; ++k) {
-        bool const won = found[k] && bit_take(avail, v[k]);
-        if (won) bit_claim(mark, v[k]);
-        bq.push(won, v[k]);
+        if (found[k]) atomicOr(&s_found[(v[k] >> 5) - wbase], 1u << (v[k] & 31));
+        bq.push(found[k], v[k]);
       }
       __syncthreads();
       if (s_n > BU_BUF - R_THREADS * BU_ILP) bq.flush(qout, qout_n, &s_base);
     }
-    __syncthreads(); // s_cand is rewritten by the next chunk
+    __syncthreads(); // s_found complete; s_cand is rewritten by the next chunk
+    if (w < words && s_found[threadIdx.x]) {
+      // word w is written by this thread only (chunks are disjoint); other
+      // blocks may read it concurrently, which only delays their hits
+      avail[w] &= ~s_found[threadIdx.x];
+      mark[w] |= s_found[threadIdx.x];
+    }
   }
   bq.flush(qout, qout_n, &s_base);
 #pragma unroll
@@ -413,9 +434,11 @@ level_body(kspn_context* ctx, cudaGraph_t g, dgraph const& gr, search_io const& 
   fio const f{ ws.q0, ws.q1, &st->qn[0], &st->qn[1], &st->cur };
   if (g) {
     cudaGraphNode_t dep = nullptr;
-    dep                 = add_kernel(g, dep, &k_fs_reduce, FS_BLOCKS, FS_THREADS, io.td_head, f, ws.blocks);
-    dep                 = add_kernel(g, dep, &k_fs_partials, 1, 1024, ws.blocks, ws.prefix, f, &st->ntiles, static_cast<unsigned long long*>(nullptr), &st->m_f);
-    dep                 = add_kernel(g, dep, &k_fs_down, FS_BLOCKS, FS_THREADS, io.td_head, f, ws.blocks, ws.prefix, ws.tile_start);
+    gate const      sg{ &st->scan, 1 };
+    dep                 = add_kernel(g, dep, &k_r_prescan, 1, 1, st);
+    dep                 = add_kernel(g, dep, &k_fs_reduce, FS_BLOCKS, FS_THREADS, io.td_head, f, ws.blocks, sg);
+    dep                 = add_kernel(g, dep, &k_fs_partials, 1, 1024, ws.blocks, ws.prefix, f, &st->ntiles, static_cast<unsigned long long*>(nullptr), &st->m_f, sg);
+    dep                 = add_kernel(g, dep, &k_fs_down, FS_BLOCKS, FS_THREADS, io.td_head, f, ws.blocks, ws.prefix, ws.tile_start, sg);
     dep                 = add_kernel(g, dep, &k_r_decide, 1, 1, st);
     dep = add_kernel(g, dep, &k_expand<take_op>, EX_BLOCKS, EX_THREADS, io.td_head, io.td_adj, f, ws.prefix, ws.tile_start, &st->ntiles, gate{ &st->mode, 0 }, take_op{ io.avail, io.mark });
     dep = add_kernel(g, dep, &k_bottom_up, bu_grid(gr.n), R_THREADS, gr.n, io.bu_head, io.bu_adj, io.avail, io.mark, f, gate{ &st->mode, 1 }, st);
@@ -423,9 +446,11 @@ level_body(kspn_context* ctx, cudaGraph_t g, dgraph const& gr, search_io const& 
     return;
   }
   cudaStream_t const s = ctx->stream;
-  k_fs_reduce<<<FS_BLOCKS, FS_THREADS, 0, s>>>(io.td_head, f, ws.blocks);
-  k_fs_partials<<<1, 1024, 0, s>>>(ws.blocks, ws.prefix, f, &st->ntiles, nullptr, &st->m_f);
-  k_fs_down<<<FS_BLOCKS, FS_THREADS, 0, s>>>(io.td_head, f, ws.blocks, ws.prefix, ws.tile_start);
+  gate const         sg{ &st->scan, 1 };
+  k_r_prescan<<<1, 1, 0, s>>>(st);
+  k_fs_reduce<<<FS_BLOCKS, FS_THREADS, 0, s>>>(io.td_head, f, ws.blocks, sg);
+  k_fs_partials<<<1, 1024, 0, s>>>(ws.blocks, ws.prefix, f, &st->ntiles, nullptr, &st->m_f, sg);
+  k_fs_down<<<FS_BLOCKS, FS_THREADS, 0, s>>>(io.td_head, f, ws.blocks, ws.prefix, ws.tile_start, sg);
   k_r_decide<<<1, 1, 0, s>>>(st);
   prof_start(ctx, 0);
   k_expand<take_op><<<EX_BLOCKS, EX_THREADS, 0, s>>>(io.td_head, io.td_adj, f, ws.prefix, ws.tile_start, &st->ntiles, gate{ &st->mode, 0 }, take_op{ io.avail, io.mark });
@@ -435,7 +460,7 @@ level_body(kspn_context* ctx, cudaGraph_t g, dgraph const& gr, search_io const& 
   prof_stop(ctx, 1);
   k_r_advance<BW><<<1, 1, 0, s>>>(st, h, 0);
   KSPN_CHECK_LAUNCH();
-  ctx->launches += 7;
+  ctx->launches += 8;
 }
 
 search_io
@@ -590,8 +615,8 @@ fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint3
   KSPN_CUDA(cudaMemcpyAsync(hs, rs, sizeof(reach_state), cudaMemcpyDeviceToHost, ctx->stream));
   KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
   if (hs->err) throw error{ KSPN_ERR_TIMEOUT, "reachability: level cap exceeded" };
-  // kernels the graph ran: init, degrees, 2 seeds, 7 per level, 3 to finish
-  if (!ctx->prof) ctx->launches += 7 + 7ull * (hs->levels_fw + hs->levels_bw);
+  // kernels the graph ran: init, degrees, 2 seeds, 8 per level, 3 to finish
+  if (!ctx->prof) ctx->launches += 7 + 8ull * (hs->levels_fw + hs->levels_bw);
   ctx->td_edges += hs->edges_td + hs->edges_bu;
   if (st && st->levels_fw == 0 && st->levels_bw == 0) {
     st->levels_fw        = hs->levels_fw;
