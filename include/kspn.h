@@ -221,6 +221,23 @@ int kspn_trim_2(kspn_context* ctx, uint32_t n, uint64_t m,
  * every id becomes the minimum vertex carrying it.  Ids must be < n. */
 int kspn_normalise(kspn_context* ctx, uint32_t n, uint32_t* d_scc_id);
 
+/* Canonical relabel that allocates nothing (no counterpart in the
+ * reference).  Same result as kspn_normalise, for callers that cannot call
+ * cudaMalloc at this point: their device memory is already handed out by
+ * their own pool or caching allocator, or they cannot afford the device-wide
+ * synchronisation an allocation may cause.  No context is needed: the
+ * scratch is a file-scope device array for at most KSPN_NOALLOC_MAX_N
+ * vertices (4 MiB, held by every GPU that loads the library until exit).
+ *  - n > KSPN_NOALLOC_MAX_N: KSPN_ERR_INVALID_ARGUMENT, nothing runs; an id
+ *    >= n is left unchanged and reported as KSPN_ERR_INVALID_ARGUMENT.
+ *  - The first call on a device looks up the array's device address; make
+ *    that first call before any stream capture.
+ *  - All calls share the array: calls that overlap on the GPU race; serialise
+ *    them.  Runs on `stream` (a cudaStream_t, NULL = default stream) and
+ *    returns after the stream has finished. */
+#define KSPN_NOALLOC_MAX_N (1u << 20)
+int kspn_normalise_noalloc(uint32_t n, uint32_t* d_scc_id, void* stream);
+
 /* backward_complement_graph (kaspan/scc/backward_complement.hpp:22-68) on
  * the device: d_bw_head[n+1] / d_bw_csr[m] receive the transpose with rows
  * in ascending order. */

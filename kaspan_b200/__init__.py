@@ -23,6 +23,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libkspn.so")
 
+NOALLOC_MAX_N = 1 << 20  # KSPN_NOALLOC_MAX_N
 PIPELINE_FAST = 0
 PIPELINE_REFERENCE = 1
 UNDECIDED = 0xFFFFFFFF
@@ -148,6 +149,7 @@ SIGNATURES = {
     "kspn_trim_1_fixpoint": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P]),
     "kspn_trim_2": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P]),
     "kspn_normalise": (_i32, [_P, _u32, _P]),
+    "kspn_normalise_noalloc": (_i32, [_u32, _P, _P]),
     "kspn_transpose": (_i32, [_P, _u32, _u64, _P, _P, _P, _P]),
     "kspn_gen_gnm": (_i32, [_P, _u32, _u64, _u64, _P, _P]),
     "kspn_gen_rmat": (_i32, [_P, _i32, _u64, _u64, _u64, _u64, _u64, _i32, _P, _P]),
