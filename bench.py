@@ -176,6 +176,7 @@ def run_kspn(args):
     pipeline = K.PIPELINE_FAST if args.pipeline == "fast" else K.PIPELINE_REFERENCE
     opt = K.default_options(pipeline=pipeline, validate=0)
     prof_opt = K.default_options(pipeline=pipeline, validate=0, profile=1)
+    trace_opt = K.default_options(pipeline=pipeline, validate=0, trace=1)
 
     def barrier():
         if world > 1:
@@ -199,6 +200,13 @@ def run_kspn(args):
         barrier()
     launches = ctx.launches - l0
     ms = ev0.elapsed_time(ev1) / args.steps
+    # phase stamps of the persistent searches (one extra step, not timed)
+    ctx.scc_device(G.n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, trace_opt, st)
+    marks = st.as_dict()["search_marks"]
+    search_phases = {}
+    for (ph, t1), (_, t0) in zip(marks[1:], marks[:-1]):
+        if t1 > t0:
+            search_phases[ph] = search_phases.get(ph, 0.0) + (t1 - t0) * 1e-6
 
     # per-kernel-class device time: the same decomposition with the library's
     # event brackets on (levels driven from the host so every expansion
@@ -284,7 +292,9 @@ def run_kspn(args):
             "clocks": clk.summary(),
             "phases": {"decided": last["decided"], "ms": {k: round(v, 4) for k, v in last["ms"].items()}, "levels_fw": last["levels_fw"],
                        "levels_bw": last["levels_bw"], "bottom_up": last["levels_bottom_up"], "label_calls": last["label_calls"],
-                       "edges_scanned": last["edges_scanned"], "trace": trace, "kernels": {k: {"ms": round(a[0] / prof_steps, 4), "GB/s": round(a[1] / (a[0] * 1e-3) / 1e9, 1) if a[0] else 0}
+                       "edges_scanned": last["edges_scanned"], "trace": trace,
+                       "search_phase_ms": {{1: "scan_partials", 2: "scan_totals", 3: "prefix", 4: "expand", 5: "sweep", 6: "level_end"}.get(k, k): round(v, 4) for k, v in search_phases.items()},
+                       "kernels": {k: {"ms": round(a[0] / prof_steps, 4), "GB/s": round(a[1] / (a[0] * 1e-3) / 1e9, 1) if a[0] else 0}
                                                                             for k, a in agg.items()}},
         }
         if not args.no_cpu_baseline:

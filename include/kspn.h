@@ -60,7 +60,8 @@ typedef struct kspn_options
   uint32_t max_label_iters; /* cap on label-propagation sweeps per search (0 = n + 2) */
   uint32_t max_rounds;      /* cap on pipeline rounds (0 = n + 2) */
   int32_t  profile;         /* 1: time kernel classes with CUDA events (kspn_stats.kernel_*) */
-  uint32_t reserved[6];
+  int32_t  trace;           /* 1: timestamp the phases of the persistent searches (kspn_stats.search_*) */
+  uint32_t reserved[5];
 } kspn_options;
 
 /* Per-call statistics (all fields written by a successful call). */
@@ -113,6 +114,13 @@ typedef struct kspn_stats
     float    ms;             /* event time of the level's expansion kernel */
     uint32_t pad;
   } trace[32];
+  /* kspn_options.trace: %globaltimer stamps (ns, from the launch) taken by
+   * block 0 of the first FW-BW's persistent searches after each phase, and
+   * the phase that ended there: 1 scan partials, 2 scan totals, 3 prefix,
+   * 4 expansion (top-down), 5 sweep (bottom-up), 6 level end. */
+  uint32_t search_marks;
+  uint32_t search_phase[128];
+  uint64_t search_ns[128];
 } kspn_stats;
 
 typedef struct kspn_context kspn_context;

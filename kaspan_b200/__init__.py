@@ -55,7 +55,8 @@ class Options(C.Structure):
         ("max_label_iters", C.c_uint32),
         ("max_rounds", C.c_uint32),
         ("profile", C.c_int32),
-        ("reserved", C.c_uint32 * 6),
+        ("trace", C.c_int32),
+        ("reserved", C.c_uint32 * 5),
     ]
 
 
@@ -93,6 +94,9 @@ class Stats(C.Structure):
         ("kernel_calls", C.c_uint64 * 4),
         ("trace_levels", C.c_uint32),
         ("trace", LevelTrace * 32),
+        ("search_marks", C.c_uint32),
+        ("search_phase", C.c_uint32 * 128),
+        ("search_ns", C.c_uint64 * 128),
     ]
 
     def as_dict(self) -> dict:
@@ -116,6 +120,7 @@ class Stats(C.Structure):
                        "discovered": t.discovered, "frontier_edges": int(t.frontier_edges), "scanned": int(t.scanned),
                        "candidates": int(t.candidates), "ms": round(float(t.ms), 4)}
                       for t in self.trace[: min(self.trace_levels, 32)]],
+            "search_marks": [(int(self.search_phase[i]), int(self.search_ns[i])) for i in range(min(self.search_marks, 128))],
         }
 
 

@@ -59,6 +59,7 @@ layout(workspace& ws, char* base, uint32_t n, uint64_t m)
   ws.vis_a             = c.take<uint32_t>(words);
   ws.vis_b             = c.take<uint32_t>(words);
   ws.mark              = c.take<uint32_t>(words);
+  ws.fresh             = c.take<uint32_t>(words);
   ws.und               = c.take<uint32_t>(words);
   ws.label             = c.take<uint32_t>(nn);
   ws.indeg             = c.take<uint32_t>(nn);
@@ -67,7 +68,7 @@ layout(workspace& ws, char* base, uint32_t n, uint64_t m)
   ws.blocks            = c.take<uint64_t>(std::max<size_t>(scan_partial_entries(nn), 4096));
   ws.pivot             = c.take<uint64_t>(8192);
   ws.tile_start        = c.take<uint32_t>(m / 2048 + 4);
-  ws.rstate            = c.take<char>(512);
+  ws.rstate            = c.take<char>(4096);
   return align_up(c.off);
 }
 
@@ -424,7 +425,7 @@ kspn_context_create_on_stream(int device, void* stream, kspn_context** out)
     KSPN_CUDA(cudaMallocHost(&h, 64 * sizeof(uint32_t)));
     ctx->h_ctr   = static_cast<uint32_t*>(h);
     ctx->h_ctr64 = reinterpret_cast<uint64_t*>(ctx->h_ctr + 32);
-    KSPN_CUDA(cudaMallocHost(&ctx->h_state, 512));
+    KSPN_CUDA(cudaMallocHost(&ctx->h_state, 4096));
     for (auto& e : ctx->ev) KSPN_CUDA(cudaEventCreate(&e));
     for (auto& e : ctx->pe) KSPN_CUDA(cudaEventCreate(&e));
   });

@@ -162,6 +162,47 @@ tile_max_scan(uint32_t* s)
   __syncthreads();
 }
 
+// Expands tile `tile` of a scanned queue (ntiles tiles, total edges):
+// calls op(u, v, valid) on every edge slot and appends the winners to bq.
+// All threads of the block call it.  Queue, prefix and tile starts are read
+// through L2 (ld.cg): inside a persistent launch other blocks wrote them.
+// s_j: EX_TILE words of shared memory; s_i: two words.
+template<typename Op>
+__device__ __forceinline__ void
+expand_tile(uint32_t tile, uint32_t ntiles, uint32_t const* q, uint32_t qn, uint64_t total, uint64_t const* prefix, uint32_t const* tile_start, uint64_t const* __restrict__ head,
+            uint32_t const* __restrict__ adj, uint32_t* s_j, uint32_t* s_i, block_queue& bq, Op const& op)
+{
+  uint64_t const t0 = static_cast<uint64_t>(tile) * EX_TILE;
+  uint64_t const t1 = t0 + EX_TILE < total ? t0 + EX_TILE : total;
+  if (threadIdx.x == 0) {
+    s_i[0] = __ldcg(tile_start + tile);
+    s_i[1] = tile + 1 < ntiles ? __ldcg(tile_start + tile + 1) : qn - 1;
+  }
+#pragma unroll
+  for (int k = 0; k < EX_ITEMS; ++k) s_j[k * EX_THREADS + threadIdx.x] = 0;
+  __syncthreads();
+  uint32_t const i0 = s_i[0], i1 = s_i[1];
+  for (uint32_t j = i0 + 1 + threadIdx.x; j <= i1; j += EX_THREADS) {
+    uint64_t const p = __ldcg(prefix + j);
+    if (p < t1) atomicMax(&s_j[p - t0], j - i0);
+  }
+  __syncthreads();
+  tile_max_scan(s_j);
+#pragma unroll 4
+  for (int k = 0; k < EX_ITEMS; ++k) {
+    uint32_t const slot  = k * EX_THREADS + threadIdx.x;
+    uint64_t const e     = t0 + slot;
+    bool const     valid = e < t1;
+    uint32_t       u = 0, v = 0;
+    if (valid) {
+      uint32_t const j = i0 + s_j[slot];
+      u                = __ldcg(q + j);
+      v                = adj[head[u] + (e - __ldcg(prefix + j))];
+    }
+    bq.push(op(u, v, valid), v);
+  }
+}
+
 // op(u, v, valid) -> bool: u = source (queued vertex), v = neighbour; true
 // appends v to the output queue.  Called by every lane (valid == false on
 // padding lanes).
@@ -179,7 +220,7 @@ k_expand(uint64_t const* __restrict__ head,
   if (g.closed()) return;
   __shared__ uint32_t s_j[EX_TILE];
   __shared__ uint32_t s_out[EX_TILE];
-  __shared__ uint32_t s_i0, s_i1, s_n, s_base;
+  __shared__ uint32_t s_i[2], s_n, s_base;
   uint32_t const*     q      = f.in();
   uint32_t* const     qout   = f.out();
   uint32_t* const     qout_n = f.out_n();
@@ -189,35 +230,7 @@ k_expand(uint64_t const* __restrict__ head,
   if (threadIdx.x == 0) s_n = 0;
   block_queue bq{ s_out, &s_n };
   for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    uint64_t const t0 = static_cast<uint64_t>(tile) * EX_TILE;
-    uint64_t const t1 = t0 + EX_TILE < total ? t0 + EX_TILE : total;
-    if (threadIdx.x == 0) {
-      s_i0 = tile_start[tile];
-      s_i1 = tile + 1 < ntiles ? tile_start[tile + 1] : qn - 1;
-    }
-#pragma unroll
-    for (int k = 0; k < EX_ITEMS; ++k) s_j[k * EX_THREADS + threadIdx.x] = 0;
-    __syncthreads();
-    uint32_t const i0 = s_i0, i1 = s_i1;
-    for (uint32_t j = i0 + 1 + threadIdx.x; j <= i1; j += EX_THREADS) {
-      uint64_t const p = prefix[j];
-      if (p < t1) atomicMax(&s_j[p - t0], j - i0);
-    }
-    __syncthreads();
-    tile_max_scan(s_j);
-#pragma unroll 4
-    for (int k = 0; k < EX_ITEMS; ++k) {
-      uint32_t const slot  = k * EX_THREADS + threadIdx.x;
-      uint64_t const e     = t0 + slot;
-      bool const     valid = e < t1;
-      uint32_t       u = 0, v = 0;
-      if (valid) {
-        uint32_t const j = i0 + s_j[slot];
-        u                = q[j];
-        v                = adj[head[u] + (e - prefix[j])];
-      }
-      bq.push(op(u, v, valid), v);
-    }
+    expand_tile(tile, ntiles, q, qn, total, prefix, tile_start, head, adj, s_j, s_i, bq, op);
     bq.flush(qout, qout_n, &s_base);
   }
 }

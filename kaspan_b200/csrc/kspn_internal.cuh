@@ -66,6 +66,16 @@ bit_claim(uint32_t* bm, uint32_t v)
   return (atomicOr(bm + (v >> 5), mask) & mask) == 0;
 }
 
+// GPU-scope acquire load (coherent across SMs, never hoisted by the
+// compiler): polls of words other blocks update inside one launch.
+__device__ __forceinline__ uint32_t
+ld_acquire(uint32_t const* p)
+{
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 __device__ __forceinline__ unsigned
 lane_id()
 {
@@ -186,6 +196,7 @@ struct workspace
   uint32_t* vis_a    = nullptr; // bitmap
   uint32_t* vis_b    = nullptr; // bitmap
   uint32_t* mark     = nullptr; // bitmap
+  uint32_t* fresh    = nullptr; // bitmap: vertices found by the last bottom-up sweep
   uint32_t* label    = nullptr; // n
   uint32_t* indeg    = nullptr; // n
   uint32_t* outdeg   = nullptr; // n
@@ -195,7 +206,7 @@ struct workspace
   uint64_t* ctr64    = nullptr; // 8 (64-bit counters)
   uint64_t* pivot    = nullptr; // per-block pivot keys (4096 u64 products + 4096 u32 ids)
   uint32_t* tile_start = nullptr; // m / 2048 + 2 (frontier expansion)
-  void*     rstate     = nullptr; // 512 B device control block of a FW-BW
+  void*     rstate     = nullptr; // 4 KiB device control blocks (FW-BW at 0, trim at 512, search stamps at 2048)
   // owned graph storage (host inputs, or a CSC built on device)
   uint64_t* g_fh = nullptr;
   uint32_t* g_fc = nullptr;
@@ -269,8 +280,9 @@ struct kspn_context
   // kernel-class timing (kspn_options.profile): two event pairs in flight
   kspn_stats*        prof       = nullptr;
   cudaEvent_t        pe[4]      = {};
-  void*              h_state    = nullptr; // pinned 512 B mirror of ws.rstate
+  void*              h_state    = nullptr; // pinned 4 KiB mirror of ws.rstate
   kspn::cached_graph fwbw;                 // one-launch FW-BW graph
+  kspn::cached_graph trim;                 // one-launch trim fixpoint graph
   kspn::dev_buffer   bufs[kspn::BUF_COUNT];
 };
 

@@ -24,15 +24,16 @@
 // Each edge costs at most one probe and each discovery two atomics; the
 // undecided set and ids are written once at the end, a word at a time.
 //
-// Level control lives on the device (reach_state): a `decide` kernel picks
-// the direction from the scan, both expansion kernels are launched and the
-// one whose gate is closed returns at once, and an `advance` kernel flips the
-// queues and sets the loop condition.  The whole FW-BW is ONE CUDA graph
-// launch with two conditional while-nodes (one per search); with profiling
-// on, the same kernels run from a host loop with CUDA events around the
-// expansion kernels.
+// Level control lives on the device (reach_state).  Each search is ONE
+// persistent cooperative launch (k_search) whose blocks run every level:
+// frontier scan, direction choice, top-down tiles or bottom-up chunks, and
+// the queue flip, separated by a bounded grid barrier.  With profiling on,
+// the same phase bodies run as separate launches from a host loop
+// (decide / expand / bottom-up / advance kernels) with CUDA events around
+// the expansion kernels.
 #include "expand.cuh"
 
+#include <algorithm>
 #include <cstring>
 #include <tuple>
 
@@ -41,7 +42,6 @@ namespace kspn {
 namespace {
 
 constexpr int R_THREADS = 256;
-constexpr int R_BIG     = 32;
 constexpr int BU_BUF    = 2048;
 constexpr int BU_ILP    = 4;
 
@@ -52,13 +52,13 @@ r_grid(uint64_t items)
   return static_cast<unsigned>(b < 148ull * 8 ? (b ? b : 1) : 148ull * 8);
 }
 
-// bottom-up: one block per chunk of R_THREADS bitmap words, capped at the
+// bottom-up: one block per (8 warps x 32 bitmap words), capped at the
 // resident-block count
 unsigned
 bu_grid(uint32_t n)
 {
-  uint64_t const chunks = ((static_cast<uint64_t>(n) + 31) / 32 + R_THREADS - 1) / R_THREADS;
-  return static_cast<unsigned>(chunks < 148ull * 4 ? (chunks ? chunks : 1) : 148ull * 4);
+  uint64_t const chunks = ((static_cast<uint64_t>(n) + 31) / 32 + 32 * (R_THREADS / 32) - 1) / (32 * (R_THREADS / 32));
+  return static_cast<unsigned>(chunks < 148ull * 5 ? (chunks ? chunks : 1) : 148ull * 5);
 }
 
 // Device-side control block of one FW-BW (lives in the workspace).
@@ -78,54 +78,44 @@ struct reach_state
   uint32_t           decided;  // SCC size
   uint32_t           min_ids;  // 1: id = smallest member, 0: id = pivot
   uint32_t           scan;     // 1: this level scans its frontier
+  uint32_t           mat;      // 1: build the frontier queue from `fresh` first (bottom-up -> top-down)
+  uint32_t           mat_n;    // slots handed out while building it
   uint32_t           levels_fw, bu_fw, levels_bw, bu_bw;
   unsigned long long m_u, m_out, m_in, m_f, alpha, beta;
   unsigned long long edges_td, edges_bu, cands_bu;
+  uint32_t           bar_count, bar_gen, bar_err; // grid barrier of the persistent search
+  uint32_t           marks;                       // phase stamps taken (kspn_options.trace)
 };
+
+// phase stamps live after the state: uint32 phase[128], uint64 ns[128]
+constexpr int MARKS = 128;
 static_assert(sizeof(reach_state) <= 512, "reach_state must fit its workspace slot");
 
+// Per search pair: cand = und, vis_a = vis_b = 0, n_und = |und| (one
+// atomic per warp), and the unexplored-edge bound m_out = m_in = m (Beamer's
+// m_u only has to be of the right size: it gates the switch to bottom-up).
 __global__ void __launch_bounds__(R_THREADS)
-k_r_init(uint32_t words, uint32_t const* __restrict__ und, uint32_t* __restrict__ cand, uint32_t* __restrict__ vis_a, uint32_t* __restrict__ vis_b, reach_state* st)
+k_r_init(uint32_t words, uint64_t m, uint32_t const* __restrict__ und, uint32_t* __restrict__ cand, uint32_t* __restrict__ vis_a, uint32_t* __restrict__ vis_b, reach_state* st)
 {
+  uint32_t c = 0;
   for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) {
-    cand[w]  = und[w];
-    vis_a[w] = 0;
-    vis_b[w] = 0;
+    uint32_t const u = und[w];
+    cand[w]          = u;
+    vis_a[w]         = 0;
+    vis_b[w]         = 0;
+    c += __popc(u);
   }
+#pragma unroll
+  for (int sh = 16; sh; sh >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, sh);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(&st->n_und, c);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    st->n_und = 0;
-    st->m_out = st->m_in = 0;
+    st->m_out = st->m_in = m;
     st->edges_td = st->edges_bu = st->cands_bu = 0;
     st->err                                    = 0;
     st->decided                                = 0;
     st->levels_fw = st->bu_fw = st->levels_bw = st->bu_bw = 0;
-  }
-}
-
-// n_und, and the out-/in-degree sums of undecided vertices.
-__global__ void __launch_bounds__(R_THREADS)
-k_und_degrees(uint32_t n, uint32_t const* __restrict__ und, uint64_t const* __restrict__ fh, uint64_t const* __restrict__ bh, reach_state* st)
-{
-  uint64_t       so = 0, si = 0;
-  uint32_t       c  = 0;
-  unsigned const lane = threadIdx.x & 31u;
-  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; t < n; t += static_cast<uint64_t>(gridDim.x) * R_THREADS) {
-    uint32_t const v = static_cast<uint32_t>(t);
-    if (!bit_get(und, v)) continue;
-    ++c;
-    so += fh[v + 1] - fh[v];
-    si += bh[v + 1] - bh[v];
-  }
-#pragma unroll
-  for (int s = 16; s; s >>= 1) {
-    c += __shfl_down_sync(0xFFFFFFFFu, c, s);
-    so += __shfl_down_sync(0xFFFFFFFFu, so, s);
-    si += __shfl_down_sync(0xFFFFFFFFu, si, s);
-  }
-  if (lane == 0) {
-    if (c) atomicAdd(&st->n_und, c);
-    if (so) atomicAdd(&st->m_out, static_cast<unsigned long long>(so));
-    if (si) atomicAdd(&st->m_in, static_cast<unsigned long long>(si));
+    st->bar_count = st->bar_gen = st->bar_err = 0;
+    st->marks                                 = 0;
   }
 }
 
@@ -146,20 +136,14 @@ k_r_seed(uint32_t* avail, uint32_t* mark, uint32_t* q0, reach_state* st)
   st->bu    = 0;
   st->mode  = 0;
   st->m_u   = BW ? st->m_in : st->m_out;
+  st->scan  = 1;
+  st->mat   = 0;
+  st->m_f   = 0;
 }
 
 // Before the frontier scan: a bottom-up search whose frontier is still
 // large stays bottom-up and needs no scan (scan = 0); otherwise scan = 1 and
 // the direction is settled after the scan by k_r_decide.
-__global__ void
-k_r_prescan(reach_state* st)
-{
-  uint32_t const qn = st->qn[st->cur & 1u];
-  st->scan          = !(st->mode == 1 && static_cast<unsigned long long>(qn) * st->beta >= st->n_und);
-  st->m_f           = 0;
-  st->qn[(st->cur & 1u) ^ 1u] = 0;
-}
-
 __global__ void
 k_r_decide(reach_state* st)
 {
@@ -170,25 +154,50 @@ k_r_decide(reach_state* st)
   if (st->mode == 0) st->edges_td += mf;
 }
 
+// End of a level: explored edges, level count, queue flip, cap, and the
+// next level's pre-scan step.  Returns the loop condition.
+// (state read through L2: counters were updated by other blocks)
 template<bool BW>
-__global__ void
-k_r_advance(reach_state* st, cudaGraphConditionalHandle h, int in_graph)
+__device__ __forceinline__ unsigned
+advance_body(reach_state* st)
 {
-  unsigned long long const mf = st->m_f;
-  st->m_u                     = st->m_u > mf ? st->m_u - mf : 0;
-  st->level += 1;
-  st->bu += st->mode;
-  st->cur ^= 1u;
-  unsigned cond = st->qn[st->cur & 1u] > 0;
-  if (cond && st->level >= st->cap) {
+  unsigned long long const mf   = __ldcg(&st->m_f);
+  unsigned long long const mu   = __ldcg(&st->m_u);
+  uint32_t const           mode = __ldcg(&st->mode);
+  uint32_t const           lvl  = __ldcg(&st->level) + 1;
+  uint32_t const           bu   = __ldcg(&st->bu) + mode;
+  uint32_t const           cur  = (__ldcg(&st->cur) ^ 1u) & 1u;
+  uint32_t const           qn   = __ldcg(&st->qn[cur]);
+  st->m_u                       = mu > mf ? mu - mf : 0;
+  st->level                     = lvl;
+  st->bu                        = bu;
+  st->cur                       = cur;
+  unsigned cond                 = qn > 0;
+  if (cond && lvl >= __ldcg(&st->cap)) {
     st->err = 1;
     cond    = 0;
   }
   if (!cond) {
-    if (BW) st->levels_bw = st->level, st->bu_bw = st->bu;
-    else st->levels_fw = st->level, st->bu_fw = st->bu;
+    if (BW) st->levels_bw = lvl, st->bu_bw = bu;
+    else st->levels_fw = lvl, st->bu_fw = bu;
+  } else {
+    // the next level's pre-scan step; a bottom-up search about to return
+    // top-down first builds its frontier queue from `fresh`
+    uint32_t const scan = !(mode == 1 && static_cast<unsigned long long>(qn) * __ldcg(&st->beta) >= __ldcg(&st->n_und));
+    st->scan            = scan;
+    st->mat             = (mode == 1 && scan) ? 1u : 0u;
+    st->mat_n           = 0;
+    st->m_f             = 0;
+    st->qn[cur ^ 1u]    = 0;
   }
-  if (in_graph) cudaGraphSetConditional(h, cond);
+  return cond;
+}
+
+template<bool BW>
+__global__ void
+k_r_advance(reach_state* st)
+{
+  advance_body<BW>(st);
 }
 
 // top-down, both directions: v joins when its bit in `avail` is taken
@@ -214,78 +223,104 @@ struct take_op
 //  * Each thread then carries BU_ILP candidates at once (interleaved row
 //    walks) so their dependent loads overlap; a row with no visited
 //    neighbour among its first R_BIG entries is finished by the whole warp.
-constexpr int BU_WORDS = R_THREADS;
+constexpr int BU_WARPS = R_THREADS / 32;
+constexpr int BU_STEPS = 32; // neighbours a candidate checks itself before its warp helps
 
-__global__ void __launch_bounds__(R_THREADS)
-k_bottom_up(uint32_t n,
-            uint64_t const* __restrict__ head,
-            uint32_t const* __restrict__ adj,
-            uint32_t* __restrict__ avail,
-            uint32_t* __restrict__ mark,
-            fio f,
-            gate g,
-            reach_state* st)
+// Per-warp shared memory of the sweep.
+struct bu_warp_smem
 {
-  if (g.closed()) return;
-  __shared__ uint32_t s_cand[BU_WORDS * 32];
-  __shared__ uint32_t s_found[BU_WORDS];
-  __shared__ uint32_t s_buf[BU_BUF];
-  __shared__ uint32_t s_n, s_base;
-  if (threadIdx.x == 0) s_n = 0;
-  __syncthreads();
-  uint32_t* const qout   = f.out();
-  uint32_t* const qout_n = f.out_n();
-  block_queue     bq{ s_buf, &s_n };
-  unsigned const  lane  = threadIdx.x & 31u;
-  uint32_t const  words = (n + 31) / 32;
-  uint64_t        nedge = 0, ncand = 0;
-  for (uint32_t wbase = blockIdx.x * BU_WORDS; wbase < words; wbase += gridDim.x * BU_WORDS) {
-    // 1. pack this chunk's candidates
-    uint32_t const w    = wbase + threadIdx.x;
-    uint32_t       word = w < words ? avail[w] : 0u;
-    s_found[threadIdx.x] = 0;
+  uint32_t cand[32 * 32]; // the warp's chunk (32 words = 1024 vertices), packed
+  uint32_t found[32];     // found bits per word of the chunk
+};
+
+// Bottom-up sweep over the chunks of 32 bitmap words given to this warp
+// (chunk c = words [32c, 32c + 32), c = first, first + step, ...).
+// Candidates are the set bits of `avail`; one joins when a neighbour in its
+// head/adj row is in `mark`.  Warps work independently (no block barrier):
+// the warp packs its chunk's candidates (popcount scan over its 32 words),
+// each lane walks BU_ILP candidates interleaved -- all neighbour loads of a
+// step, then all probes -- and rows still open after BU_STEPS neighbours
+// are finished by the whole warp with early exit.  Lane i then owns word i
+// of the chunk: it clears the found bits from avail, sets them in mark and
+// writes the word of `fresh` (the sweep's discoveries).  No queue is
+// written; the count goes to *found_count.  `avail` and `mark` are read
+// through L2 (other blocks of a persistent launch change them).
+__device__ __forceinline__ void
+bu_sweep_warp(uint32_t first,
+              uint32_t step,
+              uint32_t n,
+              uint64_t const* __restrict__ head,
+              uint32_t const* __restrict__ adj,
+              uint32_t* avail,
+              uint32_t* mark,
+              uint32_t* fresh,
+              bu_warp_smem& sm,
+              uint32_t& nfound,
+              uint64_t& nedge,
+              uint64_t& ncand)
+{
+  unsigned const lane   = threadIdx.x & 31u;
+  uint32_t const words  = (n + 31) / 32;
+  uint32_t const chunks = (words + 31) / 32;
+  for (uint32_t c = first; c < chunks; c += step) {
+    uint32_t const w    = c * 32 + lane;
+    uint32_t       word = w < words ? __ldcg(avail + w) : 0u;
     if (w == words - 1 && (n & 31)) word &= (1u << (n & 31)) - 1u;
-    uint32_t       total;
-    uint32_t       j = block_exclusive_scan<uint32_t, R_THREADS>(static_cast<uint32_t>(__popc(word)), &total);
-    while (word) {
-      uint32_t const b = __ffs(word) - 1;
-      word &= word - 1;
-      s_cand[j++] = w * 32 + b;
+    uint32_t const cnt = __popc(word);
+    uint32_t       pos = cnt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, pos, d);
+      if (lane >= static_cast<unsigned>(d)) pos += y;
     }
-    __syncthreads();
-    ncand += threadIdx.x == 0 ? total : 0;
-    // 2. walk the packed candidates, BU_ILP per thread
-    for (uint32_t r = 0; r < total; r += R_THREADS * BU_ILP) {
+    uint32_t const total = __shfl_sync(0xFFFFFFFFu, pos, 31);
+    pos -= cnt;
+    while (word) {
+      uint32_t const bb = __ffs(word) - 1;
+      word &= word - 1;
+      sm.cand[pos++] = w * 32 + bb;
+    }
+    sm.found[lane] = 0;
+    __syncwarp();
+    ncand += lane == 0 ? total : 0;
+    for (uint32_t r = 0; r < total; r += 32 * BU_ILP) {
       uint32_t v[BU_ILP];
       uint64_t b[BU_ILP], e[BU_ILP];
       bool     live[BU_ILP], found[BU_ILP];
 #pragma unroll
       for (int k = 0; k < BU_ILP; ++k) {
-        uint32_t const i = r + k * R_THREADS + threadIdx.x;
+        uint32_t const i = r + k * 32 + lane;
         live[k]          = i < total;
-        v[k]             = live[k] ? s_cand[i] : 0u;
+        v[k]             = live[k] ? sm.cand[i] : 0u;
         b[k] = e[k] = 0;
         if (live[k]) b[k] = head[v[k]], e[k] = head[v[k] + 1];
         found[k] = false;
       }
-      // interleaved walks: every candidate checks up to R_BIG neighbours
-      // itself (most meet a visited one within the first few)
-      for (int step_i = 0; step_i < R_BIG; ++step_i) {
-        bool any = false;
+      for (int s_i = 0; s_i < BU_STEPS; ++s_i) {
+        bool     act[BU_ILP];
+        uint32_t x[BU_ILP], wd[BU_ILP];
+        bool     any = false;
 #pragma unroll
         for (int k = 0; k < BU_ILP; ++k) {
-          if (live[k] && b[k] < e[k]) {
-            uint32_t const x = adj[b[k]++];
-            ++nedge;
-            if (bit_get(mark, x)) found[k] = true, live[k] = false;
-            any = true;
-          } else {
-            live[k] = false;
-          }
+          act[k] = live[k] && b[k] < e[k];
+          x[k]   = act[k] ? adj[b[k]] : 0u;
+          any |= act[k];
         }
-        if (!any) break;
+        if (!__any_sync(0xFFFFFFFFu, any)) break;
+#pragma unroll
+        for (int k = 0; k < BU_ILP; ++k) wd[k] = act[k] ? __ldcg(mark + (x[k] >> 5)) : 0u;
+#pragma unroll
+        for (int k = 0; k < BU_ILP; ++k) {
+          if (!act[k]) {
+            live[k] = false;
+            continue;
+          }
+          ++b[k];
+          ++nedge;
+          if ((wd[k] >> (x[k] & 31)) & 1u) found[k] = true, live[k] = false;
+        }
       }
-      // rows still open after R_BIG neighbours: the whole warp, one at a time
+      // rows still open: the whole warp, one at a time, with early exit
 #pragma unroll
       for (int k = 0; k < BU_ILP; ++k) {
         bool const open = live[k] && b[k] < e[k];
@@ -296,10 +331,11 @@ k_bottom_up(uint32_t n,
           uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b[k], l), e0 = __shfl_sync(0xFFFFFFFFu, e[k], l);
           bool           hit = false;
           for (uint64_t x = b0; x < e0; x += 32) {
-            bool const in   = x + lane < e0;
-            bool const mine = in && bit_get(mark, adj[x + lane]);
+            bool const     in = x + lane < e0;
+            uint32_t const y  = in ? adj[x + lane] : 0u;
+            bool const     h  = in && ((__ldcg(mark + (y >> 5)) >> (y & 31)) & 1u);
             nedge += in;
-            if (__any_sync(0xFFFFFFFFu, mine)) {
+            if (__any_sync(0xFFFFFFFFu, h)) {
               hit = true;
               break;
             }
@@ -307,28 +343,297 @@ k_bottom_up(uint32_t n,
           if (lane == l) found[k] = hit;
         }
       }
-      // a candidate belongs to this block's chunk only, so its bits can be
-      // collected in shared memory and written once per word below
 #pragma unroll
-      for (int k = 0; k < BU_ILP; ++k) {
-        if (found[k]) atomicOr(&s_found[(v[k] >> 5) - wbase], 1u << (v[k] & 31));
-        bq.push(found[k], v[k]);
+      for (int k = 0; k < BU_ILP; ++k)
+        if (found[k]) atomicOr(&sm.found[(v[k] >> 5) - c * 32], 1u << (v[k] & 31));
+    }
+    __syncwarp();
+    uint32_t const fnd = sm.found[lane];
+    if (w < words) {
+      if (fnd) {
+        atomicAnd(avail + w, ~fnd);
+        atomicOr(mark + w, fnd);
       }
-      __syncthreads();
-      if (s_n > BU_BUF - R_THREADS * BU_ILP) bq.flush(qout, qout_n, &s_base);
+      fresh[w] = fnd;
     }
-    __syncthreads(); // s_found complete; s_cand is rewritten by the next chunk
-    if (w < words && s_found[threadIdx.x]) {
-      // word w is written by this thread only (chunks are disjoint); other
-      // blocks may read it concurrently, which only delays their hits
-      avail[w] &= ~s_found[threadIdx.x];
-      mark[w] |= s_found[threadIdx.x];
-    }
+    nfound += __popc(fnd);
+    __syncwarp();
   }
-  bq.flush(qout, qout_n, &s_base);
+}
+
+// Frontier queue from `fresh` (when a search returns to top-down after
+// bottom-up sweeps): one bitmap word per thread, block scan, one global
+// atomic per block.  All threads of the block call it.
+__device__ __forceinline__ void
+materialize_block(uint32_t blk, uint32_t nblk, uint32_t n, uint32_t const* fresh, uint32_t* q, uint32_t* qn, uint32_t* s_base)
+{
+  uint32_t const words = (n + 31) / 32;
+  for (uint32_t wbase = blk * R_THREADS; wbase < words; wbase += nblk * R_THREADS) {
+    uint32_t const w    = wbase + threadIdx.x;
+    uint32_t       word = w < words ? __ldcg(fresh + w) : 0u;
+    uint32_t       total;
+    uint32_t       off = block_exclusive_scan<uint32_t, R_THREADS>(static_cast<uint32_t>(__popc(word)), &total);
+    if (threadIdx.x == 0) *s_base = total ? atomicAdd(qn, total) : 0u;
+    __syncthreads();
+    uint32_t j = *s_base + off;
+    while (word) {
+      uint32_t const bb = __ffs(word) - 1;
+      word &= word - 1;
+      q[j++] = w * 32 + bb;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(R_THREADS)
+k_materialize(uint32_t n, uint32_t const* __restrict__ fresh, fio f, reach_state* st)
+{
+  if (!st->mat) return;
+  __shared__ uint32_t s_base;
+  // the queue being built is the next level's input; its length is
+  // already known (the sweep's count), slots come from mat_n
+  materialize_block(blockIdx.x, gridDim.x, n, fresh, const_cast<uint32_t*>(f.in()), &st->mat_n, &s_base);
+}
+
+// Bottom-up sweep as its own launch (profiled levels): every chunk once,
+// the discovery count into the output counter.
+__global__ void __launch_bounds__(R_THREADS)
+k_bottom_up(uint32_t n,
+            uint64_t const* __restrict__ head,
+            uint32_t const* __restrict__ adj,
+            uint32_t* __restrict__ avail,
+            uint32_t* __restrict__ mark,
+            uint32_t* __restrict__ fresh,
+            fio f,
+            gate g,
+            reach_state* st)
+{
+  if (g.closed()) return;
+  __shared__ bu_warp_smem sm[BU_WARPS];
+  uint32_t                nfound = 0;
+  uint64_t                nedge = 0, ncand = 0;
+  unsigned const          wid = threadIdx.x >> 5;
+  bu_sweep_warp(blockIdx.x * BU_WARPS + wid, gridDim.x * BU_WARPS, n, head, adj, avail, mark, fresh, sm[wid], nfound, nedge, ncand);
 #pragma unroll
-  for (int s = 16; s; s >>= 1) nedge += __shfl_down_sync(0xFFFFFFFFu, nedge, s);
-  if (lane == 0 && nedge) atomicAdd(&st->edges_bu, static_cast<unsigned long long>(nedge));
+  for (int s = 16; s; s >>= 1) {
+    nedge += __shfl_down_sync(0xFFFFFFFFu, nedge, s);
+    nfound += __shfl_down_sync(0xFFFFFFFFu, nfound, s);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (nedge) atomicAdd(&st->edges_bu, static_cast<unsigned long long>(nedge));
+    if (nfound) atomicAdd(f.out_n(), nfound);
+    if (ncand) atomicAdd(&st->cands_bu, static_cast<unsigned long long>(ncand));
+  }
+}
+
+// ---------------------------------------------------------------- persistent search
+// One whole reachability search (every level) in ONE cooperative launch.
+// Blocks meet at a grid barrier between the phases of a level; the barrier
+// waits at most GRID_SYNC_SPINS polls, after which it sets bar_err and every
+// block leaves (the host reports KSPN_ERR_TIMEOUT) -- a launch whose blocks
+// were not all resident could therefore never hang.
+constexpr unsigned GRID_SYNC_SPINS = 1u << 22;
+
+__device__ __forceinline__ bool
+grid_sync(reach_state* st)
+{
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t const g0 = ld_acquire(&st->bar_gen);
+    __threadfence();
+    if (atomicAdd(&st->bar_count, 1u) == gridDim.x - 1) {
+      atomicExch(&st->bar_count, 0u);
+      __threadfence();
+      atomicAdd(&st->bar_gen, 1u);
+    } else {
+      unsigned spins = 0;
+      while (ld_acquire(&st->bar_gen) == g0) {
+        if (++spins > GRID_SYNC_SPINS) {
+          atomicExch(&st->bar_err, 1u);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ld_acquire(&st->bar_err) == 0;
+}
+
+struct search_args
+{
+  uint32_t        n;
+  uint32_t        trace;  // stamp phases into stamp_phase / stamp_ns
+  uint32_t*       stamp_phase;
+  uint64_t*       stamp_ns;
+  uint64_t const* td_head;
+  uint32_t const* td_adj;
+  uint64_t const* bu_head;
+  uint32_t const* bu_adj;
+  uint32_t*       avail;
+  uint32_t*       mark;
+  uint32_t*       fresh;
+  uint32_t*       q0;
+  uint32_t*       q1;
+  uint64_t*       prefix;
+  uint32_t*       tile_start;
+  uint64_t*       partial;
+  reach_state*    st;
+};
+
+__device__ __forceinline__ void
+chunk_of(uint32_t qn, uint32_t& beg, uint32_t& end)
+{
+  uint32_t const chunk = (qn + gridDim.x - 1) / gridDim.x;
+  uint64_t const b     = static_cast<uint64_t>(blockIdx.x) * chunk;
+  beg                  = static_cast<uint32_t>(b < qn ? b : qn);
+  end                  = static_cast<uint32_t>(b + chunk < qn ? b + chunk : qn);
+}
+
+__device__ __forceinline__ uint64_t
+globaltimer()
+{
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// block 0, thread 0: record that `phase` ended now
+__device__ __forceinline__ void
+stamp(search_args const& a, uint32_t phase)
+{
+  if (!a.trace || blockIdx.x != 0 || threadIdx.x != 0) return;
+  uint32_t const i = a.st->marks;
+  if (i < MARKS) {
+    a.stamp_phase[i] = phase;
+    a.stamp_ns[i]    = globaltimer();
+    a.st->marks      = i + 1;
+  }
+}
+
+template<bool BW>
+__global__ void __launch_bounds__(R_THREADS)
+k_search(search_args a)
+{
+  __shared__ bu_warp_smem sm[BU_WARPS]; // bottom-up warp chunks; sm[0..] also holds a top-down tile's rows
+  __shared__ uint32_t     s_buf[BU_BUF];
+  __shared__ uint32_t     s_i[2], s_n, s_base;
+  static_assert(sizeof(sm) >= EX_TILE * sizeof(uint32_t), "tile rows must fit the warp buffers");
+  uint32_t* const tile_rows = reinterpret_cast<uint32_t*>(sm);
+  reach_state* const  st = a.st;
+  if (threadIdx.x == 0) s_n = 0;
+  __syncthreads();
+  block_queue    bq{ s_buf, &s_n };
+  uint64_t       nedge = 0, ncand = 0;
+  uint32_t       nfound = 0;
+  for (;;) {
+    // control values, written by block 0 before the last barrier
+    uint32_t const cur = __ldcg(&st->cur) & 1u;
+    uint32_t const qn  = __ldcg(&st->qn[cur]);
+    if (qn == 0 || __ldcg(&st->err)) break;
+    if (__ldcg(&st->mat)) {
+      // back to top-down: the frontier queue from the last sweep's bits
+      materialize_block(blockIdx.x, gridDim.x, a.n, a.fresh, cur ? a.q1 : a.q0, &st->mat_n, &s_base);
+      if (!grid_sync(st)) break;
+      stamp(a, 7);
+    }
+    uint32_t const* qin    = cur ? a.q1 : a.q0;
+    uint32_t* const qout   = cur ? a.q0 : a.q1;
+    uint32_t* const qout_n = &st->qn[cur ^ 1u];
+    if (__ldcg(&st->scan)) {
+      // degrees of the frontier (top-down direction): block partial sums
+      uint32_t beg, end;
+      chunk_of(qn, beg, end);
+      uint64_t sum = 0;
+      for (uint32_t i = beg + threadIdx.x; i < end; i += R_THREADS) {
+        uint32_t const v = __ldcg(qin + i);
+        sum += a.td_head[v + 1] - a.td_head[v];
+      }
+      uint64_t total;
+      block_exclusive_scan<uint64_t, R_THREADS>(sum, &total);
+      if (threadIdx.x == 0) a.partial[blockIdx.x] = total;
+      if (!grid_sync(st)) break;
+      stamp(a, 1);
+      // block 0: scan of the partial sums, totals, direction
+      if (blockIdx.x == 0) {
+        uint32_t const nb  = gridDim.x;
+        uint32_t const per = (nb + R_THREADS - 1) / R_THREADS;
+        uint32_t const b0  = threadIdx.x * per;
+        uint64_t       loc = 0;
+        for (uint32_t i = b0; i < b0 + per && i < nb; ++i) loc += __ldcg(a.partial + i);
+        uint64_t all;
+        uint64_t run = block_exclusive_scan<uint64_t, R_THREADS>(loc, &all);
+        for (uint32_t i = b0; i < b0 + per && i < nb; ++i) {
+          uint64_t const x = __ldcg(a.partial + i);
+          a.partial[i]     = run;
+          run += x;
+        }
+        if (threadIdx.x == 0) {
+          a.prefix[qn]    = all;
+          st->ntiles      = static_cast<uint32_t>((all + EX_TILE - 1) / EX_TILE);
+          st->m_f         = all;
+          uint32_t mode   = __ldcg(&st->mode);
+          if (mode == 0 && all * __ldcg(&st->alpha) > __ldcg(&st->m_u)) mode = 1;
+          else if (mode == 1) mode = 0; // the frontier fell below n_und / beta
+          st->mode = mode;
+          if (mode == 0) st->edges_td = __ldcg(&st->edges_td) + all;
+        }
+      }
+      if (!grid_sync(st)) break;
+      stamp(a, 2);
+      if (__ldcg(&st->mode) == 0) {
+        // frontier prefix and tile starts
+        uint64_t run = __ldcg(a.partial + blockIdx.x);
+        for (uint32_t base = beg; base < end; base += R_THREADS) {
+          uint32_t const i   = base + threadIdx.x;
+          uint64_t       deg = 0;
+          if (i < end) {
+            uint32_t const v = __ldcg(qin + i);
+            deg              = a.td_head[v + 1] - a.td_head[v];
+          }
+          uint64_t       tot;
+          uint64_t const p = run + block_exclusive_scan<uint64_t, R_THREADS>(deg, &tot);
+          if (i < end) {
+            a.prefix[i] = p;
+            if (deg) {
+              uint64_t const t0 = (p + EX_TILE - 1) / EX_TILE;
+              uint64_t const t1 = (p + deg - 1) / EX_TILE;
+              for (uint64_t t = t0; t <= t1; ++t) a.tile_start[t] = i;
+            }
+          }
+          run += tot;
+        }
+        if (!grid_sync(st)) break;
+        stamp(a, 3);
+      }
+    }
+    uint32_t const phase = __ldcg(&st->mode) == 0 ? 4u : 5u;
+    if (__ldcg(&st->mode) == 0) {
+      uint32_t const ntiles = __ldcg(&st->ntiles);
+      uint64_t const total  = __ldcg(a.prefix + qn);
+      take_op const  op{ a.avail, a.mark };
+      for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        expand_tile(tile, ntiles, qin, qn, total, a.prefix, a.tile_start, a.td_head, a.td_adj, tile_rows, s_i, bq, op);
+        bq.flush(qout, qout_n, &s_base);
+      }
+    } else {
+      unsigned const wid = threadIdx.x >> 5;
+      nfound             = 0;
+      bu_sweep_warp(blockIdx.x * BU_WARPS + wid, gridDim.x * BU_WARPS, a.n, a.bu_head, a.bu_adj, a.avail, a.mark, a.fresh, sm[wid], nfound, nedge, ncand);
+#pragma unroll
+      for (int sh = 16; sh; sh >>= 1) nfound += __shfl_down_sync(0xFFFFFFFFu, nfound, sh);
+      if ((threadIdx.x & 31) == 0 && nfound) atomicAdd(qout_n, nfound);
+    }
+    if (!grid_sync(st)) break;
+    stamp(a, phase);
+    if (blockIdx.x == 0 && threadIdx.x == 0) advance_body<BW>(st);
+    if (!grid_sync(st)) break;
+    stamp(a, 6);
+  }
+#pragma unroll
+  for (int sh = 16; sh; sh >>= 1) nedge += __shfl_down_sync(0xFFFFFFFFu, nedge, sh);
+  if ((threadIdx.x & 31) == 0 && nedge) atomicAdd(&st->edges_bu, static_cast<unsigned long long>(nedge));
   if (threadIdx.x == 0 && ncand) atomicAdd(&st->cands_bu, static_cast<unsigned long long>(ncand));
 }
 
@@ -386,33 +691,6 @@ k_fwbw_finalize(uint32_t n, uint32_t const* __restrict__ vis_b, uint32_t* __rest
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(&st->decided, c);
 }
 
-// ---------------------------------------------------------------- graph building
-// Adds kernel `fn` with arguments `vals` (converted to the kernel's
-// parameter types) to graph g after `dep`.
-template<typename... KArgs, typename... Vals>
-cudaGraphNode_t
-add_kernel(cudaGraph_t g, cudaGraphNode_t dep, void (*fn)(KArgs...), unsigned grid, unsigned block, Vals... vals)
-{
-  static_assert(sizeof...(KArgs) == sizeof...(Vals), "argument count");
-  std::tuple<std::decay_t<KArgs>...> held(static_cast<std::decay_t<KArgs>>(vals)...);
-  void*                              params[sizeof...(KArgs) ? sizeof...(KArgs) : 1];
-  std::apply(
-    [&](auto&... a) {
-      int i = 0;
-      ((params[i++] = static_cast<void*>(&a)), ...);
-    },
-    held);
-  cudaKernelNodeParams p = {};
-  p.func                 = reinterpret_cast<void*>(fn);
-  p.gridDim              = dim3(grid);
-  p.blockDim             = dim3(block);
-  p.sharedMemBytes       = 0;
-  p.kernelParams         = params;
-  cudaGraphNode_t node   = nullptr;
-  KSPN_CUDA(cudaGraphAddKernelNode(&node, g, dep ? &dep : nullptr, dep ? 1 : 0, &p));
-  return node;
-}
-
 struct search_io
 {
   uint64_t const* td_head;
@@ -421,33 +699,20 @@ struct search_io
   uint32_t const* bu_adj;
   uint32_t*       avail;
   uint32_t*       mark;
+  uint32_t*       fresh;
 };
 
-// The kernels of one level, in order: into graph g (a while-body) when g is
-// given, else launched on the stream with the expansion kernels bracketed
-// by the profiling events.
+// One level as separate launches (profiled searches): the same phase
+// bodies as k_search, with CUDA events around the two expansion kernels.
 template<bool BW>
 void
-level_body(kspn_context* ctx, cudaGraph_t g, dgraph const& gr, search_io const& io, reach_state* st, cudaGraphConditionalHandle h)
+level_body(kspn_context* ctx, dgraph const& gr, search_io const& io, reach_state* st)
 {
-  auto&     ws = ctx->ws;
-  fio const f{ ws.q0, ws.q1, &st->qn[0], &st->qn[1], &st->cur };
-  if (g) {
-    cudaGraphNode_t dep = nullptr;
-    gate const      sg{ &st->scan, 1 };
-    dep                 = add_kernel(g, dep, &k_r_prescan, 1, 1, st);
-    dep                 = add_kernel(g, dep, &k_fs_reduce, FS_BLOCKS, FS_THREADS, io.td_head, f, ws.blocks, sg);
-    dep                 = add_kernel(g, dep, &k_fs_partials, 1, 1024, ws.blocks, ws.prefix, f, &st->ntiles, static_cast<unsigned long long*>(nullptr), &st->m_f, sg);
-    dep                 = add_kernel(g, dep, &k_fs_down, FS_BLOCKS, FS_THREADS, io.td_head, f, ws.blocks, ws.prefix, ws.tile_start, sg);
-    dep                 = add_kernel(g, dep, &k_r_decide, 1, 1, st);
-    dep = add_kernel(g, dep, &k_expand<take_op>, EX_BLOCKS, EX_THREADS, io.td_head, io.td_adj, f, ws.prefix, ws.tile_start, &st->ntiles, gate{ &st->mode, 0 }, take_op{ io.avail, io.mark });
-    dep = add_kernel(g, dep, &k_bottom_up, bu_grid(gr.n), R_THREADS, gr.n, io.bu_head, io.bu_adj, io.avail, io.mark, f, gate{ &st->mode, 1 }, st);
-    add_kernel(g, dep, &k_r_advance<BW>, 1, 1, st, h, 1);
-    return;
-  }
+  auto&              ws = ctx->ws;
+  fio const          f{ ws.q0, ws.q1, &st->qn[0], &st->qn[1], &st->cur };
   cudaStream_t const s = ctx->stream;
   gate const         sg{ &st->scan, 1 };
-  k_r_prescan<<<1, 1, 0, s>>>(st);
+  k_materialize<<<r_grid((gr.n + 31) / 32), R_THREADS, 0, s>>>(gr.n, io.fresh, f, st);
   k_fs_reduce<<<FS_BLOCKS, FS_THREADS, 0, s>>>(io.td_head, f, ws.blocks, sg);
   k_fs_partials<<<1, 1024, 0, s>>>(ws.blocks, ws.prefix, f, &st->ntiles, nullptr, &st->m_f, sg);
   k_fs_down<<<FS_BLOCKS, FS_THREADS, 0, s>>>(io.td_head, f, ws.blocks, ws.prefix, ws.tile_start, sg);
@@ -456,9 +721,9 @@ level_body(kspn_context* ctx, cudaGraph_t g, dgraph const& gr, search_io const& 
   k_expand<take_op><<<EX_BLOCKS, EX_THREADS, 0, s>>>(io.td_head, io.td_adj, f, ws.prefix, ws.tile_start, &st->ntiles, gate{ &st->mode, 0 }, take_op{ io.avail, io.mark });
   prof_stop(ctx, 0);
   prof_start(ctx, 1);
-  k_bottom_up<<<bu_grid(gr.n), R_THREADS, 0, s>>>(gr.n, io.bu_head, io.bu_adj, io.avail, io.mark, f, gate{ &st->mode, 1 }, st);
+  k_bottom_up<<<bu_grid(gr.n), R_THREADS, 0, s>>>(gr.n, io.bu_head, io.bu_adj, io.avail, io.mark, io.fresh, f, gate{ &st->mode, 1 }, st);
   prof_stop(ctx, 1);
-  k_r_advance<BW><<<1, 1, 0, s>>>(st, h, 0);
+  k_r_advance<BW><<<1, 1, 0, s>>>(st);
   KSPN_CHECK_LAUNCH();
   ctx->launches += 8;
 }
@@ -466,55 +731,31 @@ level_body(kspn_context* ctx, cudaGraph_t g, dgraph const& gr, search_io const& 
 search_io
 fw_io(kspn_context* ctx, dgraph const& g)
 {
-  return { g.fh, g.fc, g.bh, g.bc, ctx->ws.mark, ctx->ws.vis_a };
+  return { g.fh, g.fc, g.bh, g.bc, ctx->ws.mark, ctx->ws.vis_a, ctx->ws.fresh };
 }
 search_io
 bw_io(kspn_context* ctx, dgraph const& g)
 {
-  return { g.bh, g.bc, g.fh, g.fc, ctx->ws.vis_a, ctx->ws.vis_b };
+  return { g.bh, g.bc, g.fh, g.fc, ctx->ws.vis_a, ctx->ws.vis_b, ctx->ws.fresh };
 }
 
-// Builds the one-launch FW-BW graph for (graph, und, scc_id).
+// Cooperative launch of one persistent search: as many blocks as fit on
+// the device at once (all co-resident, which the grid barrier needs).
+template<bool BW>
 void
-build_fwbw_graph(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id)
+launch_search(kspn_context* ctx, search_args const& a)
 {
-  auto&          ws    = ctx->ws;
-  auto*          st    = reinterpret_cast<reach_state*>(ws.rstate);
-  uint32_t const words = (g.n + 31) / 32;
-  cudaGraph_t    graph = nullptr;
-  KSPN_CUDA(cudaGraphCreate(&graph, 0));
-  try {
-    cudaGraphNode_t dep = nullptr;
-    dep = add_kernel(graph, dep, &k_r_init, r_grid(words), R_THREADS, words, und, ws.mark, ws.vis_a, ws.vis_b, st);
-    dep = add_kernel(graph, dep, &k_und_degrees, r_grid(g.n), R_THREADS, g.n, und, g.fh, g.bh, st);
-    for (int bw = 0; bw < 2; ++bw) {
-      search_io const io = bw ? bw_io(ctx, g) : fw_io(ctx, g);
-      dep = bw ? add_kernel(graph, dep, &k_r_seed<true>, 1, 1, io.avail, io.mark, ws.q0, st) : add_kernel(graph, dep, &k_r_seed<false>, 1, 1, io.avail, io.mark, ws.q0, st);
-      cudaGraphConditionalHandle h;
-      KSPN_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault));
-      cudaGraphNodeParams cp = {};
-      cp.type                = cudaGraphNodeTypeConditional;
-      cp.conditional.handle  = h;
-      cp.conditional.type    = cudaGraphCondTypeWhile;
-      cp.conditional.size    = 1;
-      cudaGraphNode_t loop   = nullptr;
-      KSPN_CUDA(cudaGraphAddNode(&loop, graph, &dep, 1, &cp));
-      cudaGraph_t body = cp.conditional.phGraph_out[0];
-      if (bw) level_body<true>(ctx, body, g, io, st, h);
-      else level_body<false>(ctx, body, g, io, st, h);
-      dep = loop;
-    }
-    dep = add_kernel(graph, dep, &k_r_setid, 1, 1, st);
-    dep = add_kernel(graph, dep, &k_bitmap_min, r_grid(words), R_THREADS, g.n, ws.vis_b, st);
-    add_kernel(graph, dep, &k_fwbw_finalize, r_grid(words), R_THREADS, g.n, ws.vis_b, und, scc_id, st);
-    cudaGraphExec_t exec = nullptr;
-    KSPN_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-    ctx->fwbw.graph = graph;
-    ctx->fwbw.exec  = exec;
-  } catch (...) {
-    cudaGraphDestroy(graph);
-    throw;
+  static int bps = 0, sms = 0;
+  if (!bps) {
+    KSPN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_search<BW>, R_THREADS, 0));
+    KSPN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    if (bps < 1) throw error{ KSPN_ERR_CUDA, "persistent search kernel does not fit on an SM" };
   }
+  unsigned const grid = static_cast<unsigned>(std::min(bps * sms, 4000));
+  search_args    arg  = a;
+  void*          args[] = { &arg };
+  KSPN_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(&k_search<BW>), dim3(grid), dim3(R_THREADS), args, 0, ctx->stream));
+  ctx->launches += 1;
 }
 
 } // namespace
@@ -528,9 +769,11 @@ reach_state_bytes()
 void
 release_graphs(kspn_context* ctx)
 {
-  if (ctx->fwbw.exec) cudaGraphExecDestroy(ctx->fwbw.exec);
-  if (ctx->fwbw.graph) cudaGraphDestroy(ctx->fwbw.graph);
-  ctx->fwbw = {};
+  for (cached_graph* c : { &ctx->fwbw, &ctx->trim }) {
+    if (c->exec) cudaGraphExecDestroy(c->exec);
+    if (c->graph) cudaGraphDestroy(c->graph);
+    *c = {};
+  }
 }
 
 uint32_t
@@ -549,22 +792,37 @@ fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint3
   hs->min_ids = min_ids ? 1u : 0u;
   KSPN_CUDA(cudaMemcpyAsync(rs, hs, sizeof(reach_state), cudaMemcpyHostToDevice, ctx->stream));
 
+  uint32_t const words = (g.n + 31) / 32;
   if (!ctx->prof) {
-    graph_key const key{ g.fh, g.fc, g.bh, g.bc, und, scc_id, ws.base, g.n, g.m };
-    if (!ctx->fwbw.exec || !(ctx->fwbw.key == key)) {
-      release_graphs(ctx);
-      build_fwbw_graph(ctx, g, und, scc_id);
-      ctx->fwbw.key = key;
+    // whole searches on the device: one cooperative launch per direction
+    k_r_init<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(words, g.m, und, ws.mark, ws.vis_a, ws.vis_b, rs);
+    ctx->launches += 1;
+    for (int bw = 0; bw < 2; ++bw) {
+      search_io const io = bw ? bw_io(ctx, g) : fw_io(ctx, g);
+      auto* stamp_phase = reinterpret_cast<uint32_t*>(static_cast<char*>(ws.rstate) + 2048);
+      auto* stamp_ns    = reinterpret_cast<uint64_t*>(static_cast<char*>(ws.rstate) + 2048 + 4 * MARKS);
+      bool const tr     = opt.trace && st && st->search_marks == 0;
+      search_args const a{ g.n, tr ? 1u : 0u, stamp_phase, stamp_ns, io.td_head, io.td_adj, io.bu_head, io.bu_adj, io.avail, io.mark, io.fresh, ws.q0, ws.q1, ws.prefix, ws.tile_start, ws.blocks, rs };
+      if (bw) {
+        k_r_seed<true><<<1, 1, 0, ctx->stream>>>(io.avail, io.mark, ws.q0, rs);
+        launch_search<true>(ctx, a);
+      } else {
+        k_r_seed<false><<<1, 1, 0, ctx->stream>>>(io.avail, io.mark, ws.q0, rs);
+        launch_search<false>(ctx, a);
+      }
+      ctx->launches += 1;
     }
-    KSPN_CUDA(cudaGraphLaunch(ctx->fwbw.exec, ctx->stream));
+    k_r_setid<<<1, 1, 0, ctx->stream>>>(rs);
+    k_bitmap_min<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(g.n, ws.vis_b, rs);
+    k_fwbw_finalize<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(g.n, ws.vis_b, und, scc_id, rs);
+    KSPN_CHECK_LAUNCH();
+    ctx->launches += 3;
   } else {
     // host-driven loop over the same kernels, expansion kernels bracketed
     // by CUDA events (kspn_options.profile)
-    bool const     trace_done = st && st->levels_fw != 0; // trace the first FW-BW only
-    uint32_t const words      = (g.n + 31) / 32;
-    k_r_init<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(words, und, ws.mark, ws.vis_a, ws.vis_b, rs);
-    k_und_degrees<<<r_grid(g.n), R_THREADS, 0, ctx->stream>>>(g.n, und, g.fh, g.bh, rs);
-    ctx->launches += 2;
+    bool const trace_done = st && st->levels_fw != 0; // trace the first FW-BW only
+    k_r_init<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(words, g.m, und, ws.mark, ws.vis_a, ws.vis_b, rs);
+    ctx->launches += 1;
     for (int bw = 0; bw < 2; ++bw) {
       search_io const io = bw ? bw_io(ctx, g) : fw_io(ctx, g);
       if (bw) k_r_seed<true><<<1, 1, 0, ctx->stream>>>(io.avail, io.mark, ws.q0, rs);
@@ -580,8 +838,8 @@ fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint3
           hs->err = 1;
           break;
         }
-        if (bw) level_body<true>(ctx, nullptr, g, io, rs, cudaGraphConditionalHandle{});
-        else level_body<false>(ctx, nullptr, g, io, rs, cudaGraphConditionalHandle{});
+        if (bw) level_body<true>(ctx, g, io, rs);
+        else level_body<false>(ctx, g, io, rs);
         KSPN_CUDA(cudaMemcpyAsync(hs, rs, sizeof(reach_state), cudaMemcpyDeviceToHost, ctx->stream));
         KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
         uint32_t const qn1 = hs->qn[hs->cur & 1u];
@@ -615,8 +873,14 @@ fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint3
   KSPN_CUDA(cudaMemcpyAsync(hs, rs, sizeof(reach_state), cudaMemcpyDeviceToHost, ctx->stream));
   KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
   if (hs->err) throw error{ KSPN_ERR_TIMEOUT, "reachability: level cap exceeded" };
-  // kernels the graph ran: init, degrees, 2 seeds, 8 per level, 3 to finish
-  if (!ctx->prof) ctx->launches += 7 + 8ull * (hs->levels_fw + hs->levels_bw);
+  if (hs->bar_err) throw error{ KSPN_ERR_TIMEOUT, "reachability: grid barrier wait limit reached" };
+  if (opt.trace && st && st->search_marks == 0 && hs->marks) {
+    uint32_t const k = std::min<uint32_t>(hs->marks, MARKS);
+    KSPN_CUDA(cudaMemcpyAsync(st->search_phase, static_cast<char*>(ws.rstate) + 2048, 4 * k, cudaMemcpyDeviceToHost, ctx->stream));
+    KSPN_CUDA(cudaMemcpyAsync(st->search_ns, static_cast<char*>(ws.rstate) + 2048 + 4 * MARKS, 8 * k, cudaMemcpyDeviceToHost, ctx->stream));
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+    st->search_marks = k;
+  }
   ctx->td_edges += hs->edges_td + hs->edges_bu;
   if (st && st->levels_fw == 0 && st->levels_bw == 0) {
     st->levels_fw        = hs->levels_fw;

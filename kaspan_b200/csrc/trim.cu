@@ -14,7 +14,10 @@
 //
 // Work per launch is one thread per vertex (streaming passes) or one thread
 // per queued vertex with rows of 32+ entries taken by the whole warp.
-#include "kspn_internal.cuh"
+#include "expand.cuh"
+
+#include <cstring>
+#include <tuple>
 
 namespace kspn {
 
@@ -420,6 +423,267 @@ k_popcount(uint32_t words, uint32_t n, uint32_t const* __restrict__ bm, uint32_t
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
 }
 
+// ---------------------------------------------------------------- device-driven trim fixpoint
+// Control block of one trim fixpoint (workspace, after the FW-BW block).
+struct trim_state
+{
+  uint32_t           cur;    // queue selector (fio)
+  uint32_t           qn[2];  // queue lengths
+  uint32_t           level;  // push levels run
+  uint32_t           cap;    // level cap
+  uint32_t           err;    // 1: cap hit
+  uint32_t           decided;
+  uint32_t           list_n; // undecided vertices at the start
+  unsigned long long edges;  // edges pushed along
+};
+
+__global__ void
+k_t_init(trim_state* st)
+{
+  uint32_t const cap = st->cap;
+  st->cur = st->qn[0] = st->qn[1] = st->level = st->err = st->decided = st->list_n = 0;
+  st->edges = 0;
+  st->cap   = cap;
+}
+
+// Undecided vertex ids -> list (one bitmap word per thread, block scan of
+// popcounts, one global atomic per block).
+__global__ void __launch_bounds__(T_THREADS)
+k_t_compact(uint32_t n, uint32_t const* __restrict__ und, uint32_t* __restrict__ list, trim_state* st)
+{
+  __shared__ uint32_t s_base;
+  uint32_t const      words = (n + 31) / 32;
+  for (uint32_t wbase = blockIdx.x * T_THREADS; wbase < words; wbase += gridDim.x * T_THREADS) {
+    uint32_t const w    = wbase + threadIdx.x;
+    uint32_t       word = w < words ? und[w] : 0u;
+    if (w == words - 1 && (n & 31)) word &= (1u << (n & 31)) - 1u;
+    uint32_t total;
+    uint32_t off = block_exclusive_scan<uint32_t, T_THREADS>(static_cast<uint32_t>(__popc(word)), &total);
+    if (threadIdx.x == 0) s_base = total ? atomicAdd(&st->list_n, total) : 0;
+    __syncthreads();
+    uint32_t j = s_base + off;
+    while (word) {
+      uint32_t const b = __ffs(word) - 1;
+      word &= word - 1;
+      list[j++] = w * 32 + b;
+    }
+    __syncthreads();
+  }
+}
+
+// Live degrees of the listed (undecided) vertices; rows of WARP_BIG+ by
+// the whole warp.
+__global__ void __launch_bounds__(T_THREADS)
+k_t_live(uint64_t const* __restrict__ fh, uint32_t const* __restrict__ fc, uint64_t const* __restrict__ bh, uint32_t const* __restrict__ bc, uint32_t const* __restrict__ und, uint32_t const* __restrict__ list,
+         trim_state const* st, uint32_t* __restrict__ indeg, uint32_t* __restrict__ outdeg)
+{
+  unsigned const lane = threadIdx.x & 31u;
+  uint32_t const ln   = st->list_n;
+  uint64_t const span = (static_cast<uint64_t>(ln) + 31) & ~31ull;
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+    bool const     have = t < ln;
+    uint32_t const v    = have ? list[t] : 0u;
+    uint64_t       fb = 0, fe = 0, bb = 0, be = 0;
+    if (have) fb = fh[v], fe = fh[v + 1], bb = bh[v], be = bh[v + 1];
+    uint32_t   outc  = 0, inc = 0;
+    bool const small = have && (fe - fb) < WARP_BIG && (be - bb) < WARP_BIG;
+    if (small) {
+      for (uint64_t e = fb; e < fe; ++e) outc += bit_get(und, fc[e]);
+      for (uint64_t e = bb; e < be; ++e) inc += bit_get(und, bc[e]);
+    }
+    unsigned todo = __ballot_sync(0xFFFFFFFFu, have && !small);
+    while (todo) {
+      unsigned const l = __ffs(todo) - 1;
+      todo &= todo - 1;
+      uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, fb, l), e0 = __shfl_sync(0xFFFFFFFFu, fe, l);
+      uint64_t const b1 = __shfl_sync(0xFFFFFFFFu, bb, l), e1 = __shfl_sync(0xFFFFFFFFu, be, l);
+      uint32_t       a = 0, c = 0;
+      for (uint64_t e = b0 + lane; e < e0; e += 32) a += bit_get(und, fc[e]);
+      for (uint64_t e = b1 + lane; e < e1; e += 32) c += bit_get(und, bc[e]);
+#pragma unroll
+      for (int s = 16; s; s >>= 1) a += __shfl_xor_sync(0xFFFFFFFFu, a, s), c += __shfl_xor_sync(0xFFFFFFFFu, c, s);
+      if (lane == l) outc = a, inc = c;
+    }
+    if (have) {
+      indeg[v]  = inc;
+      outdeg[v] = outc;
+    }
+  }
+}
+
+// Listed vertices with a live degree of 0 are decided and queued (q0).
+__global__ void __launch_bounds__(T_THREADS)
+k_t_seed(uint32_t* __restrict__ und, uint32_t* __restrict__ scc_id, uint32_t const* __restrict__ indeg, uint32_t const* __restrict__ outdeg, uint32_t const* __restrict__ list, trim_state* st, uint32_t* __restrict__ q0)
+{
+  __shared__ uint32_t s_buf[DENSE_BUF];
+  __shared__ uint32_t s_n, s_base;
+  if (threadIdx.x == 0) s_n = 0;
+  __syncthreads();
+  block_queue    bq{ s_buf, &s_n };
+  uint32_t const ln   = st->list_n;
+  uint64_t const span = (static_cast<uint64_t>(ln) + T_THREADS - 1) / T_THREADS * T_THREADS;
+  uint32_t       dec  = 0;
+  for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * T_THREADS; base < span; base += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+    uint64_t const t    = base + threadIdx.x;
+    uint32_t const v    = t < ln ? list[t] : 0u;
+    bool const     dead = t < ln && (indeg[v] == 0 || outdeg[v] == 0);
+    bool const     won  = dead && bit_take(und, v);
+    if (won) {
+      scc_id[v] = v;
+      ++dec;
+    }
+    bq.push(won, v);
+    __syncthreads();
+    if (s_n > DENSE_BUF - T_THREADS) bq.flush(q0, &st->qn[0], &s_base);
+  }
+  bq.flush(q0, &st->qn[0], &s_base);
+  if (dec) atomicAdd(&st->decided, dec);
+}
+
+// One push level (both directions) from the fio input queue to its output.
+__global__ void __launch_bounds__(T_THREADS)
+k_t_push(uint64_t const* __restrict__ fh,
+         uint32_t const* __restrict__ fc,
+         uint64_t const* __restrict__ bh,
+         uint32_t const* __restrict__ bc,
+         uint32_t* __restrict__ und,
+         uint32_t* __restrict__ scc_id,
+         uint32_t* __restrict__ indeg,
+         uint32_t* __restrict__ outdeg,
+         fio f,
+         trim_state* st)
+{
+  unsigned const  lane   = threadIdx.x & 31u;
+  uint32_t const* qin    = f.in();
+  uint32_t const  qn     = f.in_n();
+  uint32_t* const qout   = f.out();
+  uint32_t* const qout_n = f.out_n();
+  uint64_t const  span   = (static_cast<uint64_t>(qn) + 31) & ~31ull;
+  uint32_t        dec    = 0;
+  uint64_t        ne     = 0;
+  auto const      hit    = [&](uint32_t w, uint32_t* deg) {
+    if (bit_get(und, w) && atomicSub(deg + w, 1u) == 1u && bit_take(und, w)) {
+      scc_id[w] = w;
+      ++dec;
+      warp_push_active(w, qout, qout_n);
+    }
+  };
+#pragma unroll
+  for (int dir = 0; dir < 2; ++dir) {
+    uint64_t const* head = dir == 0 ? fh : bh;
+    uint32_t const* adj  = dir == 0 ? fc : bc;
+    uint32_t*       deg  = dir == 0 ? indeg : outdeg;
+    for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
+      bool const     have = t < qn;
+      uint32_t const u    = have ? qin[t] : 0;
+      uint64_t       b = 0, e = 0;
+      if (have) b = head[u], e = head[u + 1];
+      bool const big = have && (e - b) >= WARP_BIG;
+      ne += e - b;
+      if (have && !big)
+        for (uint64_t x = b; x < e; ++x) hit(adj[x], deg);
+      unsigned todo = __ballot_sync(0xFFFFFFFFu, big);
+      while (todo) {
+        unsigned const l = __ffs(todo) - 1;
+        todo &= todo - 1;
+        uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b, l), e0 = __shfl_sync(0xFFFFFFFFu, e, l);
+        for (uint64_t x = b0 + lane; x < e0; x += 32) hit(adj[x], deg);
+      }
+    }
+  }
+  if (dec) atomicAdd(&st->decided, dec);
+#pragma unroll
+  for (int sh = 16; sh; sh >>= 1) ne += __shfl_down_sync(0xFFFFFFFFu, ne, sh);
+  if (lane == 0 && ne) atomicAdd(&st->edges, static_cast<unsigned long long>(ne));
+}
+
+__global__ void
+k_t_advance(trim_state* st, cudaGraphConditionalHandle h, int in_graph)
+{
+  st->level += 1;
+  st->cur ^= 1u;
+  st->qn[(st->cur & 1u) ^ 1u] = 0; // next level's output
+  unsigned cond = st->qn[st->cur & 1u] > 0;
+  if (cond && st->level >= st->cap) {
+    st->err = 1;
+    cond    = 0;
+  }
+  if (in_graph) cudaGraphSetConditional(h, cond);
+}
+
+template<typename... KArgs, typename... Vals>
+cudaGraphNode_t
+t_add_kernel(cudaGraph_t g, cudaGraphNode_t dep, void (*fn)(KArgs...), unsigned grid, unsigned block, Vals... vals)
+{
+  static_assert(sizeof...(KArgs) == sizeof...(Vals), "argument count");
+  std::tuple<std::decay_t<KArgs>...> held(static_cast<std::decay_t<KArgs>>(vals)...);
+  void*                              params[sizeof...(KArgs) ? sizeof...(KArgs) : 1];
+  std::apply(
+    [&](auto&... a) {
+      int i = 0;
+      ((params[i++] = static_cast<void*>(&a)), ...);
+    },
+    held);
+  cudaKernelNodeParams p = {};
+  p.func                 = reinterpret_cast<void*>(fn);
+  p.gridDim              = dim3(grid);
+  p.blockDim             = dim3(block);
+  p.kernelParams         = params;
+  cudaGraphNode_t node   = nullptr;
+  KSPN_CUDA(cudaGraphAddKernelNode(&node, g, dep ? &dep : nullptr, dep ? 1 : 0, &p));
+  return node;
+}
+
+trim_state*
+trim_state_dev(kspn_context* ctx)
+{
+  return reinterpret_cast<trim_state*>(static_cast<char*>(ctx->ws.rstate) + 512);
+}
+trim_state*
+trim_state_host(kspn_context* ctx)
+{
+  return reinterpret_cast<trim_state*>(static_cast<char*>(ctx->h_state) + 512);
+}
+
+void
+build_trim_graph(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id)
+{
+  auto&          ws    = ctx->ws;
+  trim_state*    st    = trim_state_dev(ctx);
+  uint32_t const words = (g.n + 31) / 32;
+  cudaGraph_t    graph = nullptr;
+  KSPN_CUDA(cudaGraphCreate(&graph, 0));
+  try {
+    unsigned const  wgrid = stream_grid(words);
+    unsigned const  vgrid = stream_grid(g.n);
+    cudaGraphNode_t dep   = nullptr;
+    dep = t_add_kernel(graph, dep, &k_t_init, 1, 1, st);
+    dep = t_add_kernel(graph, dep, &k_t_compact, wgrid, T_THREADS, g.n, und, ws.q1, st);
+    dep = t_add_kernel(graph, dep, &k_t_live, vgrid, T_THREADS, g.fh, g.fc, g.bh, g.bc, und, ws.q1, st, ws.indeg, ws.outdeg);
+    dep = t_add_kernel(graph, dep, &k_t_seed, vgrid, T_THREADS, und, scc_id, ws.indeg, ws.outdeg, ws.q1, st, ws.q0);
+    cudaGraphConditionalHandle h;
+    KSPN_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type                = cudaGraphNodeTypeConditional;
+    cp.conditional.handle  = h;
+    cp.conditional.type    = cudaGraphCondTypeWhile;
+    cp.conditional.size    = 1;
+    cudaGraphNode_t loop   = nullptr;
+    KSPN_CUDA(cudaGraphAddNode(&loop, graph, &dep, 1, &cp));
+    cudaGraph_t     body = cp.conditional.phGraph_out[0];
+    fio const       f{ ws.q0, ws.q1, &st->qn[0], &st->qn[1], &st->cur };
+    cudaGraphNode_t bdep = t_add_kernel(body, nullptr, &k_t_push, vgrid, T_THREADS, g.fh, g.fc, g.bh, g.bc, und, scc_id, ws.indeg, ws.outdeg, f, st);
+    t_add_kernel(body, bdep, &k_t_advance, 1, 1, st, h, 1);
+    cudaGraphExec_t exec = nullptr;
+    KSPN_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    ctx->trim.graph = graph;
+    ctx->trim.exec  = exec;
+  } catch (...) {
+    cudaGraphDestroy(graph);
+    throw;
+  }
+}
+
 uint32_t
 pv_result(kspn_context* ctx, unsigned nb, uint64_t* min_prod_out)
 {
@@ -522,6 +786,28 @@ trim_fixpoint(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_i
 {
   auto&    ws    = ctx->ws;
   uint32_t total = 0, qn = seed_count;
+  if (!degrees_from_first && !ctx->prof) {
+    // one graph launch: compact the undecided set, live degrees, seeds, and
+    // a device-driven loop of push levels
+    trim_state* hs = trim_state_host(ctx);
+    std::memset(hs, 0, sizeof(trim_state));
+    hs->cap = g.n + 2;
+    KSPN_CUDA(cudaMemcpyAsync(trim_state_dev(ctx), hs, sizeof(trim_state), cudaMemcpyHostToDevice, ctx->stream));
+    graph_key const key{ g.fh, g.fc, g.bh, g.bc, und, scc_id, ws.base, g.n, g.m };
+    if (!ctx->trim.exec || !(ctx->trim.key == key)) {
+      if (ctx->trim.exec) cudaGraphExecDestroy(ctx->trim.exec);
+      if (ctx->trim.graph) cudaGraphDestroy(ctx->trim.graph);
+      ctx->trim = {};
+      build_trim_graph(ctx, g, und, scc_id);
+      ctx->trim.key = key;
+    }
+    KSPN_CUDA(cudaGraphLaunch(ctx->trim.exec, ctx->stream));
+    KSPN_CUDA(cudaMemcpyAsync(hs, trim_state_dev(ctx), sizeof(trim_state), cudaMemcpyDeviceToHost, ctx->stream));
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (hs->err) throw error{ KSPN_ERR_TIMEOUT, "trim: level cap exceeded" };
+    ctx->launches += 4 + 2ull * hs->level;
+    return hs->decided;
+  }
   if (!degrees_from_first) {
     zero_counters(ctx);
     k_live_degrees<<<stream_grid(g.n), T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.fc, g.bh, g.bc, und, ws.indeg, ws.outdeg);
