@@ -114,10 +114,11 @@ typedef struct kspn_stats
     float    ms;             /* event time of the level's expansion kernel */
     uint32_t pad;
   } trace[32];
-  /* kspn_options.trace: %globaltimer stamps (ns, from the launch) taken by
-   * block 0 of the first FW-BW's persistent searches after each phase, and
-   * the phase that ended there: 1 scan partials, 2 scan totals, 3 prefix,
-   * 4 expansion (top-down), 5 sweep (bottom-up), 6 level end. */
+  /* kspn_options.trace: %globaltimer stamps (ns) taken by block 0 of the
+   * first FW-BW's persistent launch after each phase, and the phase that
+   * ended there: 0 launch start, 8 init, 4 expansion level (top-down),
+   * 5 sweep level (bottom-up), 7 frontier built from a sweep's bitmap,
+   * 9 finalize. */
   uint32_t search_marks;
   uint32_t search_phase[128];
   uint64_t search_ns[128];

@@ -65,9 +65,15 @@ layout(workspace& ws, char* base, uint32_t n, uint64_t m)
   ws.indeg             = c.take<uint32_t>(nn);
   ws.outdeg            = c.take<uint32_t>(nn);
   ws.prefix            = c.take<uint64_t>(nn);
+  ws.prefix2           = c.take<uint64_t>(nn);
   ws.blocks            = c.take<uint64_t>(std::max<size_t>(scan_partial_entries(nn), 4096));
   ws.pivot             = c.take<uint64_t>(8192);
   ws.tile_start        = c.take<uint32_t>(m / 2048 + 4);
+  ws.tile_start2       = c.take<uint32_t>(m / 2048 + 4);
+  ws.tile_zero         = c.take<uint32_t>(m / 2048 + 4);
+  ws.seed_q            = c.take<uint32_t>(4);
+  ws.seed_prefix       = c.take<uint64_t>(4);
+  ws.gbar              = c.take<char>(4096);
   ws.rstate            = c.take<char>(4096);
   return align_up(c.off);
 }
@@ -100,6 +106,8 @@ ensure_workspace(kspn_context* ctx, uint32_t n, uint64_t m)
   ws.m_cap = mcap;
   layout(ws, static_cast<char*>(p), ncap, mcap);
   KSPN_CUDA(cudaMemsetAsync(ws.ctr, 0, 64 * sizeof(uint32_t), ctx->stream));
+  KSPN_CUDA(cudaMemsetAsync(ws.tile_zero, 0, (mcap / 2048 + 4) * sizeof(uint32_t), ctx->stream));
+  KSPN_CUDA(cudaMemsetAsync(ws.gbar, 0, 4096, ctx->stream));
 }
 
 void*

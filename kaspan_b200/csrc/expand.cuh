@@ -13,7 +13,8 @@
 //      slot its row, so hub rows are split across blocks and low-degree rows
 //      are packed densely; neighbour ids are read coalesced.
 // The per-edge operation is a functor called by every lane of the warp
-// (with valid == false for padding lanes) so it may use warp-wide pushes.
+// (with valid == false for padding lanes) so it may use warp-wide pushes;
+// its probe(v) (one state word) is loaded for a batch of slots ahead.
 #pragma once
 
 #include "prim.cuh"
@@ -163,14 +164,20 @@ tile_max_scan(uint32_t* s)
 }
 
 // Expands tile `tile` of a scanned queue (ntiles tiles, total edges):
-// calls op(u, v, valid) on every edge slot and appends the winners to bq.
-// All threads of the block call it.  Queue, prefix and tile starts are read
-// through L2 (ld.cg): inside a persistent launch other blocks wrote them.
+// calls op on every edge slot of items [k_begin, k_end) (slot = item *
+// EX_THREADS + thread) and appends the winners to bq.  All threads of the
+// block call it.  Queue, prefix and tile starts are read through L2 (ld.cg):
+// inside a persistent launch other blocks wrote them.
 // s_j: EX_TILE words of shared memory; s_i: two words.
+// Slots are processed EX_BATCH at a time, each stage's loads for all of
+// them issued before any is used: row lookup, neighbour id, the op's state
+// probe (op.probe(v)), then op(u, v, valid, probed_word).
+constexpr int EX_BATCH = 4;
+
 template<typename Op>
 __device__ __forceinline__ void
 expand_tile(uint32_t tile, uint32_t ntiles, uint32_t const* q, uint32_t qn, uint64_t total, uint64_t const* prefix, uint32_t const* tile_start, uint64_t const* __restrict__ head,
-            uint32_t const* __restrict__ adj, uint32_t* s_j, uint32_t* s_i, block_queue& bq, Op const& op)
+            uint32_t const* __restrict__ adj, uint32_t* s_j, uint32_t* s_i, block_queue& bq, Op const& op, int k_begin = 0, int k_end = EX_ITEMS)
 {
   uint64_t const t0 = static_cast<uint64_t>(tile) * EX_TILE;
   uint64_t const t1 = t0 + EX_TILE < total ? t0 + EX_TILE : total;
@@ -188,24 +195,47 @@ expand_tile(uint32_t tile, uint32_t ntiles, uint32_t const* q, uint32_t qn, uint
   }
   __syncthreads();
   tile_max_scan(s_j);
-#pragma unroll 4
-  for (int k = 0; k < EX_ITEMS; ++k) {
-    uint32_t const slot  = k * EX_THREADS + threadIdx.x;
-    uint64_t const e     = t0 + slot;
-    bool const     valid = e < t1;
-    uint32_t       u = 0, v = 0;
-    if (valid) {
-      uint32_t const j = i0 + s_j[slot];
-      u                = __ldcg(q + j);
-      v                = adj[head[u] + (e - __ldcg(prefix + j))];
+  for (int k0 = k_begin; k0 < k_end; k0 += EX_BATCH) {
+    uint32_t u[EX_BATCH], v[EX_BATCH], w[EX_BATCH];
+    uint64_t idx[EX_BATCH];
+    bool     ok[EX_BATCH];
+#pragma unroll
+    for (int h = 0; h < EX_BATCH; ++h) {
+      uint32_t const slot = (k0 + h) * EX_THREADS + threadIdx.x;
+      uint64_t const e    = t0 + slot;
+      ok[h]               = k0 + h < k_end && e < t1;
+      u[h]                = 0;
+      idx[h]              = 0;
+      if (ok[h]) {
+        uint32_t const j  = i0 + s_j[slot];
+        u[h]              = __ldcg(q + j);
+        uint64_t const pj = __ldcg(prefix + j);
+        ok[h]             = e >= pj;
+        idx[h]            = e - pj; // offset in u's row
+      }
     }
-    bq.push(op(u, v, valid), v);
+#pragma unroll
+    for (int h = 0; h < EX_BATCH; ++h)
+      if (ok[h]) {
+        // the slot's edge lies in u's row by construction of prefix and
+        // tile_start; a slot that does not is skipped, never read
+        uint64_t const b = head[u[h]];
+        ok[h]            = idx[h] < head[u[h] + 1] - b;
+        idx[h] += b;
+      }
+#pragma unroll
+    for (int h = 0; h < EX_BATCH; ++h) v[h] = ok[h] ? adj[idx[h]] : 0u;
+#pragma unroll
+    for (int h = 0; h < EX_BATCH; ++h) w[h] = ok[h] ? op.probe(v[h]) : 0u;
+#pragma unroll
+    for (int h = 0; h < EX_BATCH; ++h) bq.push(op(u[h], v[h], ok[h], w[h]), v[h]);
   }
 }
 
-// op(u, v, valid) -> bool: u = source (queued vertex), v = neighbour; true
-// appends v to the output queue.  Called by every lane (valid == false on
-// padding lanes).
+// op(u, v, valid, word) -> bool: u = source (queued vertex), v = neighbour,
+// word = op.probe(v) (the op's state word of v, loaded ahead); true appends
+// v to the output queue.  Called by every lane (valid == false on padding
+// lanes).
 template<typename Op>
 __global__ void __launch_bounds__(EX_THREADS)
 k_expand(uint64_t const* __restrict__ head,

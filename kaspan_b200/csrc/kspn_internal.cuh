@@ -201,12 +201,18 @@ struct workspace
   uint32_t* indeg    = nullptr; // n
   uint32_t* outdeg   = nullptr; // n
   uint64_t* prefix   = nullptr; // n+1 (u64 scan output)
+  uint64_t* prefix2  = nullptr; // n+1 (second frontier of the persistent FW-BW)
   uint64_t* blocks   = nullptr; // scan partials
   uint32_t* ctr      = nullptr; // CTR_COUNT
   uint64_t* ctr64    = nullptr; // 8 (64-bit counters)
   uint64_t* pivot    = nullptr; // per-block pivot keys (4096 u64 products + 4096 u32 ids)
-  uint32_t* tile_start = nullptr; // m / 2048 + 2 (frontier expansion)
-  void*     rstate     = nullptr; // 4 KiB device control blocks (FW-BW at 0, trim at 512, search stamps at 2048)
+  uint32_t* tile_start  = nullptr; // m / 2048 + 4 (frontier expansion)
+  uint32_t* tile_start2 = nullptr; // m / 2048 + 4 (second frontier of the persistent FW-BW)
+  uint32_t* tile_zero   = nullptr; // m / 2048 + 4 zeros: tile starts of a one-vertex frontier
+  uint32_t* seed_q      = nullptr; // 4: the pivot as a one-vertex frontier
+  uint64_t* seed_prefix = nullptr; // 4
+  void*     gbar        = nullptr; // 4 KiB grid barrier of the persistent FW-BW (zeroed at creation)
+  void*     rstate      = nullptr; // 4 KiB device control blocks (FW-BW at 0, trim at 512, search stamps at 2048)
   // owned graph storage (host inputs, or a CSC built on device)
   uint64_t* g_fh = nullptr;
   uint32_t* g_fc = nullptr;
@@ -281,7 +287,7 @@ struct kspn_context
   kspn_stats*        prof       = nullptr;
   cudaEvent_t        pe[4]      = {};
   void*              h_state    = nullptr; // pinned 4 KiB mirror of ws.rstate
-  kspn::cached_graph fwbw;                 // one-launch FW-BW graph
+  unsigned           search_grid = 0;      // blocks of the persistent FW-BW launch
   kspn::cached_graph trim;                 // one-launch trim fixpoint graph
   kspn::dev_buffer   bufs[kspn::BUF_COUNT];
 };

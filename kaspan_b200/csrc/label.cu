@@ -56,9 +56,10 @@ struct label_fw_op
   uint32_t const* und;
   uint32_t*       label;
   uint32_t*       claim_next;
-  __device__ __forceinline__ bool operator()(uint32_t u, uint32_t v, bool valid) const
+  __device__ __forceinline__ uint32_t probe(uint32_t v) const { return und[v >> 5]; }
+  __device__ __forceinline__ bool     operator()(uint32_t u, uint32_t v, bool valid, uint32_t word) const
   {
-    if (!valid || !bit_get(und, v)) return false;
+    if (!valid || !((word >> (v & 31)) & 1u)) return false;
     uint32_t const lu = __ldcg(label + u);
     if (lu >= __ldcg(label + v)) return false;
     uint32_t const old = atomicMin(label + v, lu);
@@ -113,9 +114,10 @@ struct label_bw_op
   uint32_t*       scc_id;
   int             rot;
   // u = decided vertex, v = one of its in-neighbours; every push is a decision
-  __device__ __forceinline__ bool operator()(uint32_t u, uint32_t v, bool valid) const
+  __device__ __forceinline__ uint32_t probe(uint32_t v) const { return und[v >> 5]; }
+  __device__ __forceinline__ bool     operator()(uint32_t u, uint32_t v, bool valid, uint32_t word) const
   {
-    if (!valid || !bit_get(und, v)) return false;
+    if (!valid || !((word >> (v & 31)) & 1u)) return false;
     uint32_t const lu = label[u];
     if (label[v] != lu || !bit_take(und, v)) return false;
     scc_id[v] = rotl32(lu, rot);

@@ -24,13 +24,12 @@
 // Each edge costs at most one probe and each discovery two atomics; the
 // undecided set and ids are written once at the end, a word at a time.
 //
-// Level control lives on the device (reach_state).  Each search is ONE
-// persistent cooperative launch (k_search) whose blocks run every level:
-// frontier scan, direction choice, top-down tiles or bottom-up chunks, and
-// the queue flip, separated by a bounded grid barrier.  With profiling on,
-// the same phase bodies run as separate launches from a host loop
-// (decide / expand / bottom-up / advance kernels) with CUDA events around
-// the expansion kernels.
+// Production runs the whole FW-BW as ONE persistent cooperative launch
+// (k_fwbw, below) with one grid barrier per level.  With profiling on (or a
+// graph too large for the packed level counters) the same phase bodies run
+// as separate launches from a host loop (decide / expand / bottom-up /
+// advance kernels, control in reach_state) with CUDA events around the
+// expansion kernels.
 #include "expand.cuh"
 
 #include <algorithm>
@@ -83,8 +82,10 @@ struct reach_state
   uint32_t           levels_fw, bu_fw, levels_bw, bu_bw;
   unsigned long long m_u, m_out, m_in, m_f, alpha, beta;
   unsigned long long edges_td, edges_bu, cands_bu;
-  uint32_t           bar_count, bar_gen, bar_err; // grid barrier of the persistent search
-  uint32_t           marks;                       // phase stamps taken (kspn_options.trace)
+  uint32_t           bar_err; // 1: the persistent launch's grid barrier gave up
+  uint32_t           marks;   // phase stamps taken (kspn_options.trace)
+  unsigned long long lq[3];   // persistent launch: packed level counters (edges << qbits | vertices)
+  unsigned long long mat_q;   // persistent launch: counter of a frontier built from `fresh`
 };
 
 // phase stamps live after the state: uint32 phase[128], uint64 ns[128]
@@ -114,7 +115,7 @@ k_r_init(uint32_t words, uint64_t m, uint32_t const* __restrict__ und, uint32_t*
     st->err                                    = 0;
     st->decided                                = 0;
     st->levels_fw = st->bu_fw = st->levels_bw = st->bu_bw = 0;
-    st->bar_count = st->bar_gen = st->bar_err = 0;
+    st->bar_err                               = 0;
     st->marks                                 = 0;
   }
 }
@@ -201,13 +202,15 @@ k_r_advance(reach_state* st)
 }
 
 // top-down, both directions: v joins when its bit in `avail` is taken
+// (`word` = avail's word of v, probed ahead through L2)
 struct take_op
 {
   uint32_t* avail; // FW: cand; BW: vis_a
   uint32_t* mark;  // FW: vis_a; BW: vis_b
-  __device__ __forceinline__ bool operator()(uint32_t, uint32_t v, bool valid) const
+  __device__ __forceinline__ uint32_t probe(uint32_t v) const { return __ldcg(avail + (v >> 5)); }
+  __device__ __forceinline__ bool     operator()(uint32_t, uint32_t v, bool valid, uint32_t word) const
   {
-    if (!valid || !bit_get(avail, v) || !bit_take(avail, v)) return false;
+    if (!valid || !((word >> (v & 31)) & 1u) || !bit_take(avail, v)) return false;
     bit_claim(mark, v);
     return true;
   }
@@ -426,70 +429,144 @@ k_bottom_up(uint32_t n,
   }
 }
 
-// ---------------------------------------------------------------- persistent search
-// One whole reachability search (every level) in ONE cooperative launch.
-// Blocks meet at a grid barrier between the phases of a level; the barrier
-// waits at most GRID_SYNC_SPINS polls, after which it sets bar_err and every
-// block leaves (the host reports KSPN_ERR_TIMEOUT) -- a launch whose blocks
-// were not all resident could therefore never hang.
+// ---------------------------------------------------------------- persistent FW-BW
+// The whole FW-BW -- both searches, the SCC's id and its write-back -- is
+// ONE cooperative launch whose blocks stay resident and meet at a grid
+// barrier once per level:
+//   init      cand = und minus the pivot, vis_a = vis_b = {pivot}, |und| per
+//             block; the pivot alone is the first level's frontier.
+//   FW, BW    a top-down level writes the next level's frontier already
+//             scanned: each block flush reserves its queue slots AND its
+//             range of the frontier's edge prefix with ONE 64-bit atomic on
+//             a packed (edges << qbits | vertices) counter, then writes the
+//             queue entries, their prefix and the tile starts.  Right after
+//             the barrier every block knows the next frontier's size and
+//             edge count and can expand it (or choose bottom-up) at once.
+//             A bottom-up level only counts its discoveries (the `fresh`
+//             bitmap holds them); a level that returns to top-down first
+//             builds its frontier from that bitmap the same way (one extra
+//             barrier).
+//   finalize  smallest member (one barrier, min-id mode), then und and the
+//             ids are written a bitmap word at a time.
+// Every block derives the level's control (direction, tile count, edge
+// budget) from the same counter values read after the barrier, so nothing
+// is broadcast.  Level counters rotate over three slots: level L reads slot
+// L%3, adds to (L+1)%3 and clears (L+2)%3, which no block touches again
+// until after the next barrier.
 constexpr unsigned GRID_SYNC_SPINS = 1u << 22;
+constexpr unsigned NLEAF           = 16;
 
-__device__ __forceinline__ bool
-grid_sync(reach_state* st)
+// Two-level grid barrier with monotonically growing counters: a block adds
+// to its leaf (blockIdx % NLEAF), the last of a leaf adds to the root, and
+// every block waits for root == epoch * leaves.  Counters are never reset
+// inside a launch; `epoch` carries the count to the next launch of the same
+// grid.  The host clears the whole struct when a wait gave up.
+struct grid_barrier
 {
+  unsigned long long leaf[NLEAF][16]; // one 128-byte line per leaf
+  unsigned long long root;
+  unsigned long long pad0[15];
+  unsigned long long epoch; // barriers completed by every block
+  uint32_t           err;   // 1: a wait reached GRID_SYNC_SPINS
+  uint32_t           pad1[29];
+};
+static_assert(sizeof(grid_barrier) <= 4096, "grid barrier must fit its workspace slot");
+
+__device__ __forceinline__ unsigned long long
+ld_acquire64(unsigned long long const* p)
+{
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// All threads of every block call it.  False when a wait gave up (then every
+// block returns false here or at its next barrier, and the launch ends).
+__device__ __forceinline__ bool
+grid_sync(grid_barrier* b, unsigned long long& epoch)
+{
+  __shared__ uint32_t s_ok;
   __syncthreads();
+  ++epoch;
   if (threadIdx.x == 0) {
-    uint32_t const g0 = ld_acquire(&st->bar_gen);
+    unsigned const           nb    = gridDim.x;
+    unsigned const           nleaf = nb < NLEAF ? nb : NLEAF;
+    unsigned const           g     = blockIdx.x % nleaf;
+    unsigned long long const gsize = (nb - g + nleaf - 1) / nleaf;
     __threadfence();
-    if (atomicAdd(&st->bar_count, 1u) == gridDim.x - 1) {
-      atomicExch(&st->bar_count, 0u);
+    if (atomicAdd(&b->leaf[g][0], 1ull) + 1 == epoch * gsize) {
       __threadfence();
-      atomicAdd(&st->bar_gen, 1u);
-    } else {
-      unsigned spins = 0;
-      while (ld_acquire(&st->bar_gen) == g0) {
-        if (++spins > GRID_SYNC_SPINS) {
-          atomicExch(&st->bar_err, 1u);
-          break;
-        }
-        __nanosleep(64);
+      atomicAdd(&b->root, 1ull);
+    }
+    unsigned long long const target = epoch * nleaf;
+    uint32_t                 ok     = 1;
+    for (unsigned spins = 0; ld_acquire64(&b->root) < target; ++spins) {
+      if (spins > GRID_SYNC_SPINS || ((spins & 63u) == 63u && ld_acquire(&b->err))) {
+        atomicExch(&b->err, 1u);
+        ok = 0;
+        break;
       }
+      __nanosleep(32);
     }
     __threadfence();
+    s_ok = ok;
   }
   __syncthreads();
-  return ld_acquire(&st->bar_err) == 0;
+  return s_ok != 0;
 }
 
-struct search_args
+// A scanned frontier: queue, exclusive prefix of the queued vertices'
+// degrees, and per tile of EX_TILE edges the queue index holding its first
+// edge.
+struct frontier_buf
 {
-  uint32_t        n;
-  uint32_t        trace;  // stamp phases into stamp_phase / stamp_ns
-  uint32_t*       stamp_phase;
-  uint64_t*       stamp_ns;
-  uint64_t const* td_head;
-  uint32_t const* td_adj;
-  uint64_t const* bu_head;
-  uint32_t const* bu_adj;
-  uint32_t*       avail;
-  uint32_t*       mark;
-  uint32_t*       fresh;
-  uint32_t*       q0;
-  uint32_t*       q1;
-  uint64_t*       prefix;
-  uint32_t*       tile_start;
-  uint64_t*       partial;
-  reach_state*    st;
+  uint32_t* q;
+  uint64_t* prefix;
+  uint32_t* tile_start;
 };
 
-__device__ __forceinline__ void
-chunk_of(uint32_t qn, uint32_t& beg, uint32_t& end)
+struct fwbw_args
 {
-  uint32_t const chunk = (qn + gridDim.x - 1) / gridDim.x;
-  uint64_t const b     = static_cast<uint64_t>(blockIdx.x) * chunk;
-  beg                  = static_cast<uint32_t>(b < qn ? b : qn);
-  end                  = static_cast<uint32_t>(b + chunk < qn ? b + chunk : qn);
-}
+  uint32_t           n;
+  uint32_t           pivot;
+  uint64_t           m;
+  uint32_t           cap; // level cap per search
+  uint32_t           min_ids;
+  uint32_t           qbits; // vertex bits of the packed level counters
+  uint32_t           trace;
+  unsigned long long alpha, beta;
+  uint64_t const*    fh;
+  uint32_t const*    fc;
+  uint64_t const*    bh;
+  uint32_t const*    bc;
+  uint32_t*          und;
+  uint32_t*          scc_id;
+  uint32_t*          cand;
+  uint32_t*          vis_a;
+  uint32_t*          vis_b;
+  uint32_t*          fresh;
+  frontier_buf       fb[2];
+  frontier_buf       seed;    // q[0] = pivot, prefix[0] = 0, tile starts all 0
+  uint64_t*          partial; // one per block
+  grid_barrier*      bar;
+  reach_state*       st;
+  uint32_t*          stamp_phase;
+  uint64_t*          stamp_ns;
+};
+
+// Block-shared scratch of the persistent kernel.
+struct fwbw_smem
+{
+  bu_warp_smem          warp[BU_WARPS]; // bottom-up chunks; a top-down tile's rows alias it
+  uint32_t              buf[BU_BUF];    // block queue of a top-down tile
+  uint32_t              tile_i[2];
+  uint32_t              buf_n;
+  uint32_t              cnt;
+  unsigned long long    old;
+  unsigned long long    edges_bu, cands_bu; // bottom-up statistics of the launch
+};
+static_assert(sizeof(bu_warp_smem) * BU_WARPS >= EX_TILE * sizeof(uint32_t), "tile rows must fit the warp buffers");
+static_assert(BU_BUF == EX_TILE && BU_BUF % R_THREADS == 0, "flush: whole runs per thread");
 
 __device__ __forceinline__ uint64_t
 globaltimer()
@@ -501,7 +578,7 @@ globaltimer()
 
 // block 0, thread 0: record that `phase` ended now
 __device__ __forceinline__ void
-stamp(search_args const& a, uint32_t phase)
+stamp(fwbw_args const& a, uint32_t phase)
 {
   if (!a.trace || blockIdx.x != 0 || threadIdx.x != 0) return;
   uint32_t const i = a.st->marks;
@@ -512,129 +589,349 @@ stamp(search_args const& a, uint32_t phase)
   }
 }
 
-template<bool BW>
-__global__ void __launch_bounds__(R_THREADS)
-k_search(search_args a)
+// Tiles whose first edge lies in [p, p + d) start at queue index i; tiles
+// past the graph's m edges are never written (tile_start holds
+// m / EX_TILE + 4 entries).
+__device__ __forceinline__ void
+put_tile_starts(uint32_t* tile_start, uint64_t p, uint64_t d, uint32_t i, uint64_t m)
 {
-  __shared__ bu_warp_smem sm[BU_WARPS]; // bottom-up warp chunks; sm[0..] also holds a top-down tile's rows
-  __shared__ uint32_t     s_buf[BU_BUF];
-  __shared__ uint32_t     s_i[2], s_n, s_base;
-  static_assert(sizeof(sm) >= EX_TILE * sizeof(uint32_t), "tile rows must fit the warp buffers");
-  uint32_t* const tile_rows = reinterpret_cast<uint32_t*>(sm);
-  reach_state* const  st = a.st;
-  if (threadIdx.x == 0) s_n = 0;
+  if (!d) return;
+  uint64_t const end = p + d < m ? p + d : m;
+  for (uint64_t t = (p + EX_TILE - 1) / EX_TILE; t * EX_TILE < end; ++t) tile_start[t] = i;
+}
+
+// Appends the block queue (sm.buf[0, sm.buf_n)) to a scanned frontier.
+// Thread t owns entries [8t, 8t + 8); one block scan of the degree sums
+// and one packed atomic give every entry its queue slot and edge prefix.
+// Degrees are read twice (the second time from cache) rather than held in
+// registers.  All threads call it; leaves sm.buf_n == 0.
+__device__ __forceinline__ void
+flush_scanned(fwbw_smem& sm, frontier_buf const& out, unsigned long long* ctr, uint32_t qbits, uint64_t const* __restrict__ head, uint32_t qcap, uint64_t ecap)
+{
+  constexpr int K = BU_BUF / R_THREADS;
   __syncthreads();
-  block_queue    bq{ s_buf, &s_n };
-  uint64_t       nedge = 0, ncand = 0;
-  uint32_t       nfound = 0;
-  for (;;) {
-    // control values, written by block 0 before the last barrier
-    uint32_t const cur = __ldcg(&st->cur) & 1u;
-    uint32_t const qn  = __ldcg(&st->qn[cur]);
-    if (qn == 0 || __ldcg(&st->err)) break;
-    if (__ldcg(&st->mat)) {
-      // back to top-down: the frontier queue from the last sweep's bits
-      materialize_block(blockIdx.x, gridDim.x, a.n, a.fresh, cur ? a.q1 : a.q0, &st->mat_n, &s_base);
-      if (!grid_sync(st)) break;
+  uint32_t const cnt = sm.buf_n;
+  if (cnt) {
+    uint32_t const i0  = threadIdx.x * K;
+    uint32_t const k1  = cnt > i0 ? (cnt - i0 < K ? cnt - i0 : K) : 0u; // entries of this thread
+    uint64_t       sum = 0;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (k < k1) {
+        uint32_t const v = sm.buf[i0 + k];
+        sum += head[v + 1] - head[v];
+      }
+    uint64_t       tot;
+    uint64_t const off = block_exclusive_scan<uint64_t, R_THREADS>(sum, &tot);
+    if (threadIdx.x == 0) sm.old = atomicAdd(ctr, (static_cast<unsigned long long>(tot) << qbits) | cnt);
+    __syncthreads();
+    unsigned long long const old = sm.old;
+    uint64_t const           pos0 = (old & ((1ull << qbits) - 1)) + i0;
+    uint32_t                 pos  = static_cast<uint32_t>(pos0);
+    uint64_t                 p    = (old >> qbits) + off;
+    for (uint32_t k = 0; k < k1 && pos0 + k < qcap && p < ecap; ++k, ++pos) {
+      uint32_t const v = sm.buf[i0 + k];
+      uint64_t const d = head[v + 1] - head[v];
+      out.q[pos]       = v;
+      out.prefix[pos]  = p;
+      put_tile_starts(out.tile_start, p, d, pos, ecap);
+      p += d;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) sm.buf_n = 0;
+  __syncthreads();
+}
+
+// Frontier from the `fresh` bitmap (a search returning to top-down after
+// bottom-up sweeps), scanned like flush_scanned: a thread owns MAT_WORDS
+// consecutive words, a block pass packs (edges << 16 | vertices) per
+// thread (at most 256 * 32 * MAT_WORDS < 2^16 vertices a pass).
+constexpr int MAT_WORDS = 4;
+
+__device__ __forceinline__ void
+materialize_scanned(uint32_t n, uint32_t const* fresh, frontier_buf const& out, unsigned long long* ctr, uint32_t qbits, uint64_t const* __restrict__ head, uint64_t ecap, fwbw_smem& sm)
+{
+  uint32_t const words = (n + 31) / 32;
+  uint64_t const qcap  = n; // queue slots
+  for (uint32_t wbase = blockIdx.x * R_THREADS * MAT_WORDS; wbase < words; wbase += gridDim.x * R_THREADS * MAT_WORDS) {
+    uint32_t const w0 = wbase + threadIdx.x * MAT_WORDS;
+    uint32_t       word[MAT_WORDS];
+    uint32_t       c   = 0;
+    uint64_t       deg = 0;
+#pragma unroll
+    for (int k = 0; k < MAT_WORDS; ++k) {
+      word[k] = w0 + k < words ? __ldcg(fresh + w0 + k) : 0u;
+      c += __popc(word[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < MAT_WORDS; ++k)
+      for (uint32_t x = word[k]; x; x &= x - 1) {
+        uint32_t const v = (w0 + k) * 32 + __ffs(x) - 1;
+        deg += head[v + 1] - head[v];
+      }
+    uint64_t       tot;
+    uint64_t const off = block_exclusive_scan<uint64_t, R_THREADS>((deg << 16) | c, &tot);
+    if (tot == 0) continue; // block-uniform
+    if (threadIdx.x == 0) sm.old = atomicAdd(ctr, ((tot >> 16) << qbits) | (tot & 0xFFFFu));
+    __syncthreads();
+    unsigned long long const old = sm.old;
+    uint64_t                 pos = (old & ((1ull << qbits) - 1)) + (off & 0xFFFFu);
+    uint64_t                 p   = (old >> qbits) + (off >> 16);
+#pragma unroll
+    for (int k = 0; k < MAT_WORDS; ++k)
+      for (uint32_t x = word[k]; x && pos < qcap && p < ecap; x &= x - 1) {
+        uint32_t const v = (w0 + k) * 32 + __ffs(x) - 1;
+        uint64_t const d = head[v + 1] - head[v];
+        out.q[pos]       = v;
+        out.prefix[pos]  = p;
+        put_tile_starts(out.tile_start, p, d, static_cast<uint32_t>(pos), ecap);
+        p += d;
+        ++pos;
+      }
+    __syncthreads(); // sm.old
+  }
+}
+
+// Every level of one reachability search (BW: over in-edges, candidates
+// vis_a, reached vis_b; FW: over out-edges, candidates cand, reached vis_a).
+// `glvl` numbers levels across both searches of the launch (it selects
+// counter slots and buffers).  Block 0 records the search's level counts.
+// Returns SEARCH_DONE, SEARCH_CAPPED (level cap reached) or SEARCH_FAILED
+// (the grid barrier gave up).
+enum : int
+{
+  SEARCH_DONE   = 0,
+  SEARCH_CAPPED = 1,
+  SEARCH_FAILED = 2
+};
+
+template<bool BW>
+__device__ __forceinline__ int
+run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t n_und, uint32_t& glvl, unsigned long long& epoch)
+{
+  uint64_t const* const    td_head = BW ? a.bh : a.fh;
+  uint32_t const* const    td_adj  = BW ? a.bc : a.fc;
+  uint64_t const* const    bu_head = BW ? a.fh : a.bh;
+  uint32_t const* const    bu_adj  = BW ? a.fc : a.bc;
+  uint32_t* const          avail   = BW ? a.vis_a : a.cand;
+  uint32_t* const          mark    = BW ? a.vis_b : a.vis_a;
+  reach_state* const       st      = a.st;
+  unsigned long long const qmask   = (1ull << a.qbits) - 1;
+  uint64_t                 m_u     = a.m; // Beamer's unexplored-edge budget
+  uint32_t                 mode    = 0;   // 0 top-down, 1 bottom-up
+  bool                     mat     = false;
+  uint32_t                 bu = 0, capped = 0, lvl = 0;
+  uint64_t                 edges_td = 0;
+  // the first frontier: the pivot alone
+  unsigned long long c = (static_cast<unsigned long long>(td_head[a.pivot + 1] - td_head[a.pivot]) << a.qbits) | 1u;
+  for (;; ++lvl, ++glvl) {
+    uint32_t const     s_in = glvl % 3, s_out = (glvl + 1) % 3, s_clr = (glvl + 2) % 3;
+    frontier_buf const fin  = lvl == 0 ? a.seed : a.fb[glvl & 1];
+    frontier_buf const fout = a.fb[(glvl + 1) & 1];
+    if (lvl) c = __ldcg(&st->lq[s_in]);
+    if (mat) {
+      materialize_scanned(a.n, a.fresh, fin, &st->mat_q, a.qbits, td_head, a.m, sm);
+      if (!grid_sync(a.bar, epoch)) return SEARCH_FAILED;
       stamp(a, 7);
+      c = __ldcg(&st->mat_q);
     }
-    uint32_t const* qin    = cur ? a.q1 : a.q0;
-    uint32_t* const qout   = cur ? a.q0 : a.q1;
-    uint32_t* const qout_n = &st->qn[cur ^ 1u];
-    if (__ldcg(&st->scan)) {
-      // degrees of the frontier (top-down direction): block partial sums
-      uint32_t beg, end;
-      chunk_of(qn, beg, end);
-      uint64_t sum = 0;
-      for (uint32_t i = beg + threadIdx.x; i < end; i += R_THREADS) {
-        uint32_t const v = __ldcg(qin + i);
-        sum += a.td_head[v + 1] - a.td_head[v];
-      }
-      uint64_t total;
-      block_exclusive_scan<uint64_t, R_THREADS>(sum, &total);
-      if (threadIdx.x == 0) a.partial[blockIdx.x] = total;
-      if (!grid_sync(st)) break;
-      stamp(a, 1);
-      // block 0: scan of the partial sums, totals, direction
-      if (blockIdx.x == 0) {
-        uint32_t const nb  = gridDim.x;
-        uint32_t const per = (nb + R_THREADS - 1) / R_THREADS;
-        uint32_t const b0  = threadIdx.x * per;
-        uint64_t       loc = 0;
-        for (uint32_t i = b0; i < b0 + per && i < nb; ++i) loc += __ldcg(a.partial + i);
-        uint64_t all;
-        uint64_t run = block_exclusive_scan<uint64_t, R_THREADS>(loc, &all);
-        for (uint32_t i = b0; i < b0 + per && i < nb; ++i) {
-          uint64_t const x = __ldcg(a.partial + i);
-          a.partial[i]     = run;
-          run += x;
-        }
-        if (threadIdx.x == 0) {
-          a.prefix[qn]    = all;
-          st->ntiles      = static_cast<uint32_t>((all + EX_TILE - 1) / EX_TILE);
-          st->m_f         = all;
-          uint32_t mode   = __ldcg(&st->mode);
-          if (mode == 0 && all * __ldcg(&st->alpha) > __ldcg(&st->m_u)) mode = 1;
-          else if (mode == 1) mode = 0; // the frontier fell below n_und / beta
-          st->mode = mode;
-          if (mode == 0) st->edges_td = __ldcg(&st->edges_td) + all;
-        }
-      }
-      if (!grid_sync(st)) break;
-      stamp(a, 2);
-      if (__ldcg(&st->mode) == 0) {
-        // frontier prefix and tile starts
-        uint64_t run = __ldcg(a.partial + blockIdx.x);
-        for (uint32_t base = beg; base < end; base += R_THREADS) {
-          uint32_t const i   = base + threadIdx.x;
-          uint64_t       deg = 0;
-          if (i < end) {
-            uint32_t const v = __ldcg(qin + i);
-            deg              = a.td_head[v + 1] - a.td_head[v];
-          }
-          uint64_t       tot;
-          uint64_t const p = run + block_exclusive_scan<uint64_t, R_THREADS>(deg, &tot);
-          if (i < end) {
-            a.prefix[i] = p;
-            if (deg) {
-              uint64_t const t0 = (p + EX_TILE - 1) / EX_TILE;
-              uint64_t const t1 = (p + deg - 1) / EX_TILE;
-              for (uint64_t t = t0; t <= t1; ++t) a.tile_start[t] = i;
-            }
-          }
-          run += tot;
-        }
-        if (!grid_sync(st)) break;
-        stamp(a, 3);
-      }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->lq[s_clr] = 0;
+      if (!mat) st->mat_q = 0;
     }
-    uint32_t const phase = __ldcg(&st->mode) == 0 ? 4u : 5u;
-    if (__ldcg(&st->mode) == 0) {
-      uint32_t const ntiles = __ldcg(&st->ntiles);
-      uint64_t const total  = __ldcg(a.prefix + qn);
-      take_op const  op{ a.avail, a.mark };
-      for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        expand_tile(tile, ntiles, qin, qn, total, a.prefix, a.tile_start, a.td_head, a.td_adj, tile_rows, s_i, bq, op);
-        bq.flush(qout, qout_n, &s_base);
+    uint64_t const qn64 = c & qmask;
+    uint64_t const mf   = c >> a.qbits; // the frontier's edges (0 after a sweep)
+    if (qn64 == 0) break;
+    if (lvl >= a.cap || qn64 > a.n || mf > a.m) {
+      // level cap; or counters beyond the graph, which a correct search
+      // never produces (then nothing more is read or written)
+      capped = 1;
+      break;
+    }
+    uint32_t const qn = static_cast<uint32_t>(qn64);
+    if (mat) mode = 0;
+    else if (mode == 0 && mf * a.alpha > m_u) mode = 1;
+    unsigned long long* const octr = &st->lq[s_out];
+    if (mode == 0) {
+      edges_td += mf;
+      uint32_t const ntiles = static_cast<uint32_t>((mf + EX_TILE - 1) / EX_TILE);
+      // few tiles: split each into `parts` slot ranges on separate blocks,
+      // so a small frontier still spreads over the grid
+      uint32_t parts = 1;
+      while (parts < EX_ITEMS && static_cast<uint64_t>(ntiles) * parts * 2 <= gridDim.x) parts *= 2;
+      int const      per   = EX_ITEMS / static_cast<int>(parts);
+      uint32_t const units = ntiles * parts;
+      take_op const  op{ avail, mark };
+      block_queue    bq{ sm.buf, &sm.buf_n };
+      for (uint32_t unit = blockIdx.x; unit < units; unit += gridDim.x) {
+        int const part = static_cast<int>(unit % parts);
+        expand_tile(unit / parts, ntiles, fin.q, qn, mf, fin.prefix, fin.tile_start, td_head, td_adj, reinterpret_cast<uint32_t*>(sm.warp), sm.tile_i, bq, op, part * per, part * per + per);
+        flush_scanned(sm, fout, octr, a.qbits, td_head, a.n, a.m);
       }
     } else {
-      unsigned const wid = threadIdx.x >> 5;
-      nfound             = 0;
-      bu_sweep_warp(blockIdx.x * BU_WARPS + wid, gridDim.x * BU_WARPS, a.n, a.bu_head, a.bu_adj, a.avail, a.mark, a.fresh, sm[wid], nfound, nedge, ncand);
+      if (threadIdx.x == 0) sm.cnt = 0;
+      __syncthreads();
+      unsigned const wid    = threadIdx.x >> 5;
+      uint32_t       nfound = 0;
+      uint64_t       ne = 0, nc = 0;
+      bu_sweep_warp(blockIdx.x * BU_WARPS + wid, gridDim.x * BU_WARPS, a.n, bu_head, bu_adj, avail, mark, a.fresh, sm.warp[wid], nfound, ne, nc);
 #pragma unroll
-      for (int sh = 16; sh; sh >>= 1) nfound += __shfl_down_sync(0xFFFFFFFFu, nfound, sh);
-      if ((threadIdx.x & 31) == 0 && nfound) atomicAdd(qout_n, nfound);
+      for (int sh = 16; sh; sh >>= 1) {
+        nfound += __shfl_down_sync(0xFFFFFFFFu, nfound, sh);
+        ne += __shfl_down_sync(0xFFFFFFFFu, ne, sh);
+      }
+      if ((threadIdx.x & 31) == 0) {
+        if (nfound) atomicAdd(&sm.cnt, nfound);
+        if (ne) atomicAdd(&sm.edges_bu, static_cast<unsigned long long>(ne));
+        if (nc) atomicAdd(&sm.cands_bu, static_cast<unsigned long long>(nc)); // counted by lane 0
+      }
+      __syncthreads();
+      if (threadIdx.x == 0 && sm.cnt) atomicAdd(octr, static_cast<unsigned long long>(sm.cnt)); // vertices only
     }
-    if (!grid_sync(st)) break;
-    stamp(a, phase);
-    if (blockIdx.x == 0 && threadIdx.x == 0) advance_body<BW>(st);
-    if (!grid_sync(st)) break;
-    stamp(a, 6);
+    if (!grid_sync(a.bar, epoch)) return SEARCH_FAILED;
+    stamp(a, mode ? 5u : 4u);
+    m_u = m_u > mf ? m_u - mf : 0;
+    bu += mode;
+    mat = false;
+    if (mode == 1) {
+      // stay bottom-up while the sweep found at least n_und / beta vertices
+      uint32_t const next = static_cast<uint32_t>(__ldcg(&st->lq[s_out]) & qmask);
+      mat                 = next != 0 && static_cast<unsigned long long>(next) * a.beta < n_und;
+    }
   }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (BW) st->levels_bw = lvl, st->bu_bw = bu;
+    else st->levels_fw = lvl, st->bu_fw = bu;
+    st->edges_td += edges_td;
+  }
+  return capped ? SEARCH_CAPPED : SEARCH_DONE;
+}
+
+__global__ void __launch_bounds__(R_THREADS, 4)
+k_fwbw(fwbw_args a)
+{
+  __shared__ fwbw_smem sm;
+  reach_state* const   st    = a.st;
+  unsigned long long   epoch = __ldcg(&a.bar->epoch);
+  uint32_t const       p     = a.pivot;
+  uint32_t const       words = (a.n + 31) / 32;
+  if (threadIdx.x == 0) sm.buf_n = 0, sm.edges_bu = sm.cands_bu = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->marks = 0;
+    stamp(a, 0);
+    st->lq[0] = st->lq[1] = st->lq[2] = 0;
+    st->mat_q                         = 0;
+    st->id                            = UNDECIDED;
+    st->decided                       = 0;
+    st->edges_bu = st->cands_bu = st->edges_td = 0;
+    st->levels_fw = st->bu_fw = st->levels_bw = st->bu_bw = 0;
+    a.seed.q[0]                       = p;
+    a.seed.prefix[0]                  = 0;
+  }
+  // init: cand = und \ {p}, vis_a = vis_b = {p}; |und| per block
+  uint32_t c = 0;
+  for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) {
+    uint32_t const u   = __ldcg(a.und + w);
+    uint32_t const pin = w == (p >> 5) ? 1u << (p & 31) : 0u;
+    a.cand[w]          = u & ~pin;
+    a.vis_a[w]         = pin;
+    a.vis_b[w]         = pin;
+    c += __popc(u);
+  }
+  uint64_t tot;
+  block_exclusive_scan<uint64_t, R_THREADS>(c, &tot);
+  if (threadIdx.x == 0) a.partial[blockIdx.x] = tot;
+  uint32_t glvl = 0;
+  int      rc   = grid_sync(a.bar, epoch) ? SEARCH_DONE : SEARCH_FAILED;
+  if (rc == SEARCH_DONE) {
+    stamp(a, 8);
+    uint64_t s = 0;
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += R_THREADS) s += __ldcg(a.partial + i);
+    block_exclusive_scan<uint64_t, R_THREADS>(s, &tot);
+    uint32_t const n_und = static_cast<uint32_t>(tot);
+    // one inlined copy of the level loop, run for FW then BW
+#pragma unroll 1
+    for (int dir = 0; dir < 2 && rc == SEARCH_DONE; ++dir) {
+      if (dir) {
+        // BW: candidates are the FW-reached vertices except the pivot (each
+        // block clears its bit before its own first expansion)
+        if (threadIdx.x == 0) atomicAnd(a.vis_a + (p >> 5), ~(1u << (p & 31)));
+        __syncthreads();
+      }
+      rc = dir ? run_search<true>(a, sm, n_und, glvl, epoch) : run_search<false>(a, sm, n_und, glvl, epoch);
+    }
+  }
+  uint32_t id = p;
+  if (rc == SEARCH_DONE && a.min_ids) {
+    // smallest member = first set bit of vis_b.  Every block first looks at
+    // the same leading MIN_WORDS words (the SCC is usually dense there);
+    // only when they are all empty does the grid search the rest and meet
+    // at a barrier.  Every block reads the same words, so all take the
+    // same branch.
+    constexpr uint32_t MIN_WORDS = 4 * R_THREADS;
+    uint32_t           best      = UNDECIDED;
+    for (uint32_t w = threadIdx.x; w < MIN_WORDS && w < words; w += R_THREADS) {
+      uint32_t const s = __ldcg(a.vis_b + w);
+      if (s) {
+        best = w * 32 + (__ffs(s) - 1);
+        break;
+      }
+    }
+    best = __reduce_min_sync(0xFFFFFFFFu, best);
+    if ((threadIdx.x & 31) == 0) sm.cnt = UNDECIDED;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0 && best != UNDECIDED) atomicMin(&sm.cnt, best);
+    __syncthreads();
+    id = sm.cnt;
+    if (id == UNDECIDED) {
+      for (uint32_t w = MIN_WORDS + blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) {
+        uint32_t const s = __ldcg(a.vis_b + w);
+        if (s) {
+          best = w * 32 + (__ffs(s) - 1);
+          break; // later words of this thread only hold larger ids
+        }
+      }
+      best = __reduce_min_sync(0xFFFFFFFFu, best);
+      if ((threadIdx.x & 31) == 0 && best != UNDECIDED && best < __ldcg(&st->id)) atomicMin(&st->id, best);
+      if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
+      id = __ldcg(&st->id);
+    }
+  }
+  if (rc == SEARCH_DONE) {
+    // the SCC (vis_b) leaves und with its id: one warp per bitmap word,
+    // lane l writes vertex 32w + l (one coalesced 128-byte store per word)
+    // (a warp loads 32 words at once, then broadcasts each non-empty one)
+    unsigned const lane = threadIdx.x & 31u;
+    uint32_t       cnt  = 0;
+    for (uint32_t wb = (blockIdx.x * R_THREADS + threadIdx.x) & ~31u; wb < words; wb += gridDim.x * R_THREADS) {
+      uint32_t const w    = wb + lane;
+      uint32_t const mine = w < words ? __ldcg(a.vis_b + w) : 0u;
+      if (mine) {
+        a.und[w] &= ~mine;
+        cnt += __popc(mine);
+      }
+      for (unsigned todo = __ballot_sync(0xFFFFFFFFu, mine != 0); todo; todo &= todo - 1) {
+        unsigned const j = __ffs(todo) - 1;
+        uint32_t const s = __shfl_sync(0xFFFFFFFFu, mine, j);
+        if ((s >> lane) & 1u) a.scc_id[(wb + j) * 32 + lane] = id;
+      }
+    }
 #pragma unroll
-  for (int sh = 16; sh; sh >>= 1) nedge += __shfl_down_sync(0xFFFFFFFFu, nedge, sh);
-  if ((threadIdx.x & 31) == 0 && nedge) atomicAdd(&st->edges_bu, static_cast<unsigned long long>(nedge));
-  if (threadIdx.x == 0 && ncand) atomicAdd(&st->cands_bu, static_cast<unsigned long long>(ncand));
+    for (int sh = 16; sh; sh >>= 1) cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, sh);
+    if (lane == 0 && cnt) atomicAdd(&st->decided, cnt);
+  }
+  // statistics
+  __syncthreads();
+  if (threadIdx.x == 0 && sm.edges_bu) atomicAdd(&st->edges_bu, sm.edges_bu);
+  if (threadIdx.x == 0 && sm.cands_bu) atomicAdd(&st->cands_bu, sm.cands_bu);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->id      = id;
+    st->err     = rc == SEARCH_CAPPED ? 1u : 0u;
+    st->bar_err = rc == SEARCH_FAILED ? 1u : 0u;
+    if (rc != SEARCH_FAILED) a.bar->epoch = epoch; // every block completed the same barriers
+    stamp(a, 9);
+  }
 }
 
 __global__ void
@@ -739,23 +1036,35 @@ bw_io(kspn_context* ctx, dgraph const& g)
   return { g.bh, g.bc, g.fh, g.fc, ctx->ws.vis_a, ctx->ws.vis_b, ctx->ws.fresh };
 }
 
-// Cooperative launch of one persistent search: as many blocks as fit on
-// the device at once (all co-resident, which the grid barrier needs).
-template<bool BW>
-void
-launch_search(kspn_context* ctx, search_args const& a)
+unsigned
+bit_width64(uint64_t x)
 {
-  static int bps = 0, sms = 0;
-  if (!bps) {
-    KSPN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_search<BW>, R_THREADS, 0));
+  return x ? 64u - static_cast<unsigned>(__builtin_clzll(x)) : 0u;
+}
+
+// The packed level counters hold a frontier's vertices in the low qbits and
+// its edges above them; the frontier built from `fresh` packs (edges << 16 |
+// vertices) per block pass.
+bool
+packed_counters_fit(uint32_t n, uint64_t m)
+{
+  return bit_width64(n) + bit_width64(m) <= 64 && m < (1ull << 48);
+}
+
+// Grid of the persistent FW-BW: every block resident at once (which the
+// grid barrier needs), fixed per context (the barrier's epoch count assumes
+// the same grid at every launch).
+unsigned
+fwbw_grid(kspn_context* ctx)
+{
+  if (!ctx->search_grid) {
+    int bps = 0, sms = 0;
+    KSPN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_fwbw, R_THREADS, 0));
     KSPN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    if (bps < 1) throw error{ KSPN_ERR_CUDA, "persistent search kernel does not fit on an SM" };
+    if (bps < 1) throw error{ KSPN_ERR_CUDA, "persistent FW-BW kernel does not fit on an SM" };
+    ctx->search_grid = static_cast<unsigned>(std::min(bps * sms, 4000));
   }
-  unsigned const grid = static_cast<unsigned>(std::min(bps * sms, 4000));
-  search_args    arg  = a;
-  void*          args[] = { &arg };
-  KSPN_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(&k_search<BW>), dim3(grid), dim3(R_THREADS), args, 0, ctx->stream));
-  ctx->launches += 1;
+  return ctx->search_grid;
 }
 
 } // namespace
@@ -769,7 +1078,7 @@ reach_state_bytes()
 void
 release_graphs(kspn_context* ctx)
 {
-  for (cached_graph* c : { &ctx->fwbw, &ctx->trim }) {
+  for (cached_graph* c : { &ctx->trim }) {
     if (c->exec) cudaGraphExecDestroy(c->exec);
     if (c->graph) cudaGraphDestroy(c->graph);
     *c = {};
@@ -790,37 +1099,60 @@ fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint3
   hs->alpha   = opt.bu_enter_div ? opt.bu_enter_div : 1;
   hs->beta    = opt.bu_leave_div ? opt.bu_leave_div : 1;
   hs->min_ids = min_ids ? 1u : 0u;
-  KSPN_CUDA(cudaMemcpyAsync(rs, hs, sizeof(reach_state), cudaMemcpyHostToDevice, ctx->stream));
 
   uint32_t const words = (g.n + 31) / 32;
-  if (!ctx->prof) {
-    // whole searches on the device: one cooperative launch per direction
-    k_r_init<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(words, g.m, und, ws.mark, ws.vis_a, ws.vis_b, rs);
+  auto* const    gbar  = static_cast<grid_barrier*>(ws.gbar);
+  if (!ctx->prof && packed_counters_fit(g.n, g.m)) {
+    // the whole FW-BW on the device: one cooperative launch
+    bool const tr = opt.trace && st && st->search_marks == 0;
+    fwbw_args  a{};
+    a.n           = g.n;
+    a.pivot       = pivot;
+    a.m           = g.m;
+    a.cap         = hs->cap;
+    a.min_ids     = hs->min_ids;
+    a.qbits       = bit_width64(g.n);
+    a.trace       = tr ? 1u : 0u;
+    a.alpha       = hs->alpha;
+    a.beta        = hs->beta;
+    a.fh          = g.fh;
+    a.fc          = g.fc;
+    a.bh          = g.bh;
+    a.bc          = g.bc;
+    a.und         = und;
+    a.scc_id      = scc_id;
+    a.cand        = ws.mark;
+    a.vis_a       = ws.vis_a;
+    a.vis_b       = ws.vis_b;
+    a.fresh       = ws.fresh;
+    a.fb[0]       = { ws.q0, ws.prefix, ws.tile_start };
+    a.fb[1]       = { ws.q1, ws.prefix2, ws.tile_start2 };
+    a.seed        = { ws.seed_q, ws.seed_prefix, ws.tile_zero };
+    a.partial     = ws.blocks;
+    a.bar         = gbar;
+    a.st          = rs;
+    a.stamp_phase = reinterpret_cast<uint32_t*>(static_cast<char*>(ws.rstate) + 2048);
+    a.stamp_ns    = reinterpret_cast<uint64_t*>(static_cast<char*>(ws.rstate) + 2048 + 4 * MARKS);
+    void* args[]  = { &a };
+    KSPN_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(&k_fwbw), dim3(fwbw_grid(ctx)), dim3(R_THREADS), args, 0, ctx->stream));
     ctx->launches += 1;
-    for (int bw = 0; bw < 2; ++bw) {
-      search_io const io = bw ? bw_io(ctx, g) : fw_io(ctx, g);
-      auto* stamp_phase = reinterpret_cast<uint32_t*>(static_cast<char*>(ws.rstate) + 2048);
-      auto* stamp_ns    = reinterpret_cast<uint64_t*>(static_cast<char*>(ws.rstate) + 2048 + 4 * MARKS);
-      bool const tr     = opt.trace && st && st->search_marks == 0;
-      search_args const a{ g.n, tr ? 1u : 0u, stamp_phase, stamp_ns, io.td_head, io.td_adj, io.bu_head, io.bu_adj, io.avail, io.mark, io.fresh, ws.q0, ws.q1, ws.prefix, ws.tile_start, ws.blocks, rs };
-      if (bw) {
-        k_r_seed<true><<<1, 1, 0, ctx->stream>>>(io.avail, io.mark, ws.q0, rs);
-        launch_search<true>(ctx, a);
-      } else {
-        k_r_seed<false><<<1, 1, 0, ctx->stream>>>(io.avail, io.mark, ws.q0, rs);
-        launch_search<false>(ctx, a);
-      }
-      ctx->launches += 1;
+    // results, and the barrier's error word (read after the launch ended:
+    // a block that gave up may set it after block 0 finished)
+    auto* const hb = reinterpret_cast<uint32_t*>(static_cast<char*>(ctx->h_state) + 1024);
+    KSPN_CUDA(cudaMemcpyAsync(hs, rs, sizeof(reach_state), cudaMemcpyDeviceToHost, ctx->stream));
+    KSPN_CUDA(cudaMemcpyAsync(hb, &gbar->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (*hb || hs->bar_err) {
+      // counters of a launch that gave up are not epoch-aligned: start over
+      KSPN_CUDA(cudaMemsetAsync(gbar, 0, sizeof(grid_barrier), ctx->stream));
+      KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+      throw error{ KSPN_ERR_TIMEOUT, "reachability: grid barrier wait limit reached" };
     }
-    k_r_setid<<<1, 1, 0, ctx->stream>>>(rs);
-    k_bitmap_min<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(g.n, ws.vis_b, rs);
-    k_fwbw_finalize<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(g.n, ws.vis_b, und, scc_id, rs);
-    KSPN_CHECK_LAUNCH();
-    ctx->launches += 3;
   } else {
     // host-driven loop over the same kernels, expansion kernels bracketed
     // by CUDA events (kspn_options.profile)
     bool const trace_done = st && st->levels_fw != 0; // trace the first FW-BW only
+    KSPN_CUDA(cudaMemcpyAsync(rs, hs, sizeof(reach_state), cudaMemcpyHostToDevice, ctx->stream));
     k_r_init<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(words, g.m, und, ws.mark, ws.vis_a, ws.vis_b, rs);
     ctx->launches += 1;
     for (int bw = 0; bw < 2; ++bw) {
@@ -869,11 +1201,10 @@ fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint3
     k_fwbw_finalize<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(g.n, ws.vis_b, und, scc_id, rs);
     KSPN_CHECK_LAUNCH();
     ctx->launches += 3;
+    KSPN_CUDA(cudaMemcpyAsync(hs, rs, sizeof(reach_state), cudaMemcpyDeviceToHost, ctx->stream));
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
   }
-  KSPN_CUDA(cudaMemcpyAsync(hs, rs, sizeof(reach_state), cudaMemcpyDeviceToHost, ctx->stream));
-  KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
   if (hs->err) throw error{ KSPN_ERR_TIMEOUT, "reachability: level cap exceeded" };
-  if (hs->bar_err) throw error{ KSPN_ERR_TIMEOUT, "reachability: grid barrier wait limit reached" };
   if (opt.trace && st && st->search_marks == 0 && hs->marks) {
     uint32_t const k = std::min<uint32_t>(hs->marks, MARKS);
     KSPN_CUDA(cudaMemcpyAsync(st->search_phase, static_cast<char*>(ws.rstate) + 2048, 4 * k, cudaMemcpyDeviceToHost, ctx->stream));
