@@ -230,9 +230,10 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
   if (opt.validate) validate(ctx, g);
   if (g.n == 0) return;
 
-  uint32_t* und       = ws.und;
-  uint64_t  decided   = 0;
-  bool      label_ran = false;
+  uint32_t* und         = ws.und;
+  uint64_t  decided     = 0;
+  bool      label_ran   = false;
+  bool      und_checked = false; // und already counted empty on the device
   auto      add     = [&](int phase, uint32_t d) {
     decided += d;
     if (st) st->decided[phase] += d;
@@ -258,17 +259,52 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
     // trim_1_first's pivot (argmax in*out) lies in the giant component of
     // the graphs this targets; FW-BW runs before any further trimming, and
     // the trim fixpoint then only walks the (small) remainder
-    uint32_t const pivot = trim_1_first(ctx, g, und, scc_id, nullptr, nullptr, false);
-    add(KSPN_PHASE_TRIM_FIRST, ctx->h_ctr[CTR_AUX]);
-    if (decided < g.n) {
-      if (st) st->pivot = pivot;
-      add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pivot, opt, st, true));
+    uint32_t rounds  = 0;
+    bool     trimmed = false; // this round's trim fixpoint already ran
+    if (!ctx->prof && resident_fits(g)) {
+      // trim_1_first, then FW-BW and the trim fixpoint in ONE persistent
+      // launch that takes the pivot from device memory: one host sync
+      trim_1_first_async(ctx, g, und, scc_id);
+      KSPN_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
+      fw_bw_trim_async(ctx, g, und, scc_id, opt, st);
+      KSPN_CUDA(cudaMemcpyAsync(ctx->h_ctr, ws.ctr, 64 * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+      KSPN_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
+      KSPN_CUDA(cudaEventSynchronize(ctx->ev[3]));
+      resident_result const r  = fw_bw_trim_result(ctx, opt, st);
+      uint32_t const        tf = ctx->h_ctr[CTR_DECIDED];
+      decided += static_cast<uint64_t>(tf) + r.fwbw_decided + r.trim_decided;
+      if (st) {
+        float a = 0, b = 0;
+        KSPN_CUDA(cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[2]));
+        KSPN_CUDA(cudaEventElapsedTime(&b, ctx->ev[2], ctx->ev[3]));
+        st->ms[KSPN_PHASE_TRIM_FIRST] += a;
+        st->ms[KSPN_PHASE_FWBW] += b * r.fwbw_share;
+        st->ms[KSPN_PHASE_TRIM] += b * (1.0 - r.fwbw_share);
+        st->decided[KSPN_PHASE_TRIM_FIRST] += tf;
+        st->decided[KSPN_PHASE_FWBW] += r.fwbw_decided;
+        st->decided[KSPN_PHASE_TRIM] += r.trim_decided;
+        st->pivot = r.pivot;
+      }
+      std::swap(ctx->ev[0], ctx->ev[3]); // later phases are timed from here
+      if (decided > g.n || r.und_left != g.n - decided) throw error{ KSPN_ERR_INTERNAL, "resident pipeline: undecided count does not match" };
+      rounds      = 1;
+      trimmed     = true;
+      und_checked = decided == g.n; // the launch counted und: empty
+    } else {
+      uint32_t const pivot = trim_1_first(ctx, g, und, scc_id, nullptr, nullptr, false);
+      add(KSPN_PHASE_TRIM_FIRST, ctx->h_ctr[CTR_AUX]);
+      if (decided < g.n) {
+        if (st) st->pivot = pivot;
+        add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pivot, opt, st, true));
+      }
     }
-    int      rotation = 0;
-    uint32_t rounds   = 0;
+    int rotation = 0;
     while (decided < g.n) {
-      if (++rounds > round_cap) throw error{ KSPN_ERR_TIMEOUT, "pipeline round cap exceeded" };
-      add(KSPN_PHASE_TRIM, trim_fixpoint(ctx, g, und, scc_id, false, 0));
+      if (!trimmed) {
+        if (++rounds > round_cap) throw error{ KSPN_ERR_TIMEOUT, "pipeline round cap exceeded" };
+        add(KSPN_PHASE_TRIM, trim_fixpoint(ctx, g, und, scc_id, false, 0));
+      }
+      trimmed = false;
       if (decided < g.n && opt.trim2) {
         uint32_t const d2 = trim_2(ctx, g, und, scc_id);
         add(KSPN_PHASE_TRIM2, d2);
@@ -281,7 +317,7 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
     }
     if (st) st->rounds = rounds;
   }
-  if (decided != g.n || count_undecided(ctx, g.n, und) != 0) throw error{ KSPN_ERR_INTERNAL, "decided-vertex count does not match n" };
+  if (decided != g.n || (!und_checked && count_undecided(ctx, g.n, und) != 0)) throw error{ KSPN_ERR_INTERNAL, "decided-vertex count does not match n" };
   if (st) st->edges_scanned = ctx->h_ctr64[0] + ctx->td_edges;
   // trim (id = itself), trim-2 (id = the smaller of the pair) and FW-BW
   // (id = smallest member) already name components canonically; label

@@ -180,8 +180,14 @@ enum ctr_slot : int
   CTR_DECIDED,  // vertices decided by the running phase
   CTR_AUX,      // phase-specific
   CTR_ERR,      // error word (bounds checks, caps)
-  CTR_COUNT = 16 // slots 5.. are phase-specific (8: expansion tile count)
+  CTR_COUNT = 16, // slots 5.. are phase-specific (8: expansion tile count)
+  CTR_PV_TICKET = 15 // trim_1_first: blocks finished (the last one reduces the pivot)
 };
+
+// ws.pivot holds per-block (product, id) pivot candidates: products at
+// [0, 4096), ids as u32 from ws.pivot + 4096.  trim_1_first's last block
+// leaves the grid-wide best in slot PV_FINAL of both.
+constexpr uint32_t PV_FINAL = 4095;
 
 // Scratch owned by a context, sized for the largest graph seen.
 struct workspace
@@ -330,7 +336,20 @@ void zero_counters(kspn_context* ctx);
 int  fail(kspn_context* ctx, error const& e);
 
 // trim.cu
+// reach.cu: the resident start of the FAST pipeline -- FW-BW from
+// trim_1_first's pivot (left on the device) and the trim-1 fixpoint in one
+// persistent launch, no host sync; results after the stream synchronised.
+struct resident_result
+{
+  uint32_t pivot = 0, fwbw_decided = 0, trim_decided = 0, trim_levels = 0, und_left = 0;
+  double   fwbw_share = 1.0; // FW-BW's share of the launch's device time
+};
+bool            resident_fits(dgraph const& g);
+void            fw_bw_trim_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, kspn_options const& opt, kspn_stats* st);
+resident_result fw_bw_trim_result(kspn_context* ctx, kspn_options const& opt, kspn_stats* st);
+
 uint32_t trim_1_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* queue_out, uint32_t* queue_count_host, bool init_degrees);
+void     trim_1_first_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id); // no host sync: decided in ws.ctr, pivot in PV_FINAL
 uint32_t trim_1_normal(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id);
 uint32_t trim_fixpoint(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, bool degrees_from_first, uint32_t seed_count);
 uint32_t trim_exhaustive_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* outdeg, uint32_t* indeg);

@@ -86,6 +86,13 @@ struct reach_state
   uint32_t           marks;   // phase stamps taken (kspn_options.trace)
   unsigned long long lq[3];   // persistent launch: packed level counters (edges << qbits | vertices)
   unsigned long long mat_q;   // persistent launch: counter of a frontier built from `fresh`
+  // resident pipeline (FW-BW launch with the trim fixpoint as its tail)
+  uint32_t           pivot_used;   // pivot the launch searched from (n: none)
+  uint32_t           trim_decided; // vertices the trim tail decided
+  uint32_t           trim_levels;  // its push levels
+  uint32_t           und_left;     // undecided vertices when the launch ended
+  unsigned long long trim_edges;   // adjacency entries the trim tail read
+  unsigned long long t_ns[3];      // %globaltimer: launch start, FW-BW end, trim end
 };
 
 // phase stamps live after the state: uint32 phase[128], uint64 ns[128]
@@ -548,6 +555,13 @@ struct fwbw_args
   frontier_buf       fb[2];
   frontier_buf       seed;    // q[0] = pivot, prefix[0] = 0, tile starts all 0
   uint64_t*          partial; // one per block
+  // resident pipeline: pivot == PIVOT_FROM_DEVICE takes trim_1_first's
+  // (pv_prod, pv_id); trim != 0 runs the trim-1 fixpoint after the FW-BW
+  uint64_t const*    pv_prod;
+  uint32_t const*    pv_id;
+  uint32_t           trim;
+  uint32_t*          indeg;
+  uint32_t*          outdeg;
   grid_barrier*      bar;
   reach_state*       st;
   uint32_t*          stamp_phase;
@@ -696,7 +710,8 @@ materialize_scanned(uint32_t n, uint32_t const* fresh, frontier_buf const& out, 
 // Every level of one reachability search (BW: over in-edges, candidates
 // vis_a, reached vis_b; FW: over out-edges, candidates cand, reached vis_a).
 // `glvl` numbers levels across both searches of the launch (it selects
-// counter slots and buffers).  Block 0 records the search's level counts.
+// counter slots and buffers); `pivot` is the launch's resolved pivot (never
+// the PIVOT_FROM_DEVICE marker).  Block 0 records the search's level counts.
 // Returns SEARCH_DONE, SEARCH_CAPPED (level cap reached) or SEARCH_FAILED
 // (the grid barrier gave up).
 enum : int
@@ -708,7 +723,7 @@ enum : int
 
 template<bool BW>
 __device__ __forceinline__ int
-run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t n_und, uint32_t& glvl, unsigned long long& epoch)
+run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uint32_t& glvl, unsigned long long& epoch)
 {
   uint64_t const* const    td_head = BW ? a.bh : a.fh;
   uint32_t const* const    td_adj  = BW ? a.bc : a.fc;
@@ -724,7 +739,7 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t n_und, uint32_t& glvl, un
   uint32_t                 bu = 0, capped = 0, lvl = 0;
   uint64_t                 edges_td = 0;
   // the first frontier: the pivot alone
-  unsigned long long c = (static_cast<unsigned long long>(td_head[a.pivot + 1] - td_head[a.pivot]) << a.qbits) | 1u;
+  unsigned long long c = (static_cast<unsigned long long>(td_head[pivot + 1] - td_head[pivot]) << a.qbits) | 1u;
   for (;; ++lvl, ++glvl) {
     uint32_t const     s_in = glvl % 3, s_out = (glvl + 1) % 3, s_clr = (glvl + 2) % 3;
     frontier_buf const fin  = lvl == 0 ? a.seed : a.fb[glvl & 1];
@@ -808,17 +823,242 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t n_und, uint32_t& glvl, un
   return capped ? SEARCH_CAPPED : SEARCH_DONE;
 }
 
+// ---------------------------------------------------------------- trim tail
+// The trim-1 fixpoint on what the FW-BW left undecided, in the same launch.
+// Live degrees are counted against `snap` (und as the trim starts, written
+// by the finalize pass), so the vertices this first pass decides do not
+// disturb the counts; afterwards every decided vertex decrements each
+// still-undecided neighbour's count once per edge, and a count reaching 0
+// decides that neighbour (one push level per barrier).
+constexpr int PIVOT_FROM_DEVICE = -1; // fwbw_args.pivot: take trim_1_first's pivot
+
+// Warp-aggregated append to a queue whose length is a 64-bit counter: all
+// lanes of the warp call it (warp_push64) or only the active ones
+// (warp_push_active64).  Slots at or past `cap` are not written.
+__device__ __forceinline__ void
+warp_push64(bool pred, uint32_t v, uint32_t* q, unsigned long long* count, uint64_t cap)
+{
+  unsigned const ballot = __ballot_sync(0xFFFFFFFFu, pred);
+  if (!ballot) return;
+  unsigned const     lane = threadIdx.x & 31u, leader = __ffs(ballot) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(count, static_cast<unsigned long long>(__popc(ballot)));
+  base                = __shfl_sync(0xFFFFFFFFu, base, leader);
+  uint64_t const slot = base + __popc(ballot & ((1u << lane) - 1u));
+  if (pred && slot < cap) q[slot] = v;
+}
+__device__ __forceinline__ void
+warp_push_active64(uint32_t v, uint32_t* q, unsigned long long* count, uint64_t cap)
+{
+  unsigned const     mask = __activemask();
+  unsigned const     lane = threadIdx.x & 31u, leader = __ffs(mask) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(count, static_cast<unsigned long long>(__popc(mask)));
+  base                = __shfl_sync(mask, base, leader);
+  uint64_t const slot = base + __popc(mask & ((1u << lane) - 1u));
+  if (slot < cap) q[slot] = v;
+}
+
+__device__ __forceinline__ uint32_t
+snap_bit(uint32_t const* snap, uint32_t v)
+{
+  return (__ldcg(snap + (v >> 5)) >> (v & 31)) & 1u;
+}
+
+constexpr uint64_t TRIM_SMALL = 32; // row entries (both directions) a lane counts alone
+
+// Neighbours in adj[b, e) set in snap; four ids, then their four snap
+// words, in flight at once.
+__device__ __forceinline__ uint32_t
+count_live(uint32_t const* snap, uint32_t const* __restrict__ adj, uint64_t b, uint64_t e)
+{
+  uint32_t c = 0;
+  for (; b + 4 <= e; b += 4) {
+    uint32_t const x0 = adj[b], x1 = adj[b + 1], x2 = adj[b + 2], x3 = adj[b + 3];
+    c += snap_bit(snap, x0) + snap_bit(snap, x1) + snap_bit(snap, x2) + snap_bit(snap, x3);
+  }
+  for (; b < e; ++b) c += snap_bit(snap, adj[b]);
+  return c;
+}
+
+// First trim pass: live degrees of every undecided vertex; the dead ones
+// (no live in- or out-neighbour) are decided and queued.  A warp packs the
+// undecided vertices of 32 snap words, each lane counts one vertex, rows
+// longer than TRIM_SMALL are counted by the whole warp.
+__device__ __forceinline__ void
+trim_seed(fwbw_args const& a, fwbw_smem& sm, uint32_t* qout, unsigned long long* octr, uint32_t& dec, uint64_t& edges)
+{
+  unsigned const  lane   = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+  uint32_t const  words  = (a.n + 31) / 32;
+  uint32_t const  chunks = (words + 31) / 32;
+  uint32_t const* snap   = a.cand;
+  uint32_t* const cand   = sm.warp[wid].cand;
+  for (uint32_t ch = blockIdx.x * BU_WARPS + wid; ch < chunks; ch += gridDim.x * BU_WARPS) {
+    uint32_t const w    = ch * 32 + lane;
+    uint32_t       word = w < words ? __ldcg(snap + w) : 0u;
+    uint32_t const cnt  = __popc(word);
+    uint32_t       pos  = cnt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, pos, d);
+      if (lane >= static_cast<unsigned>(d)) pos += y;
+    }
+    uint32_t const total = __shfl_sync(0xFFFFFFFFu, pos, 31);
+    pos -= cnt;
+    for (; word; word &= word - 1) cand[pos++] = w * 32 + __ffs(word) - 1;
+    __syncwarp();
+    for (uint32_t r = 0; r < total; r += 32) {
+      uint32_t const i    = r + lane;
+      bool const     have = i < total;
+      uint32_t const x    = have ? cand[i] : 0u;
+      uint64_t       ob = 0, oe = 0, ib = 0, ie = 0;
+      if (have) ob = a.fh[x], oe = a.fh[x + 1], ib = a.bh[x], ie = a.bh[x + 1];
+      bool const small = have && (oe - ob) + (ie - ib) <= TRIM_SMALL;
+      uint32_t   co = 0, ci = 0;
+      if (small) {
+        co = count_live(snap, a.fc, ob, oe);
+        ci = count_live(snap, a.bc, ib, ie);
+      }
+      for (unsigned todo = __ballot_sync(0xFFFFFFFFu, have && !small); todo; todo &= todo - 1) {
+        unsigned const l  = __ffs(todo) - 1;
+        uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, ob, l), e0 = __shfl_sync(0xFFFFFFFFu, oe, l);
+        uint64_t const b1 = __shfl_sync(0xFFFFFFFFu, ib, l), e1 = __shfl_sync(0xFFFFFFFFu, ie, l);
+        uint32_t       xo = 0, xi = 0;
+        for (uint64_t e = b0 + lane; e < e0; e += 32) xo += snap_bit(snap, a.fc[e]);
+        for (uint64_t e = b1 + lane; e < e1; e += 32) xi += snap_bit(snap, a.bc[e]);
+#pragma unroll
+        for (int sh = 16; sh; sh >>= 1) xo += __shfl_xor_sync(0xFFFFFFFFu, xo, sh), xi += __shfl_xor_sync(0xFFFFFFFFu, xi, sh);
+        if (lane == l) co = xo, ci = xi;
+      }
+      bool const dead = have && (co == 0 || ci == 0);
+      if (dead) {
+        atomicAnd(a.und + (x >> 5), ~(1u << (x & 31)));
+        a.scc_id[x] = x;
+        ++dec;
+      } else if (have) {
+        a.outdeg[x] = co;
+        a.indeg[x]  = ci;
+      }
+      if (have) edges += (oe - ob) + (ie - ib);
+      warp_push64(dead, x, qout, octr, a.n);
+    }
+    __syncwarp();
+  }
+}
+
+// One trim push level: every queued vertex decrements its undecided
+// neighbours' live counts (out-neighbours' in-degree, in-neighbours'
+// out-degree); a neighbour whose count reaches 0 is decided and queued.
+__device__ __forceinline__ void
+trim_push(fwbw_args const& a, uint32_t const* qin, uint32_t qn, uint32_t* qout, unsigned long long* octr, uint32_t& dec, uint64_t& edges)
+{
+  unsigned const lane = threadIdx.x & 31u;
+  uint64_t const span = (static_cast<uint64_t>(qn) + 31) & ~31ull;
+  // w's und word already probed: decrement, decide and queue at 0
+  auto const hit = [&](uint32_t w, uint32_t word, uint32_t* deg) {
+    if (((word >> (w & 31)) & 1u) && atomicSub(deg + w, 1u) == 1u && bit_take(a.und, w)) {
+      a.scc_id[w] = w;
+      ++dec;
+      warp_push_active64(w, qout, octr, a.n);
+    }
+  };
+  // a lane's own row: four neighbour ids, then their four und words, in
+  // flight at once
+  auto const row = [&](uint32_t const* adj, uint64_t b, uint64_t e, uint32_t* deg) {
+    for (; b + 4 <= e; b += 4) {
+      uint32_t w[4], u[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) w[k] = adj[b + k];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) u[k] = __ldcg(a.und + (w[k] >> 5));
+#pragma unroll
+      for (int k = 0; k < 4; ++k) hit(w[k], u[k], deg);
+    }
+    for (; b < e; ++b) {
+      uint32_t const w = adj[b];
+      hit(w, __ldcg(a.und + (w >> 5)), deg);
+    }
+  };
+#pragma unroll 1
+  for (int dir = 0; dir < 2; ++dir) {
+    uint64_t const* head = dir ? a.bh : a.fh;
+    uint32_t const* adj  = dir ? a.bc : a.fc;
+    uint32_t*       deg  = dir ? a.outdeg : a.indeg;
+    for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * R_THREADS) {
+      bool const     have = t < qn;
+      uint32_t const u    = have ? __ldcg(qin + t) : 0u;
+      uint64_t       b = 0, e = 0;
+      if (have) b = head[u], e = head[u + 1];
+      bool const big = have && e - b >= TRIM_SMALL;
+      edges += e - b;
+      if (have && !big) row(adj, b, e, deg);
+      for (unsigned todo = __ballot_sync(0xFFFFFFFFu, big); todo; todo &= todo - 1) {
+        unsigned const l  = __ffs(todo) - 1;
+        uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b, l), e0 = __shfl_sync(0xFFFFFFFFu, e, l);
+        for (uint64_t x = b0 + lane; x < e0; x += 32) {
+          uint32_t const w = adj[x];
+          hit(w, __ldcg(a.und + (w >> 5)), deg);
+        }
+      }
+    }
+  }
+}
+
+// The trim fixpoint; levels continue the launch's numbering (glvl).
+__device__ __forceinline__ int
+run_trim(fwbw_args const& a, fwbw_smem& sm, uint32_t& glvl, unsigned long long& epoch)
+{
+  reach_state* const       st    = a.st;
+  unsigned long long const qmask = (1ull << a.qbits) - 1;
+  uint32_t                 dec   = 0;
+  uint64_t                 edges = 0;
+  uint32_t                 lvl   = 0;
+  int                      rc    = SEARCH_DONE;
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->lq[(glvl + 2) % 3] = 0;
+  trim_seed(a, sm, a.fb[(glvl + 1) & 1].q, &st->lq[(glvl + 1) % 3], dec, edges);
+  if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
+  ++glvl;
+  while (rc == SEARCH_DONE) {
+    uint64_t const qn = __ldcg(&st->lq[glvl % 3]) & qmask;
+    if (qn == 0) break;
+    if (lvl >= a.cap || qn > a.n) {
+      rc = SEARCH_CAPPED;
+      break;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->lq[(glvl + 2) % 3] = 0;
+    trim_push(a, a.fb[glvl & 1].q, static_cast<uint32_t>(qn), a.fb[(glvl + 1) & 1].q, &st->lq[(glvl + 1) % 3], dec, edges);
+    if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
+    ++lvl;
+    ++glvl;
+  }
+#pragma unroll
+  for (int sh = 16; sh; sh >>= 1) dec += __shfl_down_sync(0xFFFFFFFFu, dec, sh), edges += __shfl_down_sync(0xFFFFFFFFu, edges, sh);
+  if ((threadIdx.x & 31) == 0 && dec) atomicAdd(&st->trim_decided, dec);
+  if ((threadIdx.x & 31) == 0 && edges) atomicAdd(&st->trim_edges, static_cast<unsigned long long>(edges));
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->trim_levels = lvl;
+  return rc;
+}
+
 __global__ void __launch_bounds__(R_THREADS, 4)
 k_fwbw(fwbw_args a)
 {
   __shared__ fwbw_smem sm;
   reach_state* const   st    = a.st;
   unsigned long long   epoch = __ldcg(&a.bar->epoch);
-  uint32_t const       p     = a.pivot;
   uint32_t const       words = (a.n + 31) / 32;
+  uint32_t             p     = a.pivot;
+  if (p == static_cast<uint32_t>(PIVOT_FROM_DEVICE)) {
+    // trim_1_first's choice: largest in*out among its survivors; none
+    // (product 0) when it decided every vertex
+    uint64_t const prod = __ldcg(a.pv_prod);
+    uint32_t const id   = __ldcg(a.pv_id);
+    p                   = prod == 0 || id >= a.n ? a.n : id;
+  }
+  bool const search = p < a.n; // block-uniform
   if (threadIdx.x == 0) sm.buf_n = 0, sm.edges_bu = sm.cands_bu = 0;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    st->marks = 0;
+    st->t_ns[0] = globaltimer();
+    st->marks   = 0;
     stamp(a, 0);
     st->lq[0] = st->lq[1] = st->lq[2] = 0;
     st->mat_q                         = 0;
@@ -826,100 +1066,122 @@ k_fwbw(fwbw_args a)
     st->decided                       = 0;
     st->edges_bu = st->cands_bu = st->edges_td = 0;
     st->levels_fw = st->bu_fw = st->levels_bw = st->bu_bw = 0;
-    a.seed.q[0]                       = p;
-    a.seed.prefix[0]                  = 0;
+    st->pivot_used                                        = p;
+    st->trim_decided = st->trim_levels = st->und_left = 0;
+    st->trim_edges                                    = 0;
+    if (search) a.seed.q[0] = p, a.seed.prefix[0] = 0;
   }
-  // init: cand = und \ {p}, vis_a = vis_b = {p}; |und| per block
-  uint32_t c = 0;
-  for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) {
-    uint32_t const u   = __ldcg(a.und + w);
-    uint32_t const pin = w == (p >> 5) ? 1u << (p & 31) : 0u;
-    a.cand[w]          = u & ~pin;
-    a.vis_a[w]         = pin;
-    a.vis_b[w]         = pin;
-    c += __popc(u);
-  }
-  uint64_t tot;
-  block_exclusive_scan<uint64_t, R_THREADS>(c, &tot);
-  if (threadIdx.x == 0) a.partial[blockIdx.x] = tot;
+  int      rc   = SEARCH_DONE;
   uint32_t glvl = 0;
-  int      rc   = grid_sync(a.bar, epoch) ? SEARCH_DONE : SEARCH_FAILED;
-  if (rc == SEARCH_DONE) {
-    stamp(a, 8);
-    uint64_t s = 0;
-    for (uint32_t i = threadIdx.x; i < gridDim.x; i += R_THREADS) s += __ldcg(a.partial + i);
-    block_exclusive_scan<uint64_t, R_THREADS>(s, &tot);
-    uint32_t const n_und = static_cast<uint32_t>(tot);
-    // one inlined copy of the level loop, run for FW then BW
+  uint32_t id   = p;
+  if (search) {
+    // init: cand = und \ {p}, vis_a = vis_b = {p}; |und| per block
+    uint32_t c = 0;
+    for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) {
+      uint32_t const u   = __ldcg(a.und + w);
+      uint32_t const pin = w == (p >> 5) ? 1u << (p & 31) : 0u;
+      a.cand[w]          = u & ~pin;
+      a.vis_a[w]         = pin;
+      a.vis_b[w]         = pin;
+      c += __popc(u);
+    }
+    uint64_t tot;
+    block_exclusive_scan<uint64_t, R_THREADS>(c, &tot);
+    if (threadIdx.x == 0) a.partial[blockIdx.x] = tot;
+    rc = grid_sync(a.bar, epoch) ? SEARCH_DONE : SEARCH_FAILED;
+    if (rc == SEARCH_DONE) {
+      stamp(a, 8);
+      uint64_t s = 0;
+      for (uint32_t i = threadIdx.x; i < gridDim.x; i += R_THREADS) s += __ldcg(a.partial + i);
+      block_exclusive_scan<uint64_t, R_THREADS>(s, &tot);
+      uint32_t const n_und = static_cast<uint32_t>(tot);
+      // one inlined copy of the level loop, run for FW then BW
 #pragma unroll 1
-    for (int dir = 0; dir < 2 && rc == SEARCH_DONE; ++dir) {
-      if (dir) {
-        // BW: candidates are the FW-reached vertices except the pivot (each
-        // block clears its bit before its own first expansion)
-        if (threadIdx.x == 0) atomicAnd(a.vis_a + (p >> 5), ~(1u << (p & 31)));
-        __syncthreads();
-      }
-      rc = dir ? run_search<true>(a, sm, n_und, glvl, epoch) : run_search<false>(a, sm, n_und, glvl, epoch);
-    }
-  }
-  uint32_t id = p;
-  if (rc == SEARCH_DONE && a.min_ids) {
-    // smallest member = first set bit of vis_b.  Every block first looks at
-    // the same leading MIN_WORDS words (the SCC is usually dense there);
-    // only when they are all empty does the grid search the rest and meet
-    // at a barrier.  Every block reads the same words, so all take the
-    // same branch.
-    constexpr uint32_t MIN_WORDS = 4 * R_THREADS;
-    uint32_t           best      = UNDECIDED;
-    for (uint32_t w = threadIdx.x; w < MIN_WORDS && w < words; w += R_THREADS) {
-      uint32_t const s = __ldcg(a.vis_b + w);
-      if (s) {
-        best = w * 32 + (__ffs(s) - 1);
-        break;
+      for (int dir = 0; dir < 2 && rc == SEARCH_DONE; ++dir) {
+        if (dir) {
+          // BW: candidates are the FW-reached vertices except the pivot
+          // (each block clears its bit before its own first expansion)
+          if (threadIdx.x == 0) atomicAnd(a.vis_a + (p >> 5), ~(1u << (p & 31)));
+          __syncthreads();
+        }
+        rc = dir ? run_search<true>(a, sm, p, n_und, glvl, epoch) : run_search<false>(a, sm, p, n_und, glvl, epoch);
       }
     }
-    best = __reduce_min_sync(0xFFFFFFFFu, best);
-    if ((threadIdx.x & 31) == 0) sm.cnt = UNDECIDED;
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0 && best != UNDECIDED) atomicMin(&sm.cnt, best);
-    __syncthreads();
-    id = sm.cnt;
-    if (id == UNDECIDED) {
-      for (uint32_t w = MIN_WORDS + blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) {
+    if (rc == SEARCH_DONE && a.min_ids) {
+      // smallest member = first set bit of vis_b.  Every block first looks
+      // at the same leading MIN_WORDS words (the SCC is usually dense
+      // there); only when they are all empty does the grid search the rest
+      // and meet at a barrier.  Every block reads the same words, so all
+      // take the same branch.
+      constexpr uint32_t MIN_WORDS = 4 * R_THREADS;
+      uint32_t           best      = UNDECIDED;
+      for (uint32_t w = threadIdx.x; w < MIN_WORDS && w < words; w += R_THREADS) {
         uint32_t const s = __ldcg(a.vis_b + w);
         if (s) {
           best = w * 32 + (__ffs(s) - 1);
-          break; // later words of this thread only hold larger ids
+          break;
         }
       }
       best = __reduce_min_sync(0xFFFFFFFFu, best);
-      if ((threadIdx.x & 31) == 0 && best != UNDECIDED && best < __ldcg(&st->id)) atomicMin(&st->id, best);
-      if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
-      id = __ldcg(&st->id);
+      if ((threadIdx.x & 31) == 0) sm.cnt = UNDECIDED;
+      __syncthreads();
+      if ((threadIdx.x & 31) == 0 && best != UNDECIDED) atomicMin(&sm.cnt, best);
+      __syncthreads();
+      id = sm.cnt;
+      if (id == UNDECIDED) {
+        for (uint32_t w = MIN_WORDS + blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) {
+          uint32_t const s = __ldcg(a.vis_b + w);
+          if (s) {
+            best = w * 32 + (__ffs(s) - 1);
+            break; // later words of this thread only hold larger ids
+          }
+        }
+        best = __reduce_min_sync(0xFFFFFFFFu, best);
+        if ((threadIdx.x & 31) == 0 && best != UNDECIDED && best < __ldcg(&st->id)) atomicMin(&st->id, best);
+        if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
+        id = __ldcg(&st->id);
+      }
+    }
+    if (rc == SEARCH_DONE) {
+      // the SCC (vis_b) leaves und with its id; a warp loads 32 words at
+      // once, then for each non-empty one lane l writes vertex 32w + l (one
+      // coalesced 128-byte store per word).  With the trim tail every word
+      // of und is also copied to snap (cand).
+      unsigned const lane = threadIdx.x & 31u;
+      uint32_t       cnt  = 0;
+      for (uint32_t wb = (blockIdx.x * R_THREADS + threadIdx.x) & ~31u; wb < words; wb += gridDim.x * R_THREADS) {
+        uint32_t const w    = wb + lane;
+        uint32_t const mine = w < words ? __ldcg(a.vis_b + w) : 0u;
+        if (w < words && (mine || a.trim)) {
+          uint32_t const u = __ldcg(a.und + w) & ~mine;
+          if (mine) a.und[w] = u;
+          if (a.trim) a.cand[w] = u;
+          cnt += __popc(mine);
+        }
+        for (unsigned todo = __ballot_sync(0xFFFFFFFFu, mine != 0); todo; todo &= todo - 1) {
+          unsigned const j = __ffs(todo) - 1;
+          uint32_t const s = __shfl_sync(0xFFFFFFFFu, mine, j);
+          if ((s >> lane) & 1u) a.scc_id[(wb + j) * 32 + lane] = id;
+        }
+      }
+#pragma unroll
+      for (int sh = 16; sh; sh >>= 1) cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, sh);
+      if (lane == 0 && cnt) atomicAdd(&st->decided, cnt);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->t_ns[1] = globaltimer();
+    if (rc == SEARCH_DONE && a.trim) {
+      rc = grid_sync(a.bar, epoch) ? SEARCH_DONE : SEARCH_FAILED; // snap and und complete
+      if (rc == SEARCH_DONE) rc = run_trim(a, sm, glvl, epoch);
     }
   }
-  if (rc == SEARCH_DONE) {
-    // the SCC (vis_b) leaves und with its id: one warp per bitmap word,
-    // lane l writes vertex 32w + l (one coalesced 128-byte store per word)
-    // (a warp loads 32 words at once, then broadcasts each non-empty one)
-    unsigned const lane = threadIdx.x & 31u;
-    uint32_t       cnt  = 0;
-    for (uint32_t wb = (blockIdx.x * R_THREADS + threadIdx.x) & ~31u; wb < words; wb += gridDim.x * R_THREADS) {
-      uint32_t const w    = wb + lane;
-      uint32_t const mine = w < words ? __ldcg(a.vis_b + w) : 0u;
-      if (mine) {
-        a.und[w] &= ~mine;
-        cnt += __popc(mine);
-      }
-      for (unsigned todo = __ballot_sync(0xFFFFFFFFu, mine != 0); todo; todo &= todo - 1) {
-        unsigned const j = __ffs(todo) - 1;
-        uint32_t const s = __shfl_sync(0xFFFFFFFFu, mine, j);
-        if ((s >> lane) & 1u) a.scc_id[(wb + j) * 32 + lane] = id;
-      }
-    }
+  if (rc == SEARCH_DONE && a.trim) {
+    // undecided vertices left (und is final: after the trim's last barrier,
+    // or untouched when there was no pivot)
+    uint32_t c = 0;
+    for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) c += __popc(__ldcg(a.und + w));
 #pragma unroll
-    for (int sh = 16; sh; sh >>= 1) cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, sh);
-    if (lane == 0 && cnt) atomicAdd(&st->decided, cnt);
+    for (int sh = 16; sh; sh >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, sh);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(&st->und_left, c);
   }
   // statistics
   __syncthreads();
@@ -930,6 +1192,8 @@ k_fwbw(fwbw_args a)
     st->err     = rc == SEARCH_CAPPED ? 1u : 0u;
     st->bar_err = rc == SEARCH_FAILED ? 1u : 0u;
     if (rc != SEARCH_FAILED) a.bar->epoch = epoch; // every block completed the same barriers
+    if (!search) st->t_ns[1] = st->t_ns[0];
+    st->t_ns[2] = globaltimer();
     stamp(a, 9);
   }
 }
@@ -1085,6 +1349,130 @@ release_graphs(kspn_context* ctx)
   }
 }
 
+namespace {
+
+// Launches k_fwbw (pivot, or PIVOT_FROM_DEVICE; trim tail on or off) and
+// queues the copies of its results into the pinned state mirror; the
+// caller synchronises, then calls check_persistent.
+void
+launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t pivot, bool trim, kspn_options const& opt, kspn_stats* st, bool min_ids)
+{
+  auto&       ws   = ctx->ws;
+  auto* const rs   = reinterpret_cast<reach_state*>(ws.rstate);
+  auto* const hs   = reinterpret_cast<reach_state*>(ctx->h_state);
+  auto* const gbar = static_cast<grid_barrier*>(ws.gbar);
+  bool const  tr   = opt.trace && st && st->search_marks == 0;
+  fwbw_args   a{};
+  a.n           = g.n;
+  a.pivot       = pivot;
+  a.m           = g.m;
+  a.cap         = opt.max_levels ? opt.max_levels : g.n + 2;
+  a.min_ids     = min_ids ? 1u : 0u;
+  a.qbits       = bit_width64(g.n);
+  a.trace       = tr ? 1u : 0u;
+  a.alpha       = opt.bu_enter_div ? opt.bu_enter_div : 1;
+  a.beta        = opt.bu_leave_div ? opt.bu_leave_div : 1;
+  a.fh          = g.fh;
+  a.fc          = g.fc;
+  a.bh          = g.bh;
+  a.bc          = g.bc;
+  a.und         = und;
+  a.scc_id      = scc_id;
+  a.cand        = ws.mark;
+  a.vis_a       = ws.vis_a;
+  a.vis_b       = ws.vis_b;
+  a.fresh       = ws.fresh;
+  a.fb[0]       = { ws.q0, ws.prefix, ws.tile_start };
+  a.fb[1]       = { ws.q1, ws.prefix2, ws.tile_start2 };
+  a.seed        = { ws.seed_q, ws.seed_prefix, ws.tile_zero };
+  a.partial     = ws.blocks;
+  a.pv_prod     = ws.pivot + PV_FINAL;
+  a.pv_id       = reinterpret_cast<uint32_t const*>(ws.pivot + 4096) + PV_FINAL;
+  a.trim        = trim ? 1u : 0u;
+  a.indeg       = ws.indeg;
+  a.outdeg      = ws.outdeg;
+  a.bar         = gbar;
+  a.st          = rs;
+  a.stamp_phase = reinterpret_cast<uint32_t*>(static_cast<char*>(ws.rstate) + 2048);
+  a.stamp_ns    = reinterpret_cast<uint64_t*>(static_cast<char*>(ws.rstate) + 2048 + 4 * MARKS);
+  void* args[]  = { &a };
+  KSPN_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(&k_fwbw), dim3(fwbw_grid(ctx)), dim3(R_THREADS), args, 0, ctx->stream));
+  ctx->launches += 1;
+  // results, and the barrier's error word (read after the launch ended: a
+  // block that gave up may set it after block 0 finished)
+  auto* const hb = reinterpret_cast<uint32_t*>(static_cast<char*>(ctx->h_state) + 1024);
+  KSPN_CUDA(cudaMemcpyAsync(hs, rs, sizeof(reach_state), cudaMemcpyDeviceToHost, ctx->stream));
+  KSPN_CUDA(cudaMemcpyAsync(hb, &gbar->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+}
+
+// After the stream was synchronised: barrier failures and level caps.
+void
+check_persistent(kspn_context* ctx)
+{
+  auto* const hs = reinterpret_cast<reach_state*>(ctx->h_state);
+  auto* const hb = reinterpret_cast<uint32_t*>(static_cast<char*>(ctx->h_state) + 1024);
+  if (*hb || hs->bar_err) {
+    // counters of a launch that gave up are not epoch-aligned: start over
+    KSPN_CUDA(cudaMemsetAsync(ctx->ws.gbar, 0, sizeof(grid_barrier), ctx->stream));
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+    throw error{ KSPN_ERR_TIMEOUT, "reachability: grid barrier wait limit reached" };
+  }
+  if (hs->err) throw error{ KSPN_ERR_TIMEOUT, "reachability / trim: level cap exceeded" };
+}
+
+// Level statistics and phase stamps of the first FW-BW a call ran.
+void
+record_search_stats(kspn_context* ctx, kspn_options const& opt, kspn_stats* st)
+{
+  auto& ws = ctx->ws;
+  auto* hs = reinterpret_cast<reach_state*>(ctx->h_state);
+  if (opt.trace && st && st->search_marks == 0 && hs->marks) {
+    uint32_t const k = std::min<uint32_t>(hs->marks, MARKS);
+    KSPN_CUDA(cudaMemcpyAsync(st->search_phase, static_cast<char*>(ws.rstate) + 2048, 4 * k, cudaMemcpyDeviceToHost, ctx->stream));
+    KSPN_CUDA(cudaMemcpyAsync(st->search_ns, static_cast<char*>(ws.rstate) + 2048 + 4 * MARKS, 8 * k, cudaMemcpyDeviceToHost, ctx->stream));
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+    st->search_marks = k;
+  }
+  ctx->td_edges += hs->edges_td + hs->edges_bu;
+  if (st && st->levels_fw == 0 && st->levels_bw == 0) {
+    st->levels_fw        = hs->levels_fw;
+    st->levels_bw        = hs->levels_bw;
+    st->levels_bottom_up = hs->bu_fw + hs->bu_bw;
+  }
+}
+
+} // namespace
+
+bool
+resident_fits(dgraph const& g)
+{
+  return packed_counters_fit(g.n, g.m);
+}
+
+void
+fw_bw_trim_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, kspn_options const& opt, kspn_stats* st)
+{
+  launch_persistent(ctx, g, und, scc_id, static_cast<uint32_t>(PIVOT_FROM_DEVICE), true, opt, st, true);
+}
+
+resident_result
+fw_bw_trim_result(kspn_context* ctx, kspn_options const& opt, kspn_stats* st)
+{
+  check_persistent(ctx);
+  auto* hs = reinterpret_cast<reach_state*>(ctx->h_state);
+  record_search_stats(ctx, opt, st);
+  ctx->h_ctr64[0] += hs->trim_edges;
+  resident_result r;
+  r.pivot             = hs->pivot_used;
+  r.fwbw_decided      = hs->decided;
+  r.trim_decided      = hs->trim_decided;
+  r.trim_levels       = hs->trim_levels;
+  r.und_left          = hs->und_left;
+  uint64_t const span = hs->t_ns[2] > hs->t_ns[0] ? hs->t_ns[2] - hs->t_ns[0] : 0;
+  r.fwbw_share        = span ? static_cast<double>(hs->t_ns[1] - hs->t_ns[0]) / static_cast<double>(span) : 1.0;
+  return r;
+}
+
 uint32_t
 fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t pivot, kspn_options const& opt, kspn_stats* st, bool min_ids)
 {
@@ -1101,53 +1489,11 @@ fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint3
   hs->min_ids = min_ids ? 1u : 0u;
 
   uint32_t const words = (g.n + 31) / 32;
-  auto* const    gbar  = static_cast<grid_barrier*>(ws.gbar);
   if (!ctx->prof && packed_counters_fit(g.n, g.m)) {
     // the whole FW-BW on the device: one cooperative launch
-    bool const tr = opt.trace && st && st->search_marks == 0;
-    fwbw_args  a{};
-    a.n           = g.n;
-    a.pivot       = pivot;
-    a.m           = g.m;
-    a.cap         = hs->cap;
-    a.min_ids     = hs->min_ids;
-    a.qbits       = bit_width64(g.n);
-    a.trace       = tr ? 1u : 0u;
-    a.alpha       = hs->alpha;
-    a.beta        = hs->beta;
-    a.fh          = g.fh;
-    a.fc          = g.fc;
-    a.bh          = g.bh;
-    a.bc          = g.bc;
-    a.und         = und;
-    a.scc_id      = scc_id;
-    a.cand        = ws.mark;
-    a.vis_a       = ws.vis_a;
-    a.vis_b       = ws.vis_b;
-    a.fresh       = ws.fresh;
-    a.fb[0]       = { ws.q0, ws.prefix, ws.tile_start };
-    a.fb[1]       = { ws.q1, ws.prefix2, ws.tile_start2 };
-    a.seed        = { ws.seed_q, ws.seed_prefix, ws.tile_zero };
-    a.partial     = ws.blocks;
-    a.bar         = gbar;
-    a.st          = rs;
-    a.stamp_phase = reinterpret_cast<uint32_t*>(static_cast<char*>(ws.rstate) + 2048);
-    a.stamp_ns    = reinterpret_cast<uint64_t*>(static_cast<char*>(ws.rstate) + 2048 + 4 * MARKS);
-    void* args[]  = { &a };
-    KSPN_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(&k_fwbw), dim3(fwbw_grid(ctx)), dim3(R_THREADS), args, 0, ctx->stream));
-    ctx->launches += 1;
-    // results, and the barrier's error word (read after the launch ended:
-    // a block that gave up may set it after block 0 finished)
-    auto* const hb = reinterpret_cast<uint32_t*>(static_cast<char*>(ctx->h_state) + 1024);
-    KSPN_CUDA(cudaMemcpyAsync(hs, rs, sizeof(reach_state), cudaMemcpyDeviceToHost, ctx->stream));
-    KSPN_CUDA(cudaMemcpyAsync(hb, &gbar->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    launch_persistent(ctx, g, und, scc_id, pivot, false, opt, st, min_ids);
     KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
-    if (*hb || hs->bar_err) {
-      // counters of a launch that gave up are not epoch-aligned: start over
-      KSPN_CUDA(cudaMemsetAsync(gbar, 0, sizeof(grid_barrier), ctx->stream));
-      KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
-      throw error{ KSPN_ERR_TIMEOUT, "reachability: grid barrier wait limit reached" };
-    }
+    check_persistent(ctx);
   } else {
     // host-driven loop over the same kernels, expansion kernels bracketed
     // by CUDA events (kspn_options.profile)
@@ -1205,19 +1551,7 @@ fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint3
     KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
   }
   if (hs->err) throw error{ KSPN_ERR_TIMEOUT, "reachability: level cap exceeded" };
-  if (opt.trace && st && st->search_marks == 0 && hs->marks) {
-    uint32_t const k = std::min<uint32_t>(hs->marks, MARKS);
-    KSPN_CUDA(cudaMemcpyAsync(st->search_phase, static_cast<char*>(ws.rstate) + 2048, 4 * k, cudaMemcpyDeviceToHost, ctx->stream));
-    KSPN_CUDA(cudaMemcpyAsync(st->search_ns, static_cast<char*>(ws.rstate) + 2048 + 4 * MARKS, 8 * k, cudaMemcpyDeviceToHost, ctx->stream));
-    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
-    st->search_marks = k;
-  }
-  ctx->td_edges += hs->edges_td + hs->edges_bu;
-  if (st && st->levels_fw == 0 && st->levels_bw == 0) {
-    st->levels_fw        = hs->levels_fw;
-    st->levels_bw        = hs->levels_bw;
-    st->levels_bottom_up = hs->bu_fw + hs->bu_bw;
-  }
+  record_search_stats(ctx, opt, st);
   return hs->decided;
 }
 

@@ -58,8 +58,9 @@ pv_warp_reduce(pv x)
   }
   return x;
 }
+// block reduction of x into out_prod[slot] / out_id[slot]
 __device__ __forceinline__ void
-pv_block_store(pv x, uint64_t* out_prod, uint32_t* out_id)
+pv_block_store_at(pv x, uint64_t* out_prod, uint32_t* out_id, uint32_t slot)
 {
   __shared__ uint64_t sp[T_THREADS / 32];
   __shared__ uint32_t si[T_THREADS / 32];
@@ -70,8 +71,13 @@ pv_block_store(pv x, uint64_t* out_prod, uint32_t* out_id)
     pv y = { 0, NONE };
     if (threadIdx.x < T_THREADS / 32) y = { sp[threadIdx.x], si[threadIdx.x] };
     y = pv_warp_reduce(y);
-    if (threadIdx.x == 0) out_prod[blockIdx.x] = y.prod, out_id[blockIdx.x] = y.id;
+    if (threadIdx.x == 0) out_prod[slot] = y.prod, out_id[slot] = y.id;
   }
+}
+__device__ __forceinline__ void
+pv_block_store(pv x, uint64_t* out_prod, uint32_t* out_id)
+{
+  pv_block_store_at(x, out_prod, out_id, blockIdx.x);
 }
 
 // Final reduction of per-block pairs; result id in out_id[0] (NONE if no
@@ -141,6 +147,21 @@ k_trim_first(uint32_t n,
   for (int s = 16; s; s >>= 1) d += __shfl_down_sync(0xFFFFFFFFu, d, s);
   if ((threadIdx.x & 31) == 0 && d) atomicAdd(ctr + CTR_DECIDED, d);
   pv_block_store(best, blk_prod, blk_id);
+  // the last block to finish reduces every block's pair into PV_FINAL, so a
+  // later launch can read the pivot without a host round trip
+  __shared__ bool s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(ctr + CTR_PV_TICKET, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  pv x = { 0, NONE };
+  for (uint32_t i = threadIdx.x; i < gridDim.x; i += T_THREADS) x = pv_best(x, pv{ __ldcg(blk_prod + i), __ldcg(blk_id + i) });
+  pv_block_store_at(x, blk_prod, blk_id, PV_FINAL);
+  if (threadIdx.x == 0) ctr[CTR_PV_TICKET] = 0;
 }
 
 // ---------------------------------------------------------------- trim_1_normal
@@ -765,6 +786,18 @@ trim_1_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id
   ctx->h_ctr[CTR_AUX] = ctx->h_ctr[CTR_DECIDED];
   // no undecided vertex: the reference returns n (trim_1_local.hpp:21,44)
   return (prod == 0 || pivot == NONE) ? g.n : pivot;
+}
+
+void
+trim_1_first_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id)
+{
+  auto& ws = ctx->ws;
+  zero_counters(ctx);
+  prof_start(ctx);
+  k_trim_first<<<stream_grid(g.n), T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.bh, und, scc_id, nullptr, nullptr, nullptr, ws.ctr, ws.pivot, reinterpret_cast<uint32_t*>(ws.pivot + 4096));
+  prof_stop(ctx);
+  KSPN_CHECK_LAUNCH();
+  ctx->launches += 1;
 }
 
 uint32_t
