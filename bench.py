@@ -187,17 +187,18 @@ def run_kspn(args):
     st = K.Stats()
     for _ in range(args.warmup):
         ctx.scc_device(G.n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, opt, st)
-    step_stats = []
+    # one Stats per timed step, converted to dicts after the timed region
+    stats_objs = [K.Stats() for _ in range(args.steps)]
     barrier()
     l0 = ctx.launches
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         ev0.record(stream)
-        for _ in range(args.steps):
-            ctx.scc_device(G.n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, opt, st)
-            step_stats.append(st.as_dict())
+        for i in range(args.steps):
+            ctx.scc_device(G.n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, opt, stats_objs[i])
         ev1.record(stream)
         barrier()
+    step_stats = [s.as_dict() for s in stats_objs]
     launches = ctx.launches - l0
     ms = ev0.elapsed_time(ev1) / args.steps
     # phase stamps of the persistent searches (one extra step, not timed)
@@ -293,7 +294,7 @@ def run_kspn(args):
             "phases": {"decided": last["decided"], "ms": {k: round(v, 4) for k, v in last["ms"].items()}, "levels_fw": last["levels_fw"],
                        "levels_bw": last["levels_bw"], "bottom_up": last["levels_bottom_up"], "label_calls": last["label_calls"],
                        "edges_scanned": last["edges_scanned"], "trace": trace,
-                       "search_phase_ms": {{4: "expand", 5: "sweep", 7: "materialize", 8: "init", 9: "finalize"}.get(k, k): round(v, 4) for k, v in search_phases.items()},
+                       "search_phase_ms": {{4: "expand", 5: "sweep", 7: "materialize", 8: "init", 9: "end", 10: "finalize", 11: "trim_seed", 12: "trim_level"}.get(k, k): round(v, 4) for k, v in search_phases.items()},
                        "kernels": {k: {"ms": round(a[0] / prof_steps, 4), "GB/s": round(a[1] / (a[0] * 1e-3) / 1e9, 1) if a[0] else 0}
                                                                             for k, a in agg.items()}},
         }

@@ -118,7 +118,8 @@ typedef struct kspn_stats
    * first FW-BW's persistent launch after each phase, and the phase that
    * ended there: 0 launch start, 8 init, 4 expansion level (top-down),
    * 5 sweep level (bottom-up), 7 frontier built from a sweep's bitmap,
-   * 9 finalize. */
+   * 10 SCC written back, 11 trim live degrees + seeds, 12 trim push
+   * level, 9 launch end. */
   uint32_t search_marks;
   uint32_t search_phase[128];
   uint64_t search_ns[128];

@@ -322,10 +322,16 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
   // trim (id = itself), trim-2 (id = the smaller of the pair) and FW-BW
   // (id = smallest member) already name components canonically; label
   // searches name them after their root, so only then is a relabel needed
-  if (label_ran) canonicalise(ctx, g.n, scc_id, ws.label, true);
-  add(KSPN_PHASE_CANON, 0);
-  KSPN_CUDA(cudaEventRecord(t_end, ctx->stream));
-  KSPN_CUDA(cudaEventSynchronize(t_end));
+  if (und_checked) {
+    // everything was decided by the resident launch, whose completion
+    // event (now ev[0]) the host already waited for: no further sync
+    t_end = ctx->ev[0];
+  } else {
+    if (label_ran) canonicalise(ctx, g.n, scc_id, ws.label, true);
+    add(KSPN_PHASE_CANON, 0);
+    KSPN_CUDA(cudaEventRecord(t_end, ctx->stream));
+    KSPN_CUDA(cudaEventSynchronize(t_end));
+  }
   if (st) {
     float ms = 0;
     KSPN_CUDA(cudaEventElapsedTime(&ms, t_begin, t_end));

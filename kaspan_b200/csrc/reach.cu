@@ -571,15 +571,18 @@ struct fwbw_args
 // Block-shared scratch of the persistent kernel.
 struct fwbw_smem
 {
-  bu_warp_smem          warp[BU_WARPS]; // bottom-up chunks; a top-down tile's rows alias it
-  uint32_t              buf[BU_BUF];    // block queue of a top-down tile
+  // bottom-up and trim per-warp buffers; during a top-down level the same
+  // bytes hold the tile's row map (tile_rows) and the block queue (buf)
+  bu_warp_smem warp[BU_WARPS];
   uint32_t              tile_i[2];
   uint32_t              buf_n;
   uint32_t              cnt;
   unsigned long long    old;
   unsigned long long    edges_bu, cands_bu; // bottom-up statistics of the launch
+  __device__ __forceinline__ uint32_t* tile_rows() { return reinterpret_cast<uint32_t*>(warp); }
+  __device__ __forceinline__ uint32_t* buf() { return reinterpret_cast<uint32_t*>(warp) + EX_TILE; }
 };
-static_assert(sizeof(bu_warp_smem) * BU_WARPS >= EX_TILE * sizeof(uint32_t), "tile rows must fit the warp buffers");
+static_assert(sizeof(bu_warp_smem) * BU_WARPS >= (EX_TILE + BU_BUF) * sizeof(uint32_t), "tile rows and block queue must fit the warp buffers");
 static_assert(BU_BUF == EX_TILE && BU_BUF % R_THREADS == 0, "flush: whole runs per thread");
 
 __device__ __forceinline__ uint64_t
@@ -614,7 +617,7 @@ put_tile_starts(uint32_t* tile_start, uint64_t p, uint64_t d, uint32_t i, uint64
   for (uint64_t t = (p + EX_TILE - 1) / EX_TILE; t * EX_TILE < end; ++t) tile_start[t] = i;
 }
 
-// Appends the block queue (sm.buf[0, sm.buf_n)) to a scanned frontier.
+// Appends the block queue (sm.buf()[0, sm.buf_n)) to a scanned frontier.
 // Thread t owns entries [8t, 8t + 8); one block scan of the degree sums
 // and one packed atomic give every entry its queue slot and edge prefix.
 // Degrees are read twice (the second time from cache) rather than held in
@@ -632,7 +635,7 @@ flush_scanned(fwbw_smem& sm, frontier_buf const& out, unsigned long long* ctr, u
 #pragma unroll
     for (int k = 0; k < K; ++k)
       if (k < k1) {
-        uint32_t const v = sm.buf[i0 + k];
+        uint32_t const v = sm.buf()[i0 + k];
         sum += head[v + 1] - head[v];
       }
     uint64_t       tot;
@@ -644,7 +647,7 @@ flush_scanned(fwbw_smem& sm, frontier_buf const& out, unsigned long long* ctr, u
     uint32_t                 pos  = static_cast<uint32_t>(pos0);
     uint64_t                 p    = (old >> qbits) + off;
     for (uint32_t k = 0; k < k1 && pos0 + k < qcap && p < ecap; ++k, ++pos) {
-      uint32_t const v = sm.buf[i0 + k];
+      uint32_t const v = sm.buf()[i0 + k];
       uint64_t const d = head[v + 1] - head[v];
       out.q[pos]       = v;
       out.prefix[pos]  = p;
@@ -778,10 +781,10 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
       int const      per   = EX_ITEMS / static_cast<int>(parts);
       uint32_t const units = ntiles * parts;
       take_op const  op{ avail, mark };
-      block_queue    bq{ sm.buf, &sm.buf_n };
+      block_queue    bq{ sm.buf(), &sm.buf_n };
       for (uint32_t unit = blockIdx.x; unit < units; unit += gridDim.x) {
         int const part = static_cast<int>(unit % parts);
-        expand_tile(unit / parts, ntiles, fin.q, qn, mf, fin.prefix, fin.tile_start, td_head, td_adj, reinterpret_cast<uint32_t*>(sm.warp), sm.tile_i, bq, op, part * per, part * per + per);
+        expand_tile(unit / parts, ntiles, fin.q, qn, mf, fin.prefix, fin.tile_start, td_head, td_adj, sm.tile_rows(), sm.tile_i, bq, op, part * per, part * per + per);
         flush_scanned(sm, fout, octr, a.qbits, td_head, a.n, a.m);
       }
     } else {
@@ -1017,6 +1020,7 @@ run_trim(fwbw_args const& a, fwbw_smem& sm, uint32_t& glvl, unsigned long long& 
   if (blockIdx.x == 0 && threadIdx.x == 0) st->lq[(glvl + 2) % 3] = 0;
   trim_seed(a, sm, a.fb[(glvl + 1) & 1].q, &st->lq[(glvl + 1) % 3], dec, edges);
   if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
+  stamp(a, 11);
   ++glvl;
   while (rc == SEARCH_DONE) {
     uint64_t const qn = __ldcg(&st->lq[glvl % 3]) & qmask;
@@ -1028,12 +1032,13 @@ run_trim(fwbw_args const& a, fwbw_smem& sm, uint32_t& glvl, unsigned long long& 
     if (blockIdx.x == 0 && threadIdx.x == 0) st->lq[(glvl + 2) % 3] = 0;
     trim_push(a, a.fb[glvl & 1].q, static_cast<uint32_t>(qn), a.fb[(glvl + 1) & 1].q, &st->lq[(glvl + 1) % 3], dec, edges);
     if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
+    stamp(a, 12);
     ++lvl;
     ++glvl;
   }
 #pragma unroll
   for (int sh = 16; sh; sh >>= 1) dec += __shfl_down_sync(0xFFFFFFFFu, dec, sh), edges += __shfl_down_sync(0xFFFFFFFFu, edges, sh);
-  if ((threadIdx.x & 31) == 0 && dec) atomicAdd(&st->trim_decided, dec);
+  if ((threadIdx.x & 31) == 0 && dec) atomicAdd(&st->trim_decided, dec), atomicSub(&st->und_left, dec);
   if ((threadIdx.x & 31) == 0 && edges) atomicAdd(&st->trim_edges, static_cast<unsigned long long>(edges));
   if (blockIdx.x == 0 && threadIdx.x == 0) st->trim_levels = lvl;
   return rc;
@@ -1148,14 +1153,14 @@ k_fwbw(fwbw_args a)
       // coalesced 128-byte store per word).  With the trim tail every word
       // of und is also copied to snap (cand).
       unsigned const lane = threadIdx.x & 31u;
-      uint32_t       cnt  = 0;
+      uint32_t       cnt = 0, left = 0;
       for (uint32_t wb = (blockIdx.x * R_THREADS + threadIdx.x) & ~31u; wb < words; wb += gridDim.x * R_THREADS) {
         uint32_t const w    = wb + lane;
         uint32_t const mine = w < words ? __ldcg(a.vis_b + w) : 0u;
         if (w < words && (mine || a.trim)) {
           uint32_t const u = __ldcg(a.und + w) & ~mine;
           if (mine) a.und[w] = u;
-          if (a.trim) a.cand[w] = u;
+          if (a.trim) a.cand[w] = u, left += __popc(u);
           cnt += __popc(mine);
         }
         for (unsigned todo = __ballot_sync(0xFFFFFFFFu, mine != 0); todo; todo &= todo - 1) {
@@ -1165,18 +1170,20 @@ k_fwbw(fwbw_args a)
         }
       }
 #pragma unroll
-      for (int sh = 16; sh; sh >>= 1) cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, sh);
+      for (int sh = 16; sh; sh >>= 1) cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, sh), left += __shfl_down_sync(0xFFFFFFFFu, left, sh);
       if (lane == 0 && cnt) atomicAdd(&st->decided, cnt);
+      if (lane == 0 && left) atomicAdd(&st->und_left, left); // the trim subtracts its decisions
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) st->t_ns[1] = globaltimer();
+    stamp(a, 10);
     if (rc == SEARCH_DONE && a.trim) {
       rc = grid_sync(a.bar, epoch) ? SEARCH_DONE : SEARCH_FAILED; // snap and und complete
       if (rc == SEARCH_DONE) rc = run_trim(a, sm, glvl, epoch);
     }
   }
-  if (rc == SEARCH_DONE && a.trim) {
-    // undecided vertices left (und is final: after the trim's last barrier,
-    // or untouched when there was no pivot)
+  if (!search && a.trim) {
+    // no pivot: und is untouched, count it (with a pivot, und_left is the
+    // finalize pass's count minus the trim's decisions)
     uint32_t c = 0;
     for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) c += __popc(__ldcg(a.und + w));
 #pragma unroll

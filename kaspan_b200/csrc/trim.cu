@@ -92,6 +92,8 @@ k_pv_final(uint32_t nb, uint64_t* prod, uint32_t* id)
 }
 
 // ---------------------------------------------------------------- trim_1_first
+constexpr int TF_ITEMS = 4; // vertices per thread per pass of k_trim_first
+
 __global__ void __launch_bounds__(T_THREADS)
 k_trim_first(uint32_t n,
              uint64_t const* __restrict__ fh,
@@ -112,33 +114,42 @@ k_trim_first(uint32_t n,
   block_queue    bq{ s_buf, &s_n };
   pv             best = { 0, NONE };
   uint32_t       dec  = 0;
-  uint64_t const span = (static_cast<uint64_t>(n) + T_THREADS - 1) / T_THREADS * T_THREADS;
-  for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * T_THREADS; base < span; base += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
-    uint64_t const t     = base + threadIdx.x;
-    uint32_t const v     = static_cast<uint32_t>(t);
-    bool const     valid = t < n;
-    uint64_t       out = 0, in = 0;
-    if (valid) {
-      out = fh[v + 1] - fh[v];
-      in  = bh[v + 1] - bh[v];
+  // a pass covers TF_ITEMS slices of T_THREADS vertices; all offset loads
+  // of a pass are issued before any is used
+  uint64_t const pass     = static_cast<uint64_t>(T_THREADS) * TF_ITEMS;
+  for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * pass; base < n; base += static_cast<uint64_t>(gridDim.x) * pass) {
+    uint64_t f0[TF_ITEMS], f1[TF_ITEMS], b0[TF_ITEMS], b1[TF_ITEMS];
+#pragma unroll
+    for (int k = 0; k < TF_ITEMS; ++k) {
+      uint64_t const t = base + k * T_THREADS + threadIdx.x;
+      f0[k] = f1[k] = b0[k] = b1[k] = 0;
+      if (t < n) f0[k] = fh[t], f1[k] = fh[t + 1], b0[k] = bh[t], b1[k] = bh[t + 1];
     }
-    bool const     trimmed = valid && (in == 0 || out == 0);
-    bool const     live    = valid && !trimmed;
-    unsigned const word    = __ballot_sync(0xFFFFFFFFu, live);
-    if ((threadIdx.x & 31) == 0 && t < n) und[v >> 5] = word; // t = the warp's first vertex
-    if (valid) scc_id[v] = trimmed ? v : UNDECIDED;
-    if (live) {
-      if (indeg) indeg[v] = static_cast<uint32_t>(in);
-      if (outdeg) outdeg[v] = static_cast<uint32_t>(out);
-      uint64_t const prod = in * out;
-      if (prod > best.prod) best = { prod, v }; // ascending v: first strict max wins
+#pragma unroll
+    for (int k = 0; k < TF_ITEMS; ++k) {
+      uint64_t const t       = base + k * T_THREADS + threadIdx.x;
+      uint32_t const v       = static_cast<uint32_t>(t);
+      bool const     valid   = t < n;
+      uint64_t const out     = f1[k] - f0[k];
+      uint64_t const in      = b1[k] - b0[k];
+      bool const     trimmed = valid && (in == 0 || out == 0);
+      bool const     live    = valid && !trimmed;
+      unsigned const word    = __ballot_sync(0xFFFFFFFFu, live);
+      if ((threadIdx.x & 31) == 0 && t < n) und[v >> 5] = word; // t = the warp's first vertex
+      if (valid) scc_id[v] = trimmed ? v : UNDECIDED;
+      if (live) {
+        if (indeg) indeg[v] = static_cast<uint32_t>(in);
+        if (outdeg) outdeg[v] = static_cast<uint32_t>(out);
+        uint64_t const prod = in * out;
+        if (prod > best.prod) best = { prod, v }; // ascending v: first strict max wins
+      }
+      if (queue) {
+        bq.push(trimmed, v);
+        __syncthreads();
+        if (s_n > DENSE_BUF - T_THREADS) bq.flush(queue, ctr + CTR_Q0, &s_base);
+      }
+      dec += trimmed;
     }
-    if (queue) {
-      bq.push(trimmed, v);
-      __syncthreads();
-      if (s_n > DENSE_BUF - T_THREADS) bq.flush(queue, ctr + CTR_Q0, &s_base);
-    }
-    dec += trimmed;
   }
   if (queue) bq.flush(queue, ctr + CTR_Q0, &s_base);
   // decided count
@@ -766,7 +777,7 @@ trim_1_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id
 {
   auto& ws = ctx->ws;
   zero_counters(ctx);
-  unsigned const nb = stream_grid(g.n);
+  unsigned const nb = stream_grid((static_cast<uint64_t>(g.n) + TF_ITEMS - 1) / TF_ITEMS);
   prof_start(ctx);
   k_trim_first<<<nb, T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.bh, und, scc_id, init_degrees ? ws.indeg : nullptr, init_degrees ? ws.outdeg : nullptr, queue_out, ws.ctr, ws.pivot, reinterpret_cast<uint32_t*>(ws.pivot + 4096));
   prof_stop(ctx);
@@ -788,13 +799,13 @@ trim_1_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id
   return (prod == 0 || pivot == NONE) ? g.n : pivot;
 }
 
+// (the caller has zeroed ws.ctr)
 void
 trim_1_first_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id)
 {
   auto& ws = ctx->ws;
-  zero_counters(ctx);
   prof_start(ctx);
-  k_trim_first<<<stream_grid(g.n), T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.bh, und, scc_id, nullptr, nullptr, nullptr, ws.ctr, ws.pivot, reinterpret_cast<uint32_t*>(ws.pivot + 4096));
+  k_trim_first<<<stream_grid((static_cast<uint64_t>(g.n) + TF_ITEMS - 1) / TF_ITEMS), T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.bh, und, scc_id, nullptr, nullptr, nullptr, ws.ctr, ws.pivot, reinterpret_cast<uint32_t*>(ws.pivot + 4096));
   prof_stop(ctx);
   KSPN_CHECK_LAUNCH();
   ctx->launches += 1;
