@@ -264,7 +264,7 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
     if (!ctx->prof && resident_fits(g)) {
       // trim_1_first, then FW-BW and the trim fixpoint in ONE persistent
       // launch that takes the pivot from device memory: one host sync
-      trim_1_first_async(ctx, g, und, scc_id);
+      trim_1_first_async(ctx, g, und);
       KSPN_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
       fw_bw_trim_async(ctx, g, und, scc_id, opt, st);
       KSPN_CUDA(cudaMemcpyAsync(ctx->h_ctr, ws.ctr, 64 * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));

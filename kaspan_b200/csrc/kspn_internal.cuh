@@ -338,7 +338,8 @@ int  fail(kspn_context* ctx, error const& e);
 // trim.cu
 // reach.cu: the resident start of the FAST pipeline -- FW-BW from
 // trim_1_first's pivot (left on the device) and the trim-1 fixpoint in one
-// persistent launch, no host sync; results after the stream synchronised.
+// persistent launch, which then writes every vertex's id (trim_1_first_async
+// writes none); no host sync; results after the stream synchronised.
 struct resident_result
 {
   uint32_t pivot = 0, fwbw_decided = 0, trim_decided = 0, trim_levels = 0, und_left = 0;
@@ -349,7 +350,7 @@ void            fw_bw_trim_async(kspn_context* ctx, dgraph const& g, uint32_t* u
 resident_result fw_bw_trim_result(kspn_context* ctx, kspn_options const& opt, kspn_stats* st);
 
 uint32_t trim_1_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* queue_out, uint32_t* queue_count_host, bool init_degrees);
-void     trim_1_first_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id); // ws.ctr zeroed by the caller; no host sync: decided in ws.ctr, pivot in PV_FINAL
+void     trim_1_first_async(kspn_context* ctx, dgraph const& g, uint32_t* und); // ws.ctr zeroed by the caller; writes no ids; no host sync: decided in ws.ctr, pivot in PV_FINAL
 uint32_t trim_1_normal(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id);
 uint32_t trim_fixpoint(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, bool degrees_from_first, uint32_t seed_count);
 uint32_t trim_exhaustive_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* outdeg, uint32_t* indeg);

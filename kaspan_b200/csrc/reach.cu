@@ -92,6 +92,7 @@ struct reach_state
   uint32_t           trim_levels;  // its push levels
   uint32_t           und_left;     // undecided vertices when the launch ended
   unsigned long long trim_edges;   // adjacency entries the trim tail read
+  unsigned long long list_n;       // undecided vertices listed for the trim tail
   unsigned long long t_ns[3];      // %globaltimer: launch start, FW-BW end, trim end
 };
 
@@ -239,7 +240,7 @@ constexpr int BU_STEPS = 32; // neighbours a candidate checks itself before its 
 // Per-warp shared memory of the sweep.
 struct bu_warp_smem
 {
-  uint32_t cand[32 * 32]; // the warp's chunk (32 words = 1024 vertices), packed
+  uint16_t cand[32 * 32]; // the warp's chunk (32 words = 1024 vertices) packed, as offsets in the chunk
   uint32_t found[32];     // found bits per word of the chunk
 };
 
@@ -288,7 +289,7 @@ bu_sweep_warp(uint32_t first,
     while (word) {
       uint32_t const bb = __ffs(word) - 1;
       word &= word - 1;
-      sm.cand[pos++] = w * 32 + bb;
+      sm.cand[pos++] = static_cast<uint16_t>(lane * 32 + bb);
     }
     sm.found[lane] = 0;
     __syncwarp();
@@ -301,7 +302,7 @@ bu_sweep_warp(uint32_t first,
       for (int k = 0; k < BU_ILP; ++k) {
         uint32_t const i = r + k * 32 + lane;
         live[k]          = i < total;
-        v[k]             = live[k] ? sm.cand[i] : 0u;
+        v[k]             = live[k] ? c * 1024 + sm.cand[i] : 0u;
         b[k] = e[k] = 0;
         if (live[k]) b[k] = head[v[k]], e[k] = head[v[k] + 1];
         found[k] = false;
@@ -560,6 +561,7 @@ struct fwbw_args
   uint64_t const*    pv_prod;
   uint32_t const*    pv_id;
   uint32_t           trim;
+  uint32_t           ids_at_end; // resident launch: write every vertex's id at the end
   uint32_t*          indeg;
   uint32_t*          outdeg;
   grid_barrier*      bar;
@@ -884,68 +886,49 @@ count_live(uint32_t const* snap, uint32_t const* __restrict__ adj, uint64_t b, u
   return c;
 }
 
-// First trim pass: live degrees of every undecided vertex; the dead ones
-// (no live in- or out-neighbour) are decided and queued.  A warp packs the
-// undecided vertices of 32 snap words, each lane counts one vertex, rows
-// longer than TRIM_SMALL are counted by the whole warp.
+// First trim pass: live degrees of every listed undecided vertex; the dead
+// ones (no live in- or out-neighbour) are decided and queued.  A lane
+// counts one vertex; rows longer than TRIM_SMALL are counted by the whole
+// warp.
 __device__ __forceinline__ void
-trim_seed(fwbw_args const& a, fwbw_smem& sm, uint32_t* qout, unsigned long long* octr, uint32_t& dec, uint64_t& edges)
+trim_seed(fwbw_args const& a, uint32_t const* list, uint64_t list_n, uint32_t* qout, unsigned long long* octr, uint32_t& dec, uint64_t& edges)
 {
-  unsigned const  lane   = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-  uint32_t const  words  = (a.n + 31) / 32;
-  uint32_t const  chunks = (words + 31) / 32;
-  uint32_t const* snap   = a.cand;
-  uint32_t* const cand   = sm.warp[wid].cand;
-  for (uint32_t ch = blockIdx.x * BU_WARPS + wid; ch < chunks; ch += gridDim.x * BU_WARPS) {
-    uint32_t const w    = ch * 32 + lane;
-    uint32_t       word = w < words ? __ldcg(snap + w) : 0u;
-    uint32_t const cnt  = __popc(word);
-    uint32_t       pos  = cnt;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, pos, d);
-      if (lane >= static_cast<unsigned>(d)) pos += y;
+  unsigned const  lane = threadIdx.x & 31u;
+  uint32_t const* snap = a.cand;
+  uint64_t const  span = (list_n + 31) & ~31ull;
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * R_THREADS) {
+    bool const     have = t < list_n;
+    uint32_t const x    = have ? __ldcg(list + t) : 0u;
+    uint64_t       ob = 0, oe = 0, ib = 0, ie = 0;
+    if (have) ob = a.fh[x], oe = a.fh[x + 1], ib = a.bh[x], ie = a.bh[x + 1];
+    bool const small = have && (oe - ob) + (ie - ib) <= TRIM_SMALL;
+    uint32_t   co = 0, ci = 0;
+    if (small) {
+      co = count_live(snap, a.fc, ob, oe);
+      ci = count_live(snap, a.bc, ib, ie);
     }
-    uint32_t const total = __shfl_sync(0xFFFFFFFFu, pos, 31);
-    pos -= cnt;
-    for (; word; word &= word - 1) cand[pos++] = w * 32 + __ffs(word) - 1;
-    __syncwarp();
-    for (uint32_t r = 0; r < total; r += 32) {
-      uint32_t const i    = r + lane;
-      bool const     have = i < total;
-      uint32_t const x    = have ? cand[i] : 0u;
-      uint64_t       ob = 0, oe = 0, ib = 0, ie = 0;
-      if (have) ob = a.fh[x], oe = a.fh[x + 1], ib = a.bh[x], ie = a.bh[x + 1];
-      bool const small = have && (oe - ob) + (ie - ib) <= TRIM_SMALL;
-      uint32_t   co = 0, ci = 0;
-      if (small) {
-        co = count_live(snap, a.fc, ob, oe);
-        ci = count_live(snap, a.bc, ib, ie);
-      }
-      for (unsigned todo = __ballot_sync(0xFFFFFFFFu, have && !small); todo; todo &= todo - 1) {
-        unsigned const l  = __ffs(todo) - 1;
-        uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, ob, l), e0 = __shfl_sync(0xFFFFFFFFu, oe, l);
-        uint64_t const b1 = __shfl_sync(0xFFFFFFFFu, ib, l), e1 = __shfl_sync(0xFFFFFFFFu, ie, l);
-        uint32_t       xo = 0, xi = 0;
-        for (uint64_t e = b0 + lane; e < e0; e += 32) xo += snap_bit(snap, a.fc[e]);
-        for (uint64_t e = b1 + lane; e < e1; e += 32) xi += snap_bit(snap, a.bc[e]);
+    for (unsigned todo = __ballot_sync(0xFFFFFFFFu, have && !small); todo; todo &= todo - 1) {
+      unsigned const l  = __ffs(todo) - 1;
+      uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, ob, l), e0 = __shfl_sync(0xFFFFFFFFu, oe, l);
+      uint64_t const b1 = __shfl_sync(0xFFFFFFFFu, ib, l), e1 = __shfl_sync(0xFFFFFFFFu, ie, l);
+      uint32_t       xo = 0, xi = 0;
+      for (uint64_t e = b0 + lane; e < e0; e += 32) xo += snap_bit(snap, a.fc[e]);
+      for (uint64_t e = b1 + lane; e < e1; e += 32) xi += snap_bit(snap, a.bc[e]);
 #pragma unroll
-        for (int sh = 16; sh; sh >>= 1) xo += __shfl_xor_sync(0xFFFFFFFFu, xo, sh), xi += __shfl_xor_sync(0xFFFFFFFFu, xi, sh);
-        if (lane == l) co = xo, ci = xi;
-      }
-      bool const dead = have && (co == 0 || ci == 0);
-      if (dead) {
-        atomicAnd(a.und + (x >> 5), ~(1u << (x & 31)));
-        a.scc_id[x] = x;
-        ++dec;
-      } else if (have) {
-        a.outdeg[x] = co;
-        a.indeg[x]  = ci;
-      }
-      if (have) edges += (oe - ob) + (ie - ib);
-      warp_push64(dead, x, qout, octr, a.n);
+      for (int sh = 16; sh; sh >>= 1) xo += __shfl_xor_sync(0xFFFFFFFFu, xo, sh), xi += __shfl_xor_sync(0xFFFFFFFFu, xi, sh);
+      if (lane == l) co = xo, ci = xi;
     }
-    __syncwarp();
+    bool const dead = have && (co == 0 || ci == 0);
+    if (dead) {
+      atomicAnd(a.und + (x >> 5), ~(1u << (x & 31)));
+      if (!a.ids_at_end) a.scc_id[x] = x;
+      ++dec;
+    } else if (have) {
+      a.outdeg[x] = co;
+      a.indeg[x]  = ci;
+    }
+    if (have) edges += (oe - ob) + (ie - ib);
+    warp_push64(dead, x, qout, octr, a.n);
   }
 }
 
@@ -960,7 +943,7 @@ trim_push(fwbw_args const& a, uint32_t const* qin, uint32_t qn, uint32_t* qout, 
   // w's und word already probed: decrement, decide and queue at 0
   auto const hit = [&](uint32_t w, uint32_t word, uint32_t* deg) {
     if (((word >> (w & 31)) & 1u) && atomicSub(deg + w, 1u) == 1u && bit_take(a.und, w)) {
-      a.scc_id[w] = w;
+      if (!a.ids_at_end) a.scc_id[w] = w;
       ++dec;
       warp_push_active64(w, qout, octr, a.n);
     }
@@ -1009,7 +992,7 @@ trim_push(fwbw_args const& a, uint32_t const* qin, uint32_t qn, uint32_t* qout, 
 
 // The trim fixpoint; levels continue the launch's numbering (glvl).
 __device__ __forceinline__ int
-run_trim(fwbw_args const& a, fwbw_smem& sm, uint32_t& glvl, unsigned long long& epoch)
+run_trim(fwbw_args const& a, uint32_t& glvl, unsigned long long& epoch)
 {
   reach_state* const       st    = a.st;
   unsigned long long const qmask = (1ull << a.qbits) - 1;
@@ -1018,7 +1001,8 @@ run_trim(fwbw_args const& a, fwbw_smem& sm, uint32_t& glvl, unsigned long long& 
   uint32_t                 lvl   = 0;
   int                      rc    = SEARCH_DONE;
   if (blockIdx.x == 0 && threadIdx.x == 0) st->lq[(glvl + 2) % 3] = 0;
-  trim_seed(a, sm, a.fb[(glvl + 1) & 1].q, &st->lq[(glvl + 1) % 3], dec, edges);
+  // the finalize pass listed the undecided vertices in fb[glvl & 1].q
+  trim_seed(a, a.fb[glvl & 1].q, __ldcg(&st->list_n), a.fb[(glvl + 1) & 1].q, &st->lq[(glvl + 1) % 3], dec, edges);
   if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
   stamp(a, 11);
   ++glvl;
@@ -1036,12 +1020,45 @@ run_trim(fwbw_args const& a, fwbw_smem& sm, uint32_t& glvl, unsigned long long& 
     ++lvl;
     ++glvl;
   }
-#pragma unroll
-  for (int sh = 16; sh; sh >>= 1) dec += __shfl_down_sync(0xFFFFFFFFu, dec, sh), edges += __shfl_down_sync(0xFFFFFFFFu, edges, sh);
-  if ((threadIdx.x & 31) == 0 && dec) atomicAdd(&st->trim_decided, dec), atomicSub(&st->und_left, dec);
-  if ((threadIdx.x & 31) == 0 && edges) atomicAdd(&st->trim_edges, static_cast<unsigned long long>(edges));
+  // one atomic per block for each tally
+  uint64_t d_all, e_all;
+  block_exclusive_scan<uint64_t, R_THREADS>(dec, &d_all);
+  block_exclusive_scan<uint64_t, R_THREADS>(edges, &e_all);
+  if (threadIdx.x == 0 && d_all) atomicAdd(&st->trim_decided, static_cast<uint32_t>(d_all)), atomicSub(&st->und_left, static_cast<uint32_t>(d_all));
+  if (threadIdx.x == 0 && e_all) atomicAdd(&st->trim_edges, static_cast<unsigned long long>(e_all));
   if (blockIdx.x == 0 && threadIdx.x == 0) st->trim_levels = lvl;
   return rc;
+}
+
+// All ids from the bitmaps: a warp covers 32 words (1024 vertices), lane l
+// writing vertices 128j + 4l .. +3 of them (512 contiguous bytes per store
+// instruction; 16-byte stores when the output is 16-byte aligned).
+__device__ __forceinline__ void
+write_ids(fwbw_args const& a, uint32_t words, bool search, uint32_t scc)
+{
+  unsigned const lane = threadIdx.x & 31u;
+  bool const     vec  = (reinterpret_cast<uintptr_t>(a.scc_id) & 15u) == 0;
+  for (uint32_t wb = (blockIdx.x * R_THREADS + threadIdx.x) & ~31u; wb < words; wb += gridDim.x * R_THREADS) {
+    uint32_t const w   = wb + lane;
+    uint32_t const und = w < words ? __ldcg(a.und + w) : 0u;
+    uint32_t const mem = search && w < words ? __ldcg(a.vis_b + w) : 0u;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      unsigned const src = j * 4 + (lane >> 3);
+      uint32_t const uw  = __shfl_sync(0xFFFFFFFFu, und, src);
+      uint32_t const mw  = __shfl_sync(0xFFFFFFFFu, mem, src);
+      unsigned const b0  = (lane & 7u) * 4;
+      uint64_t const v0  = (static_cast<uint64_t>(wb) + src) * 32 + b0;
+      uint32_t       o[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) o[i] = ((mw >> (b0 + i)) & 1u) ? scc : (((uw >> (b0 + i)) & 1u) ? UNDECIDED : static_cast<uint32_t>(v0 + i));
+      if (vec && v0 + 4 <= a.n) *reinterpret_cast<uint4*>(a.scc_id + v0) = make_uint4(o[0], o[1], o[2], o[3]);
+      else
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if (v0 + i < a.n) a.scc_id[v0 + i] = o[i];
+    }
+  }
 }
 
 __global__ void __launch_bounds__(R_THREADS, 4)
@@ -1073,7 +1090,7 @@ k_fwbw(fwbw_args a)
     st->levels_fw = st->bu_fw = st->levels_bw = st->bu_bw = 0;
     st->pivot_used                                        = p;
     st->trim_decided = st->trim_levels = st->und_left = 0;
-    st->trim_edges                                    = 0;
+    st->trim_edges = st->list_n                       = 0;
     if (search) a.seed.q[0] = p, a.seed.prefix[0] = 0;
   }
   int      rc   = SEARCH_DONE;
@@ -1152,22 +1169,41 @@ k_fwbw(fwbw_args a)
       // once, then for each non-empty one lane l writes vertex 32w + l (one
       // coalesced 128-byte store per word).  With the trim tail every word
       // of und is also copied to snap (cand).
-      unsigned const lane = threadIdx.x & 31u;
-      uint32_t       cnt = 0, left = 0;
+      unsigned const  lane = threadIdx.x & 31u;
+      uint32_t        cnt = 0, left = 0;
+      uint32_t* const list = a.fb[glvl & 1].q; // trim: the undecided vertices
       for (uint32_t wb = (blockIdx.x * R_THREADS + threadIdx.x) & ~31u; wb < words; wb += gridDim.x * R_THREADS) {
         uint32_t const w    = wb + lane;
         uint32_t const mine = w < words ? __ldcg(a.vis_b + w) : 0u;
+        uint32_t       u    = 0;
         if (w < words && (mine || a.trim)) {
-          uint32_t const u = __ldcg(a.und + w) & ~mine;
+          u = __ldcg(a.und + w) & ~mine;
           if (mine) a.und[w] = u;
           if (a.trim) a.cand[w] = u, left += __popc(u);
           cnt += __popc(mine);
         }
-        for (unsigned todo = __ballot_sync(0xFFFFFFFFu, mine != 0); todo; todo &= todo - 1) {
-          unsigned const j = __ffs(todo) - 1;
-          uint32_t const s = __shfl_sync(0xFFFFFFFFu, mine, j);
-          if ((s >> lane) & 1u) a.scc_id[(wb + j) * 32 + lane] = id;
+        if (a.trim) {
+          // append the word's undecided vertices to the list (one atomic per warp)
+          uint32_t const c = __popc(u);
+          uint32_t       p = c;
+#pragma unroll
+          for (int d = 1; d < 32; d <<= 1) {
+            uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, p, d);
+            if (lane >= static_cast<unsigned>(d)) p += y;
+          }
+          uint32_t const     tot  = __shfl_sync(0xFFFFFFFFu, p, 31);
+          unsigned long long base = 0;
+          if (lane == 31 && tot) base = atomicAdd(&st->list_n, static_cast<unsigned long long>(tot));
+          base = __shfl_sync(0xFFFFFFFFu, base, 31) + p - c;
+          for (; u; u &= u - 1, ++base)
+            if (base < a.n) list[base] = w * 32 + __ffs(u) - 1;
         }
+        if (!a.ids_at_end)
+          for (unsigned todo = __ballot_sync(0xFFFFFFFFu, mine != 0); todo; todo &= todo - 1) {
+            unsigned const j = __ffs(todo) - 1;
+            uint32_t const s = __shfl_sync(0xFFFFFFFFu, mine, j);
+            if ((s >> lane) & 1u) a.scc_id[(wb + j) * 32 + lane] = id;
+          }
       }
 #pragma unroll
       for (int sh = 16; sh; sh >>= 1) cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, sh), left += __shfl_down_sync(0xFFFFFFFFu, left, sh);
@@ -1178,8 +1214,15 @@ k_fwbw(fwbw_args a)
     stamp(a, 10);
     if (rc == SEARCH_DONE && a.trim) {
       rc = grid_sync(a.bar, epoch) ? SEARCH_DONE : SEARCH_FAILED; // snap and und complete
-      if (rc == SEARCH_DONE) rc = run_trim(a, sm, glvl, epoch);
+      if (rc == SEARCH_DONE) rc = run_trim(a, glvl, epoch);
     }
+  }
+  if (a.ids_at_end && rc == SEARCH_DONE) {
+    // every vertex's id in one coalesced pass (und is final: after the
+    // trim's last barrier, or untouched by this launch without a pivot):
+    // SCC members the SCC's id, other decided vertices themselves (trim_1_first
+    // and the trim decide singletons), undecided ones UNDECIDED
+    write_ids(a, words, search, id);
   }
   if (!search && a.trim) {
     // no pivot: und is untouched, count it (with a pivot, und_left is the
@@ -1396,6 +1439,7 @@ launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* s
   a.pv_prod     = ws.pivot + PV_FINAL;
   a.pv_id       = reinterpret_cast<uint32_t const*>(ws.pivot + 4096) + PV_FINAL;
   a.trim        = trim ? 1u : 0u;
+  a.ids_at_end  = trim ? 1u : 0u;
   a.indeg       = ws.indeg;
   a.outdeg      = ws.outdeg;
   a.bar         = gbar;

@@ -136,7 +136,7 @@ k_trim_first(uint32_t n,
       bool const     live    = valid && !trimmed;
       unsigned const word    = __ballot_sync(0xFFFFFFFFu, live);
       if ((threadIdx.x & 31) == 0 && t < n) und[v >> 5] = word; // t = the warp's first vertex
-      if (valid) scc_id[v] = trimmed ? v : UNDECIDED;
+      if (valid && scc_id) scc_id[v] = trimmed ? v : UNDECIDED; // scc_id null: the caller writes ids later
       if (live) {
         if (indeg) indeg[v] = static_cast<uint32_t>(in);
         if (outdeg) outdeg[v] = static_cast<uint32_t>(out);
@@ -799,13 +799,14 @@ trim_1_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id
   return (prod == 0 || pivot == NONE) ? g.n : pivot;
 }
 
-// (the caller has zeroed ws.ctr)
+// (the caller has zeroed ws.ctr; ids are not written: the resident
+// launch that follows writes every vertex's id at its end)
 void
-trim_1_first_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id)
+trim_1_first_async(kspn_context* ctx, dgraph const& g, uint32_t* und)
 {
   auto& ws = ctx->ws;
   prof_start(ctx);
-  k_trim_first<<<stream_grid((static_cast<uint64_t>(g.n) + TF_ITEMS - 1) / TF_ITEMS), T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.bh, und, scc_id, nullptr, nullptr, nullptr, ws.ctr, ws.pivot, reinterpret_cast<uint32_t*>(ws.pivot + 4096));
+  k_trim_first<<<stream_grid((static_cast<uint64_t>(g.n) + TF_ITEMS - 1) / TF_ITEMS), T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.bh, und, nullptr, nullptr, nullptr, nullptr, ws.ctr, ws.pivot, reinterpret_cast<uint32_t*>(ws.pivot + 4096));
   prof_stop(ctx);
   KSPN_CHECK_LAUNCH();
   ctx->launches += 1;
