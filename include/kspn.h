@@ -123,6 +123,18 @@ typedef struct kspn_stats
   uint32_t search_marks;
   uint32_t search_phase[128];
   uint64_t search_ns[128];
+  /* The resident launch of the FAST pipeline (FW-BW, trim fixpoint and all
+   * ids in one persistent kernel; 0 when the call did not run it): its
+   * CUDA-event duration and its algorithmic DRAM traffic -- 16 B per
+   * adjacency row opened (two u64 offsets), 4 B per neighbour id read,
+   * n/8 B per pass over a vertex bitmap, 4 B per id written; probes of the
+   * state bitmaps (n/8 B each, L2-resident) are not counted. */
+  double   resident_ms;
+  uint64_t resident_bytes;
+  uint64_t resident_rows;          /* adjacency rows opened */
+  uint64_t resident_edges;         /* neighbour ids read */
+  uint32_t resident_bitmap_passes; /* passes over a vertex bitmap */
+  uint32_t resident_pad;
 } kspn_stats;
 
 typedef struct kspn_context kspn_context;

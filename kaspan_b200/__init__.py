@@ -97,6 +97,12 @@ class Stats(C.Structure):
         ("search_marks", C.c_uint32),
         ("search_phase", C.c_uint32 * 128),
         ("search_ns", C.c_uint64 * 128),
+        ("resident_ms", C.c_double),
+        ("resident_bytes", C.c_uint64),
+        ("resident_rows", C.c_uint64),
+        ("resident_edges", C.c_uint64),
+        ("resident_bitmap_passes", C.c_uint32),
+        ("resident_pad", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -121,6 +127,8 @@ class Stats(C.Structure):
                        "candidates": int(t.candidates), "ms": round(float(t.ms), 4)}
                       for t in self.trace[: min(self.trace_levels, 32)]],
             "search_marks": [(int(self.search_phase[i]), int(self.search_ns[i])) for i in range(min(self.search_marks, 128))],
+            "resident": {"ms": float(self.resident_ms), "bytes": int(self.resident_bytes), "rows": int(self.resident_rows),
+                         "edges": int(self.resident_edges), "bitmap_passes": int(self.resident_bitmap_passes)},
         }
 
 

@@ -266,17 +266,20 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
       // launch that takes the pivot from device memory: one host sync
       trim_1_first_async(ctx, g, und);
       KSPN_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
-      fw_bw_trim_async(ctx, g, und, scc_id, opt, st);
+      fw_bw_trim_async(ctx, g, und, scc_id, opt, st, ctx->ev[4]);
       KSPN_CUDA(cudaMemcpyAsync(ctx->h_ctr, ws.ctr, 64 * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
       KSPN_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
       KSPN_CUDA(cudaEventSynchronize(ctx->ev[3]));
-      resident_result const r  = fw_bw_trim_result(ctx, opt, st);
+      resident_result const r  = fw_bw_trim_result(ctx, g, opt, st);
       uint32_t const        tf = ctx->h_ctr[CTR_DECIDED];
       decided += static_cast<uint64_t>(tf) + r.fwbw_decided + r.trim_decided;
       if (st) {
         float a = 0, b = 0;
         KSPN_CUDA(cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[2]));
         KSPN_CUDA(cudaEventElapsedTime(&b, ctx->ev[2], ctx->ev[3]));
+        float k = 0;
+        KSPN_CUDA(cudaEventElapsedTime(&k, ctx->ev[2], ctx->ev[4]));
+        st->resident_ms = k;
         st->ms[KSPN_PHASE_TRIM_FIRST] += a;
         st->ms[KSPN_PHASE_FWBW] += b * r.fwbw_share;
         st->ms[KSPN_PHASE_TRIM] += b * (1.0 - r.fwbw_share);

@@ -346,8 +346,8 @@ struct resident_result
   double   fwbw_share = 1.0; // FW-BW's share of the launch's device time
 };
 bool            resident_fits(dgraph const& g);
-void            fw_bw_trim_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, kspn_options const& opt, kspn_stats* st);
-resident_result fw_bw_trim_result(kspn_context* ctx, kspn_options const& opt, kspn_stats* st);
+void            fw_bw_trim_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, kspn_options const& opt, kspn_stats* st, cudaEvent_t after_kernel);
+resident_result fw_bw_trim_result(kspn_context* ctx, dgraph const& g, kspn_options const& opt, kspn_stats* st);
 
 uint32_t trim_1_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* queue_out, uint32_t* queue_count_host, bool init_degrees);
 void     trim_1_first_async(kspn_context* ctx, dgraph const& g, uint32_t* und); // ws.ctr zeroed by the caller; writes no ids; no host sync: decided in ws.ctr, pivot in PV_FINAL

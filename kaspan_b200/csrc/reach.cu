@@ -93,6 +93,10 @@ struct reach_state
   uint32_t           und_left;     // undecided vertices when the launch ended
   unsigned long long trim_edges;   // adjacency entries the trim tail read
   unsigned long long list_n;       // undecided vertices listed for the trim tail
+  uint32_t           bu_bitmap;    // bottom-up levels that swept the bitmap
+  unsigned long long rows_td;      // rows the top-down levels expanded
+  unsigned long long pushed_td;    // vertices they queued (offsets read once more)
+  uint32_t           mats;         // frontiers built from `fresh`
   unsigned long long t_ns[3];      // %globaltimer: launch start, FW-BW end, trim end
 };
 
@@ -224,16 +228,9 @@ struct take_op
   }
 };
 
-// Bottom-up sweep: candidates are the set bits of `avail`; a candidate
-// joins (taken from avail, set in mark, queued) when a neighbour in its
-// `head/adj` row is in `mark`.
-//  * Compaction: a block reads BU_WORDS bitmap words (one per thread), and a
-//    block scan of their popcounts packs the candidate ids into shared
-//    memory, so a sweep over few candidates costs about one pass over the
-//    bitmap and lanes never idle on non-candidates.
-//  * Each thread then carries BU_ILP candidates at once (interleaved row
-//    walks) so their dependent loads overlap; a row with no visited
-//    neighbour among its first R_BIG entries is finished by the whole warp.
+// Bottom-up levels: a candidate (a set bit of avail) joins -- taken from
+// avail, set in mark -- when a neighbour in its opposite-direction row is
+// already in mark.
 constexpr int BU_WARPS = R_THREADS / 32;
 constexpr int BU_STEPS = 32; // neighbours a candidate checks itself before its warp helps
 
@@ -244,18 +241,80 @@ struct bu_warp_smem
   uint32_t found[32];     // found bits per word of the chunk
 };
 
+// Row walks of up to BU_ILP candidates per lane (v[k], live[k]): all
+// neighbour loads of a step, then all probes of `mark`; rows still open
+// after BU_STEPS neighbours are finished by the whole warp with early exit.
+// found[k]: a neighbour of v[k] is in mark.  All lanes call it.
+__device__ __forceinline__ void
+bu_rows(uint32_t const (&v)[BU_ILP], bool (&live)[BU_ILP], bool (&found)[BU_ILP], uint64_t const* __restrict__ head, uint32_t const* __restrict__ adj, uint32_t const* mark, uint64_t& nedge)
+{
+  unsigned const lane = threadIdx.x & 31u;
+  uint64_t       b[BU_ILP], e[BU_ILP];
+#pragma unroll
+  for (int k = 0; k < BU_ILP; ++k) {
+    b[k] = e[k] = 0;
+    if (live[k]) b[k] = head[v[k]], e[k] = head[v[k] + 1];
+    found[k] = false;
+  }
+  for (int s_i = 0; s_i < BU_STEPS; ++s_i) {
+    bool     act[BU_ILP];
+    uint32_t x[BU_ILP], wd[BU_ILP];
+    bool     any = false;
+#pragma unroll
+    for (int k = 0; k < BU_ILP; ++k) {
+      act[k] = live[k] && b[k] < e[k];
+      x[k]   = act[k] ? adj[b[k]] : 0u;
+      any |= act[k];
+    }
+    if (!__any_sync(0xFFFFFFFFu, any)) break;
+#pragma unroll
+    for (int k = 0; k < BU_ILP; ++k) wd[k] = act[k] ? __ldcg(mark + (x[k] >> 5)) : 0u;
+#pragma unroll
+    for (int k = 0; k < BU_ILP; ++k) {
+      if (!act[k]) {
+        live[k] = false;
+        continue;
+      }
+      ++b[k];
+      ++nedge;
+      if ((wd[k] >> (x[k] & 31)) & 1u) found[k] = true, live[k] = false;
+    }
+  }
+  // rows still open: the whole warp, one at a time, with early exit
+#pragma unroll
+  for (int k = 0; k < BU_ILP; ++k) {
+    bool const open = live[k] && b[k] < e[k];
+    unsigned   todo = __ballot_sync(0xFFFFFFFFu, open);
+    while (todo) {
+      unsigned const l = __ffs(todo) - 1;
+      todo &= todo - 1;
+      uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b[k], l), e0 = __shfl_sync(0xFFFFFFFFu, e[k], l);
+      bool           hit = false;
+      for (uint64_t x = b0; x < e0; x += 32) {
+        bool const     in = x + lane < e0;
+        uint32_t const y  = in ? adj[x + lane] : 0u;
+        bool const     h  = in && ((__ldcg(mark + (y >> 5)) >> (y & 31)) & 1u);
+        nedge += in;
+        if (__any_sync(0xFFFFFFFFu, h)) {
+          hit = true;
+          break;
+        }
+      }
+      if (lane == l) found[k] = hit;
+    }
+  }
+}
+
 // Bottom-up sweep over the chunks of 32 bitmap words given to this warp
 // (chunk c = words [32c, 32c + 32), c = first, first + step, ...).
 // Candidates are the set bits of `avail`; one joins when a neighbour in its
 // head/adj row is in `mark`.  Warps work independently (no block barrier):
 // the warp packs its chunk's candidates (popcount scan over its 32 words),
-// each lane walks BU_ILP candidates interleaved -- all neighbour loads of a
-// step, then all probes -- and rows still open after BU_STEPS neighbours
-// are finished by the whole warp with early exit.  Lane i then owns word i
-// of the chunk: it clears the found bits from avail, sets them in mark and
-// writes the word of `fresh` (the sweep's discoveries).  No queue is
-// written; the count goes to *found_count.  `avail` and `mark` are read
-// through L2 (other blocks of a persistent launch change them).
+// each lane walks BU_ILP candidates interleaved (bu_rows).  Lane i then
+// owns word i of the chunk: it clears the found bits from avail, sets them
+// in mark and writes the word of `fresh` (the sweep's discoveries).  No
+// queue is written; the discovery count goes to nfound.  `avail` and `mark` are read through L2 (other
+// blocks of a persistent launch change them).
 __device__ __forceinline__ void
 bu_sweep_warp(uint32_t first,
               uint32_t step,
@@ -296,64 +355,14 @@ bu_sweep_warp(uint32_t first,
     ncand += lane == 0 ? total : 0;
     for (uint32_t r = 0; r < total; r += 32 * BU_ILP) {
       uint32_t v[BU_ILP];
-      uint64_t b[BU_ILP], e[BU_ILP];
       bool     live[BU_ILP], found[BU_ILP];
 #pragma unroll
       for (int k = 0; k < BU_ILP; ++k) {
         uint32_t const i = r + k * 32 + lane;
         live[k]          = i < total;
         v[k]             = live[k] ? c * 1024 + sm.cand[i] : 0u;
-        b[k] = e[k] = 0;
-        if (live[k]) b[k] = head[v[k]], e[k] = head[v[k] + 1];
-        found[k] = false;
       }
-      for (int s_i = 0; s_i < BU_STEPS; ++s_i) {
-        bool     act[BU_ILP];
-        uint32_t x[BU_ILP], wd[BU_ILP];
-        bool     any = false;
-#pragma unroll
-        for (int k = 0; k < BU_ILP; ++k) {
-          act[k] = live[k] && b[k] < e[k];
-          x[k]   = act[k] ? adj[b[k]] : 0u;
-          any |= act[k];
-        }
-        if (!__any_sync(0xFFFFFFFFu, any)) break;
-#pragma unroll
-        for (int k = 0; k < BU_ILP; ++k) wd[k] = act[k] ? __ldcg(mark + (x[k] >> 5)) : 0u;
-#pragma unroll
-        for (int k = 0; k < BU_ILP; ++k) {
-          if (!act[k]) {
-            live[k] = false;
-            continue;
-          }
-          ++b[k];
-          ++nedge;
-          if ((wd[k] >> (x[k] & 31)) & 1u) found[k] = true, live[k] = false;
-        }
-      }
-      // rows still open: the whole warp, one at a time, with early exit
-#pragma unroll
-      for (int k = 0; k < BU_ILP; ++k) {
-        bool const open = live[k] && b[k] < e[k];
-        unsigned   todo = __ballot_sync(0xFFFFFFFFu, open);
-        while (todo) {
-          unsigned const l = __ffs(todo) - 1;
-          todo &= todo - 1;
-          uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b[k], l), e0 = __shfl_sync(0xFFFFFFFFu, e[k], l);
-          bool           hit = false;
-          for (uint64_t x = b0; x < e0; x += 32) {
-            bool const     in = x + lane < e0;
-            uint32_t const y  = in ? adj[x + lane] : 0u;
-            bool const     h  = in && ((__ldcg(mark + (y >> 5)) >> (y & 31)) & 1u);
-            nedge += in;
-            if (__any_sync(0xFFFFFFFFu, h)) {
-              hit = true;
-              break;
-            }
-          }
-          if (lane == l) found[k] = hit;
-        }
-      }
+      bu_rows(v, live, found, head, adj, mark, nedge);
 #pragma unroll
       for (int k = 0; k < BU_ILP; ++k)
         if (found[k]) atomicOr(&sm.found[(v[k] >> 5) - c * 32], 1u << (v[k] & 31));
@@ -712,6 +721,33 @@ materialize_scanned(uint32_t n, uint32_t const* fresh, frontier_buf const& out, 
   }
 }
 
+// Warp-aggregated append to a queue whose length is a 64-bit counter: all
+// lanes of the warp call it (warp_push64) or only the active ones
+// (warp_push_active64).  Slots at or past `cap` are not written.
+__device__ __forceinline__ void
+warp_push64(bool pred, uint32_t v, uint32_t* q, unsigned long long* count, uint64_t cap)
+{
+  unsigned const ballot = __ballot_sync(0xFFFFFFFFu, pred);
+  if (!ballot) return;
+  unsigned const     lane = threadIdx.x & 31u, leader = __ffs(ballot) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(count, static_cast<unsigned long long>(__popc(ballot)));
+  base                = __shfl_sync(0xFFFFFFFFu, base, leader);
+  uint64_t const slot = base + __popc(ballot & ((1u << lane) - 1u));
+  if (pred && slot < cap) q[slot] = v;
+}
+__device__ __forceinline__ void
+warp_push_active64(uint32_t v, uint32_t* q, unsigned long long* count, uint64_t cap)
+{
+  unsigned const     mask = __activemask();
+  unsigned const     lane = threadIdx.x & 31u, leader = __ffs(mask) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(count, static_cast<unsigned long long>(__popc(mask)));
+  base                = __shfl_sync(mask, base, leader);
+  uint64_t const slot = base + __popc(mask & ((1u << lane) - 1u));
+  if (slot < cap) q[slot] = v;
+}
+
 // Every level of one reachability search (BW: over in-edges, candidates
 // vis_a, reached vis_b; FW: over out-edges, candidates cand, reached vis_a).
 // `glvl` numbers levels across both searches of the launch (it selects
@@ -743,6 +779,7 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
   bool                     mat     = false;
   uint32_t                 bu = 0, capped = 0, lvl = 0;
   uint64_t                 edges_td = 0;
+  bool const               tally = blockIdx.x == 0 && threadIdx.x == 0; // keeps the byte-model counts in st
   // the first frontier: the pivot alone
   unsigned long long c = (static_cast<unsigned long long>(td_head[pivot + 1] - td_head[pivot]) << a.qbits) | 1u;
   for (;; ++lvl, ++glvl) {
@@ -755,6 +792,7 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
       if (!grid_sync(a.bar, epoch)) return SEARCH_FAILED;
       stamp(a, 7);
       c = __ldcg(&st->mat_q);
+      if (tally) st->mats += 1;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       st->lq[s_clr] = 0;
@@ -775,6 +813,7 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
     unsigned long long* const octr = &st->lq[s_out];
     if (mode == 0) {
       edges_td += mf;
+      if (tally) st->rows_td += qn;
       uint32_t const ntiles = static_cast<uint32_t>((mf + EX_TILE - 1) / EX_TILE);
       // few tiles: split each into `parts` slot ranges on separate blocks,
       // so a small frontier still spreads over the grid
@@ -795,6 +834,7 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
       unsigned const wid    = threadIdx.x >> 5;
       uint32_t       nfound = 0;
       uint64_t       ne = 0, nc = 0;
+      if (tally) st->bu_bitmap += 1;
       bu_sweep_warp(blockIdx.x * BU_WARPS + wid, gridDim.x * BU_WARPS, a.n, bu_head, bu_adj, avail, mark, a.fresh, sm.warp[wid], nfound, ne, nc);
 #pragma unroll
       for (int sh = 16; sh; sh >>= 1) {
@@ -814,11 +854,11 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
     m_u = m_u > mf ? m_u - mf : 0;
     bu += mode;
     mat = false;
+    uint32_t const next = static_cast<uint32_t>(__ldcg(&st->lq[s_out]) & qmask);
     if (mode == 1) {
       // stay bottom-up while the sweep found at least n_und / beta vertices
-      uint32_t const next = static_cast<uint32_t>(__ldcg(&st->lq[s_out]) & qmask);
-      mat                 = next != 0 && static_cast<unsigned long long>(next) * a.beta < n_und;
-    }
+      mat = next != 0 && static_cast<unsigned long long>(next) * a.beta < n_und;
+    } else if (tally) st->pushed_td += next;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (BW) st->levels_bw = lvl, st->bu_bw = bu;
@@ -836,33 +876,6 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
 // still-undecided neighbour's count once per edge, and a count reaching 0
 // decides that neighbour (one push level per barrier).
 constexpr int PIVOT_FROM_DEVICE = -1; // fwbw_args.pivot: take trim_1_first's pivot
-
-// Warp-aggregated append to a queue whose length is a 64-bit counter: all
-// lanes of the warp call it (warp_push64) or only the active ones
-// (warp_push_active64).  Slots at or past `cap` are not written.
-__device__ __forceinline__ void
-warp_push64(bool pred, uint32_t v, uint32_t* q, unsigned long long* count, uint64_t cap)
-{
-  unsigned const ballot = __ballot_sync(0xFFFFFFFFu, pred);
-  if (!ballot) return;
-  unsigned const     lane = threadIdx.x & 31u, leader = __ffs(ballot) - 1;
-  unsigned long long base = 0;
-  if (lane == leader) base = atomicAdd(count, static_cast<unsigned long long>(__popc(ballot)));
-  base                = __shfl_sync(0xFFFFFFFFu, base, leader);
-  uint64_t const slot = base + __popc(ballot & ((1u << lane) - 1u));
-  if (pred && slot < cap) q[slot] = v;
-}
-__device__ __forceinline__ void
-warp_push_active64(uint32_t v, uint32_t* q, unsigned long long* count, uint64_t cap)
-{
-  unsigned const     mask = __activemask();
-  unsigned const     lane = threadIdx.x & 31u, leader = __ffs(mask) - 1;
-  unsigned long long base = 0;
-  if (lane == leader) base = atomicAdd(count, static_cast<unsigned long long>(__popc(mask)));
-  base                = __shfl_sync(mask, base, leader);
-  uint64_t const slot = base + __popc(mask & ((1u << lane) - 1u));
-  if (slot < cap) q[slot] = v;
-}
 
 __device__ __forceinline__ uint32_t
 snap_bit(uint32_t const* snap, uint32_t v)
@@ -1091,6 +1104,8 @@ k_fwbw(fwbw_args a)
     st->pivot_used                                        = p;
     st->trim_decided = st->trim_levels = st->und_left = 0;
     st->trim_edges = st->list_n                       = 0;
+    st->rows_td = st->pushed_td = 0;
+    st->mats = st->bu_bitmap    = 0;
     if (search) a.seed.q[0] = p, a.seed.prefix[0] = 0;
   }
   int      rc   = SEARCH_DONE;
@@ -1405,7 +1420,8 @@ namespace {
 // queues the copies of its results into the pinned state mirror; the
 // caller synchronises, then calls check_persistent.
 void
-launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t pivot, bool trim, kspn_options const& opt, kspn_stats* st, bool min_ids)
+launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t pivot, bool trim, kspn_options const& opt, kspn_stats* st, bool min_ids,
+                  cudaEvent_t after_kernel = nullptr)
 {
   auto&       ws   = ctx->ws;
   auto* const rs   = reinterpret_cast<reach_state*>(ws.rstate);
@@ -1449,6 +1465,7 @@ launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* s
   void* args[]  = { &a };
   KSPN_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(&k_fwbw), dim3(fwbw_grid(ctx)), dim3(R_THREADS), args, 0, ctx->stream));
   ctx->launches += 1;
+  if (after_kernel) KSPN_CUDA(cudaEventRecord(after_kernel, ctx->stream));
   // results, and the barrier's error word (read after the launch ended: a
   // block that gave up may set it after block 0 finished)
   auto* const hb = reinterpret_cast<uint32_t*>(static_cast<char*>(ctx->h_state) + 1024);
@@ -1501,18 +1518,35 @@ resident_fits(dgraph const& g)
 }
 
 void
-fw_bw_trim_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, kspn_options const& opt, kspn_stats* st)
+fw_bw_trim_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, kspn_options const& opt, kspn_stats* st, cudaEvent_t after_kernel)
 {
-  launch_persistent(ctx, g, und, scc_id, static_cast<uint32_t>(PIVOT_FROM_DEVICE), true, opt, st, true);
+  launch_persistent(ctx, g, und, scc_id, static_cast<uint32_t>(PIVOT_FROM_DEVICE), true, opt, st, true, after_kernel);
 }
 
 resident_result
-fw_bw_trim_result(kspn_context* ctx, kspn_options const& opt, kspn_stats* st)
+fw_bw_trim_result(kspn_context* ctx, dgraph const& g, kspn_options const& opt, kspn_stats* st)
 {
   check_persistent(ctx);
   auto* hs = reinterpret_cast<reach_state*>(ctx->h_state);
   record_search_stats(ctx, opt, st);
   ctx->h_ctr64[0] += hs->trim_edges;
+  if (st) {
+    // algorithmic DRAM traffic of the launch (the model kspn_stats
+    // states): rows opened by bottom-up candidates, by top-down frontiers,
+    // by the vertices pushed into scanned frontiers, and by the trim (both
+    // rows of every listed and every queued vertex); neighbour ids read;
+    // bitmap passes -- init (und read, three bitmaps written), two per
+    // bitmap sweep (avail, fresh), one per frontier built from fresh,
+    // finalize (vis_b, und read + written, snap), ids (und, vis_b) -- and
+    // the ids written
+    uint64_t const rows   = hs->cands_bu + hs->rows_td + hs->pushed_td + 2 * (hs->list_n + hs->trim_decided);
+    uint64_t const edges  = hs->edges_td + hs->edges_bu + hs->trim_edges;
+    uint32_t const passes = hs->pivot_used < g.n ? 4 + 2 * hs->bu_bitmap + hs->mats + 4 + 2 : 1;
+    st->resident_rows          = rows;
+    st->resident_edges         = edges;
+    st->resident_bitmap_passes = passes;
+    st->resident_bytes         = 16 * rows + 4 * edges + passes * ((static_cast<uint64_t>(g.n) + 7) / 8) + 4ull * g.n;
+  }
   resident_result r;
   r.pivot             = hs->pivot_used;
   r.fwbw_decided      = hs->decided;
