@@ -45,9 +45,11 @@ WORKLOADS = {
     "rmat26": ("rmat", dict(scale=26, ef=16, seed=4), "R-MAT scale 26, edge factor 16, a,b,c,d=.57,.19,.19,.05, permuted ids"),
     "gnm16": ("gnm", dict(n=1 << 16, draws=1 << 19, seed=1), "directed G(n,m) n=2^16, 2^19 draws"),
     "rmat22": ("rmat", dict(scale=22, ef=16, seed=2), "R-MAT scale 22, edge factor 16, a,b,c,d=.57,.19,.19,.05, permuted ids"),
+    "rgg24": ("rgg", dict(n=1 << 24, seed=3), "2D random geometric graph n=2^24, mean undirected degree 8, each pair u->v / v->u / both / neither with p=.25"),
+    "rgg20": ("rgg", dict(n=1 << 20, seed=3), "2D random geometric graph n=2^20, mean undirected degree 8, each pair u->v / v->u / both / neither with p=.25"),
 }
 # bounded CPU sample of each workload for the reference arm / cpu_baseline
-CPU_SAMPLE = {"rmat24": "rmat22", "rmat26": "rmat22", "gnm16": "gnm16", "rmat22": "rmat22"}
+CPU_SAMPLE = {"rmat24": "rmat22", "rmat26": "rmat22", "gnm16": "gnm16", "rmat22": "rmat22", "rgg24": "rgg20", "rgg20": "rgg20"}
 
 
 def measured_peak_gbs():
@@ -112,6 +114,8 @@ def make_graph(ctx, name, rank_seed=0):
     kind, p, _ = WORKLOADS[name]
     if kind == "rmat":
         return KG.rmat(ctx, p["scale"], p["ef"], p["seed"] + rank_seed)
+    if kind == "rgg":
+        return KG.rgg(ctx, p["n"], p["seed"] + rank_seed)
     return KG.gnm(ctx, p["n"], p["draws"], p["seed"] + rank_seed)
 
 
@@ -125,7 +129,7 @@ def cpu_reference_sample(name, steps=1, warmup=0, threads_note=True):
         return None
     sname = CPU_SAMPLE[name]
     kind, p, desc = WORKLOADS[sname]
-    G = O.rmat(p["scale"], p["ef"], p["seed"]) if kind == "rmat" else O.gnm(p["n"], p["draws"], p["seed"])
+    G = O.rmat(p["scale"], p["ef"], p["seed"]) if kind == "rmat" else (O.rgg(p["n"], p["seed"]) if kind == "rgg" else O.gnm(p["n"], p["draws"], p["seed"]))
     for _ in range(warmup):
         O.ref_scc(G)
     rates = []

@@ -278,6 +278,15 @@ int kspn_gen_gnm(kspn_context* ctx, uint32_t n, uint64_t draws, uint64_t seed,
 int kspn_gen_rmat(kspn_context* ctx, int scale, uint64_t draws, uint64_t seed,
                   uint64_t t_a, uint64_t t_ab, uint64_t t_abc, int permute,
                   uint32_t* d_src, uint32_t* d_dst);
+/* Random geometric graph in the unit square (stands in for KaGen's rgg2d):
+ * n points on a g x g cell grid, squared radius r2 in units of 2^-60
+ * (pass g = floor(1/r), r2 = floor(r^2 * 2^60)); each pair within the
+ * radius becomes u->v, v->u, both or neither with probability 1/4 each.
+ * *m_out = the edge count; the edges are written when d_src and d_dst are
+ * given and hold `capacity` >= *m_out entries (otherwise, with buffers,
+ * KSPN_ERR_INVALID_ARGUMENT and *m_out set). */
+int kspn_gen_rgg(kspn_context* ctx, uint32_t n, uint64_t seed, uint32_t g, uint64_t r2,
+                 uint32_t* d_src, uint32_t* d_dst, uint64_t capacity, uint64_t* m_out);
 /* Edge list -> CSR with self-loops and duplicates removed, rows ascending.
  * d_src/d_dst are overwritten (used as scratch).  *m_out = edges kept. */
 int kspn_build_csr(kspn_context* ctx, uint32_t n, uint64_t m_raw,

@@ -166,6 +166,7 @@ SIGNATURES = {
     "kspn_transpose": (_i32, [_P, _u32, _u64, _P, _P, _P, _P]),
     "kspn_gen_gnm": (_i32, [_P, _u32, _u64, _u64, _P, _P]),
     "kspn_gen_rmat": (_i32, [_P, _i32, _u64, _u64, _u64, _u64, _u64, _i32, _P, _P]),
+    "kspn_gen_rgg": (_i32, [_P, _u32, _u64, _u32, _u64, _P, _P, _u64, _P]),
     "kspn_build_csr": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P]),
 }
 
@@ -332,6 +333,13 @@ class Context:
 
     def gen_rmat(self, scale, draws, seed, ta, tab, tabc, permute, src, dst):
         self._check(lib().kspn_gen_rmat(self.h, scale, draws, seed, ta, tab, tabc, int(permute), _ptr(src), _ptr(dst)), "gen_rmat")
+
+    def gen_rgg(self, n, seed, g, r2, src=None, dst=None, capacity=0) -> int:
+        """Edge count of the RGG; writes the edges when src/dst are given."""
+        m = C.c_uint64()
+        self._check(lib().kspn_gen_rgg(self.h, n, seed, g, r2, _ptr(src) if src is not None else None,
+                                       _ptr(dst) if dst is not None else None, capacity, C.byref(m)), "gen_rgg")
+        return m.value
 
     def build_csr(self, n, m_raw, src, dst, head, csr) -> int:
         m = C.c_uint64()

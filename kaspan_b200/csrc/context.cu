@@ -747,6 +747,20 @@ kspn_gen_rmat(kspn_context* ctx, int scale, uint64_t draws, uint64_t seed, uint6
 }
 
 int
+kspn_gen_rgg(kspn_context* ctx, uint32_t n, uint64_t seed, uint32_t g, uint64_t r2, uint32_t* d_src, uint32_t* d_dst, uint64_t capacity, uint64_t* m_out)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require((d_src == nullptr) == (d_dst == nullptr), "d_src and d_dst must both be given or both be NULL");
+    bind_device(ctx);
+    uint64_t const m = gen_rgg(ctx, n, seed, g, r2, d_src, d_dst, capacity);
+    if (m_out) *m_out = m;
+    require(!d_src || m <= capacity, "edge buffers smaller than the edge count");
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int
 kspn_build_csr(kspn_context* ctx, uint32_t n, uint64_t m_raw, uint32_t* d_src, uint32_t* d_dst, uint64_t* d_head, uint32_t* d_csr, uint64_t* m_out)
 {
   if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;

@@ -265,6 +265,7 @@ enum buffer_slot : int
   BUF_HOST_GRAPH = 0, // device copy of a host graph + output (kspn_scc)
   BUF_BUILD      = 1, // radix-sort scratch (transpose, build_csr)
   BUF_TRANSPOSE  = 2, // transpose built for kspn_scc_device without bw
+  BUF_GEN        = 3, // generator scratch (RGG points and cells)
   BUF_COUNT      = 4
 };
 
@@ -380,5 +381,7 @@ void     validate(kspn_context* ctx, dgraph const& g);
 // gen.cu
 void gen_gnm(kspn_context* ctx, uint32_t n, uint64_t draws, uint64_t seed, uint32_t* src, uint32_t* dst);
 void gen_rmat(kspn_context* ctx, int scale, uint64_t draws, uint64_t seed, uint64_t ta, uint64_t tab, uint64_t tabc, int do_perm, uint32_t* src, uint32_t* dst);
+// edge count; the edges are written when src is given and count <= cap
+uint64_t gen_rgg(kspn_context* ctx, uint32_t n, uint64_t seed, uint32_t g, uint64_t r2, uint32_t* src, uint32_t* dst, uint64_t cap);
 
 } // namespace kspn

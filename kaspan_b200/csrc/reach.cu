@@ -471,16 +471,15 @@ k_bottom_up(uint32_t n,
 // L%3, adds to (L+1)%3 and clears (L+2)%3, which no block touches again
 // until after the next barrier.
 constexpr unsigned GRID_SYNC_SPINS = 1u << 22;
-constexpr unsigned NLEAF           = 16;
 
-// Two-level grid barrier with monotonically growing counters: a block adds
-// to its leaf (blockIdx % NLEAF), the last of a leaf adds to the root, and
-// every block waits for root == epoch * leaves.  Counters are never reset
-// inside a launch; `epoch` carries the count to the next launch of the same
-// grid.  The host clears the whole struct when a wait gave up.
+// Grid barrier with a monotonically growing counter: every block adds 1
+// with a release reduction (no return value, so arrivals never wait on one
+// another) and waits, with acquire loads, until the counter reaches
+// epoch * blocks.  The counter is never reset inside a launch; `epoch`
+// carries the count to the next launch of the same grid.  The host clears
+// the whole struct when a wait gave up.
 struct grid_barrier
 {
-  unsigned long long leaf[NLEAF][16]; // one 128-byte line per leaf
   unsigned long long root;
   unsigned long long pad0[15];
   unsigned long long epoch; // barriers completed by every block
@@ -506,16 +505,8 @@ grid_sync(grid_barrier* b, unsigned long long& epoch)
   __syncthreads();
   ++epoch;
   if (threadIdx.x == 0) {
-    unsigned const           nb    = gridDim.x;
-    unsigned const           nleaf = nb < NLEAF ? nb : NLEAF;
-    unsigned const           g     = blockIdx.x % nleaf;
-    unsigned long long const gsize = (nb - g + nleaf - 1) / nleaf;
-    __threadfence();
-    if (atomicAdd(&b->leaf[g][0], 1ull) + 1 == epoch * gsize) {
-      __threadfence();
-      atomicAdd(&b->root, 1ull);
-    }
-    unsigned long long const target = epoch * nleaf;
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(&b->root), "l"(1ull) : "memory");
+    unsigned long long const target = epoch * gridDim.x;
     uint32_t                 ok     = 1;
     for (unsigned spins = 0; ld_acquire64(&b->root) < target; ++spins) {
       if (spins > GRID_SYNC_SPINS || ((spins & 63u) == 63u && ld_acquire(&b->err))) {
@@ -525,7 +516,7 @@ grid_sync(grid_barrier* b, unsigned long long& epoch)
       }
       __nanosleep(32);
     }
-    __threadfence();
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
     s_ok = ok;
   }
   __syncthreads();

@@ -1,8 +1,9 @@
 """Device-resident graphs and the seeded synthetic inputs, built with libkspn.
 
 The generators stand in for the KaGen inputs the reference benchmarks with
-(experiment/horeka/bootstrap.py:35-39): directed G(n, m) and R-MAT with a
-seeded id permutation.  Every step runs on the GPU through the C ABI:
+(experiment/horeka/bootstrap.py:35-39): directed G(n, m), R-MAT with a
+seeded id permutation, and a 2D random geometric graph (each pair within
+the radius becomes u->v, v->u, both or neither).  Every step runs on the GPU through the C ABI:
 draw the edge list (kspn_gen_*), sort + dedupe into a CSR (kspn_build_csr),
 build the transpose (kspn_transpose).  torch provides the device buffers.
 """
@@ -84,3 +85,23 @@ def rmat(ctx: Context, scale: int, edge_factor: int, seed: int, a=0.57, b=0.19, 
     dst = torch.empty(max(draws, 1), dtype=torch.int32, device=device)
     ctx.gen_rmat(scale, draws, seed, ta, tab, tabc, permute, src, dst)
     return from_edges(ctx, 1 << scale, src[:draws], dst[:draws], device)
+
+
+def rgg_params(n: int, mean_undirected_degree: float = 8.0):
+    """Cells per side g = floor(1/r) and r^2 in units of 2^-60 for radius
+    r = sqrt(deg / (pi n)) (mean undirected degree deg, boundary effects
+    ignored)."""
+    r2 = mean_undirected_degree / (math.pi * n)
+    g = max(1, int(math.floor(1.0 / math.sqrt(r2))))
+    return g, int(math.floor(r2 * float(1 << 60)))
+
+
+def rgg(ctx: Context, n: int, seed: int, mean_undirected_degree: float = 8.0, device="cuda") -> DeviceGraph:
+    import torch
+
+    g, r2 = rgg_params(n, mean_undirected_degree)
+    m_raw = ctx.gen_rgg(n, seed, g, r2)
+    src = torch.empty(max(m_raw, 1), dtype=torch.int32, device=device)
+    dst = torch.empty(max(m_raw, 1), dtype=torch.int32, device=device)
+    ctx.gen_rgg(n, seed, g, r2, src, dst, m_raw)
+    return from_edges(ctx, n, src[:m_raw], dst[:m_raw], device)

@@ -235,3 +235,34 @@ def test_generators_and_csr_build(ctx, kind):
     fwh, fwc, bwh, bwc = DG.to_host()
     assert np.array_equal(fwh, G.fwh) and np.array_equal(fwc[: G.m], G.fwc[: G.m])
     assert np.array_equal(bwh, G.bwh) and np.array_equal(bwc[: G.m], G.bwc[: G.m])
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 1000, 1 << 14, 1 << 16])
+def test_rgg_generator(ctx, n):
+    """Device RGG (kspn_gen_rgg) = the oracle's orc_rgg_points/orc_rgg_edges
+    restatement: same edge count, same CSR after dedupe, same transpose."""
+    import kaspan_b200.graphs as KG
+
+    g, r2 = KG.rgg_params(n)
+    assert (g, r2) == O.rgg_params(n)
+    G = O.rgg(n, 3)
+    DG = KG.rgg(ctx, n, 3)
+    assert DG.m == G.m
+    fwh, fwc, bwh, bwc = DG.to_host()
+    assert np.array_equal(fwh, G.fwh) and np.array_equal(fwc[: G.m], G.fwc[: G.m])
+    assert np.array_equal(bwh, G.bwh) and np.array_equal(bwc[: G.m], G.bwc[: G.m])
+
+
+def test_rgg_capacity_error(ctx):
+    import torch
+
+    import kaspan_b200.graphs as KG
+
+    n = 1 << 12
+    g, r2 = KG.rgg_params(n)
+    m = ctx.gen_rgg(n, 3, g, r2)
+    assert m > 0
+    src = torch.empty(m - 1, dtype=torch.int32, device="cuda")
+    dst = torch.empty(m - 1, dtype=torch.int32, device="cuda")
+    with pytest.raises(K.KspnError):
+        ctx.gen_rgg(n, 3, g, r2, src, dst, m - 1)
