@@ -74,6 +74,7 @@ layout(workspace& ws, char* base, uint32_t n, uint64_t m)
   ws.seed_q            = c.take<uint32_t>(4);
   ws.seed_prefix       = c.take<uint64_t>(4);
   ws.gbar              = c.take<char>(4096);
+  ws.aw                = c.take<unsigned long long>(nn + 64);
   ws.rstate            = c.take<char>(4096);
   return align_up(c.off);
 }
@@ -108,6 +109,7 @@ ensure_workspace(kspn_context* ctx, uint32_t n, uint64_t m)
   KSPN_CUDA(cudaMemsetAsync(ws.ctr, 0, 64 * sizeof(uint32_t), ctx->stream));
   KSPN_CUDA(cudaMemsetAsync(ws.tile_zero, 0, (mcap / 2048 + 4) * sizeof(uint32_t), ctx->stream));
   KSPN_CUDA(cudaMemsetAsync(ws.gbar, 0, 4096, ctx->stream));
+  KSPN_CUDA(cudaMemsetAsync(ws.aw, 0, (static_cast<size_t>(ncap) + 2 + 64) * sizeof(unsigned long long), ctx->stream));
 }
 
 void*

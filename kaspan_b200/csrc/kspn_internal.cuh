@@ -217,7 +217,8 @@ struct workspace
   uint32_t* tile_zero   = nullptr; // m / 2048 + 4 zeros: tile starts of a one-vertex frontier
   uint32_t* seed_q      = nullptr; // 4: the pivot as a one-vertex frontier
   uint64_t* seed_prefix = nullptr; // 4
-  void*     gbar        = nullptr; // 4 KiB grid barrier of the persistent FW-BW (zeroed at creation)
+  void*     gbar        = nullptr; // 4 KiB: grid barrier of the persistent FW-BW at 0, worklist counters at 1024 (zeroed at creation)
+  void*     aw          = nullptr; // n + 64 u64: worklist of the asynchronous search tail (zeroed at creation, zero outside a phase)
   void*     rstate      = nullptr; // 4 KiB device control blocks (FW-BW at 0, trim at 512, search stamps at 2048)
   // owned graph storage (host inputs, or a CSC built on device)
   uint64_t* g_fh = nullptr;

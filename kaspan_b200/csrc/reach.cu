@@ -94,6 +94,7 @@ struct reach_state
   unsigned long long trim_edges;   // adjacency entries the trim tail read
   unsigned long long list_n;       // undecided vertices listed for the trim tail
   uint32_t           bu_bitmap;    // bottom-up levels that swept the bitmap
+  uint32_t           async_phases; // searches finished on the worklist
   unsigned long long rows_td;      // rows the top-down levels expanded
   unsigned long long pushed_td;    // vertices they queued (offsets read once more)
   uint32_t           mats;         // frontiers built from `fresh`
@@ -562,6 +563,8 @@ struct fwbw_args
   uint32_t const*    pv_id;
   uint32_t           trim;
   uint32_t           ids_at_end; // resident launch: write every vertex's id at the end
+  unsigned long long* aw;        // asynchronous tail: worklist (n + 64 tagged entries, 0 when unused)
+  unsigned long long* aq;        // its counters: head at [0], tail at [16], done at [32] (own lines)
   uint32_t*          indeg;
   uint32_t*          outdeg;
   grid_barrier*      bar;
@@ -739,19 +742,167 @@ warp_push_active64(uint32_t v, uint32_t* q, unsigned long long* count, uint64_t 
   if (slot < cap) q[slot] = v;
 }
 
-// Every level of one reachability search (BW: over in-edges, candidates
-// vis_a, reached vis_b; FW: over out-edges, candidates cand, reached vis_a).
-// `glvl` numbers levels across both searches of the launch (it selects
-// counter slots and buffers); `pivot` is the launch's resolved pivot (never
-// the PIVOT_FROM_DEVICE marker).  Block 0 records the search's level counts.
-// Returns SEARCH_DONE, SEARCH_CAPPED (level cap reached) or SEARCH_FAILED
-// (the grid barrier gave up).
+// Outcome of a search phase: done, level cap reached, or the grid barrier
+// (or a worklist wait) gave up.
 enum : int
 {
   SEARCH_DONE   = 0,
   SEARCH_CAPPED = 1,
   SEARCH_FAILED = 2
 };
+
+// ---------------------------------------------------------------- asynchronous tail
+// A search whose frontier stays small level after level (a high-diameter
+// graph, e.g. RGG) pays a grid barrier and a chain of dependent loads per
+// level for little work.  The reached SET does not depend on level order,
+// so such a search finishes on a global worklist instead: entries are
+// (AW_TAG | vertex), written once per slot; a warp claims 32 slots at a
+// time, waits for each to be written, expands the vertex (take from avail,
+// set in mark, as a top-down level) and appends its finds; a warp adds its
+// finished items to the processed count when it next runs out of ready
+// slots.  The phase ends when the processed count equals the appended count
+// (nothing in flight can append any more); the used slots are then cleared to 0, so the worklist
+// is all zeros outside a phase.  Every wait is bounded.
+constexpr uint32_t           ASYNC_AFTER    = 16;        // top-down levels before a search may switch
+constexpr uint32_t           ASYNC_FRONTIER = 1u << 16;  // largest frontier that switches
+constexpr unsigned long long AW_TAG         = 1ull << 32; // marks a written slot
+constexpr int                AW_BATCH       = 8;         // neighbours a lane loads at once
+
+// warp-aggregated append of the active lanes' v (slots past cap dropped)
+__device__ __forceinline__ void
+aw_push(uint32_t v, unsigned long long* aw, unsigned long long* tail, uint64_t cap)
+{
+  unsigned const     mask = __activemask();
+  unsigned const     lane = threadIdx.x & 31u, leader = __ffs(mask) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(tail, static_cast<unsigned long long>(__popc(mask)));
+  base                = __shfl_sync(mask, base, leader);
+  uint64_t const slot = base + __popc(mask & ((1u << lane) - 1u));
+  if (slot < cap) __stcg(aw + slot, AW_TAG | v);
+}
+
+// Runs the rest of the search from frontier fin.q[0, qn).  All threads of
+// every block call it.
+__device__ __forceinline__ int
+run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, uint64_t const* __restrict__ td_head, uint32_t const* __restrict__ td_adj, uint32_t* avail, uint32_t* mark, unsigned long long& epoch,
+          uint64_t& edges)
+{
+  unsigned long long* const aw   = a.aw;
+  unsigned long long* const head = a.aq;
+  unsigned long long* const tail = a.aq + 16;
+  unsigned long long* const done = a.aq + 32;
+  uint64_t const            cap  = static_cast<uint64_t>(a.n) + 64;
+  unsigned const            lane = threadIdx.x & 31u;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; i < qn; i += static_cast<uint64_t>(gridDim.x) * R_THREADS) __stcg(aw + i, AW_TAG | __ldcg(fq + i));
+  if (blockIdx.x == 0 && threadIdx.x == 0) *head = 0, *tail = qn, *done = 0;
+  if (!grid_sync(a.bar, epoch)) return SEARCH_FAILED;
+  take_op const op{ avail, mark };
+  auto const    take   = [&](uint32_t w) { return op(0u, w, true, op.probe(w)); };
+  bool          failed = false;
+  uint32_t unpublished = 0; // items this warp finished, not yet added to done
+  for (bool alive = true; alive;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(head, 32ull);
+    base                = __shfl_sync(0xFFFFFFFFu, base, 0);
+    uint64_t const slot = base + lane;
+    bool           pending = true;
+    unsigned       spins   = 0;
+    while (__any_sync(0xFFFFFFFFu, pending)) {
+      bool     got = false;
+      uint32_t v   = 0;
+      if (pending && slot < cap) {
+        unsigned long long const e = ld_acquire64(aw + slot);
+        if (e & AW_TAG) v = static_cast<uint32_t>(e), got = true, pending = false;
+      }
+      unsigned const gmask = __ballot_sync(0xFFFFFFFFu, got);
+      if (gmask) {
+        uint64_t b = 0, e = 0;
+        if (got) b = td_head[v], e = td_head[v + 1];
+        bool const big = got && e - b > 32;
+        if (got) edges += e - b;
+        // small rows, AW_BATCH neighbours per pass: all ids, then all probes,
+        // then the takes; the warp's finds appended with one atomic per pass
+        uint64_t x = got && !big ? b : e;
+        while (__any_sync(0xFFFFFFFFu, x < e)) {
+          uint32_t w[AW_BATCH], found = 0;
+#pragma unroll
+          for (int k = 0; k < AW_BATCH; ++k) w[k] = x + k < e ? td_adj[x + k] : 0u;
+          uint32_t wd[AW_BATCH];
+#pragma unroll
+          for (int k = 0; k < AW_BATCH; ++k) wd[k] = x + k < e ? op.probe(w[k]) : 0u;
+#pragma unroll
+          for (int k = 0; k < AW_BATCH; ++k)
+            if (x + k < e && op(0u, w[k], true, wd[k])) found |= 1u << k;
+          uint32_t const     c = __popc(found);
+          uint32_t           p = c;
+#pragma unroll
+          for (int d = 1; d < 32; d <<= 1) {
+            uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, p, d);
+            if (lane >= static_cast<unsigned>(d)) p += y;
+          }
+          uint32_t const     tot  = __shfl_sync(0xFFFFFFFFu, p, 31);
+          unsigned long long base = 0;
+          if (lane == 31 && tot) base = atomicAdd(tail, static_cast<unsigned long long>(tot));
+          base = __shfl_sync(0xFFFFFFFFu, base, 31) + p - c;
+#pragma unroll
+          for (int k = 0; k < AW_BATCH; ++k)
+            if ((found >> k) & 1u) {
+              if (base < cap) __stcg(aw + base, AW_TAG | w[k]);
+              ++base;
+            }
+          x = x + AW_BATCH < e ? x + AW_BATCH : e;
+        }
+        for (unsigned todo = __ballot_sync(0xFFFFFFFFu, big); todo; todo &= todo - 1) {
+          unsigned const l  = __ffs(todo) - 1;
+          uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b, l), e0 = __shfl_sync(0xFFFFFFFFu, e, l);
+          for (uint64_t x = b0 + lane; x < e0; x += 32) {
+            uint32_t const w = td_adj[x];
+            if (take(w)) aw_push(w, aw, tail, cap);
+          }
+        }
+        // counted as done when this warp next goes idle (one atomic then)
+        unpublished += __popc(gmask);
+        spins = 0;
+      } else {
+        // nothing arrived: publish this warp's finished items (their finds
+        // are appended first), then finished when every appended item is done
+        if (unpublished) {
+          __threadfence();
+          if (lane == 0) atomicAdd(done, static_cast<unsigned long long>(unpublished));
+          unpublished = 0;
+        }
+        uint32_t stop = 0;
+        if (lane == 0) {
+          unsigned long long const d = ld_acquire64(done);
+          unsigned long long const t = ld_acquire64(tail);
+          stop                       = d == t ? 1u : 0u;
+          if (!stop && (++spins > GRID_SYNC_SPINS || ((spins & 63u) == 63u && ld_acquire(&a.bar->err)))) {
+            atomicExch(&a.bar->err, 1u);
+            stop = 2;
+          }
+        }
+        stop = __shfl_sync(0xFFFFFFFFu, stop, 0);
+        if (stop) {
+          pending = false;
+          alive   = false;
+          failed  = stop == 2;
+        } else __nanosleep(64);
+      }
+    }
+  }
+  if (!grid_sync(a.bar, epoch) || failed) return SEARCH_FAILED;
+  // leave the worklist all zeros
+  uint64_t t = __ldcg(tail);
+  t          = t < cap ? t : cap;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; i < t; i += static_cast<uint64_t>(gridDim.x) * R_THREADS) __stcg(aw + i, 0ull);
+  return SEARCH_DONE;
+}
+
+// Every level of one reachability search (BW: over in-edges, candidates
+// vis_a, reached vis_b; FW: over out-edges, candidates cand, reached vis_a).
+// `glvl` numbers levels across both searches of the launch (it selects
+// counter slots and buffers); `pivot` is the launch's resolved pivot (never
+// the PIVOT_FROM_DEVICE marker).  Block 0 records the search's level counts.
 
 template<bool BW>
 __device__ __forceinline__ int
@@ -801,6 +952,17 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
     uint32_t const qn = static_cast<uint32_t>(qn64);
     if (mat) mode = 0;
     else if (mode == 0 && mf * a.alpha > m_u) mode = 1;
+    if (mode == 0 && lvl >= ASYNC_AFTER && qn <= ASYNC_FRONTIER && a.aw) {
+      // a long, thin search: finish it on the worklist
+      uint64_t  ea = 0;
+      int const r  = run_async(a, fin.q, qn, td_head, td_adj, avail, mark, epoch, ea);
+      if (r != SEARCH_DONE) return r;
+      stamp(a, 13);
+      edges_td += ea;
+      if (tally) st->async_phases += 1;
+      ++lvl;
+      break;
+    }
     unsigned long long* const octr = &st->lq[s_out];
     if (mode == 0) {
       edges_td += mf;
@@ -1097,6 +1259,7 @@ k_fwbw(fwbw_args a)
     st->trim_edges = st->list_n                       = 0;
     st->rows_td = st->pushed_td = 0;
     st->mats = st->bu_bitmap    = 0;
+    st->async_phases            = 0;
     if (search) a.seed.q[0] = p, a.seed.prefix[0] = 0;
   }
   int      rc   = SEARCH_DONE;
@@ -1447,6 +1610,8 @@ launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* s
   a.pv_id       = reinterpret_cast<uint32_t const*>(ws.pivot + 4096) + PV_FINAL;
   a.trim        = trim ? 1u : 0u;
   a.ids_at_end  = trim ? 1u : 0u;
+  a.aw          = static_cast<unsigned long long*>(ws.aw);
+  a.aq          = reinterpret_cast<unsigned long long*>(static_cast<char*>(ws.gbar) + 1024);
   a.indeg       = ws.indeg;
   a.outdeg      = ws.outdeg;
   a.bar         = gbar;
@@ -1471,8 +1636,10 @@ check_persistent(kspn_context* ctx)
   auto* const hs = reinterpret_cast<reach_state*>(ctx->h_state);
   auto* const hb = reinterpret_cast<uint32_t*>(static_cast<char*>(ctx->h_state) + 1024);
   if (*hb || hs->bar_err) {
-    // counters of a launch that gave up are not epoch-aligned: start over
-    KSPN_CUDA(cudaMemsetAsync(ctx->ws.gbar, 0, sizeof(grid_barrier), ctx->stream));
+    // counters of a launch that gave up are not epoch-aligned, and its
+    // worklist may hold entries: start over
+    KSPN_CUDA(cudaMemsetAsync(ctx->ws.gbar, 0, 4096, ctx->stream));
+    KSPN_CUDA(cudaMemsetAsync(ctx->ws.aw, 0, (static_cast<size_t>(ctx->ws.n_cap) + 64) * sizeof(unsigned long long), ctx->stream));
     KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
     throw error{ KSPN_ERR_TIMEOUT, "reachability: grid barrier wait limit reached" };
   }
