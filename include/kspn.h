@@ -47,6 +47,18 @@ extern "C" {
 /* ---------------------------------------------------------------- options */
 #define KSPN_PIPELINE_FAST 0      /* trim_1_first, pivot FW-BW, then rounds of trim fixpoint / trim-2 / label search */
 #define KSPN_PIPELINE_REFERENCE 1 /* the phase order of kaspan::scc (kaspan/scc/scc.hpp:21-87) */
+/* The reference's variants (kaspan/scc/variant/*.hpp), phase order at one
+ * rank, where the n - n/P threshold of the residual variants is 0 (so their
+ * FW-BW / colouring blocks do not run).  The residual step is the device
+ * finish (kspn_residual); pieces too large for it, if any, are finished by
+ * label rounds.  Every pipeline yields the same partition. */
+#define KSPN_PIPELINE_HPC_LIKE 2               /* scc_hpc_like.hpp: trim_1_first, FW-BW, label rounds */
+#define KSPN_PIPELINE_HPC_TRIM_EX 3            /* scc_hpc_trim_ex.hpp: exhaustive trim, degree pivot, FW-BW, label rounds */
+#define KSPN_PIPELINE_ISPAN_LIKE 4             /* scc_ispan_like.hpp: trim_1_first, FW-BW, trim_1_normal x2, residual */
+#define KSPN_PIPELINE_TRIM_EX 5                /* scc_trim_ex.hpp: exhaustive trim, degree pivot, FW-BW, trim, {label, trim} */
+#define KSPN_PIPELINE_TRIM_EX_LIGHT_RESIDUAL 6 /* scc_trim_ex_light_residual.hpp: exhaustive trim, trim, residual */
+#define KSPN_PIPELINE_TRIM_EX_RESIDUAL 7       /* scc_trim_ex_residual.hpp: exhaustive trim, residual */
+#define KSPN_PIPELINE_COUNT 8
 
 typedef struct kspn_options
 {
@@ -234,6 +246,16 @@ int kspn_trim_1_fixpoint(kspn_context* ctx, uint32_t n, uint64_t m,
 /* Exact size-2 trim (no reference counterpart; an addition): decides
  * undecided pairs {u,v} where u's only undecided out-neighbour is v and v's
  * is u, or the same with in-neighbours. */
+/* Residual device finish (the residual step of variant/scc_trim_ex_residual.hpp:110-127:
+ * allgather_fw_sub_graph + tarjan): the sub-graph induced by the undecided
+ * vertices is split into weakly connected pieces, and every piece of at most
+ * 512 vertices and 2048 internal edges is decomposed by Tarjan in one warp's
+ * shared memory; its SCCs get their smallest member as id and leave
+ * `undecided`.  *decided = vertices decided, *pieces_left = pieces too large
+ * (left undecided); both nullable. */
+int kspn_residual(kspn_context* ctx, uint32_t n, uint64_t m,
+                  const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
+                  uint64_t* d_undecided, uint32_t* d_scc_id, uint32_t* decided, uint32_t* pieces_left);
 int kspn_trim_2(kspn_context* ctx, uint32_t n, uint64_t m,
                 const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
                 const uint64_t* d_bw_head, const uint32_t* d_bw_csr,

@@ -26,6 +26,16 @@ LIB_PATH = os.path.join(HERE, "libkspn.so")
 NOALLOC_MAX_N = 1 << 20  # KSPN_NOALLOC_MAX_N
 PIPELINE_FAST = 0
 PIPELINE_REFERENCE = 1
+PIPELINE_HPC_LIKE = 2
+PIPELINE_HPC_TRIM_EX = 3
+PIPELINE_ISPAN_LIKE = 4
+PIPELINE_TRIM_EX = 5
+PIPELINE_TRIM_EX_LIGHT_RESIDUAL = 6
+PIPELINE_TRIM_EX_RESIDUAL = 7
+# the reference's entry points: kaspan::scc and its variants (variant/*.hpp)
+PIPELINES = {"scc": PIPELINE_REFERENCE, "hpc_like": PIPELINE_HPC_LIKE, "hpc_trim_ex": PIPELINE_HPC_TRIM_EX,
+             "ispan_like": PIPELINE_ISPAN_LIKE, "trim_ex": PIPELINE_TRIM_EX,
+             "trim_ex_light_residual": PIPELINE_TRIM_EX_LIGHT_RESIDUAL, "trim_ex_residual": PIPELINE_TRIM_EX_RESIDUAL}
 UNDECIDED = 0xFFFFFFFF
 
 STATUS = {
@@ -160,6 +170,7 @@ SIGNATURES = {
     "kspn_label_search": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _i32, _P, _P]),
     "kspn_trim_1_exhaustive_first": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "kspn_trim_1_fixpoint": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P]),
+    "kspn_residual": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P]),
     "kspn_trim_2": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P]),
     "kspn_normalise": (_i32, [_P, _u32, _P]),
     "kspn_normalise_noalloc": (_i32, [_u32, _P, _P]),
@@ -320,6 +331,12 @@ class Context:
         d = C.c_uint32()
         self._check(lib().kspn_trim_2(self.h, n, m, _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc), _ptr(und), _ptr(scc_id), C.byref(d)), "trim_2")
         return d.value
+
+    def residual(self, n, m, fwh, fwc, und, scc_id):
+        """(vertices decided, pieces left undecided)."""
+        d, left = C.c_uint32(), C.c_uint32()
+        self._check(lib().kspn_residual(self.h, n, m, _ptr(fwh), _ptr(fwc), _ptr(und), _ptr(scc_id), C.byref(d), C.byref(left)), "residual")
+        return d.value, left.value
 
     def normalise(self, n, scc_id):
         self._check(lib().kspn_normalise(self.h, n, _ptr(scc_id)), "normalise")

@@ -168,7 +168,7 @@ struct graph_store
 void
 check_options(kspn_options const& o)
 {
-  if (o.pipeline != KSPN_PIPELINE_FAST && o.pipeline != KSPN_PIPELINE_REFERENCE) throw error{ KSPN_ERR_INVALID_ARGUMENT, "unknown pipeline" };
+  if (o.pipeline < 0 || o.pipeline >= KSPN_PIPELINE_COUNT) throw error{ KSPN_ERR_INVALID_ARGUMENT, "unknown pipeline" };
 }
 
 kspn_options
@@ -256,6 +256,61 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
       if (st && st->label_calls >= round_cap) throw error{ KSPN_ERR_TIMEOUT, "label-search call cap exceeded" };
       label_ran = true;
       add(KSPN_PHASE_LABEL, label_search(ctx, g, und, scc_id, ++rotation, opt, st));
+    }
+  } else if (opt.pipeline != KSPN_PIPELINE_FAST) {
+    // the reference's variants (variant/*.hpp), phase order at one rank
+    int        p        = opt.pipeline;
+    int        rotation = 0;
+    uint32_t   calls    = 0;
+    auto const label_rounds = [&](bool trim_between) {
+      while (decided < g.n) {
+        if (++calls > round_cap) throw error{ KSPN_ERR_TIMEOUT, "label-search call cap exceeded" };
+        label_ran = true;
+        add(KSPN_PHASE_LABEL, label_search(ctx, g, und, scc_id, ++rotation, opt, st));
+        if (trim_between && decided < g.n) add(KSPN_PHASE_TRIM, trim_fixpoint(ctx, g, und, scc_id, false, 0));
+      }
+    };
+    auto const fwbw_from = [&](uint32_t pivot) {
+      if (st) st->pivot = pivot;
+      add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pivot, opt, st, true));
+    };
+    bool const exhaustive = p == KSPN_PIPELINE_HPC_TRIM_EX || p == KSPN_PIPELINE_TRIM_EX || p == KSPN_PIPELINE_TRIM_EX_LIGHT_RESIDUAL || p == KSPN_PIPELINE_TRIM_EX_RESIDUAL;
+    uint32_t   pivot      = g.n;
+    if (exhaustive) add(KSPN_PHASE_TRIM_FIRST, trim_exhaustive_first(ctx, g, und, scc_id, ws.outdeg, ws.indeg));
+    else {
+      pivot = trim_1_first(ctx, g, und, scc_id, nullptr, nullptr, false);
+      add(KSPN_PHASE_TRIM_FIRST, ctx->h_ctr[CTR_AUX]);
+    }
+    switch (p) {
+    case KSPN_PIPELINE_HPC_LIKE: // scc_hpc_like.hpp:33-66
+      if (decided < g.n) fwbw_from(pivot);
+      label_rounds(false);
+      break;
+    case KSPN_PIPELINE_HPC_TRIM_EX: // scc_hpc_trim_ex.hpp:33-73
+      if (decided < g.n) fwbw_from(select_pivot_live(ctx, g, und));
+      label_rounds(false);
+      break;
+    case KSPN_PIPELINE_ISPAN_LIKE: // scc_ispan_like.hpp:33-84
+      if (decided < g.n) fwbw_from(pivot);
+      if (decided < g.n) add(KSPN_PHASE_TRIM_NORMAL, trim_1_normal(ctx, g, und, scc_id));
+      if (decided < g.n) add(KSPN_PHASE_TRIM_NORMAL, trim_1_normal(ctx, g, und, scc_id));
+      if (decided < g.n) add(KSPN_PHASE_RESIDUAL, residual(ctx, g, und, scc_id, nullptr));
+      label_rounds(false);
+      break;
+    case KSPN_PIPELINE_TRIM_EX: // scc_trim_ex.hpp:33-99
+      if (decided < g.n) fwbw_from(select_pivot_live(ctx, g, und));
+      if (decided < g.n) add(KSPN_PHASE_TRIM, trim_fixpoint(ctx, g, und, scc_id, false, 0));
+      label_rounds(true);
+      break;
+    case KSPN_PIPELINE_TRIM_EX_LIGHT_RESIDUAL: // scc_trim_ex_light_residual.hpp:33-118 (threshold 0 at one rank)
+      if (decided < g.n) add(KSPN_PHASE_TRIM, trim_fixpoint(ctx, g, und, scc_id, false, 0));
+      if (decided < g.n) add(KSPN_PHASE_RESIDUAL, residual(ctx, g, und, scc_id, nullptr));
+      label_rounds(false);
+      break;
+    default: // KSPN_PIPELINE_TRIM_EX_RESIDUAL, scc_trim_ex_residual.hpp:33-127 (threshold 0 at one rank)
+      if (decided < g.n) add(KSPN_PHASE_RESIDUAL, residual(ctx, g, und, scc_id, nullptr));
+      label_rounds(false);
+      break;
     }
   } else {
     // trim_1_first's pivot (argmax in*out) lies in the giant component of
@@ -697,6 +752,22 @@ kspn_trim_2(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_head
     dgraph const   g{ n, m, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr };
     uint32_t const d = n ? trim_2(ctx, g, reinterpret_cast<uint32_t*>(d_undecided), d_scc_id) : 0;
     if (decided) *decided = d;
+  });
+}
+
+int
+kspn_residual(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_head, const uint32_t* d_fw_csr, uint64_t* d_undecided, uint32_t* d_scc_id, uint32_t* decided, uint32_t* pieces_left)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(d_fw_head && (m == 0 || d_fw_csr) && d_undecided && d_scc_id, "null pointer");
+    bind_device(ctx);
+    ensure_workspace(ctx, n, m);
+    dgraph const   g{ n, m, d_fw_head, d_fw_csr, nullptr, nullptr };
+    uint32_t       left = 0;
+    uint32_t const d    = n ? residual(ctx, g, reinterpret_cast<uint32_t*>(d_undecided), d_scc_id, &left) : 0;
+    if (decided) *decided = d;
+    if (pieces_left) *pieces_left = left;
   });
 }
 

@@ -358,6 +358,9 @@ uint32_t trim_fixpoint(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32
 uint32_t trim_exhaustive_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* outdeg, uint32_t* indeg);
 uint32_t trim_2(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id);
 uint32_t select_pivot_live(kspn_context* ctx, dgraph const& g, uint32_t const* und);
+// residual.cu: Tarjan per weakly connected undecided piece that fits a warp's
+// shared memory; returns vertices decided, *pieces_left = pieces left over
+uint32_t residual(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* pieces_left);
 uint32_t count_undecided(kspn_context* ctx, uint32_t n, uint32_t const* und);
 
 // reach.cu

@@ -266,3 +266,50 @@ def test_rgg_capacity_error(ctx):
     dst = torch.empty(m - 1, dtype=torch.int32, device="cuda")
     with pytest.raises(K.KspnError):
         ctx.gen_rgg(n, 3, g, r2, src, dst, m - 1)
+
+
+def _wcc(G, keep):
+    """Weakly connected pieces of the sub-graph induced by `keep` (bool[n]):
+    (piece label per vertex, internal edge count per piece)."""
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.csgraph import connected_components
+
+    src = np.repeat(np.arange(G.n), np.diff(G.fwh.astype(np.int64)))
+    dst = G.fwc[: G.m].astype(np.int64)
+    ok = keep[src] & keep[dst] & (src != dst)
+    A = csr_matrix((np.ones(int(ok.sum())), (src[ok], dst[ok])), shape=(G.n, G.n))
+    _, lab = connected_components(A, directed=True, connection="weak")
+    edges = np.bincount(lab[src[ok]], minlength=lab.max() + 1)
+    return lab, edges
+
+
+@pytest.mark.parametrize("name,G", GRAPHS, ids=[g[0] for g in GRAPHS])
+def test_residual(ctx, name, G):
+    """kspn_residual = Tarjan on the sub-graph induced by the undecided
+    vertices (variant/scc_trim_ex_residual.hpp:110-127), each SCC named by
+    its smallest member -- for every weakly connected piece of at most 512
+    vertices and 2048 internal edges; larger pieces stay undecided."""
+    rng = np.random.default_rng(len(name))
+    for frac in (1.0, 0.6):
+        keep = rng.random(G.n) < frac if frac < 1.0 else np.ones(G.n, bool)
+        sid = np.where(keep, np.uint32(0xFFFFFFFF), np.arange(G.n, dtype=np.uint32)).astype(np.uint32)
+        d_bits, d_sid = bits_to_dev(O.bits_from_bytes(keep.astype(np.uint8), G.n)), u32_to_dev(sid)
+        fwh, fwc, _, _ = device(G)
+        decided, left = ctx.residual(G.n, G.m, fwh, fwc, d_bits, d_sid)
+        after = O.bytes_from_bits(dev_to_bits(d_bits), G.n).astype(bool)
+        ids = dev_to_u32(d_sid)[: G.n]
+        # expected: Tarjan of the induced sub-graph
+        src = np.repeat(np.arange(G.n, dtype=np.uint32), np.diff(G.fwh.astype(np.int64)))
+        dst = G.fwc[: G.m]
+        ok = keep[src] & keep[dst]
+        truth = O.tarjan(O.from_edges(G.n, src[ok], dst[ok]))
+        lab, edges = _wcc(G, keep)
+        size = np.bincount(lab, minlength=lab.max() + 1)
+        small = (size <= 512) & (edges <= 2048)
+        fits = keep & small[lab]
+        assert left == len(np.unique(lab[keep & ~small[lab]]))
+        assert decided == int(fits.sum())
+        assert np.array_equal(after, keep & ~fits)
+        assert np.array_equal(ids[fits], truth[fits])
+        assert np.array_equal(ids[~keep], sid[~keep])
+        assert np.all(ids[keep & ~fits] == 0xFFFFFFFF)

@@ -12,7 +12,8 @@ from kspn_testlib import KAT_IDS, device, edge_case_graphs, fuzzy_cases, kat_gra
 
 pytestmark = pytest.mark.gpu
 
-PIPELINES = [K.PIPELINE_FAST, K.PIPELINE_REFERENCE]
+PIPELINES = [K.PIPELINE_FAST, K.PIPELINE_REFERENCE, K.PIPELINE_HPC_LIKE, K.PIPELINE_HPC_TRIM_EX, K.PIPELINE_ISPAN_LIKE,
+             K.PIPELINE_TRIM_EX, K.PIPELINE_TRIM_EX_LIGHT_RESIDUAL, K.PIPELINE_TRIM_EX_RESIDUAL]
 
 
 def run_device(ctx, G, pipeline, with_bw=True):
@@ -109,3 +110,18 @@ def test_iteration_cap_reports_timeout(ctx):
         ctx.scc(G.n, G.fwh, G.fwc, G.bwh, G.bwc, options=opt)
     assert e.value.status == 4
     assert np.array_equal(ctx.scc(G.n, G.fwh, G.fwc, G.bwh, G.bwc), O.tarjan(G))
+
+
+@pytest.mark.parametrize("variant", sorted(K.PIPELINES))
+def test_variant_matches_reference(ctx, variant):
+    """Each reference entry point (kaspan::scc and variant/*.hpp, compiled
+    from its sources) and the kspn pipeline of the same name give the same
+    partition after the min-id relabel."""
+    if O.ref_lib() is None:
+        pytest.skip("oracle/_ref not built")
+    graphs = [kat_graph(), O.gnm(1 << 12, 1 << 14, 3), O.rmat(12, 8, 5), O.rgg(1 << 12, 6)]
+    graphs += [G for _, G, _ in fuzzy_cases((40, 200), seeds=(3,), degrees=(1.0, 4.0))]
+    for G in graphs:
+        ref, _ = O.ref_scc(G, variant)
+        ids, _ = run_device(ctx, G, K.PIPELINES[variant])
+        assert np.array_equal(ids, ref), (variant, G.n, G.m)
