@@ -350,6 +350,9 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
       rounds      = 1;
       trimmed     = true;
       und_checked = decided == g.n; // the launch counted und: empty
+      // what is left splits into small pieces on most graphs: Tarjan per
+      // piece in shared memory; larger pieces go on to the rounds below
+      if (decided < g.n) add(KSPN_PHASE_RESIDUAL, residual(ctx, g, und, scc_id, nullptr));
     } else {
       uint32_t const pivot = trim_1_first(ctx, g, und, scc_id, nullptr, nullptr, false);
       add(KSPN_PHASE_TRIM_FIRST, ctx->h_ctr[CTR_AUX]);
