@@ -236,6 +236,45 @@ def run_kspn(args):
         m_total = float(G.m)
     value = m_total / (ms * 1e-3)
 
+    # ---- learned vs plain pivot (same output): the workload, and the
+    # workload with decoy hubs (vertices whose in * out beats every real one
+    # while their out-edges all end at dead ends)
+    learned_vs_plain = None
+    model = K.default_pivot_model()
+    if model is not None and args.workload.startswith("rmat") and world == 1:
+        from kaspan_b200.pivot_train import decoy_rmat
+
+        def timed(graph, options, steps):
+            o = torch.empty(graph.n, dtype=torch.int32, device="cuda")
+            s_ = K.Stats()
+            ctx.scc_device(graph.n, graph.m, graph.fwh, graph.fwc, graph.bwh, graph.bwc, o, options, s_)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                ctx.scc_device(graph.n, graph.m, graph.fwh, graph.fwc, graph.bwh, graph.bwc, o, options, s_)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            d = s_.as_dict()
+            return o.cpu().numpy().view(np.uint32).copy(), {"ms_per_step": e0.elapsed_time(e1) / steps, "edges_scanned": d["edges_scanned"],
+                                                            "pivot": d["pivot"], "fwbw_decided": d["decided"]["fwbw"]}
+
+        ctx.set_pivot_model(model)
+        learned_vs_plain = {"model": "kaspan_b200/pivot_model.npy (8-32-32-1, trained on the GPU: python -m kaspan_b200.pivot_train)"}
+        for label, graph in (("workload", G), ("workload_with_decoys", None)):
+            if graph is None:
+                p_ = WORKLOADS[args.workload][1]
+                graph, hubs = decoy_rmat(ctx, p_["scale"], p_["seed"] + 100, 0.57, decoys=8)
+            ids_p, plain = timed(graph, opt, max(3, min(args.steps, 10)))
+            ids_l, learned = timed(graph, K.default_options(pipeline=pipeline, validate=0, learned_pivot=1), max(3, min(args.steps, 10)))
+            assert np.array_equal(ids_p, ids_l), "learned and plain pivots must give the same partition"
+            learned_vs_plain[label] = {"n": graph.n, "m": graph.m, "plain": plain, "learned": learned,
+                                       "speedup": plain["ms_per_step"] / learned["ms_per_step"], "identical_output": True}
+            if label != "workload":
+                del graph
+        ctx.set_pivot_model(None)
+        torch.cuda.empty_cache()
+
     # correctness spot check of the last step (canonical ids are min members)
     ids = out.cpu().numpy().view(np.uint32)
     assert (ids <= np.arange(G.n, dtype=np.uint32)).all(), "ids must name a member no larger than the vertex"
@@ -306,6 +345,7 @@ def run_kspn(args):
                          "model": last["resident"],
                          "pipeline_min_bytes": b_min, "pipeline_frac": (b_min / (ms * 1e-3)) / 1e9 / peak},
             "clocks": clk.summary(),
+            "learned_vs_plain": learned_vs_plain,
             "phases": {"decided": last["decided"], "ms": {k: round(v, 4) for k, v in last["ms"].items()}, "levels_fw": last["levels_fw"],
                        "levels_bw": last["levels_bw"], "bottom_up": last["levels_bottom_up"], "label_calls": last["label_calls"],
                        "edges_scanned": last["edges_scanned"], "trace": trace,

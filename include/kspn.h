@@ -73,7 +73,9 @@ typedef struct kspn_options
   uint32_t max_rounds;      /* cap on pipeline rounds (0 = n + 2) */
   int32_t  profile;         /* 1: time kernel classes with CUDA events (kspn_stats.kernel_*) */
   int32_t  trace;           /* 1: timestamp the phases of the persistent searches (kspn_stats.search_*) */
-  uint32_t reserved[5];
+  int32_t  learned_pivot;   /* 1: FAST pipeline picks its FW-BW pivot with the context's pivot model
+                               (kspn_set_pivot_model) instead of argmax in*out; same partition */
+  uint32_t reserved[4];
 } kspn_options;
 
 /* Per-call statistics (all fields written by a successful call). */
@@ -288,6 +290,34 @@ int kspn_normalise_noalloc(uint32_t n, uint32_t* d_scc_id, void* stream);
 int kspn_transpose(kspn_context* ctx, uint32_t n, uint64_t m,
                    const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
                    uint64_t* d_bw_head, uint32_t* d_bw_csr);
+
+/* ---------------------------------------------------------------- learned pivot
+ * No reference counterpart.  An MLP 8 -> 32 -> 32 -> 1 (ReLU; BF16-rounded
+ * weights, FP32 accumulation) scores pivot candidates by the odds that they
+ * lie in the largest SCC; the FAST pipeline with kspn_options.learned_pivot
+ * starts FW-BW from the best of trim_1_first's per-block candidates.  Only
+ * the starting vertex changes, so the partition is the same.  Parameters:
+ * W1[32][8], b1[32], W2[32][32], b2[32], w3[32], b3 (FP32). */
+#define KSPN_MLP_PARAMS 1377
+#define KSPN_MLP_FEATURES 8
+/* Copies the model (host, KSPN_MLP_PARAMS floats) to the context's device;
+ * NULL removes it. */
+int kspn_set_pivot_model(kspn_context* ctx, const float* params);
+/* Features (count x 8 FP32, device) of device vertex list d_vertices. */
+int kspn_mlp_features(kspn_context* ctx, uint32_t n, uint64_t m,
+                      const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
+                      const uint64_t* d_bw_head, const uint32_t* d_bw_csr,
+                      uint32_t count, const uint32_t* d_vertices, float* d_features);
+/* Logits of count feature rows with device parameters d_params. */
+int kspn_mlp_forward(kspn_context* ctx, uint32_t count, const float* d_features, const float* d_params, float* d_logits);
+/* Mean binary cross-entropy of sigmoid(logit) against d_labels (0 / 1) and
+ * its gradient w.r.t. the FP32 parameters (through the BF16 rounding, as a
+ * straight-through estimate): d_grad (KSPN_MLP_PARAMS), d_loss (1). */
+int kspn_mlp_gradient(kspn_context* ctx, uint32_t count, const float* d_features, const float* d_labels,
+                      const float* d_params, float* d_grad, float* d_loss);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8; step counts from 1) on the
+ * device parameters, with moment buffers d_m, d_v (KSPN_MLP_PARAMS each). */
+int kspn_mlp_adam(kspn_context* ctx, float* d_params, const float* d_grad, float* d_m, float* d_v, float lr, int step);
 
 /* ---------------------------------------------------------------- inputs */
 /*

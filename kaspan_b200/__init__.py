@@ -24,6 +24,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libkspn.so")
 
 NOALLOC_MAX_N = 1 << 20  # KSPN_NOALLOC_MAX_N
+MLP_PARAMS = 1377
+MLP_FEATURES = 8
 PIPELINE_FAST = 0
 PIPELINE_REFERENCE = 1
 PIPELINE_HPC_LIKE = 2
@@ -66,7 +68,8 @@ class Options(C.Structure):
         ("max_rounds", C.c_uint32),
         ("profile", C.c_int32),
         ("trace", C.c_int32),
-        ("reserved", C.c_uint32 * 5),
+        ("learned_pivot", C.c_int32),
+        ("reserved", C.c_uint32 * 4),
     ]
 
 
@@ -170,6 +173,11 @@ SIGNATURES = {
     "kspn_label_search": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _i32, _P, _P]),
     "kspn_trim_1_exhaustive_first": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "kspn_trim_1_fixpoint": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P]),
+    "kspn_set_pivot_model": (_i32, [_P, _P]),
+    "kspn_mlp_features": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _u32, _P, _P]),
+    "kspn_mlp_forward": (_i32, [_P, _u32, _P, _P, _P]),
+    "kspn_mlp_gradient": (_i32, [_P, _u32, _P, _P, _P, _P, _P]),
+    "kspn_mlp_adam": (_i32, [_P, _P, _P, _P, _P, C.c_float, _i32]),
     "kspn_residual": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P]),
     "kspn_trim_2": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P]),
     "kspn_normalise": (_i32, [_P, _u32, _P]),
@@ -197,6 +205,13 @@ def lib() -> C.CDLL:
             f.argtypes = args
         _lib = L
     return _lib
+
+
+def default_pivot_model():
+    """The shipped pivot model (numpy float32[MLP_PARAMS]) or None: trained
+    by `python -m kaspan_b200.pivot_train` on the GPU."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "pivot_model.npy")
+    return np.load(path).astype(np.float32) if os.path.exists(path) else None
 
 
 def default_options(**kw) -> Options:
@@ -337,6 +352,28 @@ class Context:
         d, left = C.c_uint32(), C.c_uint32()
         self._check(lib().kspn_residual(self.h, n, m, _ptr(fwh), _ptr(fwc), _ptr(und), _ptr(scc_id), C.byref(d), C.byref(left)), "residual")
         return d.value, left.value
+
+    # ---- learned pivot (no reference counterpart)
+    def set_pivot_model(self, params):
+        """params: numpy float32[MLP_PARAMS], or None to remove the model."""
+        if params is None:
+            self._check(lib().kspn_set_pivot_model(self.h, None), "set_pivot_model")
+            return
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        assert p.size == MLP_PARAMS
+        self._check(lib().kspn_set_pivot_model(self.h, p.ctypes.data), "set_pivot_model")
+
+    def mlp_features(self, n, m, fwh, fwc, bwh, bwc, vertices, features):
+        self._check(lib().kspn_mlp_features(self.h, n, m, _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc), vertices.numel(), _ptr(vertices), _ptr(features)), "mlp_features")
+
+    def mlp_forward(self, features, params, logits):
+        self._check(lib().kspn_mlp_forward(self.h, features.shape[0], _ptr(features), _ptr(params), _ptr(logits)), "mlp_forward")
+
+    def mlp_gradient(self, features, labels, params, grad, loss):
+        self._check(lib().kspn_mlp_gradient(self.h, features.shape[0], _ptr(features), _ptr(labels), _ptr(params), _ptr(grad), _ptr(loss)), "mlp_gradient")
+
+    def mlp_adam(self, params, grad, m, v, lr, step):
+        self._check(lib().kspn_mlp_adam(self.h, _ptr(params), _ptr(grad), _ptr(m), _ptr(v), float(lr), int(step)), "mlp_adam")
 
     def normalise(self, n, scc_id):
         self._check(lib().kspn_normalise(self.h, n, _ptr(scc_id)), "normalise")

@@ -322,6 +322,7 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
       // trim_1_first, then FW-BW and the trim fixpoint in ONE persistent
       // launch that takes the pivot from device memory: one host sync
       trim_1_first_async(ctx, g, und);
+      if (opt.learned_pivot && ctx->pivot_model) learned_pivot(ctx, g, ctx->pivot_model);
       KSPN_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
       fw_bw_trim_async(ctx, g, und, scc_id, opt, st, ctx->ev[4]);
       KSPN_CUDA(cudaMemcpyAsync(ctx->h_ctr, ws.ctr, 64 * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
@@ -354,8 +355,14 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
       // piece in shared memory; larger pieces go on to the rounds below
       if (decided < g.n) add(KSPN_PHASE_RESIDUAL, residual(ctx, g, und, scc_id, nullptr));
     } else {
-      uint32_t const pivot = trim_1_first(ctx, g, und, scc_id, nullptr, nullptr, false);
+      uint32_t pivot = trim_1_first(ctx, g, und, scc_id, nullptr, nullptr, false);
       add(KSPN_PHASE_TRIM_FIRST, ctx->h_ctr[CTR_AUX]);
+      if (decided < g.n && opt.learned_pivot && ctx->pivot_model) {
+        // the model's choice among trim_1_first's per-block candidates
+        learned_pivot(ctx, g, ctx->pivot_model);
+        KSPN_CUDA(cudaMemcpyAsync(&pivot, reinterpret_cast<uint32_t*>(ws.pivot + 4096) + PV_FINAL, sizeof(pivot), cudaMemcpyDeviceToHost, ctx->stream));
+        KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+      }
       if (decided < g.n) {
         if (st) st->pivot = pivot;
         add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pivot, opt, st, true));
@@ -563,6 +570,7 @@ kspn_context_destroy(kspn_context* ctx)
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   release_graphs(ctx);
+  if (ctx->pivot_model) cudaFree(ctx->pivot_model);
   if (ctx->ws.base) cudaFree(ctx->ws.base);
   if (ctx->h_ctr) cudaFreeHost(ctx->h_ctr);
   if (ctx->h_state) cudaFreeHost(ctx->h_state);
@@ -755,6 +763,85 @@ kspn_trim_2(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_head
     dgraph const   g{ n, m, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr };
     uint32_t const d = n ? trim_2(ctx, g, reinterpret_cast<uint32_t*>(d_undecided), d_scc_id) : 0;
     if (decided) *decided = d;
+  });
+}
+
+int
+kspn_set_pivot_model(kspn_context* ctx, const float* params)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    bind_device(ctx);
+    if (!params) {
+      if (ctx->pivot_model) {
+        KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+        cudaFree(ctx->pivot_model);
+      }
+      ctx->pivot_model = nullptr;
+      return;
+    }
+    if (!ctx->pivot_model) {
+      void* p = nullptr;
+      if (cudaMalloc(&p, KSPN_MLP_PARAMS * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        throw error{ KSPN_ERR_OOM, "pivot model" };
+      }
+      ctx->pivot_model = static_cast<float*>(p);
+    }
+    KSPN_CUDA(cudaMemcpyAsync(ctx->pivot_model, params, KSPN_MLP_PARAMS * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int
+kspn_mlp_features(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_head, const uint32_t* d_fw_csr, const uint64_t* d_bw_head, const uint32_t* d_bw_csr, uint32_t count,
+                  const uint32_t* d_vertices, float* d_features)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(count == 0 || (d_fw_head && d_fw_csr && d_bw_head && d_bw_csr && d_vertices && d_features), "null pointer");
+    bind_device(ctx);
+    ensure_workspace(ctx, n, m);
+    dgraph const g{ n, m, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr };
+    mlp_features(ctx, g, count, d_vertices, d_features);
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int
+kspn_mlp_forward(kspn_context* ctx, uint32_t count, const float* d_features, const float* d_params, float* d_logits)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(d_params && (count == 0 || (d_features && d_logits)), "null pointer");
+    bind_device(ctx);
+    mlp_forward(ctx, count, d_features, d_params, d_logits);
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int
+kspn_mlp_gradient(kspn_context* ctx, uint32_t count, const float* d_features, const float* d_labels, const float* d_params, float* d_grad, float* d_loss)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(d_params && d_grad && d_loss && (count == 0 || (d_features && d_labels)), "null pointer");
+    bind_device(ctx);
+    mlp_grad(ctx, count, d_features, d_labels, d_params, d_grad, d_loss);
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int
+kspn_mlp_adam(kspn_context* ctx, float* d_params, const float* d_grad, float* d_m, float* d_v, float lr, int step)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(d_params && d_grad && d_m && d_v, "null pointer");
+    require(step >= 1, "step counts from 1");
+    bind_device(ctx);
+    mlp_adam(ctx, d_params, d_grad, d_m, d_v, lr, step);
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
   });
 }
 

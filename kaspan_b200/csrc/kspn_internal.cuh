@@ -296,6 +296,7 @@ struct kspn_context
   cudaEvent_t        pe[4]      = {};
   void*              h_state    = nullptr; // pinned 4 KiB mirror of ws.rstate
   unsigned           search_grid = 0;      // blocks of the persistent FW-BW launch
+  float*             pivot_model = nullptr; // device copy of the pivot MLP (kspn_set_pivot_model)
   kspn::cached_graph trim;                 // one-launch trim fixpoint graph
   kspn::dev_buffer   bufs[kspn::BUF_COUNT];
 };
@@ -358,6 +359,14 @@ uint32_t trim_fixpoint(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32
 uint32_t trim_exhaustive_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* outdeg, uint32_t* indeg);
 uint32_t trim_2(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id);
 uint32_t select_pivot_live(kspn_context* ctx, dgraph const& g, uint32_t const* und);
+// trim.cu: k_trim_first's grid = the number of per-block pivot candidates
+unsigned pivot_candidates(uint32_t n);
+// mlp.cu: the learned pivot model (KSPN_MLP_PARAMS FP32 parameters)
+void mlp_features(kspn_context* ctx, dgraph const& g, uint32_t count, uint32_t const* vs, float* feat);
+void mlp_forward(kspn_context* ctx, uint32_t count, float const* feat, float const* params, float* out);
+void mlp_grad(kspn_context* ctx, uint32_t count, float const* feat, float const* y, float const* params, float* grad, float* loss);
+void mlp_adam(kspn_context* ctx, float* params, float const* grad, float* m, float* v, float lr, int step);
+void learned_pivot(kspn_context* ctx, dgraph const& g, float const* params);
 // residual.cu: Tarjan per weakly connected undecided piece that fits a warp's
 // shared memory; returns vertices decided, *pieces_left = pieces left over
 uint32_t residual(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* pieces_left);

@@ -777,7 +777,7 @@ trim_1_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id
 {
   auto& ws = ctx->ws;
   zero_counters(ctx);
-  unsigned const nb = stream_grid((static_cast<uint64_t>(g.n) + TF_ITEMS - 1) / TF_ITEMS);
+  unsigned const nb = pivot_candidates(g.n);
   prof_start(ctx);
   k_trim_first<<<nb, T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.bh, und, scc_id, init_degrees ? ws.indeg : nullptr, init_degrees ? ws.outdeg : nullptr, queue_out, ws.ctr, ws.pivot, reinterpret_cast<uint32_t*>(ws.pivot + 4096));
   prof_stop(ctx);
@@ -799,6 +799,12 @@ trim_1_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id
   return (prod == 0 || pivot == NONE) ? g.n : pivot;
 }
 
+unsigned
+pivot_candidates(uint32_t n)
+{
+  return stream_grid((static_cast<uint64_t>(n) + TF_ITEMS - 1) / TF_ITEMS);
+}
+
 // (the caller has zeroed ws.ctr; ids are not written: the resident
 // launch that follows writes every vertex's id at its end)
 void
@@ -806,7 +812,7 @@ trim_1_first_async(kspn_context* ctx, dgraph const& g, uint32_t* und)
 {
   auto& ws = ctx->ws;
   prof_start(ctx);
-  k_trim_first<<<stream_grid((static_cast<uint64_t>(g.n) + TF_ITEMS - 1) / TF_ITEMS), T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.bh, und, nullptr, nullptr, nullptr, nullptr, ws.ctr, ws.pivot, reinterpret_cast<uint32_t*>(ws.pivot + 4096));
+  k_trim_first<<<pivot_candidates(g.n), T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.bh, und, nullptr, nullptr, nullptr, nullptr, ws.ctr, ws.pivot, reinterpret_cast<uint32_t*>(ws.pivot + 4096));
   prof_stop(ctx);
   KSPN_CHECK_LAUNCH();
   ctx->launches += 1;
