@@ -74,8 +74,12 @@ layout(workspace& ws, char* base, uint32_t n, uint64_t m)
   ws.seed_q            = c.take<uint32_t>(4);
   ws.seed_prefix       = c.take<uint64_t>(4);
   ws.gbar              = c.take<char>(4096);
-  ws.aw                = c.take<unsigned long long>(nn + 64);
+  ws.heavy_cap         = heavy_capacity(n, m);
+  ws.aw_entries        = nn + 64 + m / HEAVY_SLICE + 32; // every vertex once, every extra slice of a heavy row once
+  ws.aw                = c.take<unsigned long long>(ws.aw_entries);
   ws.rstate            = c.take<char>(4096);
+  ws.heavy             = c.take<uint32_t>(4 * ws.heavy_cap);
+  ws.cutmap            = c.take<uint32_t>(words);
   return align_up(c.off);
 }
 
@@ -109,7 +113,8 @@ ensure_workspace(kspn_context* ctx, uint32_t n, uint64_t m)
   KSPN_CUDA(cudaMemsetAsync(ws.ctr, 0, 64 * sizeof(uint32_t), ctx->stream));
   KSPN_CUDA(cudaMemsetAsync(ws.tile_zero, 0, (mcap / 2048 + 4) * sizeof(uint32_t), ctx->stream));
   KSPN_CUDA(cudaMemsetAsync(ws.gbar, 0, 4096, ctx->stream));
-  KSPN_CUDA(cudaMemsetAsync(ws.aw, 0, (static_cast<size_t>(ncap) + 2 + 64) * sizeof(unsigned long long), ctx->stream));
+  KSPN_CUDA(cudaMemsetAsync(ws.aw, 0, ws.aw_entries * sizeof(unsigned long long), ctx->stream));
+  KSPN_CUDA(cudaMemsetAsync(ws.cutmap, 0, ((static_cast<size_t>(ncap) + 63) / 64 * 2 + 2) * sizeof(uint32_t), ctx->stream));
 }
 
 void*
@@ -318,6 +323,22 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
     // the trim fixpoint then only walks the (small) remainder
     uint32_t rounds  = 0;
     bool     trimmed = false; // this round's trim fixpoint already ran
+    // A large remainder after the first FW-BW means its pivot missed the
+    // giant component (e.g. a hub whose out-edges all end at dead ends):
+    // FW-BW again from the largest live in * out (degrees are current after
+    // a trim fixpoint), while each round still decides a share of it.
+    auto const fwbw_again = [&]() {
+      uint64_t const big = std::max<uint64_t>(g.n / 16, 1u << 16);
+      for (uint32_t again = 0; again < 3 && g.n - decided >= big; ++again) {
+        uint64_t const left = g.n - decided;
+        uint32_t const pv   = select_pivot_live(ctx, g, und);
+        if (pv >= g.n) break;
+        uint64_t const d0 = decided;
+        add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pv, opt, st, true));
+        if (decided < g.n) add(KSPN_PHASE_TRIM, trim_fixpoint(ctx, g, und, scc_id, false, 0));
+        if ((decided - d0) * 64 < left) break;
+      }
+    };
     if (!ctx->prof && resident_fits(g)) {
       // trim_1_first, then FW-BW and the trim fixpoint in ONE persistent
       // launch that takes the pivot from device memory: one host sync
@@ -351,6 +372,7 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
       rounds      = 1;
       trimmed     = true;
       und_checked = decided == g.n; // the launch counted und: empty
+      if (decided < g.n) fwbw_again();
       // what is left splits into small pieces on most graphs: Tarjan per
       // piece in shared memory; larger pieces go on to the rounds below
       if (decided < g.n) add(KSPN_PHASE_RESIDUAL, residual(ctx, g, und, scc_id, nullptr));
@@ -366,6 +388,10 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
       if (decided < g.n) {
         if (st) st->pivot = pivot;
         add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pivot, opt, st, true));
+      }
+      if (decided < g.n && g.n - decided >= std::max<uint64_t>(g.n / 16, 1u << 16)) {
+        add(KSPN_PHASE_TRIM, trim_fixpoint(ctx, g, und, scc_id, false, 0));
+        fwbw_again();
       }
     }
     int rotation = 0;

@@ -110,6 +110,61 @@ warp_push_active(uint32_t v, uint32_t* queue, uint32_t* count)
   queue[base + __popc(mask & ((1u << lane) - 1u))] = v;
 }
 
+// ---------------------------------------------------------------- heavy rows
+// A row longer than HEAVY_ROW edges is never walked by one thread or one
+// warp alone (on skewed graphs one such row would serialise a whole
+// phase): it is listed, and every warp of the grid takes slices of
+// HEAVY_SLICE edges of every listed row.
+constexpr uint32_t HEAVY_ROW   = 2048;
+constexpr uint32_t HEAVY_SLICE = 1024;
+
+// Entries of one heavy list: a list holds each vertex at most once per
+// direction, and only vertices with a row longer than HEAVY_ROW (at most
+// m / HEAVY_ROW per direction).
+inline uint64_t
+heavy_capacity(uint32_t n, uint64_t m)
+{
+  uint64_t const c = 2 * (m / HEAVY_ROW);
+  return (c < 2ull * n ? c : 2ull * n) + 32;
+}
+
+// fn(i, v, b, e) for the slices of the listed rows that fall to this warp
+// (slice s of entry i goes to warp (i + s) mod W of the grid's W warps);
+// [b, e) is one slice of v's row in `head`.  HEAVY_ONLY: rows of at most
+// HEAVY_ROW entries are skipped (their owner walks them).  All lanes of
+// every warp call it; fn is called warp-uniformly.  Entries are read
+// through L2 (the list was written by other blocks of the same launch).
+template<bool HEAVY_ONLY = false, class F>
+__device__ __forceinline__ void
+heavy_slices(uint32_t const* list, uint32_t count, uint64_t const* __restrict__ head, F&& fn)
+{
+  unsigned const lane = threadIdx.x & 31u;
+  uint32_t const W    = gridDim.x * (blockDim.x >> 5);
+  uint32_t const gw   = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  for (uint32_t base = 0; base < count; base += 32) {
+    uint32_t const i = base + lane;
+    uint32_t       v = 0;
+    uint64_t       b = 0, e = 0;
+    if (i < count) {
+      v = __ldcg(list + i);
+      b = head[v];
+      e = head[v + 1];
+    }
+    uint32_t const k = count - base < 32 ? count - base : 32;
+    for (uint32_t j = 0; j < k; ++j) {
+      uint32_t const vj = __shfl_sync(0xFFFFFFFFu, v, j);
+      uint64_t const bj = __shfl_sync(0xFFFFFFFFu, b, j), ej = __shfl_sync(0xFFFFFFFFu, e, j);
+      if (HEAVY_ONLY && ej - bj <= HEAVY_ROW) continue;
+      uint64_t const ns = (ej - bj + HEAVY_SLICE - 1) / HEAVY_SLICE;
+      uint32_t const r  = (base + j) % W;
+      for (uint64_t sl = (gw + W - r) % W; sl < ns; sl += W) {
+        uint64_t const sb = bj + sl * HEAVY_SLICE;
+        fn(base + j, vj, sb, sb + HEAVY_SLICE < ej ? sb + HEAVY_SLICE : ej);
+      }
+    }
+  }
+}
+
 // Block-aggregated append: pushes collected in shared memory during a tile (or sweep step)
 // are reserved in the global queue with ONE atomic per block and copied out
 // coalesced (a per-warp atomic on one counter serialises in L2 when a level
@@ -181,6 +236,8 @@ enum ctr_slot : int
   CTR_AUX,      // phase-specific
   CTR_ERR,      // error word (bounds checks, caps)
   CTR_COUNT = 16, // slots 5.. are phase-specific (8: expansion tile count)
+  CTR_RES_HEAVY  = 5, // residual: heavy rows listed by k_res_hook
+  CTR_TRIM_HEAVY = 6, // trim push levels (host-driven): heavy out-rows at 6, in-rows at 7; live counts: 9
   CTR_PV_TICKET = 15 // trim_1_first: blocks finished (the last one reduces the pivot)
 };
 
@@ -218,8 +275,12 @@ struct workspace
   uint32_t* seed_q      = nullptr; // 4: the pivot as a one-vertex frontier
   uint64_t* seed_prefix = nullptr; // 4
   void*     gbar        = nullptr; // 4 KiB: grid barrier of the persistent FW-BW at 0, worklist counters at 1024 (zeroed at creation)
-  void*     aw          = nullptr; // n + 64 u64: worklist of the asynchronous search tail (zeroed at creation, zero outside a phase)
+  void*     aw          = nullptr; // aw_entries u64: worklist of the asynchronous search tail (zeroed at creation, zero outside a phase)
+  size_t    aw_entries  = 0;       // n + 66 vertex items + m / HEAVY_SLICE + 32 row-slice items
   void*     rstate      = nullptr; // 4 KiB device control blocks (FW-BW at 0, trim at 512, search stamps at 2048)
+  uint32_t* heavy       = nullptr; // 4 heavy lists of heavy_cap entries (persistent FW-BW: trim seed, two trim push levels, cut bottom-up rows)
+  uint64_t  heavy_cap   = 0;
+  uint32_t* cutmap      = nullptr; // bitmap: vertices on a cut list (zero outside a search)
   // owned graph storage (host inputs, or a CSC built on device)
   uint64_t* g_fh = nullptr;
   uint32_t* g_fc = nullptr;

@@ -251,8 +251,13 @@ k_mlp_adam(float* __restrict__ params, float const* __restrict__ grad, float* __
   }
 }
 
-// Learned pivot: every per-block candidate of k_trim_first is scored; the
-// best (largest logit, then smallest id) goes to *best as an ordered key.
+// Learned pivot: every per-block candidate of k_trim_first is scored.  The
+// model acts as a filter on the plain rule: among the candidates it accepts
+// (logit >= 0: "in the largest SCC") the largest in * out wins, so the plain
+// pivot stays whenever the model accepts it; when it accepts none, the
+// largest logit wins.  Ties: smallest id.  Key for atomicMax: bit 63 =
+// accepted, bits 62..32 = the product's float bits (accepted) or the
+// logit's order key >> 1 (not accepted), low word = ~id.
 __global__ void __launch_bounds__(MLP_WARPS * 32)
 k_pivot_score(uint32_t nb, uint64_t const* __restrict__ cand_prod, uint32_t const* __restrict__ cand_id, uint32_t n, uint64_t const* __restrict__ fh, uint32_t const* __restrict__ fc,
               uint64_t const* __restrict__ bh, uint32_t const* __restrict__ bc, float const* __restrict__ params, unsigned long long* best)
@@ -266,7 +271,9 @@ k_pivot_score(uint32_t nb, uint64_t const* __restrict__ cand_prod, uint32_t cons
     mlp_features(v, fh, fc, bh, bc, f);
     float      h1, h2;
     float const z = mlp_forward(s, f, h1, h2);
-    if ((threadIdx.x & 31u) == 0) atomicMax(best, (static_cast<unsigned long long>(ordered(z)) << 32) | (0xFFFFFFFFu - v));
+    bool const               ok = z >= 0.f;
+    unsigned long long const hi = ok ? (0x80000000ull | __float_as_uint(static_cast<float>(cand_prod[i]))) : static_cast<unsigned long long>(ordered(z) >> 1);
+    if ((threadIdx.x & 31u) == 0) atomicMax(best, (hi << 32) | (0xFFFFFFFFu - v));
   }
 }
 

@@ -99,6 +99,11 @@ struct reach_state
   unsigned long long pushed_td;    // vertices they queued (offsets read once more)
   uint32_t           mats;         // frontiers built from `fresh`
   unsigned long long t_ns[3];      // %globaltimer: launch start, FW-BW end, trim end
+  uint32_t           cut_n[2];     // bottom-up rows cut short (FW, BW search; host-driven levels use [0])
+  uint32_t           fixups;       // fix-up steps run (both searches)
+  uint32_t           hseed_n;      // trim tail: listed vertices with a heavy row
+  uint32_t           hq_n[6];      // trim tail: heavy out-/in-rows listed per push level (pairs rotating like lq)
+  uint32_t           heavy_err;    // a heavy or cut list would have overflowed
 };
 
 // phase stamps live after the state: uint32 phase[128], uint64 ns[128]
@@ -175,6 +180,7 @@ template<bool BW>
 __device__ __forceinline__ unsigned
 advance_body(reach_state* st)
 {
+  st->cut_n[0]                  = 0; // (host-driven levels: the level's cut rows were walked)
   unsigned long long const mf   = __ldcg(&st->m_f);
   unsigned long long const mu   = __ldcg(&st->m_u);
   uint32_t const           mode = __ldcg(&st->mode);
@@ -242,12 +248,27 @@ struct bu_warp_smem
   uint32_t found[32];     // found bits per word of the chunk
 };
 
+// Rows cut short in bottom-up sweeps: a row the warp has walked HEAVY_ROW
+// entries of without a hit is left open (the vertex stays a candidate) and
+// its vertex listed once (map) for a fix-up step that walks the listed
+// rows in slices over the whole grid.  No bu_cut (nullptr): rows are
+// walked to the end.
+struct bu_cut
+{
+  uint32_t* map;  // bitmap of listed vertices
+  uint32_t* list; // listed vertices
+  uint32_t* n;    // list length
+  uint32_t  cap;  // list capacity (never reached: a listed row has HEAVY_ROW+ entries)
+  uint32_t* err;  // set if it were
+};
+
 // Row walks of up to BU_ILP candidates per lane (v[k], live[k]): all
 // neighbour loads of a step, then all probes of `mark`; rows still open
-// after BU_STEPS neighbours are finished by the whole warp with early exit.
-// found[k]: a neighbour of v[k] is in mark.  All lanes call it.
+// after BU_STEPS neighbours are finished by the whole warp with early exit
+// (or cut, see bu_cut).  found[k]: a neighbour of v[k] is in mark.  All
+// lanes call it.
 __device__ __forceinline__ void
-bu_rows(uint32_t const (&v)[BU_ILP], bool (&live)[BU_ILP], bool (&found)[BU_ILP], uint64_t const* __restrict__ head, uint32_t const* __restrict__ adj, uint32_t const* mark, uint64_t& nedge)
+bu_rows(uint32_t const (&v)[BU_ILP], bool (&live)[BU_ILP], bool (&found)[BU_ILP], uint64_t const* __restrict__ head, uint32_t const* __restrict__ adj, uint32_t const* mark, uint64_t& nedge, bu_cut const* cut)
 {
   unsigned const lane = threadIdx.x & 31u;
   uint64_t       b[BU_ILP], e[BU_ILP];
@@ -290,9 +311,10 @@ bu_rows(uint32_t const (&v)[BU_ILP], bool (&live)[BU_ILP], bool (&found)[BU_ILP]
       unsigned const l = __ffs(todo) - 1;
       todo &= todo - 1;
       uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b[k], l), e0 = __shfl_sync(0xFFFFFFFFu, e[k], l);
+      uint64_t const e1 = cut && e0 - b0 > HEAVY_ROW ? b0 + HEAVY_ROW : e0;
       bool           hit = false;
-      for (uint64_t x = b0; x < e0; x += 32) {
-        bool const     in = x + lane < e0;
+      for (uint64_t x = b0; x < e1; x += 32) {
+        bool const     in = x + lane < e1;
         uint32_t const y  = in ? adj[x + lane] : 0u;
         bool const     h  = in && ((__ldcg(mark + (y >> 5)) >> (y & 31)) & 1u);
         nedge += in;
@@ -301,7 +323,14 @@ bu_rows(uint32_t const (&v)[BU_ILP], bool (&live)[BU_ILP], bool (&found)[BU_ILP]
           break;
         }
       }
-      if (lane == l) found[k] = hit;
+      if (lane == l) {
+        found[k] = hit;
+        if (!hit && e1 < e0 && bit_claim(cut->map, v[k])) {
+          uint32_t const i = atomicAdd(cut->n, 1u);
+          if (i < cut->cap) cut->list[i] = v[k];
+          else atomicExch(cut->err, 1u);
+        }
+      }
     }
   }
 }
@@ -328,7 +357,8 @@ bu_sweep_warp(uint32_t first,
               bu_warp_smem& sm,
               uint32_t& nfound,
               uint64_t& nedge,
-              uint64_t& ncand)
+              uint64_t& ncand,
+              bu_cut const* cut)
 {
   unsigned const lane   = threadIdx.x & 31u;
   uint32_t const words  = (n + 31) / 32;
@@ -363,7 +393,7 @@ bu_sweep_warp(uint32_t first,
         live[k]          = i < total;
         v[k]             = live[k] ? c * 1024 + sm.cand[i] : 0u;
       }
-      bu_rows(v, live, found, head, adj, mark, nedge);
+      bu_rows(v, live, found, head, adj, mark, nedge, cut);
 #pragma unroll
       for (int k = 0; k < BU_ILP; ++k)
         if (found[k]) atomicOr(&sm.found[(v[k] >> 5) - c * 32], 1u << (v[k] & 31));
@@ -427,14 +457,18 @@ k_bottom_up(uint32_t n,
             uint32_t* __restrict__ fresh,
             fio f,
             gate g,
-            reach_state* st)
+            reach_state* st,
+            bu_cut cut)
 {
   if (g.closed()) return;
   __shared__ bu_warp_smem sm[BU_WARPS];
+  __shared__ bu_cut       s_cut;
+  if (threadIdx.x == 0) s_cut = cut;
+  __syncthreads();
   uint32_t                nfound = 0;
   uint64_t                nedge = 0, ncand = 0;
   unsigned const          wid = threadIdx.x >> 5;
-  bu_sweep_warp(blockIdx.x * BU_WARPS + wid, gridDim.x * BU_WARPS, n, head, adj, avail, mark, fresh, sm[wid], nfound, nedge, ncand);
+  bu_sweep_warp(blockIdx.x * BU_WARPS + wid, gridDim.x * BU_WARPS, n, head, adj, avail, mark, fresh, sm[wid], nfound, nedge, ncand, cut.map ? &s_cut : nullptr);
 #pragma unroll
   for (int s = 16; s; s >>= 1) {
     nedge += __shfl_down_sync(0xFFFFFFFFu, nedge, s);
@@ -444,6 +478,48 @@ k_bottom_up(uint32_t n,
     if (nedge) atomicAdd(&st->edges_bu, static_cast<unsigned long long>(nedge));
     if (nfound) atomicAdd(f.out_n(), nfound);
     if (ncand) atomicAdd(&st->cands_bu, static_cast<unsigned long long>(ncand));
+  }
+}
+
+// The rows k_bottom_up cut short, walked to the end in slices over the
+// grid: a listed candidate with a neighbour in mark joins (avail, mark and
+// fresh updated, counted into the level's output count).
+__global__ void __launch_bounds__(R_THREADS)
+k_bu_cut_rows(uint64_t const* __restrict__ head, uint32_t const* __restrict__ adj, uint32_t* avail, uint32_t* mark, uint32_t* fresh, fio f, gate g, bu_cut cut)
+{
+  if (g.closed()) return;
+  unsigned const lane   = threadIdx.x & 31u;
+  uint32_t const nc     = *cut.n < cut.cap ? *cut.n : cut.cap;
+  uint32_t       nfound = 0;
+  heavy_slices(cut.list, nc, head, [&](uint32_t, uint32_t v, uint64_t b, uint64_t e) {
+    if (!((__shfl_sync(0xFFFFFFFFu, __ldcg(avail + (v >> 5)), 0) >> (v & 31)) & 1u)) return;
+    bool hit = false;
+    for (uint64_t x = b; x < e; x += 32) {
+      bool const     in = x + lane < e;
+      uint32_t const y  = in ? adj[x + lane] : 0u;
+      if (__any_sync(0xFFFFFFFFu, in && ((__ldcg(mark + (y >> 5)) >> (y & 31)) & 1u))) {
+        hit = true;
+        break;
+      }
+    }
+    if (hit && lane == 0 && bit_take(avail, v)) {
+      atomicOr(mark + (v >> 5), 1u << (v & 31));
+      atomicOr(fresh + (v >> 5), 1u << (v & 31));
+      ++nfound;
+    }
+  });
+  if (nfound) atomicAdd(f.out_n(), nfound);
+}
+
+// Clears the listed rows' cutmap bits (the count is reset by k_r_advance).
+__global__ void __launch_bounds__(R_THREADS)
+k_bu_cut_clear(gate g, bu_cut cut)
+{
+  if (g.closed()) return;
+  uint32_t const nc = *cut.n < cut.cap ? *cut.n : cut.cap;
+  for (uint32_t i = blockIdx.x * R_THREADS + threadIdx.x; i < nc; i += gridDim.x * R_THREADS) {
+    uint32_t const v = cut.list[i];
+    atomicAnd(cut.map + (v >> 5), ~(1u << (v & 31)));
   }
 }
 
@@ -563,10 +639,17 @@ struct fwbw_args
   uint32_t const*    pv_id;
   uint32_t           trim;
   uint32_t           ids_at_end; // resident launch: write every vertex's id at the end
-  unsigned long long* aw;        // asynchronous tail: worklist (n + 64 tagged entries, 0 when unused)
+  unsigned long long* aw;        // asynchronous tail: worklist (aw_cap tagged entries, 0 when unused)
+  uint64_t           aw_cap;
   unsigned long long* aq;        // its counters: head at [0], tail at [16], done at [32] (own lines)
   uint32_t*          indeg;
   uint32_t*          outdeg;
+  // heavy rows: four lists of heavy_cap entries -- [0] trim seed (and the
+  // BW search's cut rows), [1] [2] trim push levels by parity, [3] the FW
+  // search's cut rows -- and the bitmap of cut rows (zero between searches)
+  uint32_t*          heavy;
+  uint32_t           heavy_cap;
+  uint32_t*          cutmap;
   grid_barrier*      bar;
   reach_state*       st;
   uint32_t*          stamp_phase;
@@ -584,6 +667,7 @@ struct fwbw_smem
   uint32_t              cnt;
   unsigned long long    old;
   unsigned long long    edges_bu, cands_bu; // bottom-up statistics of the launch
+  bu_cut                cut;                // the running search's cut rows
   __device__ __forceinline__ uint32_t* tile_rows() { return reinterpret_cast<uint32_t*>(warp); }
   __device__ __forceinline__ uint32_t* buf() { return reinterpret_cast<uint32_t*>(warp) + EX_TILE; }
 };
@@ -782,7 +866,10 @@ aw_push(uint32_t v, unsigned long long* aw, unsigned long long* tail, uint64_t c
 }
 
 // Runs the rest of the search from frontier fin.q[0, qn).  All threads of
-// every block call it.
+// every block call it.  An item is AW_TAG | slice << 33 | v: slice 0 of a
+// row longer than HEAVY_ROW appends the row's other HEAVY_SLICE-entry
+// slices as items of their own (so idle warps share the row) and walks the
+// first; a vertex whose row is shorter is one item.
 __device__ __forceinline__ int
 run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, uint64_t const* __restrict__ td_head, uint32_t const* __restrict__ td_adj, uint32_t* avail, uint32_t* mark, unsigned long long& epoch,
           uint64_t& edges)
@@ -791,7 +878,7 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, uint64_t const* _
   unsigned long long* const head = a.aq;
   unsigned long long* const tail = a.aq + 16;
   unsigned long long* const done = a.aq + 32;
-  uint64_t const            cap  = static_cast<uint64_t>(a.n) + 64;
+  uint64_t const            cap  = a.aw_cap;
   unsigned const            lane = threadIdx.x & 31u;
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; i < qn; i += static_cast<uint64_t>(gridDim.x) * R_THREADS) __stcg(aw + i, AW_TAG | __ldcg(fq + i));
   if (blockIdx.x == 0 && threadIdx.x == 0) *head = 0, *tail = qn, *done = 0;
@@ -809,15 +896,26 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, uint64_t const* _
     unsigned       spins   = 0;
     while (__any_sync(0xFFFFFFFFu, pending)) {
       bool     got = false;
-      uint32_t v   = 0;
+      uint32_t v = 0, sl = 0;
       if (pending && slot < cap) {
         unsigned long long const e = ld_acquire64(aw + slot);
-        if (e & AW_TAG) v = static_cast<uint32_t>(e), got = true, pending = false;
+        if (e & AW_TAG) v = static_cast<uint32_t>(e), sl = static_cast<uint32_t>(e >> 33), got = true, pending = false;
       }
       unsigned const gmask = __ballot_sync(0xFFFFFFFFu, got);
       if (gmask) {
         uint64_t b = 0, e = 0;
         if (got) b = td_head[v], e = td_head[v + 1];
+        if (got && e - b > HEAVY_ROW) {
+          if (sl == 0) {
+            // the row's other slices become items
+            uint64_t const           ns = (e - b + HEAVY_SLICE - 1) / HEAVY_SLICE;
+            unsigned long long const at = atomicAdd(tail, static_cast<unsigned long long>(ns - 1));
+            for (uint64_t j = 1; j < ns; ++j)
+              if (at + j - 1 < cap) __stcg(aw + at + j - 1, AW_TAG | (static_cast<unsigned long long>(j) << 33) | v);
+          }
+          b += static_cast<uint64_t>(sl) * HEAVY_SLICE;
+          e = b + HEAVY_SLICE < e ? b + HEAVY_SLICE : e;
+        }
         bool const big = got && e - b > 32;
         if (got) edges += e - b;
         // small rows, AW_BATCH neighbours per pass: all ids, then all probes,
@@ -922,6 +1020,12 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
   uint32_t                 bu = 0, capped = 0, lvl = 0;
   uint64_t                 edges_td = 0;
   bool const               tally = blockIdx.x == 0 && threadIdx.x == 0; // keeps the byte-model counts in st
+  bool                     fixed = false; // the last level was a fix-up step
+  // rows the sweeps cut short (bu_cut, read from shared memory where the
+  // sweep needs it; every level ends in a grid barrier, so the block's
+  // sweeps see it): the FW search lists them in heavy list 3, the BW
+  // search in list 0
+  if (threadIdx.x == 0) sm.cut = bu_cut{ a.cutmap, a.heavy + (BW ? 0u : 3u) * a.heavy_cap, &st->cut_n[BW ? 1 : 0], a.heavy_cap, &st->heavy_err };
   // the first frontier: the pivot alone
   unsigned long long c = (static_cast<unsigned long long>(td_head[pivot + 1] - td_head[pivot]) << a.qbits) | 1u;
   for (;; ++lvl, ++glvl) {
@@ -942,7 +1046,46 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
     }
     uint64_t const qn64 = c & qmask;
     uint64_t const mf   = c >> a.qbits; // the frontier's edges (0 after a sweep)
-    if (qn64 == 0) break;
+    if (qn64 == 0) {
+      // the search ran dry: rows cut short by the sweeps are walked to the
+      // end in slices over the grid; a listed candidate with a neighbour in
+      // mark joins, and the joined ones are the next (top-down) frontier.
+      // Ends when a fix-up step finds nothing.
+      uint32_t* const cut_list = a.heavy + (BW ? 0u : 3u) * a.heavy_cap;
+      uint32_t const  nc       = __ldcg(&st->cut_n[BW ? 1 : 0]);
+      if (nc == 0 || fixed) break;
+      fixed = true;
+      if (tally) st->fixups += 1;
+      unsigned const lane = threadIdx.x & 31u;
+      block_queue    bq{ sm.buf(), &sm.buf_n };
+      uint32_t const lim = nc < a.heavy_cap ? nc : a.heavy_cap;
+      for (uint32_t off = 0; off < lim; off += BU_BUF / 2) {
+        uint32_t const k = lim - off < BU_BUF / 2 ? lim - off : BU_BUF / 2; // at most k joins: the block queue holds them
+        heavy_slices(cut_list + off, k, bu_head, [&](uint32_t, uint32_t v, uint64_t b, uint64_t e) {
+          if (!((__shfl_sync(0xFFFFFFFFu, __ldcg(avail + (v >> 5)), 0) >> (v & 31)) & 1u)) return; // joined meanwhile
+          bool hit = false;
+          for (uint64_t x = b; x < e; x += 32) {
+            bool const     in = x + lane < e;
+            uint32_t const y  = in ? bu_adj[x + lane] : 0u;
+            bool const     h  = in && ((__ldcg(mark + (y >> 5)) >> (y & 31)) & 1u);
+            if (__any_sync(0xFFFFFFFFu, h)) {
+              hit = true;
+              break;
+            }
+          }
+          bool const took = hit && lane == 0 && bit_take(avail, v);
+          if (took) bit_claim(mark, v);
+          bq.push(took, v);
+        });
+        flush_scanned(sm, fout, &st->lq[s_out], a.qbits, td_head, a.n, a.m);
+      }
+      if (!grid_sync(a.bar, epoch)) return SEARCH_FAILED;
+      stamp(a, 14);
+      mode = 0;
+      mat  = false;
+      continue;
+    }
+    fixed = false;
     if (lvl >= a.cap || qn64 > a.n || mf > a.m) {
       // level cap; or counters beyond the graph, which a correct search
       // never produces (then nothing more is read or written)
@@ -960,8 +1103,9 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
       stamp(a, 13);
       edges_td += ea;
       if (tally) st->async_phases += 1;
-      ++lvl;
-      break;
+      // nothing is queued for the next level: it runs dry (or fixes up
+      // rows an earlier sweep cut short)
+      continue;
     }
     unsigned long long* const octr = &st->lq[s_out];
     if (mode == 0) {
@@ -988,7 +1132,7 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
       uint32_t       nfound = 0;
       uint64_t       ne = 0, nc = 0;
       if (tally) st->bu_bitmap += 1;
-      bu_sweep_warp(blockIdx.x * BU_WARPS + wid, gridDim.x * BU_WARPS, a.n, bu_head, bu_adj, avail, mark, a.fresh, sm.warp[wid], nfound, ne, nc);
+      bu_sweep_warp(blockIdx.x * BU_WARPS + wid, gridDim.x * BU_WARPS, a.n, bu_head, bu_adj, avail, mark, a.fresh, sm.warp[wid], nfound, ne, nc, &sm.cut);
 #pragma unroll
       for (int sh = 16; sh; sh >>= 1) {
         nfound += __shfl_down_sync(0xFFFFFFFFu, nfound, sh);
@@ -1017,6 +1161,17 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
     if (BW) st->levels_bw = lvl, st->bu_bw = bu;
     else st->levels_fw = lvl, st->bu_fw = bu;
     st->edges_td += edges_td;
+  }
+  {
+    // the cut rows' bits leave cutmap before the next search can cut (its
+    // first bottom-up sweep comes after at least one more barrier); the
+    // count itself stays (the other search lists into its own slot)
+    uint32_t const* const cut_list = a.heavy + (BW ? 0u : 3u) * a.heavy_cap;
+    uint32_t const        nc       = __ldcg(&st->cut_n[BW ? 1 : 0]);
+    for (uint32_t i = blockIdx.x * R_THREADS + threadIdx.x; i < nc && i < a.heavy_cap; i += gridDim.x * R_THREADS) {
+      uint32_t const v = __ldcg(cut_list + i);
+      atomicAnd(a.cutmap + (v >> 5), ~(1u << (v & 31)));
+    }
   }
   return capped ? SEARCH_CAPPED : SEARCH_DONE;
 }
@@ -1055,7 +1210,8 @@ count_live(uint32_t const* snap, uint32_t const* __restrict__ adj, uint64_t b, u
 // First trim pass: live degrees of every listed undecided vertex; the dead
 // ones (no live in- or out-neighbour) are decided and queued.  A lane
 // counts one vertex; rows longer than TRIM_SMALL are counted by the whole
-// warp.
+// warp; a vertex with a row longer than HEAVY_ROW is listed (heavy list 0,
+// st->hseed_n) with both counts zeroed, for run_trim's slice pass.
 __device__ __forceinline__ void
 trim_seed(fwbw_args const& a, uint32_t const* list, uint64_t list_n, uint32_t* qout, unsigned long long* octr, uint32_t& dec, uint64_t& edges)
 {
@@ -1067,13 +1223,16 @@ trim_seed(fwbw_args const& a, uint32_t const* list, uint64_t list_n, uint32_t* q
     uint32_t const x    = have ? __ldcg(list + t) : 0u;
     uint64_t       ob = 0, oe = 0, ib = 0, ie = 0;
     if (have) ob = a.fh[x], oe = a.fh[x + 1], ib = a.bh[x], ie = a.bh[x + 1];
+    bool const hv    = have && (oe - ob > HEAVY_ROW || ie - ib > HEAVY_ROW);
     bool const small = have && (oe - ob) + (ie - ib) <= TRIM_SMALL;
     uint32_t   co = 0, ci = 0;
     if (small) {
       co = count_live(snap, a.fc, ob, oe);
       ci = count_live(snap, a.bc, ib, ie);
     }
-    for (unsigned todo = __ballot_sync(0xFFFFFFFFu, have && !small); todo; todo &= todo - 1) {
+    if (hv) a.outdeg[x] = a.indeg[x] = 0; // counted in slices
+    warp_push(hv, x, a.heavy, &a.st->hseed_n);
+    for (unsigned todo = __ballot_sync(0xFFFFFFFFu, have && !small && !hv); todo; todo &= todo - 1) {
       unsigned const l  = __ffs(todo) - 1;
       uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, ob, l), e0 = __shfl_sync(0xFFFFFFFFu, oe, l);
       uint64_t const b1 = __shfl_sync(0xFFFFFFFFu, ib, l), e1 = __shfl_sync(0xFFFFFFFFu, ie, l);
@@ -1084,12 +1243,12 @@ trim_seed(fwbw_args const& a, uint32_t const* list, uint64_t list_n, uint32_t* q
       for (int sh = 16; sh; sh >>= 1) xo += __shfl_xor_sync(0xFFFFFFFFu, xo, sh), xi += __shfl_xor_sync(0xFFFFFFFFu, xi, sh);
       if (lane == l) co = xo, ci = xi;
     }
-    bool const dead = have && (co == 0 || ci == 0);
+    bool const dead = have && !hv && (co == 0 || ci == 0);
     if (dead) {
       atomicAnd(a.und + (x >> 5), ~(1u << (x & 31)));
       if (!a.ids_at_end) a.scc_id[x] = x;
       ++dec;
-    } else if (have) {
+    } else if (have && !hv) {
       a.outdeg[x] = co;
       a.indeg[x]  = ci;
     }
@@ -1101,10 +1260,29 @@ trim_seed(fwbw_args const& a, uint32_t const* list, uint64_t list_n, uint32_t* q
 // One trim push level: every queued vertex decrements its undecided
 // neighbours' live counts (out-neighbours' in-degree, in-neighbours'
 // out-degree); a neighbour whose count reaches 0 is decided and queued.
+// Heavy rows of the push levels: a queued vertex's row longer than
+// HEAVY_ROW is skipped by its lane and listed instead, in heavy list
+// 1 + ((glvl + 1) & 1) -- out-rows from the front, in-rows from the back,
+// counted in hq_n[2 * ((glvl + 1) % 3)] and the entry after it -- and the
+// next level walks the listed rows in slices over the whole grid (a push
+// one level late: the fixpoint does not depend on the order).
+struct trim_hq
+{
+  uint32_t* list; // heavy list of this parity
+  uint32_t* n;    // [0] out-rows (front), [1] in-rows (back)
+};
+
+__device__ __forceinline__ trim_hq
+trim_heavy_at(fwbw_args const& a, uint32_t glvl)
+{
+  return { a.heavy + (1 + (glvl & 1)) * a.heavy_cap, &a.st->hq_n[2 * (glvl % 3)] };
+}
+
 __device__ __forceinline__ void
-trim_push(fwbw_args const& a, uint32_t const* qin, uint32_t qn, uint32_t* qout, unsigned long long* octr, uint32_t& dec, uint64_t& edges)
+trim_push(fwbw_args const& a, uint32_t const* qin, uint32_t qn, uint32_t* qout, unsigned long long* octr, uint32_t& dec, uint64_t& edges, uint32_t glvl)
 {
   unsigned const lane = threadIdx.x & 31u;
+  trim_hq const  hin = trim_heavy_at(a, glvl), hout = trim_heavy_at(a, glvl + 1);
   uint64_t const span = (static_cast<uint64_t>(qn) + 31) & ~31ull;
   // w's und word already probed: decrement, decide and queue at 0
   auto const hit = [&](uint32_t w, uint32_t word, uint32_t* deg) {
@@ -1141,9 +1319,24 @@ trim_push(fwbw_args const& a, uint32_t const* qin, uint32_t qn, uint32_t* qout, 
       uint32_t const u    = have ? __ldcg(qin + t) : 0u;
       uint64_t       b = 0, e = 0;
       if (have) b = head[u], e = head[u + 1];
-      bool const big = have && e - b >= TRIM_SMALL;
+      bool const big = have && e - b >= TRIM_SMALL && e - b <= HEAVY_ROW;
+      bool const hv  = have && e - b > HEAVY_ROW;
       edges += e - b;
-      if (have && !big) row(adj, b, e, deg);
+      if (have && e - b < TRIM_SMALL) row(adj, b, e, deg);
+      {
+        // heavy rows: listed for the next level (one atomic per warp)
+        unsigned const bal = __ballot_sync(0xFFFFFFFFu, hv);
+        if (bal) {
+          uint32_t base = 0;
+          if (lane == 0) base = atomicAdd(hout.n + dir, static_cast<uint32_t>(__popc(bal)));
+          base = __shfl_sync(0xFFFFFFFFu, base, 0) + __popc(bal & ((1u << lane) - 1u));
+          // front and back never meet: heavy_capacity covers both directions
+          if (hv) {
+            if (base < a.heavy_cap / 2) hout.list[dir ? a.heavy_cap - 1 - base : base] = u;
+            else atomicExch(&a.st->heavy_err, 1u);
+          }
+        }
+      }
       for (unsigned todo = __ballot_sync(0xFFFFFFFFu, big); todo; todo &= todo - 1) {
         unsigned const l  = __ffs(todo) - 1;
         uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b, l), e0 = __shfl_sync(0xFFFFFFFFu, e, l);
@@ -1153,7 +1346,52 @@ trim_push(fwbw_args const& a, uint32_t const* qin, uint32_t qn, uint32_t* qout, 
         }
       }
     }
+    uint32_t const hn = __ldcg(hin.n + dir);
+    heavy_slices(dir ? hin.list + a.heavy_cap - hn : hin.list, hn, head, [&](uint32_t, uint32_t, uint64_t b0, uint64_t e0) {
+      for (uint64_t x = b0 + lane; x < e0; x += 32) {
+        uint32_t const w = adj[x];
+        hit(w, __ldcg(a.und + (w >> 5)), deg);
+      }
+    });
   }
+}
+
+// Live degrees of the hs listed heavy vertices (heavy list 0), counted in
+// slices against snap.
+__device__ __forceinline__ void
+trim_count_heavy(fwbw_args const& a, uint32_t hs)
+{
+  unsigned const lane = threadIdx.x & 31u;
+#pragma unroll 1
+  for (int dir = 0; dir < 2; ++dir) {
+    uint32_t const* adj = dir ? a.bc : a.fc;
+    uint32_t* const deg = dir ? a.indeg : a.outdeg;
+    heavy_slices(a.heavy, hs, dir ? a.bh : a.fh, [&](uint32_t, uint32_t x, uint64_t b, uint64_t e) {
+      uint32_t c = 0;
+      for (uint64_t y = b + lane; y < e; y += 32) c += snap_bit(a.cand, adj[y]);
+#pragma unroll
+      for (int sh = 16; sh; sh >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, sh);
+      if (lane == 0 && c) atomicAdd(deg + x, c);
+    });
+  }
+}
+
+// First push level: the listed heavy vertices with a live degree of 0 are
+// decided and queued (their rows are listed by the next level's walk);
+// returns how many this thread decided.
+__device__ __forceinline__ uint32_t
+trim_dead_heavy(fwbw_args const& a, uint32_t hs, uint32_t glvl)
+{
+  uint32_t dec = 0;
+  for (uint32_t i = blockIdx.x * R_THREADS + threadIdx.x; i < hs; i += gridDim.x * R_THREADS) {
+    uint32_t const x = __ldcg(a.heavy + i);
+    if ((__ldcg(a.outdeg + x) == 0 || __ldcg(a.indeg + x) == 0) && bit_take(a.und, x)) {
+      if (!a.ids_at_end) a.scc_id[x] = x;
+      ++dec;
+      warp_push_active64(x, a.fb[(glvl + 1) & 1].q, &a.st->lq[(glvl + 1) % 3], a.n);
+    }
+  }
+  return dec;
 }
 
 // The trim fixpoint; levels continue the launch's numbering (glvl).
@@ -1172,15 +1410,24 @@ run_trim(fwbw_args const& a, uint32_t& glvl, unsigned long long& epoch)
   if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
   stamp(a, 11);
   ++glvl;
+  uint32_t const hs = rc == SEARCH_DONE ? __ldcg(&st->hseed_n) : 0u;
+  if (hs) {
+    // the listed heavy vertices' live degrees, counted in slices
+    trim_count_heavy(a, hs);
+    if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
+    stamp(a, 15);
+  }
   while (rc == SEARCH_DONE) {
-    uint64_t const qn = __ldcg(&st->lq[glvl % 3]) & qmask;
-    if (qn == 0) break;
+    uint64_t const qn    = __ldcg(&st->lq[glvl % 3]) & qmask;
+    bool const     first = lvl == 0 && hs; // also decides the dead heavy vertices
+    if (qn == 0 && !first && __ldcg(&st->hq_n[2 * (glvl % 3)]) == 0 && __ldcg(&st->hq_n[2 * (glvl % 3) + 1]) == 0) break;
     if (lvl >= a.cap || qn > a.n) {
       rc = SEARCH_CAPPED;
       break;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) st->lq[(glvl + 2) % 3] = 0;
-    trim_push(a, a.fb[glvl & 1].q, static_cast<uint32_t>(qn), a.fb[(glvl + 1) & 1].q, &st->lq[(glvl + 1) % 3], dec, edges);
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->lq[(glvl + 2) % 3] = 0, st->hq_n[2 * ((glvl + 2) % 3)] = st->hq_n[2 * ((glvl + 2) % 3) + 1] = 0;
+    if (first) dec += trim_dead_heavy(a, hs, glvl);
+    trim_push(a, a.fb[glvl & 1].q, static_cast<uint32_t>(qn), a.fb[(glvl + 1) & 1].q, &st->lq[(glvl + 1) % 3], dec, edges, glvl);
     if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
     stamp(a, 12);
     ++lvl;
@@ -1260,6 +1507,9 @@ k_fwbw(fwbw_args a)
     st->rows_td = st->pushed_td = 0;
     st->mats = st->bu_bitmap    = 0;
     st->async_phases            = 0;
+    st->cut_n[0] = st->cut_n[1] = st->fixups = 0;
+    st->hseed_n = st->heavy_err = 0;
+    for (int i = 0; i < 6; ++i) st->hq_n[i] = 0;
     if (search) a.seed.q[0] = p, a.seed.prefix[0] = 0;
   }
   int      rc   = SEARCH_DONE;
@@ -1501,11 +1751,14 @@ level_body(kspn_context* ctx, dgraph const& gr, search_io const& io, reach_state
   k_expand<take_op><<<EX_BLOCKS, EX_THREADS, 0, s>>>(io.td_head, io.td_adj, f, ws.prefix, ws.tile_start, &st->ntiles, gate{ &st->mode, 0 }, take_op{ io.avail, io.mark });
   prof_stop(ctx, 0);
   prof_start(ctx, 1);
-  k_bottom_up<<<bu_grid(gr.n), R_THREADS, 0, s>>>(gr.n, io.bu_head, io.bu_adj, io.avail, io.mark, io.fresh, f, gate{ &st->mode, 1 }, st);
+  bu_cut const cut{ ws.cutmap, ws.heavy + 3 * ws.heavy_cap, &st->cut_n[0], static_cast<uint32_t>(ws.heavy_cap), &st->heavy_err };
+  k_bottom_up<<<bu_grid(gr.n), R_THREADS, 0, s>>>(gr.n, io.bu_head, io.bu_adj, io.avail, io.mark, io.fresh, f, gate{ &st->mode, 1 }, st, cut);
+  k_bu_cut_rows<<<148 * 8, R_THREADS, 0, s>>>(io.bu_head, io.bu_adj, io.avail, io.mark, io.fresh, f, gate{ &st->mode, 1 }, cut);
+  k_bu_cut_clear<<<148, R_THREADS, 0, s>>>(gate{ &st->mode, 1 }, cut);
   prof_stop(ctx, 1);
   k_r_advance<BW><<<1, 1, 0, s>>>(st);
   KSPN_CHECK_LAUNCH();
-  ctx->launches += 8;
+  ctx->launches += 10;
 }
 
 search_io
@@ -1611,9 +1864,13 @@ launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* s
   a.trim        = trim ? 1u : 0u;
   a.ids_at_end  = trim ? 1u : 0u;
   a.aw          = static_cast<unsigned long long*>(ws.aw);
+  a.aw_cap      = ws.aw_entries;
   a.aq          = reinterpret_cast<unsigned long long*>(static_cast<char*>(ws.gbar) + 1024);
   a.indeg       = ws.indeg;
   a.outdeg      = ws.outdeg;
+  a.heavy       = ws.heavy;
+  a.heavy_cap   = static_cast<uint32_t>(ws.heavy_cap);
+  a.cutmap      = ws.cutmap;
   a.bar         = gbar;
   a.st          = rs;
   a.stamp_phase = reinterpret_cast<uint32_t*>(static_cast<char*>(ws.rstate) + 2048);
@@ -1639,10 +1896,12 @@ check_persistent(kspn_context* ctx)
     // counters of a launch that gave up are not epoch-aligned, and its
     // worklist may hold entries: start over
     KSPN_CUDA(cudaMemsetAsync(ctx->ws.gbar, 0, 4096, ctx->stream));
-    KSPN_CUDA(cudaMemsetAsync(ctx->ws.aw, 0, (static_cast<size_t>(ctx->ws.n_cap) + 64) * sizeof(unsigned long long), ctx->stream));
+    KSPN_CUDA(cudaMemsetAsync(ctx->ws.aw, 0, ctx->ws.aw_entries * sizeof(unsigned long long), ctx->stream));
+    KSPN_CUDA(cudaMemsetAsync(ctx->ws.cutmap, 0, ((static_cast<size_t>(ctx->ws.n_cap) + 63) / 64 * 2 + 2) * sizeof(uint32_t), ctx->stream));
     KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
     throw error{ KSPN_ERR_TIMEOUT, "reachability: grid barrier wait limit reached" };
   }
+  if (hs->heavy_err) throw error{ KSPN_ERR_INTERNAL, "reachability / trim: heavy-row list overflow" };
   if (hs->err) throw error{ KSPN_ERR_TIMEOUT, "reachability / trim: level cap exceeded" };
 }
 
@@ -1785,6 +2044,7 @@ fw_bw(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint3
       if (hs->err) break;
     }
     if (hs->err) throw error{ KSPN_ERR_TIMEOUT, "reachability: level cap exceeded" };
+    if (hs->heavy_err) throw error{ KSPN_ERR_INTERNAL, "reachability: cut-row list overflow" };
     k_r_setid<<<1, 1, 0, ctx->stream>>>(rs);
     k_bitmap_min<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(g.n, ws.vis_b, rs);
     k_fwbw_finalize<<<r_grid(words), R_THREADS, 0, ctx->stream>>>(g.n, ws.vis_b, und, scc_id, rs);

@@ -71,35 +71,66 @@ k_res_init(uint32_t n, uint32_t const* __restrict__ und, uint32_t* __restrict__ 
     if (und_has(und, static_cast<uint32_t>(v))) parent[v] = static_cast<uint32_t>(v);
 }
 
-// u ~ v for every edge between undecided vertices
-__global__ void __launch_bounds__(RS_THREADS)
-k_res_hook(uint32_t n, uint32_t const* __restrict__ und, uint64_t const* __restrict__ fh, uint32_t const* __restrict__ fc, uint32_t* parent, uint32_t* err)
+// u ~ v (both undecided); false when a loop bound was reached
+__device__ __forceinline__ bool
+rs_unite(uint32_t* parent, uint32_t u, uint32_t v)
 {
-  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * RS_THREADS + threadIdx.x; t < n; t += static_cast<uint64_t>(gridDim.x) * RS_THREADS) {
-    uint32_t const u = static_cast<uint32_t>(t);
-    if (!und_has(und, u)) continue;
-    for (uint64_t e = fh[u], end = fh[u + 1]; e < end; ++e) {
-      uint32_t const v = fc[e];
-      if (v == u || !und_has(und, v)) continue;
-      uint32_t a = u, b = v;
-      bool     ok = false;
-      for (uint32_t it = 0; it < RS_FIND && !ok; ++it) {
-        a = rs_find(parent, a);
-        b = rs_find(parent, b);
-        if (a == UNDECIDED || b == UNDECIDED) break;
-        if (a == b) ok = true;
-        else {
-          if (a < b) {
-            uint32_t const s = a;
-            a = b, b = s;
-          }
-          // hook the larger root under the smaller
-          ok = atomicCAS(parent + a, a, b) == a;
-        }
-      }
-      if (!ok) atomicExch(err, 1u);
+  uint32_t a = u, b = v;
+  for (uint32_t it = 0; it < RS_FIND; ++it) {
+    a = rs_find(parent, a);
+    b = rs_find(parent, b);
+    if (a == UNDECIDED || b == UNDECIDED) return false;
+    if (a == b) return true;
+    if (a < b) {
+      uint32_t const s = a;
+      a = b, b = s;
     }
+    // hook the larger root under the smaller
+    if (atomicCAS(parent + a, a, b) == a) return true;
   }
+  return false;
+}
+
+__device__ __forceinline__ void
+rs_edge(uint32_t const* und, uint32_t* parent, uint32_t* err, uint32_t u, uint32_t v)
+{
+  if (v != u && und_has(und, v) && !rs_unite(parent, u, v)) atomicExch(err, 1u);
+}
+
+// u ~ v for every edge between undecided vertices.  A lane walks a row of
+// up to 32 edges, the warp one of up to HEAVY_ROW; longer rows are listed
+// for k_res_hook_heavy.
+__global__ void __launch_bounds__(RS_THREADS)
+k_res_hook(uint32_t n, uint32_t const* __restrict__ und, uint64_t const* __restrict__ fh, uint32_t const* __restrict__ fc, uint32_t* parent, uint32_t* err, uint32_t* heavy, uint32_t* heavy_n)
+{
+  unsigned const lane = threadIdx.x & 31u;
+  uint64_t const span = (static_cast<uint64_t>(n) + 31) & ~31ull;
+  for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * RS_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * RS_THREADS) {
+    uint32_t const u    = static_cast<uint32_t>(t);
+    bool const     have = t < n && und_has(und, u);
+    uint64_t       b = 0, e = 0;
+    if (have) b = fh[u], e = fh[u + 1];
+    uint64_t const len = e - b;
+    if (have && len <= 32)
+      for (uint64_t x = b; x < e; ++x) rs_edge(und, parent, err, u, fc[x]);
+    for (unsigned todo = __ballot_sync(0xFFFFFFFFu, have && len > 32 && len <= HEAVY_ROW); todo; todo &= todo - 1) {
+      unsigned const l  = __ffs(todo) - 1;
+      uint32_t const ul = __shfl_sync(0xFFFFFFFFu, u, l);
+      uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b, l), e0 = __shfl_sync(0xFFFFFFFFu, e, l);
+      for (uint64_t x = b0 + lane; x < e0; x += 32) rs_edge(und, parent, err, ul, fc[x]);
+    }
+    warp_push(have && len > HEAVY_ROW, u, heavy, heavy_n);
+  }
+}
+
+// The listed rows, in slices over every warp of the grid.
+__global__ void __launch_bounds__(RS_THREADS)
+k_res_hook_heavy(uint32_t const* __restrict__ und, uint64_t const* __restrict__ fh, uint32_t const* __restrict__ fc, uint32_t* parent, uint32_t* err, uint32_t const* heavy, uint32_t const* heavy_n)
+{
+  unsigned const lane = threadIdx.x & 31u;
+  heavy_slices(heavy, *heavy_n, fh, [&](uint32_t, uint32_t u, uint64_t b, uint64_t e) {
+    for (uint64_t x = b + lane; x < e; x += 32) rs_edge(und, parent, err, u, fc[x]);
+  });
 }
 
 // Shortens the trees (path halving; another thread's halving store may
@@ -278,7 +309,18 @@ k_res_tarjan(uint32_t const* __restrict__ seg_count,
       if (lane == 0) atomicAdd(big, 1u);
       continue;
     }
-    for (uint32_t i = lane; i < k; i += 32) p.vid[i] = vals[b + i];
+    bool heavy_row = false;
+    for (uint32_t i = lane; i < k; i += 32) {
+      uint32_t const v = vals[b + i];
+      p.vid[i]         = v;
+      heavy_row |= fh[v + 1] - fh[v] > HEAVY_ROW;
+    }
+    if (__any_sync(0xFFFFFFFFu, heavy_row)) {
+      // a member's row is too long for one lane: left to the later rounds
+      if (lane == 0) atomicAdd(big, 1u);
+      __syncwarp();
+      continue;
+    }
     __syncwarp();
     // internal out-degrees; lane l owns local vertices [l*per, l*per + per)
     uint32_t const per = (k + 31) / 32;
@@ -351,7 +393,8 @@ residual(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, ui
   uint32_t const words  = (g.n + 31) / 32;
   size_t const   hist_n = radix_hist_entries(g.n);
   size_t const   part_n = scan_partial_entries((hist_n > g.n + 1 ? hist_n : g.n + 1) + words + 1);
-  size_t const   bytes  = (6 * (static_cast<size_t>(g.n) + 64) + words + 64 + hist_n + part_n) * sizeof(uint32_t) + 32 * 256;
+  size_t const   hcap   = heavy_capacity(g.n, g.m);
+  size_t const   bytes  = (6 * (static_cast<size_t>(g.n) + 64) + words + 64 + hist_n + part_n + hcap) * sizeof(uint32_t) + 32 * 256;
   char*          base   = static_cast<char*>(context_buffer(ctx, BUF_BUILD, bytes));
   size_t         off    = 0;
   auto           take   = [&](size_t count) {
@@ -369,12 +412,14 @@ residual(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, ui
   uint32_t* wpos = take(words + 1);
   uint32_t* hist = take(hist_n);
   uint32_t* part = take(part_n);
+  uint32_t* hlist = take(hcap);
   uint32_t* parent = ws.label;
 
   zero_counters(ctx);
   unsigned const grid = rs_grid(g.n);
   k_res_init<<<grid, RS_THREADS, 0, s>>>(g.n, und, parent);
-  k_res_hook<<<grid, RS_THREADS, 0, s>>>(g.n, und, g.fh, g.fc, parent, ws.ctr + CTR_ERR);
+  k_res_hook<<<grid, RS_THREADS, 0, s>>>(g.n, und, g.fh, g.fc, parent, ws.ctr + CTR_ERR, hlist, ws.ctr + CTR_RES_HEAVY);
+  k_res_hook_heavy<<<148 * 8, RS_THREADS, 0, s>>>(und, g.fh, g.fc, parent, ws.ctr + CTR_ERR, hlist, ws.ctr + CTR_RES_HEAVY);
   k_res_compress<<<grid, RS_THREADS, 0, s>>>(g.n, und, parent, ws.ctr + CTR_ERR);
   k_res_flatten<<<grid, RS_THREADS, 0, s>>>(g.n, und, parent, ws.ctr + CTR_ERR);
   KSPN_CHECK_LAUNCH();
@@ -385,7 +430,7 @@ residual(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, ui
   uint32_t k = 0;
   KSPN_CUDA(cudaMemcpyAsync(&k, wpos + words, sizeof(k), cudaMemcpyDeviceToHost, s));
   KSPN_CUDA(cudaStreamSynchronize(s));
-  ctx->launches += 5;
+  ctx->launches += 6;
   if (k == 0) return 0;
   radix_sort_pairs(ctx, keys, vals, kalt, valt, k, 0, bits_for(g.n), hist, part);
   exclusive_scan<uint32_t>(s, f_seg_head{ keys }, k, spos, part, &ctx->launches);

@@ -26,6 +26,96 @@ namespace {
 constexpr int      T_THREADS = 256;
 constexpr uint32_t NONE      = 0xFFFFFFFFu;
 constexpr int      WARP_BIG  = 32;
+constexpr unsigned HEAVY_GRID = 148 * 8; // blocks of the heavy-row kernels
+
+// Heavy rows in the trim kernels: a vertex with a row longer than HEAVY_ROW
+// is listed by the per-vertex kernel and its rows are walked in slices by
+// every warp of a follow-up kernel (k_live_heavy, k_push_heavy).
+__device__ __forceinline__ bool
+row_heavy(uint64_t b, uint64_t e)
+{
+  return e - b > HEAVY_ROW;
+}
+
+// Live (undecided) neighbours in the listed vertices' rows, added to
+// outdeg (out-rows) and indeg (in-rows); the listing kernel zeroed both.
+__global__ void __launch_bounds__(T_THREADS)
+k_live_heavy(uint64_t const* __restrict__ fh, uint32_t const* __restrict__ fc, uint64_t const* __restrict__ bh, uint32_t const* __restrict__ bc, uint32_t const* __restrict__ und, uint32_t const* list,
+             uint32_t const* list_n, uint32_t* indeg, uint32_t* outdeg)
+{
+  unsigned const lane = threadIdx.x & 31u;
+  uint32_t const cnt  = *list_n;
+#pragma unroll 1
+  for (int dir = 0; dir < 2; ++dir) {
+    uint32_t const* adj = dir ? bc : fc;
+    uint32_t*       deg = dir ? indeg : outdeg;
+    heavy_slices(list, cnt, dir ? bh : fh, [&](uint32_t, uint32_t v, uint64_t b, uint64_t e) {
+      uint32_t c = 0;
+      for (uint64_t x = b + lane; x < e; x += 32) c += bit_get(und, adj[x]);
+#pragma unroll
+      for (int sh = 16; sh; sh >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, sh);
+      if (lane == 0 && c) atomicAdd(deg + v, c);
+    });
+  }
+}
+
+// Push step of the listed heavy rows: out-rows of list_out lower their
+// neighbours' indeg, in-rows of list_in their outdeg; a neighbour reaching
+// 0 is decided and queued (qout).
+__device__ __forceinline__ void
+push_heavy(uint64_t const* __restrict__ fh,
+           uint32_t const* __restrict__ fc,
+           uint64_t const* __restrict__ bh,
+           uint32_t const* __restrict__ bc,
+           uint32_t* __restrict__ und,
+           uint32_t* __restrict__ scc_id,
+           uint32_t* __restrict__ indeg,
+           uint32_t* __restrict__ outdeg,
+           uint32_t const* list_out,
+           uint32_t const* list_in,
+           uint32_t const* list_n, // [0] out-rows, [1] in-rows
+           uint32_t* __restrict__ qout,
+           uint32_t* __restrict__ qout_n,
+           uint32_t* __restrict__ decided)
+{
+  unsigned const lane = threadIdx.x & 31u;
+  uint32_t       dec  = 0;
+#pragma unroll 1
+  for (int dir = 0; dir < 2; ++dir) {
+    uint32_t const* adj = dir ? bc : fc;
+    uint32_t*       deg = dir ? outdeg : indeg;
+    heavy_slices<true>(dir ? list_in : list_out, list_n[dir], dir ? bh : fh, [&](uint32_t, uint32_t, uint64_t b, uint64_t e) {
+      for (uint64_t x = b + lane; x < e; x += 32) {
+        uint32_t const w = adj[x];
+        if (bit_get(und, w) && atomicSub(deg + w, 1u) == 1u && bit_take(und, w)) {
+          scc_id[w] = w;
+          ++dec;
+          warp_push_active(w, qout, qout_n);
+        }
+      }
+    });
+  }
+  if (dec) atomicAdd(decided, dec);
+}
+
+__global__ void __launch_bounds__(T_THREADS)
+k_push_heavy(uint64_t const* __restrict__ fh,
+             uint32_t const* __restrict__ fc,
+             uint64_t const* __restrict__ bh,
+             uint32_t const* __restrict__ bc,
+             uint32_t* __restrict__ und,
+             uint32_t* __restrict__ scc_id,
+             uint32_t* __restrict__ indeg,
+             uint32_t* __restrict__ outdeg,
+             uint32_t const* list_out,
+             uint32_t const* list_in,
+             uint32_t const* list_n,
+             uint32_t* __restrict__ qout,
+             uint32_t* __restrict__ qout_n,
+             uint32_t* __restrict__ decided)
+{
+  push_heavy(fh, fc, bh, bc, und, scc_id, indeg, outdeg, list_out, list_in, list_n, qout, qout_n, decided);
+}
 
 unsigned
 stream_grid(uint64_t items)
@@ -214,15 +304,21 @@ k_live_degrees(uint32_t n,
                uint32_t const* __restrict__ bc,
                uint32_t const* __restrict__ und,
                uint32_t* __restrict__ indeg,
-               uint32_t* __restrict__ outdeg)
+               uint32_t* __restrict__ outdeg,
+               uint32_t* heavy,
+               uint32_t* heavy_n)
 {
   unsigned const lane = threadIdx.x & 31u;
   uint64_t const span = (static_cast<uint64_t>(n) + 31) & ~31ull;
   for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
     uint32_t const v    = static_cast<uint32_t>(t);
-    bool const     have = t < n && bit_get(und, v);
+    bool           have = t < n && bit_get(und, v);
     uint64_t       fb = 0, fe = 0, bb = 0, be = 0;
     if (have) fb = fh[v], fe = fh[v + 1], bb = bh[v], be = bh[v + 1];
+    bool const hv = have && (row_heavy(fb, fe) || row_heavy(bb, be));
+    if (hv) indeg[v] = outdeg[v] = 0; // counted by k_live_heavy
+    warp_push(hv, v, heavy, heavy_n);
+    have &= !hv;
     uint32_t   outc  = 0, inc = 0;
     bool const small = have && (fe - fb) < WARP_BIG && (be - bb) < WARP_BIG;
     if (small) {
@@ -291,7 +387,10 @@ k_trim_push(uint64_t const* __restrict__ fh,
             uint32_t* __restrict__ qout,
             uint32_t* __restrict__ qout_n,
             uint32_t* __restrict__ ctr,
-            unsigned long long* __restrict__ edges)
+            unsigned long long* __restrict__ edges,
+            uint32_t* heavy_out,
+            uint32_t* heavy_in,
+            uint32_t* heavy_n)
 {
   unsigned const lane = threadIdx.x & 31u;
   uint64_t const span = (static_cast<uint64_t>(qn) + 31) & ~31ull;
@@ -315,9 +414,11 @@ k_trim_push(uint64_t const* __restrict__ fh,
       uint32_t const u    = have ? qin[t] : 0;
       uint64_t       b = 0, e = 0;
       if (have) b = head[u], e = head[u + 1];
-      bool const big = have && (e - b) >= WARP_BIG;
+      bool const hv  = have && row_heavy(b, e); // k_push_heavy walks it
+      bool const big = have && !hv && (e - b) >= WARP_BIG;
       ne += e - b;
-      if (have && !big)
+      warp_push(hv, u, dir == 0 ? heavy_out : heavy_in, heavy_n + dir);
+      if (have && !big && !hv)
         for (uint64_t x = b; x < e; ++x) hit(adj[x], deg);
       unsigned todo = __ballot_sync(0xFFFFFFFFu, big);
       while (todo) {
@@ -467,13 +568,33 @@ struct trim_state
   uint32_t           decided;
   uint32_t           list_n; // undecided vertices at the start
   unsigned long long edges;  // edges pushed along
+  uint32_t           heavy_n[3]; // heavy rows listed: push out-rows, push in-rows (this level), live counts
 };
+
+// The level's heavy rows (listed by k_t_push) into the same output queue.
+__global__ void __launch_bounds__(T_THREADS)
+k_t_push_heavy(uint64_t const* __restrict__ fh,
+               uint32_t const* __restrict__ fc,
+               uint64_t const* __restrict__ bh,
+               uint32_t const* __restrict__ bc,
+               uint32_t* __restrict__ und,
+               uint32_t* __restrict__ scc_id,
+               uint32_t* __restrict__ indeg,
+               uint32_t* __restrict__ outdeg,
+               fio f,
+               trim_state* st,
+               uint32_t const* heavy_out,
+               uint32_t const* heavy_in)
+{
+  push_heavy(fh, fc, bh, bc, und, scc_id, indeg, outdeg, heavy_out, heavy_in, st->heavy_n, f.out(), f.out_n(), &st->decided);
+}
 
 __global__ void
 k_t_init(trim_state* st)
 {
   uint32_t const cap = st->cap;
   st->cur = st->qn[0] = st->qn[1] = st->level = st->err = st->decided = st->list_n = 0;
+  st->heavy_n[0] = st->heavy_n[1] = st->heavy_n[2] = 0;
   st->edges = 0;
   st->cap   = cap;
 }
@@ -507,16 +628,20 @@ k_t_compact(uint32_t n, uint32_t const* __restrict__ und, uint32_t* __restrict__
 // the whole warp.
 __global__ void __launch_bounds__(T_THREADS)
 k_t_live(uint64_t const* __restrict__ fh, uint32_t const* __restrict__ fc, uint64_t const* __restrict__ bh, uint32_t const* __restrict__ bc, uint32_t const* __restrict__ und, uint32_t const* __restrict__ list,
-         trim_state const* st, uint32_t* __restrict__ indeg, uint32_t* __restrict__ outdeg)
+         trim_state* st, uint32_t* __restrict__ indeg, uint32_t* __restrict__ outdeg, uint32_t* heavy)
 {
   unsigned const lane = threadIdx.x & 31u;
   uint32_t const ln   = st->list_n;
   uint64_t const span = (static_cast<uint64_t>(ln) + 31) & ~31ull;
   for (uint64_t t = static_cast<uint64_t>(blockIdx.x) * T_THREADS + threadIdx.x; t < span; t += static_cast<uint64_t>(gridDim.x) * T_THREADS) {
-    bool const     have = t < ln;
+    bool           have = t < ln;
     uint32_t const v    = have ? list[t] : 0u;
     uint64_t       fb = 0, fe = 0, bb = 0, be = 0;
     if (have) fb = fh[v], fe = fh[v + 1], bb = bh[v], be = bh[v + 1];
+    bool const hv = have && (row_heavy(fb, fe) || row_heavy(bb, be));
+    if (hv) indeg[v] = outdeg[v] = 0; // counted by k_live_heavy
+    warp_push(hv, v, heavy, &st->heavy_n[2]);
+    have &= !hv;
     uint32_t   outc  = 0, inc = 0;
     bool const small = have && (fe - fb) < WARP_BIG && (be - bb) < WARP_BIG;
     if (small) {
@@ -583,7 +708,9 @@ k_t_push(uint64_t const* __restrict__ fh,
          uint32_t* __restrict__ indeg,
          uint32_t* __restrict__ outdeg,
          fio f,
-         trim_state* st)
+         trim_state* st,
+         uint32_t* heavy_out,
+         uint32_t* heavy_in)
 {
   unsigned const  lane   = threadIdx.x & 31u;
   uint32_t const* qin    = f.in();
@@ -610,9 +737,11 @@ k_t_push(uint64_t const* __restrict__ fh,
       uint32_t const u    = have ? qin[t] : 0;
       uint64_t       b = 0, e = 0;
       if (have) b = head[u], e = head[u + 1];
-      bool const big = have && (e - b) >= WARP_BIG;
+      bool const hv  = have && row_heavy(b, e); // k_t_push_heavy walks it
+      bool const big = have && !hv && (e - b) >= WARP_BIG;
       ne += e - b;
-      if (have && !big)
+      warp_push(hv, u, dir == 0 ? heavy_out : heavy_in, &st->heavy_n[dir]);
+      if (have && !big && !hv)
         for (uint64_t x = b; x < e; ++x) hit(adj[x], deg);
       unsigned todo = __ballot_sync(0xFFFFFFFFu, big);
       while (todo) {
@@ -633,6 +762,7 @@ __global__ void
 k_t_advance(trim_state* st, cudaGraphConditionalHandle h, int in_graph)
 {
   st->level += 1;
+  st->heavy_n[0] = st->heavy_n[1] = 0; // the level's heavy rows were walked
   st->cur ^= 1u;
   st->qn[(st->cur & 1u) ^ 1u] = 0; // next level's output
   unsigned cond = st->qn[st->cur & 1u] > 0;
@@ -691,7 +821,11 @@ build_trim_graph(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* sc
     cudaGraphNode_t dep   = nullptr;
     dep = t_add_kernel(graph, dep, &k_t_init, 1, 1, st);
     dep = t_add_kernel(graph, dep, &k_t_compact, wgrid, T_THREADS, g.n, und, ws.q1, st);
-    dep = t_add_kernel(graph, dep, &k_t_live, vgrid, T_THREADS, g.fh, g.fc, g.bh, g.bc, und, ws.q1, st, ws.indeg, ws.outdeg);
+    uint32_t* const h_out  = ws.heavy;
+    uint32_t* const h_in   = ws.heavy + ws.heavy_cap;
+    uint32_t* const h_live = ws.heavy + 2 * ws.heavy_cap;
+    dep = t_add_kernel(graph, dep, &k_t_live, vgrid, T_THREADS, g.fh, g.fc, g.bh, g.bc, und, ws.q1, st, ws.indeg, ws.outdeg, h_live);
+    dep = t_add_kernel(graph, dep, &k_live_heavy, HEAVY_GRID, T_THREADS, g.fh, g.fc, g.bh, g.bc, und, h_live, &st->heavy_n[2], ws.indeg, ws.outdeg);
     dep = t_add_kernel(graph, dep, &k_t_seed, vgrid, T_THREADS, und, scc_id, ws.indeg, ws.outdeg, ws.q1, st, ws.q0);
     cudaGraphConditionalHandle h;
     KSPN_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault));
@@ -704,7 +838,8 @@ build_trim_graph(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* sc
     KSPN_CUDA(cudaGraphAddNode(&loop, graph, &dep, 1, &cp));
     cudaGraph_t     body = cp.conditional.phGraph_out[0];
     fio const       f{ ws.q0, ws.q1, &st->qn[0], &st->qn[1], &st->cur };
-    cudaGraphNode_t bdep = t_add_kernel(body, nullptr, &k_t_push, vgrid, T_THREADS, g.fh, g.fc, g.bh, g.bc, und, scc_id, ws.indeg, ws.outdeg, f, st);
+    cudaGraphNode_t bdep = t_add_kernel(body, nullptr, &k_t_push, vgrid, T_THREADS, g.fh, g.fc, g.bh, g.bc, und, scc_id, ws.indeg, ws.outdeg, f, st, h_out, h_in);
+    bdep                 = t_add_kernel(body, bdep, &k_t_push_heavy, HEAVY_GRID, T_THREADS, g.fh, g.fc, g.bh, g.bc, und, scc_id, ws.indeg, ws.outdeg, f, st, (uint32_t const*)h_out, (uint32_t const*)h_in);
     t_add_kernel(body, bdep, &k_t_advance, 1, 1, st, h, 1);
     cudaGraphExec_t exec = nullptr;
     KSPN_CUDA(cudaGraphInstantiate(&exec, graph, 0));
@@ -748,13 +883,16 @@ run_push_levels(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc
     if (level > cap) throw error{ KSPN_ERR_TIMEOUT, "trim: level cap exceeded" };
     KSPN_CUDA(cudaMemsetAsync(ws.ctr + CTR_Q1, 0, sizeof(uint32_t), ctx->stream));
     KSPN_CUDA(cudaMemsetAsync(ws.ctr + CTR_DECIDED, 0, sizeof(uint32_t), ctx->stream));
+    KSPN_CUDA(cudaMemsetAsync(ws.ctr + CTR_TRIM_HEAVY, 0, 2 * sizeof(uint32_t), ctx->stream));
     uint64_t const e0 = ctx->h_ctr64[2];
     prof_start(ctx);
     k_trim_push<DIRS><<<stream_grid(qn), T_THREADS, 0, ctx->stream>>>(g.fh, g.fc, g.bh, g.bc, und, scc_id, ws.indeg, ws.outdeg, qa, qn, qb, ws.ctr + CTR_Q1, ws.ctr,
-                                                                       reinterpret_cast<unsigned long long*>(ws.ctr64 + 2));
+                                                                       reinterpret_cast<unsigned long long*>(ws.ctr64 + 2), ws.heavy, ws.heavy + ws.heavy_cap, ws.ctr + CTR_TRIM_HEAVY);
+    k_push_heavy<<<HEAVY_GRID, T_THREADS, 0, ctx->stream>>>(g.fh, g.fc, g.bh, g.bc, und, scc_id, ws.indeg, ws.outdeg, ws.heavy, ws.heavy + ws.heavy_cap, ws.ctr + CTR_TRIM_HEAVY, qb, ws.ctr + CTR_Q1,
+                                                            ws.ctr + CTR_DECIDED);
     prof_stop(ctx);
     KSPN_CHECK_LAUNCH();
-    ctx->launches += 1;
+    ctx->launches += 2;
     read_counters(ctx);
     // per queued vertex and direction: queue entry + offset pair; per edge:
     // id + degree atomic; per decided vertex: id write + queue write
@@ -856,15 +994,16 @@ trim_fixpoint(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_i
     KSPN_CUDA(cudaMemcpyAsync(hs, trim_state_dev(ctx), sizeof(trim_state), cudaMemcpyDeviceToHost, ctx->stream));
     KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
     if (hs->err) throw error{ KSPN_ERR_TIMEOUT, "trim: level cap exceeded" };
-    ctx->launches += 4 + 2ull * hs->level;
+    ctx->launches += 5 + 3ull * hs->level;
     return hs->decided;
   }
   if (!degrees_from_first) {
     zero_counters(ctx);
-    k_live_degrees<<<stream_grid(g.n), T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.fc, g.bh, g.bc, und, ws.indeg, ws.outdeg);
+    k_live_degrees<<<stream_grid(g.n), T_THREADS, 0, ctx->stream>>>(g.n, g.fh, g.fc, g.bh, g.bc, und, ws.indeg, ws.outdeg, ws.heavy, ws.ctr + CTR_TRIM_HEAVY + 3);
+    k_live_heavy<<<HEAVY_GRID, T_THREADS, 0, ctx->stream>>>(g.fh, g.fc, g.bh, g.bc, und, ws.heavy, ws.ctr + CTR_TRIM_HEAVY + 3, ws.indeg, ws.outdeg);
     k_seed_dead<<<stream_grid(g.n), T_THREADS, 0, ctx->stream>>>(g.n, und, scc_id, ws.indeg, ws.outdeg, ws.q0, ws.ctr);
     KSPN_CHECK_LAUNCH();
-    ctx->launches += 2;
+    ctx->launches += 3;
     read_counters(ctx);
     qn    = ctx->h_ctr[CTR_Q0];
     total = qn;
