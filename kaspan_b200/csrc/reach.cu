@@ -251,8 +251,8 @@ struct bu_warp_smem
 // Rows cut short in bottom-up sweeps: a row the warp has walked HEAVY_ROW
 // entries of without a hit is left open (the vertex stays a candidate) and
 // its vertex listed once (map) for a fix-up step that walks the listed
-// rows in slices over the whole grid.  No bu_cut (nullptr): rows are
-// walked to the end.
+// rows in slices over the whole grid.  CUT = false: rows are walked to the
+// end.
 struct bu_cut
 {
   uint32_t* map;  // bitmap of listed vertices
@@ -262,13 +262,19 @@ struct bu_cut
   uint32_t* err;  // set if it were
 };
 
+// The running sweep's cut descriptor: block-shared, set by thread 0 before
+// the sweep (a barrier between) and read only on the rare path, so the
+// sweep's hot loop holds no register for it.
+__shared__ bu_cut s_bu_cut;
+
 // Row walks of up to BU_ILP candidates per lane (v[k], live[k]): all
 // neighbour loads of a step, then all probes of `mark`; rows still open
 // after BU_STEPS neighbours are finished by the whole warp with early exit
 // (or cut, see bu_cut).  found[k]: a neighbour of v[k] is in mark.  All
 // lanes call it.
+template<bool CUT>
 __device__ __forceinline__ void
-bu_rows(uint32_t const (&v)[BU_ILP], bool (&live)[BU_ILP], bool (&found)[BU_ILP], uint64_t const* __restrict__ head, uint32_t const* __restrict__ adj, uint32_t const* mark, uint64_t& nedge, bu_cut const* cut)
+bu_rows(uint32_t const (&v)[BU_ILP], bool (&live)[BU_ILP], bool (&found)[BU_ILP], uint64_t const* __restrict__ head, uint32_t const* __restrict__ adj, uint32_t const* mark, uint64_t& nedge)
 {
   unsigned const lane = threadIdx.x & 31u;
   uint64_t       b[BU_ILP], e[BU_ILP];
@@ -311,7 +317,7 @@ bu_rows(uint32_t const (&v)[BU_ILP], bool (&live)[BU_ILP], bool (&found)[BU_ILP]
       unsigned const l = __ffs(todo) - 1;
       todo &= todo - 1;
       uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b[k], l), e0 = __shfl_sync(0xFFFFFFFFu, e[k], l);
-      uint64_t const e1 = cut && e0 - b0 > HEAVY_ROW ? b0 + HEAVY_ROW : e0;
+      uint64_t const e1 = CUT && e0 - b0 > HEAVY_ROW ? b0 + HEAVY_ROW : e0;
       bool           hit = false;
       for (uint64_t x = b0; x < e1; x += 32) {
         bool const     in = x + lane < e1;
@@ -325,10 +331,10 @@ bu_rows(uint32_t const (&v)[BU_ILP], bool (&live)[BU_ILP], bool (&found)[BU_ILP]
       }
       if (lane == l) {
         found[k] = hit;
-        if (!hit && e1 < e0 && bit_claim(cut->map, v[k])) {
-          uint32_t const i = atomicAdd(cut->n, 1u);
-          if (i < cut->cap) cut->list[i] = v[k];
-          else atomicExch(cut->err, 1u);
+        if (CUT && !hit && e1 < e0 && bit_claim(s_bu_cut.map, v[k])) {
+          uint32_t const i = atomicAdd(s_bu_cut.n, 1u);
+          if (i < s_bu_cut.cap) s_bu_cut.list[i] = v[k];
+          else atomicExch(s_bu_cut.err, 1u);
         }
       }
     }
@@ -345,6 +351,7 @@ bu_rows(uint32_t const (&v)[BU_ILP], bool (&live)[BU_ILP], bool (&found)[BU_ILP]
 // in mark and writes the word of `fresh` (the sweep's discoveries).  No
 // queue is written; the discovery count goes to nfound.  `avail` and `mark` are read through L2 (other
 // blocks of a persistent launch change them).
+template<bool CUT>
 __device__ __forceinline__ void
 bu_sweep_warp(uint32_t first,
               uint32_t step,
@@ -357,8 +364,7 @@ bu_sweep_warp(uint32_t first,
               bu_warp_smem& sm,
               uint32_t& nfound,
               uint64_t& nedge,
-              uint64_t& ncand,
-              bu_cut const* cut)
+              uint64_t& ncand)
 {
   unsigned const lane   = threadIdx.x & 31u;
   uint32_t const words  = (n + 31) / 32;
@@ -393,7 +399,7 @@ bu_sweep_warp(uint32_t first,
         live[k]          = i < total;
         v[k]             = live[k] ? c * 1024 + sm.cand[i] : 0u;
       }
-      bu_rows(v, live, found, head, adj, mark, nedge, cut);
+      bu_rows<CUT>(v, live, found, head, adj, mark, nedge);
 #pragma unroll
       for (int k = 0; k < BU_ILP; ++k)
         if (found[k]) atomicOr(&sm.found[(v[k] >> 5) - c * 32], 1u << (v[k] & 31));
@@ -462,13 +468,12 @@ k_bottom_up(uint32_t n,
 {
   if (g.closed()) return;
   __shared__ bu_warp_smem sm[BU_WARPS];
-  __shared__ bu_cut       s_cut;
-  if (threadIdx.x == 0) s_cut = cut;
+  if (threadIdx.x == 0) s_bu_cut = cut;
   __syncthreads();
   uint32_t                nfound = 0;
   uint64_t                nedge = 0, ncand = 0;
   unsigned const          wid = threadIdx.x >> 5;
-  bu_sweep_warp(blockIdx.x * BU_WARPS + wid, gridDim.x * BU_WARPS, n, head, adj, avail, mark, fresh, sm[wid], nfound, nedge, ncand, cut.map ? &s_cut : nullptr);
+  bu_sweep_warp<true>(blockIdx.x * BU_WARPS + wid, gridDim.x * BU_WARPS, n, head, adj, avail, mark, fresh, sm[wid], nfound, nedge, ncand);
 #pragma unroll
   for (int s = 16; s; s >>= 1) {
     nedge += __shfl_down_sync(0xFFFFFFFFu, nedge, s);
@@ -667,7 +672,6 @@ struct fwbw_smem
   uint32_t              cnt;
   unsigned long long    old;
   unsigned long long    edges_bu, cands_bu; // bottom-up statistics of the launch
-  bu_cut                cut;                // the running search's cut rows
   __device__ __forceinline__ uint32_t* tile_rows() { return reinterpret_cast<uint32_t*>(warp); }
   __device__ __forceinline__ uint32_t* buf() { return reinterpret_cast<uint32_t*>(warp) + EX_TILE; }
 };
@@ -1021,11 +1025,10 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
   uint64_t                 edges_td = 0;
   bool const               tally = blockIdx.x == 0 && threadIdx.x == 0; // keeps the byte-model counts in st
   bool                     fixed = false; // the last level was a fix-up step
-  // rows the sweeps cut short (bu_cut, read from shared memory where the
-  // sweep needs it; every level ends in a grid barrier, so the block's
-  // sweeps see it): the FW search lists them in heavy list 3, the BW
-  // search in list 0
-  if (threadIdx.x == 0) sm.cut = bu_cut{ a.cutmap, a.heavy + (BW ? 0u : 3u) * a.heavy_cap, &st->cut_n[BW ? 1 : 0], a.heavy_cap, &st->heavy_err };
+  // rows the sweeps cut short (s_bu_cut; every level ends in a grid
+  // barrier, so the block's sweeps see it): the FW search lists them in
+  // heavy list 3, the BW search in list 0
+  if (threadIdx.x == 0) s_bu_cut = bu_cut{ a.cutmap, a.heavy + (BW ? 0u : 3u) * a.heavy_cap, &st->cut_n[BW ? 1 : 0], a.heavy_cap, &st->heavy_err };
   // the first frontier: the pivot alone
   unsigned long long c = (static_cast<unsigned long long>(td_head[pivot + 1] - td_head[pivot]) << a.qbits) | 1u;
   for (;; ++lvl, ++glvl) {
@@ -1132,7 +1135,7 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
       uint32_t       nfound = 0;
       uint64_t       ne = 0, nc = 0;
       if (tally) st->bu_bitmap += 1;
-      bu_sweep_warp(blockIdx.x * BU_WARPS + wid, gridDim.x * BU_WARPS, a.n, bu_head, bu_adj, avail, mark, a.fresh, sm.warp[wid], nfound, ne, nc, &sm.cut);
+      bu_sweep_warp<true>(blockIdx.x * BU_WARPS + wid, gridDim.x * BU_WARPS, a.n, bu_head, bu_adj, avail, mark, a.fresh, sm.warp[wid], nfound, ne, nc);
 #pragma unroll
       for (int sh = 16; sh; sh >>= 1) {
         nfound += __shfl_down_sync(0xFFFFFFFFu, nfound, sh);
@@ -1223,19 +1226,28 @@ trim_seed(fwbw_args const& a, uint32_t const* list, uint64_t list_n, uint32_t* q
     uint32_t const x    = have ? __ldcg(list + t) : 0u;
     uint64_t       ob = 0, oe = 0, ib = 0, ie = 0;
     if (have) ob = a.fh[x], oe = a.fh[x + 1], ib = a.bh[x], ie = a.bh[x + 1];
-    bool const hv    = have && (oe - ob > HEAVY_ROW || ie - ib > HEAVY_ROW);
     bool const small = have && (oe - ob) + (ie - ib) <= TRIM_SMALL;
+    bool       hv    = false;
     uint32_t   co = 0, ci = 0;
     if (small) {
       co = count_live(snap, a.fc, ob, oe);
       ci = count_live(snap, a.bc, ib, ie);
     }
-    if (hv) a.outdeg[x] = a.indeg[x] = 0; // counted in slices
-    warp_push(hv, x, a.heavy, &a.st->hseed_n);
-    for (unsigned todo = __ballot_sync(0xFFFFFFFFu, have && !small && !hv); todo; todo &= todo - 1) {
+    for (unsigned todo = __ballot_sync(0xFFFFFFFFu, have && !small); todo; todo &= todo - 1) {
       unsigned const l  = __ffs(todo) - 1;
       uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, ob, l), e0 = __shfl_sync(0xFFFFFFFFu, oe, l);
       uint64_t const b1 = __shfl_sync(0xFFFFFFFFu, ib, l), e1 = __shfl_sync(0xFFFFFFFFu, ie, l);
+      if (e0 - b0 > HEAVY_ROW || e1 - b1 > HEAVY_ROW) {
+        // listed for the slice pass, counts zeroed for it
+        if (lane == l) {
+          hv = true;
+          a.outdeg[x] = a.indeg[x] = 0;
+          uint32_t const i = atomicAdd(&a.st->hseed_n, 1u);
+          if (i < a.heavy_cap) a.heavy[i] = x;
+          else atomicExch(&a.st->heavy_err, 1u);
+        }
+        continue;
+      }
       uint32_t       xo = 0, xi = 0;
       for (uint64_t e = b0 + lane; e < e0; e += 32) xo += snap_bit(snap, a.fc[e]);
       for (uint64_t e = b1 + lane; e < e1; e += 32) xi += snap_bit(snap, a.bc[e]);
@@ -1283,6 +1295,7 @@ trim_push(fwbw_args const& a, uint32_t const* qin, uint32_t qn, uint32_t* qout, 
 {
   unsigned const lane = threadIdx.x & 31u;
   trim_hq const  hin = trim_heavy_at(a, glvl), hout = trim_heavy_at(a, glvl + 1);
+  uint32_t const hn0 = __ldcg(hin.n), hn1 = __ldcg(hin.n + 1); // issued early
   uint64_t const span = (static_cast<uint64_t>(qn) + 31) & ~31ull;
   // w's und word already probed: decrement, decide and queue at 0
   auto const hit = [&](uint32_t w, uint32_t word, uint32_t* deg) {
@@ -1319,34 +1332,29 @@ trim_push(fwbw_args const& a, uint32_t const* qin, uint32_t qn, uint32_t* qout, 
       uint32_t const u    = have ? __ldcg(qin + t) : 0u;
       uint64_t       b = 0, e = 0;
       if (have) b = head[u], e = head[u + 1];
-      bool const big = have && e - b >= TRIM_SMALL && e - b <= HEAVY_ROW;
-      bool const hv  = have && e - b > HEAVY_ROW;
+      bool const big = have && e - b >= TRIM_SMALL;
       edges += e - b;
-      if (have && e - b < TRIM_SMALL) row(adj, b, e, deg);
-      {
-        // heavy rows: listed for the next level (one atomic per warp)
-        unsigned const bal = __ballot_sync(0xFFFFFFFFu, hv);
-        if (bal) {
-          uint32_t base = 0;
-          if (lane == 0) base = atomicAdd(hout.n + dir, static_cast<uint32_t>(__popc(bal)));
-          base = __shfl_sync(0xFFFFFFFFu, base, 0) + __popc(bal & ((1u << lane) - 1u));
-          // front and back never meet: heavy_capacity covers both directions
-          if (hv) {
-            if (base < a.heavy_cap / 2) hout.list[dir ? a.heavy_cap - 1 - base : base] = u;
-            else atomicExch(&a.st->heavy_err, 1u);
-          }
-        }
-      }
+      if (have && !big) row(adj, b, e, deg);
       for (unsigned todo = __ballot_sync(0xFFFFFFFFu, big); todo; todo &= todo - 1) {
         unsigned const l  = __ffs(todo) - 1;
         uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b, l), e0 = __shfl_sync(0xFFFFFFFFu, e, l);
+        if (e0 - b0 > HEAVY_ROW) {
+          // listed for the next level's slices (front: out-rows, back:
+          // in-rows; they never meet, heavy_capacity covers both)
+          if (lane == l) {
+            uint32_t const i = atomicAdd(hout.n + dir, 1u);
+            if (i < a.heavy_cap / 2) hout.list[dir ? a.heavy_cap - 1 - i : i] = u;
+            else atomicExch(&a.st->heavy_err, 1u);
+          }
+          continue;
+        }
         for (uint64_t x = b0 + lane; x < e0; x += 32) {
           uint32_t const w = adj[x];
           hit(w, __ldcg(a.und + (w >> 5)), deg);
         }
       }
     }
-    uint32_t const hn = __ldcg(hin.n + dir);
+    uint32_t const hn = dir ? hn1 : hn0;
     heavy_slices(dir ? hin.list + a.heavy_cap - hn : hin.list, hn, head, [&](uint32_t, uint32_t, uint64_t b0, uint64_t e0) {
       for (uint64_t x = b0 + lane; x < e0; x += 32) {
         uint32_t const w = adj[x];
