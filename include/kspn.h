@@ -319,6 +319,61 @@ int kspn_mlp_gradient(kspn_context* ctx, uint32_t count, const float* d_features
  * device parameters, with moment buffers d_m, d_v (KSPN_MLP_PARAMS each). */
 int kspn_mlp_adam(kspn_context* ctx, float* d_params, const float* d_grad, float* d_m, float* d_v, float lr, int step);
 
+/* ---------------------------------------------------------------- batched */
+/*
+ * Many independent graphs in one call (no reference counterpart: the
+ * reference decomposes one graph per `scc` call, kaspan/scc/scc.hpp:21-87;
+ * each graph here gets the partition that call gives, min-member ids).
+ * Graph g owns vertices [vtx_off[g], vtx_off[g+1]) of ONE concatenated CSR
+ * (fw) and CSC (bw) over n_total = vtx_off[count] vertices: heads hold
+ * global edge positions, rows hold LOCAL ids (0 .. n_g - 1).  Output:
+ * scc_id[vtx_off[g] + v] = the local id of the smallest member of v's SCC.
+ * Graphs of at most 512 vertices and 2048 edges are decomposed by one warp
+ * each (Tarjan in shared memory), larger ones by one block each (trim-1,
+ * FW-BW rounds, Tarjan of the remainder), all in one captured CUDA graph
+ * that later calls with the same arrays and settings replay.  Device
+ * pointers; the context's stream; synchronous.
+ */
+typedef struct kspn_batch_options {
+    uint32_t max_rounds;   /* FW-BW rounds per large graph before one thread's Tarjan finishes it (0: 64) */
+    uint32_t rem_tarjan;   /* a large graph's remainder of at most this many vertices goes to the
+                              shared-memory Tarjan (0: 512, the most it holds) */
+    uint32_t reserved[6];
+} kspn_batch_options;
+
+typedef struct kspn_batch_stats {
+    uint32_t graphs_small;  /* decomposed by one warp */
+    uint32_t graphs_large;  /* decomposed by one block */
+    uint32_t fwbw_rounds;   /* FW-BW rounds over all large graphs */
+    uint32_t tarjan_smem;   /* remainders finished in shared memory */
+    uint32_t tarjan_serial; /* remainders finished by one thread (round cap) */
+    uint32_t trim_levels;   /* trim push levels over all large graphs */
+    float    ms;            /* device time of the call (CUDA events) */
+    uint32_t reserved[9];
+} kspn_batch_stats;
+
+void kspn_batch_options_default(kspn_batch_options* opt);
+int  kspn_scc_batched(kspn_context* ctx, uint32_t count, uint64_t n_total,
+                      const uint64_t* d_vtx_off,
+                      const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
+                      const uint64_t* d_bw_head, const uint32_t* d_bw_csr,
+                      uint32_t* d_scc_id, const kspn_batch_options* opt, kspn_batch_stats* stats);
+
+/* The batch mix of uneven G(n,m) graphs (host, deterministic): graph i has
+ * n_i = round(2^U[log2_min, log2_max]) vertices and round(n_i * U[deg_min,
+ * deg_max]) edge draws, both drawn from SplitMix64 stream `seed` (the
+ * per-graph key is draw i of that stream). */
+void kspn_batch_shape(uint32_t count, uint64_t seed, uint32_t log2_min, uint32_t log2_max,
+                      float deg_min, float deg_max, uint32_t* n_out, uint64_t* draws_out);
+/* Its edge draws on the device, GLOBAL ids (vtx_off[g] + local): draw k of
+ * graph g is (u, v) uniform in [0, n_g)^2; d_draw_off = prefix of draws_out. */
+int  kspn_gen_batch(kspn_context* ctx, uint32_t count, uint64_t seed,
+                    const uint64_t* d_vtx_off, const uint64_t* d_draw_off,
+                    uint32_t* d_src, uint32_t* d_dst);
+/* Global ids -> local ids in every row of a concatenated CSR or CSC. */
+int  kspn_batch_localize(kspn_context* ctx, uint32_t count, uint64_t n_total,
+                         const uint64_t* d_vtx_off, const uint64_t* d_head, uint32_t* d_csr);
+
 /* ---------------------------------------------------------------- inputs */
 /*
  * Seeded synthetic edge lists on the device (no reference counterpart:

@@ -187,7 +187,35 @@ SIGNATURES = {
     "kspn_gen_rmat": (_i32, [_P, _i32, _u64, _u64, _u64, _u64, _u64, _i32, _P, _P]),
     "kspn_gen_rgg": (_i32, [_P, _u32, _u64, _u32, _u64, _P, _P, _u64, _P]),
     "kspn_build_csr": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P]),
+    "kspn_batch_options_default": (None, [_P]),
+    "kspn_scc_batched": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "kspn_batch_shape": (None, [_u32, _u64, _u32, _u32, C.c_float, C.c_float, _P, _P]),
+    "kspn_gen_batch": (_i32, [_P, _u32, _u64, _P, _P, _P, _P]),
+    "kspn_batch_localize": (_i32, [_P, _u32, _u64, _P, _P, _P]),
 }
+
+
+class BatchOptions(C.Structure):
+    """kspn_batch_options (include/kspn.h)."""
+    _fields_ = [("max_rounds", C.c_uint32), ("rem_tarjan", C.c_uint32), ("reserved", C.c_uint32 * 6)]
+
+
+class BatchStats(C.Structure):
+    """kspn_batch_stats (include/kspn.h)."""
+    _fields_ = [("graphs_small", C.c_uint32), ("graphs_large", C.c_uint32), ("fwbw_rounds", C.c_uint32),
+                ("tarjan_smem", C.c_uint32), ("tarjan_serial", C.c_uint32), ("trim_levels", C.c_uint32),
+                ("ms", C.c_float), ("reserved", C.c_uint32 * 9)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+def batch_shape(count: int, seed: int, log2_min: int = 8, log2_max: int = 18, deg_min: float = 0.8, deg_max: float = 6.0):
+    """(n[count] uint32, draws[count] uint64) of the batch mix (host, deterministic)."""
+    n = np.zeros(count, np.uint32)
+    d = np.zeros(count, np.uint64)
+    lib().kspn_batch_shape(count, seed, log2_min, log2_max, deg_min, deg_max, n.ctypes.data, d.ctypes.data)
+    return n, d
 
 _lib = None
 
@@ -394,6 +422,19 @@ class Context:
         self._check(lib().kspn_gen_rgg(self.h, n, seed, g, r2, _ptr(src) if src is not None else None,
                                        _ptr(dst) if dst is not None else None, capacity, C.byref(m)), "gen_rgg")
         return m.value
+
+    # ---- batched path
+    def scc_batched(self, count, n_total, vtx_off, fwh, fwc, bwh, bwc, out, options: "BatchOptions | None" = None) -> "BatchStats":
+        st = BatchStats()
+        self._check(lib().kspn_scc_batched(self.h, count, n_total, _ptr(vtx_off), _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc), _ptr(out),
+                                           C.byref(options) if options is not None else None, C.byref(st)), "scc_batched")
+        return st
+
+    def gen_batch(self, count, seed, vtx_off, draw_off, src, dst):
+        self._check(lib().kspn_gen_batch(self.h, count, seed, _ptr(vtx_off), _ptr(draw_off), _ptr(src), _ptr(dst)), "gen_batch")
+
+    def batch_localize(self, count, n_total, vtx_off, head, csr):
+        self._check(lib().kspn_batch_localize(self.h, count, n_total, _ptr(vtx_off), _ptr(head), _ptr(csr)), "batch_localize")
 
     def build_csr(self, n, m_raw, src, dst, head, csr) -> int:
         m = C.c_uint64()

@@ -596,6 +596,7 @@ kspn_context_destroy(kspn_context* ctx)
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   release_graphs(ctx);
+  batch_release(ctx);
   if (ctx->pivot_model) cudaFree(ctx->pivot_model);
   if (ctx->ws.base) cudaFree(ctx->ws.base);
   if (ctx->h_ctr) cudaFreeHost(ctx->h_ctr);
@@ -884,6 +885,67 @@ kspn_residual(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_he
     uint32_t const d    = n ? residual(ctx, g, reinterpret_cast<uint32_t*>(d_undecided), d_scc_id, &left) : 0;
     if (decided) *decided = d;
     if (pieces_left) *pieces_left = left;
+  });
+}
+
+void
+kspn_batch_options_default(kspn_batch_options* opt)
+{
+  if (opt) std::memset(opt, 0, sizeof(*opt));
+}
+
+int
+kspn_scc_batched(kspn_context* ctx, uint32_t count, uint64_t n_total, const uint64_t* d_vtx_off, const uint64_t* d_fw_head, const uint32_t* d_fw_csr, const uint64_t* d_bw_head,
+                 const uint32_t* d_bw_csr, uint32_t* d_scc_id, const kspn_batch_options* opt, kspn_batch_stats* stats)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(count == 0 || (d_vtx_off && d_fw_head && d_fw_csr && d_bw_head && d_bw_csr && d_scc_id), "null pointer");
+    require(n_total < 0xFFFFFFFFull, "n_total must be below 2^32 - 1");
+    bind_device(ctx);
+    kspn_batch_options o{};
+    if (opt) o = *opt;
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    KSPN_CUDA(cudaEventRecord(ctx->ev[KSPN_PHASES], ctx->stream));
+    scc_batched(ctx, count, n_total, d_vtx_off, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr, d_scc_id, o, stats);
+    KSPN_CUDA(cudaEventRecord(ctx->ev[KSPN_PHASES + 1], ctx->stream));
+    KSPN_CUDA(cudaEventSynchronize(ctx->ev[KSPN_PHASES + 1]));
+    if (stats) KSPN_CUDA(cudaEventElapsedTime(&stats->ms, ctx->ev[KSPN_PHASES], ctx->ev[KSPN_PHASES + 1]));
+  });
+}
+
+void
+kspn_batch_shape(uint32_t count, uint64_t seed, uint32_t log2_min, uint32_t log2_max, float deg_min, float deg_max, uint32_t* n_out, uint64_t* draws_out)
+{
+  batch_shape(count, seed, log2_min, log2_max, deg_min, deg_max, n_out, draws_out);
+}
+
+int
+kspn_gen_batch(kspn_context* ctx, uint32_t count, uint64_t seed, const uint64_t* d_vtx_off, const uint64_t* d_draw_off, uint32_t* d_src, uint32_t* d_dst)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(count == 0 || (d_vtx_off && d_draw_off && d_src && d_dst), "null pointer");
+    bind_device(ctx);
+    uint64_t total = 0;
+    if (count) {
+      KSPN_CUDA(cudaMemcpyAsync(&total, d_draw_off + count, sizeof(total), cudaMemcpyDeviceToHost, ctx->stream));
+      KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    gen_batch(ctx, count, seed, d_vtx_off, d_draw_off, total, d_src, d_dst);
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+  });
+}
+
+int
+kspn_batch_localize(kspn_context* ctx, uint32_t count, uint64_t n_total, const uint64_t* d_vtx_off, const uint64_t* d_head, uint32_t* d_csr)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(count == 0 || (d_vtx_off && d_head && d_csr), "null pointer");
+    bind_device(ctx);
+    batch_localize(ctx, count, n_total, d_vtx_off, d_head, d_csr);
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
   });
 }
 

@@ -17,6 +17,8 @@
 #include "kspn_internal.cuh"
 #include "prim.cuh"
 
+#include <cmath>
+
 namespace kspn {
 
 namespace {
@@ -272,6 +274,89 @@ gen_rgg(kspn_context* ctx, uint32_t n, uint64_t seed, uint32_t g, uint64_t r2, u
     ctx->launches += 1;
   }
   return m;
+}
+
+// ---------------------------------------------------------------- batch mix
+// Graph i's key is draw i of the stream of `seed`; its shape stream is
+// that key's stream (draw 0: size, draw 1: mean degree), its edge stream
+// the stream of key ^ "EDGE": draw k is edge k, (u, v) as in G(n, m).
+
+namespace {
+
+__host__ __device__ __forceinline__ uint64_t
+batch_key(uint64_t seed, uint32_t g)
+{
+  return draw(seed_key(seed), g);
+}
+
+__global__ void
+k_gen_batch(uint32_t count, uint64_t seed, uint64_t const* __restrict__ vtx_off, uint64_t const* __restrict__ draw_off, uint64_t total, uint32_t* __restrict__ src, uint32_t* __restrict__ dst)
+{
+  for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < total; j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    // graph of draw j: the last g with draw_off[g] <= j
+    uint32_t lo = 0, hi = count;
+    while (lo + 1 < hi) {
+      uint32_t const mid = (lo + hi) / 2;
+      if (draw_off[mid] <= j) lo = mid;
+      else hi = mid;
+    }
+    uint64_t const vo = vtx_off[lo];
+    uint64_t const n  = vtx_off[lo + 1] - vo;
+    uint64_t const d  = draw(seed_key(batch_key(seed, lo) ^ 0x45444745ull), j - draw_off[lo]);
+    src[j]            = static_cast<uint32_t>(vo + ((d & 0xFFFFFFFFull) * n >> 32));
+    dst[j]            = static_cast<uint32_t>(vo + ((d >> 32) * n >> 32));
+  }
+}
+
+__global__ void
+k_batch_localize(uint32_t count, uint64_t N, uint64_t const* __restrict__ vtx_off, uint64_t const* __restrict__ head, uint32_t* __restrict__ csr)
+{
+  for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < N; v += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    uint32_t lo = 0, hi = count;
+    while (lo + 1 < hi) {
+      uint32_t const mid = (lo + hi) / 2;
+      if (vtx_off[mid] <= v) lo = mid;
+      else hi = mid;
+    }
+    uint32_t const vo = static_cast<uint32_t>(vtx_off[lo]);
+    for (uint64_t e = head[v], end = head[v + 1]; e < end; ++e) csr[e] -= vo;
+  }
+}
+
+} // namespace
+
+void
+batch_shape(uint32_t count, uint64_t seed, uint32_t log2_min, uint32_t log2_max, float deg_min, float deg_max, uint32_t* n_out, uint64_t* draws_out)
+{
+  for (uint32_t g = 0; g < count; ++g) {
+    uint64_t const k  = seed_key(batch_key(seed, g));
+    double const   u1 = static_cast<double>(draw(k, 0) >> 11) * 0x1.0p-53;
+    double const   u2 = static_cast<double>(draw(k, 1) >> 11) * 0x1.0p-53;
+    double const   n  = std::nearbyint(std::exp2(log2_min + (static_cast<double>(log2_max) - log2_min) * u1));
+    double const   d  = deg_min + (static_cast<double>(deg_max) - deg_min) * u2;
+    n_out[g]          = static_cast<uint32_t>(n < 1 ? 1 : n);
+    draws_out[g]      = static_cast<uint64_t>(std::nearbyint(n_out[g] * d));
+  }
+}
+
+void
+gen_batch(kspn_context* ctx, uint32_t count, uint64_t seed, uint64_t const* vtx_off, uint64_t const* draw_off, uint64_t total, uint32_t* src, uint32_t* dst)
+{
+  if (!total || !count) return;
+  uint64_t const b = (total + 255) / 256;
+  k_gen_batch<<<static_cast<unsigned>(b < 148ull * 64 ? b : 148ull * 64), 256, 0, ctx->stream>>>(count, seed, vtx_off, draw_off, total, src, dst);
+  KSPN_CHECK_LAUNCH();
+  ctx->launches += 1;
+}
+
+void
+batch_localize(kspn_context* ctx, uint32_t count, uint64_t N, uint64_t const* vtx_off, uint64_t const* head, uint32_t* csr)
+{
+  if (!N || !count) return;
+  uint64_t const b = (N + 255) / 256;
+  k_batch_localize<<<static_cast<unsigned>(b < 148ull * 64 ? b : 148ull * 64), 256, 0, ctx->stream>>>(count, N, vtx_off, head, csr);
+  KSPN_CHECK_LAUNCH();
+  ctx->launches += 1;
 }
 
 } // namespace kspn

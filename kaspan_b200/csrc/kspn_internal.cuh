@@ -339,6 +339,10 @@ struct cached_graph
 };
 } // namespace kspn
 
+namespace kspn {
+struct batch_cache; // batched path: plan buffers and the captured call (batch.cu)
+}
+
 struct kspn_context
 {
   int                device     = 0;
@@ -359,6 +363,7 @@ struct kspn_context
   unsigned           search_grid = 0;      // blocks of the persistent FW-BW launch
   float*             pivot_model = nullptr; // device copy of the pivot MLP (kspn_set_pivot_model)
   kspn::cached_graph trim;                 // one-launch trim fixpoint graph
+  kspn::batch_cache* batch      = nullptr;  // batched path (kspn_scc_batched)
   kspn::dev_buffer   bufs[kspn::BUF_COUNT];
 };
 
@@ -420,6 +425,12 @@ uint32_t trim_fixpoint(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32
 uint32_t trim_exhaustive_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* outdeg, uint32_t* indeg);
 uint32_t trim_2(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id);
 uint32_t select_pivot_live(kspn_context* ctx, dgraph const& g, uint32_t const* und);
+void     scc_batched(kspn_context* ctx, uint32_t G, uint64_t N, uint64_t const* vtx_off, uint64_t const* fh, uint32_t const* fc, uint64_t const* bh, uint32_t const* bc, uint32_t* scc_id,
+                     kspn_batch_options const& opt, kspn_batch_stats* st);
+void     batch_release(kspn_context* ctx);
+void     batch_shape(uint32_t count, uint64_t seed, uint32_t log2_min, uint32_t log2_max, float deg_min, float deg_max, uint32_t* n_out, uint64_t* draws_out);
+void     gen_batch(kspn_context* ctx, uint32_t count, uint64_t seed, uint64_t const* vtx_off, uint64_t const* draw_off, uint64_t total_draws, uint32_t* src, uint32_t* dst);
+void     batch_localize(kspn_context* ctx, uint32_t count, uint64_t N, uint64_t const* vtx_off, uint64_t const* head, uint32_t* csr);
 // trim.cu: k_trim_first's grid = the number of per-block pivot candidates
 unsigned pivot_candidates(uint32_t n);
 // mlp.cu: the learned pivot model (KSPN_MLP_PARAMS FP32 parameters)

@@ -105,3 +105,54 @@ def rgg(ctx: Context, n: int, seed: int, mean_undirected_degree: float = 8.0, de
     dst = torch.empty(max(m_raw, 1), dtype=torch.int32, device=device)
     ctx.gen_rgg(n, seed, g, r2, src, dst, m_raw)
     return from_edges(ctx, n, src[:m_raw], dst[:m_raw], device)
+
+
+@dataclass
+class DeviceBatch:
+    """Many graphs in one concatenated CSR/CSC (heads: global edge
+    positions, rows: local ids), as kspn_scc_batched takes them."""
+    count: int
+    n: int  # total vertices
+    m: int  # total edges
+    vtx_off: "torch.Tensor"  # int64[count+1]
+    fwh: "torch.Tensor"
+    fwc: "torch.Tensor"
+    bwh: "torch.Tensor"
+    bwc: "torch.Tensor"
+    sizes: np.ndarray  # vertices per graph
+
+    def graph(self, g: int):
+        """Graph g as host CSR/CSC with local offsets (for checking)."""
+        vo = np.concatenate([[0], np.cumsum(self.sizes, dtype=np.uint64)])
+        a, b = int(vo[g]), int(vo[g + 1])
+        fwh = self.fwh[a: b + 1].cpu().numpy().view(np.uint64)
+        bwh = self.bwh[a: b + 1].cpu().numpy().view(np.uint64)
+        fwc = self.fwc[int(fwh[0]): int(fwh[-1])].cpu().numpy().view(np.uint32)
+        bwc = self.bwc[int(bwh[0]): int(bwh[-1])].cpu().numpy().view(np.uint32)
+        return b - a, fwh - fwh[0], fwc, bwh - bwh[0], bwc
+
+
+def batch(ctx: Context, count: int = 4096, seed: int = 5, log2_min: int = 8, log2_max: int = 18, deg_min: float = 0.8, deg_max: float = 6.0,
+          device="cuda") -> DeviceBatch:
+    """The uneven G(n, m) mix: graph i has round(2^U[log2_min, log2_max])
+    vertices and round(n * U[deg_min, deg_max]) edge draws (self-loops and
+    duplicates removed); all on the device."""
+    import torch
+
+    from . import batch_shape
+
+    sizes, draws = batch_shape(count, seed, log2_min, log2_max, deg_min, deg_max)
+    vtx_off = np.concatenate([[0], np.cumsum(sizes, dtype=np.uint64)]).astype(np.uint64)
+    draw_off = np.concatenate([[0], np.cumsum(draws, dtype=np.uint64)]).astype(np.uint64)
+    N, D = int(vtx_off[-1]), int(draw_off[-1])
+    d_vo = torch.from_numpy(vtx_off.view(np.int64).copy()).to(device)
+    d_do = torch.from_numpy(draw_off.view(np.int64).copy()).to(device)
+    src = torch.empty(max(D, 1), dtype=torch.int32, device=device)
+    dst = torch.empty(max(D, 1), dtype=torch.int32, device=device)
+    torch.cuda.synchronize()
+    ctx.gen_batch(count, seed, d_vo, d_do, src, dst)
+    G = from_edges(ctx, N, src[:D], dst[:D], device)
+    del src, dst
+    ctx.batch_localize(count, N, d_vo, G.fwh, G.fwc)
+    ctx.batch_localize(count, N, d_vo, G.bwh, G.bwc)
+    return DeviceBatch(count, N, G.m, d_vo, G.fwh, G.fwc, G.bwh, G.bwc, sizes)
