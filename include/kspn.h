@@ -329,8 +329,9 @@ int kspn_mlp_adam(kspn_context* ctx, float* d_params, const float* d_grad, float
  * global edge positions, rows hold LOCAL ids (0 .. n_g - 1).  Output:
  * scc_id[vtx_off[g] + v] = the local id of the smallest member of v's SCC.
  * Graphs of at most 512 vertices and 2048 edges are decomposed by one warp
- * each (Tarjan in shared memory), larger ones by one block each (trim-1,
- * FW-BW rounds, Tarjan of the remainder), all in one captured CUDA graph
+ * each (Tarjan in shared memory), larger ones by one block or, from
+ * n + m >= cluster_min, one thread-block cluster each (trim-1, FW-BW
+ * rounds, Tarjan of the remainder), all in one captured CUDA graph
  * that later calls with the same arrays and settings replay.  Device
  * pointers; the context's stream; synchronous.
  */
@@ -338,7 +339,11 @@ typedef struct kspn_batch_options {
     uint32_t max_rounds;   /* FW-BW rounds per large graph before one thread's Tarjan finishes it (0: 64) */
     uint32_t rem_tarjan;   /* a large graph's remainder of at most this many vertices goes to the
                               shared-memory Tarjan (0: 512, the most it holds) */
-    uint32_t reserved[6];
+    uint32_t cluster_size; /* blocks of the thread-block cluster a large graph gets (1..8; 0: 1, a block) */
+    uint32_t reserved0;
+    uint64_t cluster_min;  /* with cluster_size > 1: n + m from which a graph gets a cluster
+                              instead of one block (0: 2^16) */
+    uint32_t reserved[2];
 } kspn_batch_options;
 
 typedef struct kspn_batch_stats {
@@ -349,7 +354,9 @@ typedef struct kspn_batch_stats {
     uint32_t tarjan_serial; /* remainders finished by one thread (round cap) */
     uint32_t trim_levels;   /* trim push levels over all large graphs */
     float    ms;            /* device time of the call (CUDA events) */
-    uint32_t reserved[9];
+    uint32_t graphs_cluster; /* of the large ones: decomposed by a cluster of blocks */
+    uint32_t cluster_size;
+    uint32_t reserved[7];
 } kspn_batch_stats;
 
 void kspn_batch_options_default(kspn_batch_options* opt);
@@ -358,6 +365,41 @@ int  kspn_scc_batched(kspn_context* ctx, uint32_t count, uint64_t n_total,
                       const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
                       const uint64_t* d_bw_head, const uint32_t* d_bw_csr,
                       uint32_t* d_scc_id, const kspn_batch_options* opt, kspn_batch_stats* stats);
+
+/* ---------------------------------------------------------------- autotuner */
+/*
+ * Picks the settings of a path by timing candidates on the caller's own
+ * input (CUDA events, `reps` timed runs after one warm-up, the minimum
+ * counts): coordinate descent from *base, one setting at a time, a
+ * candidate kept when it is at least 2% faster.  Every candidate must give
+ * the same ids as the first run (checked on the device; a mismatch is
+ * KSPN_ERR_INTERNAL).  d_scc_id receives the ids.  No reference
+ * counterpart: the reference's settings are compile-time constants.
+ *  - kspn_autotune: FAST pipeline -- bu_enter_div, bu_leave_div (the
+ *    top-down / bottom-up switch points), trim2 on/off, learned_pivot on/off
+ *    (when the context holds a model);
+ *  - kspn_autotune_batched: cluster_size / cluster_min (which graphs get a
+ *    block or a thread-block cluster), rem_tarjan (FW-BW -> Tarjan switch
+ *    point), max_rounds.
+ */
+typedef struct kspn_tune_report {
+    uint32_t candidates;   /* settings timed */
+    float    default_ms;   /* the base settings */
+    float    best_ms;      /* the settings returned (<= default_ms) */
+    uint32_t reserved[5];
+} kspn_tune_report;
+
+int kspn_autotune(kspn_context* ctx, uint32_t n, uint64_t m,
+                  const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
+                  const uint64_t* d_bw_head, const uint32_t* d_bw_csr,
+                  uint32_t* d_scc_id, const kspn_options* base, uint32_t reps,
+                  kspn_options* best, kspn_tune_report* report);
+int kspn_autotune_batched(kspn_context* ctx, uint32_t count, uint64_t n_total,
+                          const uint64_t* d_vtx_off,
+                          const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
+                          const uint64_t* d_bw_head, const uint32_t* d_bw_csr,
+                          uint32_t* d_scc_id, const kspn_batch_options* base, uint32_t reps,
+                          kspn_batch_options* best, kspn_tune_report* report);
 
 /* The batch mix of uneven G(n,m) graphs (host, deterministic): graph i has
  * n_i = round(2^U[log2_min, log2_max]) vertices and round(n_i * U[deg_min,

@@ -192,19 +192,27 @@ SIGNATURES = {
     "kspn_batch_shape": (None, [_u32, _u64, _u32, _u32, C.c_float, C.c_float, _P, _P]),
     "kspn_gen_batch": (_i32, [_P, _u32, _u64, _P, _P, _P, _P]),
     "kspn_batch_localize": (_i32, [_P, _u32, _u64, _P, _P, _P]),
+    "kspn_autotune": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _u32, _P, _P]),
+    "kspn_autotune_batched": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P, _u32, _P, _P]),
 }
+
+
+class TuneReport(C.Structure):
+    """kspn_tune_report (include/kspn.h)."""
+    _fields_ = [("candidates", C.c_uint32), ("default_ms", C.c_float), ("best_ms", C.c_float), ("reserved", C.c_uint32 * 5)]
 
 
 class BatchOptions(C.Structure):
     """kspn_batch_options (include/kspn.h)."""
-    _fields_ = [("max_rounds", C.c_uint32), ("rem_tarjan", C.c_uint32), ("reserved", C.c_uint32 * 6)]
+    _fields_ = [("max_rounds", C.c_uint32), ("rem_tarjan", C.c_uint32), ("cluster_size", C.c_uint32), ("reserved0", C.c_uint32),
+                ("cluster_min", C.c_uint64), ("reserved", C.c_uint32 * 2)]
 
 
 class BatchStats(C.Structure):
     """kspn_batch_stats (include/kspn.h)."""
     _fields_ = [("graphs_small", C.c_uint32), ("graphs_large", C.c_uint32), ("fwbw_rounds", C.c_uint32),
                 ("tarjan_smem", C.c_uint32), ("tarjan_serial", C.c_uint32), ("trim_levels", C.c_uint32),
-                ("ms", C.c_float), ("reserved", C.c_uint32 * 9)]
+                ("ms", C.c_float), ("graphs_cluster", C.c_uint32), ("cluster_size", C.c_uint32), ("reserved", C.c_uint32 * 7)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -429,6 +437,20 @@ class Context:
         self._check(lib().kspn_scc_batched(self.h, count, n_total, _ptr(vtx_off), _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc), _ptr(out),
                                            C.byref(options) if options is not None else None, C.byref(st)), "scc_batched")
         return st
+
+    def autotune(self, n, m, fwh, fwc, bwh, bwc, out, base: "Options | None" = None, reps: int = 3):
+        """(best Options, TuneReport) for this graph (FAST pipeline settings)."""
+        best, rep = Options(), TuneReport()
+        self._check(lib().kspn_autotune(self.h, n, m, _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc), _ptr(out),
+                                        C.byref(base) if base is not None else None, reps, C.byref(best), C.byref(rep)), "autotune")
+        return best, rep
+
+    def autotune_batched(self, count, n_total, vtx_off, fwh, fwc, bwh, bwc, out, base: "BatchOptions | None" = None, reps: int = 3):
+        """(best BatchOptions, TuneReport) for this batch."""
+        best, rep = BatchOptions(), TuneReport()
+        self._check(lib().kspn_autotune_batched(self.h, count, n_total, _ptr(vtx_off), _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc), _ptr(out),
+                                                C.byref(base) if base is not None else None, reps, C.byref(best), C.byref(rep)), "autotune_batched")
+        return best, rep
 
     def gen_batch(self, count, seed, vtx_off, draw_off, src, dst):
         self._check(lib().kspn_gen_batch(self.h, count, seed, _ptr(vtx_off), _ptr(draw_off), _ptr(src), _ptr(dst)), "gen_batch")

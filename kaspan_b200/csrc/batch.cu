@@ -17,7 +17,9 @@
 // overlap):
 //  * k_batch_small: one warp per small graph builds its CSR in shared
 //    memory and runs the explicit-stack Tarjan of tarjan_smem.cuh;
-//  * k_batch_big: one block per large graph, claimed from the queue:
+//  * k_batch_group: one group per larger graph, claimed from a queue -- a
+//    thread-block cluster (up to 8 blocks, distributed shared memory, the
+//    cluster barrier) for graphs of n + m >= cluster_min, one block below:
 //    init (degrees, in/out = 0 decided), then rounds of {trim-1 push
 //    levels, FW-BW from the largest live in*out (SCC named by its smallest
 //    member, its members seed the next trim)} until the remainder has at
@@ -28,12 +30,15 @@
 #include "prim.cuh"
 #include "tarjan_smem.cuh"
 
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
+
 namespace kspn {
 
 namespace {
 
 constexpr int      BT_THREADS = 512;
-constexpr int      BT_WARPS   = BT_THREADS / 32;
 constexpr int      BS_WARPS   = 4; // warps per block of k_batch_small
 constexpr uint32_t BT_NONE    = 0xFFFFFFFFu;
 
@@ -56,9 +61,10 @@ struct bt_args
   uint32_t*       q1;
   uint32_t*       q2;
   uint64_t*       pos;   // N: serial Tarjan's edge cursors
-  uint32_t const* order; // graphs sorted: large ones first (n_big of them), then the small ones
-  uint32_t*       ctr;   // [0] large claimed, [1] small claimed, [2] n_big, [3] n_small, [4] err,
-                         // [5] FW-BW rounds, [6] shared-memory Tarjans, [7] serial Tarjans, [8] trim levels
+  uint32_t const* order; // graphs sorted: large, medium, small; largest first inside a class
+  uint32_t*       ctr;   // [0] large claimed, [1] small claimed, [2] n_large, [3] n_small, [4] err,
+                         // [5] FW-BW rounds, [6] shared-memory Tarjans, [7] serial Tarjans, [8] trim levels,
+                         // [9] n_medium, [10] medium claimed
   uint32_t        max_rounds; // FW-BW rounds per graph before the serial Tarjan
   uint32_t        rem_tarjan; // remainder size that goes to the shared-memory Tarjan (<= RS_MAXV)
 };
@@ -70,20 +76,23 @@ bt_get(uint32_t const* bm, uint32_t v)
 }
 
 // ---------------------------------------------------------------- plan
-// Per graph: class key for the sort (large: ~(n + m) so the largest sort
-// first; small: all ones, last) and its bitmap word count.
+// Per graph: its class -- large (n + m >= cluster_min: a cluster), medium
+// (a block), small (at most RS_MAXV vertices and RS_MAXE edges: a warp) --
+// as the sort key's top bits, ~(n + m) below them (largest first inside a
+// class), and its bitmap word count.  Class counts: ctr[2] large, ctr[9]
+// medium, ctr[3] small.
 __global__ void
-k_bt_classify(uint32_t G, uint64_t const* __restrict__ vtx_off, uint64_t const* __restrict__ fh, uint32_t* keys, uint32_t* vals, uint32_t* words, uint32_t* ctr)
+k_bt_classify(uint32_t G, uint64_t const* __restrict__ vtx_off, uint64_t const* __restrict__ fh, uint64_t cluster_min, uint32_t* keys, uint32_t* vals, uint32_t* words, uint32_t* ctr)
 {
   for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
     uint64_t const vo = vtx_off[g], n = vtx_off[g + 1] - vo;
     uint64_t const m  = fh[vo + n] - fh[vo];
-    bool const     small = n <= RS_MAXV && m <= RS_MAXE;
     uint64_t const size  = n + m;
-    keys[g]  = small ? 0xFFFFFFFFu : 0xFFFFFFFEu - static_cast<uint32_t>(size < 0xFFFFFFFEull ? size : 0xFFFFFFFEull);
+    uint32_t const cls   = n <= RS_MAXV && m <= RS_MAXE ? 2u : (size >= cluster_min ? 0u : 1u);
+    keys[g]  = (cls << 30) | (0x3FFFFFFFu - static_cast<uint32_t>(size < 0x3FFFFFFFull ? size : 0x3FFFFFFFull));
     vals[g]  = g;
     words[g] = static_cast<uint32_t>((n + 31) / 32);
-    atomicAdd(ctr + (small ? 3 : 2), 1u);
+    atomicAdd(ctr + (cls == 0 ? 2 : cls == 1 ? 9 : 3), 1u);
   }
 }
 
@@ -100,7 +109,7 @@ k_batch_small(bt_args a)
   extern __shared__ __align__(16) unsigned char bs_smem[];
   unsigned const lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
   rs_piece&      p    = reinterpret_cast<rs_piece*>(bs_smem)[wid];
-  uint32_t const nb   = __ldcg(a.ctr + 2), ns = __ldcg(a.ctr + 3);
+  uint32_t const nb   = __ldcg(a.ctr + 2) + __ldcg(a.ctr + 9), ns = __ldcg(a.ctr + 3);
   for (;;) {
     uint32_t i = 0;
     if (lane == 0) i = atomicAdd(a.ctr + 1, 1u);
@@ -123,15 +132,47 @@ k_batch_small(bt_args a)
   }
 }
 
-// ---------------------------------------------------------------- large graphs
+// ---------------------------------------------------------------- larger graphs
+// A graph goes to a GROUP: one block (medium graphs) or a thread-block
+// cluster of up to 8 blocks on different SMs (large graphs).  The group's
+// counters live in the shared memory of its rank-0 block and the others
+// reach them as distributed shared memory; group barriers are the
+// hardware cluster barrier (release / acquire at cluster scope); data other
+// blocks of the group write is read through L2.
 struct bt_smem
 {
-  uint32_t           g, qn, rem, cnt, minid, lo, hi, flag;
+  uint32_t           g, rem, cnt, minid, lo, hi, flag, pad;
   unsigned long long best;
-  unsigned long long wbest[BT_WARPS];
 };
 
-// One graph's view for the block.
+struct bt_group
+{
+  cg::cluster_group cl;
+  bt_smem*          S;   // rank 0's counters (local or distributed shared memory)
+  uint32_t          gt;  // thread index in the group
+  uint32_t          GT;  // threads in the group
+  bool              one; // a single block: block barriers suffice
+  __device__ __forceinline__ void sync() const
+  {
+    if (one) __syncthreads();
+    else cl.sync();
+  }
+  __device__ __forceinline__ bool leader() const { return gt == 0; }
+};
+
+// warp-aggregated slot from a group counter (lanes that may be inactive)
+__device__ __forceinline__ uint32_t
+bt_slot(uint32_t* counter)
+{
+  unsigned const mask = __activemask();
+  unsigned const lane = threadIdx.x & 31u, leader = __ffs(mask) - 1;
+  uint32_t       base = 0;
+  if (lane == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask)));
+  base = __shfl_sync(mask, base, leader);
+  return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+// One graph's view for the group.
 struct bt_graph
 {
   uint64_t        vo;
@@ -153,9 +194,10 @@ struct bt_graph
 // lowers its undecided out-neighbours' live in-degree and in-neighbours'
 // live out-degree; a count reaching 0 decides that neighbour (id = itself)
 // and queues it.  Queues alternate between the two buffers that are not
-// qin.  Returns the vertices decided.
+// qin.  A thread's row entries are loaded four at a time before their
+// probes.  Returns the vertices decided.
 __device__ uint32_t
-bt_trim(bt_args const& a, bt_graph const& G, bt_smem& s, uint32_t* qin, uint32_t qn)
+bt_trim(bt_args const& a, bt_graph const& G, bt_group const& g, uint32_t* qin, uint32_t qn)
 {
   uint32_t  total = 0;
   uint32_t* bufs[2];
@@ -165,36 +207,41 @@ bt_trim(bt_args const& a, bt_graph const& G, bt_smem& s, uint32_t* qin, uint32_t
   uint32_t levels = 0;
   for (uint32_t lvl = 0; qn > 0; ++lvl) {
     if (lvl > G.n + 1) {
-      if (threadIdx.x == 0) atomicExch(a.ctr + 4, 1u);
+      if (g.leader()) atomicExch(a.ctr + 4, 1u);
       break;
     }
     uint32_t* const qout = bufs[lvl & 1];
-    if (threadIdx.x == 0) s.cnt = 0;
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < qn; i += BT_THREADS) {
+    if (g.leader()) g.S->cnt = 0;
+    g.sync();
+    auto const hit = [&](uint32_t w, uint32_t* deg) {
+      if (bt_get(G.und, w) && atomicSub(deg + w, 1u) == 1u && bit_take(G.und, w)) {
+        G.ids[w]                 = w;
+        qout[bt_slot(&g.S->cnt)] = w;
+      }
+    };
+    for (uint32_t i = g.gt; i < qn; i += g.GT) {
       uint32_t const u = __ldcg(qin + i);
 #pragma unroll 1
       for (int dir = 0; dir < 2; ++dir) {
         uint64_t const* head = dir ? G.bh : G.fh;
         uint32_t const* adj  = dir ? a.bc : a.fc;
         uint32_t*       deg  = dir ? G.outdeg : G.indeg;
-        for (uint64_t e = head[u], end = head[u + 1]; e < end; ++e) {
-          uint32_t const w = adj[e];
-          if (bt_get(G.und, w) && atomicSub(deg + w, 1u) == 1u && bit_take(G.und, w)) {
-            G.ids[w]              = w;
-            qout[atomicAdd(&s.cnt, 1u)] = w;
-          }
+        uint64_t        e = head[u], end = head[u + 1];
+        for (; e + 4 <= end; e += 4) {
+          uint32_t const w0 = adj[e], w1 = adj[e + 1], w2 = adj[e + 2], w3 = adj[e + 3];
+          hit(w0, deg), hit(w1, deg), hit(w2, deg), hit(w3, deg);
         }
+        for (; e < end; ++e) hit(adj[e], deg);
       }
     }
-    __syncthreads();
-    qn = s.cnt;
+    g.sync();
+    qn = g.S->cnt;
     total += qn;
     qin = qout;
     ++levels;
-    __syncthreads();
+    g.sync();
   }
-  if (threadIdx.x == 0 && levels) atomicAdd(a.ctr + 8, levels);
+  if (g.leader() && levels) atomicAdd(a.ctr + 8, levels);
   return total;
 }
 
@@ -203,80 +250,74 @@ bt_trim(bt_args const& a, bt_graph const& G, bt_smem& s, uint32_t* qin, uint32_t
 // bits of `mark`; every reached vertex is appended to `list`.  Returns how
 // many were reached.
 __device__ uint32_t
-bt_reach(bt_args const& a, bt_graph const& G, bt_smem& s, uint64_t const* head, uint32_t const* adj, uint32_t const* cand, uint32_t* mark, uint32_t* list, uint32_t root)
+bt_reach(bt_args const& a, bt_graph const& G, bt_group const& g, uint64_t const* head, uint32_t const* adj, uint32_t const* cand, uint32_t* mark, uint32_t* list, uint32_t root)
 {
-  if (threadIdx.x == 0) {
+  if (g.leader()) {
     list[0] = root;
     atomicOr(mark + (root >> 5), 1u << (root & 31));
-    s.lo = 0;
-    s.hi = 1;
-    s.cnt = 1;
+    g.S->lo  = 0;
+    g.S->hi  = 1;
+    g.S->cnt = 1;
   }
-  __syncthreads();
+  g.sync();
   for (uint32_t lvl = 0;; ++lvl) {
-    uint32_t const lo = s.lo, hi = s.hi;
+    uint32_t const lo = g.S->lo, hi = g.S->hi;
     if (lo == hi) break;
     if (lvl > G.n + 1) {
-      if (threadIdx.x == 0) atomicExch(a.ctr + 4, 1u);
+      if (g.leader()) atomicExch(a.ctr + 4, 1u);
       break;
     }
-    for (uint32_t i = lo + threadIdx.x; i < hi; i += BT_THREADS) {
+    for (uint32_t i = lo + g.gt; i < hi; i += g.GT) {
       uint32_t const u = __ldcg(list + i);
       for (uint64_t e = head[u], end = head[u + 1]; e < end; ++e) {
         uint32_t const w = adj[e];
-        if ((cand ? bt_get(cand, w) : bt_get(G.und, w)) && bit_claim(mark, w)) list[atomicAdd(&s.cnt, 1u)] = w;
+        if ((cand ? bt_get(cand, w) : bt_get(G.und, w)) && bit_claim(mark, w)) list[bt_slot(&g.S->cnt)] = w;
       }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) s.lo = hi, s.hi = s.cnt;
-    __syncthreads();
+    g.sync();
+    if (g.leader()) g.S->lo = hi, g.S->hi = g.S->cnt;
+    g.sync();
   }
-  __syncthreads();
-  uint32_t const c = s.cnt;
-  __syncthreads();
+  uint32_t const c = g.S->cnt;
+  g.sync();
   return c;
 }
 
-// argmax over undecided v of live in * out (lowest id on ties) into s.best
-// as (prod << 32 | ~id) when prod < 2^32, else saturated
+// argmax over undecided v of live in * out (lowest id on ties), as
+// (saturated prod << 32 | ~id); BT_NONE when nothing is undecided
 __device__ uint32_t
-bt_pivot(bt_graph const& G, bt_smem& s)
+bt_pivot(bt_graph const& G, bt_group const& g)
 {
+  if (g.leader()) g.S->best = 0;
+  g.sync();
   unsigned long long best = 0;
-  for (uint32_t v = threadIdx.x; v < G.n; v += BT_THREADS) {
+  for (uint32_t v = g.gt; v < G.n; v += g.GT) {
     if (!bt_get(G.und, v)) continue;
-    uint64_t const     p   = static_cast<uint64_t>(__ldcg(G.indeg + v)) * __ldcg(G.outdeg + v);
-    unsigned long long key = (static_cast<unsigned long long>(p < 0xFFFFFFFFull ? p : 0xFFFFFFFFull) << 32) | (0xFFFFFFFFu - v);
-    best                   = key > best ? key : best;
+    uint64_t const           p   = static_cast<uint64_t>(__ldcg(G.indeg + v)) * __ldcg(G.outdeg + v);
+    unsigned long long const key = (static_cast<unsigned long long>(p < 0xFFFFFFFFull ? p : 0xFFFFFFFFull) << 32) | (0xFFFFFFFFu - v);
+    best                         = key > best ? key : best;
   }
 #pragma unroll
   for (int sh = 16; sh; sh >>= 1) {
     unsigned long long const o = __shfl_xor_sync(0xFFFFFFFFu, best, sh);
     best                       = o > best ? o : best;
   }
-  if ((threadIdx.x & 31) == 0) s.wbest[threadIdx.x >> 5] = best;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned long long b = 0;
-    for (int w = 0; w < BT_WARPS; ++w) b = s.wbest[w] > b ? s.wbest[w] : b;
-    s.best = b;
-  }
-  __syncthreads();
-  unsigned long long const b = s.best;
-  __syncthreads();
+  if ((threadIdx.x & 31) == 0 && best) atomicMax(&g.S->best, best);
+  g.sync();
+  unsigned long long const b = g.S->best;
+  g.sync();
   return b ? 0xFFFFFFFFu - static_cast<uint32_t>(b & 0xFFFFFFFFu) : BT_NONE;
 }
 
 // The remaining (undecided) vertices of a graph in id order into the
-// piece, if there are at most RS_MAXV of them with at most RS_MAXE edges
-// among them; warp 0 then runs Tarjan and writes ids.  Returns false (and
-// changes nothing) when they do not fit.
+// piece (rank 0's warp 0), if there are at most RS_MAXV of them with at
+// most RS_MAXE edges among them; then Tarjan and the ids.  Returns false
+// (and changes nothing) when they do not fit.
 __device__ bool
-bt_tarjan_smem(bt_args const& a, bt_graph const& G, bt_smem& s, rs_piece& p)
+bt_tarjan_smem(bt_args const& a, bt_graph const& G, bt_group const& g, rs_piece& p)
 {
   unsigned const lane = threadIdx.x & 31u;
-  if (threadIdx.x < 32) {
-    // ordered compaction of the und words (warp 0)
+  if (g.gt < 32) {
     uint32_t k = 0;
     for (uint32_t wb = 0; wb < G.words; wb += 32) {
       uint32_t const w    = wb + lane;
@@ -292,12 +333,12 @@ bt_tarjan_smem(bt_args const& a, bt_graph const& G, bt_smem& s, rs_piece& p)
       for (; word; word &= word - 1, ++j)
         if (j < RS_MAXV) p.vid[j] = w * 32 + __ffs(word) - 1;
       k += __shfl_sync(0xFFFFFFFFu, incl, 31);
+      if (k > RS_MAXV) break;
     }
     __syncwarp();
-    bool fits = k <= RS_MAXV;
-    // internal out-edges per listed vertex
-    uint32_t const per = (k + 31) / 32;
-    uint32_t       cnt = 0;
+    bool           fits = k <= RS_MAXV;
+    uint32_t const per  = (k + 31) / 32;
+    uint32_t       cnt  = 0;
     if (fits)
       for (uint32_t i = lane * per; i < k && i < lane * per + per; ++i) {
         uint32_t const v = p.vid[i];
@@ -313,7 +354,7 @@ bt_tarjan_smem(bt_args const& a, bt_graph const& G, bt_smem& s, rs_piece& p)
       if (lane >= static_cast<unsigned>(d)) incl += y;
     }
     uint32_t const total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-    fits             = fits && total <= RS_MAXE;
+    fits                 = fits && total <= RS_MAXE;
     if (fits) {
       uint32_t run = incl - cnt;
       for (uint32_t i = lane * per; i < k && i < lane * per + per; ++i) {
@@ -340,35 +381,34 @@ bt_tarjan_smem(bt_args const& a, bt_graph const& G, bt_smem& s, rs_piece& p)
       }
       if (lane == 0) atomicAdd(a.ctr + 6, 1u);
     }
-    if (lane == 0) s.flag = fits ? 1u : 0u;
+    if (lane == 0) g.S->flag = fits ? 1u : 0u;
   }
-  __syncthreads();
-  bool const ok = s.flag != 0;
-  __syncthreads();
+  g.sync();
+  bool const ok = g.S->flag != 0;
+  g.sync();
   return ok;
 }
 
 // One thread's iterative Tarjan (tarjan.hpp:20-136) over the undecided
 // sub-graph in global memory: index in indeg, low in outdeg, the SCC stack
 // in q0, the call stack's vertices in q1 and edge cursors in pos; on-stack
-// flags in vis_a.  The last resort after the round cap; bounded by n + m
-// steps.
+// flags in vis_a.  The last resort after the round cap; n + m steps.
 __device__ void
-bt_tarjan_serial(bt_args const& a, bt_graph const& G, uint64_t* pos)
+bt_tarjan_serial(bt_args const& a, bt_graph const& G, bt_group const& g, uint64_t* pos)
 {
-  __syncthreads();
-  for (uint32_t v = threadIdx.x; v < G.n; v += BT_THREADS) G.indeg[v] = BT_NONE;
-  for (uint32_t w = threadIdx.x; w < G.words; w += BT_THREADS) G.va[w] = 0;
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  g.sync();
+  for (uint32_t v = g.gt; v < G.n; v += g.GT) G.indeg[v] = BT_NONE;
+  for (uint32_t w = g.gt; w < G.words; w += g.GT) G.va[w] = 0;
+  g.sync();
+  if (g.leader()) {
     atomicAdd(a.ctr + 7, 1u);
     uint32_t idx = 0, sp = 0, cp = 0;
     for (uint32_t r = 0; r < G.n; ++r) {
-      if (!bt_get(G.und, r) || G.indeg[r] != BT_NONE) continue;
+      if (!bt_get(G.und, r) || __ldcg(G.indeg + r) != BT_NONE) continue;
       G.indeg[r] = G.outdeg[r] = idx++;
-      G.q0[sp++]             = r;
+      G.q0[sp++]               = r;
       G.va[r >> 5] |= 1u << (r & 31);
-      G.q1[cp] = r;
+      G.q1[cp]  = r;
       pos[cp++] = G.fh[r];
       while (cp > 0) {
         uint32_t const v = G.q1[cp - 1];
@@ -379,7 +419,7 @@ bt_tarjan_serial(bt_args const& a, bt_graph const& G, uint64_t* pos)
           if (!bt_get(G.und, w)) continue;
           if (G.indeg[w] == BT_NONE) {
             G.indeg[w] = G.outdeg[w] = idx++;
-            G.q0[sp++]             = w;
+            G.q0[sp++]               = w;
             G.va[w >> 5] |= 1u << (w & 31);
             G.q1[cp]  = w;
             pos[cp++] = G.fh[w];
@@ -408,21 +448,21 @@ bt_tarjan_serial(bt_args const& a, bt_graph const& G, uint64_t* pos)
       }
     }
   }
-  __syncthreads();
+  g.sync();
 }
 
 __device__ void
-bt_solve(bt_args const& a, uint32_t g, bt_smem& s, rs_piece& piece)
+bt_solve(bt_args const& a, uint32_t gi, bt_group const& g, rs_piece& piece)
 {
   bt_graph G;
-  G.vo     = a.vtx_off[g];
-  G.n      = static_cast<uint32_t>(a.vtx_off[g + 1] - G.vo);
+  G.vo     = a.vtx_off[gi];
+  G.n      = static_cast<uint32_t>(a.vtx_off[gi + 1] - G.vo);
   G.words  = (G.n + 31) / 32;
   G.fh     = a.fh + G.vo;
   G.bh     = a.bh + G.vo;
-  G.und    = a.und + a.word_off[g];
-  G.va     = a.vis_a + a.word_off[g];
-  G.vb     = a.vis_b + a.word_off[g];
+  G.und    = a.und + a.word_off[gi];
+  G.va     = a.vis_a + a.word_off[gi];
+  G.vb     = a.vis_b + a.word_off[gi];
   G.indeg  = a.indeg + G.vo;
   G.outdeg = a.outdeg + G.vo;
   G.ids    = a.scc_id + G.vo;
@@ -432,14 +472,14 @@ bt_solve(bt_args const& a, uint32_t g, bt_smem& s, rs_piece& piece)
   uint64_t* const pos = a.pos + G.vo;
 
   // init: all undecided, live degrees = raw degrees, in/out = 0 decided
-  for (uint32_t w = threadIdx.x; w < G.words; w += BT_THREADS) {
+  for (uint32_t w = g.gt; w < G.words; w += g.GT) {
     uint32_t const tail = G.n - w * 32;
     G.und[w]            = tail >= 32 ? 0xFFFFFFFFu : (1u << tail) - 1u;
     G.va[w] = G.vb[w] = 0;
   }
-  if (threadIdx.x == 0) s.cnt = 0;
-  __syncthreads();
-  for (uint32_t v = threadIdx.x; v < G.n; v += BT_THREADS) {
+  if (g.leader()) g.S->cnt = 0;
+  g.sync();
+  for (uint32_t v = g.gt; v < G.n; v += g.GT) {
     uint32_t const o = static_cast<uint32_t>(G.fh[v + 1] - G.fh[v]);
     uint32_t const i = static_cast<uint32_t>(G.bh[v + 1] - G.bh[v]);
     G.outdeg[v]      = o;
@@ -447,75 +487,87 @@ bt_solve(bt_args const& a, uint32_t g, bt_smem& s, rs_piece& piece)
     if (o == 0 || i == 0) {
       G.ids[v] = v;
       atomicAnd(G.und + (v >> 5), ~(1u << (v & 31)));
-      G.q0[atomicAdd(&s.cnt, 1u)] = v;
+      G.q0[bt_slot(&g.S->cnt)] = v;
     } else G.ids[v] = UNDECIDED;
   }
-  __syncthreads();
-  uint32_t qn  = s.cnt;
-  uint32_t rem = G.n - qn;
+  g.sync();
+  uint32_t  qn   = g.S->cnt;
+  uint32_t  rem  = G.n - qn;
   uint32_t* seed = G.q0;
-  __syncthreads();
+  g.sync();
   for (uint32_t round = 0;; ++round) {
-    rem -= bt_trim(a, G, s, seed, qn);
+    rem -= bt_trim(a, G, g, seed, qn);
     if (rem == 0) break;
-    if (rem <= a.rem_tarjan && bt_tarjan_smem(a, G, s, piece)) break;
+    if (rem <= a.rem_tarjan && bt_tarjan_smem(a, G, g, piece)) break;
     if (round >= a.max_rounds) {
-      bt_tarjan_serial(a, G, pos);
+      bt_tarjan_serial(a, G, g, pos);
       break;
     }
     // FW-BW from the largest live in * out
-    uint32_t const p = bt_pivot(G, s);
+    uint32_t const p = bt_pivot(G, g);
     if (p == BT_NONE) {
-      if (threadIdx.x == 0) atomicExch(a.ctr + 4, 1u);
+      if (g.leader()) atomicExch(a.ctr + 4, 1u);
       break;
     }
-    uint32_t const nf = bt_reach(a, G, s, G.fh, a.fc, nullptr, G.va, G.q1, p);
-    uint32_t const nb = bt_reach(a, G, s, G.bh, a.bc, G.va, G.vb, G.q2, p);
+    uint32_t const nf = bt_reach(a, G, g, G.fh, a.fc, nullptr, G.va, G.q1, p);
+    uint32_t const nb = bt_reach(a, G, g, G.bh, a.bc, G.va, G.vb, G.q2, p);
     // the SCC (q2): smallest member, ids, und; vis_a cleared through q1
+    if (g.leader()) g.S->minid = 0xFFFFFFFFu;
+    g.sync();
     uint32_t mn = 0xFFFFFFFFu;
-    for (uint32_t i = threadIdx.x; i < nb; i += BT_THREADS) mn = min(mn, __ldcg(G.q2 + i));
+    for (uint32_t i = g.gt; i < nb; i += g.GT) mn = min(mn, __ldcg(G.q2 + i));
     mn = __reduce_min_sync(0xFFFFFFFFu, mn);
-    if (threadIdx.x == 0) s.minid = 0xFFFFFFFFu;
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) atomicMin(&s.minid, mn);
-    __syncthreads();
-    uint32_t const id = s.minid;
-    for (uint32_t i = threadIdx.x; i < nb; i += BT_THREADS) {
+    if ((threadIdx.x & 31) == 0 && mn != 0xFFFFFFFFu) atomicMin(&g.S->minid, mn);
+    g.sync();
+    uint32_t const id = g.S->minid;
+    for (uint32_t i = g.gt; i < nb; i += g.GT) {
       uint32_t const v = __ldcg(G.q2 + i);
       G.ids[v]         = id;
       atomicAnd(G.und + (v >> 5), ~(1u << (v & 31)));
       atomicAnd(G.vb + (v >> 5), ~(1u << (v & 31)));
     }
-    for (uint32_t i = threadIdx.x; i < nf; i += BT_THREADS) {
+    for (uint32_t i = g.gt; i < nf; i += g.GT) {
       uint32_t const v = __ldcg(G.q1 + i);
       atomicAnd(G.va + (v >> 5), ~(1u << (v & 31)));
     }
-    if (threadIdx.x == 0) atomicAdd(a.ctr + 5, 1u);
-    __syncthreads();
+    if (g.leader()) atomicAdd(a.ctr + 5, 1u);
+    g.sync();
     rem -= nb;
     if (rem == 0) break;
     // the SCC's members seed the next trim
     seed = G.q2;
     qn   = nb;
   }
-  __syncthreads();
+  g.sync();
 }
 
-__global__ void __launch_bounds__(BT_THREADS)
-k_batch_big(bt_args a)
+// Persistent groups over one queue of graphs (a.order[first, first + *count)),
+// claimed through *claim.  Launched with a cluster dimension (or none: a
+// group of one block).
+__global__ void __launch_bounds__(BT_THREADS, 3) // 3 blocks per SM: the path is latency-bound, graphs in flight count most
+k_batch_group(bt_args a, uint32_t first_slot, uint32_t count_slot, uint32_t claim_slot)
 {
   extern __shared__ __align__(16) unsigned char bt_dyn[];
-  rs_piece&         piece = *reinterpret_cast<rs_piece*>(bt_dyn);
+  rs_piece&          piece = *reinterpret_cast<rs_piece*>(bt_dyn);
   __shared__ bt_smem s;
-  uint32_t const     nb = __ldcg(a.ctr + 2);
+  bt_group           g{ cg::this_cluster(), nullptr, 0, 0, false };
+  uint32_t const     csize = g.cl.num_blocks();
+  g.one                    = csize == 1;
+  g.S                      = g.one ? &s : g.cl.map_shared_rank(&s, 0);
+  g.gt                     = g.cl.block_rank() * BT_THREADS + threadIdx.x;
+  g.GT                     = csize * BT_THREADS;
+  uint32_t const first     = first_slot == BT_NONE ? 0u : __ldcg(a.ctr + first_slot);
+  uint32_t const count     = __ldcg(a.ctr + count_slot);
+  g.sync(); // every block of the cluster has started (its shared memory exists)
   for (;;) {
-    if (threadIdx.x == 0) s.g = atomicAdd(a.ctr + 0, 1u);
-    __syncthreads();
-    uint32_t const i = s.g;
-    __syncthreads();
-    if (i >= nb) break;
-    bt_solve(a, a.order[i], s, piece);
+    if (g.leader()) g.S->g = atomicAdd(a.ctr + claim_slot, 1u);
+    g.sync();
+    uint32_t const i = g.S->g;
+    g.sync();
+    if (i >= count) break;
+    bt_solve(a, a.order[first + i], g, piece);
   }
+  g.sync(); // no block leaves while another may still reach its shared memory
 }
 
 } // namespace
@@ -558,7 +610,8 @@ struct batch_cache
   void const*     key[6] = {};
   uint32_t        G = 0;
   uint64_t        N = 0;
-  uint32_t        max_rounds = 0, rem_tarjan = 0, big_blocks = 0;
+  uint32_t        max_rounds = 0, rem_tarjan = 0, block_blocks = 0, cluster_size = 0, cluster_blocks = 0;
+  uint64_t        cluster_min = 0;
   cudaStream_t    cap_stream = nullptr;
 };
 
@@ -620,8 +673,8 @@ enqueue_batch(kspn_context* ctx, batch_cache& c, bt_args const& a0)
   batch_plan&        p = c.plan;
   uint32_t const     G = c.G;
   KSPN_CUDA(cudaMemsetAsync(p.ctr, 0, 32 * sizeof(uint32_t), s));
-  unsigned const cg = div_up(G, 256);
-  k_bt_classify<<<cg < 1 ? 1 : cg, 256, 0, s>>>(G, a0.vtx_off, a0.fh, p.keys, p.order, p.words, p.ctr);
+  unsigned const cgrid = div_up(G, 256);
+  k_bt_classify<<<cgrid < 1 ? 1 : cgrid, 256, 0, s>>>(G, a0.vtx_off, a0.fh, c.cluster_min, p.keys, p.order, p.words, p.ctr);
   KSPN_CHECK_LAUNCH();
   exclusive_scan<uint64_t>(s, f_words{ p.words }, G, p.word_off, p.part64, nullptr);
   radix_sort_pairs(ctx, p.keys, p.order, p.kalt, p.valt, G, 0, 32, p.hist, p.part);
@@ -640,7 +693,23 @@ enqueue_batch(kspn_context* ctx, batch_cache& c, bt_args const& a0)
   a.ctr        = p.ctr;
   a.max_rounds = c.max_rounds;
   a.rem_tarjan = c.rem_tarjan;
-  k_batch_big<<<c.big_blocks, BT_THREADS, sizeof(rs_piece), s>>>(a);
+  // large graphs: clusters of c.cluster_size blocks; medium: single blocks
+  if (c.cluster_size > 1) {
+    cudaLaunchConfig_t   cfg{};
+    cudaLaunchAttribute  attr[1];
+    attr[0].id               = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = c.cluster_size;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim              = dim3(c.cluster_blocks);
+    cfg.blockDim             = dim3(BT_THREADS);
+    cfg.dynamicSmemBytes     = sizeof(rs_piece);
+    cfg.stream               = s;
+    cfg.attrs                = attr;
+    cfg.numAttrs             = 1;
+    KSPN_CUDA(cudaLaunchKernelEx(&cfg, k_batch_group, a, BT_NONE, 2u, 0u));
+  } else k_batch_group<<<c.block_blocks, BT_THREADS, sizeof(rs_piece), s>>>(a, BT_NONE, 2u, 0u);
+  k_batch_group<<<c.block_blocks, BT_THREADS, sizeof(rs_piece), s>>>(a, 2u, 9u, 10u);
   k_batch_small<<<148 * 4, BS_WARPS * 32, BS_WARPS * sizeof(rs_piece), s>>>(a);
   KSPN_CHECK_LAUNCH();
 }
@@ -655,11 +724,14 @@ scc_batched(kspn_context* ctx, uint32_t G, uint64_t N, uint64_t const* vtx_off, 
   uint32_t const rem = opt.rem_tarjan ? opt.rem_tarjan : RS_MAXV;
   if (rem > RS_MAXV) throw error{ KSPN_ERR_INVALID_ARGUMENT, "scc_batched: rem_tarjan > 512" };
   uint32_t const rounds = opt.max_rounds ? opt.max_rounds : 64;
+  uint32_t const csize  = opt.cluster_size ? opt.cluster_size : 1;
+  uint64_t const cmin   = csize == 1 ? ~0ull : (opt.cluster_min ? opt.cluster_min : (1ull << 16));
+  if (csize > 8) throw error{ KSPN_ERR_INVALID_ARGUMENT, "scc_batched: cluster_size > 8" };
   batch_cache*&  cp     = ctx->batch;
   if (!cp) cp = new batch_cache{};
   batch_cache&      c   = *cp;
   void const* const key[6] = { vtx_off, fh, fc, bh, bc, scc_id };
-  bool              same   = c.exec && c.G == G && c.N == N && c.max_rounds == rounds && c.rem_tarjan == rem;
+  bool              same   = c.exec && c.G == G && c.N == N && c.max_rounds == rounds && c.rem_tarjan == rem && c.cluster_size == csize && c.cluster_min == cmin;
   for (int i = 0; i < 6 && same; ++i) same = c.key[i] == key[i];
   if (!same) {
     if (c.exec) cudaGraphExecDestroy(c.exec), c.exec = nullptr;
@@ -685,13 +757,31 @@ scc_batched(kspn_context* ctx, uint32_t G, uint64_t N, uint64_t const* vtx_off, 
     carve_plan(c.plan, static_cast<char*>(base), G, N, &bytes);
     c.plan.base  = base;
     c.plan.bytes = keep;
-    c.G = G, c.N = N, c.max_rounds = rounds, c.rem_tarjan = rem;
+    c.G = G, c.N = N, c.max_rounds = rounds, c.rem_tarjan = rem, c.cluster_size = csize, c.cluster_min = cmin;
     for (int i = 0; i < 6; ++i) c.key[i] = key[i];
     int bps = 0, sms = 0;
     KSPN_CUDA(cudaFuncSetAttribute(k_batch_small, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(BS_WARPS * sizeof(rs_piece))));
-    KSPN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch_big, BT_THREADS, sizeof(rs_piece)));
+    KSPN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_batch_group, BT_THREADS, sizeof(rs_piece)));
     KSPN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
-    c.big_blocks = static_cast<uint32_t>(std::max(1, bps) * sms);
+    c.block_blocks = static_cast<uint32_t>(std::max(1, bps) * sms);
+    c.cluster_blocks = c.block_blocks;
+    if (csize > 1) {
+      cudaLaunchConfig_t  cfg{};
+      cudaLaunchAttribute attr[1];
+      attr[0].id               = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = csize;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.gridDim              = dim3(c.block_blocks / csize * csize);
+      cfg.blockDim             = dim3(BT_THREADS);
+      cfg.dynamicSmemBytes     = sizeof(rs_piece);
+      cfg.attrs                = attr;
+      cfg.numAttrs             = 1;
+      int clusters             = 0;
+      KSPN_CUDA(cudaOccupancyMaxActiveClusters(&clusters, k_batch_group, &cfg));
+      if (clusters < 1) throw error{ KSPN_ERR_CUDA, "scc_batched: no cluster of that size fits" };
+      c.cluster_blocks = static_cast<uint32_t>(clusters) * csize;
+    }
     bt_args a{};
     a.G       = G;
     a.vtx_off = vtx_off;
@@ -727,7 +817,9 @@ scc_batched(kspn_context* ctx, uint32_t G, uint64_t N, uint64_t const* vtx_off, 
   if (h[4]) throw error{ KSPN_ERR_TIMEOUT, "scc_batched: a level or round bound was reached" };
   if (st) {
     st->graphs_small     = h[3];
-    st->graphs_large     = h[2];
+    st->graphs_large     = h[2] + h[9];
+    st->graphs_cluster   = h[2];
+    st->cluster_size     = csize;
     st->fwbw_rounds      = h[5];
     st->tarjan_smem      = h[6];
     st->tarjan_serial    = h[7];

@@ -13,6 +13,9 @@
 //             Same partition (every phase only decides whole SCCs).
 #include "kspn_internal.cuh"
 
+#include <functional>
+#include <vector>
+
 #include "prim.cuh"
 
 #include <algorithm>
@@ -496,6 +499,81 @@ clear_bitset_tail(kspn_context* ctx, uint64_t* bits, uint32_t n)
 
 using namespace kspn;
 
+namespace kspn {
+namespace {
+
+// ids differing from the first run's (autotuner check)
+__global__ void
+k_tune_diff(uint64_t n, uint32_t const* __restrict__ a, uint32_t const* __restrict__ b, uint32_t* diff)
+{
+  uint32_t d = 0;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) d += a[i] != b[i];
+  if (d) atomicAdd(diff, d);
+}
+
+// Coordinate descent over `axes` (each a list of candidate setters on a
+// copy of the current best); run(T) times one candidate and returns its ms.
+template<typename T, typename Run>
+T
+tune(T base, std::vector<std::vector<std::function<void(T&)>>> const& axes, Run&& run, kspn_tune_report* rep)
+{
+  T     cur    = base;
+  float t_cur  = run(cur);
+  float t_base = t_cur;
+  uint32_t cand = 1;
+  for (auto const& axis : axes)
+    for (auto const& set : axis) {
+      T c = cur;
+      set(c);
+      if (std::memcmp(&c, &cur, sizeof(T)) == 0) continue;
+      float const t = run(c);
+      ++cand;
+      if (t < 0.98f * t_cur) cur = c, t_cur = t;
+    }
+  if (rep) {
+    std::memset(rep, 0, sizeof(*rep));
+    rep->candidates = cand;
+    rep->default_ms = t_base;
+    rep->best_ms    = t_cur;
+  }
+  return cur;
+}
+
+// The first run's ids, kept in a context buffer; later runs compared with it.
+struct tune_check
+{
+  kspn_context* ctx;
+  uint64_t      n;
+  uint32_t*     ref  = nullptr;
+  bool          have = false;
+  void          take(uint32_t const* ids)
+  {
+    if (!n) return;
+    if (!have) {
+      ref = static_cast<uint32_t*>(context_buffer(ctx, BUF_GEN, n * sizeof(uint32_t)));
+      KSPN_CUDA(cudaMemcpyAsync(ref, ids, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, ctx->stream));
+      have = true;
+      return;
+    }
+    uint32_t* const diff = ctx->ws.ctr + CTR_ERR;
+    KSPN_CUDA(cudaMemsetAsync(diff, 0, sizeof(uint32_t), ctx->stream));
+    k_tune_diff<<<148 * 8, 256, 0, ctx->stream>>>(n, ref, ids, diff);
+    KSPN_CHECK_LAUNCH();
+    uint32_t h = 0;
+    KSPN_CUDA(cudaMemcpyAsync(&h, diff, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (h) throw error{ KSPN_ERR_INTERNAL, "autotune: a candidate gave different ids" };
+  }
+};
+
+} // namespace
+
+} // namespace kspn
+
+using kspn::tune;
+using kspn::tune_check;
+using kspn::k_tune_diff;
+
 extern "C" {
 
 int
@@ -911,6 +989,114 @@ kspn_scc_batched(kspn_context* ctx, uint32_t count, uint64_t n_total, const uint
     KSPN_CUDA(cudaEventRecord(ctx->ev[KSPN_PHASES + 1], ctx->stream));
     KSPN_CUDA(cudaEventSynchronize(ctx->ev[KSPN_PHASES + 1]));
     if (stats) KSPN_CUDA(cudaEventElapsedTime(&stats->ms, ctx->ev[KSPN_PHASES], ctx->ev[KSPN_PHASES + 1]));
+  });
+}
+
+int
+kspn_autotune(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_head, const uint32_t* d_fw_csr, const uint64_t* d_bw_head, const uint32_t* d_bw_csr, uint32_t* d_scc_id,
+              const kspn_options* base, uint32_t reps, kspn_options* best, kspn_tune_report* report)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(d_fw_head && (m == 0 || d_fw_csr) && (n == 0 || d_scc_id) && best, "null pointer");
+    require(n < UNDECIDED, "n must be below 2^32 - 1");
+    kspn_options o = options_or_default(base);
+    o.validate     = 0; // validated once below
+    bind_device(ctx);
+    graph_store  store;
+    dgraph const g = with_transpose(ctx, n, m, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr, store);
+    ensure_workspace(ctx, g.n, g.m); // counters of the validation and the check
+    if (base == nullptr || base->validate) validate(ctx, g);
+    uint32_t const R = reps ? reps : 3;
+    tune_check chk{ ctx, n };
+    auto run = [&](kspn_options const& c) {
+      run_pipeline(ctx, g, d_scc_id, c, nullptr); // warm-up
+      chk.take(d_scc_id);
+      float best_ms = 1e30f;
+      for (uint32_t r = 0; r < R; ++r) {
+        KSPN_CUDA(cudaEventRecord(ctx->ev[KSPN_PHASES], ctx->stream));
+        run_pipeline(ctx, g, d_scc_id, c, nullptr);
+        KSPN_CUDA(cudaEventRecord(ctx->ev[KSPN_PHASES + 1], ctx->stream));
+        KSPN_CUDA(cudaEventSynchronize(ctx->ev[KSPN_PHASES + 1]));
+        float ms = 0;
+        KSPN_CUDA(cudaEventElapsedTime(&ms, ctx->ev[KSPN_PHASES], ctx->ev[KSPN_PHASES + 1]));
+        best_ms = std::min(best_ms, ms);
+      }
+      return best_ms;
+    };
+    using S = std::function<void(kspn_options&)>;
+    std::vector<std::vector<S>> axes;
+    {
+      std::vector<S> a;
+      for (uint32_t v : { 6u, 12u, 24u, 48u, 96u }) a.push_back([v](kspn_options& x) { x.bu_enter_div = v; });
+      axes.push_back(a);
+    }
+    {
+      std::vector<S> a;
+      for (uint32_t v : { 24u, 48u, 96u, 192u, 384u }) a.push_back([v](kspn_options& x) { x.bu_leave_div = v; });
+      axes.push_back(a);
+    }
+    axes.push_back({ [](kspn_options& x) { x.trim2 = 0; }, [](kspn_options& x) { x.trim2 = 1; } });
+    if (ctx->pivot_model) axes.push_back({ [](kspn_options& x) { x.learned_pivot = 0; }, [](kspn_options& x) { x.learned_pivot = 1; } });
+    kspn_options r = tune(o, axes, run, report);
+    r.validate     = base ? base->validate : 1;
+    *best          = r;
+    run_pipeline(ctx, g, d_scc_id, r, nullptr); // leave the chosen settings' ids
+  });
+}
+
+int
+kspn_autotune_batched(kspn_context* ctx, uint32_t count, uint64_t n_total, const uint64_t* d_vtx_off, const uint64_t* d_fw_head, const uint32_t* d_fw_csr, const uint64_t* d_bw_head,
+                      const uint32_t* d_bw_csr, uint32_t* d_scc_id, const kspn_batch_options* base, uint32_t reps, kspn_batch_options* best, kspn_tune_report* report)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(count == 0 || (d_vtx_off && d_fw_head && d_fw_csr && d_bw_head && d_bw_csr && d_scc_id), "null pointer");
+    require(best, "null pointer");
+    require(n_total < 0xFFFFFFFFull, "n_total must be below 2^32 - 1");
+    bind_device(ctx);
+    kspn_batch_options o{};
+    if (base) o = *base;
+    uint32_t const R = reps ? reps : 3;
+    tune_check     chk{ ctx, n_total };
+    auto           run = [&](kspn_batch_options const& c) {
+      scc_batched(ctx, count, n_total, d_vtx_off, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr, d_scc_id, c, nullptr); // warm-up (and capture)
+      chk.take(d_scc_id);
+      float best_ms = 1e30f;
+      for (uint32_t r = 0; r < R; ++r) {
+        KSPN_CUDA(cudaEventRecord(ctx->ev[KSPN_PHASES], ctx->stream));
+        scc_batched(ctx, count, n_total, d_vtx_off, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr, d_scc_id, c, nullptr);
+        KSPN_CUDA(cudaEventRecord(ctx->ev[KSPN_PHASES + 1], ctx->stream));
+        KSPN_CUDA(cudaEventSynchronize(ctx->ev[KSPN_PHASES + 1]));
+        float ms = 0;
+        KSPN_CUDA(cudaEventElapsedTime(&ms, ctx->ev[KSPN_PHASES], ctx->ev[KSPN_PHASES + 1]));
+        best_ms = std::min(best_ms, ms);
+      }
+      return best_ms;
+    };
+    using S = std::function<void(kspn_batch_options&)>;
+    std::vector<std::vector<S>> axes;
+    {
+      std::vector<S> a;
+      a.push_back([](kspn_batch_options& x) { x.cluster_size = 1, x.cluster_min = 0; });
+      for (uint32_t cs : { 2u, 4u, 8u })
+        for (uint64_t cm : { 1ull << 15, 1ull << 17 }) a.push_back([cs, cm](kspn_batch_options& x) { x.cluster_size = cs, x.cluster_min = cm; });
+      axes.push_back(a);
+    }
+    {
+      std::vector<S> a;
+      for (uint32_t v : { 64u, 256u, 512u }) a.push_back([v](kspn_batch_options& x) { x.rem_tarjan = v; });
+      axes.push_back(a);
+    }
+    {
+      std::vector<S> a;
+      for (uint32_t v : { 8u, 64u, 512u }) a.push_back([v](kspn_batch_options& x) { x.max_rounds = v; });
+      axes.push_back(a);
+    }
+    kspn_batch_options const r = tune(o, axes, run, report);
+    *best                      = r;
+    scc_batched(ctx, count, n_total, d_vtx_off, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr, d_scc_id, r, nullptr);
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
   });
 }
 
