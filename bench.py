@@ -161,6 +161,70 @@ def run_reference(args):
     return 0
 
 
+def run_batched(ctx, stream, args, K):
+    """The batch mix (4096 G(n, m) graphs, n log-uniform in [2^8, 2^18],
+    mean out-degree U[0.8, 6], seed 5) through kspn_scc_batched: device time
+    per call, whole-pipeline roofline, and the reference kaspan::scc on the
+    host cores over a bounded sample of the same graphs."""
+    import numpy as np
+    import torch
+
+    import kaspan_b200.graphs as KG
+
+    B = KG.batch(ctx, 4096, 5)
+    out = torch.empty(B.n, dtype=torch.int32, device="cuda")
+    steps = max(3, min(args.steps, 10))
+
+    def timed(o):
+        for _ in range(2):
+            ctx.scc_batched(B.count, B.n, B.vtx_off, B.fwh, B.fwc, B.bwh, B.bwc, out, o)
+        torch.cuda.synchronize()
+        l0 = ctx.launches
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        st = None
+        for _ in range(steps):
+            st = ctx.scc_batched(B.count, B.n, B.vtx_off, B.fwh, B.fwc, B.bwh, B.bwc, out, o)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, (ctx.launches - l0) / steps, st
+
+    ms, launches, st = timed(None)
+    best, rep = ctx.autotune_batched(B.count, B.n, B.vtx_off, B.fwh, B.fwc, B.bwh, B.bwc, out, reps=2)
+    ms_t, _, st_t = timed(best)
+    peak, peak_kind = measured_peak_gbs()
+    b_min = 2 * (8 * (B.n + 1) + 4 * B.m) + 4 * B.n
+    res = {
+        "workload": "4096 directed G(n,m) graphs, n = round(2^U[8,18]), m = round(n * U[0.8, 6]) draws, seed 5, self-loops and duplicates removed, local u32 ids, one concatenated CSR + CSC",
+        "graphs": B.count, "n": B.n, "m": B.m, "steps": steps,
+        "value": B.m / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+        "launches_per_step": launches, "captured": "one CUDA graph per call (plan + solve kernels), replayed",
+        "stats": st.as_dict(),
+        "pipeline_min_bytes": b_min, "pipeline_frac": (b_min / (ms * 1e-3)) / 1e9 / peak, "peak": peak, "peak_source": peak_kind,
+        "tuned": {"value": B.m / (ms_t * 1e-3), "ms_per_step": ms_t, "candidates": rep.candidates, "tuner_default_ms": rep.default_ms, "tuner_best_ms": rep.best_ms,
+                  "best": {"cluster_size": best.cluster_size, "cluster_min": best.cluster_min, "rem_tarjan": best.rem_tarjan, "max_rounds": best.max_rounds}},
+    }
+    if not args.no_cpu_baseline:
+        # the reference's kaspan::scc on the host cores, one call per graph,
+        # over the first 256 graphs of the mix (a bounded sample)
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        if O.ref_lib() is not None:
+            secs, edges = 0.0, 0
+            for g in range(256):
+                n, fwh, fwc, bwh, bwc = B.graph(g)
+                _, t = O.ref_scc(O.Graph(n, fwh, np.ascontiguousarray(fwc) if fwc.size else np.zeros(1, np.uint32), bwh,
+                                         np.ascontiguousarray(bwc) if bwc.size else np.zeros(1, np.uint32)))
+                secs += t
+                edges += int(fwh[-1])
+            res["cpu_baseline"] = {"value": edges / secs, "unit": UNIT, "cores": 1, "kind": "reference",
+                                   "sample": f"the first 256 graphs of the mix ({edges} edges), one kaspan::scc call each (reference code, 1 rank, 1 core)"}
+    del B, out
+    torch.cuda.empty_cache()
+    return res
+
+
 def run_kspn(args):
     import numpy as np
     import torch
@@ -275,6 +339,20 @@ def run_kspn(args):
         ctx.set_pivot_model(None)
         torch.cuda.empty_cache()
 
+    # ---- autotuner on the workload (FAST pipeline switch points, trim-2,
+    # learned pivot): what it picks and what it gains over the defaults
+    autotune = None
+    if world == 1 and not args.no_batched:
+        best, rep = ctx.autotune(G.n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, K.default_options(pipeline=pipeline, validate=0), reps=3)
+        autotune = {"candidates": rep.candidates, "default_ms": rep.default_ms, "best_ms": rep.best_ms,
+                    "best": {"bu_enter_div": best.bu_enter_div, "bu_leave_div": best.bu_leave_div, "trim2": best.trim2, "learned_pivot": best.learned_pivot}}
+
+    # ---- batched path: the 4096-graph uneven G(n, m) mix in one captured
+    # launch sequence, with the defaults and with the autotuned settings
+    batched = None
+    if world == 1 and not args.no_batched:
+        batched = run_batched(ctx, stream, args, K)
+
     # correctness spot check of the last step (canonical ids are min members)
     ids = out.cpu().numpy().view(np.uint32)
     assert (ids <= np.arange(G.n, dtype=np.uint32)).all(), "ids must name a member no larger than the vertex"
@@ -346,10 +424,12 @@ def run_kspn(args):
                          "pipeline_min_bytes": b_min, "pipeline_frac": (b_min / (ms * 1e-3)) / 1e9 / peak},
             "clocks": clk.summary(),
             "learned_vs_plain": learned_vs_plain,
+            "autotune": autotune,
+            "batched": batched,
             "phases": {"decided": last["decided"], "ms": {k: round(v, 4) for k, v in last["ms"].items()}, "levels_fw": last["levels_fw"],
                        "levels_bw": last["levels_bw"], "bottom_up": last["levels_bottom_up"], "label_calls": last["label_calls"],
                        "edges_scanned": last["edges_scanned"], "trace": trace,
-                       "search_phase_ms": {{4: "expand", 5: "sweep", 7: "materialize", 8: "init", 9: "end", 10: "finalize", 11: "trim_seed", 12: "trim_level"}.get(k, k): round(v, 4) for k, v in search_phases.items()},
+                       "search_phase_ms": {{4: "expand", 5: "sweep", 7: "materialize", 8: "init", 9: "end", 10: "finalize", 11: "trim_seed", 12: "trim_level", 13: "worklist", 14: "fix_up", 15: "trim_heavy"}.get(k, k): round(v, 4) for k, v in search_phases.items()},
                        "kernels": {k: {"ms": round(a[0] / prof_steps, 4), "GB/s": round(a[1] / (a[0] * 1e-3) / 1e9, 1) if a[0] else 0}
                                                                             for k, a in agg.items()}},
         }
@@ -374,6 +454,7 @@ def main():
     ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS))
     ap.add_argument("--pipeline", default="fast", choices=["fast", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-path and autotuner sections")
     ap.add_argument("--profile-steps", type=int, default=None, help="steps run with per-kernel event timing (default min(steps, 3))")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "kspn":
