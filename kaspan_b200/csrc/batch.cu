@@ -172,6 +172,49 @@ bt_slot(uint32_t* counter)
   return base + __popc(mask & ((1u << lane) - 1u));
 }
 
+// fn(u, e) for every edge e of every row of list[lo, hi): a warp takes 32
+// listed vertices at a time and its lanes split their edges evenly (a
+// warp-wide scan of the row lengths; each lane finds its row by a binary
+// search over the lanes' exclusive prefixes), so 32 independent loads are
+// in flight per instruction instead of one dependent row walk per thread.
+// All lanes of every warp of the group call it; fn is called by the active
+// lanes only.
+template<class F>
+__device__ __forceinline__ void
+bt_warp_edges(bt_group const& g, uint32_t const* list, uint32_t lo, uint32_t hi, uint64_t const* head, F&& fn)
+{
+  unsigned const lane = threadIdx.x & 31u;
+  uint32_t const gw = g.gt >> 5, GW = g.GT >> 5;
+  for (uint32_t base = lo + gw * 32; base < hi; base += GW * 32) {
+    uint32_t const i  = base + lane;
+    bool const     ok = i < hi;
+    uint32_t const u  = ok ? __ldcg(list + i) : 0u;
+    uint64_t const b  = ok ? head[u] : 0;
+    uint32_t const d  = ok ? static_cast<uint32_t>(head[u + 1] - b) : 0u;
+    uint32_t       incl = d;
+#pragma unroll
+    for (int sh = 1; sh < 32; sh <<= 1) {
+      uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, incl, sh);
+      if (lane >= static_cast<unsigned>(sh)) incl += y;
+    }
+    uint32_t const total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    uint32_t const excl  = incl - d;
+    for (uint32_t kb = 0; kb < total; kb += 32) {
+      uint32_t const k = kb + lane;
+      uint32_t       j = 0;
+#pragma unroll
+      for (int step = 16; step; step >>= 1) {
+        uint32_t const ex = __shfl_sync(0xFFFFFFFFu, excl, j + step);
+        if (ex <= k) j += step;
+      }
+      uint64_t const bj = __shfl_sync(0xFFFFFFFFu, b, j);
+      uint32_t const xj = __shfl_sync(0xFFFFFFFFu, excl, j);
+      uint32_t const uj = __shfl_sync(0xFFFFFFFFu, u, j);
+      if (k < total) fn(uj, bj + (k - xj));
+    }
+  }
+}
+
 // One graph's view for the group.
 struct bt_graph
 {
@@ -194,8 +237,8 @@ struct bt_graph
 // lowers its undecided out-neighbours' live in-degree and in-neighbours'
 // live out-degree; a count reaching 0 decides that neighbour (id = itself)
 // and queues it.  Queues alternate between the two buffers that are not
-// qin.  A thread's row entries are loaded four at a time before their
-// probes.  Returns the vertices decided.
+// qin; rows are walked warp-cooperatively (bt_warp_edges).  Returns the
+// vertices decided.
 __device__ uint32_t
 bt_trim(bt_args const& a, bt_graph const& G, bt_group const& g, uint32_t* qin, uint32_t qn)
 {
@@ -219,20 +262,11 @@ bt_trim(bt_args const& a, bt_graph const& G, bt_group const& g, uint32_t* qin, u
         qout[bt_slot(&g.S->cnt)] = w;
       }
     };
-    for (uint32_t i = g.gt; i < qn; i += g.GT) {
-      uint32_t const u = __ldcg(qin + i);
 #pragma unroll 1
-      for (int dir = 0; dir < 2; ++dir) {
-        uint64_t const* head = dir ? G.bh : G.fh;
-        uint32_t const* adj  = dir ? a.bc : a.fc;
-        uint32_t*       deg  = dir ? G.outdeg : G.indeg;
-        uint64_t        e = head[u], end = head[u + 1];
-        for (; e + 4 <= end; e += 4) {
-          uint32_t const w0 = adj[e], w1 = adj[e + 1], w2 = adj[e + 2], w3 = adj[e + 3];
-          hit(w0, deg), hit(w1, deg), hit(w2, deg), hit(w3, deg);
-        }
-        for (; e < end; ++e) hit(adj[e], deg);
-      }
+    for (int dir = 0; dir < 2; ++dir) {
+      uint32_t const* adj = dir ? a.bc : a.fc;
+      uint32_t*       deg = dir ? G.outdeg : G.indeg;
+      bt_warp_edges(g, qin, 0, qn, dir ? G.bh : G.fh, [&](uint32_t, uint64_t e) { hit(adj[e], deg); });
     }
     g.sync();
     qn = g.S->cnt;
@@ -267,13 +301,10 @@ bt_reach(bt_args const& a, bt_graph const& G, bt_group const& g, uint64_t const*
       if (g.leader()) atomicExch(a.ctr + 4, 1u);
       break;
     }
-    for (uint32_t i = lo + g.gt; i < hi; i += g.GT) {
-      uint32_t const u = __ldcg(list + i);
-      for (uint64_t e = head[u], end = head[u + 1]; e < end; ++e) {
-        uint32_t const w = adj[e];
-        if ((cand ? bt_get(cand, w) : bt_get(G.und, w)) && bit_claim(mark, w)) list[bt_slot(&g.S->cnt)] = w;
-      }
-    }
+    bt_warp_edges(g, list, lo, hi, head, [&](uint32_t, uint64_t e) {
+      uint32_t const w = adj[e];
+      if ((cand ? bt_get(cand, w) : bt_get(G.und, w)) && bit_claim(mark, w)) list[bt_slot(&g.S->cnt)] = w;
+    });
     g.sync();
     if (g.leader()) g.S->lo = hi, g.S->hi = g.S->cnt;
     g.sync();
