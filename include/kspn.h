@@ -416,6 +416,49 @@ int  kspn_gen_batch(kspn_context* ctx, uint32_t count, uint64_t seed,
 int  kspn_batch_localize(kspn_context* ctx, uint32_t count, uint64_t n_total,
                          const uint64_t* d_vtx_off, const uint64_t* d_head, uint32_t* d_csr);
 
+/* ---------------------------------------------------------------- manifest graph files */
+/*
+ * The reference's on-disk graph format (kaspan/scc/adapter/manifest.hpp:
+ * 19-245): a text manifest of `key value` lines (`%` starts a comment) and
+ * four binary files -- fw/bw head (n + 1 entries) and fw/bw csr (m entries)
+ * -- of dense unsigned integers, graph.head.bytes / graph.csr.bytes bytes
+ * each (1..8), in graph.endian byte order.  Paths in the manifest are
+ * relative to its directory.
+ */
+typedef struct kspn_manifest {
+    uint32_t schema_version;
+    int32_t  big_endian;        /* graph.endian: 0 little, 1 big */
+    uint64_t node_count;        /* graph.node_count */
+    uint64_t edge_count;        /* graph.edge_count */
+    int32_t  self_loops;        /* graph.contains_self_loops */
+    int32_t  duplicate_edges;   /* graph.contains_duplicate_edges */
+    uint32_t head_bytes;        /* graph.head.bytes */
+    uint32_t csr_bytes;         /* graph.csr.bytes */
+    char     graph_code[64];
+    char     graph_name[128];
+    char     fw_head_path[1024];  /* resolved against the manifest's directory */
+    char     fw_csr_path[1024];
+    char     bw_head_path[1024];
+    char     bw_csr_path[1024];
+} kspn_manifest;
+
+/* Parses a manifest (host only; every key the reference requires must be
+ * present, widths 1..8, booleans true/false, endian little/big). */
+int kspn_manifest_read(const char* path, kspn_manifest* out);
+/* Loads its four files into device arrays (u64 heads of n + 1, u32 ids of
+ * m entries): pinned host chunks, raw copies, a decode kernel on the
+ * device.  Entries beyond m (heads) or >= n (ids) are KSPN_ERR_INVALID_GRAPH. */
+int kspn_manifest_load(kspn_context* ctx, const kspn_manifest* mf,
+                       uint64_t* d_fw_head, uint32_t* d_fw_csr,
+                       uint64_t* d_bw_head, uint32_t* d_bw_csr);
+/* Writes host arrays as <dir>/<name>.manifest + four .bin files with the
+ * given entry widths and byte order (an entry that does not fit is an error). */
+int kspn_manifest_write(const char* dir, const char* name, uint32_t n, uint64_t m,
+                        const uint64_t* fw_head, const uint32_t* fw_csr,
+                        const uint64_t* bw_head, const uint32_t* bw_csr,
+                        uint32_t head_bytes, uint32_t csr_bytes, int big_endian,
+                        int self_loops, int duplicate_edges);
+
 /* ---------------------------------------------------------------- inputs */
 /*
  * Seeded synthetic edge lists on the device (no reference counterpart:

@@ -192,9 +192,45 @@ SIGNATURES = {
     "kspn_batch_shape": (None, [_u32, _u64, _u32, _u32, C.c_float, C.c_float, _P, _P]),
     "kspn_gen_batch": (_i32, [_P, _u32, _u64, _P, _P, _P, _P]),
     "kspn_batch_localize": (_i32, [_P, _u32, _u64, _P, _P, _P]),
+    "kspn_manifest_read": (_i32, [C.c_char_p, _P]),
+    "kspn_manifest_load": (_i32, [_P, _P, _P, _P, _P, _P]),
+    "kspn_manifest_write": (_i32, [C.c_char_p, C.c_char_p, _u32, _u64, _P, _P, _P, _P, _u32, _u32, _i32, _i32, _i32]),
     "kspn_autotune": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _u32, _P, _P]),
     "kspn_autotune_batched": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P, _u32, _P, _P]),
 }
+
+
+class Manifest(C.Structure):
+    """kspn_manifest (include/kspn.h)."""
+    _fields_ = [("schema_version", C.c_uint32), ("big_endian", C.c_int32), ("node_count", C.c_uint64), ("edge_count", C.c_uint64),
+                ("self_loops", C.c_int32), ("duplicate_edges", C.c_int32), ("head_bytes", C.c_uint32), ("csr_bytes", C.c_uint32),
+                ("graph_code", C.c_char * 64), ("graph_name", C.c_char * 128), ("fw_head_path", C.c_char * 1024),
+                ("fw_csr_path", C.c_char * 1024), ("bw_head_path", C.c_char * 1024), ("bw_csr_path", C.c_char * 1024)]
+
+
+def manifest_read(path: str) -> Manifest:
+    """Parse a manifest file (host only)."""
+    mf = Manifest()
+    rc = lib().kspn_manifest_read(path.encode(), C.byref(mf))
+    if rc:
+        raise KspnError(rc, f"manifest_read: {path}")
+    return mf
+
+
+def manifest_write(directory: str, name: str, n: int, fw_head, fw_csr, bw_head, bw_csr, head_bytes: int = 8, csr_bytes: int = 4,
+                   big_endian: bool = False, self_loops: bool = False, duplicate_edges: bool = False) -> str:
+    """Write host arrays (numpy u64 heads, u32 ids) in the manifest format; returns the manifest path."""
+    fw_head = np.ascontiguousarray(fw_head, np.uint64)
+    bw_head = np.ascontiguousarray(bw_head, np.uint64)
+    fw_csr = np.ascontiguousarray(fw_csr, np.uint32)
+    bw_csr = np.ascontiguousarray(bw_csr, np.uint32)
+    m = int(fw_head[n]) if n else 0
+    rc = lib().kspn_manifest_write(directory.encode(), name.encode(), n, m, fw_head.ctypes.data, fw_csr.ctypes.data if fw_csr.size else None,
+                                   bw_head.ctypes.data, bw_csr.ctypes.data if bw_csr.size else None, head_bytes, csr_bytes,
+                                   int(big_endian), int(self_loops), int(duplicate_edges))
+    if rc:
+        raise KspnError(rc, f"manifest_write: {directory}/{name}")
+    return os.path.join(directory, name + ".manifest")
 
 
 class TuneReport(C.Structure):
@@ -437,6 +473,9 @@ class Context:
         self._check(lib().kspn_scc_batched(self.h, count, n_total, _ptr(vtx_off), _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc), _ptr(out),
                                            C.byref(options) if options is not None else None, C.byref(st)), "scc_batched")
         return st
+
+    def manifest_load(self, mf: "Manifest", fwh, fwc, bwh, bwc):
+        self._check(lib().kspn_manifest_load(self.h, C.byref(mf), _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc)), "manifest_load")
 
     def autotune(self, n, m, fwh, fwc, bwh, bwc, out, base: "Options | None" = None, reps: int = 3):
         """(best Options, TuneReport) for this graph (FAST pipeline settings)."""

@@ -1100,6 +1100,46 @@ kspn_autotune_batched(kspn_context* ctx, uint32_t count, uint64_t n_total, const
   });
 }
 
+int
+kspn_manifest_read(const char* path, kspn_manifest* out)
+{
+  try {
+    if (!path || !out) return KSPN_ERR_INVALID_ARGUMENT;
+    manifest_read(path, out);
+    return KSPN_OK;
+  } catch (error const& e) {
+    return e.code;
+  } catch (...) {
+    return KSPN_ERR_INTERNAL;
+  }
+}
+
+int
+kspn_manifest_load(kspn_context* ctx, const kspn_manifest* mf, uint64_t* d_fw_head, uint32_t* d_fw_csr, uint64_t* d_bw_head, uint32_t* d_bw_csr)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(mf && d_fw_head && d_bw_head && (mf->edge_count == 0 || (d_fw_csr && d_bw_csr)), "null pointer");
+    bind_device(ctx);
+    manifest_load(ctx, *mf, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr);
+  });
+}
+
+int
+kspn_manifest_write(const char* dir, const char* name, uint32_t n, uint64_t m, const uint64_t* fw_head, const uint32_t* fw_csr, const uint64_t* bw_head, const uint32_t* bw_csr,
+                    uint32_t head_bytes, uint32_t csr_bytes, int big_endian, int self_loops, int duplicate_edges)
+{
+  try {
+    if (!dir || !name || !fw_head || !bw_head || (m && (!fw_csr || !bw_csr))) return KSPN_ERR_INVALID_ARGUMENT;
+    manifest_write(dir, name, n, m, fw_head, fw_csr, bw_head, bw_csr, head_bytes, csr_bytes, big_endian, self_loops, duplicate_edges);
+    return KSPN_OK;
+  } catch (error const& e) {
+    return e.code;
+  } catch (...) {
+    return KSPN_ERR_INTERNAL;
+  }
+}
+
 void
 kspn_batch_shape(uint32_t count, uint64_t seed, uint32_t log2_min, uint32_t log2_max, float deg_min, float deg_max, uint32_t* n_out, uint64_t* draws_out)
 {

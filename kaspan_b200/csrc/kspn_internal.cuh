@@ -428,6 +428,10 @@ uint32_t select_pivot_live(kspn_context* ctx, dgraph const& g, uint32_t const* u
 void     scc_batched(kspn_context* ctx, uint32_t G, uint64_t N, uint64_t const* vtx_off, uint64_t const* fh, uint32_t const* fc, uint64_t const* bh, uint32_t const* bc, uint32_t* scc_id,
                      kspn_batch_options const& opt, kspn_batch_stats* st);
 void     batch_release(kspn_context* ctx);
+void     manifest_read(char const* path, kspn_manifest* out);
+void     manifest_load(kspn_context* ctx, kspn_manifest const& mf, uint64_t* fh, uint32_t* fc, uint64_t* bh, uint32_t* bc);
+void     manifest_write(char const* dir, char const* name, uint32_t n, uint64_t m, uint64_t const* fh, uint32_t const* fc, uint64_t const* bh, uint32_t const* bc, uint32_t head_bytes,
+                        uint32_t csr_bytes, int big_endian, int self_loops, int duplicate_edges);
 void     batch_shape(uint32_t count, uint64_t seed, uint32_t log2_min, uint32_t log2_max, float deg_min, float deg_max, uint32_t* n_out, uint64_t* draws_out);
 void     gen_batch(kspn_context* ctx, uint32_t count, uint64_t seed, uint64_t const* vtx_off, uint64_t const* draw_off, uint64_t total_draws, uint32_t* src, uint32_t* dst);
 void     batch_localize(kspn_context* ctx, uint32_t count, uint64_t N, uint64_t const* vtx_off, uint64_t const* head, uint32_t* csr);

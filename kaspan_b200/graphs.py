@@ -156,3 +156,21 @@ def batch(ctx: Context, count: int = 4096, seed: int = 5, log2_min: int = 8, log
     ctx.batch_localize(count, N, d_vo, G.fwh, G.fwc)
     ctx.batch_localize(count, N, d_vo, G.bwh, G.bwc)
     return DeviceBatch(count, N, G.m, d_vo, G.fwh, G.fwc, G.bwh, G.bwc, sizes)
+
+
+def from_manifest(ctx: Context, path: str, device="cuda") -> DeviceGraph:
+    """A graph in the reference's manifest format, loaded onto the device
+    (kspn_manifest_read + kspn_manifest_load)."""
+    import torch
+
+    from . import manifest_read
+
+    mf = manifest_read(path)
+    n, m = int(mf.node_count), int(mf.edge_count)
+    fwh = torch.empty(n + 1, dtype=torch.int64, device=device)
+    bwh = torch.empty(n + 1, dtype=torch.int64, device=device)
+    fwc = torch.empty(max(m, 1), dtype=torch.int32, device=device)
+    bwc = torch.empty(max(m, 1), dtype=torch.int32, device=device)
+    torch.cuda.synchronize()
+    ctx.manifest_load(mf, fwh, fwc, bwh, bwc)
+    return DeviceGraph(n, m, fwh, fwc, bwh, bwc)

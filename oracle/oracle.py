@@ -95,6 +95,7 @@ def ref_lib() -> C.CDLL | None:
             "kref_label_search_pull": (None, [u32, u64, _u64p, _u32p, _u64p, _u32p, _u64p, _u32p, i32]),
             "kref_trim_1_exhaustive_first": (None, [u32, u64, _u64p, _u32p, _u64p, _u32p, _u64p, _u32p, _u32p, _u32p]),
             "kref_select_pivot_from_degree": (u32, [u32, _u64p, _u32p, _u32p]),
+            "kref_manifest_load": (i32, [C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -280,6 +281,21 @@ def ref_scc(g: Graph, variant: str = "scc"):
     if g.n:
         R.kref_normalise(g.n, ids)
     return ids, ns * 1e-9
+
+
+def ref_manifest_load(path: str):
+    """The reference's manifest loader on `path`: (n, fwh, fwc, bwh, bwc) or None."""
+    R = ref_lib()
+    n, m = C.c_uint64(), C.c_uint64()
+    if R.kref_manifest_load(path.encode(), C.byref(n), C.byref(m), None, None, None, None) != 0:
+        return None
+    fwh = np.zeros(n.value + 1, np.uint64)
+    bwh = np.zeros(n.value + 1, np.uint64)
+    fwc = np.zeros(max(m.value, 1), np.uint32)
+    bwc = np.zeros(max(m.value, 1), np.uint32)
+    if R.kref_manifest_load(path.encode(), C.byref(n), C.byref(m), fwh.ctypes.data, fwc.ctypes.data, bwh.ctypes.data, bwc.ctypes.data) != 0:
+        return None
+    return n.value, fwh, fwc[: m.value], bwh, bwc[: m.value]
 
 
 def ref_tarjan(g: Graph):

@@ -24,6 +24,7 @@
 #include <kaspan/scc/tarjan.hpp>
 #include <kaspan/scc/trim_1_exhaustive.hpp>
 #include <kaspan/scc/trim_1_local.hpp>
+#include <kaspan/scc/adapter/manifest.hpp>
 #include <kaspan/scc/variant/scc_hpc_like.hpp>
 #include <kaspan/scc/variant/scc_hpc_trim_ex.hpp>
 #include <kaspan/scc/variant/scc_ispan_like.hpp>
@@ -191,6 +192,28 @@ kref_select_pivot_from_degree(uint32_t n, uint64_t* undecided, uint32_t const* o
 {
   ensure_init();
   return select_pivot_from_degree(single_part_view{ n }, undecided, outdegree, indegree);
+}
+
+/* The reference's manifest reader and loader (kaspan/scc/adapter/
+ * manifest.hpp:132-245): *n_out / *m_out from the manifest; with arrays
+ * given (n + 1 heads, m ids each), the graph as load_graph_from_manifest
+ * builds it.  Returns 0, or -1 when the files cannot be read. */
+int
+kref_manifest_load(char const* path, uint64_t* n_out, uint64_t* m_out, uint64_t* fwh, uint32_t* fwc, uint64_t* bwh, uint32_t* bwc)
+{
+  ensure_init();
+  try {
+    auto const mf = manifest::load(path);
+    *n_out        = mf.graph_node_count;
+    *m_out        = mf.graph_edge_count;
+    if (!fwh) return 0;
+    auto const g = load_graph_from_manifest(mf);
+    for (uint64_t i = 0; i <= mf.graph_node_count; ++i) fwh[i] = g.fw.head[i], bwh[i] = g.bw.head[i];
+    for (uint64_t i = 0; i < mf.graph_edge_count; ++i) fwc[i] = g.fw.csr[i], bwc[i] = g.bw.csr[i];
+    return 0;
+  } catch (...) {
+    return -1;
+  }
 }
 
 } // extern "C"
