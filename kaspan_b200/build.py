@@ -58,7 +58,23 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     return LIB
 
 
+CLI_SRC = os.path.join(HERE, "cli", "kspn_bench.cpp")
+CLI = os.path.join(HERE, "kspn_bench")
+
+
+def build_cli(force: bool = False) -> str:
+    """The bench_kaspan-compatible command line (links libkspn.so)."""
+    if not force and os.path.exists(CLI) and os.path.getmtime(CLI) > max(os.path.getmtime(CLI_SRC), os.path.getmtime(LIB)):
+        return CLI
+    cmd = [_nvcc(), "-O2", "-std=c++20", "-I", INCLUDE, CLI_SRC, "-o", CLI + ".tmp", "-L", HERE, "-lkspn", "-Xlinker", "-rpath,$ORIGIN", "-cudart", "static"]
+    subprocess.run(cmd, check=True)
+    os.replace(CLI + ".tmp", CLI)
+    return CLI
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose="--verbose" in sys.argv,
           extra=["-Xptxas", "-v"] if "--ptxas-v" in sys.argv else None)
+    build_cli(force="--force" in sys.argv)
     print(LIB)
+    print(CLI)
