@@ -161,24 +161,36 @@ def run_reference(args):
     return 0
 
 
-def run_batched(ctx, stream, args, K):
+def run_batched(ctx, stream, args, K, world=1, rank=0):
     """The batch mix (4096 G(n, m) graphs, n log-uniform in [2^8, 2^18],
     mean out-degree U[0.8, 6], seed 5) through kspn_scc_batched: device time
     per call, whole-pipeline roofline, and the reference kaspan::scc on the
-    host cores over a bounded sample of the same graphs."""
+    host cores over a bounded sample of the same graphs.  On N GPUs each
+    rank decomposes its shard (greedy edge-balanced bin packing of the
+    graphs, no communication); the time is the max over ranks."""
     import numpy as np
     import torch
+    import torch.distributed as dist
 
     import kaspan_b200.graphs as KG
 
-    B = KG.batch(ctx, 4096, 5)
+    shard = None
+    if world > 1:
+        n_all, d_all = K.batch_shape(4096, 5)
+        shard = KG.batch_partition(n_all.astype(np.float64) + d_all.astype(np.float64), world)[rank]
+    B = KG.batch(ctx, 4096, 5, graphs=shard)
     out = torch.empty(B.n, dtype=torch.int32, device="cuda")
     steps = max(3, min(args.steps, 10))
+
+    def sync():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
 
     def timed(o):
         for _ in range(2):
             ctx.scc_batched(B.count, B.n, B.vtx_off, B.fwh, B.fwc, B.bwh, B.bwc, out, o)
-        torch.cuda.synchronize()
+        sync()
         l0 = ctx.launches
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -186,25 +198,38 @@ def run_batched(ctx, stream, args, K):
         for _ in range(steps):
             st = ctx.scc_batched(B.count, B.n, B.vtx_off, B.fwh, B.fwc, B.bwh, B.bwc, out, o)
         e1.record(stream)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / steps, (ctx.launches - l0) / steps, st
+        sync()
+        t = e0.elapsed_time(e1) / steps
+        if world > 1:
+            x = torch.tensor([t], device="cuda")
+            dist.all_reduce(x, op=dist.ReduceOp.MAX)
+            t = float(x.item())
+        return t, (ctx.launches - l0) / steps, st
 
+    m_all = float(B.m)
+    n_all_v = float(B.n)
+    if world > 1:
+        x = torch.tensor([m_all, n_all_v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(x)
+        m_all, n_all_v = float(x[0].item()), float(x[1].item())
     ms, launches, st = timed(None)
+    # every rank tunes its own shard (the same steps on every rank)
     best, rep = ctx.autotune_batched(B.count, B.n, B.vtx_off, B.fwh, B.fwc, B.bwh, B.bwc, out, reps=2)
     ms_t, _, st_t = timed(best)
     peak, peak_kind = measured_peak_gbs()
-    b_min = 2 * (8 * (B.n + 1) + 4 * B.m) + 4 * B.n
+    b_min = 2 * (8 * (n_all_v + 1) + 4 * m_all) + 4 * n_all_v
     res = {
         "workload": "4096 directed G(n,m) graphs, n = round(2^U[8,18]), m = round(n * U[0.8, 6]) draws, seed 5, self-loops and duplicates removed, local u32 ids, one concatenated CSR + CSC",
-        "graphs": B.count, "n": B.n, "m": B.m, "steps": steps,
-        "value": B.m / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+        "graphs": 4096, "n": int(n_all_v), "m": int(m_all), "steps": steps, "n_gpus": world,
+        "scaling": "strong" if world > 1 else None, "sharding": "greedy edge-balanced bin packing of whole graphs, no communication" if world > 1 else None,
+        "value": m_all / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
         "launches_per_step": launches, "captured": "one CUDA graph per call (plan + solve kernels), replayed",
         "stats": st.as_dict(),
         "pipeline_min_bytes": b_min, "pipeline_frac": (b_min / (ms * 1e-3)) / 1e9 / peak, "peak": peak, "peak_source": peak_kind,
-        "tuned": {"value": B.m / (ms_t * 1e-3), "ms_per_step": ms_t, "candidates": rep.candidates, "tuner_default_ms": rep.default_ms, "tuner_best_ms": rep.best_ms,
+        "tuned": {"value": m_all / (ms_t * 1e-3), "ms_per_step": ms_t, "candidates": rep.candidates, "tuner_default_ms": rep.default_ms, "tuner_best_ms": rep.best_ms,
                   "best": {"cluster_size": best.cluster_size, "cluster_min": best.cluster_min, "rem_tarjan": best.rem_tarjan, "max_rounds": best.max_rounds}},
     }
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
         # the reference's kaspan::scc on the host cores, one call per graph,
         # over the first 256 graphs of the mix (a bounded sample)
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -350,8 +375,8 @@ def run_kspn(args):
     # ---- batched path: the 4096-graph uneven G(n, m) mix in one captured
     # launch sequence, with the defaults and with the autotuned settings
     batched = None
-    if world == 1 and not args.no_batched:
-        batched = run_batched(ctx, stream, args, K)
+    if not args.no_batched:
+        batched = run_batched(ctx, stream, args, K, world, rank)
 
     # correctness spot check of the last step (canonical ids are min members)
     ids = out.cpu().numpy().view(np.uint32)

@@ -408,10 +408,12 @@ int kspn_autotune_batched(kspn_context* ctx, uint32_t count, uint64_t n_total,
 void kspn_batch_shape(uint32_t count, uint64_t seed, uint32_t log2_min, uint32_t log2_max,
                       float deg_min, float deg_max, uint32_t* n_out, uint64_t* draws_out);
 /* Its edge draws on the device, GLOBAL ids (vtx_off[g] + local): draw k of
- * graph g is (u, v) uniform in [0, n_g)^2; d_draw_off = prefix of draws_out. */
+ * graph g is (u, v) uniform in [0, n_g)^2; d_draw_off = prefix of draws_out.
+ * d_graph_ids (nullable): graph g of this batch is graph d_graph_ids[g] of
+ * the mix (a shard of it: the same graphs the whole mix holds). */
 int  kspn_gen_batch(kspn_context* ctx, uint32_t count, uint64_t seed,
                     const uint64_t* d_vtx_off, const uint64_t* d_draw_off,
-                    uint32_t* d_src, uint32_t* d_dst);
+                    const uint32_t* d_graph_ids, uint32_t* d_src, uint32_t* d_dst);
 /* Global ids -> local ids in every row of a concatenated CSR or CSC. */
 int  kspn_batch_localize(kspn_context* ctx, uint32_t count, uint64_t n_total,
                          const uint64_t* d_vtx_off, const uint64_t* d_head, uint32_t* d_csr);

@@ -190,7 +190,7 @@ SIGNATURES = {
     "kspn_batch_options_default": (None, [_P]),
     "kspn_scc_batched": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _P, _P]),
     "kspn_batch_shape": (None, [_u32, _u64, _u32, _u32, C.c_float, C.c_float, _P, _P]),
-    "kspn_gen_batch": (_i32, [_P, _u32, _u64, _P, _P, _P, _P]),
+    "kspn_gen_batch": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P]),
     "kspn_batch_localize": (_i32, [_P, _u32, _u64, _P, _P, _P]),
     "kspn_manifest_read": (_i32, [C.c_char_p, _P]),
     "kspn_manifest_load": (_i32, [_P, _P, _P, _P, _P, _P]),
@@ -491,8 +491,8 @@ class Context:
                                                 C.byref(base) if base is not None else None, reps, C.byref(best), C.byref(rep)), "autotune_batched")
         return best, rep
 
-    def gen_batch(self, count, seed, vtx_off, draw_off, src, dst):
-        self._check(lib().kspn_gen_batch(self.h, count, seed, _ptr(vtx_off), _ptr(draw_off), _ptr(src), _ptr(dst)), "gen_batch")
+    def gen_batch(self, count, seed, vtx_off, draw_off, src, dst, graph_ids=None):
+        self._check(lib().kspn_gen_batch(self.h, count, seed, _ptr(vtx_off), _ptr(draw_off), _ptr(graph_ids), _ptr(src), _ptr(dst)), "gen_batch")
 
     def batch_localize(self, count, n_total, vtx_off, head, csr):
         self._check(lib().kspn_batch_localize(self.h, count, n_total, _ptr(vtx_off), _ptr(head), _ptr(csr)), "batch_localize")

@@ -1147,7 +1147,7 @@ kspn_batch_shape(uint32_t count, uint64_t seed, uint32_t log2_min, uint32_t log2
 }
 
 int
-kspn_gen_batch(kspn_context* ctx, uint32_t count, uint64_t seed, const uint64_t* d_vtx_off, const uint64_t* d_draw_off, uint32_t* d_src, uint32_t* d_dst)
+kspn_gen_batch(kspn_context* ctx, uint32_t count, uint64_t seed, const uint64_t* d_vtx_off, const uint64_t* d_draw_off, const uint32_t* d_graph_ids, uint32_t* d_src, uint32_t* d_dst)
 {
   if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
   return guard(ctx, [&] {
@@ -1158,7 +1158,7 @@ kspn_gen_batch(kspn_context* ctx, uint32_t count, uint64_t seed, const uint64_t*
       KSPN_CUDA(cudaMemcpyAsync(&total, d_draw_off + count, sizeof(total), cudaMemcpyDeviceToHost, ctx->stream));
       KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
     }
-    gen_batch(ctx, count, seed, d_vtx_off, d_draw_off, total, d_src, d_dst);
+    gen_batch(ctx, count, seed, d_vtx_off, d_draw_off, d_graph_ids, total, d_src, d_dst);
     KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
   });
 }

@@ -290,7 +290,8 @@ batch_key(uint64_t seed, uint32_t g)
 }
 
 __global__ void
-k_gen_batch(uint32_t count, uint64_t seed, uint64_t const* __restrict__ vtx_off, uint64_t const* __restrict__ draw_off, uint64_t total, uint32_t* __restrict__ src, uint32_t* __restrict__ dst)
+k_gen_batch(uint32_t count, uint64_t seed, uint64_t const* __restrict__ vtx_off, uint64_t const* __restrict__ draw_off, uint32_t const* __restrict__ ids, uint64_t total, uint32_t* __restrict__ src,
+            uint32_t* __restrict__ dst)
 {
   for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < total; j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
     // graph of draw j: the last g with draw_off[g] <= j
@@ -302,7 +303,7 @@ k_gen_batch(uint32_t count, uint64_t seed, uint64_t const* __restrict__ vtx_off,
     }
     uint64_t const vo = vtx_off[lo];
     uint64_t const n  = vtx_off[lo + 1] - vo;
-    uint64_t const d  = draw(seed_key(batch_key(seed, lo) ^ 0x45444745ull), j - draw_off[lo]);
+    uint64_t const d  = draw(seed_key(batch_key(seed, ids ? ids[lo] : lo) ^ 0x45444745ull), j - draw_off[lo]);
     src[j]            = static_cast<uint32_t>(vo + ((d & 0xFFFFFFFFull) * n >> 32));
     dst[j]            = static_cast<uint32_t>(vo + ((d >> 32) * n >> 32));
   }
@@ -340,11 +341,11 @@ batch_shape(uint32_t count, uint64_t seed, uint32_t log2_min, uint32_t log2_max,
 }
 
 void
-gen_batch(kspn_context* ctx, uint32_t count, uint64_t seed, uint64_t const* vtx_off, uint64_t const* draw_off, uint64_t total, uint32_t* src, uint32_t* dst)
+gen_batch(kspn_context* ctx, uint32_t count, uint64_t seed, uint64_t const* vtx_off, uint64_t const* draw_off, uint32_t const* ids, uint64_t total, uint32_t* src, uint32_t* dst)
 {
   if (!total || !count) return;
   uint64_t const b = (total + 255) / 256;
-  k_gen_batch<<<static_cast<unsigned>(b < 148ull * 64 ? b : 148ull * 64), 256, 0, ctx->stream>>>(count, seed, vtx_off, draw_off, total, src, dst);
+  k_gen_batch<<<static_cast<unsigned>(b < 148ull * 64 ? b : 148ull * 64), 256, 0, ctx->stream>>>(count, seed, vtx_off, draw_off, ids, total, src, dst);
   KSPN_CHECK_LAUNCH();
   ctx->launches += 1;
 }

@@ -433,7 +433,7 @@ void     manifest_load(kspn_context* ctx, kspn_manifest const& mf, uint64_t* fh,
 void     manifest_write(char const* dir, char const* name, uint32_t n, uint64_t m, uint64_t const* fh, uint32_t const* fc, uint64_t const* bh, uint32_t const* bc, uint32_t head_bytes,
                         uint32_t csr_bytes, int big_endian, int self_loops, int duplicate_edges);
 void     batch_shape(uint32_t count, uint64_t seed, uint32_t log2_min, uint32_t log2_max, float deg_min, float deg_max, uint32_t* n_out, uint64_t* draws_out);
-void     gen_batch(kspn_context* ctx, uint32_t count, uint64_t seed, uint64_t const* vtx_off, uint64_t const* draw_off, uint64_t total_draws, uint32_t* src, uint32_t* dst);
+void     gen_batch(kspn_context* ctx, uint32_t count, uint64_t seed, uint64_t const* vtx_off, uint64_t const* draw_off, uint32_t const* ids, uint64_t total_draws, uint32_t* src, uint32_t* dst);
 void     batch_localize(kspn_context* ctx, uint32_t count, uint64_t N, uint64_t const* vtx_off, uint64_t const* head, uint32_t* csr);
 // trim.cu: k_trim_first's grid = the number of per-block pivot candidates
 unsigned pivot_candidates(uint32_t n);

@@ -132,16 +132,38 @@ class DeviceBatch:
         return b - a, fwh - fwh[0], fwc, bwh - bwh[0], bwc
 
 
+def batch_partition(work: np.ndarray, parts: int) -> list[np.ndarray]:
+    """Greedy longest-processing-time bin packing of graphs (by `work`, e.g.
+    n + edge draws) onto `parts` GPUs: largest first, each to the least
+    loaded part (ties: lowest part).  Deterministic; every rank computes the
+    same assignment.  Returns each part's graph indices, ascending."""
+    order = np.argsort(-np.asarray(work, np.float64), kind="stable")
+    load = np.zeros(parts, np.float64)
+    owner = np.empty(len(order), np.int64)
+    for g in order:
+        p = int(np.argmin(load))
+        owner[g] = p
+        load[p] += float(work[g])
+    return [np.nonzero(owner == p)[0] for p in range(parts)]
+
+
 def batch(ctx: Context, count: int = 4096, seed: int = 5, log2_min: int = 8, log2_max: int = 18, deg_min: float = 0.8, deg_max: float = 6.0,
-          device="cuda") -> DeviceBatch:
+          device="cuda", graphs: "np.ndarray | None" = None) -> DeviceBatch:
     """The uneven G(n, m) mix: graph i has round(2^U[log2_min, log2_max])
     vertices and round(n * U[deg_min, deg_max]) edge draws (self-loops and
-    duplicates removed); all on the device."""
+    duplicates removed); all on the device.  `graphs`: only these graphs of
+    the mix (a shard; each is the same graph the whole mix holds)."""
     import torch
 
     from . import batch_shape
 
     sizes, draws = batch_shape(count, seed, log2_min, log2_max, deg_min, deg_max)
+    ids = None
+    if graphs is not None:
+        graphs = np.asarray(graphs, np.int64)
+        sizes, draws = sizes[graphs], draws[graphs]
+        ids = torch.from_numpy(graphs.astype(np.int32)).to(device)
+        count = len(graphs)
     vtx_off = np.concatenate([[0], np.cumsum(sizes, dtype=np.uint64)]).astype(np.uint64)
     draw_off = np.concatenate([[0], np.cumsum(draws, dtype=np.uint64)]).astype(np.uint64)
     N, D = int(vtx_off[-1]), int(draw_off[-1])
@@ -150,7 +172,7 @@ def batch(ctx: Context, count: int = 4096, seed: int = 5, log2_min: int = 8, log
     src = torch.empty(max(D, 1), dtype=torch.int32, device=device)
     dst = torch.empty(max(D, 1), dtype=torch.int32, device=device)
     torch.cuda.synchronize()
-    ctx.gen_batch(count, seed, d_vo, d_do, src, dst)
+    ctx.gen_batch(count, seed, d_vo, d_do, src, dst, ids)
     G = from_edges(ctx, N, src[:D], dst[:D], device)
     del src, dst
     ctx.batch_localize(count, N, d_vo, G.fwh, G.fwc)
