@@ -45,11 +45,12 @@ WORKLOADS = {
     "rmat26": ("rmat", dict(scale=26, ef=16, seed=4), "R-MAT scale 26, edge factor 16, a,b,c,d=.57,.19,.19,.05, permuted ids"),
     "gnm16": ("gnm", dict(n=1 << 16, draws=1 << 19, seed=1), "directed G(n,m) n=2^16, 2^19 draws"),
     "rmat22": ("rmat", dict(scale=22, ef=16, seed=2), "R-MAT scale 22, edge factor 16, a,b,c,d=.57,.19,.19,.05, permuted ids"),
+    "rmat20": ("rmat", dict(scale=20, ef=16, seed=2), "R-MAT scale 20, edge factor 16, a,b,c,d=.57,.19,.19,.05, permuted ids"),
     "rgg24": ("rgg", dict(n=1 << 24, seed=3), "2D random geometric graph n=2^24, mean undirected degree 8, each pair u->v / v->u / both / neither with p=.25"),
     "rgg20": ("rgg", dict(n=1 << 20, seed=3), "2D random geometric graph n=2^20, mean undirected degree 8, each pair u->v / v->u / both / neither with p=.25"),
 }
 # bounded CPU sample of each workload for the reference arm / cpu_baseline
-CPU_SAMPLE = {"rmat24": "rmat22", "rmat26": "rmat22", "gnm16": "gnm16", "rmat22": "rmat22", "rgg24": "rgg20", "rgg20": "rgg20"}
+CPU_SAMPLE = {"rmat24": "rmat22", "rmat26": "rmat22", "gnm16": "gnm16", "rmat22": "rmat22", "rmat20": "rmat20", "rgg24": "rgg20", "rgg20": "rgg20"}
 
 
 def measured_peak_gbs():
@@ -421,11 +422,13 @@ def run_kspn(args):
         dom = max(agg, key=lambda k: agg[k][0])
         kms, kbytes, kcalls = (x / prof_steps for x in agg[dom])
     achieved = (kbytes / (kms * 1e-3)) / 1e9 if kms > 0 else 0.0
-    traffic = None
+    traffic, traffic_note = None, None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         try:
-            traffic = json.load(open(tp)).get(f"{args.workload}:{dom}")
+            tj = json.load(open(tp))
+            traffic = tj.get(f"{args.workload}:{dom}")
+            traffic_note = tj.get(f"{args.workload}:{dom}:note", "one ncu capture of this workload's launch")
         except Exception:
             traffic = None
     last = step_stats[-1]
@@ -441,7 +444,7 @@ def run_kspn(args):
             "e2e": {"value": m_total / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
+                         "traffic": traffic, "traffic_source": traffic_note, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
                          "bytes_per_step": kbytes, "ms_per_step": kms, "calls_per_step": kcalls,
                          "timing": (f"CUDA events around the {dom} launch on the library stream, every timed step" if res else
                                     f"CUDA events around each {dom} launch on the library stream, {prof_steps} profiled steps after the timed ones"),
