@@ -258,10 +258,29 @@ k_mlp_adam(float* __restrict__ params, float const* __restrict__ grad, float* __
 // largest logit wins.  Ties: smallest id.  Key for atomicMax: bit 63 =
 // accepted, bits 62..32 = the product's float bits (accepted) or the
 // logit's order key >> 1 (not accepted), low word = ~id.
+// The plain pivot first (one warp): when the model accepts it, it is the
+// answer of the rule below (the largest in * out among accepted
+// candidates), so the full scan is skipped (*done = 1).
+__global__ void __launch_bounds__(32)
+k_pivot_check(uint64_t const* __restrict__ pv_prod, uint32_t const* __restrict__ pv_id, uint32_t n, uint64_t const* __restrict__ fh, uint32_t const* __restrict__ fc,
+              uint64_t const* __restrict__ bh, uint32_t const* __restrict__ bc, float const* __restrict__ params, uint32_t* done)
+{
+  __shared__ mlp_smem s;
+  mlp_load(s, params);
+  uint32_t const v = *pv_id;
+  if (*pv_prod == 0 || v >= n) return; // no pivot: the scan decides
+  float f[MLP_IN];
+  mlp_features(v, fh, fc, bh, bc, f);
+  float      h1, h2;
+  float const z = mlp_forward(s, f, h1, h2);
+  if (threadIdx.x == 0 && z >= 0.f) *done = 1u;
+}
+
 __global__ void __launch_bounds__(MLP_WARPS * 32)
 k_pivot_score(uint32_t nb, uint64_t const* __restrict__ cand_prod, uint32_t const* __restrict__ cand_id, uint32_t n, uint64_t const* __restrict__ fh, uint32_t const* __restrict__ fc,
-              uint64_t const* __restrict__ bh, uint32_t const* __restrict__ bc, float const* __restrict__ params, unsigned long long* best)
+              uint64_t const* __restrict__ bh, uint32_t const* __restrict__ bc, float const* __restrict__ params, unsigned long long* best, uint32_t const* done)
 {
+  if (*done) return; // the plain pivot was accepted
   __shared__ mlp_smem s;
   mlp_load(s, params);
   for (uint32_t i = blockIdx.x * MLP_WARPS + (threadIdx.x >> 5); i < nb; i += gridDim.x * MLP_WARPS) {
@@ -280,10 +299,10 @@ k_pivot_score(uint32_t nb, uint64_t const* __restrict__ cand_prod, uint32_t cons
 // The chosen candidate into the pivot slot k_fwbw reads (left as it was
 // when no candidate qualified).
 __global__ void
-k_pivot_pick(unsigned long long const* best, uint64_t* pv_prod, uint32_t* pv_id)
+k_pivot_pick(unsigned long long const* best, uint64_t* pv_prod, uint32_t* pv_id, uint32_t const* done)
 {
   unsigned long long const b = *best;
-  if (b == 0) return;
+  if (*done || b == 0) return;
   *pv_id   = 0xFFFFFFFFu - static_cast<uint32_t>(b & 0xFFFFFFFFu);
   *pv_prod = 1; // any non-zero product: a pivot exists
 }
@@ -347,12 +366,15 @@ learned_pivot(kspn_context* ctx, dgraph const& g, float const* params)
 {
   auto&          ws   = ctx->ws;
   unsigned const nb   = pivot_candidates(g.n);
-  auto*          best = reinterpret_cast<unsigned long long*>(ws.ctr64 + 15);
-  KSPN_CUDA(cudaMemsetAsync(best, 0, sizeof(unsigned long long), ctx->stream));
-  k_pivot_score<<<mlp_grid(nb), MLP_WARPS * 32, 0, ctx->stream>>>(nb, ws.pivot, reinterpret_cast<uint32_t const*>(ws.pivot + 4096), g.n, g.fh, g.fc, g.bh, g.bc, params, best);
-  k_pivot_pick<<<1, 1, 0, ctx->stream>>>(best, ws.pivot + PV_FINAL, reinterpret_cast<uint32_t*>(ws.pivot + 4096) + PV_FINAL);
+  auto*          best = reinterpret_cast<unsigned long long*>(ws.ctr64 + 14); // [14] best key, [15] done flag (low word)
+  auto*          done = reinterpret_cast<uint32_t*>(ws.ctr64 + 15);
+  KSPN_CUDA(cudaMemsetAsync(best, 0, 2 * sizeof(unsigned long long), ctx->stream));
+  uint32_t const* ids = reinterpret_cast<uint32_t const*>(ws.pivot + 4096);
+  k_pivot_check<<<1, 32, 0, ctx->stream>>>(ws.pivot + PV_FINAL, ids + PV_FINAL, g.n, g.fh, g.fc, g.bh, g.bc, params, done);
+  k_pivot_score<<<mlp_grid(nb), MLP_WARPS * 32, 0, ctx->stream>>>(nb, ws.pivot, ids, g.n, g.fh, g.fc, g.bh, g.bc, params, best, done);
+  k_pivot_pick<<<1, 1, 0, ctx->stream>>>(best, ws.pivot + PV_FINAL, reinterpret_cast<uint32_t*>(ws.pivot + 4096) + PV_FINAL, done);
   KSPN_CHECK_LAUNCH();
-  ctx->launches += 2;
+  ctx->launches += 3;
 }
 
 } // namespace kspn
