@@ -343,7 +343,10 @@ typedef struct kspn_batch_options {
     uint32_t reserved0;
     uint64_t cluster_min;  /* with cluster_size > 1: n + m from which a graph gets a cluster
                               instead of one block (0: 2^16) */
-    uint32_t reserved[2];
+    uint32_t search;       /* 0 or 2: FW, then BW inside the FW set; 1: FW and BW searches of a
+                              round at the same time (SCC = their intersection; half the levels,
+                              more work: on C5 3% slower) */
+    uint32_t reserved;
 } kspn_batch_options;
 
 typedef struct kspn_batch_stats {

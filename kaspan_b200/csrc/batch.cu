@@ -67,6 +67,7 @@ struct bt_args
                          // [9] n_medium, [10] medium claimed
   uint32_t        max_rounds; // FW-BW rounds per graph before the serial Tarjan
   uint32_t        rem_tarjan; // remainder size that goes to the shared-memory Tarjan (<= RS_MAXV)
+  uint32_t        joint;      // FW and BW searches at the same time (bt_reach_joint)
 };
 
 __device__ __forceinline__ bool
@@ -142,6 +143,7 @@ k_batch_small(bt_args a)
 struct bt_smem
 {
   uint32_t           g, rem, cnt, minid, lo, hi, flag, pad;
+  uint32_t           lo2, hi2, cnt2, pad2;
   unsigned long long best;
 };
 
@@ -310,6 +312,48 @@ bt_reach(bt_args const& a, bt_graph const& G, bt_group const& g, uint64_t const*
     g.sync();
   }
   uint32_t const c = g.S->cnt;
+  g.sync();
+  return c;
+}
+
+// FW and BW reach from `root` at the same time, both among the undecided
+// vertices (FW over out-rows claiming vis_a into q1, BW over in-rows
+// claiming vis_b into q2), one group barrier per joint level: the SCC is
+// their intersection.  Half the levels of FW then BW on a graph's
+// critical path, for BW also walking vertices outside the FW set.
+// Returns (FW count, BW count).
+__device__ uint2
+bt_reach_joint(bt_args const& a, bt_graph const& G, bt_group const& g, uint32_t root)
+{
+  if (g.leader()) {
+    G.q1[0] = G.q2[0] = root;
+    atomicOr(G.va + (root >> 5), 1u << (root & 31));
+    atomicOr(G.vb + (root >> 5), 1u << (root & 31));
+    g.S->lo = g.S->lo2 = 0;
+    g.S->hi = g.S->hi2 = 1;
+    g.S->cnt = g.S->cnt2 = 1;
+  }
+  g.sync();
+  for (uint32_t lvl = 0;; ++lvl) {
+    uint32_t const lo = g.S->lo, hi = g.S->hi, lo2 = g.S->lo2, hi2 = g.S->hi2;
+    if (lo == hi && lo2 == hi2) break;
+    if (lvl > G.n + 1) {
+      if (g.leader()) atomicExch(a.ctr + 4, 1u);
+      break;
+    }
+    bt_warp_edges(g, G.q1, lo, hi, G.fh, [&](uint32_t, uint64_t e) {
+      uint32_t const w = a.fc[e];
+      if (bt_get(G.und, w) && bit_claim(G.va, w)) G.q1[bt_slot(&g.S->cnt)] = w;
+    });
+    bt_warp_edges(g, G.q2, lo2, hi2, G.bh, [&](uint32_t, uint64_t e) {
+      uint32_t const w = a.bc[e];
+      if (bt_get(G.und, w) && bit_claim(G.vb, w)) G.q2[bt_slot(&g.S->cnt2)] = w;
+    });
+    g.sync();
+    if (g.leader()) g.S->lo = hi, g.S->hi = g.S->cnt, g.S->lo2 = hi2, g.S->hi2 = g.S->cnt2;
+    g.sync();
+  }
+  uint2 const c = make_uint2(g.S->cnt, g.S->cnt2);
   g.sync();
   return c;
 }
@@ -540,19 +584,38 @@ bt_solve(bt_args const& a, uint32_t gi, bt_group const& g, rs_piece& piece)
       if (g.leader()) atomicExch(a.ctr + 4, 1u);
       break;
     }
-    uint32_t const nf = bt_reach(a, G, g, G.fh, a.fc, nullptr, G.va, G.q1, p);
-    uint32_t const nb = bt_reach(a, G, g, G.bh, a.bc, G.va, G.vb, G.q2, p);
-    // the SCC (q2): smallest member, ids, und; vis_a cleared through q1
+    uint32_t nf, nb;
+    uint32_t* scc = G.q2; // the SCC's members
+    if (a.joint) {
+      uint2 const c = bt_reach_joint(a, G, g, p);
+      nf            = c.x;
+      // members: BW-reached vertices also FW-reached, compacted into q0
+      if (g.leader()) g.S->cnt = 0;
+      g.sync();
+      for (uint32_t i = g.gt; i < c.y; i += g.GT) {
+        uint32_t const v = __ldcg(G.q2 + i);
+        if (bt_get(G.va, v)) G.q0[bt_slot(&g.S->cnt)] = v;
+        atomicAnd(G.vb + (v >> 5), ~(1u << (v & 31))); // vis_b cleared through its own list
+      }
+      g.sync();
+      nb  = g.S->cnt;
+      scc = G.q0;
+      g.sync();
+    } else {
+      nf = bt_reach(a, G, g, G.fh, a.fc, nullptr, G.va, G.q1, p);
+      nb = bt_reach(a, G, g, G.bh, a.bc, G.va, G.vb, G.q2, p);
+    }
+    // the SCC: smallest member, ids, und; vis_a cleared through q1
     if (g.leader()) g.S->minid = 0xFFFFFFFFu;
     g.sync();
     uint32_t mn = 0xFFFFFFFFu;
-    for (uint32_t i = g.gt; i < nb; i += g.GT) mn = min(mn, __ldcg(G.q2 + i));
+    for (uint32_t i = g.gt; i < nb; i += g.GT) mn = min(mn, __ldcg(scc + i));
     mn = __reduce_min_sync(0xFFFFFFFFu, mn);
     if ((threadIdx.x & 31) == 0 && mn != 0xFFFFFFFFu) atomicMin(&g.S->minid, mn);
     g.sync();
     uint32_t const id = g.S->minid;
     for (uint32_t i = g.gt; i < nb; i += g.GT) {
-      uint32_t const v = __ldcg(G.q2 + i);
+      uint32_t const v = __ldcg(scc + i);
       G.ids[v]         = id;
       atomicAnd(G.und + (v >> 5), ~(1u << (v & 31)));
       atomicAnd(G.vb + (v >> 5), ~(1u << (v & 31)));
@@ -566,7 +629,7 @@ bt_solve(bt_args const& a, uint32_t gi, bt_group const& g, rs_piece& piece)
     rem -= nb;
     if (rem == 0) break;
     // the SCC's members seed the next trim
-    seed = G.q2;
+    seed = scc;
     qn   = nb;
   }
   g.sync();
@@ -643,6 +706,7 @@ struct batch_cache
   uint64_t        N = 0;
   uint32_t        max_rounds = 0, rem_tarjan = 0, block_blocks = 0, cluster_size = 0, cluster_blocks = 0;
   uint64_t        cluster_min = 0;
+  uint32_t        joint       = 0;
   cudaStream_t    cap_stream = nullptr;
 };
 
@@ -724,6 +788,7 @@ enqueue_batch(kspn_context* ctx, batch_cache& c, bt_args const& a0)
   a.ctr        = p.ctr;
   a.max_rounds = c.max_rounds;
   a.rem_tarjan = c.rem_tarjan;
+  a.joint      = c.joint;
   // large graphs: clusters of c.cluster_size blocks; medium: single blocks
   if (c.cluster_size > 1) {
     cudaLaunchConfig_t   cfg{};
@@ -758,11 +823,12 @@ scc_batched(kspn_context* ctx, uint32_t G, uint64_t N, uint64_t const* vtx_off, 
   uint32_t const csize  = opt.cluster_size ? opt.cluster_size : 1;
   uint64_t const cmin   = csize == 1 ? ~0ull : (opt.cluster_min ? opt.cluster_min : (1ull << 16));
   if (csize > 8) throw error{ KSPN_ERR_INVALID_ARGUMENT, "scc_batched: cluster_size > 8" };
+  uint32_t const joint = opt.search == 1 ? 1u : 0u; // 1: joint searches; 0 (default), 2: FW then BW
   batch_cache*&  cp     = ctx->batch;
   if (!cp) cp = new batch_cache{};
   batch_cache&      c   = *cp;
   void const* const key[6] = { vtx_off, fh, fc, bh, bc, scc_id };
-  bool              same   = c.exec && c.G == G && c.N == N && c.max_rounds == rounds && c.rem_tarjan == rem && c.cluster_size == csize && c.cluster_min == cmin;
+  bool              same   = c.exec && c.G == G && c.N == N && c.max_rounds == rounds && c.rem_tarjan == rem && c.cluster_size == csize && c.cluster_min == cmin && c.joint == joint;
   for (int i = 0; i < 6 && same; ++i) same = c.key[i] == key[i];
   if (!same) {
     if (c.exec) cudaGraphExecDestroy(c.exec), c.exec = nullptr;
@@ -788,7 +854,7 @@ scc_batched(kspn_context* ctx, uint32_t G, uint64_t N, uint64_t const* vtx_off, 
     carve_plan(c.plan, static_cast<char*>(base), G, N, &bytes);
     c.plan.base  = base;
     c.plan.bytes = keep;
-    c.G = G, c.N = N, c.max_rounds = rounds, c.rem_tarjan = rem, c.cluster_size = csize, c.cluster_min = cmin;
+    c.G = G, c.N = N, c.max_rounds = rounds, c.rem_tarjan = rem, c.cluster_size = csize, c.cluster_min = cmin, c.joint = joint;
     for (int i = 0; i < 6; ++i) c.key[i] = key[i];
     int bps = 0, sms = 0;
     KSPN_CUDA(cudaFuncSetAttribute(k_batch_small, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(BS_WARPS * sizeof(rs_piece))));

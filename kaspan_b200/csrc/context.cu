@@ -1083,6 +1083,7 @@ kspn_autotune_batched(kspn_context* ctx, uint32_t count, uint64_t n_total, const
         for (uint64_t cm : { 1ull << 15, 1ull << 17 }) a.push_back([cs, cm](kspn_batch_options& x) { x.cluster_size = cs, x.cluster_min = cm; });
       axes.push_back(a);
     }
+    axes.push_back({ [](kspn_batch_options& x) { x.search = 1; }, [](kspn_batch_options& x) { x.search = 2; } });
     {
       std::vector<S> a;
       for (uint32_t v : { 64u, 256u, 512u }) a.push_back([v](kspn_batch_options& x) { x.rem_tarjan = v; });

@@ -69,15 +69,17 @@ def test_batched_matches_tarjan(ctx, mix):
     assert st2.fwbw_rounds == st.fwbw_rounds
 
 
+@pytest.mark.parametrize("search", [1, 2])
 @pytest.mark.parametrize("cluster_size", [1, 2, 8])
 @pytest.mark.parametrize("max_rounds,rem_tarjan", [(1, 1), (1000, 1), (2, 512), (64, 64)])
-def test_batched_routes(ctx, mix, max_rounds, rem_tarjan, cluster_size):
+def test_batched_routes(ctx, mix, max_rounds, rem_tarjan, cluster_size, search):
     """(1, 1): one FW-BW round, then one thread's Tarjan; (1000, 1): FW-BW
     rounds until nothing is left; the others mix in the shared-memory
     Tarjan of the remainder.  With cluster_size > 1, graphs of n + m >=
-    2000 go to thread-block clusters of that many blocks."""
+    2000 go to thread-block clusters of that many blocks; search 1 runs FW
+    and BW at the same time, 2 one after the other."""
     B, want = mix
-    got, st = _run(ctx, B, max_rounds=max_rounds, rem_tarjan=rem_tarjan, cluster_size=cluster_size, cluster_min=2000)
+    got, st = _run(ctx, B, max_rounds=max_rounds, rem_tarjan=rem_tarjan, cluster_size=cluster_size, cluster_min=2000, search=search)
     assert np.array_equal(got, want)
     assert st.cluster_size == cluster_size
     assert (st.graphs_cluster > 0) == (cluster_size > 1)  # size 1: every larger graph gets a block
@@ -110,7 +112,8 @@ def test_batched_edge_cases(ctx):
     ctx.batch_localize(len(graphs), N, d_vo, G.bwh, G.bwc)
     B = KG.DeviceBatch(len(graphs), N, G.m, d_vo, G.fwh, G.fwc, G.bwh, G.bwc, sizes)
     want = _oracle_ids(B)
-    for opt in ({}, {"max_rounds": 1, "rem_tarjan": 1}, {"cluster_min": 100}, {"cluster_min": 100, "cluster_size": 4, "rem_tarjan": 1}):
+    for opt in ({}, {"max_rounds": 1, "rem_tarjan": 1}, {"cluster_min": 100}, {"cluster_min": 100, "cluster_size": 4, "rem_tarjan": 1},
+                {"search": 2}, {"search": 2, "rem_tarjan": 1}):
         got, _ = _run(ctx, B, **opt)
         assert np.array_equal(got, want)
     # spot checks: the cycle is one SCC named 0, the path all singletons
