@@ -359,7 +359,9 @@ typedef struct kspn_batch_stats {
     float    ms;            /* device time of the call (CUDA events) */
     uint32_t graphs_cluster; /* of the large ones: decomposed by a cluster of blocks */
     uint32_t cluster_size;
-    uint32_t reserved[7];
+    float    phase_ms[5];   /* larger graphs, summed over their groups (group-leader clock):
+                               init, trim, pivot, searches, remainder Tarjan */
+    uint32_t reserved[2];
 } kspn_batch_stats;
 
 void kspn_batch_options_default(kspn_batch_options* opt);

@@ -248,10 +248,13 @@ class BatchStats(C.Structure):
     """kspn_batch_stats (include/kspn.h)."""
     _fields_ = [("graphs_small", C.c_uint32), ("graphs_large", C.c_uint32), ("fwbw_rounds", C.c_uint32),
                 ("tarjan_smem", C.c_uint32), ("tarjan_serial", C.c_uint32), ("trim_levels", C.c_uint32),
-                ("ms", C.c_float), ("graphs_cluster", C.c_uint32), ("cluster_size", C.c_uint32), ("reserved", C.c_uint32 * 7)]
+                ("ms", C.c_float), ("graphs_cluster", C.c_uint32), ("cluster_size", C.c_uint32), ("phase_ms", C.c_float * 5),
+                ("reserved", C.c_uint32 * 2)]
 
     def as_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("reserved", "phase_ms")}
+        d["phase_ms"] = dict(zip(("init", "trim", "pivot", "search", "remainder"), [round(x, 3) for x in self.phase_ms]))
+        return d
 
 
 def batch_shape(count: int, seed: int, log2_min: int = 8, log2_max: int = 18, deg_min: float = 0.8, deg_max: float = 6.0):

@@ -31,6 +31,7 @@
 #include "tarjan_smem.cuh"
 
 #include <cooperative_groups.h>
+#include <cstring>
 
 namespace cg = cooperative_groups;
 
@@ -217,6 +218,25 @@ bt_warp_edges(bt_group const& g, uint32_t const* list, uint32_t lo, uint32_t hi,
   }
 }
 
+// Group-leader clock of the phases of the larger graphs (init, trim,
+// pivot, searches, remainder): %globaltimer deltas summed over all groups
+// into the u64 counters after the u32 ones.
+__device__ __forceinline__ uint64_t
+bt_now()
+{
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void
+bt_phase(bt_args const& a, bt_group const& g, int k, uint64_t& t)
+{
+  if (!g.leader()) return;
+  uint64_t const now = bt_now();
+  atomicAdd(reinterpret_cast<unsigned long long*>(a.ctr + 32) + k, static_cast<unsigned long long>(now - t));
+  t = now;
+}
+
 // One graph's view for the group.
 struct bt_graph
 {
@@ -282,11 +302,19 @@ bt_trim(bt_args const& a, bt_graph const& G, bt_group const& g, uint32_t* qin, u
 }
 
 // Level-synchronous reach from `root` over head/adj rows, among vertices
-// whose bit is set in `cand` (nullptr: among undecided vertices), claiming
-// bits of `mark`; every reached vertex is appended to `list`.  Returns how
-// many were reached.
+// whose bit is set in `cand` (nullptr: among undecided vertices, n_und of
+// them), claiming bits of `mark`; every reached vertex is appended to
+// `list`.  Returns how many were reached.
+// A level whose frontier holds more than 1/BT_BU_DIV of the undecided
+// vertices runs bottom-up: every unreached candidate walks its
+// opposite-direction row (bu_head / bu_adj) until a neighbour in `mark`
+// (reached so far, this level's finds included: reachability does not
+// need BFS levels), and joins.
+constexpr uint32_t BT_BU_DIV = 5; // measured on C5: 1/2 23.1 ms, 1/3 19.2, 1/4 17.7, 1/6 17.7, 1/16 19.6, none 23.3
+
 __device__ uint32_t
-bt_reach(bt_args const& a, bt_graph const& G, bt_group const& g, uint64_t const* head, uint32_t const* adj, uint32_t const* cand, uint32_t* mark, uint32_t* list, uint32_t root)
+bt_reach(bt_args const& a, bt_graph const& G, bt_group const& g, uint64_t const* head, uint32_t const* adj, uint64_t const* bu_head, uint32_t const* bu_adj, uint32_t const* cand,
+         uint32_t* mark, uint32_t* list, uint32_t root, uint32_t n_und)
 {
   if (g.leader()) {
     list[0] = root;
@@ -303,10 +331,24 @@ bt_reach(bt_args const& a, bt_graph const& G, bt_group const& g, uint64_t const*
       if (g.leader()) atomicExch(a.ctr + 4, 1u);
       break;
     }
-    bt_warp_edges(g, list, lo, hi, head, [&](uint32_t, uint64_t e) {
-      uint32_t const w = adj[e];
-      if ((cand ? bt_get(cand, w) : bt_get(G.und, w)) && bit_claim(mark, w)) list[bt_slot(&g.S->cnt)] = w;
-    });
+    if (static_cast<uint64_t>(hi - lo) * BT_BU_DIV > n_und) {
+      for (uint32_t wd = g.gt; wd < G.words; wd += g.GT) {
+        uint32_t cw = (cand ? __ldcg(cand + wd) : __ldcg(G.und + wd)) & ~__ldcg(mark + wd);
+        while (cw) {
+          uint32_t const v = wd * 32 + __ffs(cw) - 1;
+          cw &= cw - 1;
+          for (uint64_t e = bu_head[v], end = bu_head[v + 1]; e < end; ++e)
+            if (bt_get(mark, bu_adj[e])) {
+              if (bit_claim(mark, v)) list[bt_slot(&g.S->cnt)] = v;
+              break;
+            }
+        }
+      }
+    } else
+      bt_warp_edges(g, list, lo, hi, head, [&](uint32_t, uint64_t e) {
+        uint32_t const w = adj[e];
+        if ((cand ? bt_get(cand, w) : bt_get(G.und, w)) && bit_claim(mark, w)) list[bt_slot(&g.S->cnt)] = w;
+      });
     g.sync();
     if (g.leader()) g.S->lo = hi, g.S->hi = g.S->cnt;
     g.sync();
@@ -546,6 +588,7 @@ bt_solve(bt_args const& a, uint32_t gi, bt_group const& g, rs_piece& piece)
   G.q2     = a.q2 + G.vo;
   uint64_t* const pos = a.pos + G.vo;
 
+  uint64_t t = g.leader() ? bt_now() : 0;
   // init: all undecided, live degrees = raw degrees, in/out = 0 decided
   for (uint32_t w = g.gt; w < G.words; w += g.GT) {
     uint32_t const tail = G.n - w * 32;
@@ -570,16 +613,23 @@ bt_solve(bt_args const& a, uint32_t gi, bt_group const& g, rs_piece& piece)
   uint32_t  rem  = G.n - qn;
   uint32_t* seed = G.q0;
   g.sync();
+  bt_phase(a, g, 0, t);
   for (uint32_t round = 0;; ++round) {
     rem -= bt_trim(a, G, g, seed, qn);
+    bt_phase(a, g, 1, t);
     if (rem == 0) break;
-    if (rem <= a.rem_tarjan && bt_tarjan_smem(a, G, g, piece)) break;
+    if (rem <= a.rem_tarjan && bt_tarjan_smem(a, G, g, piece)) {
+      bt_phase(a, g, 4, t);
+      break;
+    }
     if (round >= a.max_rounds) {
       bt_tarjan_serial(a, G, g, pos);
+      bt_phase(a, g, 4, t);
       break;
     }
     // FW-BW from the largest live in * out
     uint32_t const p = bt_pivot(G, g);
+    bt_phase(a, g, 2, t);
     if (p == BT_NONE) {
       if (g.leader()) atomicExch(a.ctr + 4, 1u);
       break;
@@ -602,8 +652,8 @@ bt_solve(bt_args const& a, uint32_t gi, bt_group const& g, rs_piece& piece)
       scc = G.q0;
       g.sync();
     } else {
-      nf = bt_reach(a, G, g, G.fh, a.fc, nullptr, G.va, G.q1, p);
-      nb = bt_reach(a, G, g, G.bh, a.bc, G.va, G.vb, G.q2, p);
+      nf = bt_reach(a, G, g, G.fh, a.fc, G.bh, a.bc, nullptr, G.va, G.q1, p, rem);
+      nb = bt_reach(a, G, g, G.bh, a.bc, G.fh, a.fc, G.va, G.vb, G.q2, p, nf);
     }
     // the SCC: smallest member, ids, und; vis_a cleared through q1
     if (g.leader()) g.S->minid = 0xFFFFFFFFu;
@@ -626,6 +676,7 @@ bt_solve(bt_args const& a, uint32_t gi, bt_group const& g, rs_piece& piece)
     }
     if (g.leader()) atomicAdd(a.ctr + 5, 1u);
     g.sync();
+    bt_phase(a, g, 3, t);
     rem -= nb;
     if (rem == 0) break;
     // the SCC's members seed the next trim
@@ -756,7 +807,7 @@ carve_plan(batch_plan& p, char* base, uint32_t G, uint64_t N, size_t* bytes_out)
   p.q1       = reinterpret_cast<uint32_t*>(take(4 * (N + 1)));
   p.q2       = reinterpret_cast<uint32_t*>(take(4 * (N + 1)));
   p.pos      = reinterpret_cast<uint64_t*>(take(8 * (N + 1)));
-  p.ctr      = reinterpret_cast<uint32_t*>(take(4 * 32));
+  p.ctr      = reinterpret_cast<uint32_t*>(take(4 * 64)); // [32..64): u64 phase times (bt_phase)
   *bytes_out = (off + 255) & ~size_t(255);
 }
 
@@ -767,7 +818,7 @@ enqueue_batch(kspn_context* ctx, batch_cache& c, bt_args const& a0)
   cudaStream_t const s = ctx->stream;
   batch_plan&        p = c.plan;
   uint32_t const     G = c.G;
-  KSPN_CUDA(cudaMemsetAsync(p.ctr, 0, 32 * sizeof(uint32_t), s));
+  KSPN_CUDA(cudaMemsetAsync(p.ctr, 0, 64 * sizeof(uint32_t), s));
   unsigned const cgrid = div_up(G, 256);
   k_bt_classify<<<cgrid < 1 ? 1 : cgrid, 256, 0, s>>>(G, a0.vtx_off, a0.fh, c.cluster_min, p.keys, p.order, p.words, p.ctr);
   KSPN_CHECK_LAUNCH();
@@ -908,7 +959,7 @@ scc_batched(kspn_context* ctx, uint32_t G, uint64_t N, uint64_t const* vtx_off, 
   }
   KSPN_CUDA(cudaGraphLaunch(c.exec, ctx->stream));
   ctx->launches += 1;
-  uint32_t h[32];
+  uint32_t h[64];
   KSPN_CUDA(cudaMemcpyAsync(h, c.plan.ctr, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
   KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
   if (h[4]) throw error{ KSPN_ERR_TIMEOUT, "scc_batched: a level or round bound was reached" };
@@ -921,6 +972,9 @@ scc_batched(kspn_context* ctx, uint32_t G, uint64_t N, uint64_t const* vtx_off, 
     st->tarjan_smem      = h[6];
     st->tarjan_serial    = h[7];
     st->trim_levels      = h[8];
+    uint64_t ph[5];
+    std::memcpy(ph, h + 32, sizeof(ph));
+    for (int k = 0; k < 5; ++k) st->phase_ms[k] = static_cast<float>(ph[k] * 1e-6);
   }
 }
 
