@@ -149,6 +149,13 @@ typedef struct kspn_stats
   uint64_t resident_edges;         /* neighbour ids read */
   uint32_t resident_bitmap_passes; /* passes over a vertex bitmap */
   uint32_t resident_pad;
+  /* Heavy rows (over 2048 entries) in the resident launch: bottom-up rows
+   * cut short and listed, fix-up steps that walked them, and trim vertices
+   * whose heavy rows were counted in slices. */
+  uint32_t heavy_cut_rows;
+  uint32_t heavy_fixups;
+  uint32_t heavy_trim_seeds;
+  uint32_t heavy_pad;
 } kspn_stats;
 
 typedef struct kspn_context kspn_context;

@@ -116,6 +116,10 @@ class Stats(C.Structure):
         ("resident_edges", C.c_uint64),
         ("resident_bitmap_passes", C.c_uint32),
         ("resident_pad", C.c_uint32),
+        ("heavy_cut_rows", C.c_uint32),
+        ("heavy_fixups", C.c_uint32),
+        ("heavy_trim_seeds", C.c_uint32),
+        ("heavy_pad", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -133,6 +137,7 @@ class Stats(C.Structure):
             "label_calls": self.label_calls,
             "rounds": self.rounds,
             "kernel_launches": int(self.kernel_launches),
+            "heavy": {"cut_rows": self.heavy_cut_rows, "fixups": self.heavy_fixups, "trim_seeds": self.heavy_trim_seeds},
             "kernels": {k: {"ms": float(self.kernel_ms[i]), "bytes": int(self.kernel_bytes[i]), "calls": int(self.kernel_calls[i])}
                         for i, k in enumerate(KERNEL_CLASSES)},
             "trace": [{"dir": "bw" if t.backward else "fw", "mode": "bu" if t.bottom_up else "td", "frontier": t.frontier,

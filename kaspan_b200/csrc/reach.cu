@@ -1971,6 +1971,9 @@ fw_bw_trim_result(kspn_context* ctx, dgraph const& g, kspn_options const& opt, k
     st->resident_edges         = edges;
     st->resident_bitmap_passes = passes;
     st->resident_bytes         = 16 * rows + 4 * edges + passes * ((static_cast<uint64_t>(g.n) + 7) / 8) + 4ull * g.n;
+    st->heavy_cut_rows         = hs->cut_n[0] + hs->cut_n[1];
+    st->heavy_fixups           = hs->fixups;
+    st->heavy_trim_seeds       = hs->hseed_n;
   }
   resident_result r;
   r.pivot             = hs->pivot_used;

@@ -1,0 +1,63 @@
+"""Heavy rows (over 2048 entries) in the resident launch, built so that
+every heavy route runs: a hub whose in-row starts with 3000 vertices the
+forward search never reaches and ends with one it does (a bottom-up sweep
+cuts the row short, a fix-up step finds the late neighbour), and hubs
+whose heavy out-rows all end at dead ends (left to the trim tail, which
+counts them in slices).  Output bit-identical to the oracle Tarjan."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import kaspan_b200 as K
+import kaspan_b200.graphs as KG
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _heavy_graph():
+    rng = np.random.default_rng(1)
+    src, dst = [], []
+    C2 = 3000                      # a cycle the pivot never reaches: ids 0..2999
+    src += list(range(C2)); dst += [(i + 1) % C2 for i in range(C2)]
+    H = 5000                       # the hub
+    src += list(range(C2)); dst += [H] * C2            # C2 -> H, first in H's in-row
+    g0, g1 = 6000, 40000           # the giant: a dense random SCC on ids [6000, 40000)
+    n_g = g1 - g0
+    src += list(range(g0, g1)); dst += [g0 + (i + 1) % n_g for i in range(n_g)]   # a Hamiltonian cycle
+    e = 60 * n_g                   # dense: its vertices' in * out beats H's and the decoys'; one of them is the pivot
+    src += list(rng.integers(g0, g1, e)); dst += list(rng.integers(g0, g1, e))
+    src += [g1 - 1]; dst += [H]    # the one reached in-neighbour, last in H's in-row
+    src += [H]; dst += [g0]        # H -> giant: H belongs to the giant SCC
+    # 3 hubs fed by one giant vertex each, with 2100 out-edges to dead ends:
+    # undecided after FW-BW, their heavy out-rows counted in slices by the trim tail
+    n = 60000
+    dead = 44000
+    for d in range(3):
+        hub = 41000 + d
+        src += [g0 + 7 * d]; dst += [hub]
+        src += [hub] * 2100; dst += list(range(dead + d * 2100, dead + (d + 1) * 2100))
+    return n, np.array(src, np.uint32), np.array(dst, np.uint32)
+
+
+def test_heavy_routes_match_tarjan(ctx):
+    import torch
+
+    n, s, d = _heavy_graph()
+    G = KG.from_edges(ctx, n, torch.from_numpy(s.view(np.int32)).cuda(), torch.from_numpy(d.view(np.int32)).cuda())
+    fwh, fwc, bwh, bwc = G.to_host()
+    want = O.tarjan(O.Graph(n, fwh, fwc, bwh, bwc))
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    # bottom-up from the first level on (enter when frontier edges > m_u), so
+    # H's in-row is swept bottom-up before the giant's last vertex is expanded
+    for opt in (K.default_options(validate=0), K.default_options(validate=0, bu_enter_div=1000, bu_leave_div=1)):
+        st = K.Stats()
+        ctx.scc_device(n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, opt, st)
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), want)
+        d_ = st.as_dict()
+        assert d_["heavy"]["cut_rows"] > 0 and d_["heavy"]["trim_seeds"] >= 3
+        assert want[d_["pivot"]] == want[6000]  # the pivot lies in the giant
+    assert d_["heavy"]["fixups"] > 0
+    # H is in the giant SCC
+    assert want[5000] == want[6000]
