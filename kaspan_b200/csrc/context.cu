@@ -528,7 +528,14 @@ tune(T base, std::vector<std::vector<std::function<void(T&)>>> const& axes, Run&
       if (std::memcmp(&c, &cur, sizeof(T)) == 0) continue;
       float const t = run(c);
       ++cand;
-      if (t < 0.98f * t_cur) cur = c, t_cur = t;
+      if (t < 0.98f * t_cur) {
+        // confirm against the incumbent, timed again back to back (one
+        // fast run of a candidate is often noise)
+        float const t_inc = run(cur);
+        float const t_c   = run(c);
+        if (t_c < 0.98f * t_inc) cur = c, t_cur = t_c;
+        else t_cur = std::min(t_cur, t_inc);
+      }
     }
   if (rep) {
     std::memset(rep, 0, sizeof(*rep));
