@@ -457,7 +457,7 @@ def run_kspn(args):
             "phases": {"decided": last["decided"], "ms": {k: round(v, 4) for k, v in last["ms"].items()}, "levels_fw": last["levels_fw"],
                        "levels_bw": last["levels_bw"], "bottom_up": last["levels_bottom_up"], "label_calls": last["label_calls"],
                        "edges_scanned": last["edges_scanned"], "trace": trace,
-                       "search_phase_ms": {{4: "expand", 5: "sweep", 7: "materialize", 8: "init", 9: "end", 10: "finalize", 11: "trim_seed", 12: "trim_level", 13: "worklist", 14: "fix_up", 15: "trim_heavy"}.get(k, k): round(v, 4) for k, v in search_phases.items()},
+                       "search_phase_ms": {{4: "expand", 5: "sweep", 7: "materialize", 8: "init", 9: "end", 10: "finalize", 11: "trim_seed", 12: "trim_level", 13: "worklist", 14: "fix_up", 15: "trim_heavy", 16: "trim_worklist"}.get(k, k): round(v, 4) for k, v in search_phases.items()},
                        "kernels": {k: {"ms": round(a[0] / prof_steps, 4), "GB/s": round(a[1] / (a[0] * 1e-3) / 1e9, 1) if a[0] else 0}
                                                                             for k, a in agg.items()}},
         }

@@ -155,7 +155,7 @@ typedef struct kspn_stats
   uint32_t heavy_cut_rows;
   uint32_t heavy_fixups;
   uint32_t heavy_trim_seeds;
-  uint32_t heavy_pad;
+  uint32_t trim_worklist;   /* 1: the resident trim tail finished on the worklist (long, thin peeling) */
 } kspn_stats;
 
 typedef struct kspn_context kspn_context;

@@ -78,7 +78,7 @@ layout(workspace& ws, char* base, uint32_t n, uint64_t m)
   ws.seed_prefix       = c.take<uint64_t>(4);
   ws.gbar              = c.take<char>(4096);
   ws.heavy_cap         = heavy_capacity(n, m);
-  ws.aw_entries        = nn + 64 + m / HEAVY_SLICE + 32; // every vertex once, every extra slice of a heavy row once
+  ws.aw_entries        = nn + 64 + 2 * (m / HEAVY_SLICE) + 64; // every vertex once, every slice of a heavy row (both directions) once
   ws.aw                = c.take<unsigned long long>(ws.aw_entries);
   ws.rstate            = c.take<char>(4096);
   ws.heavy             = c.take<uint32_t>(4 * ws.heavy_cap);
@@ -337,8 +337,16 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
         uint32_t const pv   = select_pivot_live(ctx, g, und);
         if (pv >= g.n) break;
         uint64_t const d0 = decided;
-        add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pv, opt, st, true));
-        if (decided < g.n) add(KSPN_PHASE_TRIM, trim_fixpoint(ctx, g, und, scc_id, false, 0));
+        if (!ctx->prof && resident_fits(g)) {
+          // one resident launch: FW-BW and the trim fixpoint (its worklist
+          // tail takes long peeling chains without a barrier per level)
+          auto const r = fw_bw_trim(ctx, g, und, scc_id, pv, opt, st);
+          add(KSPN_PHASE_FWBW, r.first);
+          add(KSPN_PHASE_TRIM, r.second);
+        } else {
+          add(KSPN_PHASE_FWBW, fw_bw(ctx, g, und, scc_id, pv, opt, st, true));
+          if (decided < g.n) add(KSPN_PHASE_TRIM, trim_fixpoint(ctx, g, und, scc_id, false, 0));
+        }
         if ((decided - d0) * 64 < left) break;
       }
     };

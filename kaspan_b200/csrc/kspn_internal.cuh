@@ -17,6 +17,7 @@
 
 #include <cstdio>
 #include <string>
+#include <utility>
 
 namespace kspn {
 
@@ -276,7 +277,7 @@ struct workspace
   uint64_t* seed_prefix = nullptr; // 4
   void*     gbar        = nullptr; // 4 KiB: grid barrier of the persistent FW-BW at 0, worklist counters at 1024 (zeroed at creation)
   void*     aw          = nullptr; // aw_entries u64: worklist of the asynchronous search tail (zeroed at creation, zero outside a phase)
-  size_t    aw_entries  = 0;       // n + 66 vertex items + m / HEAVY_SLICE + 32 row-slice items
+  size_t    aw_entries  = 0;       // n + 66 vertex items + 2 m / HEAVY_SLICE + 64 row-slice items
   void*     rstate      = nullptr; // 4 KiB device control blocks (FW-BW at 0, trim at 512, search stamps at 2048)
   uint32_t* heavy       = nullptr; // 4 heavy lists of heavy_cap entries (persistent FW-BW: trim seed, two trim push levels, cut bottom-up rows)
   uint64_t  heavy_cap   = 0;
@@ -417,6 +418,9 @@ struct resident_result
 bool            resident_fits(dgraph const& g);
 void            fw_bw_trim_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, kspn_options const& opt, kspn_stats* st, cudaEvent_t after_kernel);
 resident_result fw_bw_trim_result(kspn_context* ctx, dgraph const& g, kspn_options const& opt, kspn_stats* st);
+// FW-BW from `pivot` and the trim-1 fixpoint of the remainder in one
+// resident launch, ids written as decided; (FW-BW decided, trim decided)
+std::pair<uint32_t, uint32_t> fw_bw_trim(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t pivot, kspn_options const& opt, kspn_stats* st);
 
 uint32_t trim_1_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* queue_out, uint32_t* queue_count_host, bool init_degrees);
 void     trim_1_first_async(kspn_context* ctx, dgraph const& g, uint32_t* und); // ws.ctr zeroed by the caller; writes no ids; no host sync: decided in ws.ctr, pivot in PV_FINAL

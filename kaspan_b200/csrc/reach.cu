@@ -104,6 +104,7 @@ struct reach_state
   uint32_t           hseed_n;      // trim tail: listed vertices with a heavy row
   uint32_t           hq_n[6];      // trim tail: heavy out-/in-rows listed per push level (pairs rotating like lq)
   uint32_t           heavy_err;    // a heavy or cut list would have overflowed
+  uint32_t           trim_async;   // the trim tail finished on the worklist
 };
 
 // phase stamps live after the state: uint32 phase[128], uint64 ns[128]
@@ -1402,6 +1403,153 @@ trim_dead_heavy(fwbw_args const& a, uint32_t hs, uint32_t glvl)
   return dec;
 }
 
+// ---------------------------------------------------------------- trim worklist tail
+// A long, thin trim (peeling chains: thousands of levels of a few vertices
+// each) finishes on the same worklist as the search tail instead of one
+// grid barrier per level.  Items: AW_TAG | v (a decided vertex: push both
+// rows), or AW_TAG | AW_SLICE | dir << 63 | slice << 33 | v (slice `slice`
+// of v's out- (dir 0) or in-row (dir 1), for rows longer than HEAVY_ROW).
+// A warp takes 32 items; per direction its lanes split the edges of the
+// items' rows (warp scan of the lengths), and a neighbour whose live count
+// reaches 0 is decided and appended.  Ends when every appended item is
+// done; every wait is bounded.
+constexpr unsigned long long AW_SLICE = 1ull << 62;
+
+__device__ __forceinline__ void
+aw_push_item(unsigned long long item, bool pred, unsigned long long* aw, unsigned long long* tail, uint64_t cap)
+{
+  unsigned const mask = __ballot_sync(0xFFFFFFFFu, pred);
+  if (!mask) return;
+  unsigned const     lane = threadIdx.x & 31u, leader = __ffs(mask) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(tail, static_cast<unsigned long long>(__popc(mask)));
+  base                = __shfl_sync(0xFFFFFFFFu, base, leader);
+  uint64_t const slot = base + __popc(mask & ((1u << lane) - 1u));
+  if (pred && slot < cap) __stcg(aw + slot, item);
+}
+
+__device__ __forceinline__ int
+run_trim_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, unsigned long long& epoch, uint32_t& dec, uint64_t& edges)
+{
+  unsigned long long* const aw   = a.aw;
+  unsigned long long* const head = a.aq;
+  unsigned long long* const tail = a.aq + 16;
+  unsigned long long* const done = a.aq + 32;
+  uint64_t const            cap  = a.aw_cap;
+  unsigned const            lane = threadIdx.x & 31u;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; i < qn; i += static_cast<uint64_t>(gridDim.x) * R_THREADS) __stcg(aw + i, AW_TAG | __ldcg(fq + i));
+  if (blockIdx.x == 0 && threadIdx.x == 0) *head = 0, *tail = qn, *done = 0;
+  if (!grid_sync(a.bar, epoch)) return SEARCH_FAILED;
+  bool     failed      = false;
+  uint32_t unpublished = 0;
+  for (bool alive = true; alive;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(head, 32ull);
+    base                = __shfl_sync(0xFFFFFFFFu, base, 0);
+    uint64_t const slot = base + lane;
+    bool           pending = true;
+    unsigned       spins   = 0;
+    while (__any_sync(0xFFFFFFFFu, pending)) {
+      bool               got  = false;
+      unsigned long long item = 0;
+      if (pending && slot < cap) {
+        item = ld_acquire64(aw + slot);
+        if (item & AW_TAG) got = true, pending = false;
+      }
+      unsigned const gmask = __ballot_sync(0xFFFFFFFFu, got);
+      if (gmask) {
+        uint32_t const v = static_cast<uint32_t>(item);
+#pragma unroll 1
+        for (int dir = 0; dir < 2; ++dir) {
+          uint64_t const* hd  = dir ? a.bh : a.fh;
+          uint32_t const* adj = dir ? a.bc : a.fc;
+          uint32_t* const deg = dir ? a.outdeg : a.indeg;
+          uint64_t        b = 0, e = 0;
+          if (got) {
+            bool const is_slice = (item & AW_SLICE) != 0;
+            if (!is_slice || static_cast<int>(item >> 63) == dir) {
+              b = hd[v], e = hd[v + 1];
+              if (is_slice) {
+                b += static_cast<uint64_t>((item >> 33) & 0x1FFFFFFFull) * HEAVY_SLICE;
+                e = b + HEAVY_SLICE < e ? b + HEAVY_SLICE : e;
+              } else if (e - b > HEAVY_ROW) {
+                // a heavy row: its slices become items of their own
+                uint64_t const           ns = (e - b + HEAVY_SLICE - 1) / HEAVY_SLICE;
+                unsigned long long const at = atomicAdd(tail, static_cast<unsigned long long>(ns));
+                for (uint64_t j = 0; j < ns; ++j)
+                  if (at + j < cap) __stcg(aw + at + j, AW_TAG | AW_SLICE | (static_cast<unsigned long long>(dir) << 63) | (static_cast<unsigned long long>(j) << 33) | v);
+                e = b; // nothing walked here
+              }
+            }
+          }
+          edges += e - b;
+          // the lanes' rows split over the warp (warp scan of the lengths)
+          uint32_t const d    = static_cast<uint32_t>(e - b);
+          uint32_t       incl = d;
+#pragma unroll
+          for (int sh = 1; sh < 32; sh <<= 1) {
+            uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, incl, sh);
+            if (lane >= static_cast<unsigned>(sh)) incl += y;
+          }
+          uint32_t const total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+          uint32_t const excl  = incl - d;
+          for (uint32_t kb = 0; kb < total; kb += 32) {
+            uint32_t const k = kb + lane;
+            uint32_t       j = 0;
+#pragma unroll
+            for (int step = 16; step; step >>= 1) {
+              uint32_t const ex = __shfl_sync(0xFFFFFFFFu, excl, j + step);
+              if (ex <= k) j += step;
+            }
+            uint64_t const bj   = __shfl_sync(0xFFFFFFFFu, b, j);
+            uint32_t const xj   = __shfl_sync(0xFFFFFFFFu, excl, j);
+            bool           take = false;
+            uint32_t       w    = 0;
+            if (k < total) {
+              w    = adj[bj + (k - xj)];
+              take = ((__ldcg(a.und + (w >> 5)) >> (w & 31)) & 1u) && atomicSub(deg + w, 1u) == 1u && bit_take(a.und, w);
+              if (take) {
+                if (!a.ids_at_end) a.scc_id[w] = w;
+                ++dec;
+              }
+            }
+            aw_push_item(AW_TAG | w, take, aw, tail, cap);
+          }
+        }
+        unpublished += __popc(gmask);
+        spins = 0;
+      } else {
+        if (unpublished) {
+          __threadfence();
+          if (lane == 0) atomicAdd(done, static_cast<unsigned long long>(unpublished));
+          unpublished = 0;
+        }
+        uint32_t stop = 0;
+        if (lane == 0) {
+          unsigned long long const dn = ld_acquire64(done);
+          unsigned long long const t  = ld_acquire64(tail);
+          stop                        = dn == t ? 1u : 0u;
+          if (!stop && (++spins > GRID_SYNC_SPINS || ((spins & 63u) == 63u && ld_acquire(&a.bar->err)))) {
+            atomicExch(&a.bar->err, 1u);
+            stop = 2;
+          }
+        }
+        stop = __shfl_sync(0xFFFFFFFFu, stop, 0);
+        if (stop) {
+          pending = false;
+          alive   = false;
+          failed  = stop == 2;
+        } else __nanosleep(64);
+      }
+    }
+  }
+  if (!grid_sync(a.bar, epoch) || failed) return SEARCH_FAILED;
+  uint64_t t = __ldcg(tail);
+  t          = t < cap ? t : cap;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; i < t; i += static_cast<uint64_t>(gridDim.x) * R_THREADS) __stcg(aw + i, 0ull);
+  return SEARCH_DONE;
+}
+
 // The trim fixpoint; levels continue the launch's numbering (glvl).
 __device__ __forceinline__ int
 run_trim(fwbw_args const& a, uint32_t& glvl, unsigned long long& epoch)
@@ -1431,6 +1579,15 @@ run_trim(fwbw_args const& a, uint32_t& glvl, unsigned long long& epoch)
     if (qn == 0 && !first && __ldcg(&st->hq_n[2 * (glvl % 3)]) == 0 && __ldcg(&st->hq_n[2 * (glvl % 3) + 1]) == 0) break;
     if (lvl >= a.cap || qn > a.n) {
       rc = SEARCH_CAPPED;
+      break;
+    }
+    if (lvl >= ASYNC_AFTER && qn <= ASYNC_FRONTIER && a.aw && !first && __ldcg(&st->hq_n[2 * (glvl % 3)]) == 0 && __ldcg(&st->hq_n[2 * (glvl % 3) + 1]) == 0) {
+      // long and thin: the rest of the fixpoint on the worklist (no heavy
+      // rows are pending from the level before)
+      rc = run_trim_async(a, a.fb[glvl & 1].q, static_cast<uint32_t>(qn), epoch, dec, edges);
+      stamp(a, 16);
+      if (blockIdx.x == 0 && threadIdx.x == 0) st->trim_async = 1;
+      ++lvl;
       break;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) st->lq[(glvl + 2) % 3] = 0, st->hq_n[2 * ((glvl + 2) % 3)] = st->hq_n[2 * ((glvl + 2) % 3) + 1] = 0;
@@ -1516,7 +1673,7 @@ k_fwbw(fwbw_args a)
     st->mats = st->bu_bitmap    = 0;
     st->async_phases            = 0;
     st->cut_n[0] = st->cut_n[1] = st->fixups = 0;
-    st->hseed_n = st->heavy_err = 0;
+    st->hseed_n = st->heavy_err = st->trim_async = 0;
     for (int i = 0; i < 6; ++i) st->hq_n[i] = 0;
     if (search) a.seed.q[0] = p, a.seed.prefix[0] = 0;
   }
@@ -1836,7 +1993,7 @@ namespace {
 // caller synchronises, then calls check_persistent.
 void
 launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t pivot, bool trim, kspn_options const& opt, kspn_stats* st, bool min_ids,
-                  cudaEvent_t after_kernel = nullptr)
+                  cudaEvent_t after_kernel = nullptr, bool ids_at_end = true)
 {
   auto&       ws   = ctx->ws;
   auto* const rs   = reinterpret_cast<reach_state*>(ws.rstate);
@@ -1870,7 +2027,7 @@ launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* s
   a.pv_prod     = ws.pivot + PV_FINAL;
   a.pv_id       = reinterpret_cast<uint32_t const*>(ws.pivot + 4096) + PV_FINAL;
   a.trim        = trim ? 1u : 0u;
-  a.ids_at_end  = trim ? 1u : 0u;
+  a.ids_at_end  = trim && ids_at_end ? 1u : 0u;
   a.aw          = static_cast<unsigned long long*>(ws.aw);
   a.aw_cap      = ws.aw_entries;
   a.aq          = reinterpret_cast<unsigned long long*>(static_cast<char*>(ws.gbar) + 1024);
@@ -1974,6 +2131,7 @@ fw_bw_trim_result(kspn_context* ctx, dgraph const& g, kspn_options const& opt, k
     st->heavy_cut_rows         = hs->cut_n[0] + hs->cut_n[1];
     st->heavy_fixups           = hs->fixups;
     st->heavy_trim_seeds       = hs->hseed_n;
+    st->trim_worklist          = hs->trim_async;
   }
   resident_result r;
   r.pivot             = hs->pivot_used;
@@ -1984,6 +2142,19 @@ fw_bw_trim_result(kspn_context* ctx, dgraph const& g, kspn_options const& opt, k
   uint64_t const span = hs->t_ns[2] > hs->t_ns[0] ? hs->t_ns[2] - hs->t_ns[0] : 0;
   r.fwbw_share        = span ? static_cast<double>(hs->t_ns[1] - hs->t_ns[0]) / static_cast<double>(span) : 1.0;
   return r;
+}
+
+std::pair<uint32_t, uint32_t>
+fw_bw_trim(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t pivot, kspn_options const& opt, kspn_stats* st)
+{
+  if (pivot >= g.n) throw error{ KSPN_ERR_INVALID_ARGUMENT, "fw_bw_trim: pivot >= n" };
+  launch_persistent(ctx, g, und, scc_id, pivot, true, opt, st, true, nullptr, false);
+  KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+  check_persistent(ctx);
+  auto* hs = reinterpret_cast<reach_state*>(ctx->h_state);
+  record_search_stats(ctx, opt, st);
+  ctx->h_ctr64[0] += hs->trim_edges;
+  return { hs->decided, hs->trim_decided };
 }
 
 uint32_t

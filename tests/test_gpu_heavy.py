@@ -61,3 +61,43 @@ def test_heavy_routes_match_tarjan(ctx):
     assert d_["heavy"]["fixups"] > 0
     # H is in the giant SCC
     assert want[5000] == want[6000]
+
+
+def _chain_graph():
+    """A giant random SCC, chains of 3000 vertices into it and out of it
+    (the trim tail peels them one vertex per level), and a chain vertex with
+    2500 out-edges to dead ends (a heavy row inside the peeling)."""
+    rng = np.random.default_rng(2)
+    src, dst = [], []
+    g0, g1 = 0, 20000
+    n_g = g1 - g0
+    src += list(range(g0, g1)); dst += [g0 + (i + 1) % n_g for i in range(n_g)]
+    e = 20 * n_g
+    src += list(rng.integers(g0, g1, e)); dst += list(rng.integers(g0, g1, e))
+    nxt = g1
+    for c in range(4):
+        L = 3000
+        ch = list(range(nxt, nxt + L)); nxt += L
+        if c % 2 == 0:       # into the giant: ch[0] -> ch[1] -> ... -> giant
+            src += ch[:-1]; dst += ch[1:]; src += [ch[-1]]; dst += [g0 + c]
+        else:                # out of the giant: giant -> ch[0] -> ... -> ch[-1]
+            src += [g0 + c]; dst += [ch[0]]; src += ch[:-1]; dst += ch[1:]
+        if c == 0:           # a heavy vertex in the middle of the first chain
+            hv = ch[L // 2]
+            src += [hv] * 2500; dst += list(range(nxt, nxt + 2500)); nxt += 2500
+    return nxt, np.array(src, np.uint32), np.array(dst, np.uint32)
+
+
+def test_trim_worklist_tail(ctx):
+    import torch
+
+    n, s, d = _chain_graph()
+    G = KG.from_edges(ctx, n, torch.from_numpy(s.view(np.int32)).cuda(), torch.from_numpy(d.view(np.int32)).cuda())
+    fwh, fwc, bwh, bwc = G.to_host()
+    want = O.tarjan(O.Graph(n, fwh, fwc, bwh, bwc))
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    st = K.Stats()
+    for _ in range(2):  # a second call reuses the (all-zero) worklist
+        ctx.scc_device(n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, K.default_options(validate=0), st)
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), want)
+        assert st.as_dict()["trim_worklist"] == 1
