@@ -129,39 +129,62 @@ heavy_capacity(uint32_t n, uint64_t m)
   return (c < 2ull * n ? c : 2ull * n) + 32;
 }
 
-// fn(i, v, b, e) for the slices of the listed rows that fall to this warp
-// (slice s of entry i goes to warp (i + s) mod W of the grid's W warps);
-// [b, e) is one slice of v's row in `head`.  HEAVY_ONLY: rows of at most
-// HEAVY_ROW entries are skipped (their owner walks them).  All lanes of
-// every warp call it; fn is called warp-uniformly.  Entries are read
-// through L2 (the list was written by other blocks of the same launch).
+// fn(i, v, b, e) for the slices of the listed rows that fall to this warp:
+// the slices of the whole list are numbered in list order (entry i's slices
+// follow entry i-1's) and global slice g goes to warp g mod W of the grid's
+// W warps; [b, e) is one slice of v's row in `head`.  HEAVY_ONLY: rows of at
+// most HEAVY_ROW entries are skipped (their owner walks them).  All lanes of
+// every warp call it; fn is called warp-uniformly.  A warp reads the list
+// HS_BATCHES x 32 entries at a time (independent loads), numbers the
+// batch's slices with a warp scan and finds the entry of each slice it owns
+// with a ballot, so its cost is count / 32 scan steps plus its own slices.
+// Entries are read through L2 (the list was written by other blocks of the
+// same launch).
+constexpr uint32_t HS_BATCHES = 2;
+
 template<bool HEAVY_ONLY = false, class F>
 __device__ __forceinline__ void
 heavy_slices(uint32_t const* list, uint32_t count, uint64_t const* __restrict__ head, F&& fn)
 {
   unsigned const lane = threadIdx.x & 31u;
   uint32_t const W    = gridDim.x * (blockDim.x >> 5);
-  uint32_t const gw   = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  for (uint32_t base = 0; base < count; base += 32) {
-    uint32_t const i = base + lane;
-    uint32_t       v = 0;
-    uint64_t       b = 0, e = 0;
-    if (i < count) {
-      v = __ldcg(list + i);
-      b = head[v];
-      e = head[v + 1];
+  // offset of this warp's next slice from the start of the current batch
+  uint64_t nxt = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  for (uint32_t base = 0; base < count; base += 32 * HS_BATCHES) {
+    uint32_t v[HS_BATCHES];
+    uint64_t b[HS_BATCHES], e[HS_BATCHES];
+#pragma unroll
+    for (uint32_t k = 0; k < HS_BATCHES; ++k) {
+      uint32_t const i = base + 32 * k + lane;
+      v[k]             = i < count ? __ldcg(list + i) : 0u;
     }
-    uint32_t const k = count - base < 32 ? count - base : 32;
-    for (uint32_t j = 0; j < k; ++j) {
-      uint32_t const vj = __shfl_sync(0xFFFFFFFFu, v, j);
-      uint64_t const bj = __shfl_sync(0xFFFFFFFFu, b, j), ej = __shfl_sync(0xFFFFFFFFu, e, j);
-      if (HEAVY_ONLY && ej - bj <= HEAVY_ROW) continue;
-      uint64_t const ns = (ej - bj + HEAVY_SLICE - 1) / HEAVY_SLICE;
-      uint32_t const r  = (base + j) % W;
-      for (uint64_t sl = (gw + W - r) % W; sl < ns; sl += W) {
-        uint64_t const sb = bj + sl * HEAVY_SLICE;
-        fn(base + j, vj, sb, sb + HEAVY_SLICE < ej ? sb + HEAVY_SLICE : ej);
+#pragma unroll
+    for (uint32_t k = 0; k < HS_BATCHES; ++k) {
+      bool const in = base + 32 * k + lane < count;
+      b[k]          = in ? head[v[k]] : 0ull;
+      e[k]          = in ? head[v[k] + 1] : 0ull;
+    }
+#pragma unroll
+    for (uint32_t k = 0; k < HS_BATCHES; ++k) {
+      uint64_t const len = e[k] - b[k];
+      uint32_t const ns  = HEAVY_ONLY && len <= HEAVY_ROW ? 0u : static_cast<uint32_t>((len + HEAVY_SLICE - 1) / HEAVY_SLICE);
+      uint32_t       inc = ns; // inclusive scan of the batch's slice counts
+#pragma unroll
+      for (unsigned sh = 1; sh < 32; sh <<= 1) {
+        uint32_t const t = __shfl_up_sync(0xFFFFFFFFu, inc, sh);
+        if (lane >= sh) inc += t;
       }
+      uint32_t const total = __shfl_sync(0xFFFFFFFFu, inc, 31);
+      for (; nxt < total; nxt += W) {
+        uint32_t const o  = static_cast<uint32_t>(nxt);
+        unsigned const j  = __popc(__ballot_sync(0xFFFFFFFFu, inc <= o)); // entry holding slice o
+        uint32_t const vj = __shfl_sync(0xFFFFFFFFu, v[k], j);
+        uint64_t const bj = __shfl_sync(0xFFFFFFFFu, b[k], j), ej = __shfl_sync(0xFFFFFFFFu, e[k], j);
+        uint32_t const s  = o - __shfl_sync(0xFFFFFFFFu, inc - ns, j);
+        uint64_t const sb = bj + static_cast<uint64_t>(s) * HEAVY_SLICE;
+        fn(base + 32 * k + j, vj, sb, sb + HEAVY_SLICE < ej ? sb + HEAVY_SLICE : ej);
+      }
+      nxt -= total;
     }
   }
 }
