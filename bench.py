@@ -262,7 +262,11 @@ def run_kspn(args):
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    stream = torch.cuda.current_stream()
+    # one stream for the context's kernels, torch's work and the timing
+    # events (the legacy default stream's handle is 0, which the context
+    # would read as "make your own")
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
     ctx = K.Context(local, stream=stream)
     G = make_graph(ctx, args.workload, rank_seed=rank)
     torch.cuda.synchronize()

@@ -298,6 +298,23 @@ int kspn_transpose(kspn_context* ctx, uint32_t n, uint64_t m,
                    const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
                    uint64_t* d_bw_head, uint32_t* d_bw_csr);
 
+/* Upload of a host CSR with its transpose built on the device while the
+ * upload runs (what kspn_scc does when bw_head / bw_csr are NULL; the input
+ * preparation the reference's graph adapters end with,
+ * backward_complement_graph_part in kaspan/scc/adapter/kagen.hpp:38).
+ * Host fw_head[n+1] / fw_csr[m]
+ * are copied to d_fw_head / d_fw_csr in chunks of chunk_edges edges
+ * (0 = 8 Mi) on the context's copy stream; as each chunk arrives its
+ * (target, source) pairs are sorted on the context's stream, and after the
+ * last one d_bw_head / d_bw_csr receive the transpose, rows ascending (the
+ * same arrays as kspn_transpose).  Pinned host memory overlaps the copy
+ * with the sorting.  m must be below 2^32 - 1; fw_head[0] != 0 or
+ * fw_head[n] != m is KSPN_ERR_INVALID_GRAPH.  Returns after both are done. */
+int kspn_upload_transpose(kspn_context* ctx, uint32_t n, uint64_t m,
+                          const uint64_t* fw_head, const uint32_t* fw_csr,
+                          uint64_t* d_fw_head, uint32_t* d_fw_csr,
+                          uint64_t* d_bw_head, uint32_t* d_bw_csr, uint64_t chunk_edges);
+
 /* ---------------------------------------------------------------- learned pivot
  * No reference counterpart.  An MLP 8 -> 32 -> 32 -> 1 (ReLU; BF16-rounded
  * weights, FP32 accumulation) scores pivot candidates by the odds that they

@@ -189,6 +189,7 @@ SIGNATURES = {
     "kspn_normalise": (_i32, [_P, _u32, _P]),
     "kspn_normalise_noalloc": (_i32, [_u32, _P, _P]),
     "kspn_transpose": (_i32, [_P, _u32, _u64, _P, _P, _P, _P]),
+    "kspn_upload_transpose": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _u64]),
     "kspn_gen_gnm": (_i32, [_P, _u32, _u64, _u64, _P, _P]),
     "kspn_gen_rmat": (_i32, [_P, _i32, _u64, _u64, _u64, _u64, _u64, _i32, _P, _P]),
     "kspn_gen_rgg": (_i32, [_P, _u32, _u64, _u32, _u64, _P, _P, _u64, _P]),
@@ -461,6 +462,12 @@ class Context:
 
     def transpose(self, n, m, fwh, fwc, bwh, bwc):
         self._check(lib().kspn_transpose(self.h, n, m, _ptr(fwh), _ptr(fwc), _ptr(bwh), _ptr(bwc)), "transpose")
+
+    def upload_transpose(self, n, m, fwh_host, fwc_host, fwh, fwc, bwh, bwc, chunk_edges=0):
+        """Host CSR (pinned torch tensors or numpy) -> device CSR + CSC, the
+        CSC sorted chunk by chunk while the upload runs."""
+        self._check(lib().kspn_upload_transpose(self.h, n, m, _ptr(fwh_host), _ptr(fwc_host), _ptr(fwh), _ptr(fwc),
+                                                _ptr(bwh), _ptr(bwc), int(chunk_edges)), "upload_transpose")
 
     # ---- inputs
     def gen_gnm(self, n, draws, seed, src, dst):

@@ -700,6 +700,8 @@ kspn_context_destroy(kspn_context* ctx)
     if (e) cudaEventDestroy(e);
   for (auto& e : ctx->pe)
     if (e) cudaEventDestroy(e);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream), cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->copy_ev) cudaEventDestroy(ctx->copy_ev);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return KSPN_OK;
@@ -760,13 +762,14 @@ kspn_scc(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* fw_head, con
     auto* dfc = reinterpret_cast<uint32_t*>(p + 2 * head_b);
     auto* dbc = reinterpret_cast<uint32_t*>(p + 2 * head_b + csr_b);
     auto* dout = reinterpret_cast<uint32_t*>(p + 2 * head_b + 2 * csr_b);
-    KSPN_CUDA(cudaMemcpyAsync(dfh, fw_head, (static_cast<size_t>(n) + 1) * 8, cudaMemcpyHostToDevice, s));
-    if (m) KSPN_CUDA(cudaMemcpyAsync(dfc, fw_csr, m * 4, cudaMemcpyHostToDevice, s));
     if (has_bw) {
+      KSPN_CUDA(cudaMemcpyAsync(dfh, fw_head, (static_cast<size_t>(n) + 1) * 8, cudaMemcpyHostToDevice, s));
+      if (m) KSPN_CUDA(cudaMemcpyAsync(dfc, fw_csr, m * 4, cudaMemcpyHostToDevice, s));
       KSPN_CUDA(cudaMemcpyAsync(dbh, bw_head, (static_cast<size_t>(n) + 1) * 8, cudaMemcpyHostToDevice, s));
       if (m) KSPN_CUDA(cudaMemcpyAsync(dbc, bw_csr, m * 4, cudaMemcpyHostToDevice, s));
     } else {
-      transpose(ctx, n, m, dfh, dfc, dbh, dbc, nullptr);
+      // the CSC is built while the CSR is still arriving
+      upload_transpose(ctx, n, m, fw_head, fw_csr, dfh, dfc, dbh, dbc, 0);
     }
     dgraph const g{ n, m, dfh, dfc, dbh, dbc };
     run_pipeline(ctx, g, dout, o, stats);
@@ -1211,6 +1214,19 @@ kspn_transpose(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* d_fw_h
     require(d_fw_head && d_bw_head && (m == 0 || (d_fw_csr && d_bw_csr)), "null pointer");
     bind_device(ctx);
     transpose(ctx, n, m, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr, nullptr);
+  });
+}
+
+int
+kspn_upload_transpose(kspn_context* ctx, uint32_t n, uint64_t m, const uint64_t* fw_head, const uint32_t* fw_csr, uint64_t* d_fw_head, uint32_t* d_fw_csr, uint64_t* d_bw_head, uint32_t* d_bw_csr, uint64_t chunk_edges)
+{
+  if (!ctx) return KSPN_ERR_INVALID_ARGUMENT;
+  return guard(ctx, [&] {
+    require(fw_head && d_fw_head && d_bw_head && (m == 0 || (fw_csr && d_fw_csr && d_bw_csr)), "null pointer");
+    require(n < UNDECIDED, "n must be below 2^32 - 1");
+    bind_device(ctx);
+    upload_transpose(ctx, n, m, fw_head, fw_csr, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr, chunk_edges);
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
   });
 }
 

@@ -8,6 +8,8 @@
 //  * validate: monotone offsets, head[0] == 0, head[n] == m, ids < n.
 #include "prim.cuh"
 
+#include <algorithm>
+
 namespace kspn {
 
 namespace {
@@ -46,8 +48,10 @@ k_heads_from_sorted(uint32_t n, uint64_t m, uint32_t const* __restrict__ keys, u
 {
   uint64_t const stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i <= m; i += stride) {
-    int64_t const lo = i == 0 ? -1 : static_cast<int64_t>(keys[i - 1]);
-    int64_t const hi = i == m ? static_cast<int64_t>(n) : static_cast<int64_t>(keys[i]);
+    // ids >= n (an invalid graph, reported by validation afterwards) are
+    // clamped so that no head beyond n is written
+    int64_t const lo = i == 0 ? -1 : static_cast<int64_t>(min(keys[i - 1], n));
+    int64_t const hi = i == m ? static_cast<int64_t>(n) : static_cast<int64_t>(min(keys[i], n));
     for (int64_t v = lo + 1; v <= hi; ++v) head[v] = i;
   }
 }
@@ -85,6 +89,134 @@ k_validate(uint32_t n, uint64_t m, uint64_t const* __restrict__ head, uint32_t c
   if (blockIdx.x == 0 && threadIdx.x == 0 && (head[0] != 0 || head[n] != m)) atomicOr(err, 2u);
   for (uint64_t e = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < m; e += stride)
     if (csr[e] >= n) atomicOr(err, 4u);
+}
+
+// src[e - e0] = u for the edges e in [e0, e1) of rows [u_lo, u_hi) (rows
+// clipped to the range).  Small rows by their own lane, rows of 64+
+// entries by the whole warp.
+__global__ void
+k_expand_range(uint32_t u_lo, uint32_t u_hi, uint64_t const* __restrict__ head, uint64_t e0, uint64_t e1, uint32_t* __restrict__ src)
+{
+  uint64_t const tid   = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  unsigned const lane  = threadIdx.x & 31u;
+  uint64_t const wbase = u_lo + tid - lane;
+  if (wbase >= u_hi) return;
+  uint64_t const uu  = u_lo + tid;
+  bool const     ok  = uu < u_hi;
+  uint64_t       beg = ok ? head[uu] : 0, end = ok ? head[uu + 1] : 0;
+  beg                = beg < e0 ? e0 : beg;
+  end                = end > e1 ? e1 : end;
+  end                = end < beg ? beg : end;
+  bool const big = (end - beg) >= 64;
+  if (!big)
+    for (uint64_t e = beg; e < end; ++e) src[e - e0] = static_cast<uint32_t>(uu);
+  for (unsigned todo = __ballot_sync(0xFFFFFFFFu, big); todo; todo &= todo - 1) {
+    unsigned const l  = __ffs(todo) - 1;
+    uint64_t const b  = __shfl_sync(0xFFFFFFFFu, beg, l);
+    uint64_t const e_ = __shfl_sync(0xFFFFFFFFu, end, l);
+    uint32_t const u  = static_cast<uint32_t>(wbase + l);
+    for (uint64_t e = b + lane; e < e_; e += 32) src[e - e0] = u;
+  }
+}
+
+// Runs of equal keys in one sorted chunk (keys = targets, in CSR order
+// inside a key): first[v] = chunk index of v's first entry.
+__global__ void
+k_run_first(uint32_t n, uint32_t const* __restrict__ keys, uint32_t cnt, uint32_t* __restrict__ first)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x)
+    if (keys[i] < n && (i == 0 || keys[i - 1] != keys[i])) first[keys[i]] = i;
+}
+
+// off[i] = v's entries placed by earlier chunks + i's rank in its run: the
+// entry's offset inside v's CSC row.
+__global__ void
+k_run_off(uint32_t n, uint32_t const* __restrict__ keys, uint32_t cnt, uint32_t const* __restrict__ first, uint32_t const* __restrict__ indeg, uint32_t* __restrict__ off)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+    uint32_t const v = keys[i];
+    if (v < n) off[i] = indeg[v] + (i - first[v]);
+  }
+}
+
+// indeg[v] += the run's length, at each run's last entry
+__global__ void
+k_run_advance(uint32_t n, uint32_t const* __restrict__ keys, uint32_t cnt, uint32_t const* __restrict__ first, uint32_t* __restrict__ indeg)
+{
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+    uint32_t const v = keys[i];
+    if (v < n && (i + 1 == cnt || keys[i + 1] != v)) indeg[v] += i - first[v] + 1;
+  }
+}
+
+// Placement in bands: band b holds the vertices [bv[b], bv[b+1]) whose CSC
+// rows fill about 1/nb of bc; bv[b] = first vertex whose head reaches
+// b * m / nb.
+__global__ void
+k_band_vertices(uint32_t n, uint64_t m, uint64_t const* __restrict__ head, uint32_t nb, uint32_t* __restrict__ bv)
+{
+  uint32_t const b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b > nb) return;
+  uint64_t const target = b == nb ? m + 1 : (m / nb) * b + (m % nb) * b / nb;
+  uint32_t       lo = 0, hi = n; // first v in [0, n] with head[v] >= target (n if none)
+  while (lo < hi) {
+    uint32_t const mid = lo + (hi - lo) / 2;
+    if (head[mid] >= target) hi = mid;
+    else lo = mid + 1;
+  }
+  bv[b] = b == 0 ? 0u : (b == nb ? n : lo);
+}
+
+// seg[b * nc + c] = first entry of sorted chunk c with key >= bv[b]
+__global__ void
+k_band_segments(uint32_t const* __restrict__ skeys, uint64_t m, uint64_t chunk, uint32_t nc, uint32_t nb, uint32_t const* __restrict__ bv, uint32_t* __restrict__ seg)
+{
+  uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (nb + 1) * nc) return;
+  uint32_t const  b = t / nc, c = t % nc;
+  uint64_t const  e0  = c * chunk;
+  uint32_t const  cnt = static_cast<uint32_t>((e0 + chunk < m ? e0 + chunk : m) - e0);
+  uint32_t const* k   = skeys + e0;
+  uint32_t const  key = bv[b];
+  uint32_t        lo = 0, hi = cnt;
+  while (lo < hi) {
+    uint32_t const mid = lo + (hi - lo) / 2;
+    if (k[mid] >= key) hi = mid;
+    else lo = mid + 1;
+  }
+  seg[t] = b == nb ? cnt : lo;
+}
+
+// bc[head[v] + off[i]] = source of entry i.  A neighbour id >= n (an
+// invalid graph, which validation reports afterwards) splits runs, so
+// positions are bounded here instead of trusted.
+__global__ void
+k_place(uint32_t n, uint64_t m, uint32_t const* __restrict__ keys, uint32_t const* __restrict__ off, uint32_t const* __restrict__ vals, uint64_t const* __restrict__ head, uint32_t* __restrict__ bc)
+{
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+    uint32_t const v = keys[i];
+    if (v >= n) continue;
+    uint64_t const p = head[v] + off[i];
+    if (p < m) bc[p] = vals[i];
+  }
+}
+
+// The same placement, band by band: block x of the grid works on band
+// x / (nc * per) and chunk (x / per) % nc, so the blocks resident at one
+// time write into one or two bands' rows and L2 merges their sectors.
+__global__ void
+k_place_banded(uint32_t n, uint64_t m, uint64_t chunk, uint32_t nc, uint32_t per, uint32_t const* __restrict__ seg, uint32_t const* __restrict__ keys, uint32_t const* __restrict__ off, uint32_t const* __restrict__ vals, uint64_t const* __restrict__ head, uint32_t* __restrict__ bc)
+{
+  uint32_t const b = blockIdx.x / (nc * per), c = (blockIdx.x / per) % nc, part = blockIdx.x % per;
+  uint32_t const lo = seg[b * nc + c], hi = seg[(b + 1) * nc + c];
+  uint64_t const e0 = c * chunk;
+  for (uint32_t j = lo + part * blockDim.x + threadIdx.x; j < hi; j += per * blockDim.x) {
+    uint64_t const i = e0 + j;
+    uint32_t const v = keys[i];
+    if (v >= n) continue;
+    uint64_t const p = head[v] + off[i];
+    if (p < m) bc[p] = vals[i];
+  }
 }
 
 unsigned
@@ -149,6 +281,95 @@ transpose(kspn_context* ctx, uint32_t n, uint64_t m, uint64_t const* fh, uint32_
   ctx->launches += 2;
   (void)cnt;
   (void)part64;
+}
+
+namespace {
+constexpr uint64_t PLACE_BAND_BYTES = 32ull << 20; // a quarter of L2
+constexpr uint64_t BAND_MAX         = 4096;
+} // namespace
+
+void
+upload_transpose(kspn_context* ctx, uint32_t n, uint64_t m, uint64_t const* h_fh, uint32_t const* h_fc, uint64_t* dfh, uint32_t* dfc, uint64_t* dbh, uint32_t* dbc, uint64_t chunk)
+{
+  cudaStream_t const s = ctx->stream;
+  if (!ctx->copy_stream) {
+    KSPN_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    KSPN_CUDA(cudaEventCreateWithFlags(&ctx->copy_ev, cudaEventDisableTiming));
+  }
+  cudaStream_t const cs = ctx->copy_stream;
+  if (chunk == 0) chunk = UPLOAD_CHUNK;
+  chunk = chunk < m ? chunk : (m ? m : 1);
+  // the copies start after the work already queued on the context's stream
+  KSPN_CUDA(cudaEventRecord(ctx->copy_ev, s));
+  KSPN_CUDA(cudaStreamWaitEvent(cs, ctx->copy_ev, 0));
+  KSPN_CUDA(cudaMemcpyAsync(dfh, h_fh, (static_cast<size_t>(n) + 1) * 8, cudaMemcpyHostToDevice, cs));
+  if (n == 0 || m == 0) {
+    KSPN_CUDA(cudaMemsetAsync(dbh, 0, (static_cast<size_t>(n) + 1) * 8, s));
+    KSPN_CUDA(cudaEventRecord(ctx->copy_ev, cs));
+    KSPN_CUDA(cudaStreamWaitEvent(s, ctx->copy_ev, 0));
+    return;
+  }
+  if (m >= 0xFFFFFFFFull) throw error{ KSPN_ERR_INVALID_ARGUMENT, "upload_transpose: 2^32-1 or more edges are not supported" };
+  // the chunk row ranges come from binary searches over the host offsets
+  if (h_fh[0] != 0 || h_fh[n] != m) throw error{ KSPN_ERR_INVALID_GRAPH, "invalid graph: head[0] != 0 or head[n] != m;" };
+  size_t const hist_n = radix_hist_entries(chunk);
+  size_t const part_n = scan_partial_entries((hist_n > n + 1 ? hist_n : n + 1));
+  scratch      sc;
+  size_t const band_cap = (BAND_MAX + 1) * ((m + chunk - 1) / chunk);
+  alloc_scratch(ctx, sc, (3 * (m + 64) + 5 * (chunk + 64) + 2 * (static_cast<size_t>(n) + 64) + BAND_MAX + 64 + band_cap + 64) * sizeof(uint32_t) + (hist_n + part_n) * sizeof(uint32_t) + part_n * sizeof(uint64_t) + 16384);
+  size_t    off    = 0;
+  uint32_t* skeys  = sc.carve<uint32_t>(off, m);     // chunk-sorted targets
+  uint32_t* svals  = sc.carve<uint32_t>(off, m);     // their sources
+  uint32_t* roff   = sc.carve<uint32_t>(off, m);     // offset inside the CSC row
+  uint32_t* src    = sc.carve<uint32_t>(off, chunk); // sources of the chunk, CSR order
+  uint32_t* ka     = sc.carve<uint32_t>(off, chunk);
+  uint32_t* va     = sc.carve<uint32_t>(off, chunk);
+  uint32_t* kb     = sc.carve<uint32_t>(off, chunk);
+  uint32_t* vb     = sc.carve<uint32_t>(off, chunk);
+  uint32_t* indeg  = sc.carve<uint32_t>(off, n);
+  uint32_t* first  = sc.carve<uint32_t>(off, n);
+  uint32_t* hist   = sc.carve<uint32_t>(off, hist_n);
+  uint32_t* part   = sc.carve<uint32_t>(off, part_n);
+  uint64_t* part64 = sc.carve<uint64_t>(off, part_n);
+  uint32_t* bv     = sc.carve<uint32_t>(off, BAND_MAX + 1);
+  uint32_t* seg    = sc.carve<uint32_t>(off, band_cap);
+  KSPN_CUDA(cudaMemsetAsync(indeg, 0, static_cast<size_t>(n) * 4, s));
+  int const bits = bits_for(n);
+  for (uint64_t e0 = 0; e0 < m; e0 += chunk) {
+    uint64_t const e1  = e0 + chunk < m ? e0 + chunk : m;
+    uint32_t const cnt = static_cast<uint32_t>(e1 - e0);
+    KSPN_CUDA(cudaMemcpyAsync(dfc + e0, h_fc + e0, static_cast<size_t>(cnt) * 4, cudaMemcpyHostToDevice, cs));
+    KSPN_CUDA(cudaEventRecord(ctx->copy_ev, cs));
+    KSPN_CUDA(cudaStreamWaitEvent(s, ctx->copy_ev, 0)); // the wait binds this record
+    // rows holding [e0, e1): the host has the offsets
+    uint32_t const u_lo = static_cast<uint32_t>(std::upper_bound(h_fh, h_fh + n + 1, e0) - h_fh - 1);
+    uint32_t const u_hi = static_cast<uint32_t>(std::lower_bound(h_fh + u_lo, h_fh + n + 1, e1) - h_fh);
+    k_expand_range<<<div_up(static_cast<uint64_t>(u_hi - u_lo), 256), 256, 0, s>>>(u_lo, u_hi, dfh, e0, e1, src);
+    KSPN_CHECK_LAUNCH();
+    radix_sort_pairs_to(ctx, dfc + e0, src, skeys + e0, svals + e0, ka, va, kb, vb, cnt, bits, hist, part);
+    unsigned const g = grid_for(cnt, 256);
+    k_run_first<<<g, 256, 0, s>>>(n, skeys + e0, cnt, first);
+    k_run_off<<<g, 256, 0, s>>>(n, skeys + e0, cnt, first, indeg, roff + e0);
+    k_run_advance<<<g, 256, 0, s>>>(n, skeys + e0, cnt, first, indeg);
+    KSPN_CHECK_LAUNCH();
+    ctx->launches += 4;
+  }
+  exclusive_scan<uint64_t>(s, f_array_u32{ indeg }, n, dbh, part64, &ctx->launches);
+  // bands of about PLACE_BAND_BYTES of CSC rows; `per` blocks per (band, chunk)
+  uint64_t const nc  = (m + chunk - 1) / chunk;
+  uint64_t const nb  = std::max<uint64_t>(1, std::min<uint64_t>((m * 4 + PLACE_BAND_BYTES - 1) / PLACE_BAND_BYTES, n));
+  uint32_t const per = static_cast<uint32_t>(std::max<uint64_t>(1, std::min<uint64_t>(64, m / (nb * nc * 8192))));
+  if ((nb + 1) * nc > band_cap || nb * nc * per > 0x7FFFFFFFull) {
+    k_place<<<grid_for(m, 256), 256, 0, s>>>(n, m, skeys, roff, svals, dbh, dbc);
+    KSPN_CHECK_LAUNCH();
+    ctx->launches += 1;
+    return;
+  }
+  k_band_vertices<<<div_up(nb + 1, 256), 256, 0, s>>>(n, m, dbh, static_cast<uint32_t>(nb), bv);
+  k_band_segments<<<div_up((nb + 1) * nc, 256), 256, 0, s>>>(skeys, m, chunk, static_cast<uint32_t>(nc), static_cast<uint32_t>(nb), bv, seg);
+  k_place_banded<<<static_cast<unsigned>(nb * nc * per), 256, 0, s>>>(n, m, chunk, static_cast<uint32_t>(nc), per, seg, skeys, roff, svals, dbh, dbc);
+  KSPN_CHECK_LAUNCH();
+  ctx->launches += 3;
 }
 
 uint64_t

@@ -389,6 +389,8 @@ struct kspn_context
   kspn::cached_graph trim;                 // one-launch trim fixpoint graph
   kspn::batch_cache* batch      = nullptr;  // batched path (kspn_scc_batched)
   kspn::dev_buffer   bufs[kspn::BUF_COUNT];
+  cudaStream_t       copy_stream = nullptr; // host-graph upload (upload_transpose)
+  cudaEvent_t        copy_ev     = nullptr;
 };
 
 namespace kspn {
@@ -491,6 +493,16 @@ void canonicalise(kspn_context* ctx, uint32_t n, uint32_t* scc_id, uint32_t* scr
 
 // csr.cu
 void     transpose(kspn_context* ctx, uint32_t n, uint64_t m, uint64_t const* fh, uint32_t const* fc, uint64_t* bh, uint32_t* bc, uint32_t* scratch_n);
+// Upload of a host CSR in chunks of `chunk` edges (0: UPLOAD_CHUNK) on the
+// context's copy stream, with the CSC built on the context's stream while
+// later chunks are still in flight: each arrived chunk's (target, source)
+// pairs are radix-sorted, every entry gets its offset inside its CSC row
+// (entries of earlier chunks first, so rows stay ascending), and after the
+// last chunk one scan gives the heads and one pass places the entries.
+// Leaves (dfh, dfc) = the host CSR and (dbh, dbc) = the same CSC as
+// transpose(); work queued on the context's stream sees all of it.
+constexpr uint64_t UPLOAD_CHUNK = 8ull << 20;
+void     upload_transpose(kspn_context* ctx, uint32_t n, uint64_t m, uint64_t const* h_fh, uint32_t const* h_fc, uint64_t* dfh, uint32_t* dfc, uint64_t* dbh, uint32_t* dbc, uint64_t chunk);
 uint64_t build_csr(kspn_context* ctx, uint32_t n, uint64_t m_raw, uint32_t* src, uint32_t* dst, uint64_t* head, uint32_t* csr);
 void     validate(kspn_context* ctx, dgraph const& g);
 

@@ -157,6 +157,10 @@ struct f_frontier_degree
 // are scratch of the same size.  hist needs radix_hist_entries(count).
 size_t radix_hist_entries(uint64_t count);
 void   radix_sort_pairs(kspn_context* ctx, uint32_t* keys, uint32_t* vals, uint32_t* keys_alt, uint32_t* vals_alt, uint64_t count, int begin_bit, int end_bit, uint32_t* hist, uint32_t* hist_partial);
+// The same sort on key bits [0, end_bit) from read-only input (kin, vin) to
+// (kout, vout); (ka, va) and (kb, vb) are scratch of `count` entries each
+// (neither may alias the input or the output).
+void   radix_sort_pairs_to(kspn_context* ctx, uint32_t const* kin, uint32_t const* vin, uint32_t* kout, uint32_t* vout, uint32_t* ka, uint32_t* va, uint32_t* kb, uint32_t* vb, uint64_t count, int end_bit, uint32_t* hist, uint32_t* hist_partial);
 
 inline int
 bits_for(uint64_t n) // bits needed to represent ids in [0, n)

@@ -165,4 +165,38 @@ radix_sort_pairs(kspn_context* ctx, uint32_t* keys, uint32_t* vals, uint32_t* ke
   }
 }
 
+void
+radix_sort_pairs_to(kspn_context* ctx, uint32_t const* kin, uint32_t const* vin, uint32_t* kout, uint32_t* vout, uint32_t* ka, uint32_t* va, uint32_t* kb, uint32_t* vb, uint64_t count, int end_bit, uint32_t* hist, uint32_t* hist_partial)
+{
+  cudaStream_t const s = ctx->stream;
+  int const          passes = (end_bit + 7) / 8;
+  if (count == 0) return;
+  if (passes == 0 || count == 1) {
+    KSPN_CUDA(cudaMemcpyAsync(kout, kin, count * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    KSPN_CUDA(cudaMemcpyAsync(vout, vin, count * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    return;
+  }
+  uint32_t const num_tiles = div_up(count, RX_TILE);
+  uint64_t const entries   = static_cast<uint64_t>(256) * num_tiles;
+  uint32_t const* ki = kin;
+  uint32_t const* vi = vin;
+  for (int p = 0; p < passes; ++p) {
+    // the last pass lands in (kout, vout); the ones before alternate A / B
+    // so that no pass reads and writes one buffer
+    bool const last = p == passes - 1;
+    uint32_t*  ko   = last ? kout : (((passes - 1 - p) & 1) ? ka : kb);
+    uint32_t*  vo   = last ? vout : (((passes - 1 - p) & 1) ? va : vb);
+    int const  shift = 8 * p;
+    k_radix_hist<<<num_tiles, RX_THREADS, 0, s>>>(ki, count, shift, hist, num_tiles);
+    KSPN_CHECK_LAUNCH();
+    exclusive_scan<uint32_t>(s, f_array_u32_as_u32{ hist }, entries, hist, hist_partial, &ctx->launches);
+    k_radix_scatter<<<num_tiles, RX_THREADS, 0, s>>>(ki, vi, ko, vo, count, shift, hist, num_tiles);
+    KSPN_CHECK_LAUNCH();
+    ctx->launches += 2;
+    ki = ko;
+    vi = vo;
+  }
+}
+
+
 } // namespace kspn
