@@ -156,6 +156,8 @@ typedef struct kspn_stats
   uint32_t heavy_fixups;
   uint32_t heavy_trim_seeds;
   uint32_t trim_worklist;   /* 1: the resident trim tail finished on the worklist (long, thin peeling) */
+  uint32_t fwbw_joint;      /* 1: the BW search ran inside the FW search's worklist phase (high diameter) */
+  uint32_t stats_pad;
 } kspn_stats;
 
 typedef struct kspn_context kspn_context;

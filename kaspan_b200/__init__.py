@@ -120,6 +120,8 @@ class Stats(C.Structure):
         ("heavy_fixups", C.c_uint32),
         ("heavy_trim_seeds", C.c_uint32),
         ("trim_worklist", C.c_uint32),
+        ("fwbw_joint", C.c_uint32),
+        ("stats_pad", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -139,6 +141,7 @@ class Stats(C.Structure):
             "kernel_launches": int(self.kernel_launches),
             "heavy": {"cut_rows": self.heavy_cut_rows, "fixups": self.heavy_fixups, "trim_seeds": self.heavy_trim_seeds},
             "trim_worklist": self.trim_worklist,
+            "fwbw_joint": self.fwbw_joint,
             "kernels": {k: {"ms": float(self.kernel_ms[i]), "bytes": int(self.kernel_bytes[i]), "calls": int(self.kernel_calls[i])}
                         for i, k in enumerate(KERNEL_CLASSES)},
             "trace": [{"dir": "bw" if t.backward else "fw", "mode": "bu" if t.bottom_up else "td", "frontier": t.frontier,

@@ -284,6 +284,7 @@ struct workspace
   uint32_t* vis_b    = nullptr; // bitmap
   uint32_t* mark     = nullptr; // bitmap
   uint32_t* fresh    = nullptr; // bitmap: vertices found by the last bottom-up sweep
+  uint32_t* cand_bw  = nullptr; // bitmap: BW candidates of a joint worklist search (FW and BW at once)
   uint32_t* label    = nullptr; // n
   uint32_t* indeg    = nullptr; // n
   uint32_t* outdeg   = nullptr; // n
@@ -300,7 +301,7 @@ struct workspace
   uint64_t* seed_prefix = nullptr; // 4
   void*     gbar        = nullptr; // 4 KiB: grid barrier of the persistent FW-BW at 0, worklist counters at 1024 (zeroed at creation)
   void*     aw          = nullptr; // aw_entries u64: worklist of the asynchronous search tail (zeroed at creation, zero outside a phase)
-  size_t    aw_entries  = 0;       // n + 66 vertex items + 2 m / HEAVY_SLICE + 64 row-slice items
+  size_t    aw_entries  = 0;       // 2 (n + 2) + 64 vertex items (FW and BW at once) + 2 m / HEAVY_SLICE + 64 row-slice items
   void*     rstate      = nullptr; // 4 KiB device control blocks (FW-BW at 0, trim at 512, search stamps at 2048)
   uint32_t* heavy       = nullptr; // 4 heavy lists of heavy_cap entries (persistent FW-BW: trim seed, two trim push levels, cut bottom-up rows)
   uint64_t  heavy_cap   = 0;

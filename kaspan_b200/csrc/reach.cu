@@ -102,6 +102,7 @@ struct reach_state
   uint32_t           cut_n[2];     // bottom-up rows cut short (FW, BW search; host-driven levels use [0])
   uint32_t           fixups;       // fix-up steps run (both searches)
   uint32_t           hseed_n;      // trim tail: listed vertices with a heavy row
+  uint32_t           joint;        // the BW search ran inside the FW search's worklist phase
   uint32_t           hq_n[6];      // trim tail: heavy out-/in-rows listed per push level (pairs rotating like lq)
   uint32_t           heavy_err;    // a heavy or cut list would have overflowed
   uint32_t           trim_async;   // the trim tail finished on the worklist
@@ -636,6 +637,7 @@ struct fwbw_args
   uint32_t*          vis_a;
   uint32_t*          vis_b;
   uint32_t*          fresh;
+  uint32_t*          cand_bw; // joint worklist search: BW candidates (und minus the pivot), or null
   frontier_buf       fb[2];
   frontier_buf       seed;    // q[0] = pivot, prefix[0] = 0, tile starts all 0
   uint64_t*          partial; // one per block
@@ -870,14 +872,63 @@ aw_push(uint32_t v, unsigned long long* aw, unsigned long long* tail, uint64_t c
   if (slot < cap) __stcg(aw + slot, AW_TAG | v);
 }
 
-// Runs the rest of the search from frontier fin.q[0, qn).  All threads of
-// every block call it.  An item is AW_TAG | slice << 33 | v: slice 0 of a
-// row longer than HEAVY_ROW appends the row's other HEAVY_SLICE-entry
-// slices as items of their own (so idle warps share the row) and walks the
-// first; a vertex whose row is shorter is one item.
+// Finds a warp keeps on its own stack (in its shared buffer) and expands in
+// its next round instead of appending them: a hop then costs the chain of
+// loads of one expansion, not a trip through the worklist to whichever warp
+// claimed the slot.  Finds past AW_LOCAL_KEEP go to the worklist, where idle
+// warps pick them up.  Stack entries are items (below) with slice 0.
+constexpr uint32_t           AW_LOCAL_KEEP = 64;
+constexpr unsigned long long AW_BW         = 1ull << 63; // item of the BW search of a joint phase
+static_assert(sizeof(bu_warp_smem) >= AW_LOCAL_KEEP * sizeof(unsigned long long), "local stack must fit the warp buffer");
+
+// One search's arrays in the worklist phase: rows to walk, the candidates a
+// find is taken from, the set it joins.
+struct aw_dir
+{
+  uint64_t const* head;
+  uint32_t const* adj;
+  uint32_t*       avail;
+  uint32_t*       mark;
+};
+
+// Appends the finds of one pass: lane has c finds, at positions [q, q + c)
+// of the warp's tot (exclusive scan); the first min(tot, room) go to the
+// stack, the others to the worklist.  Warp-uniform; returns the stack's new
+// size.
+struct aw_sink
+{
+  unsigned long long* stk;
+  unsigned long long* aw;
+  unsigned long long* tail;
+  uint64_t            cap;
+  __device__ __forceinline__ uint32_t reserve(uint32_t ls_n, uint32_t tot, unsigned long long& gbase, uint32_t& nloc) const
+  {
+    uint32_t const room = ls_n < AW_LOCAL_KEEP ? AW_LOCAL_KEEP - ls_n : 0u;
+    nloc                = tot < room ? tot : room;
+    unsigned long long b = 0;
+    if ((threadIdx.x & 31u) == 0 && tot > nloc) b = atomicAdd(tail, static_cast<unsigned long long>(tot - nloc));
+    gbase = __shfl_sync(0xFFFFFFFFu, b, 0);
+    return ls_n + nloc;
+  }
+  __device__ __forceinline__ void put(uint32_t ls_n, uint32_t nloc, unsigned long long gbase, uint32_t q, unsigned long long item) const
+  {
+    if (q < nloc) stk[ls_n + q] = item;
+    else if (gbase + (q - nloc) < cap) __stcg(aw + gbase + (q - nloc), item);
+  }
+};
+
+// Runs the rest of the search from frontier fq[0, qn) (direction d0).  With
+// d1 (a joint phase) the other search runs in the same phase from its first
+// vertex seed1: its items carry AW_BW.  All threads of every block call it.
+// An item is AW_TAG | dir << 63 | slice << 33 | v: slice 0 of a row longer
+// than HEAVY_ROW appends the row's other HEAVY_SLICE-entry slices as items
+// of their own (so idle warps share the row) and walks the first; a vertex
+// whose row is shorter is one item.  Each round a warp polls its claimed
+// slots and fills its other lanes from its own stack; the done count only
+// grows while the stack is empty, so done == appended still means that
+// nothing is left anywhere.
 __device__ __forceinline__ int
-run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, uint64_t const* __restrict__ td_head, uint32_t const* __restrict__ td_adj, uint32_t* avail, uint32_t* mark, unsigned long long& epoch,
-          uint64_t& edges)
+run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, aw_dir const* d1, uint32_t seed1, unsigned long long& epoch, uint64_t& edges, fwbw_smem& sm)
 {
   unsigned long long* const aw   = a.aw;
   unsigned long long* const head = a.aq;
@@ -885,112 +936,167 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, uint64_t const* _
   unsigned long long* const done = a.aq + 32;
   uint64_t const            cap  = a.aw_cap;
   unsigned const            lane = threadIdx.x & 31u;
+  unsigned const            lt   = (1u << lane) - 1u;
+  bool const                joint = d1 != nullptr;
+  aw_dir const              e1    = joint ? *d1 : d0;
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; i < qn; i += static_cast<uint64_t>(gridDim.x) * R_THREADS) __stcg(aw + i, AW_TAG | __ldcg(fq + i));
-  if (blockIdx.x == 0 && threadIdx.x == 0) *head = 0, *tail = qn, *done = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (joint) __stcg(aw + qn, AW_TAG | AW_BW | seed1);
+    *head = 0, *tail = qn + (joint ? 1u : 0u), *done = 0;
+  }
   if (!grid_sync(a.bar, epoch)) return SEARCH_FAILED;
-  take_op const op{ avail, mark };
-  auto const    take   = [&](uint32_t w) { return op(0u, w, true, op.probe(w)); };
-  bool          failed = false;
-  uint32_t unpublished = 0; // items this warp finished, not yet added to done
+  aw_sink const sink{ reinterpret_cast<unsigned long long*>(&sm.warp[threadIdx.x >> 5]), aw, tail, cap };
+  bool          failed      = false;
+  uint32_t      unpublished = 0; // worklist items this warp finished, not yet added to done
+  uint32_t      ls_n        = 0; // items on this warp's stack (warp-uniform)
+  bool          batch       = false;
+  bool          pending     = false;
+  uint64_t      slot        = 0;
+  unsigned      spins       = 0;
   for (bool alive = true; alive;) {
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(head, 32ull);
-    base                = __shfl_sync(0xFFFFFFFFu, base, 0);
-    uint64_t const slot = base + lane;
-    bool           pending = true;
-    unsigned       spins   = 0;
-    while (__any_sync(0xFFFFFFFFu, pending)) {
-      bool     got = false;
-      uint32_t v = 0, sl = 0;
-      if (pending && slot < cap) {
-        unsigned long long const e = ld_acquire64(aw + slot);
-        if (e & AW_TAG) v = static_cast<uint32_t>(e), sl = static_cast<uint32_t>(e >> 33), got = true, pending = false;
-      }
-      unsigned const gmask = __ballot_sync(0xFFFFFFFFu, got);
-      if (gmask) {
-        uint64_t b = 0, e = 0;
-        if (got) b = td_head[v], e = td_head[v + 1];
-        if (got && e - b > HEAVY_ROW) {
-          if (sl == 0) {
-            // the row's other slices become items
-            uint64_t const           ns = (e - b + HEAVY_SLICE - 1) / HEAVY_SLICE;
-            unsigned long long const at = atomicAdd(tail, static_cast<unsigned long long>(ns - 1));
-            for (uint64_t j = 1; j < ns; ++j)
-              if (at + j - 1 < cap) __stcg(aw + at + j - 1, AW_TAG | (static_cast<unsigned long long>(j) << 33) | v);
-          }
-          b += static_cast<uint64_t>(sl) * HEAVY_SLICE;
-          e = b + HEAVY_SLICE < e ? b + HEAVY_SLICE : e;
+    if (!batch) {
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(head, 32ull);
+      slot    = __shfl_sync(0xFFFFFFFFu, base, 0) + lane;
+      pending = true;
+      batch   = true;
+    }
+    bool               got  = false;
+    unsigned long long item = 0;
+    // an idle warp (spins > 0, stack empty) first looks at its lowest
+    // pending slot only: slots are reserved in order and written right
+    // after, so the others are rarely ready before it; thousands of idle
+    // warps polling 32 slots each would crowd the busy ones out of L2
+    bool look = pending && slot < cap;
+    if (spins && ls_n == 0) {
+      unsigned const pm    = __ballot_sync(0xFFFFFFFFu, look);
+      bool           ready = false;
+      if (pm && lane == static_cast<unsigned>(__ffs(pm) - 1)) ready = (ld_acquire64(aw + slot) & AW_TAG) != 0;
+      if (!__any_sync(0xFFFFFFFFu, ready)) look = false;
+    }
+    if (look) {
+      unsigned long long const e = ld_acquire64(aw + slot);
+      if (e & AW_TAG) item = e, got = true, pending = false;
+    }
+    unsigned const gm = __ballot_sync(0xFFFFFFFFu, got); // worklist items this round
+    if (ls_n) {
+      // the lanes left free take the top of the stack
+      unsigned const freem = ~gm;
+      uint32_t const nfree = __popc(freem);
+      uint32_t const k     = ls_n < nfree ? ls_n : nfree;
+      uint32_t const r     = __popc(freem & lt);
+      if (!got && r < k) item = sink.stk[ls_n - k + r], got = true;
+      ls_n -= k;
+      __syncwarp(); // the slots just read are reused by this round's finds
+    }
+    batch                = __any_sync(0xFFFFFFFFu, pending);
+    unsigned const gmask = __ballot_sync(0xFFFFFFFFu, got);
+    if (gmask) {
+      uint32_t const           v   = static_cast<uint32_t>(item);
+      uint32_t const           sl  = static_cast<uint32_t>(item >> 33) & 0x3FFFFFFFu;
+      unsigned long long const dir = item & AW_BW;
+      aw_dir const             d   = dir ? e1 : d0;
+      uint64_t                 b = 0, e = 0;
+      if (got) b = d.head[v], e = d.head[v + 1];
+      if (got && e - b > HEAVY_ROW) {
+        if (sl == 0) {
+          // the row's other slices become items
+          uint64_t const           ns = (e - b + HEAVY_SLICE - 1) / HEAVY_SLICE;
+          unsigned long long const at = atomicAdd(tail, static_cast<unsigned long long>(ns - 1));
+          for (uint64_t j = 1; j < ns; ++j)
+            if (at + j - 1 < cap) __stcg(aw + at + j - 1, AW_TAG | dir | (static_cast<unsigned long long>(j) << 33) | v);
         }
-        bool const big = got && e - b > 32;
-        if (got) edges += e - b;
-        // small rows, AW_BATCH neighbours per pass: all ids, then all probes,
-        // then the takes; the warp's finds appended with one atomic per pass
-        uint64_t x = got && !big ? b : e;
-        while (__any_sync(0xFFFFFFFFu, x < e)) {
-          uint32_t w[AW_BATCH], found = 0;
+        b += static_cast<uint64_t>(sl) * HEAVY_SLICE;
+        e = b + HEAVY_SLICE < e ? b + HEAVY_SLICE : e;
+      }
+      bool const big = got && e - b > 32;
+      if (got) edges += e - b;
+      // small rows, AW_BATCH neighbours per pass: all ids, then all probes,
+      // then the takes; the warp's finds placed with at most one atomic per pass
+      uint64_t x = got && !big ? b : e;
+      while (__any_sync(0xFFFFFFFFu, x < e)) {
+        uint32_t w[AW_BATCH], found = 0;
 #pragma unroll
-          for (int k = 0; k < AW_BATCH; ++k) w[k] = x + k < e ? td_adj[x + k] : 0u;
-          uint32_t wd[AW_BATCH];
+        for (int k = 0; k < AW_BATCH; ++k) w[k] = x + k < e ? d.adj[x + k] : 0u;
+        uint32_t wd[AW_BATCH];
 #pragma unroll
-          for (int k = 0; k < AW_BATCH; ++k) wd[k] = x + k < e ? op.probe(w[k]) : 0u;
+        for (int k = 0; k < AW_BATCH; ++k) wd[k] = x + k < e ? __ldcg(d.avail + (w[k] >> 5)) : 0u;
+#pragma unroll
+        for (int k = 0; k < AW_BATCH; ++k)
+          if (x + k < e && ((wd[k] >> (w[k] & 31)) & 1u) && bit_take(d.avail, w[k])) bit_claim(d.mark, w[k]), found |= 1u << k;
+        uint32_t const c = __popc(found);
+        uint32_t       p = c;
+#pragma unroll
+        for (int dd = 1; dd < 32; dd <<= 1) {
+          uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, p, dd);
+          if (lane >= static_cast<unsigned>(dd)) p += y;
+        }
+        uint32_t const tot = __shfl_sync(0xFFFFFFFFu, p, 31);
+        if (tot) {
+          unsigned long long gbase;
+          uint32_t           nloc;
+          uint32_t const     next = sink.reserve(ls_n, tot, gbase, nloc);
+          uint32_t           q    = p - c;
 #pragma unroll
           for (int k = 0; k < AW_BATCH; ++k)
-            if (x + k < e && op(0u, w[k], true, wd[k])) found |= 1u << k;
-          uint32_t const     c = __popc(found);
-          uint32_t           p = c;
-#pragma unroll
-          for (int d = 1; d < 32; d <<= 1) {
-            uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, p, d);
-            if (lane >= static_cast<unsigned>(d)) p += y;
-          }
-          uint32_t const     tot  = __shfl_sync(0xFFFFFFFFu, p, 31);
-          unsigned long long base = 0;
-          if (lane == 31 && tot) base = atomicAdd(tail, static_cast<unsigned long long>(tot));
-          base = __shfl_sync(0xFFFFFFFFu, base, 31) + p - c;
-#pragma unroll
-          for (int k = 0; k < AW_BATCH; ++k)
-            if ((found >> k) & 1u) {
-              if (base < cap) __stcg(aw + base, AW_TAG | w[k]);
-              ++base;
-            }
-          x = x + AW_BATCH < e ? x + AW_BATCH : e;
+            if ((found >> k) & 1u) sink.put(ls_n, nloc, gbase, q++, AW_TAG | dir | w[k]);
+          ls_n = next;
         }
-        for (unsigned todo = __ballot_sync(0xFFFFFFFFu, big); todo; todo &= todo - 1) {
-          unsigned const l  = __ffs(todo) - 1;
-          uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b, l), e0 = __shfl_sync(0xFFFFFFFFu, e, l);
-          for (uint64_t x = b0 + lane; x < e0; x += 32) {
-            uint32_t const w = td_adj[x];
-            if (take(w)) aw_push(w, aw, tail, cap);
-          }
-        }
-        // counted as done when this warp next goes idle (one atomic then)
-        unpublished += __popc(gmask);
-        spins = 0;
-      } else {
-        // nothing arrived: publish this warp's finished items (their finds
-        // are appended first), then finished when every appended item is done
-        if (unpublished) {
-          __threadfence();
-          if (lane == 0) atomicAdd(done, static_cast<unsigned long long>(unpublished));
-          unpublished = 0;
-        }
-        uint32_t stop = 0;
-        if (lane == 0) {
-          unsigned long long const d = ld_acquire64(done);
-          unsigned long long const t = ld_acquire64(tail);
-          stop                       = d == t ? 1u : 0u;
-          if (!stop && (++spins > GRID_SYNC_SPINS || ((spins & 63u) == 63u && ld_acquire(&a.bar->err)))) {
-            atomicExch(&a.bar->err, 1u);
-            stop = 2;
-          }
-        }
-        stop = __shfl_sync(0xFFFFFFFFu, stop, 0);
-        if (stop) {
-          pending = false;
-          alive   = false;
-          failed  = stop == 2;
-        } else __nanosleep(64);
+        x = x + AW_BATCH < e ? x + AW_BATCH : e;
       }
+      for (unsigned todo = __ballot_sync(0xFFFFFFFFu, big); todo; todo &= todo - 1) {
+        unsigned const           l   = __ffs(todo) - 1;
+        uint64_t const           b0  = __shfl_sync(0xFFFFFFFFu, b, l), e0 = __shfl_sync(0xFFFFFFFFu, e, l);
+        unsigned long long const dl  = __shfl_sync(0xFFFFFFFFu, dir, l);
+        aw_dir const             dd_ = dl ? e1 : d0;
+        for (uint64_t xb = b0; xb < e0; xb += 32) {
+          uint64_t const x1 = xb + lane;
+          uint32_t       w  = 0;
+          bool           f  = false;
+          if (x1 < e0) {
+            w = dd_.adj[x1];
+            f = ((__ldcg(dd_.avail + (w >> 5)) >> (w & 31)) & 1u) && bit_take(dd_.avail, w);
+            if (f) bit_claim(dd_.mark, w);
+          }
+          unsigned const fm = __ballot_sync(0xFFFFFFFFu, f);
+          if (fm) {
+            unsigned long long gbase;
+            uint32_t           nloc;
+            uint32_t const     next = sink.reserve(ls_n, __popc(fm), gbase, nloc);
+            if (f) sink.put(ls_n, nloc, gbase, __popc(fm & lt), AW_TAG | dl | w);
+            ls_n = next;
+          }
+        }
+      }
+      __syncwarp(); // this round's stack writes before the next round's reads
+      // worklist items are counted as done when this warp next goes idle
+      // (its stack empty, so their finds are expanded or appended)
+      unpublished += __popc(gm);
+      spins = 0;
+    } else {
+      // nothing arrived and the stack is empty: publish this warp's finished
+      // items, then finished when every appended item is done
+      if (unpublished) {
+        __threadfence();
+        if (lane == 0) atomicAdd(done, static_cast<unsigned long long>(unpublished));
+        unpublished = 0;
+      }
+      uint32_t stop = 0;
+      ++spins; // every lane: the count steers warp-wide choices above
+      if (lane == 0) {
+        unsigned long long const dn = ld_acquire64(done);
+        unsigned long long const t  = ld_acquire64(tail);
+        stop                        = dn == t ? 1u : 0u;
+        if (!stop && (spins > GRID_SYNC_SPINS || ((spins & 63u) == 63u && ld_acquire(&a.bar->err)))) {
+          atomicExch(&a.bar->err, 1u);
+          stop = 2;
+        }
+      }
+      stop = __shfl_sync(0xFFFFFFFFu, stop, 0);
+      if (stop) {
+        alive  = false;
+        failed = stop == 2;
+      } else __nanosleep(spins < 32 ? 64u : (spins < 256 ? 256u : 1024u)); // longer idle, longer sleep
     }
   }
   if (!grid_sync(a.bar, epoch) || failed) return SEARCH_FAILED;
@@ -1009,7 +1115,7 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, uint64_t const* _
 
 template<bool BW>
 __device__ __forceinline__ int
-run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uint32_t& glvl, unsigned long long& epoch)
+run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uint32_t& glvl, unsigned long long& epoch, bool& joint)
 {
   uint64_t const* const    td_head = BW ? a.bh : a.fh;
   uint32_t const* const    td_adj  = BW ? a.bc : a.fc;
@@ -1101,9 +1207,17 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
     else if (mode == 0 && mf * a.alpha > m_u) mode = 1;
     if (mode == 0 && lvl >= ASYNC_AFTER && qn <= ASYNC_FRONTIER && a.aw) {
       // a long, thin search: finish it on the worklist
-      uint64_t  ea = 0;
-      int const r  = run_async(a, fin.q, qn, td_head, td_adj, avail, mark, epoch, ea);
+      // The FW search's first worklist phase also runs the whole BW search
+      // (from the pivot, over every undecided vertex: FW(p) and BW(p) meet
+      // in the SCC, so BW need not wait for FW's set), and the BW level
+      // loop is skipped: a high-diameter graph pays its depth once.
+      uint64_t     ea = 0;
+      aw_dir const d0{ td_head, td_adj, avail, mark };
+      aw_dir const d1{ a.bh, a.bc, a.cand_bw, a.vis_b };
+      bool const   j  = !BW && a.cand_bw && !joint;
+      int const    r  = run_async(a, fin.q, qn, d0, j ? &d1 : nullptr, pivot, epoch, ea, sm);
       if (r != SEARCH_DONE) return r;
+      joint = joint || j;
       stamp(a, 13);
       edges_td += ea;
       if (tally) st->async_phases += 1;
@@ -1673,7 +1787,7 @@ k_fwbw(fwbw_args a)
     st->mats = st->bu_bitmap    = 0;
     st->async_phases            = 0;
     st->cut_n[0] = st->cut_n[1] = st->fixups = 0;
-    st->hseed_n = st->heavy_err = st->trim_async = 0;
+    st->hseed_n = st->heavy_err = st->trim_async = st->joint = 0;
     for (int i = 0; i < 6; ++i) st->hq_n[i] = 0;
     if (search) a.seed.q[0] = p, a.seed.prefix[0] = 0;
   }
@@ -1689,6 +1803,7 @@ k_fwbw(fwbw_args a)
       a.cand[w]          = u & ~pin;
       a.vis_a[w]         = pin;
       a.vis_b[w]         = pin;
+      if (a.cand_bw) a.cand_bw[w] = u & ~pin;
       c += __popc(u);
     }
     uint64_t tot;
@@ -1702,15 +1817,24 @@ k_fwbw(fwbw_args a)
       block_exclusive_scan<uint64_t, R_THREADS>(s, &tot);
       uint32_t const n_und = static_cast<uint32_t>(tot);
       // one inlined copy of the level loop, run for FW then BW
+      bool joint = false; // the FW search's worklist phase ran BW as well
 #pragma unroll 1
       for (int dir = 0; dir < 2 && rc == SEARCH_DONE; ++dir) {
+        if (dir && joint) {
+          // BW(p) over every undecided vertex is complete: the SCC is
+          // FW(p) & BW(p)
+          for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) a.vis_b[w] = __ldcg(a.vis_b + w) & __ldcg(a.vis_a + w);
+          if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
+          if (blockIdx.x == 0 && threadIdx.x == 0) st->joint = 1;
+          break;
+        }
         if (dir) {
           // BW: candidates are the FW-reached vertices except the pivot
           // (each block clears its bit before its own first expansion)
           if (threadIdx.x == 0) atomicAnd(a.vis_a + (p >> 5), ~(1u << (p & 31)));
           __syncthreads();
         }
-        rc = dir ? run_search<true>(a, sm, p, n_und, glvl, epoch) : run_search<false>(a, sm, p, n_und, glvl, epoch);
+        rc = dir ? run_search<true>(a, sm, p, n_und, glvl, epoch, joint) : run_search<false>(a, sm, p, n_und, glvl, epoch, joint);
       }
     }
     if (rc == SEARCH_DONE && a.min_ids) {
@@ -2020,6 +2144,7 @@ launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* s
   a.vis_a       = ws.vis_a;
   a.vis_b       = ws.vis_b;
   a.fresh       = ws.fresh;
+  a.cand_bw     = ws.cand_bw;
   a.fb[0]       = { ws.q0, ws.prefix, ws.tile_start };
   a.fb[1]       = { ws.q1, ws.prefix2, ws.tile_start2 };
   a.seed        = { ws.seed_q, ws.seed_prefix, ws.tile_zero };
@@ -2132,6 +2257,7 @@ fw_bw_trim_result(kspn_context* ctx, dgraph const& g, kspn_options const& opt, k
     st->heavy_fixups           = hs->fixups;
     st->heavy_trim_seeds       = hs->hseed_n;
     st->trim_worklist          = hs->trim_async;
+    st->fwbw_joint             = hs->joint;
   }
   resident_result r;
   r.pivot             = hs->pivot_used;

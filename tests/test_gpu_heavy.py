@@ -101,3 +101,55 @@ def test_trim_worklist_tail(ctx):
         ctx.scc_device(n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, K.default_options(validate=0), st)
         assert np.array_equal(out.cpu().numpy().view(np.uint32), want)
         assert st.as_dict()["trim_worklist"] == 1
+
+
+def _long_cycle_graph(n_cyc=60000, heavy=False):
+    """A cycle of n_cyc vertices (so both searches outlast the level loop and
+    finish on the worklist), the pivot on it by degree, plus side chains
+    that FW reaches but BW does not and vice versa (FW(p) and BW(p) each
+    hold vertices outside the SCC), and with `heavy` a hub on the cycle
+    whose out- and in-rows are sliced (slice items of both directions)."""
+    rng = np.random.default_rng(7)
+    src, dst = [], []
+    cyc = np.arange(n_cyc)
+    src += list(cyc); dst += list((cyc + 1) % n_cyc)
+    n = n_cyc
+    # the pivot: vertex 0 gets extra in and out edges from/to cycle vertices
+    k = 40
+    src += [0] * k; dst += list(rng.integers(1, n_cyc, k))
+    src += list(rng.integers(1, n_cyc, k)); dst += [0] * k
+    # side chains: out of the cycle (FW only) and into it (BW only)
+    for start in rng.integers(0, n_cyc, 30):
+        L = 500
+        ids = np.arange(n, n + L); n += L
+        src += [int(start)] + list(ids[:-1]); dst += list(ids)
+    for start in rng.integers(0, n_cyc, 30):
+        L = 500
+        ids = np.arange(n, n + L); n += L
+        src += list(ids); dst += list(ids[1:]) + [int(start)]
+    if heavy:
+        # vertex n_cyc // 2 (on the cycle) points at 5000 fresh dead ends and
+        # is pointed at by 5000 fresh sources: both its rows are heavy
+        h = n_cyc // 2
+        outs = np.arange(n, n + 5000); n += 5000
+        ins = np.arange(n, n + 5000); n += 5000
+        src += [h] * 5000 + list(ins); dst += list(outs) + [h] * 5000
+    return n, np.array(src, np.uint32), np.array(dst, np.uint32)
+
+
+@pytest.mark.parametrize("heavy", [False, True])
+def test_joint_worklist_search(ctx, heavy):
+    import torch
+
+    n, s, d = _long_cycle_graph(heavy=heavy)
+    G = KG.from_edges(ctx, n, torch.from_numpy(s.view(np.int32)).cuda(), torch.from_numpy(d.view(np.int32)).cuda())
+    fwh, fwc, bwh, bwc = G.to_host()
+    want = O.tarjan(O.Graph(n, fwh, fwc, bwh, bwc))
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    for _ in range(2):  # a second call reuses the (all-zero) worklist
+        st = K.Stats()
+        ctx.scc_device(n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, K.default_options(validate=0), st)
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), want)
+        dct = st.as_dict()
+        assert dct["fwbw_joint"] == 1, "the BW search should run inside the FW worklist phase"
+        assert dct["levels_bw"] == 0
