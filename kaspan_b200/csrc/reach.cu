@@ -1222,7 +1222,11 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
       edges_td += ea;
       if (tally) st->async_phases += 1;
       // nothing is queued for the next level: it runs dry (or fixes up
-      // rows an earlier sweep cut short)
+      // rows an earlier sweep cut short).  This level may have built its
+      // frontier from `fresh` (a bottom-up sweep before it): that is
+      // consumed, and the next level must not build it again
+      mode = 0;
+      mat  = false;
       continue;
     }
     unsigned long long* const octr = &st->lq[s_out];

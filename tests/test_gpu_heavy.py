@@ -153,3 +153,47 @@ def test_joint_worklist_search(ctx, heavy):
         dct = st.as_dict()
         assert dct["fwbw_joint"] == 1, "the BW search should run inside the FW worklist phase"
         assert dct["levels_bw"] == 0
+
+
+def _path_core_chain_graph():
+    """Pivot p (largest in*out: 3000 in-edges from sources, 3000 out-edges to
+    sinks, both decided by trim_1_first) -> a 12-vertex path -> a dense core
+    of 20000 vertices (levels 13-15 top-down; level 16 turns bottom-up, and
+    the level that builds its frontier from the sweeps' finds comes after
+    level 16 with a small frontier, so it switches straight to the
+    worklist) -> a 3000-vertex chain back to p.  One SCC of p + path +
+    core + chain."""
+    rng = np.random.default_rng(11)
+    C, P, L, X = 20000, 12, 3000, 3000
+    p = C
+    path = np.arange(C + 1, C + 1 + P)
+    chain = np.arange(C + 1 + P, C + 1 + P + L)
+    sinks = np.arange(chain[-1] + 1, chain[-1] + 1 + X)
+    srcs = np.arange(sinks[-1] + 1, sinks[-1] + 1 + X)
+    n = int(srcs[-1]) + 1
+    src, dst = [], []
+    core = np.arange(C)
+    src += list(core); dst += list((core + 1) % C)                      # the core is one cycle ...
+    e = 20 * C
+    src += list(rng.integers(0, C, e)); dst += list(rng.integers(0, C, e))  # ... and dense
+    src += [p] + list(path[:-1]) + [int(path[-1])]; dst += list(path) + [0]  # p -> path -> core
+    src += [1] + list(chain[:-1]) + [int(chain[-1])]; dst += list(chain) + [p]  # core -> chain -> p
+    src += [p] * X + list(srcs); dst += list(sinks) + [p] * X
+    return n, np.array(src, np.uint32), np.array(dst, np.uint32)
+
+
+def test_bottom_up_then_worklist(ctx):
+    import torch
+
+    n, s, d = _path_core_chain_graph()
+    G = KG.from_edges(ctx, n, torch.from_numpy(s.view(np.int32)).cuda(), torch.from_numpy(d.view(np.int32)).cuda())
+    fwh, fwc, bwh, bwc = G.to_host()
+    want = O.tarjan(O.Graph(n, fwh, fwc, bwh, bwc))
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    for _ in range(2):
+        st = K.Stats()
+        ctx.scc_device(n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, K.default_options(validate=0), st)
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), want)
+        dct = st.as_dict()
+        assert dct["levels_bottom_up"] > 0, "the search should run bottom-up levels in the core"
+        assert dct["fwbw_joint"] == 1, "and finish on the worklist after them"
