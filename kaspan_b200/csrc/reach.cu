@@ -954,7 +954,10 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, 
   uint64_t      slot        = 0;
   unsigned      spins       = 0;
   for (bool alive = true; alive;) {
-    if (!batch) {
+    if (!batch && ls_n == 0) {
+      // only a warp without its own work claims slots: items appended to
+      // the worklist then land with warps that are polling, not behind a
+      // busy warp's round
       unsigned long long base = 0;
       if (lane == 0) base = atomicAdd(head, 32ull);
       slot    = __shfl_sync(0xFFFFFFFFu, base, 0) + lane;
