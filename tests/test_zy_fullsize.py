@@ -1,6 +1,6 @@
 """Full-size parity (run with KSPN_FULLSIZE=1; minutes of CPU time for the
-reference's Tarjan): the BASELINE shapes generated on the device at their
-full size, decomposed by the FAST pipeline, and compared bit for bit with
+reference's Tarjan): R-MAT s24 / s26, RGG 2^24 and G(2^16, 2^19) generated on
+the device at their full size, decomposed by the FAST pipeline, and compared bit for bit with
 the reference's own Tarjan (oracle/_ref, tarjan.hpp:20-136) on the same CSR.
 Collected before test_zz_no_alloc.py."""
 from __future__ import annotations
