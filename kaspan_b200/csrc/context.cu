@@ -79,7 +79,7 @@ layout(workspace& ws, char* base, uint32_t n, uint64_t m)
   ws.seed_prefix       = c.take<uint64_t>(4);
   ws.gbar              = c.take<char>(4096);
   ws.heavy_cap         = heavy_capacity(n, m);
-  ws.aw_entries        = 2 * nn + 64 + 2 * (m / HEAVY_SLICE) + 64; // every vertex once per direction, every slice of a heavy row (both directions) once
+  ws.aw_entries        = 4 * nn + 2 * AW_STALE + 4 * (m / HEAVY_SLICE) + 128; // see run_async: half for duplicates, the passes around the switch, one winning item per vertex and direction, the heavy-row slices
   ws.aw                = c.take<unsigned long long>(ws.aw_entries);
   ws.rstate            = c.take<char>(4096);
   ws.heavy             = c.take<uint32_t>(4 * ws.heavy_cap);

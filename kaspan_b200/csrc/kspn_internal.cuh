@@ -59,6 +59,14 @@ bit_take(uint32_t* bm, uint32_t v)
   return (atomicAnd(bm + (v >> 5), ~mask) & mask) != 0;
 }
 
+// Sets bit v without waiting for the old word (no result: the atomic is
+// issued and the thread goes on).
+__device__ __forceinline__ void
+bit_set_async(uint32_t* bm, uint32_t v)
+{
+  atomicOr(bm + (v >> 5), 1u << (v & 31));
+}
+
 // Sets bit v; true iff this call set it.
 __device__ __forceinline__ bool
 bit_claim(uint32_t* bm, uint32_t v)
@@ -118,6 +126,11 @@ warp_push_active(uint32_t v, uint32_t* queue, uint32_t* count)
 // HEAVY_SLICE edges of every listed row.
 constexpr uint32_t HEAVY_ROW   = 2048;
 constexpr uint32_t HEAVY_SLICE = 1024;
+// Worklist items that the passes of every warp of the persistent search can
+// push around its switch to exact takes: two passes of at most 32 lanes x 8
+// finds for each of AW_GRID_MAX blocks x 8 warps.
+constexpr int    AW_GRID_MAX = 1024;
+constexpr size_t AW_STALE    = size_t(2) * AW_GRID_MAX * 8 * 32 * 8;
 
 // Entries of one heavy list: a list holds each vertex at most once per
 // direction, and only vertices with a row longer than HEAVY_ROW (at most
@@ -301,7 +314,7 @@ struct workspace
   uint64_t* seed_prefix = nullptr; // 4
   void*     gbar        = nullptr; // 4 KiB: grid barrier of the persistent FW-BW at 0, worklist counters at 1024 (zeroed at creation)
   void*     aw          = nullptr; // aw_entries u64: worklist of the asynchronous search tail (zeroed at creation, zero outside a phase)
-  size_t    aw_entries  = 0;       // 2 (n + 2) + 64 vertex items (FW and BW at once) + 2 m / HEAVY_SLICE + 64 row-slice items
+  size_t    aw_entries  = 0;       // 4 (n + 2) + 2 AW_STALE vertex items (FW and BW at once, duplicate pushes) + 4 m / HEAVY_SLICE + 128 row-slice items
   void*     rstate      = nullptr; // 4 KiB device control blocks (FW-BW at 0, trim at 512, search stamps at 2048)
   uint32_t* heavy       = nullptr; // 4 heavy lists of heavy_cap entries (persistent FW-BW: trim seed, two trim push levels, cut bottom-up rows)
   uint64_t  heavy_cap   = 0;

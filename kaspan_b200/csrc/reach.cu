@@ -879,7 +879,9 @@ aw_push(uint32_t v, unsigned long long* aw, unsigned long long* tail, uint64_t c
 // warps pick them up.  Stack entries are items (below) with slice 0.
 constexpr uint32_t           AW_LOCAL_KEEP = 8;
 constexpr unsigned long long AW_BW         = 1ull << 63; // item of the BW search of a joint phase
+constexpr unsigned long long AW_TAKEN      = 1ull << 62; // the vertex was taken when it was pushed (else its consumer takes it)
 static_assert(sizeof(bu_warp_smem) >= AW_LOCAL_KEEP * sizeof(unsigned long long), "local stack must fit the warp buffer");
+static_assert(R_THREADS / 32 == 8 && AW_BATCH == 8, "AW_STALE counts 8 warps per block and 8 finds per lane per pass");
 
 // One search's arrays in the worklist phase: rows to walk, the candidates a
 // find is taken from, the set it joins.
@@ -939,9 +941,9 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, 
   unsigned const            lt   = (1u << lane) - 1u;
   bool const                joint = d1 != nullptr;
   aw_dir const              e1    = joint ? *d1 : d0;
-  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; i < qn; i += static_cast<uint64_t>(gridDim.x) * R_THREADS) __stcg(aw + i, AW_TAG | __ldcg(fq + i));
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; i < qn; i += static_cast<uint64_t>(gridDim.x) * R_THREADS) __stcg(aw + i, AW_TAG | AW_TAKEN | __ldcg(fq + i));
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    if (joint) __stcg(aw + qn, AW_TAG | AW_BW | seed1);
+    if (joint) __stcg(aw + qn, AW_TAG | AW_TAKEN | AW_BW | seed1);
     *head = 0, *tail = qn + (joint ? 1u : 0u), *done = 0;
   }
   if (!grid_sync(a.bar, epoch)) return SEARCH_FAILED;
@@ -949,6 +951,16 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, 
   bool          failed      = false;
   uint32_t      unpublished = 0; // worklist items this warp finished, not yet added to done
   uint32_t      ls_n        = 0; // items on this warp's stack (warp-uniform)
+  // A find whose probe shows it available is pushed without taking it:
+  // its consumer takes it (the atomic issued beside the row-offset loads,
+  // so the hop waits for one of them, not both) and drops the item if
+  // another push of the same vertex won.  Duplicate items use worklist
+  // slots, so once this warp's last reservation passed half of them it
+  // takes its finds itself (exactly, AW_TAKEN); the worklist holds
+  // 4n + 2 AW_STALE + 4m / HEAVY_SLICE items: half, the passes of every
+  // warp around the switch, one winning item per vertex and direction, and
+  // the slices (only a winner appends them).
+  bool          exact       = false; // warp-uniform
   bool          batch       = false;
   bool          pending     = false;
   uint64_t      slot        = 0;
@@ -996,18 +1008,26 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, 
     unsigned const gmask = __ballot_sync(0xFFFFFFFFu, got);
     if (gmask) {
       uint32_t const           v   = static_cast<uint32_t>(item);
-      uint32_t const           sl  = static_cast<uint32_t>(item >> 33) & 0x3FFFFFFFu;
+      uint32_t const           sl  = static_cast<uint32_t>(item >> 33) & 0x1FFFFFFFu;
       unsigned long long const dir = item & AW_BW;
       aw_dir const             d   = dir ? e1 : d0;
       uint64_t                 b = 0, e = 0;
-      if (got) b = d.head[v], e = d.head[v + 1];
+      bool                     won = got;
+      if (got) {
+        // an untaken item: take it now (the atomic and the offset loads in
+        // flight together); a lost take means a duplicate, which is dropped
+        if (!(item & AW_TAKEN) && sl == 0) won = bit_take(d.avail, v);
+        b = d.head[v], e = d.head[v + 1];
+        if (!(item & AW_TAKEN) && sl == 0 && won) bit_set_async(d.mark, v);
+        if (!won) e = b;
+      }
       if (got && e - b > HEAVY_ROW) {
         if (sl == 0) {
-          // the row's other slices become items
+          // the row's other slices become items (by the winner only)
           uint64_t const           ns = (e - b + HEAVY_SLICE - 1) / HEAVY_SLICE;
           unsigned long long const at = atomicAdd(tail, static_cast<unsigned long long>(ns - 1));
           for (uint64_t j = 1; j < ns; ++j)
-            if (at + j - 1 < cap) __stcg(aw + at + j - 1, AW_TAG | dir | (static_cast<unsigned long long>(j) << 33) | v);
+            if (at + j - 1 < cap) __stcg(aw + at + j - 1, AW_TAG | AW_TAKEN | dir | (static_cast<unsigned long long>(j) << 33) | v);
         }
         b += static_cast<uint64_t>(sl) * HEAVY_SLICE;
         e = b + HEAVY_SLICE < e ? b + HEAVY_SLICE : e;
@@ -1018,6 +1038,7 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, 
       // then the takes; the warp's finds placed with at most one atomic per pass
       uint64_t x = got && !big ? b : e;
       while (__any_sync(0xFFFFFFFFu, x < e)) {
+        unsigned long long const tk = exact ? AW_TAKEN : 0ull; // the pass's finds were taken here
         uint32_t w[AW_BATCH], found = 0;
 #pragma unroll
         for (int k = 0; k < AW_BATCH; ++k) w[k] = x + k < e ? d.adj[x + k] : 0u;
@@ -1026,7 +1047,10 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, 
         for (int k = 0; k < AW_BATCH; ++k) wd[k] = x + k < e ? __ldcg(d.avail + (w[k] >> 5)) : 0u;
 #pragma unroll
         for (int k = 0; k < AW_BATCH; ++k)
-          if (x + k < e && ((wd[k] >> (w[k] & 31)) & 1u) && bit_take(d.avail, w[k])) bit_claim(d.mark, w[k]), found |= 1u << k;
+          if (x + k < e && ((wd[k] >> (w[k] & 31)) & 1u)) {
+            if (!exact) found |= 1u << k;
+            else if (bit_take(d.avail, w[k])) bit_set_async(d.mark, w[k]), found |= 1u << k;
+          }
         uint32_t const c = __popc(found);
         uint32_t       p = c;
 #pragma unroll
@@ -1039,10 +1063,11 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, 
           unsigned long long gbase;
           uint32_t           nloc;
           uint32_t const     next = sink.reserve(ls_n, tot, gbase, nloc);
+          exact                   = exact || gbase > cap / 2;
           uint32_t           q    = p - c;
 #pragma unroll
           for (int k = 0; k < AW_BATCH; ++k)
-            if ((found >> k) & 1u) sink.put(ls_n, nloc, gbase, q++, AW_TAG | dir | w[k]);
+            if ((found >> k) & 1u) sink.put(ls_n, nloc, gbase, q++, AW_TAG | tk | dir | w[k]);
           ls_n = next;
         }
         x = x + AW_BATCH < e ? x + AW_BATCH : e;
@@ -1058,15 +1083,20 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, 
           bool           f  = false;
           if (x1 < e0) {
             w = dd_.adj[x1];
-            f = ((__ldcg(dd_.avail + (w >> 5)) >> (w & 31)) & 1u) && bit_take(dd_.avail, w);
-            if (f) bit_claim(dd_.mark, w);
+            f = ((__ldcg(dd_.avail + (w >> 5)) >> (w & 31)) & 1u) != 0;
+            if (f && exact) {
+              f = bit_take(dd_.avail, w);
+              if (f) bit_set_async(dd_.mark, w);
+            }
           }
           unsigned const fm = __ballot_sync(0xFFFFFFFFu, f);
           if (fm) {
             unsigned long long gbase;
             uint32_t           nloc;
             uint32_t const     next = sink.reserve(ls_n, __popc(fm), gbase, nloc);
-            if (f) sink.put(ls_n, nloc, gbase, __popc(fm & lt), AW_TAG | dl | w);
+            unsigned long long const tk = exact ? AW_TAKEN : 0ull; // before this chunk's switch
+            exact                       = exact || gbase > cap / 2;
+            if (f) sink.put(ls_n, nloc, gbase, __popc(fm & lt), AW_TAG | tk | dl | w);
             ls_n = next;
           }
         }
@@ -2094,7 +2124,9 @@ fwbw_grid(kspn_context* ctx)
     KSPN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_fwbw, R_THREADS, 0));
     KSPN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
     if (bps < 1) throw error{ KSPN_ERR_CUDA, "persistent FW-BW kernel does not fit on an SM" };
-    ctx->search_grid = static_cast<unsigned>(std::min(bps * sms, 4000));
+    // at most AW_GRID_MAX blocks: the worklist's spare slots (AW_STALE)
+    // are sized for that many warps
+    ctx->search_grid = static_cast<unsigned>(std::min<int>(bps * sms, AW_GRID_MAX));
   }
   return ctx->search_grid;
 }
