@@ -877,7 +877,7 @@ aw_push(uint32_t v, unsigned long long* aw, unsigned long long* tail, uint64_t c
 // loads of one expansion, not a trip through the worklist to whichever warp
 // claimed the slot.  Finds past AW_LOCAL_KEEP go to the worklist, where idle
 // warps pick them up.  Stack entries are items (below) with slice 0.
-constexpr uint32_t           AW_LOCAL_KEEP = 8;
+constexpr uint32_t           AW_LOCAL_KEEP = 16;
 constexpr unsigned long long AW_BW         = 1ull << 63; // item of the BW search of a joint phase
 constexpr unsigned long long AW_TAKEN      = 1ull << 62; // the vertex was taken when it was pushed (else its consumer takes it)
 static_assert(sizeof(bu_warp_smem) >= AW_LOCAL_KEEP * sizeof(unsigned long long), "local stack must fit the warp buffer");
