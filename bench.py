@@ -14,10 +14,17 @@ value   = edges of the graph / device time per step (CUDA events on the
 e2e     = the same metric through the host C-ABI call kspn_scc with pinned
           HOST buffers: forward CSR copied in, transpose built on the device,
           labels copied out, every step.
-roofline: the dominant kernel class's algorithmic bytes / its event-timed
+roofline: the dominant kernel's algorithmic bytes / its event-timed
           duration, against MEASURED_PEAKS.json's HBM copy bandwidth.
 cpu_baseline: the reference's own kaspan::scc (oracle/_ref, compiled from its
-          sources; 1 core, MPI absent) on a bounded sample of the workload.
+          sources; 1 core, MPI absent) on the same graph, one call.
+rmat26  = the R-MAT scale-26 configuration (the learned-pivot one): device
+          time, learned vs plain pivot, end to end, roofline.
+
+--impl reference: the reference's kaspan::scc on the host cores, one call per
+step on the identical graph (the oracle's C generator draws the same edges
+as the device generator), except R-MAT s26, whose one-rank reference call
+takes about a minute: its reference arm decomposes R-MAT s24.
 
 Multi-GPU (torchrun): every rank decomposes its own seeded instance (seed +
 rank); value = edges over all ranks / max-over-ranks time ("weak" scaling,
@@ -49,8 +56,10 @@ WORKLOADS = {
     "rgg24": ("rgg", dict(n=1 << 24, seed=3), "2D random geometric graph n=2^24, mean undirected degree 8, each pair u->v / v->u / both / neither with p=.25"),
     "rgg20": ("rgg", dict(n=1 << 20, seed=3), "2D random geometric graph n=2^20, mean undirected degree 8, each pair u->v / v->u / both / neither with p=.25"),
 }
-# bounded CPU sample of each workload for the reference arm / cpu_baseline
-CPU_SAMPLE = {"rmat24": "rmat22", "rmat26": "rmat22", "gnm16": "gnm16", "rmat22": "rmat22", "rmat20": "rmat20", "rgg24": "rgg20", "rgg20": "rgg20"}
+# The reference arm decomposes the identical graph, except where one
+# reference call takes about a minute (R-MAT s26: 1.06 B edges and a 16 GiB
+# hash set at one rank), so W + K calls would not end within minutes.
+REFERENCE_GRAPH = {"rmat26": "rmat24"}
 
 
 def measured_peak_gbs():
@@ -120,41 +129,59 @@ def make_graph(ctx, name, rank_seed=0):
     return KG.gnm(ctx, p["n"], p["draws"], p["seed"] + rank_seed)
 
 
-def cpu_reference_sample(name, steps=1, warmup=0, threads_note=True):
-    """Reference kaspan::scc (oracle/_ref) on the CPU sample of `name`:
-    returns (edges/s list per timed step, sample description, m)."""
+def host_graph(name):
+    """The workload graph on the host, drawn by the oracle's C generators
+    (the same edges as the device generators, tested bit-identical)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    kind, p, _ = WORKLOADS[name]
+    if kind == "rmat":
+        return O.rmat(p["scale"], p["ef"], p["seed"])
+    if kind == "rgg":
+        return O.rgg(p["n"], p["seed"])
+    return O.gnm(p["n"], p["draws"], p["seed"])
+
+
+def reference_calls(G, steps, warmup=0):
+    """The reference's kaspan::scc (oracle/_ref) on host graph G: edges/s of
+    each timed call, or None when oracle/_ref is absent."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
     if O.ref_lib() is None:
         return None
-    sname = CPU_SAMPLE[name]
-    kind, p, desc = WORKLOADS[sname]
-    G = O.rmat(p["scale"], p["ef"], p["seed"]) if kind == "rmat" else (O.rgg(p["n"], p["seed"]) if kind == "rgg" else O.gnm(p["n"], p["draws"], p["seed"]))
     for _ in range(warmup):
         O.ref_scc(G)
-    rates = []
-    for _ in range(steps):
-        _, secs = O.ref_scc(G)
-        rates.append(G.m / secs)
-    return rates, f"{desc}: n={G.n}, m={G.m}; one kaspan::scc call per step (reference code, 1 rank, 1 core)", G.m
+    return [G.m / O.ref_scc(G)[1] for _ in range(steps)]
 
 
 def run_reference(args):
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    res = cpu_reference_sample(args.workload, steps=args.steps, warmup=args.warmup)
-    if res is None:
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    if O.ref_lib() is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libkspn_ref.so was not built (reference sources absent at build time)"}))
         return 0
-    rates, sample, m = res
+    gname = REFERENCE_GRAPH.get(args.workload, args.workload)
+    G = host_graph(gname)
+    rates = reference_calls(G, args.steps, args.warmup)
     v = statistics.mean(rates)
+    same = gname == args.workload
+    sample = (f"the workload graph itself ({WORKLOADS[gname][2]}: n={G.n}, m={G.m}), one kaspan::scc call per step "
+              "(reference code compiled from its sources, 1 rank, 1 core)")
+    if not same:
+        sample = (f"{WORKLOADS[gname][2]} (n={G.n}, m={G.m}) standing in for {WORKLOADS[args.workload][2]}: one reference "
+                  "call on the full workload takes about a minute; one kaspan::scc call per step (1 rank, 1 core)")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * m / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-        "data": "synthetic (seeded generators standing in for KaGen R-MAT / G(n,m))",
-        "config": {"workload": WORKLOADS[args.workload][2], "sample": sample, "mpi": "absent on this host: single rank"},
+        "ms_per_step": 1e3 * G.m / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded generators standing in for KaGen R-MAT / G(n,m) / RGG)",
+        "config": {"workload": WORKLOADS[args.workload][2], "n": G.n, "m": G.m, "same_graph": same, "sample": sample,
+                   "mpi": "absent on this host: single rank"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -251,6 +278,114 @@ def run_batched(ctx, stream, args, K, world=1, rank=0):
     return res
 
 
+def timed_steps(ctx, stream, G, opt, steps, out):
+    """`steps` decompositions of device graph G back to back between two
+    CUDA events on the library's stream: (ms per step, Stats of each step)."""
+    import torch
+
+    import kaspan_b200 as K
+
+    stats = [K.Stats() for _ in range(steps)]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(steps):
+        ctx.scc_device(G.n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, opt, stats[i])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, stats
+
+
+def resident_roofline(step_stats, peak):
+    """The resident launch k_fwbw over the timed steps: algorithmic bytes per
+    launch (its device counters) / its CUDA-event duration."""
+    res = [d["resident"] for d in step_stats if d["resident"]["ms"] > 0]
+    if not res:
+        return None
+    kms = sum(r["ms"] for r in res) / len(res)
+    kbytes = sum(r["bytes"] for r in res) / len(res)
+    achieved = (kbytes / (kms * 1e-3)) / 1e9
+    return {"kernel": "k_fwbw", "achieved": achieved, "frac": achieved / peak, "bytes_per_step": kbytes, "ms_per_step": kms}
+
+
+def host_e2e(ctx, stream, G, opt, steps, warmup):
+    """kspn_scc with pinned host buffers (forward CSR in, transpose built on
+    the device, labels out) every step: (ms per step, labels of the last)."""
+    import numpy as np
+    import torch
+
+    fwh_h = G.fwh.cpu().pin_memory()
+    fwc_h = G.fwc.cpu().pin_memory()
+    out_h = torch.empty(G.n, dtype=torch.int32).pin_memory()
+    for _ in range(warmup):
+        ctx.scc_host_ptr(G.n, G.m, fwh_h, fwc_h, None, None, out_h, opt)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(steps):
+        ctx.scc_host_ptr(G.n, G.m, fwh_h, fwc_h, None, None, out_h, opt)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3) / steps
+    return ms, out_h.numpy().view(np.uint32).copy()
+
+
+def learned_vs_plain(ctx, stream, graph, pipeline, steps):
+    """The same graph decomposed from the plain pivot (largest in * out) and
+    from the learned one; identical output asserted."""
+    import numpy as np
+    import torch
+
+    import kaspan_b200 as K
+
+    o = torch.empty(graph.n, dtype=torch.int32, device="cuda")
+    res = {"n": graph.n, "m": graph.m}
+    ids = {}
+    for name, opt in (("plain", K.default_options(pipeline=pipeline, validate=0)),
+                      ("learned", K.default_options(pipeline=pipeline, validate=0, learned_pivot=1))):
+        timed_steps(ctx, stream, graph, opt, 1, o)
+        ms, st = timed_steps(ctx, stream, graph, opt, steps, o)
+        d = st[-1].as_dict()
+        ids[name] = o.cpu().numpy().view(np.uint32).copy()
+        res[name] = {"ms_per_step": ms, "edges_scanned": d["edges_scanned"], "pivot": d["pivot"], "fwbw_decided": d["decided"]["fwbw"]}
+    assert np.array_equal(ids["plain"], ids["learned"]), "learned and plain pivots must give the same partition"
+    res["speedup"] = res["plain"]["ms_per_step"] / res["learned"]["ms_per_step"]
+    res["identical_output"] = True
+    return res
+
+
+def run_rmat26(ctx, stream, args, peak, K):
+    """R-MAT scale 26 (n = 2^26, 1.06 B edges, CSR + CSC 9.5 GB), the
+    learned-pivot configuration: device time per decomposition, k_fwbw's
+    roofline, learned vs plain pivot, and end to end through kspn_scc."""
+    import torch
+
+    import kaspan_b200.graphs as KG
+
+    G = KG.rmat(ctx, 26, 16, 4)
+    out = torch.empty(G.n, dtype=torch.int32, device="cuda")
+    opt = K.default_options(validate=0)
+    steps = max(3, min(args.steps, 10))
+    timed_steps(ctx, stream, G, opt, 3, out)
+    ms, st = timed_steps(ctx, stream, G, opt, steps, out)
+    dicts = [s.as_dict() for s in st]
+    res = {"workload": WORKLOADS["rmat26"][2], "n": G.n, "m": G.m, "steps": steps, "value": G.m / (ms * 1e-3), "unit": UNIT,
+           "ms_per_step": ms, "roofline": resident_roofline(dicts, peak),
+           "pipeline_frac": (2 * (8 * (G.n + 1) + 4 * G.m) + 4 * G.n) / (ms * 1e-3) / 1e9 / peak}
+    model = K.default_pivot_model()
+    if model is not None:
+        ctx.set_pivot_model(model)
+        res["learned_vs_plain"] = learned_vs_plain(ctx, stream, G, K.PIPELINE_FAST, steps)
+        ctx.set_pivot_model(None)
+    e2e_ms, _ = host_e2e(ctx, stream, G, K.default_options(validate=0), 3, 1)
+    res["e2e"] = {"value": G.m / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms, "h2d_bytes_per_step": 8 * (G.n + 1) + 4 * G.m,
+                  "d2h_bytes_per_step": 4 * G.n}
+    res["cpu_baseline"] = {"note": "not run by default: one reference kaspan::scc call on this graph takes about a minute at one rank"}
+    del G, out
+    torch.cuda.empty_cache()
+    return res
+
+
 def run_kspn(args):
     import numpy as np
     import torch
@@ -275,6 +410,7 @@ def run_kspn(args):
     opt = K.default_options(pipeline=pipeline, validate=0)
     prof_opt = K.default_options(pipeline=pipeline, validate=0, profile=1)
     trace_opt = K.default_options(pipeline=pipeline, validate=0, trace=1)
+    peak, peak_kind = measured_peak_gbs()
 
     def barrier():
         if world > 1:
@@ -299,6 +435,7 @@ def run_kspn(args):
     step_stats = [s.as_dict() for s in stats_objs]
     launches = ctx.launches - l0
     ms = ev0.elapsed_time(ev1) / args.steps
+    ids = out.cpu().numpy().view(np.uint32).copy()
     # phase stamps of the persistent searches (one extra step, not timed)
     ctx.scc_device(G.n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, trace_opt, st)
     marks = st.as_dict()["search_marks"]
@@ -312,6 +449,7 @@ def run_kspn(args):
     # kernel launch is bracketed on the library's stream)
     agg = {k: [0.0, 0, 0] for k in K.KERNEL_CLASSES}
     prof_steps = args.profile_steps if args.profile_steps is not None else max(1, min(args.steps, 3))
+    trace = []
     for _ in range(prof_steps):
         ctx.scc_device(G.n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, prof_opt, st)
         trace = st.as_dict()["trace"]
@@ -333,39 +471,18 @@ def run_kspn(args):
     # ---- learned vs plain pivot (same output): the workload, and the
     # workload with decoy hubs (vertices whose in * out beats every real one
     # while their out-edges all end at dead ends)
-    learned_vs_plain = None
+    lvp = None
     model = K.default_pivot_model()
     if model is not None and args.workload.startswith("rmat") and world == 1:
         from kaspan_b200.pivot_train import decoy_rmat
 
-        def timed(graph, options, steps):
-            o = torch.empty(graph.n, dtype=torch.int32, device="cuda")
-            s_ = K.Stats()
-            ctx.scc_device(graph.n, graph.m, graph.fwh, graph.fwc, graph.bwh, graph.bwc, o, options, s_)
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            for _ in range(steps):
-                ctx.scc_device(graph.n, graph.m, graph.fwh, graph.fwc, graph.bwh, graph.bwc, o, options, s_)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            d = s_.as_dict()
-            return o.cpu().numpy().view(np.uint32).copy(), {"ms_per_step": e0.elapsed_time(e1) / steps, "edges_scanned": d["edges_scanned"],
-                                                            "pivot": d["pivot"], "fwbw_decided": d["decided"]["fwbw"]}
-
         ctx.set_pivot_model(model)
-        learned_vs_plain = {"model": "kaspan_b200/pivot_model.npy (8-32-32-1, trained on the GPU: python -m kaspan_b200.pivot_train)"}
-        for label, graph in (("workload", G), ("workload_with_decoys", None)):
-            if graph is None:
-                p_ = WORKLOADS[args.workload][1]
-                graph, hubs = decoy_rmat(ctx, p_["scale"], p_["seed"] + 100, 0.57, decoys=8)
-            ids_p, plain = timed(graph, opt, max(3, min(args.steps, 10)))
-            ids_l, learned = timed(graph, K.default_options(pipeline=pipeline, validate=0, learned_pivot=1), max(3, min(args.steps, 10)))
-            assert np.array_equal(ids_p, ids_l), "learned and plain pivots must give the same partition"
-            learned_vs_plain[label] = {"n": graph.n, "m": graph.m, "plain": plain, "learned": learned,
-                                       "speedup": plain["ms_per_step"] / learned["ms_per_step"], "identical_output": True}
-            if label != "workload":
-                del graph
+        lvp = {"model": "kaspan_b200/pivot_model.npy (8-32-32-1, trained on the GPU: python -m kaspan_b200.pivot_train)"}
+        lvp["workload"] = learned_vs_plain(ctx, stream, G, pipeline, max(3, min(args.steps, 10)))
+        p_ = WORKLOADS[args.workload][1]
+        Gd, _hubs = decoy_rmat(ctx, p_["scale"], p_["seed"] + 100, 0.57, decoys=8)
+        lvp["workload_with_decoys"] = learned_vs_plain(ctx, stream, Gd, pipeline, max(3, min(args.steps, 10)))
+        del Gd
         ctx.set_pivot_model(None)
         torch.cuda.empty_cache()
 
@@ -384,30 +501,16 @@ def run_kspn(args):
         batched = run_batched(ctx, stream, args, K, world, rank)
 
     # correctness spot check of the last step (canonical ids are min members)
-    ids = out.cpu().numpy().view(np.uint32)
     assert (ids <= np.arange(G.n, dtype=np.uint32)).all(), "ids must name a member no larger than the vertex"
 
     # ---- end to end through the host C ABI (pinned buffers, bw built on device)
-    fwh_h = G.fwh.cpu().pin_memory()
-    fwc_h = G.fwc.cpu().pin_memory()
-    out_h = torch.empty(G.n, dtype=torch.int32).pin_memory()
-    e2e_opt = K.default_options(pipeline=opt.pipeline, validate=0)
-    for _ in range(max(1, min(args.warmup, 2))):
-        ctx.scc_host_ptr(G.n, G.m, fwh_h, fwc_h, None, None, out_h, e2e_opt)
     barrier()
-    e2e_steps = max(1, min(args.steps, 5))
-    t0 = time.perf_counter()
-    ev0.record(stream)
-    for _ in range(e2e_steps):
-        ctx.scc_host_ptr(G.n, G.m, fwh_h, fwc_h, None, None, out_h, e2e_opt)
-    ev1.record(stream)
-    barrier()
-    e2e_ms = max(ev0.elapsed_time(ev1), (time.perf_counter() - t0) * 1e3) / e2e_steps
+    e2e_ms, e2e_ids = host_e2e(ctx, stream, G, K.default_options(pipeline=opt.pipeline, validate=0), max(1, min(args.steps, 5)), max(1, min(args.warmup, 2)))
     if world > 1:
         t = torch.tensor([e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    assert np.array_equal(out_h.numpy().view(np.uint32), ids), "host path and device path disagree"
+    assert np.array_equal(e2e_ids, ids), "host path and device path disagree"
     h2d = 8 * (G.n + 1) + 4 * G.m
     d2h = 4 * G.n
 
@@ -415,28 +518,27 @@ def run_kspn(args):
     # FW-BW, trim fixpoint and every id in one persistent kernel), timed by
     # the library's CUDA events around that launch on its stream, with the
     # algorithmic bytes its device counters give (model in include/kspn.h)
-    peak, peak_kind = measured_peak_gbs()
-    res = [d["resident"] for d in step_stats if d["resident"]["ms"] > 0]
-    dom = "k_fwbw"
-    if res:
-        kms = sum(r["ms"] for r in res) / len(res)
-        kbytes = sum(r["bytes"] for r in res) / len(res)
-        kcalls = 1.0
-    else:  # the call did not take the resident path (profiled or oversized)
+    roof = resident_roofline(step_stats, peak)
+    if roof is None:  # the call did not take the resident path (profiled or oversized)
         dom = max(agg, key=lambda k: agg[k][0])
-        kms, kbytes, kcalls = (x / prof_steps for x in agg[dom])
-    achieved = (kbytes / (kms * 1e-3)) / 1e9 if kms > 0 else 0.0
+        kms, kbytes, _ = (x / prof_steps for x in agg[dom])
+        a_ = (kbytes / (kms * 1e-3)) / 1e9 if kms > 0 else 0.0
+        roof = {"kernel": dom, "achieved": a_, "frac": a_ / peak, "bytes_per_step": kbytes, "ms_per_step": kms}
     traffic, traffic_note = None, None
     tp = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tp):
         try:
             tj = json.load(open(tp))
-            traffic = tj.get(f"{args.workload}:{dom}")
-            traffic_note = tj.get(f"{args.workload}:{dom}:note", "one ncu capture of this workload's launch")
+            traffic = tj.get(f"{args.workload}:{roof['kernel']}")
+            traffic_note = tj.get(f"{args.workload}:{roof['kernel']}:note")
         except Exception:
             traffic = None
     last = step_stats[-1]
     b_min = 2 * (8 * (G.n + 1) + 4 * G.m) + 4 * G.n
+
+    rmat26 = None
+    if rank == 0 and world == 1 and args.workload == "rmat24" and not args.no_rmat26:
+        rmat26 = run_rmat26(ctx, stream, args, peak, K)
 
     if rank == 0:
         line = {
@@ -447,15 +549,15 @@ def run_kspn(args):
                        "parallelism": f"{world} independent instance(s), one per GPU", "l2": "inputs larger than L2 (126 MB)"},
             "e2e": {"value": m_total / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "roofline": {"bound": "hbm", "kernel": roof["kernel"], "achieved": roof["achieved"], "peak": peak, "unit": "GB/s", "frac": roof["frac"],
                          "traffic": traffic, "traffic_source": traffic_note, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_kind})",
-                         "bytes_per_step": kbytes, "ms_per_step": kms, "calls_per_step": kcalls,
-                         "timing": (f"CUDA events around the {dom} launch on the library stream, every timed step" if res else
-                                    f"CUDA events around each {dom} launch on the library stream, {prof_steps} profiled steps after the timed ones"),
+                         "bytes_per_step": roof["bytes_per_step"], "ms_per_step": roof["ms_per_step"], "calls_per_step": 1.0,
+                         "timing": f"CUDA events around the {roof['kernel']} launch on the library stream, every timed step",
                          "model": last["resident"],
                          "pipeline_min_bytes": b_min, "pipeline_frac": (b_min / (ms * 1e-3)) / 1e9 / peak},
             "clocks": clk.summary(),
-            "learned_vs_plain": learned_vs_plain,
+            "learned_vs_plain": lvp,
+            "rmat26": rmat26,
             "autotune": autotune,
             "batched": batched,
             "phases": {"decided": last["decided"], "ms": {k: round(v, 4) for k, v in last["ms"].items()}, "levels_fw": last["levels_fw"],
@@ -463,13 +565,18 @@ def run_kspn(args):
                        "edges_scanned": last["edges_scanned"], "trace": trace,
                        "search_phase_ms": {{4: "expand", 5: "sweep", 7: "materialize", 8: "init", 9: "end", 10: "finalize", 11: "trim_seed", 12: "trim_level", 13: "worklist", 14: "fix_up", 15: "trim_heavy", 16: "trim_worklist"}.get(k, k): round(v, 4) for k, v in search_phases.items()},
                        "kernels": {k: {"ms": round(a[0] / prof_steps, 4), "GB/s": round(a[1] / (a[0] * 1e-3) / 1e9, 1) if a[0] else 0}
-                                                                            for k, a in agg.items()}},
+                                   for k, a in agg.items()}},
         }
-        if not args.no_cpu_baseline:
-            res = cpu_reference_sample(args.workload, steps=1, warmup=0)
-            if res is not None:
-                rates, sample, _ = res
-                line["cpu_baseline"] = {"value": rates[0], "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample}
+        if not args.no_cpu_baseline and world == 1:
+            # the reference's kaspan::scc on this very graph (its host copy), one call
+            fwh, fwc, bwh, bwc = G.to_host()
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle as O
+
+            rates = reference_calls(O.Graph(G.n, np.ascontiguousarray(fwh), np.ascontiguousarray(fwc), np.ascontiguousarray(bwh), np.ascontiguousarray(bwc)), 1)
+            if rates is not None:
+                line["cpu_baseline"] = {"value": rates[0], "unit": UNIT, "cores": 1, "kind": "reference",
+                                        "sample": f"the workload graph itself (n={G.n}, m={G.m}), one kaspan::scc call (reference code, 1 rank, 1 core)"}
         print(json.dumps(line))
     ctx.close()
     if world > 1:
@@ -487,6 +594,7 @@ def main():
     ap.add_argument("--pipeline", default="fast", choices=["fast", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-path and autotuner sections")
+    ap.add_argument("--no-rmat26", action="store_true", help="skip the R-MAT scale-26 section")
     ap.add_argument("--profile-steps", type=int, default=None, help="steps run with per-kernel event timing (default min(steps, 3))")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "kspn":

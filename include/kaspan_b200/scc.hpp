@@ -42,8 +42,9 @@ public:
   int status;
 };
 
-// One context per thread on device 0, created on first use (contexts are
-// not shared between threads).
+// One context per thread, created on first use on the thread's current
+// CUDA device (cudaGetDevice at that first call; a later device change on
+// the thread is not followed).  Contexts are not shared between threads.
 inline kspn_context*
 thread_context()
 {
@@ -54,7 +55,7 @@ thread_context()
   };
   thread_local holder h;
   if (!h.ctx) {
-    int const rc = kspn_context_create(0, &h.ctx);
+    int const rc = kspn_context_create(KSPN_DEVICE_CURRENT, &h.ctx);
     if (rc != KSPN_OK) throw error(rc, "kspn_context_create");
   }
   return h.ctx;

@@ -75,7 +75,20 @@ typedef struct kspn_options
   int32_t  trace;           /* 1: timestamp the phases of the persistent searches (kspn_stats.search_*) */
   int32_t  learned_pivot;   /* 1: FAST pipeline picks its FW-BW pivot with the context's pivot model
                                (kspn_set_pivot_model) instead of argmax in*out; same partition */
-  uint32_t reserved[4];
+  /* Test hooks of the resident FW-BW launch; leave them 0 in production.
+   *  wait_limit     polls a grid-barrier or worklist wait makes before it
+   *                 gives up (KSPN_ERR_TIMEOUT); 0 = 2^22 (about half a second)
+   *  drop_barrier   the launch's last block leaves at its k-th grid barrier
+   *                 (k >= 1, counted from the launch start) without arriving,
+   *                 so the other blocks' waits run out: a host-side stand-in
+   *                 for a block that never arrives
+   *  aw_exact_after worklist items after which the search tail's warps take
+   *                 every find themselves instead of leaving the take to its
+   *                 consumer; 0 = half the worklist */
+  uint32_t wait_limit;
+  uint32_t drop_barrier;
+  uint32_t aw_exact_after;
+  uint32_t reserved[1];
 } kspn_options;
 
 /* Per-call statistics (all fields written by a successful call). */
@@ -170,6 +183,9 @@ size_t      kspn_options_size(void);
 size_t      kspn_stats_size(void);
 const char* kspn_strerror(int status);
 const char* kspn_last_error(const kspn_context* ctx); /* detail of the last failure on ctx */
+/* device: a CUDA device ordinal, or KSPN_DEVICE_CURRENT for the calling
+ * thread's current device (cudaGetDevice at creation). */
+#define KSPN_DEVICE_CURRENT (-1)
 int         kspn_context_create(int device, kspn_context** out);
 /* Uses a caller stream (cudaStream_t passed as void*); NULL = a new stream. */
 int         kspn_context_create_on_stream(int device, void* stream, kspn_context** out);
@@ -283,8 +299,10 @@ int kspn_normalise(kspn_context* ctx, uint32_t n, uint32_t* d_scc_id);
  * synchronisation an allocation may cause.  No context is needed: the
  * scratch is a file-scope device array for at most KSPN_NOALLOC_MAX_N
  * vertices (4 MiB, held by every GPU that loads the library until exit).
- *  - n > KSPN_NOALLOC_MAX_N: KSPN_ERR_INVALID_ARGUMENT, nothing runs; an id
- *    >= n is left unchanged and reported as KSPN_ERR_INVALID_ARGUMENT.
+ *  - n > KSPN_NOALLOC_MAX_N: KSPN_ERR_INVALID_ARGUMENT, nothing runs.
+ *  - An id >= n: KSPN_ERR_INVALID_ARGUMENT (kspn_normalise reports
+ *    KSPN_ERR_INTERNAL there), and the array is left PARTLY relabelled: the
+ *    ids >= n are unchanged, every id < n is already relabelled.
  *  - The first call on a device looks up the array's device address; make
  *    that first call before any stream capture.
  *  - All calls share the array: calls that overlap on the GPU race; serialise

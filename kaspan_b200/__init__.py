@@ -69,7 +69,10 @@ class Options(C.Structure):
         ("profile", C.c_int32),
         ("trace", C.c_int32),
         ("learned_pivot", C.c_int32),
-        ("reserved", C.c_uint32 * 4),
+        ("wait_limit", C.c_uint32),
+        ("drop_barrier", C.c_uint32),
+        ("aw_exact_after", C.c_uint32),
+        ("reserved", C.c_uint32 * 1),
     ]
 
 

@@ -645,6 +645,10 @@ kspn_context_create_on_stream(int device, void* stream, kspn_context** out)
 {
   if (!out) return KSPN_ERR_INVALID_ARGUMENT;
   *out      = nullptr;
+  if (device == KSPN_DEVICE_CURRENT && cudaGetDevice(&device) != cudaSuccess) {
+    cudaGetLastError();
+    return KSPN_ERR_NO_DEVICE;
+  }
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count <= device || device < 0) {
     cudaGetLastError();

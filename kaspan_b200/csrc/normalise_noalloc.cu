@@ -19,7 +19,9 @@
 //  * all calls share the one array: calls whose work overlaps on the GPU
 //    (different streams, or different host threads on one device) race and
 //    corrupt each other's result; serialise them;
-//  * the call waits for its stream to finish (it reads back an error word).
+//  * the call waits for its stream to finish (it reads back an error word);
+//  * an id >= n is reported as KSPN_ERR_INVALID_ARGUMENT after the ids < n
+//    were relabelled (the array is left partly relabelled).
 // Each call rewrites the part of the array it uses before reading it, so
 // nothing left by an earlier call leaks into the result.
 #include "kspn_internal.cuh"
@@ -113,6 +115,6 @@ kspn_normalise_noalloc(uint32_t n, uint32_t* d_scc_id, void* stream)
     cudaGetLastError();
     return KSPN_ERR_CUDA;
   }
-  // ids >= n were left as they were, as kspn_normalise leaves them
+  // ids >= n were left as they were; the ids < n are relabelled
   return err ? KSPN_ERR_INVALID_ARGUMENT : KSPN_OK;
 }

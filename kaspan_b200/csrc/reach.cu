@@ -554,7 +554,7 @@ k_bu_cut_clear(gate g, bu_cut cut)
 // is broadcast.  Level counters rotate over three slots: level L reads slot
 // L%3, adds to (L+1)%3 and clears (L+2)%3, which no block touches again
 // until after the next barrier.
-constexpr unsigned GRID_SYNC_SPINS = 1u << 22;
+constexpr unsigned GRID_SYNC_SPINS = 1u << 22; // default wait limit (kspn_options.wait_limit = 0)
 
 // Grid barrier with a monotonically growing counter: every block adds 1
 // with a release reduction (no return value, so arrivals never wait on one
@@ -567,7 +567,7 @@ struct grid_barrier
   unsigned long long root;
   unsigned long long pad0[15];
   unsigned long long epoch; // barriers completed by every block
-  uint32_t           err;   // 1: a wait reached GRID_SYNC_SPINS
+  uint32_t           err;   // 1: a wait reached the wait limit
   uint32_t           pad1[29];
 };
 static_assert(sizeof(grid_barrier) <= 4096, "grid barrier must fit its workspace slot");
@@ -580,27 +580,37 @@ ld_acquire64(unsigned long long const* p)
   return v;
 }
 
+// Barrier count of the running launch at its start (thread 0 of each block
+// sets it before the block's first barrier).
+__shared__ unsigned long long s_epoch0;
+
 // All threads of every block call it.  False when a wait gave up (then every
 // block returns false here or at its next barrier, and the launch ends).
+// `limit` bounds the polls; with drop != 0 the grid's last block leaves the
+// drop-th barrier of the launch without arriving (the test hook of
+// kspn_options.drop_barrier), so the others' waits run out.
 __device__ __forceinline__ bool
-grid_sync(grid_barrier* b, unsigned long long& epoch)
+grid_sync(grid_barrier* b, unsigned long long& epoch, unsigned limit, unsigned drop)
 {
   __shared__ uint32_t s_ok;
   __syncthreads();
   ++epoch;
   if (threadIdx.x == 0) {
-    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(&b->root), "l"(1ull) : "memory");
-    unsigned long long const target = epoch * gridDim.x;
-    uint32_t                 ok     = 1;
-    for (unsigned spins = 0; ld_acquire64(&b->root) < target; ++spins) {
-      if (spins > GRID_SYNC_SPINS || ((spins & 63u) == 63u && ld_acquire(&b->err))) {
-        atomicExch(&b->err, 1u);
-        ok = 0;
-        break;
+    uint32_t ok = 1;
+    if (drop && blockIdx.x == gridDim.x - 1 && epoch - s_epoch0 == drop) ok = 0;
+    else {
+      asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(&b->root), "l"(1ull) : "memory");
+      unsigned long long const target = epoch * gridDim.x;
+      for (unsigned spins = 0; ld_acquire64(&b->root) < target; ++spins) {
+        if (spins > limit || ((spins & 63u) == 63u && ld_acquire(&b->err))) {
+          atomicExch(&b->err, 1u);
+          ok = 0;
+          break;
+        }
+        __nanosleep(32);
       }
-      __nanosleep(32);
+      asm volatile("fence.acq_rel.gpu;" ::: "memory");
     }
-    asm volatile("fence.acq_rel.gpu;" ::: "memory");
     s_ok = ok;
   }
   __syncthreads();
@@ -662,7 +672,16 @@ struct fwbw_args
   reach_state*       st;
   uint32_t*          stamp_phase;
   uint64_t*          stamp_ns;
+  uint32_t           wait_limit;   // polls before a wait gives up
+  uint32_t           drop_barrier; // test hook: the last block leaves this barrier of the launch (0 = off)
+  uint64_t           aw_exact;     // worklist items after which warps take their finds exactly
 };
+
+__device__ __forceinline__ bool
+gsync(fwbw_args const& a, unsigned long long& epoch)
+{
+  return grid_sync(a.bar, epoch, a.wait_limit, a.drop_barrier);
+}
 
 // Block-shared scratch of the persistent kernel.
 struct fwbw_smem
@@ -946,7 +965,7 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, 
     if (joint) __stcg(aw + qn, AW_TAG | AW_TAKEN | AW_BW | seed1);
     *head = 0, *tail = qn + (joint ? 1u : 0u), *done = 0;
   }
-  if (!grid_sync(a.bar, epoch)) return SEARCH_FAILED;
+  if (!gsync(a, epoch)) return SEARCH_FAILED;
   aw_sink const sink{ reinterpret_cast<unsigned long long*>(&sm.warp[threadIdx.x >> 5]), aw, tail, cap };
   bool          failed      = false;
   uint32_t      unpublished = 0; // worklist items this warp finished, not yet added to done
@@ -1063,7 +1082,7 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, 
           unsigned long long gbase;
           uint32_t           nloc;
           uint32_t const     next = sink.reserve(ls_n, tot, gbase, nloc);
-          exact                   = exact || gbase > cap / 2;
+          exact                   = exact || gbase > a.aw_exact;
           uint32_t           q    = p - c;
 #pragma unroll
           for (int k = 0; k < AW_BATCH; ++k)
@@ -1095,7 +1114,7 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, 
             uint32_t           nloc;
             uint32_t const     next = sink.reserve(ls_n, __popc(fm), gbase, nloc);
             unsigned long long const tk = exact ? AW_TAKEN : 0ull; // before this chunk's switch
-            exact                       = exact || gbase > cap / 2;
+            exact                       = exact || gbase > a.aw_exact;
             if (f) sink.put(ls_n, nloc, gbase, __popc(fm & lt), AW_TAG | tk | dl | w);
             ls_n = next;
           }
@@ -1120,7 +1139,7 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, 
         unsigned long long const dn = ld_acquire64(done);
         unsigned long long const t  = ld_acquire64(tail);
         stop                        = dn == t ? 1u : 0u;
-        if (!stop && (spins > GRID_SYNC_SPINS || ((spins & 63u) == 63u && ld_acquire(&a.bar->err)))) {
+        if (!stop && (spins > a.wait_limit || ((spins & 63u) == 63u && ld_acquire(&a.bar->err)))) {
           atomicExch(&a.bar->err, 1u);
           stop = 2;
         }
@@ -1132,7 +1151,7 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, 
       } else __nanosleep(spins < 32 ? 64u : (spins < 256 ? 256u : 1024u)); // longer idle, longer sleep
     }
   }
-  if (!grid_sync(a.bar, epoch) || failed) return SEARCH_FAILED;
+  if (!gsync(a, epoch) || failed) return SEARCH_FAILED;
   // leave the worklist all zeros
   uint64_t t = __ldcg(tail);
   t          = t < cap ? t : cap;
@@ -1178,7 +1197,7 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
     if (lvl) c = __ldcg(&st->lq[s_in]);
     if (mat) {
       materialize_scanned(a.n, a.fresh, fin, &st->mat_q, a.qbits, td_head, a.m, sm);
-      if (!grid_sync(a.bar, epoch)) return SEARCH_FAILED;
+      if (!gsync(a, epoch)) return SEARCH_FAILED;
       stamp(a, 7);
       c = __ldcg(&st->mat_q);
       if (tally) st->mats += 1;
@@ -1222,7 +1241,7 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
         });
         flush_scanned(sm, fout, &st->lq[s_out], a.qbits, td_head, a.n, a.m);
       }
-      if (!grid_sync(a.bar, epoch)) return SEARCH_FAILED;
+      if (!gsync(a, epoch)) return SEARCH_FAILED;
       stamp(a, 14);
       mode = 0;
       mat  = false;
@@ -1301,7 +1320,7 @@ run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, ui
       __syncthreads();
       if (threadIdx.x == 0 && sm.cnt) atomicAdd(octr, static_cast<unsigned long long>(sm.cnt)); // vertices only
     }
-    if (!grid_sync(a.bar, epoch)) return SEARCH_FAILED;
+    if (!gsync(a, epoch)) return SEARCH_FAILED;
     stamp(a, mode ? 5u : 4u);
     m_u = m_u > mf ? m_u - mf : 0;
     bu += mode;
@@ -1590,7 +1609,7 @@ run_trim_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, unsigned lon
   unsigned const            lane = threadIdx.x & 31u;
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; i < qn; i += static_cast<uint64_t>(gridDim.x) * R_THREADS) __stcg(aw + i, AW_TAG | __ldcg(fq + i));
   if (blockIdx.x == 0 && threadIdx.x == 0) *head = 0, *tail = qn, *done = 0;
-  if (!grid_sync(a.bar, epoch)) return SEARCH_FAILED;
+  if (!gsync(a, epoch)) return SEARCH_FAILED;
   bool     failed      = false;
   uint32_t unpublished = 0;
   for (bool alive = true; alive;) {
@@ -1680,7 +1699,7 @@ run_trim_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, unsigned lon
           unsigned long long const dn = ld_acquire64(done);
           unsigned long long const t  = ld_acquire64(tail);
           stop                        = dn == t ? 1u : 0u;
-          if (!stop && (++spins > GRID_SYNC_SPINS || ((spins & 63u) == 63u && ld_acquire(&a.bar->err)))) {
+          if (!stop && (++spins > a.wait_limit || ((spins & 63u) == 63u && ld_acquire(&a.bar->err)))) {
             atomicExch(&a.bar->err, 1u);
             stop = 2;
           }
@@ -1694,7 +1713,7 @@ run_trim_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, unsigned lon
       }
     }
   }
-  if (!grid_sync(a.bar, epoch) || failed) return SEARCH_FAILED;
+  if (!gsync(a, epoch) || failed) return SEARCH_FAILED;
   uint64_t t = __ldcg(tail);
   t          = t < cap ? t : cap;
   for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; i < t; i += static_cast<uint64_t>(gridDim.x) * R_THREADS) __stcg(aw + i, 0ull);
@@ -1714,14 +1733,14 @@ run_trim(fwbw_args const& a, uint32_t& glvl, unsigned long long& epoch)
   if (blockIdx.x == 0 && threadIdx.x == 0) st->lq[(glvl + 2) % 3] = 0;
   // the finalize pass listed the undecided vertices in fb[glvl & 1].q
   trim_seed(a, a.fb[glvl & 1].q, __ldcg(&st->list_n), a.fb[(glvl + 1) & 1].q, &st->lq[(glvl + 1) % 3], dec, edges);
-  if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
+  if (!gsync(a, epoch)) rc = SEARCH_FAILED;
   stamp(a, 11);
   ++glvl;
   uint32_t const hs = rc == SEARCH_DONE ? __ldcg(&st->hseed_n) : 0u;
   if (hs) {
     // the listed heavy vertices' live degrees, counted in slices
     trim_count_heavy(a, hs);
-    if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
+    if (!gsync(a, epoch)) rc = SEARCH_FAILED;
     stamp(a, 15);
   }
   while (rc == SEARCH_DONE) {
@@ -1744,7 +1763,7 @@ run_trim(fwbw_args const& a, uint32_t& glvl, unsigned long long& epoch)
     if (blockIdx.x == 0 && threadIdx.x == 0) st->lq[(glvl + 2) % 3] = 0, st->hq_n[2 * ((glvl + 2) % 3)] = st->hq_n[2 * ((glvl + 2) % 3) + 1] = 0;
     if (first) dec += trim_dead_heavy(a, hs, glvl);
     trim_push(a, a.fb[glvl & 1].q, static_cast<uint32_t>(qn), a.fb[(glvl + 1) & 1].q, &st->lq[(glvl + 1) % 3], dec, edges, glvl);
-    if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
+    if (!gsync(a, epoch)) rc = SEARCH_FAILED;
     stamp(a, 12);
     ++lvl;
     ++glvl;
@@ -1806,7 +1825,7 @@ k_fwbw(fwbw_args a)
     p                   = prod == 0 || id >= a.n ? a.n : id;
   }
   bool const search = p < a.n; // block-uniform
-  if (threadIdx.x == 0) sm.buf_n = 0, sm.edges_bu = sm.cands_bu = 0;
+  if (threadIdx.x == 0) sm.buf_n = 0, sm.edges_bu = sm.cands_bu = 0, s_epoch0 = epoch;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->t_ns[0] = globaltimer();
     st->marks   = 0;
@@ -1846,7 +1865,7 @@ k_fwbw(fwbw_args a)
     uint64_t tot;
     block_exclusive_scan<uint64_t, R_THREADS>(c, &tot);
     if (threadIdx.x == 0) a.partial[blockIdx.x] = tot;
-    rc = grid_sync(a.bar, epoch) ? SEARCH_DONE : SEARCH_FAILED;
+    rc = gsync(a, epoch) ? SEARCH_DONE : SEARCH_FAILED;
     if (rc == SEARCH_DONE) {
       stamp(a, 8);
       uint64_t s = 0;
@@ -1861,7 +1880,7 @@ k_fwbw(fwbw_args a)
           // BW(p) over every undecided vertex is complete: the SCC is
           // FW(p) & BW(p)
           for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) a.vis_b[w] = __ldcg(a.vis_b + w) & __ldcg(a.vis_a + w);
-          if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
+          if (!gsync(a, epoch)) rc = SEARCH_FAILED;
           if (blockIdx.x == 0 && threadIdx.x == 0) st->joint = 1;
           break;
         }
@@ -1905,7 +1924,7 @@ k_fwbw(fwbw_args a)
         }
         best = __reduce_min_sync(0xFFFFFFFFu, best);
         if ((threadIdx.x & 31) == 0 && best != UNDECIDED && best < __ldcg(&st->id)) atomicMin(&st->id, best);
-        if (!grid_sync(a.bar, epoch)) rc = SEARCH_FAILED;
+        if (!gsync(a, epoch)) rc = SEARCH_FAILED;
         id = __ldcg(&st->id);
       }
     }
@@ -1958,7 +1977,7 @@ k_fwbw(fwbw_args a)
     if (blockIdx.x == 0 && threadIdx.x == 0) st->t_ns[1] = globaltimer();
     stamp(a, 10);
     if (rc == SEARCH_DONE && a.trim) {
-      rc = grid_sync(a.bar, epoch) ? SEARCH_DONE : SEARCH_FAILED; // snap and und complete
+      rc = gsync(a, epoch) ? SEARCH_DONE : SEARCH_FAILED; // snap and und complete
       if (rc == SEARCH_DONE) rc = run_trim(a, glvl, epoch);
     }
   }
@@ -2204,6 +2223,10 @@ launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* s
   a.st          = rs;
   a.stamp_phase = reinterpret_cast<uint32_t*>(static_cast<char*>(ws.rstate) + 2048);
   a.stamp_ns    = reinterpret_cast<uint64_t*>(static_cast<char*>(ws.rstate) + 2048 + 4 * MARKS);
+  a.wait_limit   = opt.wait_limit ? opt.wait_limit : GRID_SYNC_SPINS;
+  a.drop_barrier = opt.drop_barrier;
+  // an earlier switch only cuts duplicates; a later one could overrun the worklist's bound
+  a.aw_exact     = opt.aw_exact_after && opt.aw_exact_after < ws.aw_entries / 2 ? opt.aw_exact_after : ws.aw_entries / 2;
   void* args[]  = { &a };
   KSPN_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(&k_fwbw), dim3(fwbw_grid(ctx)), dim3(R_THREADS), args, 0, ctx->stream));
   ctx->launches += 1;

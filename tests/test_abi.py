@@ -69,3 +69,32 @@ def test_null_context_is_rejected():
     assert L.kspn_scc_device(None, 1, 0, None, None, None, None, None, None, None) == 1
     assert L.kspn_normalise(None, 1, None) == 1
     assert L.kspn_options_default(None) == 1
+
+
+STANDIN_VIEW = r"""
+#include <kaspan_b200/scc.hpp>
+#include <cstdint>
+// the members of the reference's bidi_graph_part_view<single_part_view>
+// (kaspan/graph/bidi_graph_part.hpp:12-28) with index_t = INDEX
+struct part_t { std::uint32_t n_; std::uint32_t n() const { return n_; } int world_size() const { return 1; } };
+struct view { part_t part; INDEX local_fw_m, local_bw_m; struct { INDEX* head; std::uint32_t* csr; } fw, bw; };
+void call(view v, std::uint32_t* ids) { kaspan_b200::scc(v, ids); }
+"""
+
+
+@pytest.mark.parametrize("index", ["std::uint64_t", "std::uint32_t"])
+def test_cpp_dropin_header_compiles(tmp_path, index):
+    """The C++ drop-in instantiates for 64- and 32-bit offsets (the 32-bit
+    path widens them on the host) against a stand-in with the reference
+    view's members; the GPU test runs it on the reference's own type."""
+    import shutil
+    import subprocess
+
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no g++")
+    src = tmp_path / "standin.cpp"
+    src.write_text(STANDIN_VIEW)
+    inc = os.path.join(os.path.dirname(HEADER))
+    r = subprocess.run([gxx, "-std=c++20", "-fsyntax-only", f"-DINDEX={index}", "-I", inc, str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr

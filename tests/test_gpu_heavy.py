@@ -197,3 +197,27 @@ def test_bottom_up_then_worklist(ctx):
         dct = st.as_dict()
         assert dct["levels_bottom_up"] > 0, "the search should run bottom-up levels in the core"
         assert dct["fwbw_joint"] == 1, "and finish on the worklist after them"
+
+
+# The worklist tail leaves a find's take to its consumer until a warp's
+# reservation passes half the worklist (4 M items and more), which no small
+# graph reaches; kspn_options.aw_exact_after moves that switch so the exact
+# branch (finds taken by the warp that found them) and the switch itself run
+# here.  1: exact after the first reservation; 2000: mid-phase.
+@pytest.mark.parametrize("after", [1, 2000])
+@pytest.mark.parametrize("shape", ["joint", "joint_heavy", "bottom_up_then_worklist", "chain", "heavy"])
+def test_worklist_exact_takes(ctx, shape, after):
+    import torch
+
+    n, s, d = {"joint": lambda: _long_cycle_graph(), "joint_heavy": lambda: _long_cycle_graph(heavy=True),
+               "bottom_up_then_worklist": _path_core_chain_graph, "chain": _chain_graph, "heavy": _heavy_graph}[shape]()
+    G = KG.from_edges(ctx, n, torch.from_numpy(s.view(np.int32)).cuda(), torch.from_numpy(d.view(np.int32)).cuda())
+    fwh, fwc, bwh, bwc = G.to_host()
+    want = O.tarjan(O.Graph(n, fwh, fwc, bwh, bwc))
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    for _ in range(2):  # the worklist must be left all zeros for the next call
+        st = K.Stats()
+        ctx.scc_device(n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, K.default_options(validate=0, aw_exact_after=after), st)
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), want)
+    if shape.startswith("joint"):
+        assert st.as_dict()["fwbw_joint"] == 1

@@ -112,6 +112,30 @@ def test_iteration_cap_reports_timeout(ctx):
     assert np.array_equal(ctx.scc(G.n, G.fwh, G.fwc, G.bwh, G.bwc), O.tarjan(G))
 
 
+@pytest.mark.parametrize("graph,drop", [("rmat", 1), ("rmat", 2), ("rmat", 4), ("cycle", 18), ("cycle", 19)])
+def test_barrier_wait_limit_reports_timeout(ctx, graph, drop):
+    """The resident launch's grid barrier gives up after its wait limit: the
+    grid's last block leaves barrier `drop` without arriving (the test hook
+    kspn_options.drop_barrier, a block that never arrives), the other blocks'
+    bounded waits run out, the launch ends through the barrier's error word,
+    and the call reports KSPN_ERR_TIMEOUT.  The next call on the same context
+    is exact.  On the long cycle the dropped barriers lie where the search
+    moves to its worklist tail (after 16 levels)."""
+    if graph == "rmat":
+        G = O.rmat(14, 8, 3)
+    else:
+        n = 60000
+        c = np.arange(n, dtype=np.uint32)
+        G = O.from_edges(n, c, (c + 1) % n)
+    want = O.tarjan(G)
+    for limit in (1 << 10, 1 << 14):
+        with pytest.raises(K.KspnError) as e:
+            ctx.scc(G.n, G.fwh, G.fwc, G.bwh, G.bwc, options=K.default_options(drop_barrier=drop, wait_limit=limit))
+        assert e.value.status == 4
+        assert "barrier" in str(e.value)
+        assert np.array_equal(ctx.scc(G.n, G.fwh, G.fwc, G.bwh, G.bwc), want)
+
+
 @pytest.mark.parametrize("variant", sorted(K.PIPELINES))
 def test_variant_matches_reference(ctx, variant):
     """Each reference entry point (kaspan::scc and variant/*.hpp, compiled

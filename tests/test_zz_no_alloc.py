@@ -50,3 +50,30 @@ def test_noalloc_relabel_rejects_too_many_vertices():
     buf = torch.zeros(8, dtype=torch.int32, device="cuda")
     assert L.kspn_normalise_noalloc(K.NOALLOC_MAX_N + 1, C.c_void_p(buf.data_ptr()), None) == 1
     assert L.kspn_normalise_noalloc(0, None, None) == 0
+
+
+def test_noalloc_relabel_reports_out_of_range_id():
+    """An id >= n is KSPN_ERR_INVALID_ARGUMENT; the array is then partly
+    relabelled: that id is unchanged and every id < n is already replaced
+    by the smallest vertex carrying it.  The next call is unaffected."""
+    import torch
+
+    L = K.lib()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    n = 5000
+    ids = np.random.default_rng(3).integers(0, n, n).astype(np.uint32)
+    ids[123] = n + 7
+    got = u32_to_dev(ids)
+    torch.cuda.synchronize()
+    assert L.kspn_normalise_noalloc(n, C.c_void_p(got.data_ptr()), stream) == 1
+    valid = ids < n
+    first = np.full(n, 0xFFFFFFFF, np.uint32)
+    np.minimum.at(first, ids[valid], np.nonzero(valid)[0].astype(np.uint32))
+    want = ids.copy()
+    want[valid] = first[ids[valid]]
+    assert np.array_equal(dev_to_u32(got)[:n], want)
+    ok = np.random.default_rng(4).integers(0, n, n).astype(np.uint32)
+    got = u32_to_dev(ok)
+    torch.cuda.synchronize()
+    assert L.kspn_normalise_noalloc(n, C.c_void_p(got.data_ptr()), stream) == 0
+    assert np.array_equal(dev_to_u32(got)[:n], O.normalise(ok))
