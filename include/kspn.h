@@ -169,8 +169,8 @@ typedef struct kspn_stats
   uint32_t heavy_fixups;
   uint32_t heavy_trim_seeds;
   uint32_t trim_worklist;   /* 1: the resident trim tail finished on the worklist (long, thin peeling) */
-  uint32_t fwbw_joint;      /* 1: the BW search ran inside the FW search's worklist phase (high diameter) */
-  uint32_t stats_pad;
+  uint32_t fwbw_joint;      /* 1: the FW and BW searches of the resident launch ran side by side */
+  uint32_t search_worklist; /* 1: the resident launch's searches finished on the worklist (high diameter) */
 } kspn_stats;
 
 typedef struct kspn_context kspn_context;
@@ -466,6 +466,65 @@ int  kspn_gen_batch(kspn_context* ctx, uint32_t count, uint64_t seed,
 /* Global ids -> local ids in every row of a concatenated CSR or CSC. */
 int  kspn_batch_localize(kspn_context* ctx, uint32_t count, uint64_t n_total,
                          const uint64_t* d_vtx_off, const uint64_t* d_head, uint32_t* d_csr);
+
+/* ---------------------------------------------------------------- one graph over several GPUs
+ * One rank's device steps of the sharded decomposition (kaspan_b200/shard.py
+ * drives them, one process per GPU, and runs the exchanges between ranks).
+ * They replace the rank-local work of the reference's distributed
+ * kaspan::scc (kaspan/scc/scc.hpp:21-87) on its 1D vertex partition: rank r
+ * owns vertices [lo, lo + n_loc) of an n-vertex graph and their rows of the
+ * CSR and the transpose with GLOBAL neighbour ids (the reference's
+ * bidi_graph_part_view of one rank, kaspan/graph/bidi_graph_part.hpp:12-28);
+ * heads hold local offsets (n_loc + 1 entries).  Local vertex state is a
+ * bitmap over the local range (u32 words, bit v = global vertex lo + v);
+ * scc_id holds global ids.  Device pointers; ctx's stream; each call returns
+ * after its stream work has finished.
+ */
+/* trim_1_first on the local rows (kaspan/scc/trim_1_local.hpp:12-46):
+ * d_und written in full, decided vertices get their own global id, the
+ * others UNDECIDED; *best_prod / *best_id = the largest in * out among the
+ * local survivors and its smallest global id (UNDECIDED when none). */
+int kspn_shard_trim_first(kspn_context* ctx, uint32_t n_loc, uint32_t lo, const uint64_t* d_fw_head, const uint64_t* d_bw_head,
+                          uint32_t* d_und, uint32_t* d_scc_id, uint64_t* best_prod, uint32_t* best_id, uint32_t* decided);
+/* The pivot rule on the remaining graph (kaspan/scc/pivot.hpp:53-74, raw
+ * degrees): largest in * out among the undecided local vertices. */
+int kspn_shard_pivot(kspn_context* ctx, uint32_t n_loc, uint32_t lo, const uint64_t* d_fw_head, const uint64_t* d_bw_head,
+                     const uint32_t* d_und, uint64_t* best_prod, uint32_t* best_id);
+/* Start of an FW-BW search: candidates of both searches = und, reached = {},
+ * the bitmaps of ids sent to other shards (n bits each) cleared. */
+int kspn_shard_search_begin(kspn_context* ctx, uint32_t n_loc, uint32_t n, const uint32_t* d_und, uint32_t* d_cand_fw, uint32_t* d_cand_bw,
+                            uint32_t* d_vis_fw, uint32_t* d_vis_bw, uint32_t* d_sent_fw, uint32_t* d_sent_bw);
+/* One top-down level of one search over the local rows (the forward rows for
+ * FW, the transposed ones for BW; cache_forward_backward_search,
+ * kaspan/scc/cache_pivot_search.hpp:16-104): a local neighbour still in
+ * d_cand is taken (set in d_vis, appended to d_next after the *next_n
+ * entries already there; *next_n updated); a remote one is claimed once per
+ * search in d_sent and sent to its owner: d_send receives the remote ids
+ * grouped by owning shard (shard r owns [d_bounds[r], d_bounds[r + 1])),
+ * counts[parts] (host) their number per shard -- the payload and counts of
+ * the reference's frontier exchange (kaspan/scc/frontier.hpp:237-282).
+ * d_remote (remote_cap entries) and d_counts (2 * parts) are scratch. */
+int kspn_shard_expand(kspn_context* ctx, uint32_t n_loc, uint32_t lo, const uint64_t* d_head, const uint32_t* d_adj,
+                      const uint32_t* d_frontier, uint32_t frontier_n, uint32_t* d_cand, uint32_t* d_vis, uint32_t* d_sent,
+                      uint32_t* d_next, uint32_t next_cap, uint32_t* next_n, uint32_t* d_remote, uint32_t remote_cap,
+                      uint32_t parts, const uint32_t* d_bounds, uint32_t* d_send, uint32_t* d_counts, uint32_t* counts);
+/* Ids other shards sent this one (global ids in its range): taken as local
+ * finds (appended to d_next after *next_n entries). */
+int kspn_shard_receive(kspn_context* ctx, uint32_t n_loc, uint32_t lo, const uint32_t* d_recv, uint32_t recv_n, uint32_t* d_cand,
+                       uint32_t* d_vis, uint32_t* d_next, uint32_t next_cap, uint32_t* next_n);
+/* Smallest global id in FW & BW on this shard (UNDECIDED if none). */
+int kspn_shard_scc_min(kspn_context* ctx, uint32_t n_loc, uint32_t lo, const uint32_t* d_vis_fw, const uint32_t* d_vis_bw, uint32_t* min_id);
+/* The SCC FW & BW leaves d_und; its local members get id `id`. */
+int kspn_shard_finalize(kspn_context* ctx, uint32_t n_loc, const uint32_t* d_vis_fw, const uint32_t* d_vis_bw, uint32_t* d_und,
+                        uint32_t* d_scc_id, uint32_t id, uint32_t* decided);
+/* The residual sub-graph's edges leaving this shard (the local part of
+ * allgather_fw_sub_graph, kaspan/scc/allgather_sub_graph.hpp:253-301):
+ * (lo + v, u) for every undecided local v and out-neighbour u undecided in
+ * d_global_und (ceil(n / 32) words of the whole graph); *count = their
+ * number, written while it stays below cap. */
+int kspn_shard_residual(kspn_context* ctx, uint32_t n_loc, uint32_t lo, const uint64_t* d_fw_head, const uint32_t* d_fw_csr,
+                        const uint32_t* d_und, const uint32_t* d_global_und, uint32_t* d_src, uint32_t* d_dst, uint64_t cap,
+                        uint64_t* count);
 
 /* ---------------------------------------------------------------- manifest graph files */
 /*

@@ -124,7 +124,7 @@ class Stats(C.Structure):
         ("heavy_trim_seeds", C.c_uint32),
         ("trim_worklist", C.c_uint32),
         ("fwbw_joint", C.c_uint32),
-        ("stats_pad", C.c_uint32),
+        ("search_worklist", C.c_uint32),
     ]
 
     def as_dict(self) -> dict:
@@ -145,6 +145,7 @@ class Stats(C.Structure):
             "heavy": {"cut_rows": self.heavy_cut_rows, "fixups": self.heavy_fixups, "trim_seeds": self.heavy_trim_seeds},
             "trim_worklist": self.trim_worklist,
             "fwbw_joint": self.fwbw_joint,
+            "search_worklist": self.search_worklist,
             "kernels": {k: {"ms": float(self.kernel_ms[i]), "bytes": int(self.kernel_bytes[i]), "calls": int(self.kernel_calls[i])}
                         for i, k in enumerate(KERNEL_CLASSES)},
             "trace": [{"dir": "bw" if t.backward else "fw", "mode": "bu" if t.bottom_up else "td", "frontier": t.frontier,
@@ -195,6 +196,14 @@ SIGNATURES = {
     "kspn_normalise": (_i32, [_P, _u32, _P]),
     "kspn_normalise_noalloc": (_i32, [_u32, _P, _P]),
     "kspn_transpose": (_i32, [_P, _u32, _u64, _P, _P, _P, _P]),
+    "kspn_shard_trim_first": (_i32, [_P, _u32, _u32, _P, _P, _P, _P, _P, _P, _P]),
+    "kspn_shard_pivot": (_i32, [_P, _u32, _u32, _P, _P, _P, _P, _P]),
+    "kspn_shard_search_begin": (_i32, [_P, _u32, _u32, _P, _P, _P, _P, _P, _P, _P]),
+    "kspn_shard_expand": (_i32, [_P, _u32, _u32, _P, _P, _P, _u32, _P, _P, _P, _P, _u32, _P, _P, _u32, _u32, _P, _P, _P, _P]),
+    "kspn_shard_receive": (_i32, [_P, _u32, _u32, _P, _u32, _P, _P, _P, _u32, _P]),
+    "kspn_shard_scc_min": (_i32, [_P, _u32, _u32, _P, _P, _P]),
+    "kspn_shard_finalize": (_i32, [_P, _u32, _P, _P, _P, _P, _u32, _P]),
+    "kspn_shard_residual": (_i32, [_P, _u32, _u32, _P, _P, _P, _P, _P, _P, _u64, _P]),
     "kspn_upload_transpose": (_i32, [_P, _u32, _u64, _P, _P, _P, _P, _P, _P, _u64]),
     "kspn_gen_gnm": (_i32, [_P, _u32, _u64, _u64, _P, _P]),
     "kspn_gen_rmat": (_i32, [_P, _i32, _u64, _u64, _u64, _u64, _u64, _i32, _P, _P]),

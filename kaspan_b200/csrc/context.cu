@@ -63,6 +63,7 @@ layout(workspace& ws, char* base, uint32_t n, uint64_t m)
   ws.vis_b             = c.take<uint32_t>(words);
   ws.mark              = c.take<uint32_t>(words);
   ws.fresh             = c.take<uint32_t>(words);
+  ws.fresh_bw          = c.take<uint32_t>(words);
   ws.cand_bw           = c.take<uint32_t>(words);
   ws.und               = c.take<uint32_t>(words);
   ws.label             = c.take<uint32_t>(nn);
@@ -74,6 +75,12 @@ layout(workspace& ws, char* base, uint32_t n, uint64_t m)
   ws.pivot             = c.take<uint64_t>(8192);
   ws.tile_start        = c.take<uint32_t>(m / 2048 + 4);
   ws.tile_start2       = c.take<uint32_t>(m / 2048 + 4);
+  ws.q2                = c.take<uint32_t>(nn);
+  ws.q3                = c.take<uint32_t>(nn);
+  ws.prefix3           = c.take<uint64_t>(nn);
+  ws.prefix4           = c.take<uint64_t>(nn);
+  ws.tile_start3       = c.take<uint32_t>(m / 2048 + 4);
+  ws.tile_start4       = c.take<uint32_t>(m / 2048 + 4);
   ws.tile_zero         = c.take<uint32_t>(m / 2048 + 4);
   ws.seed_q            = c.take<uint32_t>(4);
   ws.seed_prefix       = c.take<uint64_t>(4);
@@ -83,7 +90,7 @@ layout(workspace& ws, char* base, uint32_t n, uint64_t m)
   ws.aw                = c.take<unsigned long long>(ws.aw_entries);
   ws.rstate            = c.take<char>(4096);
   ws.heavy             = c.take<uint32_t>(4 * ws.heavy_cap);
-  ws.cutmap            = c.take<uint32_t>(words);
+  ws.cutmap            = c.take<uint32_t>(2 * words);
   return align_up(c.off);
 }
 
@@ -118,7 +125,7 @@ ensure_workspace(kspn_context* ctx, uint32_t n, uint64_t m)
   KSPN_CUDA(cudaMemsetAsync(ws.tile_zero, 0, (mcap / 2048 + 4) * sizeof(uint32_t), ctx->stream));
   KSPN_CUDA(cudaMemsetAsync(ws.gbar, 0, 4096, ctx->stream));
   KSPN_CUDA(cudaMemsetAsync(ws.aw, 0, ws.aw_entries * sizeof(unsigned long long), ctx->stream));
-  KSPN_CUDA(cudaMemsetAsync(ws.cutmap, 0, ((static_cast<size_t>(ncap) + 63) / 64 * 2 + 2) * sizeof(uint32_t), ctx->stream));
+  KSPN_CUDA(cudaMemsetAsync(ws.cutmap, 0, 2 * ((static_cast<size_t>(ncap) + 63) / 64 * 2 + 2) * sizeof(uint32_t), ctx->stream));
 }
 
 void*

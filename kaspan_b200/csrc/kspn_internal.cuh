@@ -296,7 +296,8 @@ struct workspace
   uint32_t* vis_a    = nullptr; // bitmap
   uint32_t* vis_b    = nullptr; // bitmap
   uint32_t* mark     = nullptr; // bitmap
-  uint32_t* fresh    = nullptr; // bitmap: vertices found by the last bottom-up sweep
+  uint32_t* fresh    = nullptr; // bitmap: vertices found by the last bottom-up sweep (FW search)
+  uint32_t* fresh_bw = nullptr; // the same for the BW search of the persistent FW-BW
   uint32_t* cand_bw  = nullptr; // bitmap: BW candidates of a joint worklist search (FW and BW at once)
   uint32_t* label    = nullptr; // n
   uint32_t* indeg    = nullptr; // n
@@ -309,6 +310,13 @@ struct workspace
   uint64_t* pivot    = nullptr; // per-block pivot keys (4096 u64 products + 4096 u32 ids)
   uint32_t* tile_start  = nullptr; // m / 2048 + 4 (frontier expansion)
   uint32_t* tile_start2 = nullptr; // m / 2048 + 4 (second frontier of the persistent FW-BW)
+  // the BW search's frontier pair in the persistent FW-BW (FW and BW run side by side)
+  uint32_t* q2          = nullptr; // n
+  uint32_t* q3          = nullptr; // n
+  uint64_t* prefix3     = nullptr; // n+1
+  uint64_t* prefix4     = nullptr; // n+1
+  uint32_t* tile_start3 = nullptr; // m / 2048 + 4
+  uint32_t* tile_start4 = nullptr; // m / 2048 + 4
   uint32_t* tile_zero   = nullptr; // m / 2048 + 4 zeros: tile starts of a one-vertex frontier
   uint32_t* seed_q      = nullptr; // 4: the pivot as a one-vertex frontier
   uint64_t* seed_prefix = nullptr; // 4
@@ -318,7 +326,7 @@ struct workspace
   void*     rstate      = nullptr; // 4 KiB device control blocks (FW-BW at 0, trim at 512, search stamps at 2048)
   uint32_t* heavy       = nullptr; // 4 heavy lists of heavy_cap entries (persistent FW-BW: trim seed, two trim push levels, cut bottom-up rows)
   uint64_t  heavy_cap   = 0;
-  uint32_t* cutmap      = nullptr; // bitmap: vertices on a cut list (zero outside a search)
+  uint32_t* cutmap      = nullptr; // bitmaps: vertices on a cut list, FW search then BW search (2 x words; zero outside a search)
   // owned graph storage (host inputs, or a CSC built on device)
   uint64_t* g_fh = nullptr;
   uint32_t* g_fc = nullptr;
@@ -366,7 +374,8 @@ enum buffer_slot : int
   BUF_BUILD      = 1, // radix-sort scratch (transpose, build_csr)
   BUF_TRANSPOSE  = 2, // transpose built for kspn_scc_device without bw
   BUF_GEN        = 3, // generator scratch (RGG points and cells)
-  BUF_COUNT      = 4
+  BUF_SHARD      = 4, // counters of the sharded steps (shard.cu)
+  BUF_COUNT      = 5
 };
 
 struct cached_graph
@@ -443,6 +452,22 @@ void* context_buffer(kspn_context* ctx, int slot, size_t bytes); // grown on dem
 void read_counters(kspn_context* ctx); // D2H of ws.ctr / ws.ctr64 + stream sync
 void zero_counters(kspn_context* ctx);
 int  fail(kspn_context* ctx, error const& e);
+
+// Runs an entry point's body: KSPN_OK, or the status of the error it threw
+// (detail kept for kspn_last_error).  No exception crosses the C ABI.
+template<class F>
+int
+run_guarded(kspn_context* ctx, F&& body)
+{
+  try {
+    body();
+    return KSPN_OK;
+  } catch (error const& e) {
+    return fail(ctx, e);
+  } catch (...) {
+    return fail(ctx, error{ KSPN_ERR_INTERNAL, "unexpected exception" });
+  }
+}
 
 // trim.cu
 // reach.cu: the resident start of the FAST pipeline -- FW-BW from

@@ -84,8 +84,10 @@ struct reach_state
   unsigned long long edges_td, edges_bu, cands_bu;
   uint32_t           bar_err; // 1: the persistent launch's grid barrier gave up
   uint32_t           marks;   // phase stamps taken (kspn_options.trace)
-  unsigned long long lq[3];   // persistent launch: packed level counters (edges << qbits | vertices)
-  unsigned long long mat_q;   // persistent launch: counter of a frontier built from `fresh`
+  unsigned long long lq[3];   // persistent launch: packed level counters (edges << qbits | vertices), FW search
+  unsigned long long mat_q;   // persistent launch: counter of a frontier built from `fresh`, FW search
+  unsigned long long lq_bw[3]; // the same for the BW search (FW and BW run side by side)
+  unsigned long long mat_q_bw;
   // resident pipeline (FW-BW launch with the trim fixpoint as its tail)
   uint32_t           pivot_used;   // pivot the launch searched from (n: none)
   uint32_t           trim_decided; // vertices the trim tail decided
@@ -106,6 +108,7 @@ struct reach_state
   uint32_t           hq_n[6];      // trim tail: heavy out-/in-rows listed per push level (pairs rotating like lq)
   uint32_t           heavy_err;    // a heavy or cut list would have overflowed
   uint32_t           trim_async;   // the trim tail finished on the worklist
+  uint32_t           restricts;    // passes that cut one search's candidates down to the other's set
 };
 
 // phase stamps live after the state: uint32 phase[128], uint64 ns[128]
@@ -241,7 +244,6 @@ struct take_op
 // avail, set in mark -- when a neighbour in its opposite-direction row is
 // already in mark.
 constexpr int BU_WARPS = R_THREADS / 32;
-constexpr int BU_STEPS = 32; // neighbours a candidate checks itself before its warp helps
 
 // Per-warp shared memory of the sweep.
 struct bu_warp_smem
@@ -253,8 +255,7 @@ struct bu_warp_smem
 // Rows cut short in bottom-up sweeps: a row the warp has walked HEAVY_ROW
 // entries of without a hit is left open (the vertex stays a candidate) and
 // its vertex listed once (map) for a fix-up step that walks the listed
-// rows in slices over the whole grid.  CUT = false: rows are walked to the
-// end.
+// rows in slices over the whole grid.
 struct bu_cut
 {
   uint32_t* map;  // bitmap of listed vertices
@@ -264,19 +265,21 @@ struct bu_cut
   uint32_t* err;  // set if it were
 };
 
-// The running sweep's cut descriptor: block-shared, set by thread 0 before
-// the sweep (a barrier between) and read only on the rare path, so the
-// sweep's hot loop holds no register for it.
-__shared__ bu_cut s_bu_cut;
+// The sweeps' cut descriptors (FW search, BW search): block-shared, set by
+// thread 0 before the first sweep (a barrier between) and read only on the
+// rare path, so the sweep's hot loop holds no register for them.
+__shared__ bu_cut s_bu_cut[2];
 
 // Row walks of up to BU_ILP candidates per lane (v[k], live[k]): all
 // neighbour loads of a step, then all probes of `mark`; rows still open
-// after BU_STEPS neighbours are finished by the whole warp with early exit
-// (or cut, see bu_cut).  found[k]: a neighbour of v[k] is in mark.  All
-// lanes call it.
-template<bool CUT>
+// after BU_STEPS neighbours are finished by the whole warp with early exit,
+// a row longer than HEAVY_ROW cut short and listed (bu_cut).  found[k]: a
+// neighbour of v[k] is in mark.  All lanes call it.
+constexpr int BU_STEPS = 32; // neighbours a candidate checks itself before its warp helps
+
 __device__ __forceinline__ void
-bu_rows(uint32_t const (&v)[BU_ILP], bool (&live)[BU_ILP], bool (&found)[BU_ILP], uint64_t const* __restrict__ head, uint32_t const* __restrict__ adj, uint32_t const* mark, uint64_t& nedge)
+bu_rows(uint32_t const (&v)[BU_ILP], bool (&live)[BU_ILP], bool (&found)[BU_ILP], uint64_t const* __restrict__ head, uint32_t const* __restrict__ adj, uint32_t const* mark,
+        bu_cut const& cut, uint64_t& nedge)
 {
   unsigned const lane = threadIdx.x & 31u;
   uint64_t       b[BU_ILP], e[BU_ILP];
@@ -319,7 +322,7 @@ bu_rows(uint32_t const (&v)[BU_ILP], bool (&live)[BU_ILP], bool (&found)[BU_ILP]
       unsigned const l = __ffs(todo) - 1;
       todo &= todo - 1;
       uint64_t const b0 = __shfl_sync(0xFFFFFFFFu, b[k], l), e0 = __shfl_sync(0xFFFFFFFFu, e[k], l);
-      uint64_t const e1 = CUT && e0 - b0 > HEAVY_ROW ? b0 + HEAVY_ROW : e0;
+      uint64_t const e1 = e0 - b0 > HEAVY_ROW ? b0 + HEAVY_ROW : e0;
       bool           hit = false;
       for (uint64_t x = b0; x < e1; x += 32) {
         bool const     in = x + lane < e1;
@@ -333,91 +336,87 @@ bu_rows(uint32_t const (&v)[BU_ILP], bool (&live)[BU_ILP], bool (&found)[BU_ILP]
       }
       if (lane == l) {
         found[k] = hit;
-        if (CUT && !hit && e1 < e0 && bit_claim(s_bu_cut.map, v[k])) {
-          uint32_t const i = atomicAdd(s_bu_cut.n, 1u);
-          if (i < s_bu_cut.cap) s_bu_cut.list[i] = v[k];
-          else atomicExch(s_bu_cut.err, 1u);
+        if (!hit && e1 < e0 && bit_claim(cut.map, v[k])) {
+          uint32_t const i = atomicAdd(cut.n, 1u);
+          if (i < cut.cap) cut.list[i] = v[k];
+          else atomicExch(cut.err, 1u);
         }
       }
     }
   }
 }
 
-// Bottom-up sweep over the chunks of 32 bitmap words given to this warp
-// (chunk c = words [32c, 32c + 32), c = first, first + step, ...).
+// Bottom-up sweep of chunk c (bitmap words [32c, 32c + 32)) by one warp.
 // Candidates are the set bits of `avail`; one joins when a neighbour in its
 // head/adj row is in `mark`.  Warps work independently (no block barrier):
-// the warp packs its chunk's candidates (popcount scan over its 32 words),
-// each lane walks BU_ILP candidates interleaved (bu_rows).  Lane i then
-// owns word i of the chunk: it clears the found bits from avail, sets them
-// in mark and writes the word of `fresh` (the sweep's discoveries).  No
-// queue is written; the discovery count goes to nfound.  `avail` and `mark` are read through L2 (other
+// the warp packs its chunk's candidates (popcount scan over its 32 words)
+// as 16-bit offsets in shared memory, each lane walks BU_ILP candidates'
+// rows interleaved (bu_rows).  Lane i then owns word i of the chunk: it
+// clears the found bits from avail, sets them in mark and writes the word
+// of `fresh` (the sweep's discoveries).  No queue is written; the discovery
+// count goes to nfound.  `avail` and `mark` are read through L2 (other
 // blocks of a persistent launch change them).
-template<bool CUT>
 __device__ __forceinline__ void
-bu_sweep_warp(uint32_t first,
-              uint32_t step,
-              uint32_t n,
-              uint64_t const* __restrict__ head,
-              uint32_t const* __restrict__ adj,
-              uint32_t* avail,
-              uint32_t* mark,
-              uint32_t* fresh,
-              bu_warp_smem& sm,
-              uint32_t& nfound,
-              uint64_t& nedge,
-              uint64_t& ncand)
+bu_sweep_chunk(uint32_t c,
+               uint32_t n,
+               uint64_t const* __restrict__ head,
+               uint32_t const* __restrict__ adj,
+               uint32_t* avail,
+               uint32_t* mark,
+               uint32_t* fresh,
+               bu_cut const& cut,
+               bu_warp_smem& sm,
+               uint32_t& nfound,
+               uint64_t& nedge,
+               uint64_t& ncand)
 {
-  unsigned const lane   = threadIdx.x & 31u;
-  uint32_t const words  = (n + 31) / 32;
-  uint32_t const chunks = (words + 31) / 32;
-  for (uint32_t c = first; c < chunks; c += step) {
-    uint32_t const w    = c * 32 + lane;
-    uint32_t       word = w < words ? __ldcg(avail + w) : 0u;
-    if (w == words - 1 && (n & 31)) word &= (1u << (n & 31)) - 1u;
-    uint32_t const cnt = __popc(word);
-    uint32_t       pos = cnt;
+  unsigned const lane  = threadIdx.x & 31u;
+  uint32_t const words = (n + 31) / 32;
+  uint32_t const w     = c * 32 + lane;
+  uint32_t       word  = w < words ? __ldcg(avail + w) : 0u;
+  if (w == words - 1 && (n & 31)) word &= (1u << (n & 31)) - 1u;
+  uint32_t const cnt = __popc(word);
+  uint32_t       pos = cnt;
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, pos, d);
-      if (lane >= static_cast<unsigned>(d)) pos += y;
-    }
-    uint32_t const total = __shfl_sync(0xFFFFFFFFu, pos, 31);
-    pos -= cnt;
-    while (word) {
-      uint32_t const bb = __ffs(word) - 1;
-      word &= word - 1;
-      sm.cand[pos++] = static_cast<uint16_t>(lane * 32 + bb);
-    }
-    sm.found[lane] = 0;
-    __syncwarp();
-    ncand += lane == 0 ? total : 0;
-    for (uint32_t r = 0; r < total; r += 32 * BU_ILP) {
-      uint32_t v[BU_ILP];
-      bool     live[BU_ILP], found[BU_ILP];
-#pragma unroll
-      for (int k = 0; k < BU_ILP; ++k) {
-        uint32_t const i = r + k * 32 + lane;
-        live[k]          = i < total;
-        v[k]             = live[k] ? c * 1024 + sm.cand[i] : 0u;
-      }
-      bu_rows<CUT>(v, live, found, head, adj, mark, nedge);
-#pragma unroll
-      for (int k = 0; k < BU_ILP; ++k)
-        if (found[k]) atomicOr(&sm.found[(v[k] >> 5) - c * 32], 1u << (v[k] & 31));
-    }
-    __syncwarp();
-    uint32_t const fnd = sm.found[lane];
-    if (w < words) {
-      if (fnd) {
-        atomicAnd(avail + w, ~fnd);
-        atomicOr(mark + w, fnd);
-      }
-      fresh[w] = fnd;
-    }
-    nfound += __popc(fnd);
-    __syncwarp();
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, pos, d);
+    if (lane >= static_cast<unsigned>(d)) pos += y;
   }
+  uint32_t const total = __shfl_sync(0xFFFFFFFFu, pos, 31);
+  pos -= cnt;
+  while (word) {
+    uint32_t const bb = __ffs(word) - 1;
+    word &= word - 1;
+    sm.cand[pos++] = static_cast<uint16_t>(lane * 32 + bb);
+  }
+  sm.found[lane] = 0;
+  __syncwarp();
+  ncand += lane == 0 ? total : 0;
+  for (uint32_t r = 0; r < total; r += 32 * BU_ILP) {
+    uint32_t v[BU_ILP];
+    bool     live[BU_ILP], found[BU_ILP];
+#pragma unroll
+    for (int k = 0; k < BU_ILP; ++k) {
+      uint32_t const i = r + k * 32 + lane;
+      live[k]          = i < total;
+      v[k]             = live[k] ? c * 1024 + sm.cand[i] : 0u;
+    }
+    bu_rows(v, live, found, head, adj, mark, cut, nedge);
+#pragma unroll
+    for (int k = 0; k < BU_ILP; ++k)
+      if (found[k]) atomicOr(&sm.found[(v[k] >> 5) - c * 32], 1u << (v[k] & 31));
+  }
+  __syncwarp();
+  uint32_t const fnd = sm.found[lane];
+  if (w < words) {
+    if (fnd) {
+      atomicAnd(avail + w, ~fnd);
+      atomicOr(mark + w, fnd);
+    }
+    fresh[w] = fnd;
+  }
+  nfound += __popc(fnd);
+  __syncwarp();
 }
 
 // Frontier queue from `fresh` (when a search returns to top-down after
@@ -470,12 +469,14 @@ k_bottom_up(uint32_t n,
 {
   if (g.closed()) return;
   __shared__ bu_warp_smem sm[BU_WARPS];
-  if (threadIdx.x == 0) s_bu_cut = cut;
+  if (threadIdx.x == 0) s_bu_cut[0] = cut;
   __syncthreads();
-  uint32_t                nfound = 0;
-  uint64_t                nedge = 0, ncand = 0;
-  unsigned const          wid = threadIdx.x >> 5;
-  bu_sweep_warp<true>(blockIdx.x * BU_WARPS + wid, gridDim.x * BU_WARPS, n, head, adj, avail, mark, fresh, sm[wid], nfound, nedge, ncand);
+  uint32_t       nfound = 0;
+  uint64_t       nedge = 0, ncand = 0;
+  unsigned const wid    = threadIdx.x >> 5;
+  uint32_t const chunks = ((n + 31) / 32 + 31) / 32;
+  for (uint32_t c = blockIdx.x * BU_WARPS + wid; c < chunks; c += gridDim.x * BU_WARPS)
+    bu_sweep_chunk(c, n, head, adj, avail, mark, fresh, s_bu_cut[0], sm[wid], nfound, nedge, ncand);
 #pragma unroll
   for (int s = 16; s; s >>= 1) {
     nedge += __shfl_down_sync(0xFFFFFFFFu, nedge, s);
@@ -647,8 +648,10 @@ struct fwbw_args
   uint32_t*          vis_a;
   uint32_t*          vis_b;
   uint32_t*          fresh;
-  uint32_t*          cand_bw; // joint worklist search: BW candidates (und minus the pivot), or null
+  uint32_t*          fresh_bw; // the BW search's sweep discoveries
+  uint32_t*          cand_bw;  // BW candidates (und minus the pivot, then what BW has not reached)
   frontier_buf       fb[2];
+  frontier_buf       fb_bw[2]; // the BW search's frontier pair
   frontier_buf       seed;    // q[0] = pivot, prefix[0] = 0, tile starts all 0
   uint64_t*          partial; // one per block
   // resident pipeline: pivot == PIVOT_FROM_DEVICE takes trim_1_first's
@@ -667,7 +670,8 @@ struct fwbw_args
   // search's cut rows -- and the bitmap of cut rows (zero between searches)
   uint32_t*          heavy;
   uint32_t           heavy_cap;
-  uint32_t*          cutmap;
+  uint32_t*          cutmap;    // FW search's cut rows; the BW search's follow at cutmap + cut_words
+  uint32_t           cut_words;
   grid_barrier*      bar;
   reach_state*       st;
   uint32_t*          stamp_phase;
@@ -878,19 +882,6 @@ constexpr uint32_t           ASYNC_FRONTIER = 1u << 16;  // largest frontier tha
 constexpr unsigned long long AW_TAG         = 1ull << 32; // marks a written slot
 constexpr int                AW_BATCH       = 8;         // neighbours a lane loads at once
 
-// warp-aggregated append of the active lanes' v (slots past cap dropped)
-__device__ __forceinline__ void
-aw_push(uint32_t v, unsigned long long* aw, unsigned long long* tail, uint64_t cap)
-{
-  unsigned const     mask = __activemask();
-  unsigned const     lane = threadIdx.x & 31u, leader = __ffs(mask) - 1;
-  unsigned long long base = 0;
-  if (lane == leader) base = atomicAdd(tail, static_cast<unsigned long long>(__popc(mask)));
-  base                = __shfl_sync(mask, base, leader);
-  uint64_t const slot = base + __popc(mask & ((1u << lane) - 1u));
-  if (slot < cap) __stcg(aw + slot, AW_TAG | v);
-}
-
 // Finds a warp keeps on its own stack (in its shared buffer) and expands in
 // its next round instead of appending them: a hop then costs the chain of
 // loads of one expansion, not a trip through the worklist to whichever warp
@@ -938,9 +929,10 @@ struct aw_sink
   }
 };
 
-// Runs the rest of the search from frontier fq[0, qn) (direction d0).  With
-// d1 (a joint phase) the other search runs in the same phase from its first
-// vertex seed1: its items carry AW_BW.  All threads of every block call it.
+// Runs the rest of the search from frontier fq0[0, qn0) (direction d0).
+// With d1 (a joint phase) the other search runs in the same phase from its
+// frontier fq1[0, qn1): its items carry AW_BW.  All threads of every block
+// call it.
 // An item is AW_TAG | dir << 63 | slice << 33 | v: slice 0 of a row longer
 // than HEAVY_ROW appends the row's other HEAVY_SLICE-entry slices as items
 // of their own (so idle warps share the row) and walks the first; a vertex
@@ -949,7 +941,8 @@ struct aw_sink
 // grows while the stack is empty, so done == appended still means that
 // nothing is left anywhere.
 __device__ __forceinline__ int
-run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, aw_dir const* d1, uint32_t seed1, unsigned long long& epoch, uint64_t& edges, fwbw_smem& sm)
+run_async(fwbw_args const& a, uint32_t const* fq0, uint32_t qn0, aw_dir const d0, uint32_t const* fq1, uint32_t qn1, aw_dir const* d1, unsigned long long& epoch,
+          uint64_t& edges, fwbw_smem& sm)
 {
   unsigned long long* const aw   = a.aw;
   unsigned long long* const head = a.aq;
@@ -960,11 +953,10 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, 
   unsigned const            lt   = (1u << lane) - 1u;
   bool const                joint = d1 != nullptr;
   aw_dir const              e1    = joint ? *d1 : d0;
-  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; i < qn; i += static_cast<uint64_t>(gridDim.x) * R_THREADS) __stcg(aw + i, AW_TAG | AW_TAKEN | __ldcg(fq + i));
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    if (joint) __stcg(aw + qn, AW_TAG | AW_TAKEN | AW_BW | seed1);
-    *head = 0, *tail = qn + (joint ? 1u : 0u), *done = 0;
-  }
+  uint32_t const            qb    = joint ? qn1 : 0u;
+  for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * R_THREADS + threadIdx.x; i < qn0 + qb; i += static_cast<uint64_t>(gridDim.x) * R_THREADS)
+    __stcg(aw + i, i < qn0 ? AW_TAG | AW_TAKEN | __ldcg(fq0 + i) : AW_TAG | AW_TAKEN | AW_BW | __ldcg(fq1 + (i - qn0)));
+  if (blockIdx.x == 0 && threadIdx.x == 0) *head = 0, *tail = qn0 + qb, *done = 0;
   if (!gsync(a, epoch)) return SEARCH_FAILED;
   aw_sink const sink{ reinterpret_cast<unsigned long long*>(&sm.warp[threadIdx.x >> 5]), aw, tail, cap };
   bool          failed      = false;
@@ -1159,195 +1151,342 @@ run_async(fwbw_args const& a, uint32_t const* fq, uint32_t qn, aw_dir const d0, 
   return SEARCH_DONE;
 }
 
-// Every level of one reachability search (BW: over in-edges, candidates
-// vis_a, reached vis_b; FW: over out-edges, candidates cand, reached vis_a).
-// `glvl` numbers levels across both searches of the launch (it selects
-// counter slots and buffers); `pivot` is the launch's resolved pivot (never
-// the PIVOT_FROM_DEVICE marker).  Block 0 records the search's level counts.
+// ---------------------------------------------------------------- joint level loop
+// The FW and BW searches from the pivot run side by side, one grid barrier
+// per level for both: FW over out-edges (candidates cand, reached vis_a),
+// BW over in-edges (candidates cand_bw, reached vis_b), each from the pivot
+// over every undecided vertex, and the SCC is FW(p) & BW(p).  Each search
+// keeps its own direction (top-down or bottom-up, Beamer's rule), frontier
+// pair, level counters, sweep bitmap and cut list; a level runs both
+// searches' steps over the whole grid (top-down tiles of both in one unit
+// range, bottom-up chunks of both in one chunk range), so the latency-bound
+// thin levels of the two searches overlap instead of adding up.  When one
+// search ends, the other's candidates are cut down to the finished search's
+// set (an SCC member reaches or is reached by the pivot inside the SCC, so
+// nothing of the SCC is lost) -- after that it costs what the restricted
+// search of the reference would.  When every running search is top-down
+// and thin after ASYNC_AFTER levels, both finish on the worklist together.
 
-template<bool BW>
-__device__ __forceinline__ int
-run_search(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uint32_t& glvl, unsigned long long& epoch, bool& joint)
+// One search's arrays.
+struct jdir
 {
-  uint64_t const* const    td_head = BW ? a.bh : a.fh;
-  uint32_t const* const    td_adj  = BW ? a.bc : a.fc;
-  uint64_t const* const    bu_head = BW ? a.fh : a.bh;
-  uint32_t const* const    bu_adj  = BW ? a.fc : a.bc;
-  uint32_t* const          avail   = BW ? a.vis_a : a.cand;
-  uint32_t* const          mark    = BW ? a.vis_b : a.vis_a;
-  reach_state* const       st      = a.st;
-  unsigned long long const qmask   = (1ull << a.qbits) - 1;
-  uint64_t                 m_u     = a.m; // Beamer's unexplored-edge budget
-  uint32_t                 mode    = 0;   // 0 top-down, 1 bottom-up
-  bool                     mat     = false;
-  uint32_t                 bu = 0, capped = 0, lvl = 0;
-  uint64_t                 edges_td = 0;
+  uint64_t const*     td_head;
+  uint32_t const*     td_adj;
+  uint64_t const*     bu_head;
+  uint32_t const*     bu_adj;
+  uint32_t*           avail;
+  uint32_t*           mark;
+  uint32_t*           fresh;
+  frontier_buf        fb0, fb1; // the pair, by level parity
+  unsigned long long* lq;       // 3 rotating level counters
+  unsigned long long* mat_q;
+  uint32_t*           cut_list;
+  uint32_t*           cut_n;
+};
+
+__device__ __forceinline__ jdir
+joint_dir(fwbw_args const& a, int d)
+{
+  reach_state* const st = a.st;
+  if (d == 0) return jdir{ a.fh, a.fc, a.bh, a.bc, a.cand, a.vis_a, a.fresh, a.fb[0], a.fb[1], st->lq, &st->mat_q, a.heavy + 3u * a.heavy_cap, &st->cut_n[0] };
+  return jdir{ a.bh, a.bc, a.fh, a.fc, a.cand_bw, a.vis_b, a.fresh_bw, a.fb_bw[0], a.fb_bw[1], st->lq_bw, &st->mat_q_bw, a.heavy, &st->cut_n[1] };
+}
+
+__device__ __forceinline__ frontier_buf const&
+jbuf(jdir const& D, uint32_t parity)
+{
+  return parity & 1u ? D.fb1 : D.fb0;
+}
+
+// Block-shared control of the loop: thread 0 of every block computes it from
+// the same counters (so every block takes the same branches; nothing is
+// broadcast), the other threads read it after a block barrier.
+enum : uint32_t
+{
+  JK_NONE  = 0,
+  JK_TD    = 1, // top-down expansion
+  JK_BU    = 2, // bottom-up sweep
+  JK_FIXUP = 3  // cut rows walked in slices
+};
+struct jctl
+{
+  unsigned long long c[2];        // the level's frontier: edges << qbits | vertices
+  unsigned long long m_u[2];      // Beamer's unexplored-edge budget
+  unsigned long long edges_td[2]; // top-down edges expanded
+  uint32_t           lvl[2], bu[2], mode[2], mat[2], fixed[2], live[2], kind[2];
+  uint32_t           restrict_to[2]; // 1: cut this search's candidates down to the other's set first
+  uint32_t           capped, async, any_td, any_bu;
+  uint32_t           cnt[2];
+};
+__shared__ jctl s_j;
+
+__device__ __forceinline__ int
+run_joint(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uint32_t& glvl, unsigned long long& epoch)
+{
+  reach_state* const       st    = a.st;
+  unsigned long long const qmask = (1ull << a.qbits) - 1;
   bool const               tally = blockIdx.x == 0 && threadIdx.x == 0; // keeps the byte-model counts in st
-  bool                     fixed = false; // the last level was a fix-up step
-  // rows the sweeps cut short (s_bu_cut; every level ends in a grid
-  // barrier, so the block's sweeps see it): the FW search lists them in
-  // heavy list 3, the BW search in list 0
-  if (threadIdx.x == 0) s_bu_cut = bu_cut{ a.cutmap, a.heavy + (BW ? 0u : 3u) * a.heavy_cap, &st->cut_n[BW ? 1 : 0], a.heavy_cap, &st->heavy_err };
-  // the first frontier: the pivot alone
-  unsigned long long c = (static_cast<unsigned long long>(td_head[pivot + 1] - td_head[pivot]) << a.qbits) | 1u;
-  for (;; ++lvl, ++glvl) {
-    uint32_t const     s_in = glvl % 3, s_out = (glvl + 1) % 3, s_clr = (glvl + 2) % 3;
-    frontier_buf const fin  = lvl == 0 ? a.seed : a.fb[glvl & 1];
-    frontier_buf const fout = a.fb[(glvl + 1) & 1];
-    if (lvl) c = __ldcg(&st->lq[s_in]);
-    if (mat) {
-      materialize_scanned(a.n, a.fresh, fin, &st->mat_q, a.qbits, td_head, a.m, sm);
+  unsigned const           lane  = threadIdx.x & 31u;
+  unsigned const           wid   = threadIdx.x >> 5;
+  uint32_t const           words = (a.n + 31) / 32;
+  if (threadIdx.x == 0) {
+    s_bu_cut[0] = bu_cut{ a.cutmap, a.heavy + 3u * a.heavy_cap, &st->cut_n[0], a.heavy_cap, &st->heavy_err };
+    s_bu_cut[1] = bu_cut{ a.cutmap + a.cut_words, a.heavy, &st->cut_n[1], a.heavy_cap, &st->heavy_err };
+    for (int d = 0; d < 2; ++d) {
+      uint64_t const* h = d ? a.bh : a.fh;
+      s_j.c[d]          = (static_cast<unsigned long long>(h[pivot + 1] - h[pivot]) << a.qbits) | 1u; // the pivot alone
+      s_j.m_u[d]        = a.m;
+      s_j.edges_td[d]   = 0;
+      s_j.lvl[d] = s_j.bu[d] = s_j.mode[d] = s_j.mat[d] = s_j.fixed[d] = 0;
+      s_j.live[d]                                                      = 1;
+      s_j.restrict_to[d]                                               = 0;
+    }
+    s_j.capped = 0;
+  }
+  int rc = SEARCH_DONE;
+  for (;; ++glvl) {
+    __syncthreads();
+    uint32_t const s_out = (glvl + 1) % 3, s_clr = (glvl + 2) % 3;
+    // frontiers that return to top-down are built from the sweeps' finds first
+    if (s_j.mat[0] || s_j.mat[1]) {
+#pragma unroll 1
+      for (int d = 0; d < 2; ++d)
+        if (s_j.mat[d]) {
+          jdir const D = joint_dir(a, d);
+          materialize_scanned(a.n, D.fresh, jbuf(D, glvl), D.mat_q, a.qbits, D.td_head, a.m, sm);
+        }
       if (!gsync(a, epoch)) return SEARCH_FAILED;
       stamp(a, 7);
-      c = __ldcg(&st->mat_q);
-      if (tally) st->mats += 1;
+      if (threadIdx.x == 0)
+        for (int d = 0; d < 2; ++d)
+          if (s_j.mat[d]) s_j.c[d] = __ldcg(joint_dir(a, d).mat_q);
+      if (tally) st->mats += (s_j.mat[0] ? 1u : 0u) + (s_j.mat[1] ? 1u : 0u);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-      st->lq[s_clr] = 0;
-      if (!mat) st->mat_q = 0;
-    }
-    uint64_t const qn64 = c & qmask;
-    uint64_t const mf   = c >> a.qbits; // the frontier's edges (0 after a sweep)
-    if (qn64 == 0) {
-      // the search ran dry: rows cut short by the sweeps are walked to the
-      // end in slices over the grid; a listed candidate with a neighbour in
-      // mark joins, and the joined ones are the next (top-down) frontier.
-      // Ends when a fix-up step finds nothing.
-      uint32_t* const cut_list = a.heavy + (BW ? 0u : 3u) * a.heavy_cap;
-      uint32_t const  nc       = __ldcg(&st->cut_n[BW ? 1 : 0]);
-      if (nc == 0 || fixed) break;
-      fixed = true;
-      if (tally) st->fixups += 1;
-      unsigned const lane = threadIdx.x & 31u;
-      block_queue    bq{ sm.buf(), &sm.buf_n };
-      uint32_t const lim = nc < a.heavy_cap ? nc : a.heavy_cap;
-      for (uint32_t off = 0; off < lim; off += BU_BUF / 2) {
-        uint32_t const k = lim - off < BU_BUF / 2 ? lim - off : BU_BUF / 2; // at most k joins: the block queue holds them
-        heavy_slices(cut_list + off, k, bu_head, [&](uint32_t, uint32_t v, uint64_t b, uint64_t e) {
-          if (!((__shfl_sync(0xFFFFFFFFu, __ldcg(avail + (v >> 5)), 0) >> (v & 31)) & 1u)) return; // joined meanwhile
-          bool hit = false;
-          for (uint64_t x = b; x < e; x += 32) {
-            bool const     in = x + lane < e;
-            uint32_t const y  = in ? bu_adj[x + lane] : 0u;
-            bool const     h  = in && ((__ldcg(mark + (y >> 5)) >> (y & 31)) & 1u);
-            if (__any_sync(0xFFFFFFFFu, h)) {
-              hit = true;
-              break;
-            }
+    if (threadIdx.x == 0) {
+      if (blockIdx.x == 0)
+        for (int d = 0; d < 2; ++d) {
+          jdir const D = joint_dir(a, d);
+          D.lq[s_clr]  = 0;
+          if (!s_j.mat[d]) *D.mat_q = 0;
+        }
+      bool async = a.aw != nullptr, live = false;
+      s_j.restrict_to[0] = s_j.restrict_to[1] = 0; // one pass, in the level the partner ended
+      for (int d = 0; d < 2; ++d) {
+        s_j.kind[d] = JK_NONE;
+        if (!s_j.live[d]) continue;
+        unsigned long long const c  = s_j.c[d];
+        uint64_t const           qn = c & qmask, mf = c >> a.qbits;
+        if (qn == 0) {
+          // the search ran dry: rows the sweeps cut short are walked to the
+          // end in slices; it ends when a fix-up step finds nothing
+          if (__ldcg(joint_dir(a, d).cut_n) == 0 || s_j.fixed[d]) {
+            s_j.live[d] = 0;
+            if (s_j.live[d ^ 1]) s_j.restrict_to[d ^ 1] = 1; // the other search keeps only this one's set
+            continue;
           }
-          bool const took = hit && lane == 0 && bit_take(avail, v);
-          if (took) bit_claim(mark, v);
-          bq.push(took, v);
-        });
-        flush_scanned(sm, fout, &st->lq[s_out], a.qbits, td_head, a.n, a.m);
+          s_j.kind[d] = JK_FIXUP;
+          async       = false;
+          live        = true;
+          continue;
+        }
+        live          = true;
+        s_j.fixed[d]  = 0;
+        if (s_j.lvl[d] >= a.cap || qn > a.n || mf > a.m) {
+          // level cap; or counters beyond the graph, which a correct search
+          // never produces (then nothing more is read or written)
+          s_j.capped = 1;
+          break;
+        }
+        if (s_j.mat[d]) s_j.mode[d] = 0;
+        else if (s_j.mode[d] == 0 && mf * a.alpha > s_j.m_u[d]) s_j.mode[d] = 1;
+        s_j.kind[d] = s_j.mode[d] ? JK_BU : JK_TD;
+        if (!(s_j.mode[d] == 0 && s_j.lvl[d] >= ASYNC_AFTER && qn <= ASYNC_FRONTIER)) async = false;
       }
-      if (!gsync(a, epoch)) return SEARCH_FAILED;
-      stamp(a, 14);
-      mode = 0;
-      mat  = false;
-      continue;
+      s_j.async  = async && live && !s_j.capped;
+      s_j.any_td = s_j.kind[0] == JK_TD || s_j.kind[1] == JK_TD;
+      s_j.any_bu = s_j.kind[0] == JK_BU || s_j.kind[1] == JK_BU;
+      if (!live) s_j.capped |= 2; // both searches are done
+      s_j.cnt[0] = s_j.cnt[1] = 0;
     }
-    fixed = false;
-    if (lvl >= a.cap || qn64 > a.n || mf > a.m) {
-      // level cap; or counters beyond the graph, which a correct search
-      // never produces (then nothing more is read or written)
-      capped = 1;
-      break;
-    }
-    uint32_t const qn = static_cast<uint32_t>(qn64);
-    if (mat) mode = 0;
-    else if (mode == 0 && mf * a.alpha > m_u) mode = 1;
-    if (mode == 0 && lvl >= ASYNC_AFTER && qn <= ASYNC_FRONTIER && a.aw) {
-      // a long, thin search: finish it on the worklist
-      // The FW search's first worklist phase also runs the whole BW search
-      // (from the pivot, over every undecided vertex: FW(p) and BW(p) meet
-      // in the SCC, so BW need not wait for FW's set), and the BW level
-      // loop is skipped: a high-diameter graph pays its depth once.
-      uint64_t     ea = 0;
-      aw_dir const d0{ td_head, td_adj, avail, mark };
-      aw_dir const d1{ a.bh, a.bc, a.cand_bw, a.vis_b };
-      bool const   j  = !BW && a.cand_bw && !joint;
-      int const    r  = run_async(a, fin.q, qn, d0, j ? &d1 : nullptr, pivot, epoch, ea, sm);
+    __syncthreads();
+    if (s_j.capped) break;
+    // a search that lost its partner: keep only candidates in the partner's set
+#pragma unroll 1
+    for (int d = 0; d < 2; ++d)
+      if (s_j.restrict_to[d] && s_j.live[d]) {
+        if (tally) st->restricts += 1;
+        uint32_t* const       av = joint_dir(a, d).avail;
+        uint32_t const* const ot = joint_dir(a, d ^ 1).mark;
+        for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) {
+          uint32_t const keep = __ldcg(ot + w), cur = __ldcg(av + w);
+          if (cur & ~keep) atomicAnd(av + w, keep);
+        }
+      }
+    if (s_j.async) {
+      // long and thin: both searches finish on the worklist
+      uint64_t   ea = 0;
+      int const  d0 = s_j.live[0] ? 0 : 1;
+      bool const two = s_j.live[0] && s_j.live[1];
+      jdir const D0 = joint_dir(a, d0), D1 = joint_dir(a, 1);
+      aw_dir const w0{ D0.td_head, D0.td_adj, D0.avail, D0.mark };
+      aw_dir const w1{ D1.td_head, D1.td_adj, D1.avail, D1.mark };
+      frontier_buf const f0 = s_j.lvl[d0] == 0 ? a.seed : jbuf(D0, glvl);
+      frontier_buf const f1 = s_j.lvl[1] == 0 ? a.seed : jbuf(D1, glvl);
+      int const r = run_async(a, f0.q, static_cast<uint32_t>(s_j.c[d0] & qmask), w0, f1.q, static_cast<uint32_t>(s_j.c[1] & qmask), two ? &w1 : nullptr, epoch, ea, sm);
       if (r != SEARCH_DONE) return r;
-      joint = joint || j;
       stamp(a, 13);
-      edges_td += ea;
+      if (threadIdx.x == 0) {
+        s_j.edges_td[d0] += ea;
+        for (int d = 0; d < 2; ++d)
+          if (s_j.live[d]) s_j.c[d] = 0, s_j.mode[d] = 0, s_j.mat[d] = 0, s_j.lvl[d] += 1; // nothing queued: next it runs dry (or fixes up cut rows)
+      }
       if (tally) st->async_phases += 1;
-      // nothing is queued for the next level: it runs dry (or fixes up
-      // rows an earlier sweep cut short).  This level may have built its
-      // frontier from `fresh` (a bottom-up sweep before it): that is
-      // consumed, and the next level must not build it again
-      mode = 0;
-      mat  = false;
       continue;
     }
-    unsigned long long* const octr = &st->lq[s_out];
-    if (mode == 0) {
-      edges_td += mf;
-      if (tally) st->rows_td += qn;
-      uint32_t const ntiles = static_cast<uint32_t>((mf + EX_TILE - 1) / EX_TILE);
-      // few tiles: split each into `parts` slot ranges on separate blocks,
-      // so a small frontier still spreads over the grid
-      uint32_t parts = 1;
-      while (parts < EX_ITEMS && static_cast<uint64_t>(ntiles) * parts * 2 <= gridDim.x) parts *= 2;
-      int const      per   = EX_ITEMS / static_cast<int>(parts);
-      uint32_t const units = ntiles * parts;
-      take_op const  op{ avail, mark };
-      block_queue    bq{ sm.buf(), &sm.buf_n };
-      for (uint32_t unit = blockIdx.x; unit < units; unit += gridDim.x) {
-        int const part = static_cast<int>(unit % parts);
-        expand_tile(unit / parts, ntiles, fin.q, qn, mf, fin.prefix, fin.tile_start, td_head, td_adj, sm.tile_rows(), sm.tile_i, bq, op, part * per, part * per + per);
-        flush_scanned(sm, fout, octr, a.qbits, td_head, a.n, a.m);
+    // ---- the level's steps
+    if (s_j.any_td || s_j.kind[0] == JK_FIXUP || s_j.kind[1] == JK_FIXUP) {
+      uint32_t ntl[2] = { 0, 0 }, parts[2] = { 1, 1 }, units[2] = { 0, 0 };
+      uint32_t const share = s_j.kind[0] == JK_TD && s_j.kind[1] == JK_TD ? 4u : 2u; // the grid is split between two expansions
+#pragma unroll
+      for (int d = 0; d < 2; ++d)
+        if (s_j.kind[d] == JK_TD) {
+          uint64_t const mf = s_j.c[d] >> a.qbits;
+          ntl[d]            = static_cast<uint32_t>((mf + EX_TILE - 1) / EX_TILE);
+          // few tiles: split each into `parts` slot ranges on separate blocks,
+          // so a small frontier still spreads over the grid
+          while (parts[d] < EX_ITEMS && static_cast<uint64_t>(ntl[d]) * parts[d] * share <= gridDim.x) parts[d] *= 2;
+          units[d] = ntl[d] * parts[d];
+        }
+      block_queue bq{ sm.buf(), &sm.buf_n };
+      for (uint32_t unit = blockIdx.x; unit < units[0] + units[1]; unit += gridDim.x) {
+        int const          d    = unit < units[0] ? 0 : 1;
+        uint32_t const     u    = d ? unit - units[0] : unit;
+        uint32_t const     pd   = d ? parts[1] : parts[0];
+        jdir const         D    = joint_dir(a, d);
+        frontier_buf const fin  = s_j.lvl[d] == 0 ? a.seed : jbuf(D, glvl);
+        int const          per  = EX_ITEMS / static_cast<int>(pd);
+        int const          part = static_cast<int>(u % pd);
+        take_op const      op{ D.avail, D.mark };
+        expand_tile(u / pd, d ? ntl[1] : ntl[0], fin.q, static_cast<uint32_t>(s_j.c[d] & qmask), s_j.c[d] >> a.qbits, fin.prefix, fin.tile_start, D.td_head, D.td_adj, sm.tile_rows(), sm.tile_i, bq, op,
+                    part * per, part * per + per);
+        flush_scanned(sm, jbuf(D, glvl + 1), &D.lq[s_out], a.qbits, D.td_head, a.n, a.m);
       }
-    } else {
-      if (threadIdx.x == 0) sm.cnt = 0;
-      __syncthreads();
-      unsigned const wid    = threadIdx.x >> 5;
-      uint32_t       nfound = 0;
-      uint64_t       ne = 0, nc = 0;
-      if (tally) st->bu_bitmap += 1;
-      bu_sweep_warp<true>(blockIdx.x * BU_WARPS + wid, gridDim.x * BU_WARPS, a.n, bu_head, bu_adj, avail, mark, a.fresh, sm.warp[wid], nfound, ne, nc);
+#pragma unroll 1
+      for (int d = 0; d < 2; ++d)
+        if (s_j.kind[d] == JK_FIXUP) {
+          jdir const     D   = joint_dir(a, d);
+          uint32_t const nc  = __ldcg(D.cut_n);
+          uint32_t const lim = nc < a.heavy_cap ? nc : a.heavy_cap;
+          for (uint32_t off = 0; off < lim; off += BU_BUF / 2) {
+            uint32_t const k = lim - off < BU_BUF / 2 ? lim - off : BU_BUF / 2; // at most k joins: the block queue holds them
+            heavy_slices(D.cut_list + off, k, D.bu_head, [&](uint32_t, uint32_t v, uint64_t b, uint64_t e) {
+              if (!((__shfl_sync(0xFFFFFFFFu, __ldcg(D.avail + (v >> 5)), 0) >> (v & 31)) & 1u)) return; // joined meanwhile
+              bool hit = false;
+              for (uint64_t x = b; x < e; x += 32) {
+                bool const     in = x + lane < e;
+                uint32_t const y  = in ? D.bu_adj[x + lane] : 0u;
+                bool const     h  = in && ((__ldcg(D.mark + (y >> 5)) >> (y & 31)) & 1u);
+                if (__any_sync(0xFFFFFFFFu, h)) {
+                  hit = true;
+                  break;
+                }
+              }
+              bool const took = hit && lane == 0 && bit_take(D.avail, v);
+              if (took) bit_claim(D.mark, v);
+              bq.push(took, v);
+            });
+            flush_scanned(sm, jbuf(D, glvl + 1), &D.lq[s_out], a.qbits, D.td_head, a.n, a.m);
+          }
+          if (tally) st->fixups += 1;
+        }
+    }
+    if (s_j.any_bu) {
+      // both searches' chunks in one range, spread over every warp of the grid
+      uint32_t const chunks = (words + 31) / 32;
+      uint32_t const c0     = s_j.kind[0] == JK_BU ? chunks : 0u;
+      uint32_t const c1     = s_j.kind[1] == JK_BU ? chunks : 0u;
+      uint32_t       nf0 = 0, nf1 = 0;
+      uint64_t       ne = 0, ncd = 0;
+      for (uint32_t cc = blockIdx.x * BU_WARPS + wid; cc < c0 + c1; cc += gridDim.x * BU_WARPS) {
+        int const      d = cc < c0 ? 0 : 1;
+        jdir const     D = joint_dir(a, d);
+        uint32_t       f = 0;
+        bu_sweep_chunk(d ? cc - c0 : cc, a.n, D.bu_head, D.bu_adj, D.avail, D.mark, D.fresh, s_bu_cut[d], sm.warp[wid], f, ne, ncd);
+        if (d) nf1 += f;
+        else nf0 += f;
+      }
 #pragma unroll
       for (int sh = 16; sh; sh >>= 1) {
-        nfound += __shfl_down_sync(0xFFFFFFFFu, nfound, sh);
+        nf0 += __shfl_down_sync(0xFFFFFFFFu, nf0, sh);
+        nf1 += __shfl_down_sync(0xFFFFFFFFu, nf1, sh);
         ne += __shfl_down_sync(0xFFFFFFFFu, ne, sh);
       }
-      if ((threadIdx.x & 31) == 0) {
-        if (nfound) atomicAdd(&sm.cnt, nfound);
+      if (lane == 0) {
+        if (nf0) atomicAdd(&s_j.cnt[0], nf0);
+        if (nf1) atomicAdd(&s_j.cnt[1], nf1);
         if (ne) atomicAdd(&sm.edges_bu, static_cast<unsigned long long>(ne));
-        if (nc) atomicAdd(&sm.cands_bu, static_cast<unsigned long long>(nc)); // counted by lane 0
+        if (ncd) atomicAdd(&sm.cands_bu, static_cast<unsigned long long>(ncd)); // counted by lane 0
       }
       __syncthreads();
-      if (threadIdx.x == 0 && sm.cnt) atomicAdd(octr, static_cast<unsigned long long>(sm.cnt)); // vertices only
+      if (threadIdx.x == 0)
+        for (int d = 0; d < 2; ++d)
+          if (s_j.cnt[d]) atomicAdd(&joint_dir(a, d).lq[s_out], static_cast<unsigned long long>(s_j.cnt[d])); // vertices only
+      if (tally) st->bu_bitmap += (c0 ? 1u : 0u) + (c1 ? 1u : 0u);
     }
     if (!gsync(a, epoch)) return SEARCH_FAILED;
-    stamp(a, mode ? 5u : 4u);
-    m_u = m_u > mf ? m_u - mf : 0;
-    bu += mode;
-    mat = false;
-    uint32_t const next = static_cast<uint32_t>(__ldcg(&st->lq[s_out]) & qmask);
-    if (mode == 1) {
-      // stay bottom-up while the sweep found at least n_und / beta vertices
-      mat = next != 0 && static_cast<unsigned long long>(next) * a.beta < n_und;
-    } else if (tally) st->pushed_td += next;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    if (BW) st->levels_bw = lvl, st->bu_bw = bu;
-    else st->levels_fw = lvl, st->bu_fw = bu;
-    st->edges_td += edges_td;
-  }
-  {
-    // the cut rows' bits leave cutmap before the next search can cut (its
-    // first bottom-up sweep comes after at least one more barrier); the
-    // count itself stays (the other search lists into its own slot)
-    uint32_t const* const cut_list = a.heavy + (BW ? 0u : 3u) * a.heavy_cap;
-    uint32_t const        nc       = __ldcg(&st->cut_n[BW ? 1 : 0]);
-    for (uint32_t i = blockIdx.x * R_THREADS + threadIdx.x; i < nc && i < a.heavy_cap; i += gridDim.x * R_THREADS) {
-      uint32_t const v = __ldcg(cut_list + i);
-      atomicAnd(a.cutmap + (v >> 5), ~(1u << (v & 31)));
+    stamp(a, s_j.any_td ? 4u : (s_j.any_bu ? 5u : 14u));
+    if (threadIdx.x == 0) {
+      for (int d = 0; d < 2; ++d) {
+        uint32_t const k = s_j.kind[d];
+        if (k == JK_NONE) continue;
+        jdir const               D    = joint_dir(a, d);
+        unsigned long long const next = __ldcg(&D.lq[s_out]);
+        uint64_t const           mf   = s_j.c[d] >> a.qbits;
+        s_j.lvl[d] += 1;
+        s_j.mat[d] = 0;
+        if (k == JK_FIXUP) {
+          s_j.fixed[d] = 1;
+          s_j.mode[d]  = 0;
+        } else {
+          s_j.m_u[d] = s_j.m_u[d] > mf ? s_j.m_u[d] - mf : 0;
+          if (k == JK_BU) {
+            s_j.bu[d] += 1;
+            // stay bottom-up while the sweep found at least n_und / beta vertices
+            uint64_t const nx = next & qmask;
+            s_j.mat[d]        = nx != 0 && nx * a.beta < n_und;
+          } else {
+            s_j.edges_td[d] += mf;
+            if (tally) st->rows_td += s_j.c[d] & qmask, st->pushed_td += next & qmask;
+          }
+        }
+        s_j.c[d] = next;
+      }
     }
   }
-  return capped ? SEARCH_CAPPED : SEARCH_DONE;
+  if (s_j.capped & 1) rc = SEARCH_CAPPED;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->levels_fw = s_j.lvl[0], st->bu_fw = s_j.bu[0];
+    st->levels_bw = s_j.lvl[1], st->bu_bw = s_j.bu[1];
+    st->edges_td += s_j.edges_td[0] + s_j.edges_td[1];
+    st->joint = 1;
+  }
+  // the cut rows' bits leave the cut maps before the next search can cut
+  // (its first sweep comes after at least one more barrier)
+#pragma unroll 1
+  for (int d = 0; d < 2; ++d) {
+    jdir const     D  = joint_dir(a, d);
+    uint32_t const nc = __ldcg(D.cut_n);
+    for (uint32_t i = blockIdx.x * R_THREADS + threadIdx.x; i < nc && i < a.heavy_cap; i += gridDim.x * R_THREADS) {
+      uint32_t const v = __ldcg(D.cut_list + i);
+      atomicAnd(s_bu_cut[d].map + (v >> 5), ~(1u << (v & 31)));
+    }
+  }
+  if (rc == SEARCH_DONE) {
+    // the SCC: FW(p) & BW(p)
+    for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) a.vis_b[w] = __ldcg(a.vis_b + w) & __ldcg(a.vis_a + w);
+    if (!gsync(a, epoch)) return SEARCH_FAILED;
+  }
+  return rc;
 }
 
 // ---------------------------------------------------------------- trim tail
@@ -1831,7 +1970,8 @@ k_fwbw(fwbw_args a)
     st->marks   = 0;
     stamp(a, 0);
     st->lq[0] = st->lq[1] = st->lq[2] = 0;
-    st->mat_q                         = 0;
+    st->lq_bw[0] = st->lq_bw[1] = st->lq_bw[2] = 0;
+    st->mat_q = st->mat_q_bw = 0;
     st->id                            = UNDECIDED;
     st->decided                       = 0;
     st->edges_bu = st->cands_bu = st->edges_td = 0;
@@ -1843,7 +1983,7 @@ k_fwbw(fwbw_args a)
     st->mats = st->bu_bitmap    = 0;
     st->async_phases            = 0;
     st->cut_n[0] = st->cut_n[1] = st->fixups = 0;
-    st->hseed_n = st->heavy_err = st->trim_async = st->joint = 0;
+    st->hseed_n = st->heavy_err = st->trim_async = st->joint = st->restricts = 0;
     for (int i = 0; i < 6; ++i) st->hq_n[i] = 0;
     if (search) a.seed.q[0] = p, a.seed.prefix[0] = 0;
   }
@@ -1859,7 +1999,7 @@ k_fwbw(fwbw_args a)
       a.cand[w]          = u & ~pin;
       a.vis_a[w]         = pin;
       a.vis_b[w]         = pin;
-      if (a.cand_bw) a.cand_bw[w] = u & ~pin;
+      a.cand_bw[w]       = u & ~pin;
       c += __popc(u);
     }
     uint64_t tot;
@@ -1872,26 +2012,7 @@ k_fwbw(fwbw_args a)
       for (uint32_t i = threadIdx.x; i < gridDim.x; i += R_THREADS) s += __ldcg(a.partial + i);
       block_exclusive_scan<uint64_t, R_THREADS>(s, &tot);
       uint32_t const n_und = static_cast<uint32_t>(tot);
-      // one inlined copy of the level loop, run for FW then BW
-      bool joint = false; // the FW search's worklist phase ran BW as well
-#pragma unroll 1
-      for (int dir = 0; dir < 2 && rc == SEARCH_DONE; ++dir) {
-        if (dir && joint) {
-          // BW(p) over every undecided vertex is complete: the SCC is
-          // FW(p) & BW(p)
-          for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) a.vis_b[w] = __ldcg(a.vis_b + w) & __ldcg(a.vis_a + w);
-          if (!gsync(a, epoch)) rc = SEARCH_FAILED;
-          if (blockIdx.x == 0 && threadIdx.x == 0) st->joint = 1;
-          break;
-        }
-        if (dir) {
-          // BW: candidates are the FW-reached vertices except the pivot
-          // (each block clears its bit before its own first expansion)
-          if (threadIdx.x == 0) atomicAnd(a.vis_a + (p >> 5), ~(1u << (p & 31)));
-          __syncthreads();
-        }
-        rc = dir ? run_search<true>(a, sm, p, n_und, glvl, epoch, joint) : run_search<false>(a, sm, p, n_und, glvl, epoch, joint);
-      }
+      rc = run_joint(a, sm, p, n_und, glvl, epoch);
     }
     if (rc == SEARCH_DONE && a.min_ids) {
       // smallest member = first set bit of vis_b.  Every block first looks
@@ -2202,9 +2323,12 @@ launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* s
   a.vis_a       = ws.vis_a;
   a.vis_b       = ws.vis_b;
   a.fresh       = ws.fresh;
+  a.fresh_bw    = ws.fresh_bw;
   a.cand_bw     = ws.cand_bw;
   a.fb[0]       = { ws.q0, ws.prefix, ws.tile_start };
   a.fb[1]       = { ws.q1, ws.prefix2, ws.tile_start2 };
+  a.fb_bw[0]    = { ws.q2, ws.prefix3, ws.tile_start3 };
+  a.fb_bw[1]    = { ws.q3, ws.prefix4, ws.tile_start4 };
   a.seed        = { ws.seed_q, ws.seed_prefix, ws.tile_zero };
   a.partial     = ws.blocks;
   a.pv_prod     = ws.pivot + PV_FINAL;
@@ -2219,6 +2343,7 @@ launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* s
   a.heavy       = ws.heavy;
   a.heavy_cap   = static_cast<uint32_t>(ws.heavy_cap);
   a.cutmap      = ws.cutmap;
+  a.cut_words   = static_cast<uint32_t>((static_cast<size_t>(ws.n_cap) + 63) / 64 * 2 + 2);
   a.bar         = gbar;
   a.st          = rs;
   a.stamp_phase = reinterpret_cast<uint32_t*>(static_cast<char*>(ws.rstate) + 2048);
@@ -2249,7 +2374,7 @@ check_persistent(kspn_context* ctx)
     // worklist may hold entries: start over
     KSPN_CUDA(cudaMemsetAsync(ctx->ws.gbar, 0, 4096, ctx->stream));
     KSPN_CUDA(cudaMemsetAsync(ctx->ws.aw, 0, ctx->ws.aw_entries * sizeof(unsigned long long), ctx->stream));
-    KSPN_CUDA(cudaMemsetAsync(ctx->ws.cutmap, 0, ((static_cast<size_t>(ctx->ws.n_cap) + 63) / 64 * 2 + 2) * sizeof(uint32_t), ctx->stream));
+    KSPN_CUDA(cudaMemsetAsync(ctx->ws.cutmap, 0, 2 * ((static_cast<size_t>(ctx->ws.n_cap) + 63) / 64 * 2 + 2) * sizeof(uint32_t), ctx->stream));
     KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
     throw error{ KSPN_ERR_TIMEOUT, "reachability: grid barrier wait limit reached" };
   }
@@ -2306,11 +2431,12 @@ fw_bw_trim_result(kspn_context* ctx, dgraph const& g, kspn_options const& opt, k
     // rows of every listed and every queued vertex); neighbour ids read;
     // bitmap passes -- init (und read, three bitmaps written), two per
     // bitmap sweep (avail, fresh), one per frontier built from fresh,
-    // finalize (vis_b, und read + written, snap), ids (und, vis_b) -- and
-    // the ids written
+    // the SCC as FW & BW (both read, one written), a restriction of one
+    // search to the other's set (two read), finalize (vis_b, und read +
+    // written, snap), ids (und, vis_b) -- and the ids written
     uint64_t const rows   = hs->cands_bu + hs->rows_td + hs->pushed_td + 2 * (hs->list_n + hs->trim_decided);
     uint64_t const edges  = hs->edges_td + hs->edges_bu + hs->trim_edges;
-    uint32_t const passes = hs->pivot_used < g.n ? 4 + 2 * hs->bu_bitmap + hs->mats + 4 + 2 : 1;
+    uint32_t const passes = hs->pivot_used < g.n ? 4 + 2 * hs->bu_bitmap + hs->mats + 3 + 2 * hs->restricts + 4 + 2 : 1;
     st->resident_rows          = rows;
     st->resident_edges         = edges;
     st->resident_bitmap_passes = passes;
@@ -2320,6 +2446,7 @@ fw_bw_trim_result(kspn_context* ctx, dgraph const& g, kspn_options const& opt, k
     st->heavy_trim_seeds       = hs->hseed_n;
     st->trim_worklist          = hs->trim_async;
     st->fwbw_joint             = hs->joint;
+    st->search_worklist        = hs->async_phases ? 1u : 0u;
   }
   resident_result r;
   r.pivot             = hs->pivot_used;

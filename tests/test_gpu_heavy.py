@@ -151,8 +151,8 @@ def test_joint_worklist_search(ctx, heavy):
         ctx.scc_device(n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, K.default_options(validate=0), st)
         assert np.array_equal(out.cpu().numpy().view(np.uint32), want)
         dct = st.as_dict()
-        assert dct["fwbw_joint"] == 1, "the BW search should run inside the FW worklist phase"
-        assert dct["levels_bw"] == 0
+        assert dct["fwbw_joint"] == 1, "FW and BW run side by side"
+        assert dct["search_worklist"] == 1, "and finish on the worklist together"
 
 
 def _path_core_chain_graph():
@@ -196,7 +196,7 @@ def test_bottom_up_then_worklist(ctx):
         assert np.array_equal(out.cpu().numpy().view(np.uint32), want)
         dct = st.as_dict()
         assert dct["levels_bottom_up"] > 0, "the search should run bottom-up levels in the core"
-        assert dct["fwbw_joint"] == 1, "and finish on the worklist after them"
+        assert dct["search_worklist"] == 1, "and finish on the worklist after them"
 
 
 # The worklist tail leaves a find's take to its consumer until a warp's
@@ -220,4 +220,4 @@ def test_worklist_exact_takes(ctx, shape, after):
         ctx.scc_device(n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, K.default_options(validate=0, aw_exact_after=after), st)
         assert np.array_equal(out.cpu().numpy().view(np.uint32), want)
     if shape.startswith("joint"):
-        assert st.as_dict()["fwbw_joint"] == 1
+        assert st.as_dict()["search_worklist"] == 1
