@@ -56,6 +56,10 @@ WORKLOADS = {
     "rgg24": ("rgg", dict(n=1 << 24, seed=3), "2D random geometric graph n=2^24, mean undirected degree 8, each pair u->v / v->u / both / neither with p=.25"),
     "rgg20": ("rgg", dict(n=1 << 20, seed=3), "2D random geometric graph n=2^20, mean undirected degree 8, each pair u->v / v->u / both / neither with p=.25"),
 }
+# kspn pipelines by name: the FAST pipeline, kaspan::scc's phase order
+# ("reference") and the reference's six variants (variant/*.hpp)
+PIPELINES = {"fast": 0, "reference": 1, "hpc_like": 2, "hpc_trim_ex": 3, "ispan_like": 4, "trim_ex": 5, "trim_ex_light_residual": 6, "trim_ex_residual": 7}
+
 # The reference arm decomposes the identical graph, except where one
 # reference call takes about a minute (R-MAT s26: 1.06 B edges and a 16 GiB
 # hash set at one rank), so W + K calls would not end within minutes.
@@ -386,6 +390,57 @@ def run_rmat26(ctx, stream, args, peak, K):
     return res
 
 
+def run_sharded(ctx, args, K, world, rank):
+    """ONE graph over all ranks (kaspan_b200/shard.py: a contiguous vertex
+    range per GPU, frontier exchange over NCCL every level): the workload of
+    seed 0 on every rank, sharded; time per decomposition = max over ranks
+    (the ranks meet at a collective every level).  Its ids are checked
+    against the single-GPU decomposition of the same graph."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from kaspan_b200 import shard as SH
+
+    G = make_graph(ctx, args.workload, rank_seed=0)
+    want = torch.empty(G.n, dtype=torch.int32, device="cuda")
+    ctx.scc_device(G.n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, want, K.default_options(validate=0))
+    fwh_h = G.fwh.cpu().numpy().view(np.uint64)
+    bounds = SH.partition_bounds(G.n, fwh_h, world)
+    lo, hi = bounds[rank], bounds[rank + 1]
+    bwh_h = G.bwh.cpu().numpy().view(np.uint64)
+    fb, fe, bb, be = int(fwh_h[lo]), int(fwh_h[hi]), int(bwh_h[lo]), int(bwh_h[hi])
+    S = SH.Shard(G.n, rank, world, bounds, (G.fwh[lo: hi + 1] - fb).contiguous(), G.fwc[fb: max(fe, fb + 1)].contiguous(),
+                 (G.bwh[lo: hi + 1] - bb).contiguous(), G.bwc[bb: max(be, bb + 1)].contiguous())
+    want_local = want[lo:hi].cpu().numpy().view(np.uint32).copy()
+    m = G.m
+    del G, want
+    torch.cuda.empty_cache()
+    ex = SH.Exchange()
+    times, st = [], None
+    for i in range(3):
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = SH.ShardStats()
+        ids = SH.scc_sharded(SH.CudaShardOps(ctx, S), ex, S, stats=st)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        t = torch.tensor([dt], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        times.append(float(t.item()))
+    ok = bool(np.array_equal(ids.cpu().numpy().view(np.uint32), want_local))
+    okt = torch.tensor([1 if ok else 0], device="cuda")
+    dist.all_reduce(okt, op=dist.ReduceOp.MIN)
+    ms = 1e3 * min(times[1:])
+    return {"workload": WORKLOADS[args.workload][2], "n": S.n, "m": m, "ranks": world, "bounds": bounds,
+            "value": m / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "scaling": "strong (one graph, all ranks)",
+            "timing": "host wall clock around the whole sharded call, max over ranks (every level meets at a collective), best of 2 after 1 warm-up",
+            "exchange": "NCCL all_to_all_single of frontier ids per level + all-reduces", "identical_to_single_gpu": bool(okt.item()),
+            "rounds": st.rounds, "levels": st.levels, "ids_sent_rank0": st.exchanged,
+            "decided": {"trim_first": st.decided_trim, "fwbw": st.decided_fwbw, "residual": st.decided_residual}}
+
+
 def run_kspn(args):
     import numpy as np
     import torch
@@ -406,7 +461,7 @@ def run_kspn(args):
     G = make_graph(ctx, args.workload, rank_seed=rank)
     torch.cuda.synchronize()
     out = torch.empty(G.n, dtype=torch.int32, device="cuda")
-    pipeline = K.PIPELINE_FAST if args.pipeline == "fast" else K.PIPELINE_REFERENCE
+    pipeline = PIPELINES[args.pipeline]
     opt = K.default_options(pipeline=pipeline, validate=0)
     prof_opt = K.default_options(pipeline=pipeline, validate=0, profile=1)
     trace_opt = K.default_options(pipeline=pipeline, validate=0, trace=1)
@@ -539,6 +594,7 @@ def run_kspn(args):
     rmat26 = None
     if rank == 0 and world == 1 and args.workload == "rmat24" and not args.no_rmat26:
         rmat26 = run_rmat26(ctx, stream, args, peak, K)
+    sharded = run_sharded(ctx, args, K, world, rank) if world > 1 else None
 
     if rank == 0:
         line = {
@@ -558,6 +614,7 @@ def run_kspn(args):
             "clocks": clk.summary(),
             "learned_vs_plain": lvp,
             "rmat26": rmat26,
+            "sharded": sharded,
             "autotune": autotune,
             "batched": batched,
             "phases": {"decided": last["decided"], "ms": {k: round(v, 4) for k, v in last["ms"].items()}, "levels_fw": last["levels_fw"],
@@ -591,7 +648,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="kspn", choices=["kspn", "reference"])
     ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS))
-    ap.add_argument("--pipeline", default="fast", choices=["fast", "reference"])
+    ap.add_argument("--pipeline", default="fast", choices=sorted(PIPELINES), help="fast (default), or the phase order of a reference entry point")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-path and autotuner sections")
     ap.add_argument("--no-rmat26", action="store_true", help="skip the R-MAT scale-26 section")
