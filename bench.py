@@ -4,8 +4,9 @@
                     [--workload rmat24|rmat26|rgg24|gnm16] [--pipeline fast|reference]
 
 A step is one complete decomposition of the workload graph (strongly
-connected components, canonical min-id labels).  Default workload: directed
-R-MAT scale 24, edge factor 16, a,b,c,d = .57,.19,.19,.05, seeded id
+connected components, canonical min-id labels).  Default workload: the
+learned-pivot configuration, directed R-MAT scale 26 (2^26 vertices, 1.06 B
+edges after dedup), edge factor 16, a,b,c,d = .57,.19,.19,.05, seeded id
 permutation, self-loops and duplicates removed, u32 ids, u64 offsets --
 generated on the device by the library's own seeded generator.
 
@@ -16,15 +17,23 @@ e2e     = the same metric through the host C-ABI call kspn_scc with pinned
           labels copied out, every step.
 roofline: the dominant kernel's algorithmic bytes / its event-timed
           duration, against MEASURED_PEAKS.json's HBM copy bandwidth.
+learned_vs_plain: the workload decomposed from the plain max(in * out)
+          pivot and from the shipped pivot model's, same output asserted;
+          and the same on the workload with decoy hubs.
 cpu_baseline: the reference's own kaspan::scc (oracle/_ref, compiled from its
-          sources; 1 core, MPI absent) on the same graph, one call.
-rmat26  = the R-MAT scale-26 configuration (the learned-pivot one): device
-          time, learned vs plain pivot, end to end, roofline.
+          sources; 1 core, MPI absent), one call on a bounded sample: the
+          workload itself where one call takes seconds, R-MAT scale 24
+          (a quarter of the scale-26 workload) for R-MAT scale 26.
+other_rmat = the other R-MAT configuration (scale 24 beside the scale-26
+          workload, and the reverse): device time, roofline, learned vs
+          plain pivot, end to end.
 
---impl reference: the reference's kaspan::scc on the host cores, one call per
-step on the identical graph (the oracle's C generator draws the same edges
-as the device generator), except R-MAT s26, whose one-rank reference call
-takes about a minute: its reference arm decomposes R-MAT s24.
+--impl reference: the reference's kaspan::scc on the host cores on the
+identical graph (the oracle's C generator draws the same edges as the
+device generator), one call per step; where one call takes tens of seconds
+(R-MAT scale 26: 1.06 B edges and a 16 GiB hash set at one rank) the arm
+times as many calls as fit in --reference-seconds (at least one) and
+states the count.
 
 Multi-GPU (torchrun): every rank decomposes its own seeded instance (seed +
 rank); value = edges over all ranks / max-over-ranks time ("weak" scaling,
@@ -60,10 +69,10 @@ WORKLOADS = {
 # ("reference") and the reference's six variants (variant/*.hpp)
 PIPELINES = {"fast": 0, "reference": 1, "hpc_like": 2, "hpc_trim_ex": 3, "ispan_like": 4, "trim_ex": 5, "trim_ex_light_residual": 6, "trim_ex_residual": 7}
 
-# The reference arm decomposes the identical graph, except where one
-# reference call takes about a minute (R-MAT s26: 1.06 B edges and a 16 GiB
-# hash set at one rank), so W + K calls would not end within minutes.
-REFERENCE_GRAPH = {"rmat26": "rmat24"}
+# The other R-MAT configuration reported beside an R-MAT workload, and the
+# bounded sample the kspn arm's cpu_baseline decomposes on the host.
+OTHER_RMAT = {"rmat26": "rmat24", "rmat24": "rmat26"}
+CPU_SAMPLE = {"rmat26": "rmat24"}
 
 
 def measured_peak_gbs():
@@ -147,17 +156,27 @@ def host_graph(name):
     return O.gnm(p["n"], p["draws"], p["seed"])
 
 
-def reference_calls(G, steps, warmup=0):
+def reference_calls(G, steps, warmup=0, budget_s=None):
     """The reference's kaspan::scc (oracle/_ref) on host graph G: edges/s of
-    each timed call, or None when oracle/_ref is absent."""
+    each timed call, or None when oracle/_ref is absent.  With budget_s the
+    warm-up calls are skipped and the timed calls stop once their total
+    passes budget_s (at least one call)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
     if O.ref_lib() is None:
         return None
-    for _ in range(warmup):
-        O.ref_scc(G)
-    return [G.m / O.ref_scc(G)[1] for _ in range(steps)]
+    if budget_s is None:
+        for _ in range(warmup):
+            O.ref_scc(G)
+    rates, spent = [], 0.0
+    for _ in range(steps):
+        secs = O.ref_scc(G)[1]
+        rates.append(G.m / secs)
+        spent += secs
+        if budget_s is not None and spent >= budget_s:
+            break
+    return rates
 
 
 def run_reference(args):
@@ -170,22 +189,24 @@ def run_reference(args):
     if O.ref_lib() is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libkspn_ref.so was not built (reference sources absent at build time)"}))
         return 0
-    gname = REFERENCE_GRAPH.get(args.workload, args.workload)
-    G = host_graph(gname)
-    rates = reference_calls(G, args.steps, args.warmup)
+    t0 = time.perf_counter()
+    G = host_graph(args.workload)
+    gen_s = time.perf_counter() - t0
+    budget = args.reference_seconds if G.m > (1 << 29) else None
+    rates = reference_calls(G, args.steps, args.warmup, budget)
     v = statistics.mean(rates)
-    same = gname == args.workload
-    sample = (f"the workload graph itself ({WORKLOADS[gname][2]}: n={G.n}, m={G.m}), one kaspan::scc call per step "
+    sample = (f"the workload graph itself ({WORKLOADS[args.workload][2]}: n={G.n}, m={G.m}), one kaspan::scc call per step "
               "(reference code compiled from its sources, 1 rank, 1 core)")
-    if not same:
-        sample = (f"{WORKLOADS[gname][2]} (n={G.n}, m={G.m}) standing in for {WORKLOADS[args.workload][2]}: one reference "
-                  "call on the full workload takes about a minute; one kaspan::scc call per step (1 rank, 1 core)")
+    if budget is not None:
+        sample += (f"; {len(rates)} timed call(s) of the {args.steps} asked, no warm-up calls: one call takes "
+                   f"{1e3 * G.m / v / 1e3:.0f} s, so the arm stops after {budget:.0f} s of calls")
     line = {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": len(rates),
+        "warmup": 0 if budget is not None else args.warmup, "steps_asked": args.steps,
         "ms_per_step": 1e3 * G.m / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (seeded generators standing in for KaGen R-MAT / G(n,m) / RGG)",
-        "config": {"workload": WORKLOADS[args.workload][2], "n": G.n, "m": G.m, "same_graph": same, "sample": sample,
-                   "mpi": "absent on this host: single rank"},
+        "config": {"workload": WORKLOADS[args.workload][2], "n": G.n, "m": G.m, "same_graph": True, "sample": sample,
+                   "host_generation_s": round(gen_s, 1), "mpi": "absent on this host: single rank"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -208,9 +229,9 @@ def run_batched(ctx, stream, args, K, world=1, rank=0):
 
     shard = None
     if world > 1:
-        n_all, d_all = K.batch_shape(4096, 5)
+        n_all, d_all = K.batch_shape(args.batch_graphs, 5, 8, args.batch_max_log2)
         shard = KG.batch_partition(n_all.astype(np.float64) + d_all.astype(np.float64), world)[rank]
-    B = KG.batch(ctx, 4096, 5, graphs=shard)
+    B = KG.batch(ctx, args.batch_graphs, 5, 8, args.batch_max_log2, graphs=shard)
     out = torch.empty(B.n, dtype=torch.int32, device="cuda")
     steps = max(3, min(args.steps, 10))
 
@@ -251,8 +272,8 @@ def run_batched(ctx, stream, args, K, world=1, rank=0):
     peak, peak_kind = measured_peak_gbs()
     b_min = 2 * (8 * (n_all_v + 1) + 4 * m_all) + 4 * n_all_v
     res = {
-        "workload": "4096 directed G(n,m) graphs, n = round(2^U[8,18]), m = round(n * U[0.8, 6]) draws, seed 5, self-loops and duplicates removed, local u32 ids, one concatenated CSR + CSC",
-        "graphs": 4096, "n": int(n_all_v), "m": int(m_all), "steps": steps, "n_gpus": world,
+        "workload": f"{args.batch_graphs} directed G(n,m) graphs, n = round(2^U[8,{args.batch_max_log2}]), m = round(n * U[0.8, 6]) draws, seed 5, self-loops and duplicates removed, local u32 ids, one concatenated CSR + CSC",
+        "graphs": args.batch_graphs, "n": int(n_all_v), "m": int(m_all), "steps": steps, "n_gpus": world,
         "scaling": "strong" if world > 1 else None, "sharding": "greedy edge-balanced bin packing of whole graphs, no communication" if world > 1 else None,
         "value": m_all / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
         "launches_per_step": launches, "captured": "one CUDA graph per call (plan + solve kernels), replayed",
@@ -269,7 +290,7 @@ def run_batched(ctx, stream, args, K, world=1, rank=0):
 
         if O.ref_lib() is not None:
             secs, edges = 0.0, 0
-            for g in range(256):
+            for g in range(min(256, B.count)):
                 n, fwh, fwc, bwh, bwc = B.graph(g)
                 _, t = O.ref_scc(O.Graph(n, fwh, np.ascontiguousarray(fwc) if fwc.size else np.zeros(1, np.uint32), bwh,
                                          np.ascontiguousarray(bwc) if bwc.size else np.zeros(1, np.uint32)))
@@ -358,22 +379,23 @@ def learned_vs_plain(ctx, stream, graph, pipeline, steps):
     return res
 
 
-def run_rmat26(ctx, stream, args, peak, K):
-    """R-MAT scale 26 (n = 2^26, 1.06 B edges, CSR + CSC 9.5 GB), the
-    learned-pivot configuration: device time per decomposition, k_fwbw's
-    roofline, learned vs plain pivot, and end to end through kspn_scc."""
+def run_other_rmat(ctx, stream, args, peak, K, name, cpu_sample):
+    """The other R-MAT configuration (`name`: scale 24 beside the scale-26
+    workload, or the reverse): device time per decomposition, k_fwbw's
+    roofline, learned vs plain pivot and end to end through kspn_scc.  With
+    cpu_sample, also one reference kaspan::scc call on this graph's host
+    copy (the kspn arm's bounded cpu_baseline sample)."""
+    import numpy as np
     import torch
 
-    import kaspan_b200.graphs as KG
-
-    G = KG.rmat(ctx, 26, 16, 4)
+    G = make_graph(ctx, name)
     out = torch.empty(G.n, dtype=torch.int32, device="cuda")
     opt = K.default_options(validate=0)
     steps = max(3, min(args.steps, 10))
     timed_steps(ctx, stream, G, opt, 3, out)
     ms, st = timed_steps(ctx, stream, G, opt, steps, out)
     dicts = [s.as_dict() for s in st]
-    res = {"workload": WORKLOADS["rmat26"][2], "n": G.n, "m": G.m, "steps": steps, "value": G.m / (ms * 1e-3), "unit": UNIT,
+    res = {"workload": WORKLOADS[name][2], "n": G.n, "m": G.m, "steps": steps, "value": G.m / (ms * 1e-3), "unit": UNIT,
            "ms_per_step": ms, "roofline": resident_roofline(dicts, peak),
            "pipeline_frac": (2 * (8 * (G.n + 1) + 4 * G.m) + 4 * G.n) / (ms * 1e-3) / 1e9 / peak}
     model = K.default_pivot_model()
@@ -384,10 +406,20 @@ def run_rmat26(ctx, stream, args, peak, K):
     e2e_ms, _ = host_e2e(ctx, stream, G, K.default_options(validate=0), 3, 1)
     res["e2e"] = {"value": G.m / (e2e_ms * 1e-3), "unit": UNIT, "ms_per_step": e2e_ms, "h2d_bytes_per_step": 8 * (G.n + 1) + 4 * G.m,
                   "d2h_bytes_per_step": 4 * G.n}
-    res["cpu_baseline"] = {"note": "not run by default: one reference kaspan::scc call on this graph takes about a minute at one rank"}
+    cpu = None
+    if cpu_sample:
+        fwh, fwc, bwh, bwc = G.to_host()
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        rates = reference_calls(O.Graph(G.n, np.ascontiguousarray(fwh), np.ascontiguousarray(fwc), np.ascontiguousarray(bwh), np.ascontiguousarray(bwc)), 1)
+        if rates is not None:
+            cpu = {"value": rates[0], "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"{WORKLOADS[name][2]} (n={G.n}, m={G.m}), the same generator at a quarter of the workload's scale: "
+                             "one kaspan::scc call (reference code, 1 rank, 1 core); --impl reference times the workload itself"}
     del G, out
     torch.cuda.empty_cache()
-    return res
+    return res, cpu
 
 
 def run_sharded(ctx, args, K, world, rank):
@@ -591,9 +623,10 @@ def run_kspn(args):
     last = step_stats[-1]
     b_min = 2 * (8 * (G.n + 1) + 4 * G.m) + 4 * G.n
 
-    rmat26 = None
-    if rank == 0 and world == 1 and args.workload == "rmat24" and not args.no_rmat26:
-        rmat26 = run_rmat26(ctx, stream, args, peak, K)
+    other, other_cpu = None, None
+    oname = OTHER_RMAT.get(args.workload)
+    if rank == 0 and world == 1 and oname and not args.no_other_rmat:
+        other, other_cpu = run_other_rmat(ctx, stream, args, peak, K, oname, not args.no_cpu_baseline and CPU_SAMPLE.get(args.workload) == oname)
     sharded = run_sharded(ctx, args, K, world, rank) if world > 1 else None
 
     if rank == 0:
@@ -613,7 +646,7 @@ def run_kspn(args):
                          "pipeline_min_bytes": b_min, "pipeline_frac": (b_min / (ms * 1e-3)) / 1e9 / peak},
             "clocks": clk.summary(),
             "learned_vs_plain": lvp,
-            "rmat26": rmat26,
+            "other_rmat": other,
             "sharded": sharded,
             "autotune": autotune,
             "batched": batched,
@@ -624,7 +657,9 @@ def run_kspn(args):
                        "kernels": {k: {"ms": round(a[0] / prof_steps, 4), "GB/s": round(a[1] / (a[0] * 1e-3) / 1e9, 1) if a[0] else 0}
                                    for k, a in agg.items()}},
         }
-        if not args.no_cpu_baseline and world == 1:
+        if other_cpu is not None:
+            line["cpu_baseline"] = other_cpu
+        elif not args.no_cpu_baseline and world == 1 and args.workload not in CPU_SAMPLE:
             # the reference's kaspan::scc on this very graph (its host copy), one call
             fwh, fwc, bwh, bwc = G.to_host()
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -647,11 +682,15 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="kspn", choices=["kspn", "reference"])
-    ap.add_argument("--workload", default="rmat24", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="rmat26", choices=sorted(WORKLOADS))
     ap.add_argument("--pipeline", default="fast", choices=sorted(PIPELINES), help="fast (default), or the phase order of a reference entry point")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-path and autotuner sections")
-    ap.add_argument("--no-rmat26", action="store_true", help="skip the R-MAT scale-26 section")
+    ap.add_argument("--no-other-rmat", action="store_true", help="skip the other R-MAT configuration's section")
+    ap.add_argument("--reference-seconds", type=float, default=150.0,
+                    help="--impl reference on graphs above 2^29 edges: stop timing calls after this many seconds (at least one call)")
+    ap.add_argument("--batch-graphs", type=int, default=4096, help="graphs of the batch mix (default 4096)")
+    ap.add_argument("--batch-max-log2", type=int, default=18, help="largest graph of the batch mix: 2^this vertices (default 18)")
     ap.add_argument("--profile-steps", type=int, default=None, help="steps run with per-kernel event timing (default min(steps, 3))")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "kspn":

@@ -362,13 +362,25 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
       // trim_1_first, then FW-BW and the trim fixpoint in ONE persistent
       // launch that takes the pivot from device memory: one host sync
       trim_1_first_async(ctx, g, und);
-      if (opt.learned_pivot && ctx->pivot_model) learned_pivot(ctx, g, ctx->pivot_model);
       KSPN_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
+      // with the learned rule the launch first scores the plain pivot (no
+      // extra launch when the model accepts it)
       fw_bw_trim_async(ctx, g, und, scc_id, opt, st, ctx->ev[4]);
       KSPN_CUDA(cudaMemcpyAsync(ctx->h_ctr, ws.ctr, 64 * sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
       KSPN_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
       KSPN_CUDA(cudaEventSynchronize(ctx->ev[3]));
-      resident_result const r  = fw_bw_trim_result(ctx, g, opt, st);
+      resident_result r = fw_bw_trim_result(ctx, g, opt, st);
+      if (r.pivot_rejected) {
+        // the model rejected the plain pivot: score every candidate, then
+        // the resident launch from the model's choice (no second check)
+        learned_pivot(ctx, g, ctx->pivot_model, false);
+        kspn_options o2  = opt;
+        o2.learned_pivot = 0;
+        fw_bw_trim_async(ctx, g, und, scc_id, o2, st, ctx->ev[4]);
+        KSPN_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
+        KSPN_CUDA(cudaEventSynchronize(ctx->ev[3]));
+        r = fw_bw_trim_result(ctx, g, opt, st);
+      }
       uint32_t const        tf = ctx->h_ctr[CTR_DECIDED];
       decided += static_cast<uint64_t>(tf) + r.fwbw_decided + r.trim_decided;
       if (st) {

@@ -477,7 +477,8 @@ run_guarded(kspn_context* ctx, F&& body)
 struct resident_result
 {
   uint32_t pivot = 0, fwbw_decided = 0, trim_decided = 0, trim_levels = 0, und_left = 0;
-  double   fwbw_share = 1.0; // FW-BW's share of the launch's device time
+  double   fwbw_share     = 1.0;   // FW-BW's share of the launch's device time
+  bool     pivot_rejected = false; // the pivot model rejected trim_1_first's pivot: the launch ended after its first level
 };
 bool            resident_fits(dgraph const& g);
 void            fw_bw_trim_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, kspn_options const& opt, kspn_stats* st, cudaEvent_t after_kernel);
@@ -510,7 +511,7 @@ void mlp_features(kspn_context* ctx, dgraph const& g, uint32_t count, uint32_t c
 void mlp_forward(kspn_context* ctx, uint32_t count, float const* feat, float const* params, float* out);
 void mlp_grad(kspn_context* ctx, uint32_t count, float const* feat, float const* y, float const* params, float* grad, float* loss);
 void mlp_adam(kspn_context* ctx, float* params, float const* grad, float* m, float* v, float lr, int step);
-void learned_pivot(kspn_context* ctx, dgraph const& g, float const* params);
+void learned_pivot(kspn_context* ctx, dgraph const& g, float const* params, bool check = true);
 // residual.cu: Tarjan per weakly connected undecided piece that fits a warp's
 // shared memory; returns vertices decided, *pieces_left = pieces left over
 uint32_t residual(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* pieces_left);

@@ -7,24 +7,9 @@
 // (in * out, id) pairs that k_trim_first leaves in ws.pivot (one per 1024
 // vertices).
 //
-// Network: 8 FP32 features -> 32 (ReLU) -> 32 (ReLU) -> 1 (logit of "the
-// vertex lies in the largest SCC").  Weights are kept FP32 for training and
-// rounded to BF16 for every forward pass; all sums accumulate in FP32.  One
-// warp evaluates one sample: lane j owns hidden unit j of both layers.
-//
-// Features of vertex v (raw degrees; the first MLP_SAMPLE neighbours of each
-// row are sampled):
-//   0 log2(1 + out(v)) / 16          1 log2(1 + in(v)) / 16
-//   2 log2(1 + mean out(w), w out-neighbour) / 16
-//   3 log2(1 + mean in(w), w in-neighbour) / 16
-//   4 share of sampled out-neighbours with out(w) = 0 (dead ends)
-//   5 share of sampled in-neighbours with in(w) = 0 (pure sources)
-//   6 log2(1 + mean in(w), w out-neighbour) / 16
-//   7 log2(1 + mean out(w), w in-neighbour) / 16
-//
-// Parameter layout (MLP_PARAMS floats): W1[32][8], b1[32], W2[32][32],
-// b2[32], w3[32], b3.
+// Network, features and parameter layout: mlp.cuh.
 #include "kspn_internal.cuh"
+#include "mlp.cuh"
 #include "prim.cuh"
 
 #include <cuda_bf16.h>
@@ -35,66 +20,7 @@ namespace kspn {
 
 namespace {
 
-constexpr int MLP_IN     = 8;
-constexpr int MLP_H      = 32;
-constexpr int MLP_SAMPLE = 64;
-constexpr int O_W1 = 0, O_B1 = O_W1 + MLP_H * MLP_IN, O_W2 = O_B1 + MLP_H, O_B2 = O_W2 + MLP_H * MLP_H, O_W3 = O_B2 + MLP_H, O_B3 = O_W3 + MLP_H;
-constexpr int MLP_NPARAM = O_B3 + 1;
-static_assert(MLP_NPARAM == KSPN_MLP_PARAMS, "parameter count");
 constexpr int MLP_WARPS = 8; // warps per block of the MLP kernels
-
-__device__ __forceinline__ float
-log2p(float x)
-{
-  return log2f(1.0f + x);
-}
-
-// Features of v into f[0..8) (all lanes of the warp call it; every lane
-// gets the same values).
-__device__ __forceinline__ void
-mlp_features(uint32_t v, uint64_t const* __restrict__ fh, uint32_t const* __restrict__ fc, uint64_t const* __restrict__ bh, uint32_t const* __restrict__ bc, float (&f)[MLP_IN])
-{
-  unsigned const lane = threadIdx.x & 31u;
-  uint64_t const ob = fh[v], oe = fh[v + 1], ib = bh[v], ie = bh[v + 1];
-  float          so_out = 0, so_in = 0, si_in = 0, si_out = 0, sinks = 0, srcs = 0;
-  uint32_t const no = static_cast<uint32_t>(oe - ob < MLP_SAMPLE ? oe - ob : MLP_SAMPLE);
-  uint32_t const ni = static_cast<uint32_t>(ie - ib < MLP_SAMPLE ? ie - ib : MLP_SAMPLE);
-  for (uint32_t k = lane; k < no; k += 32) {
-    uint32_t const w  = fc[ob + k];
-    float const    ow = static_cast<float>(fh[w + 1] - fh[w]);
-    float const    iw = static_cast<float>(bh[w + 1] - bh[w]);
-    so_out += ow;
-    so_in += iw;
-    sinks += ow == 0.f ? 1.f : 0.f;
-  }
-  for (uint32_t k = lane; k < ni; k += 32) {
-    uint32_t const w  = bc[ib + k];
-    float const    ow = static_cast<float>(fh[w + 1] - fh[w]);
-    float const    iw = static_cast<float>(bh[w + 1] - bh[w]);
-    si_in += iw;
-    si_out += ow;
-    srcs += iw == 0.f ? 1.f : 0.f;
-  }
-#pragma unroll
-  for (int sh = 16; sh; sh >>= 1) {
-    so_out += __shfl_xor_sync(0xFFFFFFFFu, so_out, sh);
-    so_in += __shfl_xor_sync(0xFFFFFFFFu, so_in, sh);
-    si_in += __shfl_xor_sync(0xFFFFFFFFu, si_in, sh);
-    si_out += __shfl_xor_sync(0xFFFFFFFFu, si_out, sh);
-    sinks += __shfl_xor_sync(0xFFFFFFFFu, sinks, sh);
-    srcs += __shfl_xor_sync(0xFFFFFFFFu, srcs, sh);
-  }
-  float const inv_o = no ? 1.f / static_cast<float>(no) : 0.f;
-  float const inv_i = ni ? 1.f / static_cast<float>(ni) : 0.f;
-  f[0]              = log2p(static_cast<float>(oe - ob)) * (1.f / 16);
-  f[1]              = log2p(static_cast<float>(ie - ib)) * (1.f / 16);
-  f[2]              = log2p(so_out * inv_o) * (1.f / 16);
-  f[3]              = log2p(si_in * inv_i) * (1.f / 16);
-  f[4]              = sinks * inv_o;
-  f[5]              = srcs * inv_i;
-  f[6]              = log2p(so_in * inv_o) * (1.f / 16);
-  f[7]              = log2p(si_out * inv_i) * (1.f / 16);
-}
 
 // BF16-rounded weights of a block, in shared memory.
 struct mlp_smem
@@ -109,24 +35,10 @@ mlp_load(mlp_smem& s, float const* __restrict__ params)
   __syncthreads();
 }
 
-// Forward pass of one sample by one warp: returns the logit (all lanes);
-// h1, h2 = this lane's hidden units.
 __device__ __forceinline__ float
 mlp_forward(mlp_smem const& s, float const (&x)[MLP_IN], float& h1, float& h2)
 {
-  unsigned const lane = threadIdx.x & 31u;
-  float          a    = s.w[O_B1 + lane];
-#pragma unroll
-  for (int k = 0; k < MLP_IN; ++k) a += s.w[O_W1 + lane * MLP_IN + k] * x[k];
-  h1      = a > 0.f ? a : 0.f;
-  float b = s.w[O_B2 + lane];
-#pragma unroll
-  for (int i = 0; i < MLP_H; ++i) b += s.w[O_W2 + lane * MLP_H + i] * __shfl_sync(0xFFFFFFFFu, h1, i);
-  h2      = b > 0.f ? b : 0.f;
-  float z = s.w[O_W3 + lane] * h2;
-#pragma unroll
-  for (int sh = 16; sh; sh >>= 1) z += __shfl_xor_sync(0xFFFFFFFFu, z, sh);
-  return z + s.w[O_B3];
+  return mlp_forward_w(mlp_weights_smem{ s.w }, x, h1, h2);
 }
 
 // ordered key of a float (larger float -> larger unsigned)
@@ -360,9 +272,12 @@ mlp_adam(kspn_context* ctx, float* params, float const* grad, float* m, float* v
 }
 
 // Rewrites the pivot slot that k_trim_first filled (trim_1_first_async)
-// with the model's choice among its per-block candidates.
+// with the model's choice among its per-block candidates.  With check, the
+// plain pivot in the slot is scored first and kept if the model accepts it;
+// without, every candidate is scored (the resident launch has already
+// scored the plain pivot and rejected it).
 void
-learned_pivot(kspn_context* ctx, dgraph const& g, float const* params)
+learned_pivot(kspn_context* ctx, dgraph const& g, float const* params, bool check)
 {
   auto&          ws   = ctx->ws;
   unsigned const nb   = pivot_candidates(g.n);
@@ -370,11 +285,14 @@ learned_pivot(kspn_context* ctx, dgraph const& g, float const* params)
   auto*          done = reinterpret_cast<uint32_t*>(ws.ctr64 + 15);
   KSPN_CUDA(cudaMemsetAsync(best, 0, 2 * sizeof(unsigned long long), ctx->stream));
   uint32_t const* ids = reinterpret_cast<uint32_t const*>(ws.pivot + 4096);
-  k_pivot_check<<<1, 32, 0, ctx->stream>>>(ws.pivot + PV_FINAL, ids + PV_FINAL, g.n, g.fh, g.fc, g.bh, g.bc, params, done);
+  if (check) {
+    k_pivot_check<<<1, 32, 0, ctx->stream>>>(ws.pivot + PV_FINAL, ids + PV_FINAL, g.n, g.fh, g.fc, g.bh, g.bc, params, done);
+    ctx->launches += 1;
+  }
   k_pivot_score<<<mlp_grid(nb), MLP_WARPS * 32, 0, ctx->stream>>>(nb, ws.pivot, ids, g.n, g.fh, g.fc, g.bh, g.bc, params, best, done);
   k_pivot_pick<<<1, 1, 0, ctx->stream>>>(best, ws.pivot + PV_FINAL, reinterpret_cast<uint32_t*>(ws.pivot + 4096) + PV_FINAL, done);
   KSPN_CHECK_LAUNCH();
-  ctx->launches += 3;
+  ctx->launches += 2;
 }
 
 } // namespace kspn

@@ -31,6 +31,7 @@
 // advance kernels, control in reach_state) with CUDA events around the
 // expansion kernels.
 #include "expand.cuh"
+#include "mlp.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -109,6 +110,7 @@ struct reach_state
   uint32_t           heavy_err;    // a heavy or cut list would have overflowed
   uint32_t           trim_async;   // the trim tail finished on the worklist
   uint32_t           restricts;    // passes that cut one search's candidates down to the other's set
+  uint32_t           pivot_rejected; // the pivot model rejected the launch's pivot: the launch ended after its first level
 };
 
 // phase stamps live after the state: uint32 phase[128], uint64 ns[128]
@@ -679,6 +681,7 @@ struct fwbw_args
   uint32_t           wait_limit;   // polls before a wait gives up
   uint32_t           drop_barrier; // test hook: the last block leaves this barrier of the launch (0 = off)
   uint64_t           aw_exact;     // worklist items after which warps take their finds exactly
+  float const*       model;        // pivot MLP parameters: the launch scores its pivot first (null: no check)
 };
 
 __device__ __forceinline__ bool
@@ -860,9 +863,10 @@ warp_push_active64(uint32_t v, uint32_t* q, unsigned long long* count, uint64_t 
 // (or a worklist wait) gave up.
 enum : int
 {
-  SEARCH_DONE   = 0,
-  SEARCH_CAPPED = 1,
-  SEARCH_FAILED = 2
+  SEARCH_DONE     = 0,
+  SEARCH_CAPPED   = 1,
+  SEARCH_FAILED   = 2,
+  SEARCH_REJECTED = 3 // the pivot model rejected the pivot: the launch ended after its first level
 };
 
 // ---------------------------------------------------------------- asynchronous tail
@@ -1343,6 +1347,17 @@ run_joint(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uin
       if (tally) st->async_phases += 1;
       continue;
     }
+    if (glvl == 0 && a.model && blockIdx.x == gridDim.x - 1 && threadIdx.x < 32) {
+      // the pivot model scores the pivot during the first level, in the
+      // grid's last block (which expands nothing there unless the pivot's
+      // rows span the grid): the learned rule keeps the plain pivot when
+      // the model accepts it; a rejection ends the launch at this level's
+      // barrier and the host scores every candidate
+      float f[MLP_IN], h1, h2;
+      mlp_features(pivot, a.fh, a.fc, a.bh, a.bc, f);
+      float const z = mlp_forward_w(mlp_weights_global{ a.model }, f, h1, h2);
+      if (threadIdx.x == 0 && !(z >= 0.f)) st->pivot_rejected = 1;
+    }
     // ---- the level's steps
     if (s_j.any_td || s_j.kind[0] == JK_FIXUP || s_j.kind[1] == JK_FIXUP) {
       uint32_t ntl[2] = { 0, 0 }, parts[2] = { 1, 1 }, units[2] = { 0, 0 };
@@ -1434,6 +1449,7 @@ run_joint(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uin
       if (tally) st->bu_bitmap += (c0 ? 1u : 0u) + (c1 ? 1u : 0u);
     }
     if (!gsync(a, epoch)) return SEARCH_FAILED;
+    if (glvl == 0 && a.model && __ldcg(&st->pivot_rejected)) return SEARCH_REJECTED;
     stamp(a, s_j.any_td ? 4u : (s_j.any_bu ? 5u : 14u));
     if (threadIdx.x == 0) {
       for (int d = 0; d < 2; ++d) {
@@ -1481,11 +1497,8 @@ run_joint(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uin
       atomicAnd(s_bu_cut[d].map + (v >> 5), ~(1u << (v & 31)));
     }
   }
-  if (rc == SEARCH_DONE) {
-    // the SCC: FW(p) & BW(p)
-    for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) a.vis_b[w] = __ldcg(a.vis_b + w) & __ldcg(a.vis_a + w);
-    if (!gsync(a, epoch)) return SEARCH_FAILED;
-  }
+  // the SCC is FW(p) & BW(p): the min-id search and the finalize pass read
+  // both bitmaps, and the finalize pass leaves the intersection in vis_b
   return rc;
 }
 
@@ -1984,6 +1997,7 @@ k_fwbw(fwbw_args a)
     st->async_phases            = 0;
     st->cut_n[0] = st->cut_n[1] = st->fixups = 0;
     st->hseed_n = st->heavy_err = st->trim_async = st->joint = st->restricts = 0;
+    st->pivot_rejected = 0;
     for (int i = 0; i < 6; ++i) st->hq_n[i] = 0;
     if (search) a.seed.q[0] = p, a.seed.prefix[0] = 0;
   }
@@ -2015,7 +2029,7 @@ k_fwbw(fwbw_args a)
       rc = run_joint(a, sm, p, n_und, glvl, epoch);
     }
     if (rc == SEARCH_DONE && a.min_ids) {
-      // smallest member = first set bit of vis_b.  Every block first looks
+      // smallest member = first set bit of vis_a & vis_b.  Every block first looks
       // at the same leading MIN_WORDS words (the SCC is usually dense
       // there); only when they are all empty does the grid search the rest
       // and meet at a barrier.  Every block reads the same words, so all
@@ -2023,7 +2037,7 @@ k_fwbw(fwbw_args a)
       constexpr uint32_t MIN_WORDS = 4 * R_THREADS;
       uint32_t           best      = UNDECIDED;
       for (uint32_t w = threadIdx.x; w < MIN_WORDS && w < words; w += R_THREADS) {
-        uint32_t const s = __ldcg(a.vis_b + w);
+        uint32_t const s = __ldcg(a.vis_b + w) & __ldcg(a.vis_a + w);
         if (s) {
           best = w * 32 + (__ffs(s) - 1);
           break;
@@ -2037,7 +2051,7 @@ k_fwbw(fwbw_args a)
       id = sm.cnt;
       if (id == UNDECIDED) {
         for (uint32_t w = MIN_WORDS + blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) {
-          uint32_t const s = __ldcg(a.vis_b + w);
+          uint32_t const s = __ldcg(a.vis_b + w) & __ldcg(a.vis_a + w);
           if (s) {
             best = w * 32 + (__ffs(s) - 1);
             break; // later words of this thread only hold larger ids
@@ -2059,8 +2073,10 @@ k_fwbw(fwbw_args a)
       uint32_t* const list = a.fb[glvl & 1].q; // trim: the undecided vertices
       for (uint32_t wb = (blockIdx.x * R_THREADS + threadIdx.x) & ~31u; wb < words; wb += gridDim.x * R_THREADS) {
         uint32_t const w    = wb + lane;
-        uint32_t const mine = w < words ? __ldcg(a.vis_b + w) : 0u;
+        uint32_t const vb   = w < words ? __ldcg(a.vis_b + w) : 0u;
+        uint32_t const mine = vb & (w < words ? __ldcg(a.vis_a + w) : 0u); // the SCC: FW & BW
         uint32_t       u    = 0;
+        if (mine != vb) a.vis_b[w] = mine; // the ids pass reads the SCC from vis_b
         if (w < words && (mine || a.trim)) {
           u = __ldcg(a.und + w) & ~mine;
           if (mine) a.und[w] = u;
@@ -2296,7 +2312,7 @@ namespace {
 // caller synchronises, then calls check_persistent.
 void
 launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t pivot, bool trim, kspn_options const& opt, kspn_stats* st, bool min_ids,
-                  cudaEvent_t after_kernel = nullptr, bool ids_at_end = true)
+                  cudaEvent_t after_kernel = nullptr, bool ids_at_end = true, float const* model = nullptr)
 {
   auto&       ws   = ctx->ws;
   auto* const rs   = reinterpret_cast<reach_state*>(ws.rstate);
@@ -2352,6 +2368,7 @@ launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* s
   a.drop_barrier = opt.drop_barrier;
   // an earlier switch only cuts duplicates; a later one could overrun the worklist's bound
   a.aw_exact     = opt.aw_exact_after && opt.aw_exact_after < ws.aw_entries / 2 ? opt.aw_exact_after : ws.aw_entries / 2;
+  a.model        = model;
   void* args[]  = { &a };
   KSPN_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(&k_fwbw), dim3(fwbw_grid(ctx)), dim3(R_THREADS), args, 0, ctx->stream));
   ctx->launches += 1;
@@ -2414,7 +2431,9 @@ resident_fits(dgraph const& g)
 void
 fw_bw_trim_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, kspn_options const& opt, kspn_stats* st, cudaEvent_t after_kernel)
 {
-  launch_persistent(ctx, g, und, scc_id, static_cast<uint32_t>(PIVOT_FROM_DEVICE), true, opt, st, true, after_kernel);
+  // with the learned rule the launch scores trim_1_first's pivot itself
+  float const* model = opt.learned_pivot && ctx->pivot_model ? ctx->pivot_model : nullptr;
+  launch_persistent(ctx, g, und, scc_id, static_cast<uint32_t>(PIVOT_FROM_DEVICE), true, opt, st, true, after_kernel, true, model);
 }
 
 resident_result
@@ -2431,12 +2450,12 @@ fw_bw_trim_result(kspn_context* ctx, dgraph const& g, kspn_options const& opt, k
     // rows of every listed and every queued vertex); neighbour ids read;
     // bitmap passes -- init (und read, three bitmaps written), two per
     // bitmap sweep (avail, fresh), one per frontier built from fresh,
-    // the SCC as FW & BW (both read, one written), a restriction of one
-    // search to the other's set (two read), finalize (vis_b, und read +
-    // written, snap), ids (und, vis_b) -- and the ids written
+    // a restriction of one search to the other's set (two read), finalize
+    // (vis_a and vis_b read, und read + written, snap), ids (und, vis_b) --
+    // and the ids written
     uint64_t const rows   = hs->cands_bu + hs->rows_td + hs->pushed_td + 2 * (hs->list_n + hs->trim_decided);
     uint64_t const edges  = hs->edges_td + hs->edges_bu + hs->trim_edges;
-    uint32_t const passes = hs->pivot_used < g.n ? 4 + 2 * hs->bu_bitmap + hs->mats + 3 + 2 * hs->restricts + 4 + 2 : 1;
+    uint32_t const passes = hs->pivot_used < g.n ? 4 + 2 * hs->bu_bitmap + hs->mats + 2 * hs->restricts + 5 + 2 : 1;
     st->resident_rows          = rows;
     st->resident_edges         = edges;
     st->resident_bitmap_passes = passes;
@@ -2449,6 +2468,7 @@ fw_bw_trim_result(kspn_context* ctx, dgraph const& g, kspn_options const& opt, k
     st->search_worklist        = hs->async_phases ? 1u : 0u;
   }
   resident_result r;
+  r.pivot_rejected    = hs->pivot_rejected != 0;
   r.pivot             = hs->pivot_used;
   r.fwbw_decided      = hs->decided;
   r.trim_decided      = hs->trim_decided;

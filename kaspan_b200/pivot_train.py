@@ -8,9 +8,15 @@ b = c = (1 - a - .05) / 2, seeds 1000..1063; every second one carries
 decoy hubs (a vertex with `fan` in-edges from random vertices and `fan`
 out-edges to fresh dead ends, `fan` sized so that its in * out beats every
 real vertex, while its SCC is itself).  Labels come from plain runs of the FAST
-pipeline: 1 when the vertex lies in the largest SCC.  Samples: the 1024
-vertices with the largest in * out, plus the decoys.  Loss: mean binary
-cross-entropy; optimiser: Adam (kspn_mlp_gradient / kspn_mlp_adam).
+pipeline and are soft: log2(1 + |SCC(v)|) / log2(1 + |largest SCC|), 1 in
+the largest SCC, near 0 for a singleton -- a pivot is worth the share of
+the graph its FW-BW round decides, so a vertex of a large SCC that is not
+the largest is not taught as a miss.  The logit's sign is the decision: a
+vertex is accepted where the model predicts a label of at least 1/2 (an
+SCC of about the square root of the largest one or more).  Samples: the
+1024 vertices with the largest in * out, plus the decoys.  Loss: mean
+binary cross-entropy against the soft labels (its floor is the labels'
+mean binary entropy); optimiser: Adam (kspn_mlp_gradient / kspn_mlp_adam).
 """
 from __future__ import annotations
 
@@ -65,15 +71,24 @@ def decoy_rmat(ctx: Context, scale: int, seed: int, a: float, decoys: int = 0, f
     return KG.from_edges(ctx, n, src, dst), hubs
 
 
-def largest_scc_labels(ctx: Context, G) -> "torch.Tensor":
-    """1.0 where the vertex lies in the largest SCC (plain FAST run)."""
+def scc_size_labels(ctx: Context, G) -> "torch.Tensor":
+    """log2(1 + |SCC(v)|) / log2(1 + |largest SCC|) per vertex (plain FAST
+    run): 1.0 in the largest SCC."""
     import torch
 
     out = torch.empty(G.n, dtype=torch.int32, device="cuda")
     ctx.scc_device(G.n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, out, default_options(pipeline=PIPELINE_FAST))
     ids = out.long()
-    big = torch.bincount(ids, minlength=G.n).argmax()
-    return (ids == big).float()
+    size = torch.bincount(ids, minlength=G.n).double()
+    return (torch.log2(1.0 + size[ids]) / torch.log2(1.0 + size.max())).float()
+
+
+def label_entropy(Y) -> float:
+    """Mean binary entropy of soft labels (nats): the BCE loss's floor."""
+    import torch
+
+    y = Y.double().clamp(1e-12, 1 - 1e-12)
+    return float((-(y * torch.log(y) + (1 - y) * torch.log(1 - y))).mean().item())
 
 
 def candidates(G, k: int = 1024, extra=None):
@@ -100,7 +115,7 @@ def features(ctx: Context, G, verts):
 def samples(ctx: Context, G, hubs, k: int = 1024):
     import torch
 
-    y = largest_scc_labels(ctx, G)
+    y = scc_size_labels(ctx, G)
     c = candidates(G, k, hubs)
     return features(ctx, G, c), y[c.long()].contiguous()
 
@@ -167,7 +182,8 @@ def main():
         X, Y = training_set(ctx, args.graphs, args.scale)
         params, losses = train(ctx, X, Y, steps=args.steps)
     np.save(args.out, params)
-    print(f"{len(Y)} samples ({int(Y.sum().item())} in a largest SCC); loss {losses[0][1]:.4f} -> {losses[-1][1]:.4f}; wrote {args.out}")
+    print(f"{len(Y)} samples ({int((Y == 1).sum().item())} in a largest SCC); loss {losses[0][1]:.4f} -> {losses[-1][1]:.4f} "
+          f"(floor {label_entropy(Y):.4f}); wrote {args.out}")
 
 
 if __name__ == "__main__":

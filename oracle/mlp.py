@@ -34,13 +34,14 @@ def unpack(params: np.ndarray):
 
 
 def features(fwh, fwc, bwh, bwc, vertices) -> np.ndarray:
-    """The eight features of each vertex (kaspan_b200/csrc/mlp.cu header)."""
+    """The eight features of each vertex (kaspan_b200/csrc/mlp.cuh header)."""
     fwh = fwh.astype(np.int64)
     bwh = bwh.astype(np.int64)
     out_deg = np.diff(fwh)
     in_deg = np.diff(bwh)
     F = np.zeros((len(vertices), IN), np.float64)
     lg = lambda x: np.log2(1.0 + x) / 16.0  # noqa: E731
+    live = (out_deg > 0) & (in_deg > 0)  # survives trim round 1 (trim_1_local.hpp:12-46)
     for r, v in enumerate(vertices):
         on = fwc[fwh[v]: fwh[v] + min(out_deg[v], SAMPLE)].astype(np.int64)
         inn = bwc[bwh[v]: bwh[v] + min(in_deg[v], SAMPLE)].astype(np.int64)
@@ -48,9 +49,17 @@ def features(fwh, fwc, bwh, bwc, vertices) -> np.ndarray:
         F[r, 1] = lg(in_deg[v])
         F[r, 2] = lg(out_deg[on].mean()) if len(on) else 0.0
         F[r, 3] = lg(in_deg[inn].mean()) if len(inn) else 0.0
-        F[r, 4] = (out_deg[on] == 0).mean() if len(on) else 0.0
-        F[r, 5] = (in_deg[inn] == 0).mean() if len(inn) else 0.0
-        F[r, 6] = lg(in_deg[on].mean()) if len(on) else 0.0
+        F[r, 4] = live[on].mean() if len(on) else 0.0
+        F[r, 5] = live[inn].mean() if len(inn) else 0.0
+        # the trim round that removes v, judged from its samples: 1 (a
+        # degree is 0), 2 (no sampled out- or in-neighbour survives round 1),
+        # later or never
+        if not len(on) or not len(inn):
+            F[r, 6] = 0.0
+        elif not live[on].any() or not live[inn].any():
+            F[r, 6] = 0.5
+        else:
+            F[r, 6] = 1.0
         F[r, 7] = lg(out_deg[inn].mean()) if len(inn) else 0.0
     return F
 

@@ -7,6 +7,7 @@ exchange is a host collective between launches).  Between GPUs the same
 loop runs its exchanges over NCCL."""
 from __future__ import annotations
 
+import datetime
 import os
 import socket
 
@@ -56,7 +57,7 @@ def test_sharded_one_rank(ctx, name):
 
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(_free_port())
-    dist.init_process_group("gloo", rank=0, world_size=1)
+    dist.init_process_group("gloo", rank=0, world_size=1, timeout=datetime.timedelta(seconds=90))
     try:
         G = GRAPHS[name]()
         lo, ids, st = _run_rank(ctx, G, 0, 1)
@@ -75,7 +76,7 @@ def _rank_main(rank, world, port, name, q):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     torch.cuda.set_device(0)
-    dist.init_process_group("gloo", rank=rank, world_size=world)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=90))
     try:
         with K.Context(0) as ctx:
             G = GRAPHS[name]()
@@ -92,13 +93,19 @@ def test_sharded_two_ranks_one_gpu(name):
     c = mp.get_context("spawn")
     q = c.Queue()
     port = _free_port()
-    procs = [c.Process(target=_rank_main, args=(r, 2, port, name, q)) for r in range(2)]
+    procs = [c.Process(target=_rank_main, args=(r, 2, port, name, q), daemon=True) for r in range(2)]
     for p in procs:
         p.start()
-    got = [q.get(timeout=300) for _ in range(2)]
-    for p in procs:
-        p.join(timeout=120)
-        assert p.exitcode == 0
+    try:
+        got = [q.get(timeout=240) for _ in range(2)]
+        for p in procs:
+            p.join(timeout=120)
+            assert p.exitcode == 0
+    finally:
+        for p in procs:
+            if p.is_alive():
+                p.terminate()
+                p.join(timeout=30)
     G = GRAPHS[name]()
     ids = np.full(G.n, 0xFFFFFFFF, np.uint32)
     for rank, lo, part, exchanged, rounds in got:

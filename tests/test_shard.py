@@ -9,6 +9,7 @@ the whole graph.  The GPU test (test_gpu_shard.py) runs the same loop with
 the CUDA steps."""
 from __future__ import annotations
 
+import datetime
 import os
 import socket
 
@@ -159,7 +160,7 @@ def _rank_main(rank, world, port, name, q):
 
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
-    dist.init_process_group("gloo", rank=rank, world_size=world)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=90))
     try:
         G = _graphs()[name] or kat_graph()
         bounds = SH.partition_bounds(G.n, G.fwh, world, align=64)
@@ -188,13 +189,19 @@ def test_sharded_loop_matches_tarjan(world, name):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, world, port, name, q)) for r in range(world)]
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, name, q), daemon=True) for r in range(world)]
     for p in procs:
         p.start()
-    got = [q.get(timeout=240) for _ in range(world)]
-    for p in procs:
-        p.join(timeout=60)
-        assert p.exitcode == 0
+    try:
+        got = [q.get(timeout=240) for _ in range(world)]
+        for p in procs:
+            p.join(timeout=60)
+            assert p.exitcode == 0
+    finally:
+        for p in procs:
+            if p.is_alive():
+                p.terminate()
+                p.join(timeout=30)
     from kspn_testlib import kat_graph
 
     G = _graphs()[name] or kat_graph()
