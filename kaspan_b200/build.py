@@ -66,7 +66,7 @@ def build_cli(force: bool = False) -> str:
     """The bench_kaspan-compatible command line (links libkspn.so)."""
     if not force and os.path.exists(CLI) and os.path.getmtime(CLI) > max(os.path.getmtime(CLI_SRC), os.path.getmtime(LIB)):
         return CLI
-    cmd = [_nvcc(), "-O2", "-std=c++20", "-I", INCLUDE, CLI_SRC, "-o", CLI + ".tmp", "-L", HERE, "-lkspn", "-Xlinker", "-rpath,$ORIGIN", "-cudart", "static"]
+    cmd = [_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-std=c++20", "-I", INCLUDE, CLI_SRC, "-o", CLI + ".tmp", "-L", HERE, "-lkspn", "-Xlinker", "-rpath,$ORIGIN", "-cudart", "static"]
     subprocess.run(cmd, check=True)
     os.replace(CLI + ".tmp", CLI)
     return CLI

@@ -370,6 +370,11 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
       KSPN_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
       KSPN_CUDA(cudaEventSynchronize(ctx->ev[3]));
       resident_result r = fw_bw_trim_result(ctx, g, opt, st);
+      if (r.resumed) {
+        // the phase clock's end after the resume launch
+        KSPN_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
+        KSPN_CUDA(cudaEventSynchronize(ctx->ev[3]));
+      }
       if (r.pivot_rejected) {
         // the model rejected the plain pivot: score every candidate, then
         // the resident launch from the model's choice (no second check)
@@ -380,6 +385,10 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
         KSPN_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
         KSPN_CUDA(cudaEventSynchronize(ctx->ev[3]));
         r = fw_bw_trim_result(ctx, g, opt, st);
+        if (r.resumed) {
+          KSPN_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
+          KSPN_CUDA(cudaEventSynchronize(ctx->ev[3]));
+        }
       }
       uint32_t const        tf = ctx->h_ctr[CTR_DECIDED];
       decided += static_cast<uint64_t>(tf) + r.fwbw_decided + r.trim_decided;

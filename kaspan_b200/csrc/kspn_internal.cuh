@@ -408,6 +408,10 @@ struct kspn_context
   cudaEvent_t        pe[4]      = {};
   void*              h_state    = nullptr; // pinned 4 KiB mirror of ws.rstate
   unsigned           search_grid = 0;      // blocks of the persistent FW-BW launch
+  unsigned           resume_grid = 0;      // blocks of its resume launch (the worklist phase)
+  unsigned           bar_grid    = 0;      // grid of the last launch on the workspace's grid barrier
+  alignas(16) unsigned char fwbw_last[1024] = {}; // arguments of the last persistent FW-BW launch (a resume launch reuses them)
+  cudaEvent_t        fwbw_after  = nullptr; // event the last launch records after its kernel (re-recorded after a resume)
   float*             pivot_model = nullptr; // device copy of the pivot MLP (kspn_set_pivot_model)
   kspn::cached_graph trim;                 // one-launch trim fixpoint graph
   kspn::batch_cache* batch      = nullptr;  // batched path (kspn_scc_batched)
@@ -478,7 +482,8 @@ struct resident_result
 {
   uint32_t pivot = 0, fwbw_decided = 0, trim_decided = 0, trim_levels = 0, und_left = 0;
   double   fwbw_share     = 1.0;   // FW-BW's share of the launch's device time
-  bool     pivot_rejected = false; // the pivot model rejected trim_1_first's pivot: the launch ended after its first level
+  bool     pivot_rejected = false;
+  bool     resumed        = false; // the worklist phase ran in a resume launch (after one more host round trip) // the pivot model rejected trim_1_first's pivot: the launch ended after its first level
 };
 bool            resident_fits(dgraph const& g);
 void            fw_bw_trim_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, kspn_options const& opt, kspn_stats* st, cudaEvent_t after_kernel);

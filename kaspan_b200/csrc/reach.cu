@@ -111,6 +111,7 @@ struct reach_state
   uint32_t           trim_async;   // the trim tail finished on the worklist
   uint32_t           restricts;    // passes that cut one search's candidates down to the other's set
   uint32_t           pivot_rejected; // the pivot model rejected the launch's pivot: the launch ended after its first level
+  uint32_t           handoff;        // the launch ended where its worklist phase starts; a resume launch continues
 };
 
 // phase stamps live after the state: uint32 phase[128], uint64 ns[128]
@@ -247,11 +248,18 @@ struct take_op
 // already in mark.
 constexpr int BU_WARPS = R_THREADS / 32;
 
+// Sparse sweeps hand a warp up to BU_GROUP consecutive chunks at once, so
+// that their few candidates share the dependent head -> neighbour -> probe
+// chains instead of paying one chain per chunk; a group is sized for about
+// BU_GROUP_CANDS candidates.
+constexpr int      BU_GROUP       = 8;
+constexpr uint32_t BU_GROUP_CANDS = 256;
+
 // Per-warp shared memory of the sweep.
 struct bu_warp_smem
 {
-  uint16_t cand[32 * 32]; // the warp's chunk (32 words = 1024 vertices) packed, as offsets in the chunk
-  uint32_t found[32];     // found bits per word of the chunk
+  uint16_t cand[32 * 32];       // the warp's chunk (32 words = 1024 vertices) or group packed, as offsets from its first vertex
+  uint32_t found[32 * BU_GROUP]; // found bits per word of the chunk or group
 };
 
 // Rows cut short in bottom-up sweeps: a row the warp has walked HEAVY_ROW
@@ -419,6 +427,115 @@ bu_sweep_chunk(uint32_t c,
   }
   nfound += __popc(fnd);
   __syncwarp();
+}
+
+// Bottom-up sweep of the cnt <= BU_GROUP consecutive chunks [c0, c0 + cnt)
+// by one warp (cnt = 1 on dense levels): lane i loads word i of every chunk
+// (independent loads); the chunks are then taken in segments of at most
+// 32 x 32 candidates (the pack buffer), each packed once and walked in
+// batches of 32 x BU_ILP as bu_rows does, after which lane i writes back
+// word i of each chunk of the segment.  On a sparse level one segment holds
+// the whole group, so its few candidates share one dependent head ->
+// neighbour -> probe chain instead of one chain per chunk.
+__device__ __forceinline__ void
+bu_sweep_group(uint32_t c0,
+               uint32_t cnt,
+               uint32_t n,
+               uint64_t const* __restrict__ head,
+               uint32_t const* __restrict__ adj,
+               uint32_t* avail,
+               uint32_t* mark,
+               uint32_t* fresh,
+               bu_cut const& cut,
+               bu_warp_smem& sm,
+               uint32_t& nfound,
+               uint64_t& nedge,
+               uint64_t& ncand)
+{
+  unsigned const lane  = threadIdx.x & 31u;
+  uint32_t const words = (n + 31) / 32;
+  // the chunks' words wait in the lane's own slots of `found` until their
+  // segment is packed (no register array across the scans)
+#pragma unroll
+  for (int g = 0; g < BU_GROUP; ++g) {
+    uint32_t const w = (c0 + g) * 32 + lane;
+    uint32_t       x = static_cast<uint32_t>(g) < cnt && w < words ? __ldcg(avail + w) : 0u;
+    if (w == words - 1 && (n & 31)) x &= (1u << (n & 31)) - 1u;
+    sm.found[g * 32 + lane] = x;
+  }
+  for (uint32_t s0 = 0; s0 < cnt;) {
+    // the segment [s0, s1): whole chunks while the pack buffer holds them
+    // (warp-uniform; a chunk alone always fits)
+    uint32_t s1 = s0, total = 0;
+    while (s1 < cnt) {
+      uint32_t const t = __reduce_add_sync(0xFFFFFFFFu, static_cast<uint32_t>(__popc(sm.found[s1 * 32 + lane])));
+      if (s1 > s0 && total + t > 32 * 32) break;
+      total += t;
+      ++s1;
+    }
+    uint32_t cl = 0;
+    for (uint32_t g = s0; g < s1; ++g) cl += __popc(sm.found[g * 32 + lane]);
+    uint32_t pos = cl;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, pos, d);
+      if (lane >= static_cast<unsigned>(d)) pos += y;
+    }
+    pos -= cl;
+    for (uint32_t g = s0; g < s1; ++g) {
+      uint32_t word = sm.found[g * 32 + lane];
+      while (word) {
+        uint32_t const bb = __ffs(word) - 1;
+        word &= word - 1;
+        sm.cand[pos++] = static_cast<uint16_t>((g - s0) * 1024 + lane * 32 + bb);
+      }
+      sm.found[g * 32 + lane] = 0;
+    }
+    __syncwarp();
+    ncand += lane == 0 ? total : 0;
+    uint32_t const vbase = (c0 + s0) * 1024;
+    for (uint32_t r = 0; r < total; r += 32 * BU_ILP) {
+      uint32_t v[BU_ILP];
+      bool     live[BU_ILP], found[BU_ILP];
+#pragma unroll
+      for (int k = 0; k < BU_ILP; ++k) {
+        uint32_t const i = r + k * 32 + lane;
+        live[k]          = i < total;
+        v[k]             = live[k] ? vbase + sm.cand[i] : 0u;
+      }
+      bu_rows(v, live, found, head, adj, mark, cut, nedge);
+#pragma unroll
+      for (int k = 0; k < BU_ILP; ++k)
+        if (found[k]) atomicOr(&sm.found[(v[k] >> 5) - c0 * 32], 1u << (v[k] & 31));
+    }
+    __syncwarp();
+    for (uint32_t g = s0; g < s1; ++g) {
+      uint32_t const w   = (c0 + g) * 32 + lane;
+      uint32_t const fnd = sm.found[g * 32 + lane];
+      if (w < words) {
+        if (fnd) {
+          atomicAnd(avail + w, ~fnd);
+          atomicOr(mark + w, fnd);
+        }
+        fresh[w] = fnd;
+      }
+      nfound += __popc(fnd);
+    }
+    __syncwarp();
+    s0 = s1;
+  }
+}
+
+// Chunks per sweep group for a bottom-up level over `cand` candidates of n
+// vertices (1: dense, chunk by chunk): the largest power of two up to
+// BU_GROUP whose expected candidates stay within BU_GROUP_CANDS.
+__device__ __forceinline__ uint32_t
+bu_group_size(uint64_t cand, uint32_t n)
+{
+  uint64_t const per_chunk = n ? cand * 1024 / n : 0;
+  uint32_t       g         = 1;
+  while (g < BU_GROUP && per_chunk * 2 * g <= BU_GROUP_CANDS) g *= 2;
+  return g;
 }
 
 // Frontier queue from `fresh` (when a search returns to top-down after
@@ -682,6 +799,9 @@ struct fwbw_args
   uint32_t           drop_barrier; // test hook: the last block leaves this barrier of the launch (0 = off)
   uint64_t           aw_exact;     // worklist items after which warps take their finds exactly
   float const*       model;        // pivot MLP parameters: the launch scores its pivot first (null: no check)
+  void*              jsave;        // the level loop's saved control (handoff, resume)
+  uint32_t           handoff;      // 1: end the launch where the worklist phase would start (SEARCH_HANDOFF)
+  uint32_t           resume;       // 1: continue a launch that handed off, at its worklist phase
 };
 
 __device__ __forceinline__ bool
@@ -866,7 +986,8 @@ enum : int
   SEARCH_DONE     = 0,
   SEARCH_CAPPED   = 1,
   SEARCH_FAILED   = 2,
-  SEARCH_REJECTED = 3 // the pivot model rejected the pivot: the launch ended after its first level
+  SEARCH_REJECTED = 3, // the pivot model rejected the pivot: the launch ended after its first level
+  SEARCH_HANDOFF  = 4  // the launch ended where the worklist phase starts; a resume launch runs it
 };
 
 // ---------------------------------------------------------------- asynchronous tail
@@ -885,6 +1006,7 @@ constexpr uint32_t           ASYNC_AFTER    = 16;        // top-down levels befo
 constexpr uint32_t           ASYNC_FRONTIER = 1u << 16;  // largest frontier that switches
 constexpr unsigned long long AW_TAG         = 1ull << 32; // marks a written slot
 constexpr int                AW_BATCH       = 8;         // neighbours a lane loads at once
+constexpr int                AW_WARPS       = 8;         // warps per block that take worklist items (the others wait at the phase's end)
 
 // Finds a warp keeps on its own stack (in its shared buffer) and expands in
 // its next round instead of appending them: a hop then costs the chain of
@@ -980,7 +1102,7 @@ run_async(fwbw_args const& a, uint32_t const* fq0, uint32_t qn0, aw_dir const d0
   bool          pending     = false;
   uint64_t      slot        = 0;
   unsigned      spins       = 0;
-  for (bool alive = true; alive;) {
+  for (bool alive = (threadIdx.x >> 5) < AW_WARPS; alive;) {
     if (!batch && ls_n == 0) {
       // only a warp without its own work claims slots: items appended to
       // the worklist then land with warps that are polling, not behind a
@@ -1217,6 +1339,8 @@ struct jctl
   unsigned long long c[2];        // the level's frontier: edges << qbits | vertices
   unsigned long long m_u[2];      // Beamer's unexplored-edge budget
   unsigned long long edges_td[2]; // top-down edges expanded
+  unsigned long long seen[2];     // vertices this search has reached (the pivot included)
+  uint32_t           grp[2];      // chunks per bottom-up sweep group this level
   uint32_t           lvl[2], bu[2], mode[2], mat[2], fixed[2], live[2], kind[2];
   uint32_t           restrict_to[2]; // 1: cut this search's candidates down to the other's set first
   uint32_t           capped, async, any_td, any_bu;
@@ -1224,8 +1348,17 @@ struct jctl
 };
 __shared__ jctl s_j;
 
+// The level loop's control where a launch handed off its worklist phase
+// (written by block 0, read by every block of the resume launch).
+struct joint_save
+{
+  jctl               j;
+  uint32_t           glvl, n_und;
+  unsigned long long barriers; // grid barriers the handing-off launch completed (the drop_barrier test hook counts on)
+};
+
 __device__ __forceinline__ int
-run_joint(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uint32_t& glvl, unsigned long long& epoch)
+run_joint(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uint32_t& glvl, unsigned long long& epoch, bool resume)
 {
   reach_state* const       st    = a.st;
   unsigned long long const qmask = (1ull << a.qbits) - 1;
@@ -1236,96 +1369,117 @@ run_joint(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uin
   if (threadIdx.x == 0) {
     s_bu_cut[0] = bu_cut{ a.cutmap, a.heavy + 3u * a.heavy_cap, &st->cut_n[0], a.heavy_cap, &st->heavy_err };
     s_bu_cut[1] = bu_cut{ a.cutmap + a.cut_words, a.heavy, &st->cut_n[1], a.heavy_cap, &st->heavy_err };
-    for (int d = 0; d < 2; ++d) {
+    if (resume) s_j = static_cast<joint_save const*>(a.jsave)->j;
+    for (int d = 0; d < 2 && !resume; ++d) {
       uint64_t const* h = d ? a.bh : a.fh;
       s_j.c[d]          = (static_cast<unsigned long long>(h[pivot + 1] - h[pivot]) << a.qbits) | 1u; // the pivot alone
       s_j.m_u[d]        = a.m;
       s_j.edges_td[d]   = 0;
+      s_j.seen[d]       = 1;
       s_j.lvl[d] = s_j.bu[d] = s_j.mode[d] = s_j.mat[d] = s_j.fixed[d] = 0;
       s_j.live[d]                                                      = 1;
       s_j.restrict_to[d]                                               = 0;
     }
-    s_j.capped = 0;
+    if (!resume) s_j.capped = 0;
   }
-  int rc = SEARCH_DONE;
+  int  rc         = SEARCH_DONE;
+  bool resume_now = resume; // the first iteration of a resume launch starts at its worklist phase
   for (;; ++glvl) {
     __syncthreads();
     uint32_t const s_out = (glvl + 1) % 3, s_clr = (glvl + 2) % 3;
-    // frontiers that return to top-down are built from the sweeps' finds first
-    if (s_j.mat[0] || s_j.mat[1]) {
+    if (!resume_now) {
+      // frontiers that return to top-down are built from the sweeps' finds first
+      if (s_j.mat[0] || s_j.mat[1]) {
 #pragma unroll 1
-      for (int d = 0; d < 2; ++d)
-        if (s_j.mat[d]) {
-          jdir const D = joint_dir(a, d);
-          materialize_scanned(a.n, D.fresh, jbuf(D, glvl), D.mat_q, a.qbits, D.td_head, a.m, sm);
-        }
-      if (!gsync(a, epoch)) return SEARCH_FAILED;
-      stamp(a, 7);
-      if (threadIdx.x == 0)
         for (int d = 0; d < 2; ++d)
-          if (s_j.mat[d]) s_j.c[d] = __ldcg(joint_dir(a, d).mat_q);
-      if (tally) st->mats += (s_j.mat[0] ? 1u : 0u) + (s_j.mat[1] ? 1u : 0u);
-    }
-    if (threadIdx.x == 0) {
-      if (blockIdx.x == 0)
+          if (s_j.mat[d]) {
+            jdir const D = joint_dir(a, d);
+            materialize_scanned(a.n, D.fresh, jbuf(D, glvl), D.mat_q, a.qbits, D.td_head, a.m, sm);
+          }
+        if (!gsync(a, epoch)) return SEARCH_FAILED;
+        stamp(a, 7);
+        if (threadIdx.x == 0)
+          for (int d = 0; d < 2; ++d)
+            if (s_j.mat[d]) s_j.c[d] = __ldcg(joint_dir(a, d).mat_q);
+        if (tally) st->mats += (s_j.mat[0] ? 1u : 0u) + (s_j.mat[1] ? 1u : 0u);
+      }
+      if (threadIdx.x == 0) {
+        if (blockIdx.x == 0)
+          for (int d = 0; d < 2; ++d) {
+            jdir const D = joint_dir(a, d);
+            D.lq[s_clr]  = 0;
+            if (!s_j.mat[d]) *D.mat_q = 0;
+          }
+        bool async = a.aw != nullptr, live = false;
+        s_j.restrict_to[0] = s_j.restrict_to[1] = 0; // one pass, in the level the partner ended
         for (int d = 0; d < 2; ++d) {
-          jdir const D = joint_dir(a, d);
-          D.lq[s_clr]  = 0;
-          if (!s_j.mat[d]) *D.mat_q = 0;
-        }
-      bool async = a.aw != nullptr, live = false;
-      s_j.restrict_to[0] = s_j.restrict_to[1] = 0; // one pass, in the level the partner ended
-      for (int d = 0; d < 2; ++d) {
-        s_j.kind[d] = JK_NONE;
-        if (!s_j.live[d]) continue;
-        unsigned long long const c  = s_j.c[d];
-        uint64_t const           qn = c & qmask, mf = c >> a.qbits;
-        if (qn == 0) {
-          // the search ran dry: rows the sweeps cut short are walked to the
-          // end in slices; it ends when a fix-up step finds nothing
-          if (__ldcg(joint_dir(a, d).cut_n) == 0 || s_j.fixed[d]) {
-            s_j.live[d] = 0;
-            if (s_j.live[d ^ 1]) s_j.restrict_to[d ^ 1] = 1; // the other search keeps only this one's set
+          s_j.kind[d] = JK_NONE;
+          if (!s_j.live[d]) continue;
+          unsigned long long const c  = s_j.c[d];
+          uint64_t const           qn = c & qmask, mf = c >> a.qbits;
+          if (qn == 0) {
+            // the search ran dry: rows the sweeps cut short are walked to the
+            // end in slices; it ends when a fix-up step finds nothing
+            if (__ldcg(joint_dir(a, d).cut_n) == 0 || s_j.fixed[d]) {
+              s_j.live[d] = 0;
+              if (s_j.live[d ^ 1]) s_j.restrict_to[d ^ 1] = 1; // the other search keeps only this one's set
+              continue;
+            }
+            s_j.kind[d] = JK_FIXUP;
+            async       = false;
+            live        = true;
             continue;
           }
-          s_j.kind[d] = JK_FIXUP;
-          async       = false;
-          live        = true;
-          continue;
+          live          = true;
+          s_j.fixed[d]  = 0;
+          if (s_j.lvl[d] >= a.cap || qn > a.n || mf > a.m) {
+            // level cap; or counters beyond the graph, which a correct search
+            // never produces (then nothing more is read or written)
+            s_j.capped = 1;
+            break;
+          }
+          if (s_j.mat[d]) s_j.mode[d] = 0;
+          else if (s_j.mode[d] == 0 && mf * a.alpha > s_j.m_u[d]) s_j.mode[d] = 1;
+          s_j.kind[d] = s_j.mode[d] ? JK_BU : JK_TD;
+          s_j.grp[d]  = s_j.mode[d] ? bu_group_size(n_und > s_j.seen[d] ? n_und - s_j.seen[d] : 0, a.n) : 1u;
+          if (!(s_j.mode[d] == 0 && s_j.lvl[d] >= ASYNC_AFTER && qn <= ASYNC_FRONTIER)) async = false;
         }
-        live          = true;
-        s_j.fixed[d]  = 0;
-        if (s_j.lvl[d] >= a.cap || qn > a.n || mf > a.m) {
-          // level cap; or counters beyond the graph, which a correct search
-          // never produces (then nothing more is read or written)
-          s_j.capped = 1;
-          break;
-        }
-        if (s_j.mat[d]) s_j.mode[d] = 0;
-        else if (s_j.mode[d] == 0 && mf * a.alpha > s_j.m_u[d]) s_j.mode[d] = 1;
-        s_j.kind[d] = s_j.mode[d] ? JK_BU : JK_TD;
-        if (!(s_j.mode[d] == 0 && s_j.lvl[d] >= ASYNC_AFTER && qn <= ASYNC_FRONTIER)) async = false;
+        s_j.async  = async && live && !s_j.capped;
+        s_j.any_td = s_j.kind[0] == JK_TD || s_j.kind[1] == JK_TD;
+        s_j.any_bu = s_j.kind[0] == JK_BU || s_j.kind[1] == JK_BU;
+        if (!live) s_j.capped |= 2; // both searches are done
+        s_j.cnt[0] = s_j.cnt[1] = 0;
       }
-      s_j.async  = async && live && !s_j.capped;
-      s_j.any_td = s_j.kind[0] == JK_TD || s_j.kind[1] == JK_TD;
-      s_j.any_bu = s_j.kind[0] == JK_BU || s_j.kind[1] == JK_BU;
-      if (!live) s_j.capped |= 2; // both searches are done
-      s_j.cnt[0] = s_j.cnt[1] = 0;
-    }
-    __syncthreads();
-    if (s_j.capped) break;
-    // a search that lost its partner: keep only candidates in the partner's set
+      __syncthreads();
+      if (s_j.capped) break;
+      // a search that lost its partner: keep only candidates in the partner's set
 #pragma unroll 1
-    for (int d = 0; d < 2; ++d)
-      if (s_j.restrict_to[d] && s_j.live[d]) {
-        if (tally) st->restricts += 1;
-        uint32_t* const       av = joint_dir(a, d).avail;
-        uint32_t const* const ot = joint_dir(a, d ^ 1).mark;
-        for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) {
-          uint32_t const keep = __ldcg(ot + w), cur = __ldcg(av + w);
-          if (cur & ~keep) atomicAnd(av + w, keep);
+      for (int d = 0; d < 2; ++d)
+        if (s_j.restrict_to[d] && s_j.live[d]) {
+          if (tally) st->restricts += 1;
+          uint32_t* const       av = joint_dir(a, d).avail;
+          uint32_t const* const ot = joint_dir(a, d ^ 1).mark;
+          for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) {
+            uint32_t const keep = __ldcg(ot + w), cur = __ldcg(av + w);
+            if (cur & ~keep) atomicAnd(av + w, keep);
+          }
         }
+    }
+    resume_now = false;
+    if (s_j.async && a.handoff) {
+      // the worklist phase runs in a launch with more registers per thread
+      // (its hop chains stay in flight without spills): save the control
+      // and end this launch; the resume launch starts at this point
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        auto* const js = static_cast<joint_save*>(a.jsave);
+        js->j          = s_j;
+        js->glvl       = glvl;
+        js->n_und      = n_und;
+        js->barriers   = epoch - s_epoch0;
+        st->handoff    = 1;
       }
+      return SEARCH_HANDOFF;
+    }
     if (s_j.async) {
       // long and thin: both searches finish on the worklist
       uint64_t   ea = 0;
@@ -1416,17 +1570,21 @@ run_joint(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uin
         }
     }
     if (s_j.any_bu) {
-      // both searches' chunks in one range, spread over every warp of the grid
+      // both searches' chunks (or sparse groups of chunks) in one range,
+      // spread over every warp of the grid
       uint32_t const chunks = (words + 31) / 32;
-      uint32_t const c0     = s_j.kind[0] == JK_BU ? chunks : 0u;
-      uint32_t const c1     = s_j.kind[1] == JK_BU ? chunks : 0u;
+      uint32_t const g0     = s_j.grp[0], g1 = s_j.grp[1];
+      uint32_t const c0     = s_j.kind[0] == JK_BU ? (chunks + g0 - 1) / g0 : 0u;
+      uint32_t const c1     = s_j.kind[1] == JK_BU ? (chunks + g1 - 1) / g1 : 0u;
       uint32_t       nf0 = 0, nf1 = 0;
       uint64_t       ne = 0, ncd = 0;
       for (uint32_t cc = blockIdx.x * BU_WARPS + wid; cc < c0 + c1; cc += gridDim.x * BU_WARPS) {
-        int const      d = cc < c0 ? 0 : 1;
-        jdir const     D = joint_dir(a, d);
-        uint32_t       f = 0;
-        bu_sweep_chunk(d ? cc - c0 : cc, a.n, D.bu_head, D.bu_adj, D.avail, D.mark, D.fresh, s_bu_cut[d], sm.warp[wid], f, ne, ncd);
+        int const      d  = cc < c0 ? 0 : 1;
+        jdir const     D  = joint_dir(a, d);
+        uint32_t const gs = d ? g1 : g0;
+        uint32_t const ch = (d ? cc - c0 : cc) * gs;
+        uint32_t       f  = 0;
+        bu_sweep_group(ch, chunks - ch < gs ? chunks - ch : gs, a.n, D.bu_head, D.bu_adj, D.avail, D.mark, D.fresh, s_bu_cut[d], sm.warp[wid], f, ne, ncd);
         if (d) nf1 += f;
         else nf0 += f;
       }
@@ -1476,6 +1634,7 @@ run_joint(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uin
           }
         }
         s_j.c[d] = next;
+        s_j.seen[d] += next & qmask;
       }
     }
   }
@@ -1961,7 +2120,12 @@ write_ids(fwbw_args const& a, uint32_t words, bool search, uint32_t scc)
   }
 }
 
-__global__ void __launch_bounds__(R_THREADS, 4)
+// MINB: blocks per SM the launch is compiled for.  The level loop runs
+// with 4 (64 registers per thread); a search that moves to the worklist
+// phase hands off to a resume launch with 2 (128 registers), whose hop
+// chains keep their loads in flight without spills.
+template<int MINB>
+__global__ void __launch_bounds__(R_THREADS, MINB)
 k_fwbw(fwbw_args a)
 {
   __shared__ fwbw_smem sm;
@@ -1977,8 +2141,10 @@ k_fwbw(fwbw_args a)
     p                   = prod == 0 || id >= a.n ? a.n : id;
   }
   bool const search = p < a.n; // block-uniform
-  if (threadIdx.x == 0) sm.buf_n = 0, sm.edges_bu = sm.cands_bu = 0, s_epoch0 = epoch;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  // a resume launch numbers its barriers on from the launch it continues
+  if (threadIdx.x == 0) sm.buf_n = 0, sm.edges_bu = sm.cands_bu = 0, s_epoch0 = a.resume ? epoch - static_cast<joint_save const*>(a.jsave)->barriers : epoch;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && a.resume) st->handoff = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && !a.resume) {
     st->t_ns[0] = globaltimer();
     st->marks   = 0;
     stamp(a, 0);
@@ -1997,14 +2163,19 @@ k_fwbw(fwbw_args a)
     st->async_phases            = 0;
     st->cut_n[0] = st->cut_n[1] = st->fixups = 0;
     st->hseed_n = st->heavy_err = st->trim_async = st->joint = st->restricts = 0;
-    st->pivot_rejected = 0;
+    st->pivot_rejected = st->handoff = 0;
     for (int i = 0; i < 6; ++i) st->hq_n[i] = 0;
     if (search) a.seed.q[0] = p, a.seed.prefix[0] = 0;
   }
   int      rc   = SEARCH_DONE;
   uint32_t glvl = 0;
   uint32_t id   = p;
-  if (search) {
+  uint32_t n_und = 0;
+  if (search && a.resume) {
+    auto const* js = static_cast<joint_save const*>(a.jsave);
+    glvl           = js->glvl;
+    n_und          = js->n_und;
+  } else if (search) {
     // init: cand = und \ {p}, vis_a = vis_b = {p}; |und| per block
     uint32_t c = 0;
     for (uint32_t w = blockIdx.x * R_THREADS + threadIdx.x; w < words; w += gridDim.x * R_THREADS) {
@@ -2025,9 +2196,11 @@ k_fwbw(fwbw_args a)
       uint64_t s = 0;
       for (uint32_t i = threadIdx.x; i < gridDim.x; i += R_THREADS) s += __ldcg(a.partial + i);
       block_exclusive_scan<uint64_t, R_THREADS>(s, &tot);
-      uint32_t const n_und = static_cast<uint32_t>(tot);
-      rc = run_joint(a, sm, p, n_und, glvl, epoch);
+      n_und = static_cast<uint32_t>(tot);
     }
+  }
+  if (search) {
+    if (rc == SEARCH_DONE) rc = run_joint(a, sm, p, n_und, glvl, epoch, a.resume != 0);
     if (rc == SEARCH_DONE && a.min_ids) {
       // smallest member = first set bit of vis_a & vis_b.  Every block first looks
       // at the same leading MIN_WORDS words (the SCC is usually dense
@@ -2277,7 +2450,7 @@ fwbw_grid(kspn_context* ctx)
 {
   if (!ctx->search_grid) {
     int bps = 0, sms = 0;
-    KSPN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_fwbw, R_THREADS, 0));
+    KSPN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_fwbw<4>, R_THREADS, 0));
     KSPN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
     if (bps < 1) throw error{ KSPN_ERR_CUDA, "persistent FW-BW kernel does not fit on an SM" };
     // at most AW_GRID_MAX blocks: the worklist's spare slots (AW_STALE)
@@ -2285,6 +2458,30 @@ fwbw_grid(kspn_context* ctx)
     ctx->search_grid = static_cast<unsigned>(std::min<int>(bps * sms, AW_GRID_MAX));
   }
   return ctx->search_grid;
+}
+
+// The grid barrier's arrival counter advances by the grid size per
+// barrier (a wait's target is epoch x grid), so it restarts from zero when a
+// launch's grid differs from the last one's on this barrier.
+void
+barrier_for_grid(kspn_context* ctx, unsigned grid)
+{
+  if (ctx->bar_grid == grid) return;
+  KSPN_CUDA(cudaMemsetAsync(ctx->ws.gbar, 0, offsetof(grid_barrier, err), ctx->stream));
+  ctx->bar_grid = grid;
+}
+
+unsigned
+resume_grid(kspn_context* ctx)
+{
+  if (!ctx->resume_grid) {
+    int bps = 0, sms = 0;
+    KSPN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_fwbw<2>, R_THREADS, 0));
+    KSPN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    if (bps < 1) throw error{ KSPN_ERR_CUDA, "persistent FW-BW resume kernel does not fit on an SM" };
+    ctx->resume_grid = static_cast<unsigned>(std::min<int>(bps * sms, AW_GRID_MAX));
+  }
+  return ctx->resume_grid;
 }
 
 } // namespace
@@ -2369,8 +2566,16 @@ launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* s
   // an earlier switch only cuts duplicates; a later one could overrun the worklist's bound
   a.aw_exact     = opt.aw_exact_after && opt.aw_exact_after < ws.aw_entries / 2 ? opt.aw_exact_after : ws.aw_entries / 2;
   a.model        = model;
-  void* args[]  = { &a };
-  KSPN_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(&k_fwbw), dim3(fwbw_grid(ctx)), dim3(R_THREADS), args, 0, ctx->stream));
+  a.jsave        = static_cast<char*>(ws.gbar) + 2048;
+  a.handoff      = 1;
+  a.resume       = 0;
+  static_assert(sizeof(fwbw_args) <= sizeof(ctx->fwbw_last), "launch arguments must fit their copy in the context");
+  static_assert(sizeof(joint_save) <= 2048, "saved level control must fit its workspace slot");
+  std::memcpy(ctx->fwbw_last, &a, sizeof(a));
+  ctx->fwbw_after = after_kernel;
+  void* args[]    = { &a };
+  barrier_for_grid(ctx, fwbw_grid(ctx));
+  KSPN_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(&k_fwbw<4>), dim3(fwbw_grid(ctx)), dim3(R_THREADS), args, 0, ctx->stream));
   ctx->launches += 1;
   if (after_kernel) KSPN_CUDA(cudaEventRecord(after_kernel, ctx->stream));
   // results, and the barrier's error word (read after the launch ended: a
@@ -2380,12 +2585,31 @@ launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* s
   KSPN_CUDA(cudaMemcpyAsync(hb, &gbar->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
 }
 
-// After the stream was synchronised: barrier failures and level caps.
-void
+// After the stream was synchronised: a launch that handed off its worklist
+// phase is continued by the resume launch (same arguments, 128 registers
+// per thread; one more host round trip, only on graphs that reach that
+// phase); then barrier failures and level caps.  Returns whether a resume
+// launch ran.
+bool
 check_persistent(kspn_context* ctx)
 {
   auto* const hs = reinterpret_cast<reach_state*>(ctx->h_state);
-  auto* const hb = reinterpret_cast<uint32_t*>(static_cast<char*>(ctx->h_state) + 1024);
+  auto* const hb      = reinterpret_cast<uint32_t*>(static_cast<char*>(ctx->h_state) + 1024);
+  bool const  resumed = hs->handoff && !*hb && !hs->bar_err;
+  if (resumed) {
+    fwbw_args a;
+    std::memcpy(&a, ctx->fwbw_last, sizeof(a));
+    a.handoff    = 0;
+    a.resume     = 1;
+    void* args[] = { &a };
+    barrier_for_grid(ctx, resume_grid(ctx));
+    KSPN_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<void const*>(&k_fwbw<2>), dim3(resume_grid(ctx)), dim3(R_THREADS), args, 0, ctx->stream));
+    ctx->launches += 1;
+    if (ctx->fwbw_after) KSPN_CUDA(cudaEventRecord(ctx->fwbw_after, ctx->stream));
+    KSPN_CUDA(cudaMemcpyAsync(hs, ctx->ws.rstate, sizeof(reach_state), cudaMemcpyDeviceToHost, ctx->stream));
+    KSPN_CUDA(cudaMemcpyAsync(hb, &static_cast<grid_barrier*>(ctx->ws.gbar)->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
   if (*hb || hs->bar_err) {
     // counters of a launch that gave up are not epoch-aligned, and its
     // worklist may hold entries: start over
@@ -2397,6 +2621,7 @@ check_persistent(kspn_context* ctx)
   }
   if (hs->heavy_err) throw error{ KSPN_ERR_INTERNAL, "reachability / trim: heavy-row list overflow" };
   if (hs->err) throw error{ KSPN_ERR_TIMEOUT, "reachability / trim: level cap exceeded" };
+  return resumed;
 }
 
 // Level statistics and phase stamps of the first FW-BW a call ran.
@@ -2439,7 +2664,7 @@ fw_bw_trim_async(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* sc
 resident_result
 fw_bw_trim_result(kspn_context* ctx, dgraph const& g, kspn_options const& opt, kspn_stats* st)
 {
-  check_persistent(ctx);
+  bool const resumed = check_persistent(ctx);
   auto* hs = reinterpret_cast<reach_state*>(ctx->h_state);
   record_search_stats(ctx, opt, st);
   ctx->h_ctr64[0] += hs->trim_edges;
@@ -2468,6 +2693,7 @@ fw_bw_trim_result(kspn_context* ctx, dgraph const& g, kspn_options const& opt, k
     st->search_worklist        = hs->async_phases ? 1u : 0u;
   }
   resident_result r;
+  r.resumed           = resumed;
   r.pivot_rejected    = hs->pivot_rejected != 0;
   r.pivot             = hs->pivot_used;
   r.fwbw_decided      = hs->decided;

@@ -940,7 +940,17 @@ trim_1_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id
 unsigned
 pivot_candidates(uint32_t n)
 {
-  return stream_grid((static_cast<uint64_t>(n) + TF_ITEMS - 1) / TF_ITEMS);
+  // k_trim_first's grid, which is also the number of per-block pivot
+  // candidates: one wave of resident blocks (blocks per SM x SMs), so no
+  // partial last wave leaves SMs idle, or fewer blocks for a small graph
+  static unsigned const wave = [] {
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trim_first, T_THREADS, 0) != cudaSuccess || per_sm <= 0) per_sm = 4;
+    return static_cast<unsigned>(std::min(sms * per_sm, static_cast<int>(PV_FINAL)));
+  }();
+  uint64_t const b = (static_cast<uint64_t>(n) + static_cast<uint64_t>(T_THREADS) * TF_ITEMS - 1) / (static_cast<uint64_t>(T_THREADS) * TF_ITEMS);
+  return static_cast<unsigned>(b < wave ? (b ? b : 1) : wave);
 }
 
 // (the caller has zeroed ws.ctr; ids are not written: the resident
