@@ -63,6 +63,7 @@ WORKLOADS = {
     "rmat22": ("rmat", dict(scale=22, ef=16, seed=2), "R-MAT scale 22, edge factor 16, a,b,c,d=.57,.19,.19,.05, permuted ids"),
     "rmat20": ("rmat", dict(scale=20, ef=16, seed=2), "R-MAT scale 20, edge factor 16, a,b,c,d=.57,.19,.19,.05, permuted ids"),
     "rgg24": ("rgg", dict(n=1 << 24, seed=3), "2D random geometric graph n=2^24, mean undirected degree 8, each pair u->v / v->u / both / neither with p=.25"),
+    "rgg22": ("rgg", dict(n=1 << 22, seed=3), "2D random geometric graph n=2^22, mean undirected degree 8, each pair u->v / v->u / both / neither with p=.25"),
     "rgg20": ("rgg", dict(n=1 << 20, seed=3), "2D random geometric graph n=2^20, mean undirected degree 8, each pair u->v / v->u / both / neither with p=.25"),
 }
 # kspn pipelines by name: the FAST pipeline, kaspan::scc's phase order

@@ -800,7 +800,6 @@ struct fwbw_args
   uint64_t           aw_exact;     // worklist items after which warps take their finds exactly
   float const*       model;        // pivot MLP parameters: the launch scores its pivot first (null: no check)
   void*              jsave;        // the level loop's saved control (handoff, resume)
-  uint32_t           handoff;      // 1: end the launch where the worklist phase would start (SEARCH_HANDOFF)
   uint32_t           resume;       // 1: continue a launch that handed off, at its worklist phase
 };
 
@@ -1357,6 +1356,7 @@ struct joint_save
   unsigned long long barriers; // grid barriers the handing-off launch completed (the drop_barrier test hook counts on)
 };
 
+template<int MINB>
 __device__ __forceinline__ int
 run_joint(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uint32_t& glvl, unsigned long long& epoch, bool resume)
 {
@@ -1466,7 +1466,7 @@ run_joint(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uin
         }
     }
     resume_now = false;
-    if (s_j.async && a.handoff) {
+    if (MINB != 2 && s_j.async) {
       // the worklist phase runs in a launch with more registers per thread
       // (its hop chains stay in flight without spills): save the control
       // and end this launch; the resume launch starts at this point
@@ -1480,26 +1480,28 @@ run_joint(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uin
       }
       return SEARCH_HANDOFF;
     }
-    if (s_j.async) {
-      // long and thin: both searches finish on the worklist
-      uint64_t   ea = 0;
-      int const  d0 = s_j.live[0] ? 0 : 1;
-      bool const two = s_j.live[0] && s_j.live[1];
-      jdir const D0 = joint_dir(a, d0), D1 = joint_dir(a, 1);
-      aw_dir const w0{ D0.td_head, D0.td_adj, D0.avail, D0.mark };
-      aw_dir const w1{ D1.td_head, D1.td_adj, D1.avail, D1.mark };
-      frontier_buf const f0 = s_j.lvl[d0] == 0 ? a.seed : jbuf(D0, glvl);
-      frontier_buf const f1 = s_j.lvl[1] == 0 ? a.seed : jbuf(D1, glvl);
-      int const r = run_async(a, f0.q, static_cast<uint32_t>(s_j.c[d0] & qmask), w0, f1.q, static_cast<uint32_t>(s_j.c[1] & qmask), two ? &w1 : nullptr, epoch, ea, sm);
-      if (r != SEARCH_DONE) return r;
-      stamp(a, 13);
-      if (threadIdx.x == 0) {
-        s_j.edges_td[d0] += ea;
-        for (int d = 0; d < 2; ++d)
-          if (s_j.live[d]) s_j.c[d] = 0, s_j.mode[d] = 0, s_j.mat[d] = 0, s_j.lvl[d] += 1; // nothing queued: next it runs dry (or fixes up cut rows)
+    if constexpr (MINB == 2) {
+      if (s_j.async) {
+        // long and thin: both searches finish on the worklist
+        uint64_t   ea = 0;
+        int const  d0 = s_j.live[0] ? 0 : 1;
+        bool const two = s_j.live[0] && s_j.live[1];
+        jdir const D0 = joint_dir(a, d0), D1 = joint_dir(a, 1);
+        aw_dir const w0{ D0.td_head, D0.td_adj, D0.avail, D0.mark };
+        aw_dir const w1{ D1.td_head, D1.td_adj, D1.avail, D1.mark };
+        frontier_buf const f0 = s_j.lvl[d0] == 0 ? a.seed : jbuf(D0, glvl);
+        frontier_buf const f1 = s_j.lvl[1] == 0 ? a.seed : jbuf(D1, glvl);
+        int const r = run_async(a, f0.q, static_cast<uint32_t>(s_j.c[d0] & qmask), w0, f1.q, static_cast<uint32_t>(s_j.c[1] & qmask), two ? &w1 : nullptr, epoch, ea, sm);
+        if (r != SEARCH_DONE) return r;
+        stamp(a, 13);
+        if (threadIdx.x == 0) {
+          s_j.edges_td[d0] += ea;
+          for (int d = 0; d < 2; ++d)
+            if (s_j.live[d]) s_j.c[d] = 0, s_j.mode[d] = 0, s_j.mat[d] = 0, s_j.lvl[d] += 1; // nothing queued: next it runs dry (or fixes up cut rows)
+        }
+        if (tally) st->async_phases += 1;
+        continue;
       }
-      if (tally) st->async_phases += 1;
-      continue;
     }
     if (glvl == 0 && a.model && blockIdx.x == gridDim.x - 1 && threadIdx.x < 32) {
       // the pivot model scores the pivot during the first level, in the
@@ -2200,7 +2202,7 @@ k_fwbw(fwbw_args a)
     }
   }
   if (search) {
-    if (rc == SEARCH_DONE) rc = run_joint(a, sm, p, n_und, glvl, epoch, a.resume != 0);
+    if (rc == SEARCH_DONE) rc = run_joint<MINB>(a, sm, p, n_und, glvl, epoch, a.resume != 0);
     if (rc == SEARCH_DONE && a.min_ids) {
       // smallest member = first set bit of vis_a & vis_b.  Every block first looks
       // at the same leading MIN_WORDS words (the SCC is usually dense
@@ -2567,7 +2569,6 @@ launch_persistent(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* s
   a.aw_exact     = opt.aw_exact_after && opt.aw_exact_after < ws.aw_entries / 2 ? opt.aw_exact_after : ws.aw_entries / 2;
   a.model        = model;
   a.jsave        = static_cast<char*>(ws.gbar) + 2048;
-  a.handoff      = 1;
   a.resume       = 0;
   static_assert(sizeof(fwbw_args) <= sizeof(ctx->fwbw_last), "launch arguments must fit their copy in the context");
   static_assert(sizeof(joint_save) <= 2048, "saved level control must fit its workspace slot");
@@ -2599,7 +2600,6 @@ check_persistent(kspn_context* ctx)
   if (resumed) {
     fwbw_args a;
     std::memcpy(&a, ctx->fwbw_last, sizeof(a));
-    a.handoff    = 0;
     a.resume     = 1;
     void* args[] = { &a };
     barrier_for_grid(ctx, resume_grid(ctx));
