@@ -609,7 +609,7 @@ def run_kspn(args):
     roof = resident_roofline(step_stats, peak)
     if roof is None:  # the call did not take the resident path (profiled or oversized)
         dom = max(agg, key=lambda k: agg[k][0])
-        kms, kbytes, _ = (x / prof_steps for x in agg[dom])
+        kms, kbytes, _ = (x / max(prof_steps, 1) for x in agg[dom])
         a_ = (kbytes / (kms * 1e-3)) / 1e9 if kms > 0 else 0.0
         roof = {"kernel": dom, "achieved": a_, "frac": a_ / peak, "bytes_per_step": kbytes, "ms_per_step": kms}
     traffic, traffic_note = None, None
@@ -655,7 +655,7 @@ def run_kspn(args):
                        "levels_bw": last["levels_bw"], "bottom_up": last["levels_bottom_up"], "label_calls": last["label_calls"],
                        "edges_scanned": last["edges_scanned"], "trace": trace,
                        "search_phase_ms": {{4: "expand", 5: "sweep", 7: "materialize", 8: "init", 9: "end", 10: "finalize", 11: "trim_seed", 12: "trim_level", 13: "worklist", 14: "fix_up", 15: "trim_heavy", 16: "trim_worklist"}.get(k, k): round(v, 4) for k, v in search_phases.items()},
-                       "kernels": {k: {"ms": round(a[0] / prof_steps, 4), "GB/s": round(a[1] / (a[0] * 1e-3) / 1e9, 1) if a[0] else 0}
+                       "kernels": {k: {"ms": round(a[0] / max(prof_steps, 1), 4), "GB/s": round(a[1] / (a[0] * 1e-3) / 1e9, 1) if a[0] else 0}
                                    for k, a in agg.items()}},
         }
         if other_cpu is not None:
