@@ -88,7 +88,10 @@ typedef struct kspn_options
   uint32_t wait_limit;
   uint32_t drop_barrier;
   uint32_t aw_exact_after;
-  uint32_t reserved[1];
+  int32_t  learned_seeds;   /* 1: label searches order their seeds by the context's pivot model: vertices
+                               the model scores higher get smaller labels (they win the min-label
+                               propagation and become roots first); 0 = the reference's rotated ids.
+                               Needs a model and n <= 2^31; same partition either way */
 } kspn_options;
 
 /* Per-call statistics (all fields written by a successful call). */

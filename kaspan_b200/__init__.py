@@ -72,7 +72,7 @@ class Options(C.Structure):
         ("wait_limit", C.c_uint32),
         ("drop_barrier", C.c_uint32),
         ("aw_exact_after", C.c_uint32),
-        ("reserved", C.c_uint32 * 1),
+        ("learned_seeds", C.c_int32),
     ]
 
 

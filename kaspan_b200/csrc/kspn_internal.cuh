@@ -375,7 +375,8 @@ enum buffer_slot : int
   BUF_TRANSPOSE  = 2, // transpose built for kspn_scc_device without bw
   BUF_GEN        = 3, // generator scratch (RGG points and cells)
   BUF_SHARD      = 4, // counters of the sharded steps (shard.cu)
-  BUF_COUNT      = 5
+  BUF_SEEDS      = 5, // learned seed order of the label searches: score bucket per vertex (label.cu)
+  BUF_COUNT      = 6
 };
 
 struct cached_graph

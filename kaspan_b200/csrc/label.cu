@@ -13,7 +13,16 @@
 // its undecided out-neighbours with atomicMin, and joins the next level's
 // worklist (a per-level claim bitmap keeps each vertex once per level).
 // The backward closure pushes from newly decided vertices over in-edges.
+//
+// Learned seed order (kspn_options.learned_seeds, no reference
+// counterpart): map(v) = bucket(v) << s | (v ^ mask), where s bits hold a
+// vertex id, bucket(v) ranks the pivot model's score (a higher score, a
+// smaller bucket, so the vertex wins the min-label propagation) and mask
+// varies the order inside a bucket from call to call as the rotation does.
+// map is injective on [0, n) and never UNDECIDED, so the fixpoint, the
+// roots and the partition are those of any other seed order.
 #include "expand.cuh"
+#include "mlp.cuh"
 
 namespace kspn {
 
@@ -29,9 +38,51 @@ l_grid(uint64_t items)
   return static_cast<unsigned>(b < 148ull * 8 ? (b ? b : 1) : 148ull * 8);
 }
 
+// A search's seed order: the reference's rotated ids, or the learned order.
+struct seed_map
+{
+  uint32_t const* bucket; // null: rotr(v, rot)
+  int             rot;
+  uint32_t        shift;  // id bits of a learned label
+  uint32_t        mask;   // xor of the id bits (this call's order inside a bucket)
+  __device__ __forceinline__ uint32_t map(uint32_t v) const { return bucket ? (__ldg(bucket + v) << shift) | (v ^ mask) : rotr32(v, rot); }
+  __device__ __forceinline__ uint32_t unmap(uint32_t l) const { return bucket ? (l & ((1u << shift) - 1u)) ^ mask : rotl32(l, rot); }
+};
+
+// The pivot model's score of every undecided vertex as a bucket in
+// [0, nbuckets - 1): sigmoid(logit) high -> bucket low.  One warp per vertex
+// (the features sample its rows); the top bucket stays unused, so no label
+// is UNDECIDED.
+__global__ void __launch_bounds__(L_THREADS)
+k_seed_buckets(uint32_t n, uint32_t const* __restrict__ und, uint64_t const* __restrict__ fh, uint32_t const* __restrict__ fc, uint64_t const* __restrict__ bh,
+               uint32_t const* __restrict__ bc, float const* __restrict__ params, uint32_t nbuckets, uint32_t* __restrict__ bucket)
+{
+  unsigned const lane  = threadIdx.x & 31u;
+  uint32_t const words = (n + 31) / 32;
+  uint32_t const gw    = (blockIdx.x * L_THREADS + threadIdx.x) >> 5;
+  uint32_t const nw    = (gridDim.x * L_THREADS) >> 5;
+  for (uint32_t w = gw; w < words; w += nw) {
+    uint32_t word = und[w];
+    if (w == words - 1 && (n & 31)) word &= (1u << (n & 31)) - 1u;
+    while (word) {
+      uint32_t const v = w * 32 + (__ffs(word) - 1);
+      word &= word - 1;
+      float f[MLP_IN], h1, h2;
+      mlp_features(v, fh, fc, bh, bc, f);
+      float const z = mlp_forward_w(mlp_weights_global{ params }, f, h1, h2);
+      if (lane == 0) {
+        float const    p = 1.f / (1.f + expf(-z));
+        float const    q = (1.f - p) * static_cast<float>(nbuckets - 1);
+        uint32_t const b = q >= static_cast<float>(nbuckets - 2) ? nbuckets - 2 : (q > 0.f ? static_cast<uint32_t>(q) : 0u);
+        bucket[v]        = b;
+      }
+    }
+  }
+}
+
 // label = map(v) for undecided v (all queued), UNDECIDED otherwise.
 __global__ void __launch_bounds__(L_THREADS)
-k_label_init(uint32_t n, uint32_t const* __restrict__ und, uint32_t* __restrict__ label, int rot, uint32_t* __restrict__ q, uint32_t* __restrict__ qn)
+k_label_init(uint32_t n, uint32_t const* __restrict__ und, uint32_t* __restrict__ label, seed_map sm, uint32_t* __restrict__ q, uint32_t* __restrict__ qn)
 {
   __shared__ uint32_t s_buf[DENSE_BUF];
   __shared__ uint32_t s_n, s_base;
@@ -43,7 +94,7 @@ k_label_init(uint32_t n, uint32_t const* __restrict__ und, uint32_t* __restrict_
     uint64_t const t    = base + threadIdx.x;
     uint32_t const v    = static_cast<uint32_t>(t);
     bool const     live = t < n && bit_get(und, v);
-    if (t < n) label[v] = live ? rotr32(v, rot) : UNDECIDED;
+    if (t < n) label[v] = live ? sm.map(v) : UNDECIDED;
     bq.push(live, v);
     __syncthreads();
     if (s_n > DENSE_BUF - L_THREADS) bq.flush(q, qn, &s_base);
@@ -81,7 +132,7 @@ k_unclaim(uint32_t const* __restrict__ q, uint32_t const* __restrict__ qn_ptr, u
 }
 
 __global__ void __launch_bounds__(L_THREADS)
-k_label_roots(uint32_t n, uint32_t* __restrict__ und, uint32_t const* __restrict__ label, uint32_t* __restrict__ scc_id, int rot, uint32_t* __restrict__ q, uint32_t* __restrict__ qn, uint32_t* __restrict__ decided)
+k_label_roots(uint32_t n, uint32_t* __restrict__ und, uint32_t const* __restrict__ label, uint32_t* __restrict__ scc_id, seed_map sm, uint32_t* __restrict__ q, uint32_t* __restrict__ qn, uint32_t* __restrict__ decided)
 {
   __shared__ uint32_t s_buf[DENSE_BUF];
   __shared__ uint32_t s_n, s_base;
@@ -93,7 +144,7 @@ k_label_roots(uint32_t n, uint32_t* __restrict__ und, uint32_t const* __restrict
   for (uint64_t base = static_cast<uint64_t>(blockIdx.x) * L_THREADS; base < span; base += static_cast<uint64_t>(gridDim.x) * L_THREADS) {
     uint64_t const t    = base + threadIdx.x;
     uint32_t const v    = static_cast<uint32_t>(t);
-    bool const     root = t < n && bit_get(und, v) && label[v] == rotr32(v, rot);
+    bool const     root = t < n && bit_get(und, v) && label[v] == sm.map(v);
     bool const     won  = root && bit_take(und, v);
     if (won) {
       scc_id[v] = v;
@@ -112,7 +163,7 @@ struct label_bw_op
   uint32_t*       und;
   uint32_t const* label;
   uint32_t*       scc_id;
-  int             rot;
+  seed_map        sm;
   // u = decided vertex, v = one of its in-neighbours; every push is a decision
   __device__ __forceinline__ uint32_t probe(uint32_t v) const { return und[v >> 5]; }
   __device__ __forceinline__ bool     operator()(uint32_t u, uint32_t v, bool valid, uint32_t word) const
@@ -120,7 +171,7 @@ struct label_bw_op
     if (!valid || !((word >> (v & 31)) & 1u)) return false;
     uint32_t const lu = label[u];
     if (label[v] != lu || !bit_take(und, v)) return false;
-    scc_id[v] = rotl32(lu, rot);
+    scc_id[v] = sm.unmap(lu);
     return true;
   }
 };
@@ -138,10 +189,20 @@ label_search(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id
   auto*          edges = reinterpret_cast<unsigned long long*>(ws.ctr64);
   uint32_t const cap   = opt.max_label_iters ? opt.max_label_iters : g.n + 2;
 
+  seed_map sm{ nullptr, rotation, 0, 0 };
+  if (opt.learned_seeds && ctx->pivot_model && g.n > 0 && g.n <= (1u << 31)) {
+    // the learned order: every undecided vertex scored once per call
+    uint32_t const shift = std::max<uint32_t>(1u, static_cast<uint32_t>(32 - __builtin_clz(g.n - 1 | 1u)));
+    auto* const    bk    = static_cast<uint32_t*>(context_buffer(ctx, BUF_SEEDS, static_cast<size_t>(g.n) * 4));
+    k_seed_buckets<<<l_grid(g.n / 8 + 1), L_THREADS, 0, ctx->stream>>>(g.n, und, g.fh, g.fc, g.bh, g.bc, ctx->pivot_model, 1u << (32 - shift), bk);
+    KSPN_CHECK_LAUNCH();
+    ctx->launches += 1;
+    sm = seed_map{ bk, rotation, shift, (static_cast<uint32_t>(rotation) * 0x9E3779B9u) & ((1u << shift) - 1u) };
+  }
   zero_counters(ctx);
   KSPN_CUDA(cudaMemsetAsync(ws.vis_a, 0, words * 4, ctx->stream));
   KSPN_CUDA(cudaMemsetAsync(ws.vis_b, 0, words * 4, ctx->stream));
-  k_label_init<<<l_grid(g.n), L_THREADS, 0, ctx->stream>>>(g.n, und, ws.label, rotation, q[0], qc[0]);
+  k_label_init<<<l_grid(g.n), L_THREADS, 0, ctx->stream>>>(g.n, und, ws.label, sm, q[0], qc[0]);
   KSPN_CHECK_LAUNCH();
   ctx->launches += 1;
 
@@ -171,7 +232,7 @@ label_search(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id
   // roots, then the backward closure inside each label class
   KSPN_CUDA(cudaMemsetAsync(ws.ctr + CTR_Q0, 0, 2 * sizeof(uint32_t), ctx->stream));
   KSPN_CUDA(cudaMemsetAsync(ws.ctr + CTR_DECIDED, 0, sizeof(uint32_t), ctx->stream));
-  k_label_roots<<<l_grid(g.n), L_THREADS, 0, ctx->stream>>>(g.n, und, ws.label, scc_id, rotation, q[0], qc[0], ws.ctr + CTR_DECIDED);
+  k_label_roots<<<l_grid(g.n), L_THREADS, 0, ctx->stream>>>(g.n, und, ws.label, scc_id, sm, q[0], qc[0], ws.ctr + CTR_DECIDED);
   KSPN_CHECK_LAUNCH();
   ctx->launches += 1;
   read_counters(ctx);
@@ -183,7 +244,7 @@ label_search(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id
     KSPN_CUDA(cudaMemsetAsync(qc[nxt], 0, sizeof(uint32_t), ctx->stream));
     uint32_t const fq = ctx->h_ctr[CTR_Q0 + cur];
     uint64_t const eb = ctx->h_ctr64[0];
-    expand_level(ctx, g.bh, g.bc, q[cur], qc[cur], ws.ctr + CTR_NTILES, edges, ws.tile_start, q[nxt], qc[nxt], label_bw_op{ und, ws.label, scc_id, rotation });
+    expand_level(ctx, g.bh, g.bc, q[cur], qc[cur], ws.ctr + CTR_NTILES, edges, ws.tile_start, q[nxt], qc[nxt], label_bw_op{ und, ws.label, scc_id, sm });
     read_counters(ctx);
     uint32_t const pushed = ctx->h_ctr[CTR_Q0 + nxt];
     decided += pushed;

@@ -163,3 +163,35 @@ def test_in_kernel_check_costs_no_launch(ctx):
             assert learned["decided"] == plain["decided"]
     finally:
         ctx.set_pivot_model(None)
+
+
+@pytest.mark.parametrize("pipeline", [K.PIPELINE_REFERENCE, K.PIPELINE_HPC_LIKE, K.PIPELINE_HPC_TRIM_EX, K.PIPELINE_TRIM_EX])
+def test_learned_seed_order_exact(ctx, pipeline):
+    """The label searches with the learned seed order (the shipped model
+    ranks the seeds, kspn_options.learned_seeds) give the identical
+    partition on every pipeline that runs them: planted-partition graphs
+    and the synthetic shapes, against Tarjan."""
+    import torch
+
+    from kspn_testlib import device, fuzzy_cases
+
+    model = K.default_pivot_model()
+    if model is None:
+        pytest.skip("no shipped pivot model")
+    ctx.set_pivot_model(model)
+    try:
+        graphs = [G for _, G, _ in fuzzy_cases((37, 150, 299), seeds=(4,), degrees=(1.0, 4.0))]
+        graphs += [O.rmat(13, 8, 3), O.rgg(1 << 13, 5), O.gnm(5000, 20000, 6)]
+        calls = []
+        for G in graphs:
+            fwh, fwc, bwh, bwc = device(G)
+            want = O.tarjan(G)
+            for seeds in (0, 1):
+                out = torch.empty(max(G.n, 1), dtype=torch.int32, device="cuda")
+                st = K.Stats()
+                ctx.scc_device(G.n, G.m, fwh, fwc, bwh, bwc, out, K.default_options(pipeline=pipeline, learned_seeds=seeds), st)
+                assert np.array_equal(out.cpu().numpy().view(np.uint32)[: G.n], want), (G.n, seeds)
+                calls.append(st.label_calls)
+        assert sum(calls) > 0, "the pipeline should run label searches on these graphs"
+    finally:
+        ctx.set_pivot_model(None)
