@@ -270,6 +270,15 @@ def run_batched(ctx, stream, args, K, world=1, rank=0):
     # every rank tunes its own shard (the same steps on every rank)
     best, rep = ctx.autotune_batched(B.count, B.n, B.vtx_off, B.fwh, B.fwc, B.bwh, B.bwc, out, reps=2)
     ms_t, _, st_t = timed(best)
+    # route 1: the mix as one graph (a super-source linked to every graph's
+    # pivot, the single-graph pipeline), same ids checked
+    ref_ids = out.clone()
+    uo = K.BatchOptions()
+    K.lib().kspn_batch_options_default(__import__("ctypes").byref(uo))
+    uo.route = 1
+    ms_u, launches_u, st_u = timed(uo)
+    union_same = bool(torch.equal(out, ref_ids))
+    assert union_same, "the union route must give the per-graph route's ids"
     peak, peak_kind = measured_peak_gbs()
     b_min = 2 * (8 * (n_all_v + 1) + 4 * m_all) + 4 * n_all_v
     res = {
@@ -280,6 +289,9 @@ def run_batched(ctx, stream, args, K, world=1, rank=0):
         "launches_per_step": launches, "captured": "one CUDA graph per call (plan + solve kernels), replayed",
         "stats": st.as_dict(),
         "pipeline_min_bytes": b_min, "pipeline_frac": (b_min / (ms * 1e-3)) / 1e9 / peak, "peak": peak, "peak_source": peak_kind,
+        "union_route": {"value": m_all / (ms_u * 1e-3), "ms_per_step": ms_u, "launches_per_step": launches_u, "identical_output": union_same,
+                        "taken": st_u.graphs_small == 0 and st_u.graphs_large == B.count,
+                        "how": "kspn_batch_options.route = 1: the mix as ONE graph with global ids plus a super-source whose rows list every graph's pivot; the single-graph pipeline (trim, one FW-BW deciding a component in every graph at once, trim fixpoint, residual); host-driven, not one captured graph"},
         "tuned": {"value": m_all / (ms_t * 1e-3), "ms_per_step": ms_t, "candidates": rep.candidates, "tuner_default_ms": rep.default_ms, "tuner_best_ms": rep.best_ms,
                   "best": {"cluster_size": best.cluster_size, "cluster_min": best.cluster_min, "rem_tarjan": best.rem_tarjan, "max_rounds": best.max_rounds}},
     }
@@ -376,6 +388,32 @@ def learned_vs_plain(ctx, stream, graph, pipeline, steps):
         res[name] = {"ms_per_step": ms, "edges_scanned": d["edges_scanned"], "pivot": d["pivot"], "fwbw_decided": d["decided"]["fwbw"]}
     assert np.array_equal(ids["plain"], ids["learned"]), "learned and plain pivots must give the same partition"
     res["speedup"] = res["plain"]["ms_per_step"] / res["learned"]["ms_per_step"]
+    res["identical_output"] = True
+    return res
+
+
+def seed_order(ctx, stream, graph, steps):
+    """The label searches' seed order, rotated ids (the reference's) vs the
+    pivot model's ranking, in kaspan::scc's phase order (trim_1_first,
+    FW-BW, trim_1_normal, label searches until done); identical output
+    asserted."""
+    import numpy as np
+    import torch
+
+    import kaspan_b200 as K
+
+    o = torch.empty(graph.n, dtype=torch.int32, device="cuda")
+    res = {"pipeline": "scc (the reference's phase order)"}
+    ids = {}
+    for name, seeds in (("rotated", 0), ("learned", 1)):
+        opt = K.default_options(pipeline=K.PIPELINE_REFERENCE, validate=0, learned_seeds=seeds)
+        timed_steps(ctx, stream, graph, opt, 1, o)
+        ms, st = timed_steps(ctx, stream, graph, opt, steps, o)
+        d = st[-1].as_dict()
+        ids[name] = o.cpu().numpy().view(np.uint32).copy()
+        res[name] = {"ms_per_step": ms, "label_calls": d["label_calls"], "label_decided": d["decided"]["label"]}
+    assert np.array_equal(ids["rotated"], ids["learned"]), "the seed order must not change the partition"
+    res["speedup"] = res["rotated"]["ms_per_step"] / res["learned"]["ms_per_step"]
     res["identical_output"] = True
     return res
 
@@ -567,6 +605,7 @@ def run_kspn(args):
         ctx.set_pivot_model(model)
         lvp = {"model": "kaspan_b200/pivot_model.npy (8-32-32-1, trained on the GPU: python -m kaspan_b200.pivot_train)"}
         lvp["workload"] = learned_vs_plain(ctx, stream, G, pipeline, max(3, min(args.steps, 10)))
+        lvp["seed_order"] = seed_order(ctx, stream, G, 3)
         p_ = WORKLOADS[args.workload][1]
         Gd, _hubs = decoy_rmat(ctx, p_["scale"], p_["seed"] + 100, 0.57, decoys=8)
         lvp["workload_with_decoys"] = learned_vs_plain(ctx, stream, Gd, pipeline, max(3, min(args.steps, 10)))
@@ -688,7 +727,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-path and autotuner sections")
     ap.add_argument("--no-other-rmat", action="store_true", help="skip the other R-MAT configuration's section")
-    ap.add_argument("--reference-seconds", type=float, default=150.0,
+    ap.add_argument("--reference-seconds", type=float, default=100.0,
                     help="--impl reference on graphs above 2^29 edges: stop timing calls after this many seconds (at least one call)")
     ap.add_argument("--batch-graphs", type=int, default=4096, help="graphs of the batch mix (default 4096)")
     ap.add_argument("--batch-max-log2", type=int, default=18, help="largest graph of the batch mix: 2^this vertices (default 18)")

@@ -393,7 +393,11 @@ typedef struct kspn_batch_options {
     uint32_t search;       /* 0 or 2: FW, then BW inside the FW set; 1: FW and BW searches of a
                               round at the same time (SCC = their intersection; half the levels,
                               more work: on C5 3% slower) */
-    uint32_t reserved;
+    uint32_t route;        /* 0: the per-graph kernels above, one captured CUDA graph; 1: the mix as ONE
+                              graph with global ids plus a super-source linked to every graph's
+                              pivot, through the single-graph pipeline (one FW-BW decides a component
+                              in every graph at once; host-driven, several synchronisations); falls
+                              back to 0 when the super-source would not be the pipeline's pivot */
 } kspn_batch_options;
 
 typedef struct kspn_batch_stats {

@@ -263,7 +263,7 @@ class TuneReport(C.Structure):
 class BatchOptions(C.Structure):
     """kspn_batch_options (include/kspn.h)."""
     _fields_ = [("max_rounds", C.c_uint32), ("rem_tarjan", C.c_uint32), ("cluster_size", C.c_uint32), ("reserved0", C.c_uint32),
-                ("cluster_min", C.c_uint64), ("search", C.c_uint32), ("reserved", C.c_uint32)]
+                ("cluster_min", C.c_uint64), ("search", C.c_uint32), ("route", C.c_uint32)]
 
 
 class BatchStats(C.Structure):

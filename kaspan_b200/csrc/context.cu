@@ -339,6 +339,7 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
     // FW-BW again from the largest live in * out (degrees are current after
     // a trim fixpoint), while each round still decides a share of it.
     auto const fwbw_again = [&]() {
+      if (ctx->union_route) return; // a batch mix: one pivot decides one component of one graph
       uint64_t const big = std::max<uint64_t>(g.n / 16, 1u << 16);
       for (uint32_t again = 0; again < 3 && g.n - decided >= big; ++again) {
         uint64_t const left = g.n - decided;
@@ -474,6 +475,51 @@ run_pipeline(kspn_context* ctx, dgraph const& g, uint32_t* scc_id, kspn_options 
     st->ms_total        = ms;
     st->kernel_launches = ctx->launches - launches0;
   }
+}
+
+// The batch mix as one graph (kspn_batch_options.route = 1, batch_union.cu):
+// false when the super-source would not be the pipeline's pivot (the
+// caller then takes the per-graph route).
+bool
+scc_batched_union(kspn_context* ctx, uint32_t count, uint64_t n, uint64_t const* vtx_off, uint64_t const* fh, uint32_t const* fc, uint64_t const* bh, uint32_t const* bc,
+                  uint32_t* scc_id, kspn_batch_stats* st)
+{
+  if (count == 0 || n == 0) return true;
+  if (n + 1 >= static_cast<uint64_t>(UNDECIDED)) return false; // the super-source needs an id below UNDECIDED
+  uint64_t m = 0;
+  KSPN_CUDA(cudaMemcpyAsync(&m, fh + n, sizeof(m), cudaMemcpyDeviceToHost, ctx->stream));
+  KSPN_CUDA(cudaStreamSynchronize(ctx->stream));
+  size_t const heads = align_up((n + 2) * sizeof(uint64_t)), rows = align_up(std::max<uint64_t>(m + count, 1) * sizeof(uint32_t));
+  size_t const ids = align_up((n + 1) * sizeof(uint32_t)), piv = align_up(static_cast<size_t>(count) * sizeof(uint32_t));
+  char* const  base = static_cast<char*>(context_buffer(ctx, BUF_UNION, 2 * heads + 2 * rows + ids + piv + 256));
+  auto* const  ufh  = reinterpret_cast<uint64_t*>(base);
+  auto* const  ubh  = reinterpret_cast<uint64_t*>(base + heads);
+  auto* const  ufc  = reinterpret_cast<uint32_t*>(base + 2 * heads);
+  auto* const  ubc  = reinterpret_cast<uint32_t*>(base + 2 * heads + rows);
+  auto* const  uid  = reinterpret_cast<uint32_t*>(base + 2 * heads + 2 * rows);
+  auto* const  pv   = reinterpret_cast<uint32_t*>(base + 2 * heads + 2 * rows + ids);
+  auto* const  pn   = reinterpret_cast<uint32_t*>(base + 2 * heads + 2 * rows + ids + piv);
+  auto* const  mx   = reinterpret_cast<unsigned long long*>(base + 2 * heads + 2 * rows + ids + piv + 128);
+  unsigned long long maxprod = 0;
+  uint32_t const     P       = union_build(ctx, count, n, m, vtx_off, fh, fc, bh, bc, ufh, ufc, ubh, ubc, pv, pn, mx, &maxprod);
+  if (static_cast<unsigned long long>(P) * P <= maxprod) return false;
+  dgraph const ug{ static_cast<uint32_t>(n + 1), m + P, ufh, ufc, ubh, ubc };
+  kspn_options o{};
+  kspn_options_default(&o);
+  o.validate = 0;
+  struct route_flag
+  {
+    kspn_context* c;
+    ~route_flag() { c->union_route = false; }
+  } flag{ ctx };
+  ctx->union_route = true;
+  run_pipeline(ctx, ug, uid, o, nullptr);
+  union_rename(ctx, count, n, vtx_off, uid, scc_id);
+  if (st) {
+    st->graphs_large = count;
+    st->fwbw_rounds  = 1;
+  }
+  return true;
 }
 
 // Resolves the transpose: given, or built on the device into `store`.
@@ -1036,7 +1082,8 @@ kspn_scc_batched(kspn_context* ctx, uint32_t count, uint64_t n_total, const uint
     if (opt) o = *opt;
     if (stats) std::memset(stats, 0, sizeof(*stats));
     KSPN_CUDA(cudaEventRecord(ctx->ev[KSPN_PHASES], ctx->stream));
-    scc_batched(ctx, count, n_total, d_vtx_off, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr, d_scc_id, o, stats);
+    if (o.route != 1 || !scc_batched_union(ctx, count, n_total, d_vtx_off, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr, d_scc_id, stats))
+      scc_batched(ctx, count, n_total, d_vtx_off, d_fw_head, d_fw_csr, d_bw_head, d_bw_csr, d_scc_id, o, stats);
     KSPN_CUDA(cudaEventRecord(ctx->ev[KSPN_PHASES + 1], ctx->stream));
     KSPN_CUDA(cudaEventSynchronize(ctx->ev[KSPN_PHASES + 1]));
     if (stats) KSPN_CUDA(cudaEventElapsedTime(&stats->ms, ctx->ev[KSPN_PHASES], ctx->ev[KSPN_PHASES + 1]));

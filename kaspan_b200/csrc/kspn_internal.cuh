@@ -376,7 +376,8 @@ enum buffer_slot : int
   BUF_GEN        = 3, // generator scratch (RGG points and cells)
   BUF_SHARD      = 4, // counters of the sharded steps (shard.cu)
   BUF_SEEDS      = 5, // learned seed order of the label searches: score bucket per vertex (label.cu)
-  BUF_COUNT      = 6
+  BUF_UNION      = 6, // the batch mix as one graph (batch_union.cu)
+  BUF_COUNT      = 7
 };
 
 struct cached_graph
@@ -411,6 +412,7 @@ struct kspn_context
   unsigned           search_grid = 0;      // blocks of the persistent FW-BW launch
   unsigned           resume_grid = 0;      // blocks of its resume launch (the worklist phase)
   unsigned           bar_grid    = 0;      // grid of the last launch on the workspace's grid barrier
+  bool               union_route = false;  // the pipeline runs on a batch mix as one graph: no second FW-BW
   alignas(16) unsigned char fwbw_last[1024] = {}; // arguments of the last persistent FW-BW launch (a resume launch reuses them)
   cudaEvent_t        fwbw_after  = nullptr; // event the last launch records after its kernel (re-recorded after a resume)
   float*             pivot_model = nullptr; // device copy of the pivot MLP (kspn_set_pivot_model)
@@ -500,6 +502,10 @@ uint32_t trim_fixpoint(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32
 uint32_t trim_exhaustive_first(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id, uint32_t* outdeg, uint32_t* indeg);
 uint32_t trim_2(kspn_context* ctx, dgraph const& g, uint32_t* und, uint32_t* scc_id);
 uint32_t select_pivot_live(kspn_context* ctx, dgraph const& g, uint32_t const* und);
+uint32_t union_build(kspn_context* ctx, uint32_t count, uint64_t n, uint64_t m, uint64_t const* vtx_off, uint64_t const* fh_in, uint32_t const* fc_in, uint64_t const* bh_in,
+                     uint32_t const* bc_in, uint64_t* fh, uint32_t* fc, uint64_t* bh, uint32_t* bc, uint32_t* piv, uint32_t* p_dev, unsigned long long* maxprod_dev,
+                     unsigned long long* maxprod);
+void     union_rename(kspn_context* ctx, uint32_t count, uint64_t n, uint64_t const* vtx_off, uint32_t const* uid, uint32_t* scc_id);
 void     scc_batched(kspn_context* ctx, uint32_t G, uint64_t N, uint64_t const* vtx_off, uint64_t const* fh, uint32_t const* fc, uint64_t const* bh, uint32_t const* bc, uint32_t* scc_id,
                      kspn_batch_options const& opt, kspn_batch_stats* st);
 void     batch_release(kspn_context* ctx);

@@ -119,3 +119,40 @@ def test_batched_edge_cases(ctx):
     # spot checks: the cycle is one SCC named 0, the path all singletons
     assert np.all(want[int(vo[2]): int(vo[3])] == 0)
     assert np.array_equal(want[int(vo[3]): int(vo[4])], np.arange(k, dtype=np.uint32))
+
+
+def test_batched_union_route(ctx, mix):
+    """route 1: the mix as one graph with a super-source linked to every
+    graph's pivot, through the single-graph pipeline; the same ids as the
+    per-graph route and as Tarjan, on a repeated call too."""
+    B, want = mix
+    for _ in range(2):
+        got, st = _run(ctx, B, route=1)
+        assert np.array_equal(got, want)
+        assert st.graphs_large == B.count and st.graphs_small == 0  # the union route ran
+
+
+def test_batched_union_route_edge_cases(ctx):
+    """The union route on a graph of one vertex (no pivot), self-loops only,
+    a long cycle, a long path and two cycles joined by a path."""
+    import torch
+
+    graphs = [(1, []), (3, [(0, 0), (1, 1), (2, 2)])]
+    k = 3000
+    graphs.append((k, [(i, (i + 1) % k) for i in range(k)]))
+    graphs.append((k, [(i, i + 1) for i in range(k - 1)]))
+    graphs.append((700, [(i, (i + 1) % 300) for i in range(300)] + [(299, 300)] + [(300 + i, 300 + (i + 1) % 400) for i in range(400)]))
+    sizes = np.array([g[0] for g in graphs], np.uint32)
+    vo = np.concatenate([[0], np.cumsum(sizes, dtype=np.uint64)])
+    N = int(vo[-1])
+    src = np.concatenate([np.array([e[0] for e in es], np.uint64) + vo[i] for i, (n, es) in enumerate(graphs)]).astype(np.uint32)
+    dst = np.concatenate([np.array([e[1] for e in es], np.uint64) + vo[i] for i, (n, es) in enumerate(graphs)]).astype(np.uint32)
+    G = KG.from_edges(ctx, N, torch.from_numpy(src.view(np.int32)).cuda(), torch.from_numpy(dst.view(np.int32)).cuda())
+    d_vo = torch.from_numpy(vo.astype(np.int64)).cuda()
+    ctx.batch_localize(len(graphs), N, d_vo, G.fwh, G.fwc)
+    ctx.batch_localize(len(graphs), N, d_vo, G.bwh, G.bwc)
+    B = KG.DeviceBatch(len(graphs), N, G.m, d_vo, G.fwh, G.fwc, G.bwh, G.bwc, sizes)
+    want = _oracle_ids(B)
+    got, st = _run(ctx, B, route=1)
+    assert np.array_equal(got, want)
+    assert st.graphs_large == len(graphs)

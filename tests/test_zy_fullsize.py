@@ -7,7 +7,7 @@ also compared with the reference's own kaspan::scc (kaspan/scc/scc.hpp:21-87)
 after normalise_scc_id.  The 4096-graph batch mix (C5) is decomposed by
 kspn_scc_batched in one call and compared, graph by graph, with the
 reference Tarjan of the whole mix as one graph with global ids (its SCCs are
-the graphs' SCCs).  Minutes of host time in all; collected before
+the graphs' SCCs), through both batched routes.  Minutes of host time in all; collected before
 test_zz_no_alloc.py."""
 from __future__ import annotations
 
@@ -92,3 +92,11 @@ def test_full_batch_mix_vs_reference_tarjan(ctx):
           f"small={st.graphs_small} large={st.graphs_large}")
     assert st.graphs_small + st.graphs_large == B.count
     assert np.array_equal(got, want)
+    # route 1 (the mix as one graph through a super-source) on the same mix
+    o = K.BatchOptions()
+    K.lib().kspn_batch_options_default(__import__("ctypes").byref(o))
+    o.route = 1
+    out = torch.empty(B.n, dtype=torch.int32, device="cuda")
+    st = ctx.scc_batched(B.count, B.n, B.vtx_off, B.fwh, B.fwc, B.bwh, B.bwc, out, o)
+    print(f"C5 union route: kspn {st.ms:.2f} ms, taken={st.graphs_large == B.count}")
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), want)
