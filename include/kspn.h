@@ -411,8 +411,11 @@ typedef struct kspn_batch_stats {
     uint32_t graphs_cluster; /* of the large ones: decomposed by a cluster of blocks */
     uint32_t cluster_size;
     float    phase_ms[5];   /* larger graphs, summed over their groups (group-leader clock):
-                               init, trim, pivot, searches, remainder Tarjan */
-    uint32_t reserved[2];
+                               init, trim, pivot, searches, remainder Tarjan; route 1: the
+                               pipeline's trim_1_first, trim, (unused), FW-BW, residual + label
+                               searches + relabel */
+    uint32_t label_calls;   /* route 1: label searches the union needed */
+    uint32_t reserved[1];
 } kspn_batch_stats;
 
 void kspn_batch_options_default(kspn_batch_options* opt);

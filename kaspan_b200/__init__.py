@@ -271,7 +271,7 @@ class BatchStats(C.Structure):
     _fields_ = [("graphs_small", C.c_uint32), ("graphs_large", C.c_uint32), ("fwbw_rounds", C.c_uint32),
                 ("tarjan_smem", C.c_uint32), ("tarjan_serial", C.c_uint32), ("trim_levels", C.c_uint32),
                 ("ms", C.c_float), ("graphs_cluster", C.c_uint32), ("cluster_size", C.c_uint32), ("phase_ms", C.c_float * 5),
-                ("reserved", C.c_uint32 * 2)]
+                ("label_calls", C.c_uint32), ("reserved", C.c_uint32 * 1)]
 
     def as_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ("reserved", "phase_ms")}

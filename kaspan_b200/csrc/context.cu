@@ -513,11 +513,19 @@ scc_batched_union(kspn_context* ctx, uint32_t count, uint64_t n, uint64_t const*
     ~route_flag() { c->union_route = false; }
   } flag{ ctx };
   ctx->union_route = true;
-  run_pipeline(ctx, ug, uid, o, nullptr);
+  kspn_stats ps;
+  run_pipeline(ctx, ug, uid, o, st ? &ps : nullptr);
   union_rename(ctx, count, n, vtx_off, uid, scc_id);
   if (st) {
+    // the single-graph pipeline's phases in the batch stats' slots:
+    // trim_first, trim (+ trim-2), FW-BW, residual + label + relabel
     st->graphs_large = count;
     st->fwbw_rounds  = 1;
+    st->phase_ms[0]  = ps.ms[KSPN_PHASE_TRIM_FIRST];
+    st->phase_ms[1]  = ps.ms[KSPN_PHASE_TRIM] + ps.ms[KSPN_PHASE_TRIM2] + ps.ms[KSPN_PHASE_TRIM_NORMAL];
+    st->phase_ms[3]  = ps.ms[KSPN_PHASE_FWBW];
+    st->phase_ms[4]  = ps.ms[KSPN_PHASE_RESIDUAL] + ps.ms[KSPN_PHASE_LABEL] + ps.ms[KSPN_PHASE_CANON];
+    st->label_calls  = ps.label_calls;
   }
   return true;
 }
