@@ -177,7 +177,8 @@ constexpr int EX_BATCH = 4;
 template<typename Op>
 __device__ __forceinline__ void
 expand_tile(uint32_t tile, uint32_t ntiles, uint32_t const* q, uint32_t qn, uint64_t total, uint64_t const* prefix, uint32_t const* tile_start, uint64_t const* __restrict__ head,
-            uint32_t const* __restrict__ adj, uint32_t* s_j, uint32_t* s_i, block_queue& bq, Op const& op, int k_begin = 0, int k_end = EX_ITEMS)
+            uint32_t const* __restrict__ adj, uint32_t* s_j, uint32_t* s_i, block_queue& bq, Op const& op, int k_begin = 0, int k_end = EX_ITEMS,
+            uint32_t* s_q = nullptr, uint64_t* s_p = nullptr)
 {
   uint64_t const t0 = static_cast<uint64_t>(tile) * EX_TILE;
   uint64_t const t1 = t0 + EX_TILE < total ? t0 + EX_TILE : total;
@@ -195,6 +196,14 @@ expand_tile(uint32_t tile, uint32_t ntiles, uint32_t const* q, uint32_t qn, uint
   }
   __syncthreads();
   tile_max_scan(s_j);
+  // the tile's frontier rows (queue entries and edge prefixes) staged in
+  // shared memory when they fit (<= 512 rows): every slot's row lookup is
+  // then a shared-memory read instead of two L2 reads
+  bool const staged = s_q && i1 - i0 + 1 <= 512;
+  if (staged) {
+    for (uint32_t r = threadIdx.x; r <= i1 - i0; r += EX_THREADS) s_q[r] = __ldcg(q + i0 + r), s_p[r] = __ldcg(prefix + i0 + r);
+    __syncthreads();
+  }
   for (int k0 = k_begin; k0 < k_end; k0 += EX_BATCH) {
     uint32_t u[EX_BATCH], v[EX_BATCH], w[EX_BATCH];
     uint64_t idx[EX_BATCH];
@@ -208,8 +217,8 @@ expand_tile(uint32_t tile, uint32_t ntiles, uint32_t const* q, uint32_t qn, uint
       idx[h]              = 0;
       if (ok[h]) {
         uint32_t const j  = i0 + s_j[slot];
-        u[h]              = __ldcg(q + j);
-        uint64_t const pj = __ldcg(prefix + j);
+        u[h]              = staged ? s_q[j - i0] : __ldcg(q + j);
+        uint64_t const pj = staged ? s_p[j - i0] : __ldcg(prefix + j);
         ok[h]             = e >= pj;
         idx[h]            = e - pj; // offset in u's row
       }

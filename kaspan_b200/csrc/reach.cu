@@ -823,7 +823,7 @@ struct fwbw_smem
   __device__ __forceinline__ uint32_t* tile_rows() { return reinterpret_cast<uint32_t*>(warp); }
   __device__ __forceinline__ uint32_t* buf() { return reinterpret_cast<uint32_t*>(warp) + EX_TILE; }
 };
-static_assert(sizeof(bu_warp_smem) * BU_WARPS >= (EX_TILE + BU_BUF) * sizeof(uint32_t), "tile rows and block queue must fit the warp buffers");
+static_assert(sizeof(bu_warp_smem) * BU_WARPS >= (EX_TILE + BU_BUF + 512 * 3) * sizeof(uint32_t), "tile rows and block queue must fit the warp buffers");
 static_assert(BU_BUF == EX_TILE && BU_BUF % R_THREADS == 0, "flush: whole runs per thread");
 
 __device__ __forceinline__ uint64_t
@@ -1539,7 +1539,8 @@ run_joint(fwbw_args const& a, fwbw_smem& sm, uint32_t pivot, uint32_t n_und, uin
         int const          part = static_cast<int>(u % pd);
         take_op const      op{ D.avail, D.mark };
         expand_tile(u / pd, d ? ntl[1] : ntl[0], fin.q, static_cast<uint32_t>(s_j.c[d] & qmask), s_j.c[d] >> a.qbits, fin.prefix, fin.tile_start, D.td_head, D.td_adj, sm.tile_rows(), sm.tile_i, bq, op,
-                    part * per, part * per + per);
+                    part * per, part * per + per, reinterpret_cast<uint32_t*>(sm.warp) + EX_TILE + BU_BUF,
+                    reinterpret_cast<uint64_t*>(reinterpret_cast<uint32_t*>(sm.warp) + EX_TILE + BU_BUF + 512));
         flush_scanned(sm, jbuf(D, glvl + 1), &D.lq[s_out], a.qbits, D.td_head, a.n, a.m);
       }
 #pragma unroll 1
