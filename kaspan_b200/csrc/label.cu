@@ -61,20 +61,27 @@ k_seed_buckets(uint32_t n, uint32_t const* __restrict__ und, uint64_t const* __r
   uint32_t const words = (n + 31) / 32;
   uint32_t const gw    = (blockIdx.x * L_THREADS + threadIdx.x) >> 5;
   uint32_t const nw    = (gridDim.x * L_THREADS) >> 5;
-  for (uint32_t w = gw; w < words; w += nw) {
-    uint32_t word = und[w];
-    if (w == words - 1 && (n & 31)) word &= (1u << (n & 31)) - 1u;
-    while (word) {
-      uint32_t const v = w * 32 + (__ffs(word) - 1);
-      word &= word - 1;
-      float f[MLP_IN], h1, h2;
-      mlp_features(v, fh, fc, bh, bc, f);
-      float const z = mlp_forward_w(mlp_weights_global{ params }, f, h1, h2);
-      if (lane == 0) {
-        float const    p = 1.f / (1.f + expf(-z));
-        float const    q = (1.f - p) * static_cast<float>(nbuckets - 1);
-        uint32_t const b = q >= static_cast<float>(nbuckets - 2) ? nbuckets - 2 : (q > 0.f ? static_cast<uint32_t>(q) : 0u);
-        bucket[v]        = b;
+  // a warp takes 32 words at once (one per lane, one coalesced load), then
+  // scores the set bits of the non-empty ones, one vertex at a time
+  for (uint32_t wb = gw * 32; wb < words; wb += nw * 32) {
+    uint32_t const w  = wb + lane;
+    uint32_t       mw = w < words ? und[w] : 0u;
+    if (w == words - 1 && (n & 31)) mw &= (1u << (n & 31)) - 1u;
+    for (unsigned todo = __ballot_sync(0xFFFFFFFFu, mw != 0); todo; todo &= todo - 1) {
+      unsigned const src  = __ffs(todo) - 1;
+      uint32_t       word = __shfl_sync(0xFFFFFFFFu, mw, src);
+      while (word) {
+        uint32_t const v = (wb + src) * 32 + (__ffs(word) - 1);
+        word &= word - 1;
+        float f[MLP_IN], h1, h2;
+        mlp_features(v, fh, fc, bh, bc, f);
+        float const z = mlp_forward_w(mlp_weights_global{ params }, f, h1, h2);
+        if (lane == 0) {
+          float const    p = 1.f / (1.f + expf(-z));
+          float const    q = (1.f - p) * static_cast<float>(nbuckets - 1);
+          uint32_t const b = q >= static_cast<float>(nbuckets - 2) ? nbuckets - 2 : (q > 0.f ? static_cast<uint32_t>(q) : 0u);
+          bucket[v]        = b;
+        }
       }
     }
   }
