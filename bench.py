@@ -667,7 +667,13 @@ def run_kspn(args):
     oname = OTHER_RMAT.get(args.workload)
     if rank == 0 and world == 1 and oname and not args.no_other_rmat:
         other, other_cpu = run_other_rmat(ctx, stream, args, peak, K, oname, not args.no_cpu_baseline and CPU_SAMPLE.get(args.workload) == oname)
-    sharded = run_sharded(ctx, args, K, world, rank) if world > 1 else None
+    sharded = None
+    if world > 1:
+        # an extra section: a failure here must not cost the main line
+        try:
+            sharded = run_sharded(ctx, args, K, world, rank)
+        except Exception as exc:  # noqa: BLE001
+            sharded = {"error": f"{type(exc).__name__}: {exc}"[:300]}
 
     if rank == 0:
         line = {
