@@ -310,6 +310,7 @@ bt_trim(bt_args const& a, bt_graph const& G, bt_group const& g, uint32_t* qin, u
 // opposite-direction row (bu_head / bu_adj) until a neighbour in `mark`
 // (reached so far, this level's finds included: reachability does not
 // need BFS levels), and joins.
+constexpr int      BT_BU_ILP = 2; // candidates a thread walks side by side in a bottom-up level
 constexpr uint32_t BT_BU_DIV = 5; // measured on C5: 1/2 23.1 ms, 1/3 19.2, 1/4 17.7, 1/6 17.7, 1/16 19.6, none 23.3
 
 __device__ uint32_t
@@ -332,16 +333,41 @@ bt_reach(bt_args const& a, bt_graph const& G, bt_group const& g, uint64_t const*
       break;
     }
     if (static_cast<uint64_t>(hi - lo) * BT_BU_DIV > n_und) {
+      // a thread walks up to BT_BU_ILP candidates of its word side by side
+      // (their offset loads, then their neighbour loads, then their probes
+      // in flight together) instead of one dependent row walk at a time
       for (uint32_t wd = g.gt; wd < G.words; wd += g.GT) {
         uint32_t cw = (cand ? __ldcg(cand + wd) : __ldcg(G.und + wd)) & ~__ldcg(mark + wd);
         while (cw) {
-          uint32_t const v = wd * 32 + __ffs(cw) - 1;
-          cw &= cw - 1;
-          for (uint64_t e = bu_head[v], end = bu_head[v + 1]; e < end; ++e)
-            if (bt_get(mark, bu_adj[e])) {
-              if (bit_claim(mark, v)) list[bt_slot(&g.S->cnt)] = v;
-              break;
+          uint32_t v[BT_BU_ILP];
+          uint64_t b[BT_BU_ILP], e[BT_BU_ILP];
+#pragma unroll
+          for (int k = 0; k < BT_BU_ILP; ++k) {
+            v[k] = UNDECIDED;
+            b[k] = e[k] = 0;
+            if (cw) {
+              v[k] = wd * 32 + __ffs(cw) - 1;
+              cw &= cw - 1;
             }
+          }
+#pragma unroll
+          for (int k = 0; k < BT_BU_ILP; ++k)
+            if (v[k] != UNDECIDED) b[k] = bu_head[v[k]], e[k] = bu_head[v[k] + 1];
+          for (bool more = true; more;) {
+            uint32_t x[BT_BU_ILP];
+#pragma unroll
+            for (int k = 0; k < BT_BU_ILP; ++k) x[k] = b[k] < e[k] ? bu_adj[b[k]] : 0u;
+            more = false;
+#pragma unroll
+            for (int k = 0; k < BT_BU_ILP; ++k) {
+              if (b[k] >= e[k]) continue;
+              if (bt_get(mark, x[k])) {
+                if (bit_claim(mark, v[k])) list[bt_slot(&g.S->cnt)] = v[k];
+                e[k] = b[k]; // done
+              } else if (++b[k] < e[k])
+                more = true;
+            }
+          }
         }
       }
     } else
