@@ -37,7 +37,10 @@ states the count.
 
 Multi-GPU (torchrun): every rank decomposes its own seeded instance (seed +
 rank); value = edges over all ranks / max-over-ranks time ("weak" scaling,
-no data-path collective).  --impl reference runs on rank 0 only.
+no data-path collective).  A `sharded` section adds ONE graph
+(--sharded-workload, R-MAT scale 22 by default) decomposed over all ranks
+with a frontier exchange per level (kaspan_b200/shard.py).  --impl
+reference runs on rank 0 only.
 """
 from __future__ import annotations
 
@@ -463,17 +466,18 @@ def run_other_rmat(ctx, stream, args, peak, K, name, cpu_sample):
 
 def run_sharded(ctx, args, K, world, rank):
     """ONE graph over all ranks (kaspan_b200/shard.py: a contiguous vertex
-    range per GPU, frontier exchange over NCCL every level): the workload of
-    seed 0 on every rank, sharded; time per decomposition = max over ranks
-    (the ranks meet at a collective every level).  Its ids are checked
-    against the single-GPU decomposition of the same graph."""
+    range per GPU, frontier exchange over NCCL every level): the graph of
+    --sharded-workload (seed 0 on every rank), sharded; time per
+    decomposition = max over ranks (the ranks meet at a collective every
+    level).  Its ids are checked against the single-GPU decomposition of the
+    same graph."""
     import numpy as np
     import torch
     import torch.distributed as dist
 
     from kaspan_b200 import shard as SH
 
-    G = make_graph(ctx, args.workload, rank_seed=0)
+    G = make_graph(ctx, args.sharded_workload, rank_seed=0)
     want = torch.empty(G.n, dtype=torch.int32, device="cuda")
     ctx.scc_device(G.n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, want, K.default_options(validate=0))
     fwh_h = G.fwh.cpu().numpy().view(np.uint64)
@@ -504,7 +508,7 @@ def run_sharded(ctx, args, K, world, rank):
     okt = torch.tensor([1 if ok else 0], device="cuda")
     dist.all_reduce(okt, op=dist.ReduceOp.MIN)
     ms = 1e3 * min(times[1:])
-    return {"workload": WORKLOADS[args.workload][2], "n": S.n, "m": m, "ranks": world, "bounds": bounds,
+    return {"workload": WORKLOADS[args.sharded_workload][2], "n": S.n, "m": m, "ranks": world, "bounds": bounds,
             "value": m / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms, "scaling": "strong (one graph, all ranks)",
             "timing": "host wall clock around the whole sharded call, max over ranks (every level meets at a collective), best of 2 after 1 warm-up",
             "exchange": "NCCL all_to_all_single of frontier ids per level + all-reduces", "identical_to_single_gpu": bool(okt.item()),
@@ -733,6 +737,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-path and autotuner sections")
     ap.add_argument("--no-other-rmat", action="store_true", help="skip the other R-MAT configuration's section")
+    ap.add_argument("--sharded-workload", default="rmat22", choices=sorted(WORKLOADS),
+                    help="graph of the N > 1 sharded section (one graph over all ranks; default R-MAT scale 22)")
     ap.add_argument("--reference-seconds", type=float, default=100.0,
                     help="--impl reference on graphs above 2^29 edges: stop timing calls after this many seconds (at least one call)")
     ap.add_argument("--batch-graphs", type=int, default=4096, help="graphs of the batch mix (default 4096)")

@@ -73,9 +73,16 @@ def test_trim_1_first(ctx, name, G):
 def test_forward_backward_search(ctx, name, G):
     R = ref()
     bits, sid, pivot = state_after(G, ())
-    if pivot >= G.n:
-        pytest.skip("trim_1_first decided every vertex")
     fwh, fwc, bwh, bwc = device(G)
+    if pivot >= G.n:
+        # trim_1_first decided every vertex: no pivot; the phase call rejects
+        # a pivot >= n with KSPN_ERR_INVALID_ARGUMENT and changes nothing
+        d_bits, d_sid = bits_to_dev(bits), u32_to_dev(sid)
+        with pytest.raises(K.KspnError) as e:
+            ctx.forward_backward_search(G.n, G.m, fwh, fwc, bwh, bwc, d_bits, d_sid, G.n)
+        assert e.value.status == 1
+        assert bits_equal(dev_to_bits(d_bits), bits, G.n)
+        return
     d_bits, d_sid = bits_to_dev(bits), u32_to_dev(sid)
     before = O.bytes_from_bits(bits, G.n).sum()
     R.kref_fw_bw(G.n, G.m, G.fwh, G.fwc, G.bwh, G.bwc, bits, sid, pivot)
