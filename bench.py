@@ -454,11 +454,15 @@ def run_other_rmat(ctx, stream, args, peak, K, name, cpu_sample):
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
 
-        rates = reference_calls(O.Graph(G.n, np.ascontiguousarray(fwh), np.ascontiguousarray(fwc), np.ascontiguousarray(bwh), np.ascontiguousarray(bwc)), 1)
+        HG = O.Graph(G.n, np.ascontiguousarray(fwh), np.ascontiguousarray(fwc), np.ascontiguousarray(bwh), np.ascontiguousarray(bwc))
+        rates = reference_calls(HG, 1)
         if rates is not None:
             cpu = {"value": rates[0], "unit": UNIT, "cores": 1, "kind": "reference",
                    "sample": f"{WORKLOADS[name][2]} (n={G.n}, m={G.m}), the same generator at a quarter of the workload's scale: "
                              "one kaspan::scc call (reference code, 1 rank, 1 core); --impl reference times the workload itself"}
+            # the reference's own sequential Tarjan on the same sample (its oracle)
+            _, secs = O.ref_tarjan(HG)
+            cpu["tarjan"] = {"value": G.m / secs, "unit": UNIT, "cores": 1, "kind": "reference", "what": "kaspan::tarjan (kaspan/scc/tarjan.hpp), one call"}
     del G, out
     torch.cuda.empty_cache()
     return res, cpu
