@@ -119,33 +119,92 @@ k_expand_range(uint32_t u_lo, uint32_t u_hi, uint64_t const* __restrict__ head, 
   }
 }
 
-// Runs of equal keys in one sorted chunk (keys = targets, in CSR order
-// inside a key): first[v] = chunk index of v's first entry.
-__global__ void
-k_run_first(uint32_t n, uint32_t const* __restrict__ keys, uint32_t cnt, uint32_t* __restrict__ first)
+// Offsets of one sorted chunk's entries inside their CSC rows, one block per
+// RO_THREADS * RO_ITEMS consecutive entries (each thread RO_ITEMS of them):
+// an entry's run of equal keys (one target) starts at the largest run start
+// at or before it (a block-wide max-scan; a run that began in an earlier
+// block is found by a binary search over the sorted keys), the run's start
+// reads the target's placed count once and shares it in shared memory, and
+// off[i] = that count + i's rank in the run.  One random read per run
+// instead of two per entry.
+constexpr int RO_THREADS = 256, RO_ITEMS = 8;
+__global__ void __launch_bounds__(RO_THREADS)
+k_run_offsets(uint32_t n, uint32_t const* __restrict__ keys, uint32_t cnt, uint32_t const* __restrict__ indeg, uint32_t* __restrict__ off)
 {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x)
-    if (keys[i] < n && (i == 0 || keys[i - 1] != keys[i])) first[keys[i]] = i;
-}
-
-// off[i] = v's entries placed by earlier chunks + i's rank in its run: the
-// entry's offset inside v's CSC row.
-__global__ void
-k_run_off(uint32_t n, uint32_t const* __restrict__ keys, uint32_t cnt, uint32_t const* __restrict__ first, uint32_t const* __restrict__ indeg, uint32_t* __restrict__ off)
-{
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-    uint32_t const v = keys[i];
-    if (v < n) off[i] = indeg[v] + (i - first[v]);
+  __shared__ uint32_t s_base[RO_THREADS * RO_ITEMS];
+  __shared__ uint32_t s_wmax[RO_THREADS / 32];
+  __shared__ uint32_t s_pre, s_prebase;
+  uint32_t const b0 = blockIdx.x * (RO_THREADS * RO_ITEMS);
+  if (b0 >= cnt) return;
+  uint32_t const i0 = b0 + threadIdx.x * RO_ITEMS;
+  uint32_t       key[RO_ITEMS];
+  uint32_t       last = 0; // largest run start among this thread's items (0: none)
+  bool           has  = false;
+#pragma unroll
+  for (int k = 0; k < RO_ITEMS; ++k) {
+    uint32_t const i = i0 + k;
+    key[k]           = i < cnt ? keys[i] : UNDECIDED;
+    bool const start = i < cnt && (i == 0 || keys[i - 1] != key[k]);
+    if (start) last = i, has = true;
+  }
+  if (threadIdx.x == 0) {
+    // the run holding the block's first entry may have started earlier
+    uint32_t const v = keys[b0];
+    uint32_t       lo = 0, hi = b0; // first index in [0, b0] whose key is v
+    if (b0 > 0 && keys[b0 - 1] == v) {
+      while (lo < hi) {
+        uint32_t const mid = lo + (hi - lo) / 2;
+        if (keys[mid] >= v) hi = mid;
+        else lo = mid + 1;
+      }
+    } else lo = b0;
+    s_pre     = lo;
+    s_prebase = v < n ? indeg[v] : 0u;
+  }
+  // block-wide inclusive max-scan of the threads' last run starts
+  uint32_t incl = has ? last : 0u;
+  unsigned const lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t const y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+    if (lane >= static_cast<unsigned>(d)) incl = max(incl, y);
+  }
+  if (lane == 31) s_wmax[wid] = incl;
+  __syncthreads();
+  uint32_t prev = s_pre; // starts before this thread's first item
+  for (uint32_t w = 0; w < wid; ++w) prev = max(prev, s_wmax[w]);
+  uint32_t const wexcl = __shfl_up_sync(0xFFFFFFFFu, incl, 1);
+  if (lane > 0) prev = max(prev, wexcl);
+  // run starts in this block publish their target's placed count
+  uint32_t gstart[RO_ITEMS];
+  uint32_t cur = prev;
+#pragma unroll
+  for (int k = 0; k < RO_ITEMS; ++k) {
+    uint32_t const i = i0 + k;
+    if (i < cnt && (i == 0 || keys[i - 1] != key[k])) {
+      cur                = i;
+      s_base[i - b0]     = key[k] < n ? indeg[key[k]] : 0u;
+    }
+    gstart[k] = cur;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < RO_ITEMS; ++k) {
+    uint32_t const i = i0 + k;
+    if (i >= cnt || key[k] >= n) continue;
+    uint32_t const base = gstart[k] >= b0 ? s_base[gstart[k] - b0] : s_prebase;
+    off[i]              = base + (i - gstart[k]);
   }
 }
 
-// indeg[v] += the run's length, at each run's last entry
+// placed count of each run's target, after the chunk: its last entry's
+// offset + 1
 __global__ void
-k_run_advance(uint32_t n, uint32_t const* __restrict__ keys, uint32_t cnt, uint32_t const* __restrict__ first, uint32_t* __restrict__ indeg)
+k_run_ends(uint32_t n, uint32_t const* __restrict__ keys, uint32_t cnt, uint32_t const* __restrict__ off, uint32_t* __restrict__ indeg)
 {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
     uint32_t const v = keys[i];
-    if (v < n && (i + 1 == cnt || keys[i + 1] != v)) indeg[v] += i - first[v] + 1;
+    if (v < n && (i + 1 == cnt || keys[i + 1] != v)) indeg[v] = off[i] + 1;
   }
 }
 
@@ -316,7 +375,7 @@ upload_transpose(kspn_context* ctx, uint32_t n, uint64_t m, uint64_t const* h_fh
   size_t const part_n = scan_partial_entries((hist_n > n + 1 ? hist_n : n + 1));
   scratch      sc;
   size_t const band_cap = (BAND_MAX + 1) * ((m + chunk - 1) / chunk);
-  alloc_scratch(ctx, sc, (3 * (m + 64) + 5 * (chunk + 64) + 2 * (static_cast<size_t>(n) + 64) + BAND_MAX + 64 + band_cap + 64) * sizeof(uint32_t) + (hist_n + part_n) * sizeof(uint32_t) + part_n * sizeof(uint64_t) + 16384);
+  alloc_scratch(ctx, sc, (3 * (m + 64) + 5 * (chunk + 64) + (static_cast<size_t>(n) + 64) + BAND_MAX + 64 + band_cap + 64) * sizeof(uint32_t) + (hist_n + part_n) * sizeof(uint32_t) + part_n * sizeof(uint64_t) + 16384);
   size_t    off    = 0;
   uint32_t* skeys  = sc.carve<uint32_t>(off, m);     // chunk-sorted targets
   uint32_t* svals  = sc.carve<uint32_t>(off, m);     // their sources
@@ -327,7 +386,6 @@ upload_transpose(kspn_context* ctx, uint32_t n, uint64_t m, uint64_t const* h_fh
   uint32_t* kb     = sc.carve<uint32_t>(off, chunk);
   uint32_t* vb     = sc.carve<uint32_t>(off, chunk);
   uint32_t* indeg  = sc.carve<uint32_t>(off, n);
-  uint32_t* first  = sc.carve<uint32_t>(off, n);
   uint32_t* hist   = sc.carve<uint32_t>(off, hist_n);
   uint32_t* part   = sc.carve<uint32_t>(off, part_n);
   uint64_t* part64 = sc.carve<uint64_t>(off, part_n);
@@ -348,11 +406,10 @@ upload_transpose(kspn_context* ctx, uint32_t n, uint64_t m, uint64_t const* h_fh
     KSPN_CHECK_LAUNCH();
     radix_sort_pairs_to(ctx, dfc + e0, src, skeys + e0, svals + e0, ka, va, kb, vb, cnt, bits, hist, part);
     unsigned const g = grid_for(cnt, 256);
-    k_run_first<<<g, 256, 0, s>>>(n, skeys + e0, cnt, first);
-    k_run_off<<<g, 256, 0, s>>>(n, skeys + e0, cnt, first, indeg, roff + e0);
-    k_run_advance<<<g, 256, 0, s>>>(n, skeys + e0, cnt, first, indeg);
+    k_run_offsets<<<div_up(cnt, RO_THREADS * RO_ITEMS), RO_THREADS, 0, s>>>(n, skeys + e0, cnt, indeg, roff + e0);
+    k_run_ends<<<g, 256, 0, s>>>(n, skeys + e0, cnt, roff + e0, indeg);
     KSPN_CHECK_LAUNCH();
-    ctx->launches += 4;
+    ctx->launches += 3;
   }
   exclusive_scan<uint64_t>(s, f_array_u32{ indeg }, n, dbh, part64, &ctx->launches);
   // bands of about PLACE_BAND_BYTES of CSC rows; `per` blocks per (band, chunk)
